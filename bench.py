@@ -1,0 +1,445 @@
+"""Benchmark of the reconstruction hot path: SPDHG epochs per second on the B200 (diffractom's SPDHGPoisson with the
+single-phase forward operator), with the CPU oracle timed beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ti256|al99]
+
+A step is one SPDHG epoch (M subset iterations, each a pass over all orientation batches: adjoint of the subset's
+dual change, primal update, forward of the next subset). Workloads are seeded synthetic stand-ins with the shapes
+of the benchmark configurations (no dataset exists for them):
+
+  ti256  256 x 256 pixels, 360 rotation angles over 180 deg, 263 translations, 360 eta bins, 8 rings of hexagonal Ti
+         (a 2.95, c 4.68 A), K = 20000 orientations (sigma 2 deg, random in the fundamental zone), 200 Voronoi grains
+         plus 10 % fine-grained random background, Poisson counts with mean 50, 20 subsets        (the default)
+  al99   99 x 99 pixels, 180 angles over 180 deg, 103 translations, 180 eta bins, 5 rings of cubic Al, K = 1000
+         (sigma 3 deg), 30 grains, mean 100 counts, 10 subsets
+
+Output: one JSON line (rank 0). value = epochs/s of the whole job on device-resident inputs (CUDA events around
+exactly `steps` epochs after `warmup` untimed ones; inputs are larger than L2, which is not flushed); e2e = the same
+metric through the public API (SPDHGPoisson.run on NumPy arrays: uploads, set-up, epochs, downloads); roofline of the
+dominant kernel from CUDA events around its launches inside the timed region; cpu_baseline = the CPU oracle
+(oracle/oracle.c, float32, all host threads) on a bounded sample of the same epoch.
+
+With --gpus N > 1 (torchrun) every rank runs the whole reconstruction on its GPU (independent replicas, weak
+scaling); value is the sum over ranks of epochs / (max over ranks of the time).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SPDHG epochs/s BF16-TC vs FP32 at ≤1e-3 FP64 deviance err; serve p50/p99"
+
+WORKLOADS = {
+    "ti256": dict(cfg=dict(Nx=256, Ny=256, My=263, N_Omega=360, angle_range=[0, 180], cor_offset=0.0, N_eta=360,
+                           eta_angle_range=[0, 360], energy=12.398 / 0.3, k_direction_0=[0, 0, 1],
+                           p_direction_0=[1, 0, 0], detector_direction_origin=[0, -1, 0],
+                           detector_direction_positive_90=[0, 0, -1]),
+                  material=dict(a=2.95, c=4.68, gamma=120, symmetry_group="hexagonal", wavelength_A=0.3,
+                                hkl_list=[[1, 0, 0], [0, 0, 2], [1, 0, 1], [1, 0, 2], [1, 1, 0], [1, 0, 3],
+                                          [2, 0, 0], [1, 1, 2]]),
+                  K=20000, sigma_deg=2.0, grains=200, background=0.10, mean_counts=50.0, subsets=20, epochs=30,
+                  max_gb=8.0),
+    "al99": dict(cfg=dict(Nx=99, Ny=99, My=103, N_Omega=180, angle_range=[0, 180], cor_offset=0.0, N_eta=180,
+                          eta_angle_range=[0, 360], energy=12.398 / 0.3, k_direction_0=[0, 0, 1],
+                          p_direction_0=[1, 0, 0], detector_direction_origin=[0, -1, 0],
+                          detector_direction_positive_90=[0, 0, -1]),
+                 material=dict(a=4.05, symmetry_group="cubic", wavelength_A=0.3,
+                               hkl_list=[[1, 1, 1], [2, 0, 0], [2, 2, 0], [3, 1, 1], [2, 2, 2]]),
+                 K=1000, sigma_deg=3.0, grains=30, background=0.0, mean_counts=100.0, subsets=10, epochs=20,
+                 max_gb=2.0),
+}
+
+
+# ----------------------------------------------------------------------------------------------- workload
+def make_problem(name, seed=0):
+    """(cfg, Material, Grid, workload dict): seeded orientations."""
+    from diffractom_b200 import Grid, Material
+    w = WORKLOADS[name]
+    mat = Material.from_lattice_parameters(**w["material"])
+    grid = Grid.from_random_fundamental_zone(w["K"], mat.crystal_system, np.deg2rad(w["sigma_deg"]), seed=seed)
+    return dict(w["cfg"]), mat, grid, w
+
+
+def phantom(op, w, seed=1):
+    """x_true (K, Ny, Nx) on the device: Voronoi grains in the field of view, one orientation each (weight 1), plus
+    a fraction of the pixels with one more random orientation (weight 0.5)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    supp = op.support_mask()
+    ys, xs = np.nonzero(supp)
+    seeds = rng.choice(len(ys), w["grains"], replace=False)
+    sy, sx = ys[seeds].astype(np.float64), xs[seeds].astype(np.float64)
+    grain_k = rng.choice(op.K, w["grains"], replace=False)
+    yy, xx = np.mgrid[:op.Ny, :op.Nx]
+    d2 = (yy.ravel()[:, None] - sy[None]) ** 2 + (xx.ravel()[:, None] - sx[None]) ** 2
+    owner = grain_k[np.argmin(d2, axis=1)]
+    inside = supp.ravel()
+    x = torch.zeros((op.K, op.Ny * op.Nx), dtype=torch.float32, device=op.device)
+    pix = np.nonzero(inside)[0]
+    x[torch.as_tensor(owner[pix], device=op.device), torch.as_tensor(pix, device=op.device)] = 1.0
+    if w["background"] > 0:
+        bg = rng.choice(pix, int(w["background"] * len(pix)), replace=False)
+        kb = rng.integers(0, op.K, len(bg))
+        x[torch.as_tensor(kb, device=op.device), torch.as_tensor(bg, device=op.device)] += 0.5
+    return x.reshape(op.coeff_shape)
+
+
+def counts(op, x_true, mean, seed=2):
+    """Poisson counts with the given mean of the prediction A x_true (scaled)."""
+    import torch
+    ax = op.direct(x_true)
+    lam = ax * (mean / float(ax.double().mean().item()))
+    g = torch.Generator(device=op.device)
+    g.manual_seed(seed)
+    return torch.poisson(lam, generator=g)
+
+
+# ----------------------------------------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi samples of this GPU's SM clock and throttle reasons while the timed region runs."""
+
+    def __init__(self, index):
+        self.rows = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(index), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            time.sleep(0.3)
+            self.proc.terminate()
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[3:]) if v.lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------------------------------------------- CPU oracle
+def cpu_sample(op, w, sp_seed=0):
+    """One SPDHG iteration of one orientation batch on the CPU oracle (float32, all threads): dual step on one
+    subset's rows, that subset's adjoint (PF product, backprojection), the primal update, the next subset's forward.
+    Returns (seconds per epoch extrapolated: x M subsets x batches, threads, description)."""
+    from oracle.oracle import OracleOperator, _p, lib
+    L = lib()
+    M = w["subsets"]
+    b0 = op.batches[0]
+    kb = b0["K_batch"]
+    subsets = [np.arange(m, op.N_Omega, M) for m in range(M)]
+    sub_a, sub_f = subsets[0], subsets[1]
+    orc = OracleOperator.from_operator(op, precision="f32", batches=[(0, kb)])
+    rows = np.union1d(sub_a, sub_f)
+    # the PF matrix of the sample's angles only (a subset of the rows of the batch's CSR)
+    keep = np.zeros(op.N_Omega, bool)
+    keep[rows] = True
+    orc_rows = OracleOperator(coords=orc.coords[rows], poles=orc.poles, axis_start=orc.axis_start,
+                              axis_count=orc.axis_count, inv_sigma2=orc.inv_sigma2, norm=orc.norm, quad_w=orc.quad_w,
+                              geo=orc.geo[rows], scale=orc.scale, n_taps=orc.n_taps, kernel=orc.kernel, Nx=op.Nx,
+                              Ny=op.Ny, My=op.My, cut=orc.cut, batches=[(0, kb)], precision="f32")
+    ia = np.searchsorted(rows, sub_a)
+    jf = np.searchsorted(rows, sub_f)
+    orc_rows.csr(0, kb)                                    # set-up, not timed
+    rng = np.random.default_rng(0)
+    npix = op.Nx * op.Ny
+    nrow = len(rows)
+    data = rng.random((nrow, op.My, op.N_seg)).astype(np.float32)
+    b = rng.poisson(50, data.shape).astype(np.float32)
+    y = np.zeros_like(data)
+    sig = np.full_like(data, 1e-3)
+    x = rng.random((kb, npix)).astype(np.float32)
+    z = np.zeros_like(x)
+    T = np.full_like(x, 1e-3)
+    t0 = time.perf_counter()
+    om = np.ascontiguousarray(ia, np.int32)
+    row = op.My * op.N_seg
+    L.orc_dual_update_sub(_p(y), _p(data), _p(sig), _p(b), None, 0, None, 0, None, 0, 1e-3, _p(om), row,
+                          len(om) * row)
+    t_dual = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    dz = orc_rows.adjoint(data, subset=ia).reshape(kb, npix)
+    L.orc_spdhg_update(_p(x), _p(z), _p(T), _p(np.ascontiguousarray(dz)), float(M), 0.0, x.size)
+    orc_rows.forward(x, subset=jf, data=data)
+    t_batch = time.perf_counter() - t1
+    n_batches = -(-op.K // kb)
+    per_epoch = M * (t_dual + n_batches * t_batch)
+    threads = int(L.orc_num_threads())
+    desc = (f"1 SPDHG iteration (subset of {len(sub_a)} angles) of 1 orientation batch ({kb} of {op.K}), "
+            f"extrapolated x {M} subsets x {n_batches} batches; dual step per subset")
+    return per_epoch, threads, desc, time.perf_counter() - t0
+
+
+# ----------------------------------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="ti256", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    a = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    if a.impl == "reference":
+        return run_reference(a, rank)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    from diffractom_b200 import SPDHGPoisson, SinglePhaseForwardOperator
+    from diffractom_b200 import _lib
+    cfg, mat, grid, w = make_problem(a.workload)
+    t_build = time.perf_counter()
+    op = SinglePhaseForwardOperator(cfg, mat, grid, w["max_gb"], normalized=True)
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t_build
+    x_true = phantom(op, w)
+    b = counts(op, x_true, w["mean_counts"])
+    del x_true
+    torch.cuda.empty_cache()
+
+    sp = SPDHGPoisson(op, subsets=w["subsets"], seed=0)
+    x0 = torch.zeros(op.coeff_shape, dtype=torch.float32, device=op.device)
+    sp._setup(x0, b)
+    never = 1 << 30
+    sp._iterate(a.warmup, diagnostics_interval=never, final=False)
+    stream = op.stream()
+    timers = KernelTimers(op)
+    stream.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = Clocks(local)
+    n0 = _lib.lib().dfx_launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    timers.on()
+    sp._iterate(a.steps, diagnostics_interval=never, final=False)
+    timers.off()
+    end.record(stream)
+    end.synchronize()
+    launches = _lib.lib().dfx_launch_count() - n0 - timers.n_extra
+    clk = clocks.stop()
+    ms = start.elapsed_time(end)
+    t_max = ms
+    if dist is not None:
+        tt = torch.tensor([ms], device=op.device, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+        dist.barrier()
+    value = world * a.steps / (t_max / 1e3)
+    # deviance of the iterate after warm-up + timed epochs (float64 reduction)
+    D = torch.empty(op.data_shape, dtype=torch.float32, device=op.device)
+    op.direct_cl(sp.x, D)
+    f_final = sp._deviance(D)
+    sp._finish()
+    roof = timers.roofline(op)
+
+    e2e = None
+    if not a.no_e2e:
+        e2e = measure_e2e(op, w, b, a.steps)
+    cpu = None
+    if rank == 0 and not a.no_cpu:
+        per_epoch, threads, desc, took = cpu_sample(op, w)
+        cpu = {"value": 1.0 / per_epoch, "unit": "epochs/s", "cores": threads, "kind": "port",
+               "sample": desc + f" ({took:.1f} s of CPU time)"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "epochs/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson counts)",
+            "config": {"workload": a.workload, "K": op.K, "pixels": f"{op.Nx}x{op.Ny}", "N_Omega": op.N_Omega,
+                       "My": op.My, "N_eta": op.N_eta, "rings": op.N_peaks, "subsets": w["subsets"],
+                       "batches": len(op.batches), "K_batch_max": op.K_batch_max, "pf_mode": op.pf_mode,
+                       "pf_nnz": op.sparse_nnz, "precision_path": "fp32", "l2": "inputs larger than L2, no flush",
+                       "parallelism": f"replicas x{world}", "operator_build_s": round(t_build, 2),
+                       "final_deviance_f64": f_final},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+class KernelTimers:
+    """CUDA events around the launches of chosen kernels inside the timed region (same stream), for the roofline."""
+
+    NAMES = ("dfx_radon_forward", "dfx_radon_backward", "dfx_spmm_pf_forward", "dfx_spmm_pf_adjoint",
+             "dfx_gather_channels", "dfx_scatter_channels", "dfx_spdhg_primal_update", "dfx_spdhg_dual_update")
+
+    def __init__(self, op):
+        self.op = op
+        self.events = {n: [] for n in self.NAMES}
+        self.args = {n: [] for n in self.NAMES}
+        self.n_extra = 0
+        self._orig = op._call
+
+    def on(self):
+        import torch
+        op = self.op
+
+        def call(name, *args):
+            if name in self.events:
+                s = op.stream()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+                self._orig(name, *args)
+                e1.record(s)
+                self.events[name].append((e0, e1))
+                self.args[name].append(args)
+            else:
+                self._orig(name, *args)
+        op._call = call
+
+    def off(self):
+        self.op._call = self._orig
+
+    def roofline(self, op):
+        import torch
+        torch.cuda.synchronize()
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() \
+            else {}
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        per = {}
+        for n, evs in self.events.items():
+            if evs:
+                per[n] = [e0.elapsed_time(e1) for e0, e1 in evs]
+        tot = {n: sum(v) for n, v in per.items()}
+        dom = max(tot, key=tot.get)
+        ms = float(np.mean(per[dom]))
+        nbytes, flops = algorithmic_work(op, dom, self.args[dom])
+        achieved = nbytes / (ms / 1e3) / 1e9
+        share = {n: round(t / sum(tot.values()), 4) for n, t in sorted(tot.items(), key=lambda t: -t[1])}
+        fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12          # FP32 FMA lanes x 2 flops x max SM clock (TFLOP/s)
+        return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                "mean_launch_ms": ms, "launches": len(per[dom]),
+                "fp32_tflops": flops / (ms / 1e3) / 1e12 if flops else None, "fp32_peak_tflops_nominal": fp32_peak,
+                "fp32_frac_of_nominal": (flops / (ms / 1e3) / 1e12) / fp32_peak if flops else None,
+                "time_share_of_timed_kernels": share}
+
+
+def algorithmic_work(op, name, args_list):
+    """(bytes, flops) per launch (mean over the recorded launches) of a kernel: its own inputs + outputs once, and the
+    multiply-adds of its non-zero taps / entries (an FMA = 2 flops)."""
+    nb, nf = [], []
+    npix = op.Nx * op.Ny
+    for args in args_list:
+        if name in ("dfx_radon_forward", "dfx_radon_backward"):
+            n_ang, kb = args[3], args[8]
+            nb.append(4 * kb * (npix + n_ang * op.My))
+            nf.append(2 * 2 * npix * n_ang * kb)            # ~2 taps per pixel and angle
+        elif name in ("dfx_spmm_pf_forward", "dfx_spmm_pf_adjoint"):
+            n_sub = args[6]
+            kb = args[10] if name == "dfx_spmm_pf_forward" else args[8]
+            frac = n_sub / op.N_Omega
+            nnz = sum(sb["nnz"] for sb in op.sparse_batches) / len(op.sparse_batches) * frac
+            nb.append(4 * n_sub * op.My * (kb + 2 * op.N_seg) + 6 * nnz)
+            nf.append(2 * nnz * op.My)
+        elif name in ("dfx_gather_channels", "dfx_scatter_channels"):
+            nb.append(2 * 4 * npix * args[4])
+            nf.append(0)
+        elif name == "dfx_spdhg_primal_update":
+            nb.append(4 * 6 * args[6])
+            nf.append(0)
+        else:
+            nb.append(4 * 7 * args[12] * args[13])
+            nf.append(0)
+    return float(np.mean(nb)), float(np.mean(nf))
+
+
+def measure_e2e(op, w, b_dev, steps):
+    """The metric through the public API on host arrays: SPDHGPoisson.run(NumPy x0, NumPy b, steps epochs)."""
+    import torch
+    from diffractom_b200 import SPDHGPoisson
+    b_host = torch.empty(b_dev.shape, dtype=torch.float32, pin_memory=True)
+    b_host.copy_(b_dev)
+    b_np = b_host.numpy()
+    x0 = np.zeros(op.coeff_shape, np.float32)
+    sp = SPDHGPoisson(op, subsets=w["subsets"], seed=0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    x = sp.run(x0, b_np, steps, diagnostics_interval=steps)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    h2d = b_np.nbytes + x0.nbytes
+    d2h = x.nbytes + sp.state["y"].nbytes + sp.state["z"].nbytes
+    return {"value": steps / dt, "unit": "epochs/s", "h2d_bytes_per_step": h2d // steps,
+            "d2h_bytes_per_step": d2h // steps,
+            "includes": "upload of x0 and b, step sizes S and T (1 forward + M subset adjoints), epochs, final "
+                        "deviance, download of x, y, z"}
+
+
+def run_reference(a, rank):
+    """The reference arm: diffractom's path on the host cores. The reference is Python + OpenCL; no OpenCL runtime
+    exists here, so its CPU restatement (oracle/, float32, all threads) is timed: each step is the bounded sample of
+    cpu_sample, extrapolated to a full epoch."""
+    if rank != 0:
+        return 0
+    import torch
+    from diffractom_b200.geometry import OperatorGeometry
+    cfg, mat, grid, w = make_problem(a.workload)
+    geom = OperatorGeometry(cfg, mat, grid, normalized=True)
+    kb = min(256, geom.K)
+    geom.batches = [{"k_start": k0, "K_batch": min(kb, geom.K - k0)} for k0 in range(0, geom.K, kb)]
+    for _ in range(max(0, min(a.warmup, 1))):
+        cpu_sample(geom, w)
+    per = []
+    took = 0.0
+    for _ in range(max(1, min(a.steps, 3))):
+        pe, threads, desc, t = cpu_sample(geom, w)
+        per.append(pe)
+        took += t
+    per_epoch = float(np.mean(per))
+    value = 1.0 / per_epoch
+    line = {"metric": METRIC, "value": value, "unit": "epochs/s", "n_gpus": 0, "steps": len(per),
+            "warmup": a.warmup, "ms_per_step": per_epoch * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": a.workload, "K": geom.K, "pixels": f"{geom.Nx}x{geom.Ny}",
+                       "subsets": w["subsets"]},
+            "cpu_baseline": {"value": value, "unit": "epochs/s", "cores": threads, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": "epochs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "diffractom runs its path as OpenCL kernels (pyopencl); no OpenCL runtime or pyopencl is "
+                    "installed, so the timed reference is its CPU restatement in oracle/ (float32, OpenMP)"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

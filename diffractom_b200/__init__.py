@@ -1,0 +1,25 @@
+"""diffractom_b200: diffractom's reconstruction hot path (the single-phase forward operator, its adjoint and the
+SPDHG / FISTA Poisson solvers) as hand-written sm_100a CUDA kernels behind a C ABI, with diffractom's Python API.
+
+    from diffractom_b200 import Material, Grid, SinglePhaseForwardOperator, SPDHGPoisson
+
+Device arrays are CUDA torch tensors (float32, contiguous) in place of pyopencl arrays; NumPy arrays are accepted
+where diffractom accepts them. The CUDA library is built in-tree by `python -m diffractom_b200.build`.
+"""
+from .grid import Grid, MatrixGrid
+from .material import Material, group_reflections_into_rings
+from .quadrature import QuadratureRule
+
+__all__ = ["Grid", "MatrixGrid", "Material", "QuadratureRule", "group_reflections_into_rings",
+           "SinglePhaseForwardOperator", "SPDHGPoisson", "estimate_L_power"]
+
+
+def __getattr__(name):
+    # the device classes import torch and the CUDA library only when used
+    if name in ("SinglePhaseForwardOperator", "estimate_L_power"):
+        from . import operator
+        return getattr(operator, name)
+    if name == "SPDHGPoisson":
+        from .spdhg import SPDHGPoisson
+        return SPDHGPoisson
+    raise AttributeError(name)

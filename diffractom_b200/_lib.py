@@ -1,0 +1,99 @@
+"""ctypes binding of the C ABI (include/diffractom_b200.h) implemented by diffractom_b200/_lib/libdfx_b200.so.
+
+There is no fallback: if the library is missing (python -m diffractom_b200.build makes it) or cannot be loaded,
+every operator call fails with an ImportError. Status codes become the exception types of the reference's Python
+API: bad arguments ValueError, scratch too small MemoryError, launch / CUDA errors RuntimeError, a device-side wait
+that ran out TimeoutError.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_double, c_float, c_int, c_int32, c_int64, c_size_t, c_void_p
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libdfx_b200.so"
+
+DFX_OK, DFX_EINVAL, DFX_ENOMEM, DFX_ELAUNCH, DFX_ETIMEOUT, DFX_ECUDA = range(6)
+ABI_VERSION = 1
+
+
+class PFGeometry(ctypes.Structure):
+    """dfx_pf_geometry: device pointers of the operator's PF inputs and their sizes."""
+    _fields_ = [("coords", c_void_p), ("poles", c_void_p), ("axis_start", c_void_p), ("axis_count", c_void_p),
+                ("inv_sigma2", c_void_p), ("norm", c_void_p), ("quad_w", c_void_p), ("intens", c_void_p),
+                ("R", c_int32), ("C", c_int32), ("P", c_int32), ("A", c_int32), ("S", c_int32),
+                ("S_eta", c_int32), ("K", c_int32), ("cut", c_float)]
+
+
+P, I, L, F, S = c_void_p, c_int, c_int64, c_float, c_void_p   # pointer, int, int64, float, stream
+SIGNATURES = {
+    "dfx_abi_version": ([], c_int),
+    "dfx_last_error": ([], ctypes.c_char_p),
+    "dfx_launch_count": ([], ctypes.c_uint64),
+    "dfx_gather_channels": ([P, P, L, I, I, I, S], c_int),
+    "dfx_scatter_channels": ([P, P, L, I, I, I, S], c_int),
+    "dfx_radon_forward": ([P, P, P, I, I, I, I, I, I, I, F, S], c_int),
+    "dfx_radon_backward": ([P, P, P, I, I, I, I, I, I, I, I, S], c_int),
+    "dfx_pf_dense": ([POINTER(PFGeometry), I, I, P, S], c_int),
+    "dfx_pf_csr_count": ([POINTER(PFGeometry), P, I, I, I, I, P, S], c_int),
+    "dfx_pf_csr_fill": ([POINTER(PFGeometry), P, I, I, I, I, P, P, P, S], c_int),
+    "dfx_scan_scratch_bytes": ([L], c_size_t),
+    "dfx_scan_exclusive_i32": ([P, P, L, P, c_size_t, S], c_int),
+    "dfx_spmm_pf_forward": ([P, P, P, P, P, P, I, I, I, I, I, I, S], c_int),
+    "dfx_spmm_pf_adjoint": ([P, P, P, P, P, P, I, I, I, I, I, F, I, S], c_int),
+    "dfx_zero_rows": ([P, P, I, L, S], c_int),
+    "dfx_fill_f32": ([P, F, L, S], c_int),
+    "dfx_spdhg_dual_update": ([P, P, P, P, P, L, P, L, P, L, F, P, I, L, S], c_int),
+    "dfx_spdhg_primal_update": ([P, P, P, P, F, F, L, S], c_int),
+    "dfx_dual_steps": ([P, P, P, L, F, L, S], c_int),
+    "dfx_set_mask_ones": ([P, P, L, L, S], c_int),
+    "dfx_tinit": ([P, L, S], c_int),
+    "dfx_tmin": ([P, P, P, L, F, L, S], c_int),
+    "dfx_tfinal": ([P, L, S], c_int),
+    "dfx_support_ones": ([P, P, L, L, S], c_int),
+    "dfx_project_support": ([P, P, L, L, S], c_int),
+    "dfx_reduce_scratch_bytes": ([L], c_size_t),
+    "dfx_poisson_value_grad": ([P, P, P, L, P, L, P, L, F, I, I, F, L, P, P, c_size_t, S], c_int),
+    "dfx_mean_counted": ([P, P, L, L, P, P, c_size_t, S], c_int),
+    "dfx_dot_f64": ([P, P, L, P, P, c_size_t, S], c_int),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded library (ImportError if it is missing or does not export the ABI)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"the CUDA library {LIB_PATH} is missing: build it with `python -m diffractom_b200.build`")
+    try:
+        h = ctypes.CDLL(str(LIB_PATH))
+    except OSError as e:
+        raise ImportError(f"cannot load {LIB_PATH}: {e}") from e
+    for name, (args, res) in SIGNATURES.items():
+        f = getattr(h, name, None)
+        if f is None:
+            raise ImportError(f"{LIB_PATH} does not export {name}")
+        f.argtypes = args
+        f.restype = res
+    if h.dfx_abi_version() != ABI_VERSION:
+        raise ImportError(f"{LIB_PATH}: ABI version {h.dfx_abi_version()}, expected {ABI_VERSION}")
+    _lib = h
+    return h
+
+
+_EXC = {DFX_EINVAL: ValueError, DFX_ENOMEM: MemoryError, DFX_ELAUNCH: RuntimeError, DFX_ETIMEOUT: TimeoutError,
+        DFX_ECUDA: RuntimeError}
+
+
+def check(status: int) -> None:
+    if status != DFX_OK:
+        msg = lib().dfx_last_error().decode(errors="replace")
+        raise _EXC.get(status, RuntimeError)(msg or f"diffractom_b200 error {status}")
+
+
+def call(name: str, *args) -> None:
+    """Call an entry point that returns a status; raise on error."""
+    check(getattr(lib(), name)(*args))

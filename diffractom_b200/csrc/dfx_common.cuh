@@ -1,0 +1,60 @@
+// Shared pieces of the sm_100a kernels of diffractom_b200: status codes, the per-thread error message, launch
+// checks and the float32 arithmetic conventions that the CPU oracle restates bit for bit.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "../../include/diffractom_b200.h"
+
+namespace dfx {
+
+// Last error message of the calling host thread (dfx_last_error returns it).
+void set_error(const char *fmt, ...);
+
+// Status of the launch just issued on the calling thread (cudaGetLastError), with the kernel's name.
+int launch_status(const char *what);
+
+inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+#define DFX_REQUIRE(cond, ...)                  \
+    do {                                        \
+        if (!(cond)) {                          \
+            ::dfx::set_error(__VA_ARGS__);      \
+            return DFX_EINVAL;                  \
+        }                                       \
+    } while (0)
+
+// ---- detector coordinate and tap weight of the parallel-beam projector (the oracle's convention) ----
+// Rows run along the image axis with the larger coefficient |X| or |Y| (A); t = A u + (B v + T0) with two
+// correctly rounded fused multiply-adds, so forward and backward projection see the same t and the same weights.
+struct AngleGeo {
+    float A, B, T0, w;     // row-axis coefficient, column coefficient, offset, angle weight
+    int rows_are_y;        // 1: u = x (rows of constant y), 0: u = y
+    float hw, top, iw;     // trapezoid: half width (1 + |A|) / 2, plateau min(1, |A|), 1 / |A|
+};
+
+__device__ __forceinline__ AngleGeo load_geo(const float4 *geo, int a) {
+    const float4 g = __ldg(geo + a);
+    AngleGeo o;
+    o.rows_are_y = fabsf(g.x) >= fabsf(g.y);
+    o.A = o.rows_are_y ? g.x : g.y;
+    o.B = o.rows_are_y ? g.y : g.x;
+    o.T0 = g.z;
+    o.w = g.w;
+    const float aA = fabsf(o.A);
+    o.hw = __fmul_rn(0.5f, __fadd_rn(1.0f, aA));
+    o.top = fminf(1.0f, aA);
+    o.iw = __frcp_rn(aA);
+    return o;
+}
+
+// K(d) for d = t - s: trapezoid (kernel 1) or hat (kernel 0).
+template <int KERNEL>
+__device__ __forceinline__ float tap_weight(const AngleGeo &g, float d) {
+    if (KERNEL == 1) return __fmul_rn(fminf(fmaxf(__fsub_rn(g.hw, fabsf(d)), 0.0f), g.top), g.iw);
+    return fmaxf(__fsub_rn(1.0f, fabsf(d)), 0.0f);
+}
+
+}  // namespace dfx

@@ -1,0 +1,431 @@
+// Pole-figure (PF) matrix of the single-phase operator on sm_100a: entry evaluation, CSR construction, and the two
+// sparse products with the channel-fastest sinogram batch (FP32).
+//
+// CSR construction: one warp per CSR row. The lanes evaluate the row's 32 next entries in column order, a ballot
+// orders the non-zeros, so every row is written in ascending column order and the structure is a pure function of
+// the float32 entry values: the CSR of the dense batch, bit for bit, with no sort and no atomics. Adjoint rows
+// (angle, orientation) run over the segments j = c * P + p; forward rows (angle, segment) over the orientations.
+//
+// Products: a block owns one angle, TY detector positions and 128 CSR rows (one per thread). The dense operand of
+// the block (TY lines of the sinogram or of the data) is staged in shared memory a chunk of columns at a time,
+// transposed so that the TY values of one column are contiguous (float4 reads); every CSR entry is read once per
+// block and used TY times from a register.
+#include "dfx_common.cuh"
+
+namespace dfx {
+
+__device__ __forceinline__ float pf_entry(const dfx_pf_geometry &g, int r, int kg, int c, int p)
+{
+    const int a0 = __ldg(g.axis_start + p), a1 = __ldg(g.axis_start + p + 1);
+    const float *pole = g.poles + (int64_t)kg * g.A * 3;
+    const float inv = __ldg(g.inv_sigma2 + kg);
+    float w_total = 0.0f;
+    for (int s = 0; s < g.S; ++s)
+        for (int se = 0; se < g.S_eta; ++se) {
+            const float *v = g.coords + ((((int64_t)(r * g.S + s) * g.C + c) * g.S_eta + se) * g.P + p) * 3;
+            const float vx = __ldg(v), vy = __ldg(v + 1), vz = __ldg(v + 2);
+            float w_node = 0.0f;
+            for (int a = a0; a < a1; ++a) {
+                const float nx = __ldg(pole + 3 * a), ny = __ldg(pole + 3 * a + 1), nz = __ldg(pole + 3 * a + 2);
+                const float d = fabsf(__fmaf_rn(nz, vz, __fmaf_rn(ny, vy, __fmul_rn(nx, vx))));
+                float t = 0.0f;
+                const float e1 = __fmul_rn(__fsub_rn(1.0f, d), inv);
+                if (e1 < g.cut) t = __fadd_rn(t, expf(-e1));
+                const float e2 = __fmul_rn(__fadd_rn(1.0f, d), inv);
+                if (e2 < g.cut) t = __fadd_rn(t, expf(-e2));
+                w_node = __fmaf_rn(__ldg(g.axis_count + a), t, w_node);
+            }
+            if (g.quad_w) w_total = __fmaf_rn(__ldg(g.quad_w + s * g.S_eta + se), w_node, w_total);
+            else w_total = __fadd_rn(w_total, w_node);
+        }
+    const float norm = __ldg(g.norm + kg);
+    float val = g.quad_w ? __fmul_rn(w_total, norm) : __fmul_rn(__fdiv_rn(w_total, (float)(g.S * g.S_eta)), norm);
+    if (g.intens) val = __fmul_rn(val, __ldg(g.intens + p));
+    return val;
+}
+
+__global__ void pf_dense_kernel(dfx_pf_geometry g, int k0, int kb, float *__restrict__ out)
+{
+    const int64_t total = (int64_t)g.R * kb * g.C * g.P;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int p = (int)(i % g.P);
+        int64_t t = i / g.P;
+        const int c = (int)(t % g.C);
+        t /= g.C;
+        const int k = (int)(t % kb);
+        const int r = (int)(t / kb);
+        out[i] = pf_entry(g, r, k0 + k, c, p);
+    }
+}
+
+// One warp per CSR row: FILL = 0 counts the row's non-zeros, FILL = 1 writes them in column order.
+template <int FWD, int FILL>
+__global__ void __launch_bounds__(256) pf_csr_kernel(dfx_pf_geometry g, const int32_t *__restrict__ rows, int n_rows,
+                                                     int k0, int kb, int32_t *__restrict__ counts,
+                                                     const int32_t *__restrict__ row_ptr, uint16_t *__restrict__ col,
+                                                     float *__restrict__ val)
+{
+    const int lane = threadIdx.x & 31;
+    const int CP = g.C * g.P;
+    const int64_t n_csr = (int64_t)n_rows * (FWD ? CP : kb);
+    const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= n_csr) return;
+    const int s = (int)(row / (FWD ? CP : kb));
+    const int q = (int)(row % (FWD ? CP : kb));        // orientation (adjoint rows) or segment (forward rows)
+    const int r = rows ? __ldg(rows + s) : s;
+    const int n_cols = FWD ? kb : CP;
+    int pos = FILL ? __ldg(row_ptr + row) : 0;
+    const int end = FILL ? __ldg(row_ptr + row + 1) : 0;   // writes stay inside the row whatever happens
+    int n = 0;
+    for (int base = 0; base < n_cols; base += 32) {
+        const int col_i = base + lane;
+        float v = 0.0f;
+        if (col_i < n_cols) {
+            if (FWD) v = pf_entry(g, r, k0 + col_i, q / g.P, q % g.P);
+            else v = pf_entry(g, r, k0 + q, col_i / g.P, col_i % g.P);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, v != 0.0f);
+        if (FILL && v != 0.0f) {
+            const int o = pos + __popc(m & ((1u << lane) - 1u));
+            if (o < end) {
+                col[o] = (uint16_t)col_i;
+                val[o] = v;
+            }
+        }
+        pos += __popc(m);
+        n += __popc(m);
+    }
+    if (!FILL && lane == 0) counts[row] = n;
+}
+
+// ---- exclusive scan of int32 (three passes: tile sums, scan of the tile sums, tile scans) ----
+constexpr int SCAN_THREADS = 256, SCAN_PER = 8, SCAN_TILE = SCAN_THREADS * SCAN_PER;
+
+__device__ __forceinline__ int block_exclusive(int x, int *sh, int *total)
+{
+    // exclusive scan over the block of one value per thread
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) sh[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        int w = lane < (SCAN_THREADS >> 5) ? sh[lane] : 0;
+        int wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        if (lane < (SCAN_THREADS >> 5)) sh[lane] = wi - w;
+        if (lane == (SCAN_THREADS >> 5) - 1) *total = wi;
+    }
+    __syncthreads();
+    const int r = sh[wid] + inc - x;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) scan_tile_sums(const int32_t *__restrict__ in, int64_t n,
+                                                              int32_t *__restrict__ sums)
+{
+    __shared__ int sh[32];
+    __shared__ int tot;
+    const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_PER;
+    int s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_PER; ++i) s += (base + i < n) ? in[base + i] : 0;
+    block_exclusive(s, sh, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) scan_sums(int32_t *__restrict__ sums, int64_t n_tiles,
+                                                         int32_t *__restrict__ out_total)
+{
+    __shared__ int sh[32];
+    __shared__ int tot;
+    int carry = 0;
+    for (int64_t b = 0; b < n_tiles; b += SCAN_THREADS) {
+        const int64_t i = b + threadIdx.x;
+        const int x = i < n_tiles ? sums[i] : 0;
+        const int e = block_exclusive(x, sh, &tot);
+        if (i < n_tiles) sums[i] = carry + e;
+        carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out_total = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) scan_tiles(const int32_t *in, int64_t n,
+                                                          const int32_t *__restrict__ sums, int32_t *out)
+{
+    __shared__ int sh[32];
+    __shared__ int tot;
+    const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_PER;
+    int v[SCAN_PER];
+    int s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_PER; ++i) {
+        v[i] = (base + i < n) ? in[base + i] : 0;
+        s += v[i];
+    }
+    int e = block_exclusive(s, sh, &tot) + sums[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < SCAN_PER; ++i) {
+        if (base + i < n) out[base + i] = e;
+        e += v[i];
+    }
+}
+
+// ---- sparse products ----
+constexpr int SP_THREADS = 128;   // CSR rows per block
+constexpr int TY = 16;            // detector positions per block
+constexpr int TYP = TY + 4;       // padded column of the staged tile (keeps float4 alignment)
+constexpr int CHUNK = 512;        // columns staged per pass (CHUNK * TYP * 4 = 40 KB)
+
+__global__ void __launch_bounds__(SP_THREADS) spmm_forward_kernel(
+    const float *__restrict__ sino, const int32_t *__restrict__ row_ptr, const uint16_t *__restrict__ col_k,
+    const float *__restrict__ val, float *__restrict__ data, const int32_t *__restrict__ omegas, int my, int cp,
+    int kstride, int kb, int compact)
+{
+    __shared__ __align__(16) float lz[CHUNK * TYP];
+    const int j = blockIdx.x * SP_THREADS + threadIdx.x;
+    const int y0 = blockIdx.y * TY;
+    const int s = blockIdx.z;
+    const int r = omegas ? __ldg(omegas + s) : s;
+    const int ny = min(TY, my - y0);
+    const int64_t rr = (int64_t)(compact ? s : r) * cp + j;
+    int i = 0, e = 0;
+    if (j < cp) { i = __ldg(row_ptr + rr); e = __ldg(row_ptr + rr + 1); }
+    const bool nonempty = i < e;
+    float acc[TY];
+#pragma unroll
+    for (int t = 0; t < TY; ++t) acc[t] = 0.0f;
+    const float *zl = sino + ((int64_t)s * my + y0) * kstride;
+    for (int k0 = 0; k0 < kb; k0 += CHUNK) {
+        const int kn = min(CHUNK, kb - k0);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < TY * kn; idx += SP_THREADS) {
+            const int t = idx / kn, kk = idx - t * kn;
+            lz[kk * TYP + t] = t < ny ? __ldg(zl + (int64_t)t * kstride + k0 + kk) : 0.0f;
+        }
+        __syncthreads();
+        const int k1 = k0 + kn;
+        for (; i < e; ++i) {
+            const int k = __ldg(col_k + i);
+            if (k >= k1) break;
+            const float v = __ldg(val + i);
+            const float4 *z4 = reinterpret_cast<const float4 *>(lz + (k - k0) * TYP);
+#pragma unroll
+            for (int q = 0; q < TY / 4; ++q) {
+                const float4 z = z4[q];
+                acc[4 * q + 0] = __fmaf_rn(v, z.x, acc[4 * q + 0]);
+                acc[4 * q + 1] = __fmaf_rn(v, z.y, acc[4 * q + 1]);
+                acc[4 * q + 2] = __fmaf_rn(v, z.z, acc[4 * q + 2]);
+                acc[4 * q + 3] = __fmaf_rn(v, z.w, acc[4 * q + 3]);
+            }
+        }
+    }
+    if (j < cp && nonempty) {
+        float *dl = data + ((int64_t)r * my + y0) * cp + j;
+#pragma unroll
+        for (int t = 0; t < TY; ++t)
+            if (t < ny) dl[(int64_t)t * cp] += acc[t];
+    }
+}
+
+__global__ void __launch_bounds__(SP_THREADS) spmm_adjoint_kernel(
+    const float *__restrict__ data, const int32_t *__restrict__ row_ptr, const uint16_t *__restrict__ col_j,
+    const float *__restrict__ val, float *__restrict__ sino, const int32_t *__restrict__ omegas, int my, int kb,
+    int cp, int kstride, float alpha, int compact)
+{
+    __shared__ __align__(16) float ld[CHUNK * TYP];
+    const int k = blockIdx.x * SP_THREADS + threadIdx.x;
+    const int y0 = blockIdx.y * TY;
+    const int s = blockIdx.z;
+    const int r = omegas ? __ldg(omegas + s) : s;
+    const int ny = min(TY, my - y0);
+    int i = 0, e = 0;
+    if (k < kb) {
+        const int64_t rr = (int64_t)(compact ? s : r) * kb + k;
+        i = __ldg(row_ptr + rr);
+        e = __ldg(row_ptr + rr + 1);
+    }
+    float acc[TY];
+#pragma unroll
+    for (int t = 0; t < TY; ++t) acc[t] = 0.0f;
+    const float *dl = data + ((int64_t)r * my + y0) * cp;
+    for (int j0 = 0; j0 < cp; j0 += CHUNK) {
+        const int jn = min(CHUNK, cp - j0);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < TY * jn; idx += SP_THREADS) {
+            const int t = idx / jn, jj = idx - t * jn;
+            ld[jj * TYP + t] = t < ny ? __ldg(dl + (int64_t)t * cp + j0 + jj) : 0.0f;
+        }
+        __syncthreads();
+        const int j1 = j0 + jn;
+        for (; i < e; ++i) {
+            const int j = __ldg(col_j + i);
+            if (j >= j1) break;
+            const float v = __ldg(val + i);
+            const float4 *d4 = reinterpret_cast<const float4 *>(ld + (j - j0) * TYP);
+#pragma unroll
+            for (int q = 0; q < TY / 4; ++q) {
+                const float4 d = d4[q];
+                acc[4 * q + 0] = __fmaf_rn(v, d.x, acc[4 * q + 0]);
+                acc[4 * q + 1] = __fmaf_rn(v, d.y, acc[4 * q + 1]);
+                acc[4 * q + 2] = __fmaf_rn(v, d.z, acc[4 * q + 2]);
+                acc[4 * q + 3] = __fmaf_rn(v, d.w, acc[4 * q + 3]);
+            }
+        }
+    }
+    if (k < kstride) {
+        float *zl = sino + ((int64_t)s * my + y0) * kstride + k;
+#pragma unroll
+        for (int t = 0; t < TY; ++t)
+            if (t < ny) zl[(int64_t)t * kstride] = k < kb ? alpha * acc[t] : 0.0f;
+    }
+}
+
+__global__ void zero_rows_kernel(float *__restrict__ data, const int32_t *__restrict__ omegas, int n_sub,
+                                 int64_t row_len)
+{
+    const int64_t n = (int64_t)n_sub * row_len;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = i / row_len;
+        data[(int64_t)__ldg(omegas + s) * row_len + (i - s * row_len)] = 0.0f;
+    }
+}
+
+static int check_geometry(const dfx_pf_geometry *g)
+{
+    DFX_REQUIRE(g && g->coords && g->poles && g->axis_start && g->axis_count && g->inv_sigma2 && g->norm,
+                "pf: geometry has null pointers");
+    DFX_REQUIRE(g->R > 0 && g->C > 0 && g->P > 0 && g->A > 0 && g->S > 0 && g->S_eta > 0 && g->K > 0,
+                "pf: bad geometry sizes");
+    return DFX_OK;
+}
+
+static unsigned grid_for(int64_t n, int threads)
+{
+    const int64_t b = cdiv(n, threads);
+    return (unsigned)(b < 148 * 64 ? (b > 0 ? b : 1) : 148 * 64);
+}
+
+}  // namespace dfx
+
+using namespace dfx;
+
+extern "C" int dfx_pf_dense(const dfx_pf_geometry *g, int k0, int kb, float *out, void *stream)
+{
+    int st = check_geometry(g);
+    if (st) return st;
+    DFX_REQUIRE(out && k0 >= 0 && kb > 0 && k0 + kb <= g->K, "pf_dense: bad batch");
+    const int64_t n = (int64_t)g->R * kb * g->C * g->P;
+    pf_dense_kernel<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(*g, k0, kb, out);
+    return launch_status("pf_dense");
+}
+
+static int pf_csr(const dfx_pf_geometry *g, const int32_t *rows, int n_rows, int k0, int kb, int fwd, int fill,
+                  int32_t *counts, const int32_t *row_ptr, uint16_t *col, float *val, void *stream)
+{
+    int st = check_geometry(g);
+    if (st) return st;
+    DFX_REQUIRE(n_rows > 0 && k0 >= 0 && kb > 0 && k0 + kb <= g->K, "pf_csr: bad batch (rows %d, k0 %d, kb %d, K %d)",
+                n_rows, k0, kb, g->K);
+    DFX_REQUIRE(kb <= 65536 && (int64_t)g->C * g->P <= 65536, "pf_csr: columns exceed the 16-bit index range");
+    DFX_REQUIRE(fill ? (row_ptr && col && val) : (counts != nullptr), "pf_csr: null output");
+    const int64_t n_csr = (int64_t)n_rows * (fwd ? (int64_t)g->C * g->P : kb);
+    const int warps = 8;
+    const int64_t blocks = cdiv(n_csr, warps);
+    DFX_REQUIRE(blocks < 2147483647, "pf_csr: too many rows");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (fwd && fill)
+        pf_csr_kernel<1, 1><<<(unsigned)blocks, 32 * warps, 0, s>>>(*g, rows, n_rows, k0, kb, counts, row_ptr, col, val);
+    else if (fwd)
+        pf_csr_kernel<1, 0><<<(unsigned)blocks, 32 * warps, 0, s>>>(*g, rows, n_rows, k0, kb, counts, row_ptr, col, val);
+    else if (fill)
+        pf_csr_kernel<0, 1><<<(unsigned)blocks, 32 * warps, 0, s>>>(*g, rows, n_rows, k0, kb, counts, row_ptr, col, val);
+    else
+        pf_csr_kernel<0, 0><<<(unsigned)blocks, 32 * warps, 0, s>>>(*g, rows, n_rows, k0, kb, counts, row_ptr, col, val);
+    return launch_status(fill ? "pf_csr_fill" : "pf_csr_count");
+}
+
+extern "C" int dfx_pf_csr_count(const dfx_pf_geometry *g, const int32_t *rows, int n_rows, int k0, int kb,
+                                int forward_rows, int32_t *counts, void *stream)
+{
+    return pf_csr(g, rows, n_rows, k0, kb, forward_rows ? 1 : 0, 0, counts, nullptr, nullptr, nullptr, stream);
+}
+
+extern "C" int dfx_pf_csr_fill(const dfx_pf_geometry *g, const int32_t *rows, int n_rows, int k0, int kb,
+                               int forward_rows, const int32_t *row_ptr, uint16_t *col, float *val, void *stream)
+{
+    return pf_csr(g, rows, n_rows, k0, kb, forward_rows ? 1 : 0, 1, nullptr, row_ptr, col, val, stream);
+}
+
+extern "C" size_t dfx_scan_scratch_bytes(int64_t n)
+{
+    return (size_t)(cdiv(n > 0 ? n : 1, SCAN_TILE) + 1) * sizeof(int32_t);
+}
+
+extern "C" int dfx_scan_exclusive_i32(const int32_t *in, int32_t *out, int64_t n, void *scratch,
+                                      size_t scratch_bytes, void *stream)
+{
+    DFX_REQUIRE(in && out && scratch && n >= 0, "scan: bad arguments");
+    if (scratch_bytes < dfx_scan_scratch_bytes(n)) {
+        set_error("scan: scratch of %zu bytes, %zu needed", scratch_bytes, dfx_scan_scratch_bytes(n));
+        return DFX_ENOMEM;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t tiles = cdiv(n > 0 ? n : 1, SCAN_TILE);
+    DFX_REQUIRE(tiles < 2147483647, "scan: too long");
+    int32_t *sums = (int32_t *)scratch;
+    scan_tile_sums<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, sums);
+    int st = launch_status("scan_tile_sums");
+    if (st) return st;
+    scan_sums<<<1, SCAN_THREADS, 0, s>>>(sums, tiles, out + n);
+    st = launch_status("scan_sums");
+    if (st) return st;
+    if (n == 0) return DFX_OK;
+    scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, sums, out);
+    return launch_status("scan_tiles");
+}
+
+extern "C" int dfx_spmm_pf_forward(const float *sino, const int32_t *row_ptr, const uint16_t *col_k, const float *val,
+                                   float *data, const int32_t *omegas, int n_sub, int my, int cp, int kstride, int kb,
+                                   int compact, void *stream)
+{
+    DFX_REQUIRE(sino && row_ptr && col_k && val && data, "spmm_forward: null pointer");
+    DFX_REQUIRE(n_sub > 0 && my > 0 && cp > 0 && kb > 0 && kb <= kstride, "spmm_forward: bad sizes");
+    DFX_REQUIRE(n_sub <= 65535 && cdiv(my, TY) <= 65535, "spmm_forward: grid too large");
+    dim3 grid((unsigned)cdiv(cp, SP_THREADS), (unsigned)cdiv(my, TY), (unsigned)n_sub);
+    spmm_forward_kernel<<<grid, SP_THREADS, 0, (cudaStream_t)stream>>>(sino, row_ptr, col_k, val, data, omegas, my, cp,
+                                                                       kstride, kb, compact);
+    return launch_status("spmm_pf_forward");
+}
+
+extern "C" int dfx_spmm_pf_adjoint(const float *data, const int32_t *row_ptr, const uint16_t *col_j, const float *val,
+                                   float *sino, const int32_t *omegas, int n_sub, int my, int kb, int cp, int kstride,
+                                   float alpha, int compact, void *stream)
+{
+    DFX_REQUIRE(sino && row_ptr && col_j && val && data, "spmm_adjoint: null pointer");
+    DFX_REQUIRE(n_sub > 0 && my > 0 && cp > 0 && kb > 0 && kb <= kstride, "spmm_adjoint: bad sizes");
+    DFX_REQUIRE(n_sub <= 65535 && cdiv(my, TY) <= 65535, "spmm_adjoint: grid too large");
+    dim3 grid((unsigned)cdiv(kstride, SP_THREADS), (unsigned)cdiv(my, TY), (unsigned)n_sub);
+    spmm_adjoint_kernel<<<grid, SP_THREADS, 0, (cudaStream_t)stream>>>(data, row_ptr, col_j, val, sino, omegas, my,
+                                                                       kb, cp, kstride, alpha, compact);
+    return launch_status("spmm_pf_adjoint");
+}
+
+extern "C" int dfx_zero_rows(float *data, const int32_t *omegas, int n_sub, int64_t row_len, void *stream)
+{
+    DFX_REQUIRE(data && omegas && n_sub >= 0 && row_len > 0, "zero_rows: bad arguments");
+    if (n_sub == 0) return DFX_OK;
+    zero_rows_kernel<<<grid_for((int64_t)n_sub * row_len, 256), 256, 0, (cudaStream_t)stream>>>(data, omegas, n_sub,
+                                                                                                 row_len);
+    return launch_status("zero_rows");
+}

@@ -1,0 +1,367 @@
+// Element-wise and reduction kernels of the Poisson solvers (SPDHGPoisson, FISTAPoisson) on sm_100a.
+//
+// Element-wise kernels are grid-stride loops over 64-bit indices (one pass over HBM, vectorised where the layout
+// allows). Reductions sum in float64: every block reduces its grid-stride share with warp shuffles into one partial
+// in the caller's scratch, and one block sums the partials in a fixed order, so the result does not depend on
+// timing (bitwise reproducible for a given launch shape).
+#include "dfx_common.cuh"
+
+namespace dfx {
+
+constexpr int EW_THREADS = 256;
+constexpr int RED_THREADS = 256;
+constexpr int RED_BLOCKS_MAX = 148 * 8;
+
+static unsigned ew_grid(int64_t n)
+{
+    const int64_t b = cdiv(n, EW_THREADS);
+    return (unsigned)(b < 148 * 32 ? (b > 0 ? b : 1) : 148 * 32);
+}
+
+static int red_blocks(int64_t n)
+{
+    const int64_t b = cdiv(n, RED_THREADS * 4);
+    return (int)(b < RED_BLOCKS_MAX ? (b > 0 ? b : 1) : RED_BLOCKS_MAX);
+}
+
+__device__ __forceinline__ float periodic(const float *a, int64_t period, int64_t i, float dflt)
+{
+    return period ? __ldg(a + (i % period)) : dflt;
+}
+
+// sum over the block of NS doubles per thread, written by thread 0 to out[0 .. NS-1]
+template <int NS>
+__device__ __forceinline__ void block_sum(double (&v)[NS], double *out)
+{
+    __shared__ double sh[NS][RED_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+        double x = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[q][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            double s = 0.0;
+            for (int w = 0; w < RED_THREADS / 32; ++w) s += sh[q][w];
+            out[q] = s;
+        }
+    }
+}
+
+// out[q] = sum of the nb partials part[b * NS + q] (one block, fixed order)
+template <int NS>
+__global__ void __launch_bounds__(RED_THREADS) finish_sums(const double *__restrict__ part, int nb, double *out)
+{
+    double v[NS];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nb; b += RED_THREADS) s += part[(int64_t)b * NS + q];
+        v[q] = s;
+    }
+    block_sum<NS>(v, out);
+}
+
+// ---- SPDHG ----
+__global__ void dual_update_kernel(float *__restrict__ y, float *__restrict__ d, const float *__restrict__ sig,
+                                   const float *__restrict__ b, const float *__restrict__ w, int64_t pw,
+                                   const float *__restrict__ g, int64_t pg, const float *__restrict__ bg, int64_t pbg,
+                                   float eps, const int32_t *__restrict__ omegas, int64_t row, int64_t n)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = t / row;
+        const int64_t i = (int64_t)__ldg(omegas + s) * row + (t - s * row);
+        const float wi = periodic(w, pw, i, 1.0f), si = sig[i];
+        const float yo = y[i];
+        float yn = 0.0f;
+        if (wi != 0.0f && si != 0.0f) {
+            const float gi = periodic(g, pg, i, 1.0f);
+            const double sc = __ddiv_rn((double)wi, (double)gi);
+            const double rr = __dadd_rn((double)periodic(bg, pbg, i, 0.0f), __dmul_rn((double)eps, (double)gi));
+            const double v = __dadd_rn(__dadd_rn((double)yo, __dmul_rn((double)si, (double)d[i])),
+                                       __dmul_rn((double)si, rr));
+            const double dd = __dsub_rn(v, sc);
+            const double disc = __dadd_rn(__dmul_rn(dd, dd), __dmul_rn(__dmul_rn(__dmul_rn(4.0, (double)si), sc),
+                                                                       (double)b[i]));
+            yn = (float)__dmul_rn(0.5, __dsub_rn(__dadd_rn(v, sc), __dsqrt_rn(disc)));
+        }
+        d[i] = yn - yo;
+        y[i] = yn;
+    }
+}
+
+__global__ void primal_update_kernel(float *__restrict__ x, float *__restrict__ z, const float *__restrict__ T,
+                                     const float *__restrict__ dz, float inv_p, float lam, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float di = dz[i];
+        const float zi = __fadd_rn(z[i], di);
+        z[i] = zi;
+        const float zb = __fadd_rn(zi, __fmul_rn(inv_p, di));
+        const float t = T[i];
+        x[i] = t > 0.0f ? fmaxf(0.0f, __fsub_rn(x[i], __fmul_rn(t, __fadd_rn(zb, lam)))) : 0.0f;
+    }
+}
+
+__global__ void dual_steps_kernel(float *__restrict__ sig, const float *__restrict__ rowsum,
+                                  const float *__restrict__ w, int64_t pw, float sigma0, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float rs = rowsum[i];
+        sig[i] = (periodic(w, pw, i, 1.0f) != 0.0f && rs > 0.0f) ? __fdiv_rn(sigma0, rs) : 0.0f;
+    }
+}
+
+__global__ void set_mask_ones_kernel(float *__restrict__ u, const float *__restrict__ w, int64_t pw, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        u[i] = periodic(w, pw, i, 1.0f) != 0.0f ? 1.0f : 0.0f;
+}
+
+__global__ void fill_kernel(float *__restrict__ x, float value, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = value;
+}
+
+__global__ void tinit_kernel(float *__restrict__ T, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        T[i] = __int_as_float(0x7f800000);
+}
+
+__global__ void tmin_kernel(float *__restrict__ T, const float *__restrict__ colsum, const uint8_t *__restrict__ supp,
+                            int64_t npix, float c, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const bool inside = supp ? __ldg(supp + (i % npix)) != 0 : true;
+        const float cs = colsum[i];
+        if (inside && cs > 0.0f) T[i] = fminf(T[i], __fdiv_rn(c, cs));
+    }
+}
+
+__global__ void tfinal_kernel(float *__restrict__ T, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (isinf(T[i])) T[i] = 0.0f;
+}
+
+__global__ void support_ones_kernel(float *__restrict__ x, const uint8_t *__restrict__ supp, int64_t npix, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = (supp ? __ldg(supp + (i % npix)) != 0 : true) ? 1.0f : 0.0f;
+}
+
+__global__ void project_support_kernel(float *__restrict__ x, const uint8_t *__restrict__ supp, int64_t npix,
+                                       int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if ((supp && __ldg(supp + (i % npix)) == 0) || x[i] < 0.0f) x[i] = 0.0f;
+}
+
+// ---- reductions ----
+__global__ void __launch_bounds__(RED_THREADS) poisson_value_grad_kernel(
+    float *__restrict__ mu, const float *__restrict__ b, const float *__restrict__ w, int64_t pw,
+    const float *__restrict__ g, int64_t pg, const float *__restrict__ bg, int64_t pbg, float eps, int write_grad,
+    int mode, float floor_counts, int64_t n, double *__restrict__ part)
+{
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float wi = periodic(w, pw, i, 1.0f);
+        float gr = 0.0f;
+        if (wi != 0.0f) {
+            const float gi = periodic(g, pg, i, 1.0f);
+            const double bi = (double)b[i];
+            const double sc = (double)wi / (double)gi;
+            if (mode == 0) {
+                const double m = (double)fmaxf(mu[i], 0.0f) + (double)periodic(bg, pbg, i, 0.0f) + (double)eps * gi;
+                double val = m - bi;
+                if (bi > 0.0) val += bi * log(bi / m);
+                v[0] += sc * val;
+                gr = (float)(sc * (1.0 - bi / m));
+            } else {
+                const double r = (double)mu[i] + (double)periodic(bg, pbg, i, 0.0f) - bi;
+                const double c = sc / fmax(bi, (double)floor_counts * gi);
+                v[0] += 0.5 * c * r * r;
+                gr = (float)(c * r);
+            }
+        }
+        if (write_grad) mu[i] = gr;
+    }
+    block_sum<1>(v, part + blockIdx.x);
+}
+
+__global__ void __launch_bounds__(RED_THREADS) mean_counted_kernel(const float *__restrict__ b,
+                                                                   const float *__restrict__ w, int64_t pw, int64_t n,
+                                                                   double *__restrict__ part)
+{
+    double v[2] = {0.0, 0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (periodic(w, pw, i, 1.0f) != 0.0f) {
+            v[0] += (double)b[i];
+            v[1] += 1.0;
+        }
+    block_sum<2>(v, part + 2 * blockIdx.x);
+}
+
+__global__ void __launch_bounds__(RED_THREADS) dot_kernel(const float *__restrict__ x, const float *__restrict__ y,
+                                                          int64_t n, double *__restrict__ part)
+{
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v[0] += y ? (double)x[i] * (double)y[i] : (double)x[i];
+    block_sum<1>(v, part + blockIdx.x);
+}
+
+static int check_scratch(void *scratch, size_t bytes, int64_t n, int ns)
+{
+    const size_t need = (size_t)red_blocks(n) * ns * sizeof(double);
+    if (!scratch || bytes < need) {
+        set_error("reduction: scratch of %zu bytes, %zu needed", bytes, need);
+        return DFX_ENOMEM;
+    }
+    return DFX_OK;
+}
+
+}  // namespace dfx
+
+using namespace dfx;
+
+#define EW_LAUNCH(kernel, n, stream, ...)                                                                   \
+    do {                                                                                                    \
+        kernel<<<ew_grid(n), EW_THREADS, 0, (cudaStream_t)(stream)>>>(__VA_ARGS__);                         \
+        return launch_status(#kernel);                                                                      \
+    } while (0)
+
+extern "C" int dfx_spdhg_dual_update(float *y, float *d, const float *sig, const float *b, const float *w, int64_t pw,
+                                     const float *g, int64_t pg, const float *bg, int64_t pbg, float eps,
+                                     const int32_t *omegas, int n_sub, int64_t row_len, void *stream)
+{
+    DFX_REQUIRE(y && d && sig && b && omegas && n_sub >= 0 && row_len > 0, "dual_update: bad arguments");
+    DFX_REQUIRE((!pw || w) && (!pg || g) && (!pbg || bg), "dual_update: periodic array missing");
+    const int64_t n = (int64_t)n_sub * row_len;
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(dual_update_kernel, n, stream, y, d, sig, b, w, pw, g, pg, bg, pbg, eps, omegas, row_len, n);
+}
+
+extern "C" int dfx_spdhg_primal_update(float *x, float *z, const float *T, const float *dz, float inv_p, float lam,
+                                       int64_t n, void *stream)
+{
+    DFX_REQUIRE(x && z && T && dz && n >= 0, "primal_update: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(primal_update_kernel, n, stream, x, z, T, dz, inv_p, lam, n);
+}
+
+extern "C" int dfx_dual_steps(float *sig, const float *rowsum, const float *w, int64_t pw, float sigma0, int64_t n,
+                              void *stream)
+{
+    DFX_REQUIRE(sig && rowsum && (!pw || w) && n >= 0, "dual_steps: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(dual_steps_kernel, n, stream, sig, rowsum, w, pw, sigma0, n);
+}
+
+extern "C" int dfx_set_mask_ones(float *u, const float *w, int64_t pw, int64_t n, void *stream)
+{
+    DFX_REQUIRE(u && (!pw || w) && n >= 0, "set_mask_ones: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(set_mask_ones_kernel, n, stream, u, w, pw, n);
+}
+
+extern "C" int dfx_fill_f32(float *x, float value, int64_t n, void *stream)
+{
+    DFX_REQUIRE(x && n >= 0, "fill: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(fill_kernel, n, stream, x, value, n);
+}
+
+extern "C" int dfx_tinit(float *T, int64_t n, void *stream)
+{
+    DFX_REQUIRE(T && n >= 0, "tinit: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(tinit_kernel, n, stream, T, n);
+}
+
+extern "C" int dfx_tmin(float *T, const float *colsum, const uint8_t *supp, int64_t npix, float c, int64_t n,
+                        void *stream)
+{
+    DFX_REQUIRE(T && colsum && n >= 0 && (!supp || npix > 0), "tmin: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(tmin_kernel, n, stream, T, colsum, supp, npix, c, n);
+}
+
+extern "C" int dfx_tfinal(float *T, int64_t n, void *stream)
+{
+    DFX_REQUIRE(T && n >= 0, "tfinal: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(tfinal_kernel, n, stream, T, n);
+}
+
+extern "C" int dfx_support_ones(float *x, const uint8_t *supp, int64_t npix, int64_t n, void *stream)
+{
+    DFX_REQUIRE(x && n >= 0 && (!supp || npix > 0), "support_ones: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(support_ones_kernel, n, stream, x, supp, npix, n);
+}
+
+extern "C" int dfx_project_support(float *x, const uint8_t *supp, int64_t npix, int64_t n, void *stream)
+{
+    DFX_REQUIRE(x && n >= 0 && (!supp || npix > 0), "project_support: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(project_support_kernel, n, stream, x, supp, npix, n);
+}
+
+extern "C" size_t dfx_reduce_scratch_bytes(int64_t n) { return (size_t)red_blocks(n) * 4 * sizeof(double); }
+
+extern "C" int dfx_poisson_value_grad(float *mu, const float *b, const float *w, int64_t pw, const float *g,
+                                      int64_t pg, const float *bg, int64_t pbg, float eps, int write_grad, int mode,
+                                      float floor_counts, int64_t n, double *out, void *scratch, size_t scratch_bytes,
+                                      void *stream)
+{
+    DFX_REQUIRE(mu && b && out && n >= 0 && (!pw || w) && (!pg || g) && (!pbg || bg), "poisson_value_grad: bad args");
+    int st = check_scratch(scratch, scratch_bytes, n, 1);
+    if (st) return st;
+    const int nb = red_blocks(n);
+    cudaStream_t s = (cudaStream_t)stream;
+    double *part = (double *)scratch;
+    poisson_value_grad_kernel<<<nb, RED_THREADS, 0, s>>>(mu, b, w, pw, g, pg, bg, pbg, eps, write_grad, mode,
+                                                         floor_counts, n, part);
+    st = launch_status("poisson_value_grad");
+    if (st) return st;
+    finish_sums<1><<<1, RED_THREADS, 0, s>>>(part, nb, out);
+    return launch_status("finish_sums");
+}
+
+extern "C" int dfx_mean_counted(const float *b, const float *w, int64_t pw, int64_t n, double *out, void *scratch,
+                                size_t scratch_bytes, void *stream)
+{
+    DFX_REQUIRE(b && out && n >= 0 && (!pw || w), "mean_counted: bad arguments");
+    int st = check_scratch(scratch, scratch_bytes, n, 2);
+    if (st) return st;
+    const int nb = red_blocks(n);
+    cudaStream_t s = (cudaStream_t)stream;
+    mean_counted_kernel<<<nb, RED_THREADS, 0, s>>>(b, w, pw, n, (double *)scratch);
+    st = launch_status("mean_counted");
+    if (st) return st;
+    finish_sums<2><<<1, RED_THREADS, 0, s>>>((const double *)scratch, nb, out);
+    return launch_status("finish_sums");
+}
+
+extern "C" int dfx_dot_f64(const float *x, const float *y, int64_t n, double *out, void *scratch, size_t scratch_bytes,
+                           void *stream)
+{
+    DFX_REQUIRE(x && out && n >= 0, "dot: bad arguments");
+    int st = check_scratch(scratch, scratch_bytes, n, 1);
+    if (st) return st;
+    const int nb = red_blocks(n);
+    cudaStream_t s = (cudaStream_t)stream;
+    dot_kernel<<<nb, RED_THREADS, 0, s>>>(x, y, n, (double *)scratch);
+    st = launch_status("dot");
+    if (st) return st;
+    finish_sums<1><<<1, RED_THREADS, 0, s>>>((const double *)scratch, nb, out);
+    return launch_status("finish_sums");
+}

@@ -1,0 +1,536 @@
+"""SinglePhaseForwardOperator: the single-phase texture-tomography forward operator and its adjoint on a B200.
+
+Drop-in for diffractom's SinglePhaseForwardOperator (operators/single_phase_forward_operator.py, "SPFO" below): the
+same constructor signature, cfg keys, batching (max_gb), array layouts and methods used by the solvers, with CUDA
+torch tensors in place of pyopencl arrays. The model (SPFO:158-164):
+
+    data = PF @ Radon(coeffs),   coeffs (K, Ny, Nx),   data (N_Omega, My, N_eta * N_rings)
+
+computed batch by batch over the orientations: the Radon transform of every orientation's image (channel-fastest,
+the batch's orientations are the channels), then per rotation angle the product of the sinogram (My x Kb) with the
+sparse pole-figure matrix (Kb x N_eta * N_rings). The adjoint is the exact transpose: the transposed products
+(scaled by N_Omega / pi) and the backprojection with angle weights pi / N_Omega.
+
+All device work goes through the C ABI of diffractom_b200/_lib/libdfx_b200.so (hand-written sm_100a kernels); torch
+only holds the device memory and provides the stream. Host set-up (quadrature, probed directions, pole axes,
+projector geometry) is float64 NumPy, uploaded as float32 (geometry.py).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+import warnings
+from typing import Any, Mapping
+
+import numpy as np
+import torch
+
+from . import _lib
+from .arrays import as_host, check_device, is_device
+from .geometry import OperatorGeometry, interleaved_subsets
+from .quadrature import DEFAULT_TOL
+
+SPARSE_BATCH_MAX = 1024   # largest orientation batch of the sparse modes (SPFO:134)
+SPARSE_MIN_BATCHES = 4    # sparse modes: at least this many batches (SPFO:135)
+CAND_BYTES = 2 + 4 + 4 + 4 + 4          # per candidate / non-zero scratch of the reference's generator
+NNZ_BYTES = 2 + 4 + 4 + 2 + 4 + 2 + 4   # (pf_generate.py:29-30), used by the batch-size rule
+KSTRIDE_ALIGN = 8                        # channel stride of the batch buffers (two float4 per thread)
+
+
+def _stream_handle(stream) -> ctypes.c_void_p:
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class SinglePhaseForwardOperator:
+    """Single-material pole-figure forward operator (SPFO:158)."""
+
+    coefficient_layout = "dense"
+    _pf_forward_csr = True
+
+    def __init__(self, cfg: Mapping[str, Any], material, grid, max_gb: float, verbose: bool = False,
+                 normalized: bool = False, ctx=None, queue=None, pf_mode: str = "auto", sparse_max_fill: float = 0.3,
+                 sparse_max_fill_partial: float = 0.1, sparse_max_gb: float | None = None, projector: str = "auto",
+                 radon_kernel: str | None = None, fft_max_gb: float = 1.5, reserve_coefficient_arrays: int = 3,
+                 pf_cutoff_sigma: float | None = 4.0, quadrature="auto", quadrature_tol: float = DEFAULT_TOL,
+                 intensity_model=None, sparse_batch_max: int = SPARSE_BATCH_MAX, rings=None, ring_two_theta=None,
+                 reflection_two_theta: bool = False, window_parallax=None, ring_intensities=None, **kwargs):
+        """Arguments as diffractom's (SPFO:169-197). ctx: None, a torch.device or a CUDA device index (the GPU);
+        queue: None (the current torch stream at every call) or a torch.cuda.Stream. ring_intensities: with
+        normalized=False, the integrated intensity of every ring (diffractom computes them from structure factors,
+        which this package does not model); fft_max_gb is accepted for compatibility.
+
+        Not provided (NotImplementedError): projector "fft" / "gratopy", pf_mode "dense" (the sparse products give
+        the same operator), reflection_two_theta, window_parallax, custom rings with overlap weights other than 1."""
+        lib = _lib.lib()                                    # fails loudly without the CUDA library
+        if not torch.cuda.is_available():
+            raise RuntimeError("SinglePhaseForwardOperator needs a CUDA device")
+        if isinstance(ctx, torch.device):
+            self.device = ctx
+        elif isinstance(ctx, int):
+            self.device = torch.device("cuda", ctx)
+        else:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self._lib = lib
+        self.queue = queue if isinstance(queue, torch.cuda.Stream) else None
+        self.ctx = self.device
+        self.verbose = verbose
+        self.reserve_coefficient_arrays = int(reserve_coefficient_arrays)
+        self.pf_cutoff_sigma = pf_cutoff_sigma
+        self.sparse_batch_max = int(sparse_batch_max)
+        self.cfg = {**cfg, **kwargs}
+        self.material, self.grid = material, grid
+        if reflection_two_theta or window_parallax is not None:
+            raise NotImplementedError("reflection_two_theta and window_parallax are not provided by this operator")
+        if projector not in ("auto", "native", "fft", "gratopy"):
+            raise ValueError(f"projector must be 'auto', 'native', 'fft' or 'gratopy', not {projector!r}")
+        if projector in ("fft", "gratopy"):
+            raise NotImplementedError(f"projector {projector!r} is not provided (the native projector is)")
+        if pf_mode not in ("dense", "sparse", "generated", "auto"):
+            raise ValueError(f"pf_mode must be 'dense', 'sparse', 'generated' or 'auto', not {pf_mode!r}")
+        if pf_mode == "dense":
+            raise NotImplementedError("pf_mode='dense' is not provided: 'sparse' applies the same matrix")
+        if radon_kernel is None:
+            radon_kernel = "trapezoid"
+        self.projector = "native"
+        self.radon_kernel = radon_kernel
+
+        # ---- host set-up (SPFO:376-494): rings, quadrature, probed directions, poles, projector geometry
+        geom = OperatorGeometry(self.cfg, material, grid, normalized=normalized, quadrature=quadrature,
+                                quadrature_tol=quadrature_tol, pf_cutoff_sigma=pf_cutoff_sigma,
+                                radon_kernel=radon_kernel, rings=rings, ring_two_theta=ring_two_theta,
+                                ring_intensities=ring_intensities)
+        self.__dict__.update({k: v for k, v in vars(geom).items() if k != "cfg"})
+        self.geometry = geom
+        self.pf_batch_max_gb = float(max_gb)
+        self._kernel_id = 1 if radon_kernel == "trapezoid" else 0
+
+        # ---- device copies
+        dev = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=self.device)
+        self.coords_gpu = dev(self.coords_cpu)
+        self.poles_gpu = dev(self.poles_cpu)
+        self.axis_start_gpu = dev(self.axis_start_cpu, torch.int32)
+        self.axis_count_gpu = dev(self.axis_count_cpu)
+        self.inv_sigma2_gpu = dev(self.inv_sigma2_cpu)
+        self.norm_factor_gpu = dev(self.norm_factor_cpu)
+        self.quad_weights_gpu = None if self.quad_weights_cpu is None else dev(self.quad_weights_cpu)
+        self.intens_gpu = None if self.normalized else dev(self.intens_cpu)
+        self.geo_gpu = dev(self.radon_geo.geo)
+        self._pfg = _lib.PFGeometry(
+            self.coords_gpu.data_ptr(), self.poles_gpu.data_ptr(), self.axis_start_gpu.data_ptr(),
+            self.axis_count_gpu.data_ptr(), self.inv_sigma2_gpu.data_ptr(), self.norm_factor_gpu.data_ptr(),
+            None if self.quad_weights_gpu is None else self.quad_weights_gpu.data_ptr(),
+            None if self.intens_gpu is None else self.intens_gpu.data_ptr(),
+            self.N_Omega, self.N_eta, self.N_peaks, self.N_axes, self.N_Omega_subdivisions, self.N_eta_subdivisions,
+            self.K, float(self.pf_cut))
+        self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
+        self.omega_subsets = None
+        self._sub = []
+        self._streamer = None
+
+        # ---- batches and the sparse PF matrix (SPFO:1026-1094, 1207-1373)
+        self.get_pf_batches_for_material()
+        self.pf_mode = pf_mode
+        self.sparse_batches = None
+        self.pf_storage = None
+        if sparse_max_gb is None:
+            sparse_max_gb = self.default_sparse_budget_gb()
+        self._pf_build = dict(mode=pf_mode, max_fill=sparse_max_fill, max_gb=sparse_max_gb,
+                              max_fill_partial=sparse_max_fill_partial)
+        self.build_sparse_pf(**self._pf_build)
+
+    # ------------------------------------------------------------------ small helpers
+    def stream(self) -> torch.cuda.Stream:
+        return self.queue if self.queue is not None else torch.cuda.current_stream(self.device)
+
+    def _s(self):
+        return _stream_handle(self.stream())
+
+    def _call(self, name, *args):
+        _lib.check(getattr(self._lib, name)(*args))
+
+    def scratch(self, nbytes: int) -> torch.Tensor:
+        """A device scratch buffer of at least nbytes (reused; grows on demand)."""
+        if self._scratch.numel() < nbytes:
+            self._scratch = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=self.device)
+        return self._scratch
+
+    def detector_shifts(self):
+        return self.geometry.detector_shifts()
+
+    @property
+    def coeff_shape(self):
+        return (self.K, self.Ny, self.Nx)
+
+    @property
+    def data_shape(self):
+        return (self.N_Omega, self.My, self.N_seg)
+
+    @property
+    def npix(self) -> int:
+        return self.Nx * self.Ny
+
+    def support_mask(self):
+        """(Ny, Nx) bool mask of the pixels inside the field of view at every projection angle (SPFO:544-547)."""
+        return self.geometry.support_mask()
+
+    # ------------------------------------------------------------------ batching
+    def get_pf_batches_for_material(self, K_batch=None):
+        """Orientation batches: K_batch each, or as many as a dense PF batch of max_gb holds (SPFO:1026-1094);
+        K_batch_max rounded up to a multiple of 4, 2^31 element limits of the batch buffers."""
+        R, C, P, K = self.N_Omega, self.N_eta, self.N_peaks, self.K
+        bytes_per_K = R * C * P * 4
+        max_bytes = self.pf_batch_max_gb * (1024 ** 3)
+        if K_batch is not None:
+            kbm = max(1, min(int(K_batch), K))
+        elif bytes_per_K > 0.01:
+            kbm = min(max(int(max_bytes // bytes_per_K), 1), K)
+        else:
+            kbm = 1
+        self.batches = [{"k_start": k0, "k_end": min(k0 + kbm, K), "K_batch": min(k0 + kbm, K) - k0}
+                        for k0 in range(0, K, kbm)]
+        self.K_batch_max = -(-max(b["K_batch"] for b in self.batches) // 4) * 4
+        checks = [("sinogram batch (N_Omega, My, K_batch)", R * self.My * self.K_batch_max),
+                  ("image batch (Nx, Ny, K_batch)", self.Nx * self.Ny * self.K_batch_max)]
+        if K_batch is None:
+            checks.append(("PF batch (N_Omega, K_batch, N_eta, N_rings)", R * self.K_batch_max * C * P))
+        for name, n in checks:
+            if n >= 2 ** 31:
+                raise ValueError(f"The {name} has {n} elements, more than 2^31 - 1; lower max_gb.")
+        self.Kstride = -(-self.K_batch_max // KSTRIDE_ALIGN) * KSTRIDE_ALIGN
+        self._alloc_batch_buffers()
+        return self.batches
+
+    def _alloc_batch_buffers(self):
+        self.coeffs_sino_C = torch.empty((self.N_Omega, self.My, self.Kstride), dtype=torch.float32,
+                                         device=self.device)
+        self._img_k = torch.empty((self.npix, self.Kstride), dtype=torch.float32, device=self.device)
+
+    def sparse_batch_size(self, fill):
+        """Orientations per batch of the sparse modes (SPFO:1377-1397)."""
+        R, CP, npix = self.N_Omega, self.N_seg, self.Nx * self.Ny
+        nnz_per_k = 1.1 * fill * R * CP
+        bytes_per_k = 4 * (R * self.My + 6 * npix) + 8 * R + (CAND_BYTES + NNZ_BYTES) * nnz_per_k
+        kb = int(self.pf_batch_max_gb * 1024 ** 3 // bytes_per_k)
+        limit = min(self.sparse_batch_max, (2 ** 31 - 1) // max(R * self.My, npix, int(nnz_per_k) + 1, R))
+        return max(self.K_batch_max, min(kb, limit, -(-self.K // SPARSE_MIN_BATCHES)))
+
+    def default_sparse_budget_gb(self):
+        """Half of the free device memory after a solver's reserve (SPFO:1180-1203)."""
+        coeff_bytes = 4 * self.Nx * self.Ny * self.K
+        data_bytes = 4 * self.N_Omega * self.My * self.N_seg
+        buffers = 4 * self.K_batch_max * (self.N_Omega * self.My + self.Nx * self.Ny)
+        free, total = torch.cuda.mem_get_info(self.device)
+        free = free - self.reserve_coefficient_arrays * coeff_bytes - 2 * data_bytes - buffers - 1024 ** 3
+        return 0.5 * max(free, 0) / 1024 ** 3
+
+    # ------------------------------------------------------------------ sparse PF matrix
+    def _csr(self, k0, kb, fwd, rows=None, n_rows=None, row_ptr=None, out=None):
+        """Count (and scan) or fill one CSR of a batch: returns (row_ptr, nnz) when counting, fills `out` (col, val)
+        when row_ptr is given. rows: int32 device tensor of angle indices (None: all)."""
+        n_rows = self.N_Omega if rows is None else int(rows.numel())
+        n = n_rows * (self.N_seg if fwd else kb)
+        rp = rows.data_ptr() if rows is not None else None
+        s = self._s()
+        if row_ptr is None:
+            cnt = torch.empty(n + 1, dtype=torch.int32, device=self.device)
+            self._call("dfx_pf_csr_count", ctypes.byref(self._pfg), rp, n_rows, k0, kb, int(fwd), cnt.data_ptr(), s)
+            nb = self._lib.dfx_scan_scratch_bytes(n)
+            scr = self.scratch(nb)
+            self._call("dfx_scan_exclusive_i32", cnt.data_ptr(), cnt.data_ptr(), n, scr.data_ptr(), nb, s)
+            return cnt, int(cnt[n].item())
+        col, val = out
+        self._call("dfx_pf_csr_fill", ctypes.byref(self._pfg), rp, n_rows, k0, kb, int(fwd), row_ptr.data_ptr(),
+                   col.data_ptr(), val.data_ptr(), s)
+
+    def _make_csr(self, k0, kb, fwd, rows=None):
+        rp, nnz = self._csr(k0, kb, fwd, rows)
+        n = max(nnz, 1)
+        col = torch.empty(n, dtype=torch.int16, device=self.device)        # uint16 bit pattern
+        val = torch.empty(n, dtype=torch.float32, device=self.device)
+        self._csr(k0, kb, fwd, rows, row_ptr=rp, out=(col, val))
+        return rp, col, val, nnz
+
+    def build_sparse_pf(self, mode="auto", max_fill=0.3, max_gb=None, max_fill_partial=0.1):
+        """The sparse PF matrix per orientation batch (SPFO:1207-1373): the fill fraction of the first (dense-sized)
+        batch sets the sparse batch size; both CSR copies of every batch are stored if they fit in max_gb ("sparse"),
+        otherwise (and with mode "generated") the row pointers are kept and the entries are generated again in every
+        call. The structure is the dense batch's CSR, bit for bit (dfx_pf_csr_*)."""
+        t0 = time.perf_counter()
+        R, CP = self.N_Omega, self.N_seg
+        if self.K_batch_max > 65535 or CP > 65535:
+            raise ValueError(f"K_batch_max = {self.K_batch_max} or N_eta * N_rings = {CP} exceeds the 16-bit index "
+                             "range of the sparse PF matrix; use a smaller max_gb")
+        b0 = self.batches[0]
+        _, nnz0 = self._csr(b0["k_start"], b0["K_batch"], False)
+        fill = nnz0 / (R * b0["K_batch"] * CP)
+        self.sparse_fill_first = fill
+        if mode == "auto" and fill > max_fill:
+            warnings.warn(f"PF fill fraction {100 * fill:.1f} % > {100 * max_fill:.1f} %: the reference would apply the "
+                          "dense matrix; the sparse products compute the same operator", stacklevel=2)
+        self.get_pf_batches_for_material(K_batch=self.sparse_batch_size(fill))
+        nb = len(self.batches)
+        est = [int(math.ceil(1.02 * fill * R * b["K_batch"] * CP)) + 16 for b in self.batches]
+        both = sum(12 * n for n in est) + nb * 4 * (R * CP + 1) + sum(4 * (R * b["K_batch"] + 1) for b in self.batches)
+        budget = np.inf if max_gb is None else max_gb * 1024 ** 3
+        store = mode in ("auto", "sparse") and both <= budget
+        if mode == "sparse" and not store:
+            raise MemoryError(f"Sparse PF matrix: estimated size {both / 1024 ** 3:.1f} GB > {max_gb:.1f} GB; use "
+                              "pf_mode='generated' or 'auto', or raise sparse_max_gb.")
+        self.sparse_batches = []
+        self._gen_cap = 0
+        nnz_total = 0
+        for b in self.batches:
+            k0, kb = b["k_start"], b["K_batch"]
+            if store:
+                rpa, cj, va, nnz = self._make_csr(k0, kb, False)
+                rpf, ck, vf, nnz_f = self._make_csr(k0, kb, True)
+                assert nnz_f == nnz, (nnz, nnz_f)
+                self.sparse_batches.append(dict(row_ptr_a=rpa, col_j=cj, val_a=va, row_ptr_f=rpf, col_k=ck, val_f=vf,
+                                                nnz=nnz))
+            else:
+                rpa, nnz = self._csr(k0, kb, False)
+                rpf, _ = self._csr(k0, kb, True)
+                self.sparse_batches.append(dict(row_ptr_a=rpa, row_ptr_f=rpf, nnz=nnz, generated=True))
+                self._gen_cap = max(self._gen_cap, nnz)
+            nnz_total += nnz
+        if not store:
+            n = max(self._gen_cap, 1)
+            self._gen_col = torch.empty(n, dtype=torch.int16, device=self.device)
+            self._gen_val = torch.empty(n, dtype=torch.float32, device=self.device)
+        self.pf_mode = "sparse" if store else "generated"
+        self.pf_storage = "both" if store else "none"
+        self.sparse_nnz = nnz_total
+        self.sparse_fill = nnz_total / (R * self.K * CP)
+        self.pf_setup_s = time.perf_counter() - t0
+        if self.verbose:
+            print(f"Sparse PF matrix: {nnz_total} non-zeros (fill {100 * self.sparse_fill:.3f} %), {nb} batches of up "
+                  f"to {self.K_batch_max}, stored: {self.pf_storage}; set up in {self.pf_setup_s:.2f} s")
+
+    def _pf_batch(self, ib, forward, m=None):
+        """(row_ptr, col, val, compact) of batch ib for the forward or adjoint product; m: subset (its rows)."""
+        sb = self.sparse_batches[ib]
+        b = self.batches[ib]
+        key = "f" if forward else "a"
+        if not sb.get("generated"):
+            return sb["row_ptr_" + key], sb["col_k" if forward else "col_j"], sb["val_" + key], 0
+        if m is None:
+            rp, rows, compact = sb["row_ptr_" + key], None, 0
+        else:
+            rp, rows, compact = self._sub[m]["row_ptr"][ib][key], self._sub[m]["omegas"], 1
+        self._csr(b["k_start"], b["K_batch"], forward, rows, row_ptr=rp, out=(self._gen_col, self._gen_val))
+        return rp, self._gen_col, self._gen_val, compact
+
+    # ------------------------------------------------------------------ omega subsets
+    def set_omega_subsets(self, subsets):
+        """Subsets of the rotation angles for the subset forms direct_cl / adjoint_cl(subset=m) (SPFO:1541-1599):
+        an int M (angle i in subset i % M) or a list of index arrays; returns the sorted index arrays."""
+        if self.pf_mode not in ("sparse", "generated"):
+            raise NotImplementedError(f"omega subsets need pf_mode 'sparse' or 'generated' (this operator: "
+                                      f"{self.pf_mode!r})")
+        R = self.N_Omega
+        if np.isscalar(subsets):
+            subsets = interleaved_subsets(R, int(subsets))
+        out = []
+        for s in subsets:
+            s = np.unique(np.asarray(s, dtype=np.int64))
+            if s.size == 0 or s[0] < 0 or s[-1] >= R:
+                raise ValueError(f"every subset must hold angle indices in 0 .. {R - 1}")
+            out.append(s)
+        old = self.omega_subsets
+        if old is not None and len(old) == len(out) and all(np.array_equal(a, b) for a, b in zip(old, out)):
+            return out
+        self.release_omega_subsets()
+        self.omega_subsets = out
+        for s in out:
+            om = torch.as_tensor(s.astype(np.int32), device=self.device)
+            geo = self.geo_gpu[torch.as_tensor(s, device=self.device)].contiguous()
+            entry = dict(omegas=om, geo=geo, n=len(s), row_ptr=None)
+            if any(sb.get("generated") for sb in self.sparse_batches):
+                entry["row_ptr"] = []
+                for b in self.batches:
+                    rpa, nnz = self._csr(b["k_start"], b["K_batch"], False, om)
+                    rpf, _ = self._csr(b["k_start"], b["K_batch"], True, om)
+                    entry["row_ptr"].append({"a": rpa, "f": rpf})
+            self._sub.append(entry)
+        return out
+
+    def release_omega_subsets(self):
+        self._sub = []
+        self.omega_subsets = None
+
+    @property
+    def _sub_omegas(self):
+        return [e["omegas"] for e in self._sub]
+
+    def _subset(self, subset):
+        if self.omega_subsets is None:
+            raise ValueError("no omega subsets defined: call set_omega_subsets first")
+        return int(subset)
+
+    def zero_subset_rows(self, data, subset):
+        """data rows of the angles of subset m <- 0 (SPFO:1638-1644)."""
+        m = self._subset(subset)
+        e = self._sub[m]
+        self._call("dfx_zero_rows", data.data_ptr(), e["omegas"].data_ptr(), e["n"], self.My * self.N_seg, self._s())
+
+    def _fill(self, t: torch.Tensor, value: float = 0.0):
+        self._call("dfx_fill_f32", t.data_ptr(), float(value), t.numel(), self._s())
+
+    # ------------------------------------------------------------------ forward / adjoint
+    def direct_cl(self, coeffs, data, subset=None):
+        """In-place forward operator data = PF @ Radon(coeffs) (SPFO:1646-1662); subset=m: only the rows of the angles
+        of subset m are written (the other rows are left as they are)."""
+        check_device(coeffs, self.coeff_shape, "coeffs")
+        check_device(data, self.data_shape, "data")
+        if subset is None:
+            self._fill(data, 0.0)
+        else:
+            self.zero_subset_rows(data, subset)
+        for ib, b in enumerate(self.batches):
+            self._direct_batch(coeffs, b["k_start"], self.K, ib, data, subset)
+
+    def _direct_batch(self, src, k_src, K_src, ib, data, subset=None):
+        """Add the forward projection of batch ib to data; its coefficients are orientations k_src .. k_src+Kb-1 of
+        src, a (K_src, Ny, Nx) array (SPFO:1664-1728)."""
+        b = self.batches[ib]
+        Kb = b["K_batch"]
+        s = self._s()
+        if subset is None:
+            geo, n_ang, om, m = self.geo_gpu, self.N_Omega, None, None
+        else:
+            m = self._subset(subset)
+            e = self._sub[m]
+            geo, n_ang, om = e["geo"], e["n"], e["omegas"]
+        self._call("dfx_gather_channels", src.data_ptr(), self._img_k.data_ptr(), self.npix, k_src, Kb, self.Kstride, s)
+        self._call("dfx_radon_forward", self._img_k.data_ptr(), self.coeffs_sino_C.data_ptr(), geo.data_ptr(), n_ang,
+                   self.Nx, self.Ny, self.My, self.Kstride, Kb, self._kernel_id, float(self.radon_geo.scale), s)
+        rp, col, val, compact = self._pf_batch(ib, True, m)
+        self._call("dfx_spmm_pf_forward", self.coeffs_sino_C.data_ptr(), rp.data_ptr(), col.data_ptr(),
+                   val.data_ptr(), data.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My,
+                   self.N_seg, self.Kstride, Kb, compact, s)
+
+    def adjoint_cl(self, data, coeffs, subset=None):
+        """In-place adjoint coeffs = A^T data (SPFO:1800-1817); subset=m: A_m^T (rows of subset m only)."""
+        check_device(data, self.data_shape, "data")
+        check_device(coeffs, self.coeff_shape, "coeffs")
+        for ib, b in enumerate(self.batches):
+            self._adjoint_batch(data, ib, coeffs, b["k_start"], self.K, subset)
+
+    def _adjoint_batch(self, data, ib, target, k_target, K_target, subset=None):
+        """A^T data of batch ib into orientations k_target .. k_target+Kb-1 of target (SPFO:1966-2033)."""
+        b = self.batches[ib]
+        Kb = b["K_batch"]
+        s = self._s()
+        if subset is None:
+            geo, n_ang, om, m = self.geo_gpu, self.N_Omega, None, None
+        else:
+            m = self._subset(subset)
+            e = self._sub[m]
+            geo, n_ang, om = e["geo"], e["n"], e["omegas"]
+        alpha = float(np.float32(self.N_Omega / np.pi))
+        rp, col, val, compact = self._pf_batch(ib, False, m)
+        self._call("dfx_spmm_pf_adjoint", data.data_ptr(), rp.data_ptr(), col.data_ptr(), val.data_ptr(),
+                   self.coeffs_sino_C.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My, Kb,
+                   self.N_seg, self.Kstride, alpha, compact, s)
+        self._call("dfx_radon_backward", self.coeffs_sino_C.data_ptr(), self._img_k.data_ptr(), geo.data_ptr(), n_ang,
+                   self.Nx, self.Ny, self.My, self.Kstride, Kb, self._kernel_id, int(self.radon_geo.n_taps), s)
+        self._call("dfx_scatter_channels", self._img_k.data_ptr(), target.data_ptr(), self.npix, k_target, Kb,
+                   self.Kstride, s)
+
+    def adjoint_batches_cl(self, data, out_batch, update):
+        """The adjoint one batch at a time into the first Kb * Ny * Nx elements of out_batch, then update(k0, Kb)
+        (SPFO:1819-1838)."""
+        check_device(data, self.data_shape, "data")
+        assert out_batch.dtype == torch.float32 and out_batch.numel() >= self.npix * self.K_batch_max
+        for ib, b in enumerate(self.batches):
+            self._adjoint_batch(data, ib, out_batch, 0, self.K_batch_max)
+            update(b["k_start"], b["K_batch"])
+
+    def direct(self, coeffs):
+        """Forward operator allocating its output: a CUDA tensor for a CUDA tensor; for a NumPy array (K, Ny, Nx) the
+        coefficients are streamed to the GPU batch by batch and a NumPy array is returned (SPFO:1107-1127)."""
+        if is_device(coeffs):
+            data = torch.empty(self.data_shape, dtype=torch.float32, device=self.device)
+            self.direct_cl(coeffs, data)
+            return data
+        x = as_host(coeffs, self.coeff_shape, "coeffs")
+        data = torch.empty(self.data_shape, dtype=torch.float32, device=self.device)
+        from .streaming import streamer_for
+        streamer_for(self).forward(x.reshape(-1), data)
+        return data.cpu().numpy()
+
+    def adjoint(self, data):
+        """Adjoint allocating its output (SPFO:1777-1796): CUDA tensor in, CUDA tensor out; NumPy in, NumPy out with
+        the coefficients streamed to the host batch by batch."""
+        if is_device(data):
+            coeffs = torch.empty(self.coeff_shape, dtype=torch.float32, device=self.device)
+            self.adjoint_cl(data, coeffs)
+            return coeffs
+        d = torch.as_tensor(as_host(data, self.data_shape, "data"), device=self.device)
+        out = np.empty(self.coeff_shape, np.float32)
+        from .streaming import streamer_for
+        streamer_for(self).adjoint_to_host(d, out.reshape(-1))
+        return out
+
+    # ------------------------------------------------------------------ memory
+    def device_bytes(self):
+        """Device memory held by the operator (batch buffers, sparse PF matrix, geometry)."""
+        n = 0
+        for t in (self.coeffs_sino_C, self._img_k, self.coords_gpu, self.poles_gpu, self._scratch):
+            n += t.numel() * t.element_size()
+        for sb in self.sparse_batches or []:
+            n += sum(v.numel() * v.element_size() for v in sb.values() if isinstance(v, torch.Tensor))
+        for t in (getattr(self, "_gen_col", None), getattr(self, "_gen_val", None)):
+            if t is not None:
+                n += t.numel() * t.element_size()
+        return n
+
+    def release_streamer(self):
+        if self._streamer is not None:
+            self._streamer.release()
+            self._streamer = None
+
+    def free_memory(self):
+        """Release the operator's device buffers (SPFO:957-1020)."""
+        self.release_omega_subsets()
+        self.release_streamer()
+        self.sparse_batches = None
+        self.coeffs_sino_C = self._img_k = None
+        self._gen_col = self._gen_val = None
+        self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
+        torch.cuda.synchronize(self.device)
+
+
+def estimate_L_power(op, niter: int = 20, seed: int = 0, eps: float = 1e-30, verbose: int = 1) -> float:
+    """Lipschitz constant ||A^T A|| by power iteration (SPFO:2136-2206); the start vector is the reference's
+    (a standard normal (Nx, Ny, K) draw stored pixel-fastest) and the dot products are float64 (dfx_dot_f64)."""
+    if niter < 1:
+        raise ValueError("niter must be >= 1")
+    rng = np.random.default_rng(seed)
+    x_host = np.ascontiguousarray(rng.standard_normal((op.Nx, op.Ny, op.K)).astype(np.float32).transpose(2, 1, 0))
+    x = torch.as_tensor(x_host, device=op.device)
+    Ax = torch.empty(op.data_shape, dtype=torch.float32, device=op.device)
+    z = torch.empty(op.coeff_shape, dtype=torch.float32, device=op.device)
+    out = torch.zeros(1, dtype=torch.float64, device=op.device)
+    lib = op._lib
+
+    def dot(a, b=None):
+        nb = lib.dfx_reduce_scratch_bytes(a.numel())
+        scr = op.scratch(nb)
+        _lib.call("dfx_dot_f64", a.data_ptr(), None if b is None else b.data_ptr(), a.numel(), out.data_ptr(),
+                  scr.data_ptr(), nb, op._s())
+        return float(out.item())
+
+    x.mul_(float(np.float32(1.0 / (np.sqrt(dot(x, x)) + eps))))
+    L_est = 0.0
+    for it in range(niter):
+        op.direct_cl(x, Ax)
+        op.adjoint_cl(Ax, z)
+        L_est = dot(x, z) / (dot(x, x) + eps)
+        zn = np.sqrt(dot(z, z)) + eps
+        z.mul_(float(np.float32(1.0 / zn)))
+        x, z = z, x
+        if verbose:
+            print(f"[power {it + 1:02d}] L_est={L_est:.6e}  ||z||={zn:.6e}")
+    return float(L_est)

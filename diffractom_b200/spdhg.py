@@ -1,0 +1,253 @@
+"""SPDHGPoisson: stochastic primal-dual hybrid gradient over omega subsets for the Poisson deviance, on a B200.
+
+Drop-in for diffractom's SPDHGPoisson (optimization/spdhg_poisson.py) without the total-variation block: the same
+arguments, subset schedule (numpy default_rng(seed) permutations, an epoch never starting with the subset that ended
+the previous one), step sizes (diagonal preconditioning: S_i = gamma / (A 1_S)_i, T_j = min_m p_m / (gamma (A_m^T
+1_counted)_j), gamma = sqrt(rho), rho = 3e4 / mean(b)^2 by default), the same pass structure (one pass over the
+orientation batches per iteration: the adjoint of the current subset's dual change, the update of z and x, the
+forward of the next subset) and the same state dict.
+
+Iteration, for the next subset m (p_m = 1 / M):
+    y_m'  <- prox_{S F_m*}(y_m + S A_m x)            rows of subset m, closed form in float64
+    dz    <- A_m^T (y_m' - y_m);  z <- z + dz;  x <- max(0, x - T (z + dz / p_m + lam))
+Device arrays: x, z, T (coefficient-sized), y, S, D (data-sized; D holds A_m x of the next subset and the dual
+change of the current one) and one batch-sized dz.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .arrays import as_host, check_device, is_device
+from .solvers import Reducer, as_device_data, periodic, support_mask_to_device
+
+RHO_AUTO = 3e4
+NAMES = ("x", "z", "T")
+
+
+class SPDHGPoisson:
+    """SPDHG over omega subsets for the Poisson deviance (module docstring)."""
+
+    def __init__(self, operator, subsets=8, prox_kind="nonneg", lam=0.0, support="fov", eps_counts=1e-3, rho="auto",
+                 seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None):
+        """Arguments as diffractom's SPDHGPoisson (spdhg_poisson.py:301-302). resident: accepted; the coefficient
+        arrays of a NumPy x0 are kept on the device when they fit (this package's streaming of solver state is the
+        operator's direct / adjoint streaming). tv > 0 (the TV block) is not provided."""
+        if prox_kind not in ("nonneg", "nonneg_l1"):
+            raise ValueError("SPDHGPoisson supports prox_kind 'nonneg' and 'nonneg_l1'")
+        if not (resident in ("auto", "all", "none") or set(resident) <= set(NAMES + ("qx", "qy"))):
+            raise ValueError(f"resident must be 'auto', 'all', 'none' or a list of names from {NAMES}")
+        if float(tv) != 0.0 or tv_tree is not None:
+            raise NotImplementedError("the total-variation block of SPDHGPoisson is not provided")
+        self.op = operator
+        self.ctx, self.queue = operator.ctx, operator.queue
+        self.subsets = operator.set_omega_subsets(subsets)
+        self.M = len(self.subsets)
+        self.lam = float(lam) if prox_kind == "nonneg_l1" else 0.0
+        self.eps_counts = float(eps_counts)
+        self.rho = rho if rho == "auto" else float(rho)
+        self.rng = np.random.default_rng(seed)
+        self.resident = resident
+        self.tv, self.tv_prob = 0.0, 0.0
+        self._p_data = 1.0 / self.M
+        self._inv_p_data = float(self.M)
+        self._last = None
+        self.support_gpu = support_mask_to_device(operator, support, operator.device)
+        self.state = None
+
+    # ---------------------------------------------------------------- schedule
+    def _epoch_order(self):
+        """A random permutation of the subsets that does not start with the last subset of the previous epoch
+        (spdhg_poisson.py:363-371)."""
+        perm = self.rng.permutation(self.M)
+        if self.M > 1 and int(perm[0]) == self._last:
+            perm[[0, 1]] = perm[[1, 0]]
+        self._last = int(perm[-1])
+        return [int(m) for m in perm]
+
+    def _epoch_sequence(self):
+        return self._epoch_order()
+
+    # ---------------------------------------------------------------- device steps
+    def _dual(self, m):
+        op = self.op
+        e = op._sub[m]
+        _lib.call("dfx_spdhg_dual_update", self.y.data_ptr(), self.D.data_ptr(), self.sig.data_ptr(),
+                  self.b.data_ptr(), _ptr(self.w), self.pw, _ptr(self.g), self.pg, _ptr(self.bg), self.pbg,
+                  self.eps_counts, e["omegas"].data_ptr(), e["n"], op.My * op.N_seg, op._s())
+
+    def _pass(self, adj, fwd):
+        """One pass over the batches: adjoint of subset adj's dual change (in D), z and x updated; then the forward
+        of the new x for subset fwd ("full": all rows) added to D (spdhg_poisson.py:430-484)."""
+        op = self.op
+        npix, kmax = op.npix, op.K_batch_max
+        s = op._s()
+        sub = None if fwd == "full" else fwd
+        for ib, b in enumerate(op.batches):
+            k0, kb = b["k_start"], b["K_batch"]
+            off = k0 * npix * 4
+            n = kb * npix
+            if adj is not None:
+                op._adjoint_batch(self.D, ib, self.dz, 0, kmax, subset=adj)
+                _lib.call("dfx_spdhg_primal_update", self.x.data_ptr() + off, self.z.data_ptr() + off,
+                          self.T.data_ptr() + off, self.dz.data_ptr(), float(self._inv_p_data), self.lam, n, s)
+            if fwd is not None:
+                op._direct_batch(self.x, k0, op.K, ib, self.D, sub)
+
+    def _deviance(self, mu):
+        return self.red.deviance(mu, self.b, self.w, self.pw, self.g, self.pg, self.bg, self.pbg, self.eps_counts)
+
+    # ---------------------------------------------------------------- run
+    def run(self, x0, b, n_epochs, weights=None, gain=None, background=None, verbose=0, diagnostics_interval=1,
+            callback=None, state=None):
+        """As diffractom's SPDHGPoisson.run (spdhg_poisson.py:513-751). x0: a CUDA tensor (updated in place and
+        returned) or a NumPy array (updated in place if C-contiguous float32, else converted; returned)."""
+        self._setup(x0, b, weights, gain, background, state)
+        self._iterate(n_epochs, verbose, diagnostics_interval, callback)
+        return self._finish()
+
+    def _setup(self, x0, b, weights=None, gain=None, background=None, state=None):
+        """Upload, step sizes S and T, support projection, warm start (spdhg_poisson.py:520-662)."""
+        self._t_start = time.perf_counter()
+        op = self.op
+        dev = op.device
+        cshape, dshape = tuple(op.coeff_shape), tuple(op.data_shape)
+        npix = op.npix
+        s = op._s()
+        self._x_on_gpu = is_device(x0)
+        self._host_x = None if self._x_on_gpu else as_host(x0, cshape, "x0")
+        self.x = check_device(x0, cshape, "x0") if self._x_on_gpu else torch.as_tensor(self._host_x, device=dev)
+        self.b = as_device_data(b, dshape, dev)
+        self.w, self.pw = periodic(weights, dshape, "weights", dev)
+        self.g, self.pg = periodic(gain, dshape, "gain", dev)
+        self.bg, self.pbg = periodic(background, dshape, "background", dev)
+        if self.pg and float(self.g.min().item()) <= 0:
+            raise ValueError("the gain must be positive everywhere")
+        self.red = Reducer(op)
+        self.y = torch.zeros(dshape, dtype=torch.float32, device=dev)
+        self.sig = torch.empty(dshape, dtype=torch.float32, device=dev)
+        self.D = torch.empty(dshape, dtype=torch.float32, device=dev)
+        self.dz = torch.empty(npix * op.K_batch_max, dtype=torch.float32, device=dev)
+        supp = self.support_gpu
+        sp = None if supp is None else supp.data_ptr()
+        npx = 0 if supp is None else npix
+
+        rho = self.rho
+        if rho == "auto":
+            sb, sn = self.red.mean_counted(self.b, self.w, self.pw)
+            mean_b = sb / max(sn, 1.0)
+            rho = RHO_AUTO / mean_b ** 2 if mean_b > 0 else 1.0
+        self.rho_used = float(rho)
+        gamma = np.sqrt(rho)
+        p = self._p_data
+        self.resident_used = NAMES
+        self.z = torch.zeros(cshape, dtype=torch.float32, device=dev)
+        if state is not None and state.get("z") is not None:
+            self.z.copy_(torch.as_tensor(as_host(state["z"], cshape, "state['z']")))
+        self.T = torch.empty(cshape, dtype=torch.float32, device=dev)
+
+        # S from the row sums A 1_S (spdhg_poisson.py:621-629)
+        op._fill(self.D, 0.0)
+        for ib, bt in enumerate(op.batches):
+            _lib.call("dfx_support_ones", self.dz.data_ptr(), sp, npx, npix * bt["K_batch"], s)
+            op._direct_batch(self.dz, 0, op.K_batch_max, ib, self.D)
+        rs, rn = self.red.mean_counted(self.D, self.w, self.pw)
+        bs, bn = self.red.mean_counted(self.b, self.w, self.pw)
+        self.scales = {"row_sum_mean": rs / max(rn, 1.0), "b_mean": bs / max(bn, 1.0),
+                       "gain_mean": 1.0 if self.pg == 0 else float(self.g.double().mean().item())}
+        _lib.call("dfx_dual_steps", self.sig.data_ptr(), self.D.data_ptr(), _ptr(self.w), self.pw, float(gamma),
+                  self.D.numel(), s)
+        # T from the subsets' column sums over the counted points (spdhg_poisson.py:630-643)
+        _lib.call("dfx_set_mask_ones", self.D.data_ptr(), _ptr(self.w), self.pw, self.D.numel(), s)
+        c = float(np.float32(p / gamma))
+        for ib, bt in enumerate(op.batches):
+            off = bt["k_start"] * npix * 4
+            n = bt["K_batch"] * npix
+            tb = self.T.data_ptr() + off
+            _lib.call("dfx_tinit", tb, n, s)
+            for m in range(self.M):
+                op._adjoint_batch(self.D, ib, self.dz, 0, op.K_batch_max, subset=m)
+                _lib.call("dfx_tmin", tb, self.dz.data_ptr(), sp, npx, c, n, s)
+            _lib.call("dfx_tfinal", tb, n, s)
+        _lib.call("dfx_project_support", self.x.data_ptr(), sp, npx, self.x.numel(), s)
+        if state is not None:
+            self.y.copy_(torch.as_tensor(as_host(state["y"], dshape, "state['y']")))
+            if state.get("z") is None:
+                op.adjoint_cl(self.y, self.z)
+        self._t_setup = time.perf_counter() - self._t_start
+        self._ep0 = int(state["epoch"]) if state is not None else 0
+        self.iter_stats = []
+        self._f = float("nan")
+        self._seq = self._epoch_sequence()
+        op.zero_subset_rows(self.D, self._seq[0])
+        self._pass(None, self._seq[0])
+
+    def _iterate(self, n_epochs, verbose=0, diagnostics_interval=1, callback=None, final=True):
+        """n_epochs epochs (spdhg_poisson.py:664-719). final=False: the last of them is not the run's last (no
+        closing full forward unless diagnostics fall there), so that epochs can be run in several calls."""
+        op = self.op
+        dev = op.device
+        seq = self._seq
+        for e in range(n_epochs):
+            ep = self._ep0 + len(self.iter_stats) + 1
+            last = final and e + 1 == n_epochs
+            want_f = (len(self.iter_stats) + 1) % max(1, diagnostics_interval) == 0 or last
+            nseq = None
+            for j, m in enumerate(seq):
+                end_of_epoch = j + 1 == len(seq)
+                if not end_of_epoch:
+                    nb = seq[j + 1]
+                elif not last:
+                    nseq = self._epoch_sequence()
+                    nb = nseq[0]
+                else:
+                    nb = None
+                self._dual(m)
+                if (end_of_epoch and want_f) or nb is None or nb == m:
+                    self._pass(m, None)
+                    if (end_of_epoch and want_f) or nb is not None:
+                        op._fill(self.D, 0.0)
+                        self._pass(None, "full")
+                        if end_of_epoch and want_f:
+                            self._f = self._deviance(self.D)
+                else:
+                    op.zero_subset_rows(self.D, nb)
+                    self._pass(m, nb)
+            if nseq is not None:
+                seq = nseq
+            self._seq = seq
+            if callback is not None or verbose:
+                op.stream().synchronize()
+            stats = {"epoch": ep, "f": self._f if want_f else None, "rho": self.rho_used,
+                     "time": time.perf_counter() - self._t_start}
+            self.iter_stats.append(stats)
+            stop = False
+            if callback is not None:
+                if not self._x_on_gpu:
+                    self._host_x[...] = self.x.cpu().numpy()
+                stop = bool(callback(ep, self.x if self._x_on_gpu else self._host_x, stats))
+            if verbose and want_f:
+                print(f"[spdhg epoch {ep:4d}] f={self._f:.8e} {time.perf_counter() - self._t_start:.1f} s",
+                      flush=True)
+            if stop:
+                break
+
+    def _finish(self):
+        self.state = {"epoch": self._ep0 + len(self.iter_stats), "z": self.z.cpu().numpy(), "y": self.y.cpu().numpy()}
+        self.final_stats = {"epochs": len(self.iter_stats), "final_f": self._f, "setup_s": self._t_setup,
+                            "rho": self.rho_used, "subsets": self.M, "resident": self.resident_used,
+                            "time": time.perf_counter() - self._t_start, "tv": 0.0, "tv_prob": 0.0, **self.scales}
+        x = self.x
+        if not self._x_on_gpu:
+            self._host_x[...] = x.cpu().numpy()
+        out = x if self._x_on_gpu else self._host_x
+        self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = self.dz = self.z = self.T = None
+        self.x = None
+        return out
+
+
+def _ptr(t):
+    return None if t is None else t.data_ptr()

@@ -1,0 +1,178 @@
+/*
+ * diffractom_b200 — C ABI of the sm_100a kernels of diffractom's reconstruction hot path.
+ *
+ * Every entry point enqueues work on the CUDA stream it is given (a cudaStream_t passed as void *, NULL = the legacy
+ * default stream) and returns at once; it allocates nothing: buffers, including scratch, are passed in by the caller
+ * (sizes from the *_scratch_bytes queries). Device pointers are plain CUDA device addresses. Layouts follow the
+ * reference: coefficients (K, Ny, Nx) float32 C order, data (N_Omega, My, N_eta * N_rings) with segment
+ * j = eta_bin * N_rings + ring, channel-fastest batch buffers img_k (Nx * Ny, Kstride) and sino_k (angles, My, Kstride).
+ *
+ * Return value: DFX_OK, or an error code; dfx_last_error() then describes it (per host thread). No C++ exception
+ * crosses this interface.
+ *
+ * Each declaration names the reference code it replaces (file:line within msaca-okse/diffractom, src/diffractom/
+ * abbreviated): OpenCL kernels launched through pyopencl, which are the reference's only "foreign" interface on this
+ * path; the Python methods that launch them are mirrored by the package diffractom_b200 on top of this ABI.
+ */
+#ifndef DIFFRACTOM_B200_H
+#define DIFFRACTOM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DFX_OK 0
+#define DFX_EINVAL 1     /* bad argument (size, alignment, null pointer, out-of-range option) */
+#define DFX_ENOMEM 2     /* scratch too small */
+#define DFX_ELAUNCH 3    /* a kernel launch failed */
+#define DFX_ETIMEOUT 4   /* a bounded device-side wait ran out */
+#define DFX_ECUDA 5      /* another CUDA runtime error */
+
+#define DFX_ABI_VERSION 1
+
+int dfx_abi_version(void);
+const char *dfx_last_error(void);
+/* Number of kernels this library has launched since it was loaded (all host threads); no reference counterpart
+ * (instrumentation for benchmarks). */
+uint64_t dfx_launch_count(void);
+
+/* ---------------------------------------------------------------- parallel-beam Radon transform
+ * geo: (n_angles, 4) float32 device array (X, Y, T0, angle weight), operators/parallel_radon.py:106-124.
+ * kernel: 0 hat, 1 trapezoid (pixel footprint). Channels k < kb of kstride are computed, kstride % 8 == 0,
+ * channels kb .. kstride-1 of the output are written as 0. */
+
+/* replaces gather_channels_k_fastest (operators/radon_kernels.cl:222-244; ParallelRadon.gather, parallel_radon.py:221-229):
+ * img_k[p, k] = coeffs[k0 + k, p] for k < kb, 0 for kb <= k < kstride. */
+int dfx_gather_channels(const float *coeffs, float *img_k, int64_t npix, int k0, int kb, int kstride, void *stream);
+
+/* replaces scatter_channels_k_fastest (radon_kernels.cl:192-215; ParallelRadon.scatter, parallel_radon.py:231-236):
+ * coeffs[k0 + k, p] = img_k[p, k] for k < kb. */
+int dfx_scatter_channels(const float *img_k, float *coeffs, int64_t npix, int k0, int kb, int kstride, void *stream);
+
+/* replaces radon_forward_k / radon_forward_tiled (radon_kernels.cl:44-101, 262-372; ParallelRadon.forward,
+ * parallel_radon.py:283-301): sino_k[a, s, k] = scale * sum_pixels K(t_a(pixel) - s) img_k[pixel, k]. */
+int dfx_radon_forward(const float *img_k, float *sino_k, const float *geo, int n_angles, int nx, int ny, int n_det,
+                      int kstride, int kb, int kernel, float scale, void *stream);
+
+/* replaces radon_backward_k / radon_backward_tiled (radon_kernels.cl:106-141, 378-449; ParallelRadon.backward,
+ * parallel_radon.py:303-318): img_k[pixel, k] = sum_a w_a sum_s K(t_a(pixel) - s) sino_k[a, s, k], pixel-driven, no
+ * atomics. n_taps: the most bins a pixel touches (ParallelRadon.n_taps). */
+int dfx_radon_backward(const float *sino_k, float *img_k, const float *geo, int n_angles, int nx, int ny, int n_det,
+                       int kstride, int kb, int kernel, int n_taps, void *stream);
+
+/* ---------------------------------------------------------------- pole-figure matrix
+ * The PF entry of (angle r, orientation k, eta bin c, ring p) is pf_entry of operators/pf_generate.cl:62-140
+ * (== pfmatrix_eval_poles, operators/create_pfo_matrix.py:108-199), times the ring intensity unless normalized. */
+typedef struct dfx_pf_geometry {
+    const float *coords;       /* (R, S, C, S_eta, P, 3) probed directions */
+    const float *poles;        /* (K, A, 3) pole axes rotated by every orientation */
+    const int32_t *axis_start; /* (P + 1) */
+    const float *axis_count;   /* (A) */
+    const float *inv_sigma2;   /* (K) */
+    const float *norm;         /* (K) 1 / (8 pi sigma^2) */
+    const float *quad_w;       /* (S * S_eta) product weights, NULL: the midpoint rule (mean over the nodes) */
+    const float *intens;       /* (P) ring intensities, NULL: normalized (every ring weight 1) */
+    int32_t R, C, P, A, S, S_eta, K;
+    float cut;                 /* exponent at which the Gaussian is cut (pf_cutoff_sigma^2 / 2) */
+} dfx_pf_geometry;
+
+/* replaces pfmatrix_eval_poles + SCALE_PF_BY_INTENSITY_INPLACE (create_pfo_matrix.py:108-199, pf_kernels.cl:450-465;
+ * SPFO:1130-1164): dense batch out (R, kb, C, P) of orientations k0 .. k0+kb-1. */
+int dfx_pf_dense(const dfx_pf_geometry *g, int k0, int kb, float *out, void *stream);
+
+/* Sparse PF of a batch of orientations k0 .. k0+kb-1, restricted to the angles rows[0 .. n_rows-1] (rows NULL: all R
+ * angles). Replaces the generator pf_gen_* (pf_generate.cl:146-377, pf_generate.py:218-303) and the dense-batch CSR
+ * build pf_count_rows_* / pf_fill_rows_* (pf_kernels.cl:482-548): the CSR is the one of the dense batch, bit for bit
+ * in its structure.
+ *   forward_rows = 0: adjoint rows (s, k) = s * kb + k listing eta/ring segments j ascending (col: j)
+ *   forward_rows = 1: forward rows (s, j) = s * C * P + j listing orientations k ascending (col: k)
+ * count: counts[row] = non-zeros of the row (row_ptr = exclusive scan of counts, dfx_scan_exclusive_i32);
+ * fill:  col (uint16) and val at row_ptr[row] .. row_ptr[row + 1]. */
+int dfx_pf_csr_count(const dfx_pf_geometry *g, const int32_t *rows, int n_rows, int k0, int kb, int forward_rows,
+                     int32_t *counts, void *stream);
+int dfx_pf_csr_fill(const dfx_pf_geometry *g, const int32_t *rows, int n_rows, int k0, int kb, int forward_rows,
+                    const int32_t *row_ptr, uint16_t *col, float *val, void *stream);
+
+/* Exclusive prefix sum of n int32 (out may alias in), replaces pyopencl's ExclusiveScanKernel (pf_generate.py:69):
+ * out[0] = 0, out[i] = in[0] + ... + in[i - 1] for i <= n (out has n + 1 entries; in is read for i < n). */
+size_t dfx_scan_scratch_bytes(int64_t n);
+int dfx_scan_exclusive_i32(const int32_t *in, int32_t *out, int64_t n, void *scratch, size_t scratch_bytes,
+                           void *stream);
+
+/* replaces spmm_pf_forward_c / spmm_pf_forward_sub (pf_kernels.cl:597-641, SPFO:38-80): for the n_sub angles
+ * omegas (NULL: all, n_sub = R): data[omegas[s], y, j] += sum_k val * sino[s, y, k] over the forward CSR; rows of the
+ * CSR are s * CP + j if compact, else omegas[s] * CP + j. Empty CSR rows leave data untouched. */
+int dfx_spmm_pf_forward(const float *sino, const int32_t *row_ptr, const uint16_t *col_k, const float *val,
+                        float *data, const int32_t *omegas, int n_sub, int my, int cp, int kstride, int kb,
+                        int compact, void *stream);
+
+/* replaces spmm_pf_adjoint_c / spmm_pf_adjoint_sub (pf_kernels.cl:644-687, SPFO:82-123):
+ * sino[s, y, k] = alpha * sum_j val * data[omegas[s], y, j] for k < kb over the adjoint CSR (rows s * kb + k if
+ * compact, else omegas[s] * kb + k); channels kb .. kstride-1 of sino are set to 0. */
+int dfx_spmm_pf_adjoint(const float *data, const int32_t *row_ptr, const uint16_t *col_j, const float *val,
+                        float *sino, const int32_t *omegas, int n_sub, int my, int kb, int cp, int kstride,
+                        float alpha, int compact, void *stream);
+
+/* replaces zero_rows (SPFO:126-132): data rows omegas[s] (row_len floats each) <- 0. */
+int dfx_zero_rows(float *data, const int32_t *omegas, int n_sub, int64_t row_len, void *stream);
+
+/* replaces data.fill(0.0) of the pyopencl arrays (SPFO:1658 and the solvers): x[0 .. n-1] = value. */
+int dfx_fill_f32(float *x, float value, int64_t n, void *stream);
+
+/* ---------------------------------------------------------------- Poisson solvers
+ * Periodic arrays (weights w, gain g, background bg): element i uses a[i % period]; period 0: the constant 1, 1, 0
+ * (fista_poisson.py:287-308). */
+
+/* replaces dual_update_sub (optimization/spdhg_poisson.py:69-91): on the rows of the angles omegas (row_len data
+ * points each), d holds A x on entry and the dual change on exit; y <- prox_{sigma F*}(y + sigma A x), float64 math. */
+int dfx_spdhg_dual_update(float *y, float *d, const float *sig, const float *b, const float *w, int64_t pw,
+                          const float *g, int64_t pg, const float *bg, int64_t pbg, float eps,
+                          const int32_t *omegas, int n_sub, int64_t row_len, void *stream);
+
+/* replaces spdhg_update (spdhg_poisson.py:95-106): z += dz; x = T > 0 ? max(0, x - T (z + inv_p dz + lam)) : 0. */
+int dfx_spdhg_primal_update(float *x, float *z, const float *T, const float *dz, float inv_p, float lam, int64_t n,
+                            void *stream);
+
+/* replaces dual_steps (optimization/pdhg_poisson.py:79-84): sig = w != 0 && rowsum > 0 ? sigma0 / rowsum : 0. */
+int dfx_dual_steps(float *sig, const float *rowsum, const float *w, int64_t pw, float sigma0, int64_t n, void *stream);
+
+/* replaces set_mask_ones (pdhg_poisson.py:113-116): u = w != 0 ? 1 : 0. */
+int dfx_set_mask_ones(float *u, const float *w, int64_t pw, int64_t n, void *stream);
+
+/* replaces tinit / tmin / tfinal (spdhg_poisson.py:252-272), on n elements of a batch of whole images (npix pixels
+ * each, supp (npix) uint8 or NULL): T = +inf; T = min(T, c / colsum) where inside and colsum > 0; T = 0 where +inf. */
+int dfx_tinit(float *T, int64_t n, void *stream);
+int dfx_tmin(float *T, const float *colsum, const uint8_t *supp, int64_t npix, float c, int64_t n, void *stream);
+int dfx_tfinal(float *T, int64_t n, void *stream);
+
+/* replaces support_ones / project_support (fista_poisson.py:256-263, 277-281): x = inside ? 1 : 0;
+ * x = 0 where outside or x < 0. */
+int dfx_support_ones(float *x, const uint8_t *supp, int64_t npix, int64_t n, void *stream);
+int dfx_project_support(float *x, const uint8_t *supp, int64_t npix, int64_t n, void *stream);
+
+/* FP64 reductions. Each writes its sums (float64) to out on the device; the partials go through scratch
+ * (dfx_reduce_scratch_bytes(n) bytes). */
+size_t dfx_reduce_scratch_bytes(int64_t n);
+
+/* replaces poisson_value_grad (fista_poisson.py:72-113) with write_grad and mode: out[0] = sum_i w/g [m - b + b log(b/m)]
+ * (mode 0, m = max(mu, 0) + bg + eps g) or its quadratic approximation at the data (mode 1); write_grad: mu <- df/dmu. */
+int dfx_poisson_value_grad(float *mu, const float *b, const float *w, int64_t pw, const float *g, int64_t pg,
+                           const float *bg, int64_t pbg, float eps, int write_grad, int mode, float floor_counts,
+                           int64_t n, double *out, void *scratch, size_t scratch_bytes, void *stream);
+
+/* replaces mean_counted (pdhg_poisson.py:97-111): out[0] = sum of b over w != 0, out[1] = their number. */
+int dfx_mean_counted(const float *b, const float *w, int64_t pw, int64_t n, double *out, void *scratch,
+                     size_t scratch_bytes, void *stream);
+
+/* sums of x (and of x^2, x * y) in float64 for diagnostics and power iterations (replaces clarray.sum / vdot,
+ * SPFO:2169-2185): out[0] = sum x_i y_i (y NULL: sum x_i). */
+int dfx_dot_f64(const float *x, const float *y, int64_t n, double *out, void *scratch, size_t scratch_bytes,
+                void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

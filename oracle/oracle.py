@@ -1,0 +1,286 @@
+"""CPU oracle of diffractom's reconstruction hot path: TEST INFRASTRUCTURE ONLY.
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm, as the checker of the CUDA
+kernels or as the timed CPU baseline; the package diffractom_b200 never imports it. It wraps oracle/_build/liboracle.so
+(the C restatement in oracle.c / oracle_core.h, built by oracle/Makefile) and composes its functions into the operator
+and the SPDHG iteration of the reference (functions cite the reference file:line they follow):
+
+  OracleOperator    forward / adjoint of SinglePhaseForwardOperator (SPFO:1646-1728, 1966-2033), full or per angle
+                    subset, batch by batch, with the PF matrix evaluated densely (create_pfo_matrix.py:108-199) and
+                    compacted into the two CSR copies (pf_kernels.cl:482-548)
+  spdhg_reference   SPDHGPoisson.run (optimization/spdhg_poisson.py:513-751) for GPU-resident arrays, without TV
+
+Parity pins (tests/test_oracle.py): OracleOperator against the reference's float64 ReferenceModel on the golden
+fixtures of tests/golden (forward and transpose within 2e-5 of the maximum, as the reference's own
+tests/test_differentiable.py:31-40; the PF matrix likewise), and the host geometry against the same fixtures.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from ctypes import c_double, c_float, c_int, c_int64, c_uint64, c_void_p
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        h = ctypes.CDLL(str(LIB))
+        P, I, F = c_void_p, c_int, c_float
+        for suf in ("_f64", "_f32"):
+            getattr(h, "orc_radon_forward" + suf).argtypes = [P, P, P, I, I, I, I, I, I, I, F]
+            getattr(h, "orc_radon_backward" + suf).argtypes = [P, P, P, I, I, I, I, I, I, I]
+            getattr(h, "orc_spmm_forward" + suf).argtypes = [P, P, P, P, P, P, I, I, I, I, I]
+            getattr(h, "orc_spmm_adjoint" + suf).argtypes = [P, P, P, P, P, P, I, I, I, I, I, F, I]
+        h.orc_pf_dense.argtypes = [P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, I]
+        h.orc_csr_counts.argtypes = [P, I, I, I, P, P]
+        h.orc_csr_fill.argtypes = [P, I, I, I, P, P, P, P, P, P]
+        h.orc_dual_update_sub.argtypes = [P, P, P, P, P, c_uint64, P, c_uint64, P, c_uint64, F, P, c_uint64,
+                                          c_uint64]
+        h.orc_spdhg_update.argtypes = [P, P, P, P, F, F, c_uint64]
+        h.orc_deviance.argtypes = [P, P, P, c_uint64, P, c_uint64, P, c_uint64, F, c_uint64]
+        h.orc_deviance.restype = c_double
+        h.orc_num_threads.restype = c_int
+        _lib = h
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(c_void_p)
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+class OracleOperator:
+    """The reference operator on the CPU from its host geometry (float32 arrays as the reference uploads them)."""
+
+    def __init__(self, *, coords, poles, axis_start, axis_count, inv_sigma2, norm, quad_w, geo, scale, n_taps,
+                 kernel, Nx, Ny, My, cut, batches, intens=None, precision="f64"):
+        self.coords = _c(coords, np.float32)
+        self.R, self.S, self.C, self.Se, self.P = self.coords.shape[:5]
+        self.poles = _c(poles, np.float32)
+        self.K, self.A = self.poles.shape[:2]
+        self.axis_start = _c(axis_start, np.int32)
+        self.axis_count = _c(axis_count, np.float32)
+        self.inv_sigma2, self.norm = _c(inv_sigma2, np.float32), _c(norm, np.float32)
+        self.quad_w = None if quad_w is None or np.size(quad_w) == 0 else _c(quad_w, np.float32)
+        self.intens = None if intens is None else _c(intens, np.float32)
+        self.geo = _c(geo, np.float32)
+        self.scale, self.n_taps = float(scale), int(n_taps)
+        self.kernel = 1 if kernel in ("trapezoid", 1) else 0
+        self.Nx, self.Ny, self.My = int(Nx), int(Ny), int(My)
+        self.cut = float(cut)
+        self.CP = self.C * self.P
+        self.batches = [(int(k0), int(kb)) for k0, kb in batches]
+        self.suffix = "_" + precision
+        self._csr = {}
+
+    @classmethod
+    def from_operator(cls, op, precision="f64", batches=None):
+        """The oracle of a diffractom_b200 operator (or of its OperatorGeometry): its host arrays and its batches
+        (default: the operator's, one batch of all orientations for a bare geometry)."""
+        if batches is None:
+            batches = ([(b["k_start"], b["K_batch"]) for b in op.batches] if hasattr(op, "batches")
+                       else [(0, op.K)])
+        return cls(coords=op.coords_cpu, poles=op.poles_cpu, axis_start=op.axis_start_cpu, axis_count=op.axis_count_cpu,
+                   inv_sigma2=op.inv_sigma2_cpu, norm=op.norm_factor_cpu, quad_w=op.quad_weights_cpu,
+                   geo=op.radon_geo.geo, scale=op.radon_geo.scale, n_taps=op.radon_geo.n_taps, kernel=op.radon_kernel,
+                   Nx=op.Nx, Ny=op.Ny, My=op.My, cut=op.pf_cut, batches=batches,
+                   intens=None if op.normalized else op.intens_cpu, precision=precision)
+
+    # ---- PF matrix
+    def pf_dense(self, k0, kb):
+        out = np.empty((self.R, kb, self.C, self.P), np.float32)
+        lib().orc_pf_dense(_p(self.coords), _p(self.poles), _p(self.axis_start), _p(self.axis_count),
+                           _p(self.inv_sigma2), _p(self.norm), _p(self.quad_w), _p(self.intens), _p(out), self.R, k0,
+                           kb, self.C, self.P, self.A, self.S, self.Se, self.cut, int(self.intens is None))
+        return out
+
+    def csr(self, k0, kb):
+        """Both CSR copies of the batch (adjoint rows r * kb + k over j; forward rows r * CP + j over k)."""
+        key = (k0, kb)
+        if key not in self._csr:
+            pf = _c(self.pf_dense(k0, kb).reshape(self.R, kb, self.CP), np.float32)
+            ca = np.empty(self.R * kb, np.int32)
+            cf = np.empty(self.R * self.CP, np.int32)
+            lib().orc_csr_counts(_p(pf), self.R, kb, self.CP, _p(ca), _p(cf))
+            pa = np.zeros(self.R * kb + 1, np.int32)
+            np.cumsum(ca, out=pa[1:])
+            pfw = np.zeros(self.R * self.CP + 1, np.int32)
+            np.cumsum(cf, out=pfw[1:])
+            nnz = int(pa[-1])
+            cj, va = np.empty(max(nnz, 1), np.uint16), np.empty(max(nnz, 1), np.float32)
+            ck, vf = np.empty(max(nnz, 1), np.uint16), np.empty(max(nnz, 1), np.float32)
+            lib().orc_csr_fill(_p(pf), self.R, kb, self.CP, _p(pa), _p(cj), _p(va), _p(pfw), _p(ck), _p(vf))
+            self._csr[key] = dict(row_ptr_a=pa, col_j=cj[:nnz], val_a=va[:nnz], row_ptr_f=pfw, col_k=ck[:nnz],
+                                  val_f=vf[:nnz], nnz=nnz)
+        return self._csr[key]
+
+    # ---- operator
+    def forward(self, x, subset=None, data=None):
+        """data (R, My, CP) = A x; subset (angle indices): only those rows are written (the others kept from data,
+        default zeros)."""
+        x = _c(x, np.float32).reshape(self.K, -1)
+        npix = self.Nx * self.Ny
+        if data is None:
+            data = np.zeros((self.R, self.My, self.CP), np.float32)
+        else:
+            data = _c(data, np.float32)
+        angles = np.arange(self.R) if subset is None else np.asarray(subset, np.int64)
+        data[angles] = 0.0
+        om = _c(angles, np.int32)
+        geo = _c(self.geo[angles], np.float32)
+        L = lib()
+        for k0, kb in self.batches:
+            img = _c(x[k0:k0 + kb].T, np.float32)                    # (npix, kb) channel-fastest
+            sino = np.empty((len(angles), self.My, kb), np.float32)
+            getattr(L, "orc_radon_forward" + self.suffix)(_p(img), _p(sino), _p(geo), len(angles), self.Nx, self.Ny,
+                                                          self.My, kb, kb, self.kernel, self.scale)
+            c = self.csr(k0, kb)
+            getattr(L, "orc_spmm_forward" + self.suffix)(_p(sino), _p(c["row_ptr_f"]), _p(c["col_k"]), _p(c["val_f"]),
+                                                         _p(data), _p(om), len(angles), self.My, self.CP, kb, 0)
+        return data
+
+    def adjoint(self, data, subset=None):
+        """coeffs (K, Ny, Nx) = A^T data (subset: the rows of those angles only)."""
+        data = _c(data, np.float32)
+        npix = self.Nx * self.Ny
+        angles = np.arange(self.R) if subset is None else np.asarray(subset, np.int64)
+        om = _c(angles, np.int32)
+        geo = _c(self.geo[angles], np.float32)
+        out = np.empty((self.K, npix), np.float32)
+        alpha = float(np.float32(self.R / np.pi))
+        L = lib()
+        for k0, kb in self.batches:
+            c = self.csr(k0, kb)
+            sino = np.empty((len(angles), self.My, kb), np.float32)
+            getattr(L, "orc_spmm_adjoint" + self.suffix)(_p(data), _p(c["row_ptr_a"]), _p(c["col_j"]),
+                                                         _p(c["val_a"]), _p(sino), _p(om), len(angles), self.My, kb,
+                                                         self.CP, kb, alpha, 0)
+            img = np.empty((npix, kb), np.float32)
+            getattr(L, "orc_radon_backward" + self.suffix)(_p(sino), _p(img), _p(geo), len(angles), self.Nx, self.Ny,
+                                                           self.My, kb, kb, self.kernel)
+            out[k0:k0 + kb] = img.T
+        return out.reshape(self.K, self.Ny, self.Nx)
+
+
+def periodic(a, n_data, dshape):
+    """(array, period) as the solvers take weights / gain / background (fista_poisson.py:287-308)."""
+    if a is None:
+        return None, 0
+    h = np.ascontiguousarray(a, dtype=np.float32).ravel()
+    if h.size == 1:
+        h = np.full(dshape[-1], float(h[0]), np.float32)
+    return h, int(h.size)
+
+
+def deviance(mu, b, w=None, g=None, bg=None, eps=1e-3):
+    """Poisson deviance in float64 (fista_poisson.py:72-113, mode 0)."""
+    mu, b = _c(mu, np.float32), _c(b, np.float32)
+    w, pw = periodic(w, b.size, b.shape)
+    g, pg = periodic(g, b.size, b.shape)
+    bg, pbg = periodic(bg, b.size, b.shape)
+    return float(lib().orc_deviance(_p(mu), _p(b), _p(w), pw, _p(g), pg, _p(bg), pbg, eps, b.size))
+
+
+def epoch_order(rng, M, last):
+    """SPDHGPoisson._epoch_order (spdhg_poisson.py:363-371): a permutation not starting with the last subset."""
+    perm = rng.permutation(M)
+    if M > 1 and int(perm[0]) == last:
+        perm[[0, 1]] = perm[[1, 0]]
+    return [int(m) for m in perm], int(perm[-1])
+
+
+def spdhg_reference(op: OracleOperator, subsets, b, n_epochs, x0=None, weights=None, gain=None, background=None,
+                    support=None, eps_counts=1e-3, rho="auto", seed=0, lam=0.0, diagnostics_interval=1):
+    """SPDHGPoisson.run without TV for arrays on the device (spdhg_poisson.py:513-719, setup 558-662): returns
+    (x, y, z, [deviance per diagnostics epoch], rho). The float64 parts (dual prox, deviance, mean) are float64
+    here as in the reference; the operator is the oracle's."""
+    L = lib()
+    R, My, CP = op.R, op.My, op.CP
+    dshape = (R, My, CP)
+    b = _c(b, np.float32)
+    n = b.size
+    row = My * CP
+    w, pw = periodic(weights, n, dshape)
+    g, pg = periodic(gain, n, dshape)
+    bg, pbg = periodic(background, n, dshape)
+    M = len(subsets)
+    subsets = [np.asarray(s, np.int64) for s in subsets]
+    p = 1.0 / M
+    K, npix = op.K, op.Nx * op.Ny
+    supp = np.ones(npix, bool) if support is None else np.asarray(support, bool).ravel()
+    wv = np.ones(n, np.float32) if w is None else np.resize(w, n)
+    counted = wv != 0
+    if rho == "auto":
+        sb, sn = float(np.sum(b.ravel()[counted], dtype=np.float64)), float(np.count_nonzero(counted))
+        mean_b = sb / max(sn, 1.0)
+        rho = 3e4 / mean_b ** 2 if mean_b > 0 else 1.0
+    gamma = np.sqrt(rho)
+    ones = np.broadcast_to(supp.astype(np.float32), (K, npix)).reshape(K, op.Ny, op.Nx)
+    rowsum = op.forward(ones)
+    sig = np.where(counted.reshape(dshape) & (rowsum > 0), np.float32(gamma) / np.where(rowsum > 0, rowsum, 1),
+                   0).astype(np.float32)
+    mask = counted.reshape(dshape).astype(np.float32)
+    T = np.full((K, npix), np.inf, np.float32)
+    for s in subsets:
+        cs = op.adjoint(mask, subset=s).reshape(K, npix)
+        upd = supp[None, :] & (cs > 0)
+        T = np.where(upd, np.minimum(T, np.float32(p / gamma) / np.where(cs > 0, cs, 1)), T).astype(np.float32)
+    T[np.isinf(T)] = 0.0
+    x = np.zeros((K, npix), np.float32) if x0 is None else _c(x0, np.float32).reshape(K, npix).copy()
+    x[:, ~supp] = 0.0
+    x = np.maximum(x, 0)
+    z = np.zeros((K, npix), np.float32)
+    y = np.zeros(dshape, np.float32)
+    D = np.zeros(dshape, np.float32)
+    rng = np.random.default_rng(seed)
+    last = None
+    devs = []
+    seq, last = epoch_order(rng, M, last)
+    D = op.forward(x, subset=subsets[seq[0]], data=D)
+    inv_p = np.float32(M)
+    for e in range(n_epochs):
+        final = e + 1 == n_epochs
+        want = (e + 1) % max(1, diagnostics_interval) == 0 or final
+        nseq = None
+        for j, m in enumerate(seq):
+            eoe = j + 1 == len(seq)
+            if not eoe:
+                nb = seq[j + 1]
+            elif not final:
+                nseq, last = epoch_order(rng, M, last)
+                nb = nseq[0]
+            else:
+                nb = None
+            om = _c(subsets[m], np.int32)
+            L.orc_dual_update_sub(_p(y), _p(D), _p(sig), _p(b), _p(w), pw, _p(g), pg, _p(bg), pbg, eps_counts,
+                                  _p(om), row, len(om) * row)
+            dz = op.adjoint(D, subset=subsets[m]).reshape(K, npix)
+            L.orc_spdhg_update(_p(x), _p(z), _p(T), _p(_c(dz, np.float32)), float(inv_p), float(lam), x.size)
+            if (eoe and want) or nb is None or nb == m:
+                if (eoe and want) or nb is not None:
+                    D = op.forward(x)
+                    if eoe and want:
+                        devs.append(deviance(D, b, w, g, bg, eps_counts))
+            else:
+                D = op.forward(x, subset=subsets[nb], data=D)
+        if nseq is not None:
+            seq = nseq
+    return x.reshape(K, op.Ny, op.Nx), y, z.reshape(K, op.Ny, op.Nx), devs, rho

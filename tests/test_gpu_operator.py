@@ -1,0 +1,143 @@
+"""The CUDA operator against the CPU oracle (same geometry, same batches) and against the reference's fixtures:
+forward / adjoint values, the sparse PF structure bit for bit, the adjoint identity over the reference's angle
+ranges, the omega-subset forms in both PF storage modes, NumPy streaming, and reproducibility."""
+import numpy as np
+import pytest
+
+from conftest import CASES, case_inputs
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def make_operator(d, **kw):
+    from diffractom_b200 import SinglePhaseForwardOperator
+    cfg, mat, grid = case_inputs(d)
+    kw.setdefault("max_gb", 1e-5)
+    return SinglePhaseForwardOperator(cfg, mat, grid, normalized=True, quadrature=d["quadrature"],
+                                      radon_kernel=d["kernel"], **kw)
+
+
+def oracle_of(op):
+    from oracle.oracle import OracleOperator
+    return OracleOperator.from_operator(op)
+
+
+def rel(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - b).max() / np.abs(b).max())
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_forward_adjoint_match_oracle_and_reference(golden, name):
+    d = golden(name)
+    op = make_operator(d)
+    assert len(op.batches) > 1
+    orc = oracle_of(op)
+    c = torch.as_tensor(d["c"], device="cuda")
+    r = torch.as_tensor(d["r"], device="cuda")
+    fwd = op.direct(c).cpu().numpy()
+    adj = op.adjoint(r).cpu().numpy()
+    assert rel(fwd, orc.forward(d["c"])) < 1e-5
+    assert rel(adj, orc.adjoint(d["r"])) < 1e-5
+    # the reference's own tolerance against its float64 model (tests/test_differentiable.py:39)
+    assert rel(fwd, d["fwd"]) < 2e-5
+    assert rel(adj * np.float64(d["scale"]), d["adj"]) < 2e-5
+
+
+@pytest.mark.parametrize("name", ["diff_auto_trapezoid", "al5_small", "ti8_small"])
+def test_sparse_pf_structure_is_bit_exact(golden, name):
+    d = golden(name)
+    op = make_operator(d)
+    orc = oracle_of(op)
+    for sb, b in zip(op.sparse_batches, op.batches):
+        ref = orc.csr(b["k_start"], b["K_batch"])
+        nnz = ref["nnz"]
+        assert sb["nnz"] == nnz
+        for dev_key, ref_key in (("row_ptr_a", "row_ptr_a"), ("row_ptr_f", "row_ptr_f")):
+            assert np.array_equal(sb[dev_key].cpu().numpy(), ref[ref_key])
+        assert np.array_equal(sb["col_j"].cpu().numpy()[:nnz].view(np.uint16), ref["col_j"])
+        assert np.array_equal(sb["col_k"].cpu().numpy()[:nnz].view(np.uint16), ref["col_k"])
+        for key in ("val_a", "val_f"):
+            v = sb[key].cpu().numpy()[:nnz].astype(np.float64)
+            np.testing.assert_allclose(v, ref[key], rtol=2e-6, atol=0)   # float32 exp: a few ulp
+
+
+@pytest.mark.parametrize("name", ["adj_0_180", "adj_0_360", "adj_0_90", "adj_180_0"])
+def test_adjoint_is_transpose(golden, name):
+    d = golden(name)
+    op = make_operator(d)
+    rng = np.random.default_rng(1)
+    x = (rng.random(op.coeff_shape) * op.support_mask()[None]).astype(np.float32)
+    y = rng.random(op.data_shape).astype(np.float32)
+    ax = op.direct(torch.as_tensor(x, device="cuda")).cpu().numpy()
+    aty = op.adjoint(torch.as_tensor(y, device="cuda")).cpu().numpy()
+    lhs = float(np.dot(x.ravel().astype(np.float64), aty.ravel()))
+    rhs = float(np.dot(ax.ravel().astype(np.float64), y.ravel()))
+    assert rhs > 0 and abs(lhs / rhs - 1) < 1e-5
+
+
+@pytest.mark.parametrize("pf_mode", ["sparse", "generated"])
+@pytest.mark.parametrize("subsets", [4, "blocks"])
+def test_subset_forward_and_adjoint(golden, pf_mode, subsets):
+    d = golden("adj_0_360")
+    op = make_operator(d, pf_mode=pf_mode)
+    assert op.pf_mode == pf_mode and len(op.batches) > 1
+    R = op.N_Omega
+    subs = op.set_omega_subsets(4 if subsets == 4 else [np.arange(0, 7), np.arange(7, 20), np.arange(20, R)])
+    rng = np.random.default_rng(6)
+    x = (rng.random(op.coeff_shape) * op.support_mask()[None]).astype(np.float32)
+    y = rng.random(op.data_shape).astype(np.float32)
+    xd, yd = torch.as_tensor(x, device="cuda"), torch.as_tensor(y, device="cuda")
+    full = op.direct(xd).cpu().numpy()
+    adj = op.adjoint(yd).cpu().numpy()
+    adj_sum = np.zeros_like(adj)
+    for m, s in enumerate(subs):
+        dd = torch.full(op.data_shape, -7.0, device="cuda")
+        op.direct_cl(xd, dd, subset=m)
+        dd = dd.cpu().numpy()
+        np.testing.assert_allclose(dd[s], full[s], rtol=1e-5, atol=1e-6 * np.abs(full).max())
+        assert np.all(dd[np.setdiff1d(np.arange(R), s)] == -7.0)
+        a_m = torch.empty(op.coeff_shape, device="cuda")
+        op.adjoint_cl(yd, a_m, subset=m)
+        a_m = a_m.cpu().numpy()
+        adj_sum += a_m
+        lhs = float(np.dot(dd[s].ravel().astype(np.float64), y[s].ravel()))
+        rhs = float(np.dot(x.ravel().astype(np.float64), a_m.ravel()))
+        assert abs(lhs / rhs - 1) < 1e-5
+    np.testing.assert_allclose(adj_sum, adj, rtol=1e-4, atol=1e-5 * np.abs(adj).max())
+
+
+def test_generated_equals_stored(golden):
+    d = golden("al5_small")
+    a, b = make_operator(d, pf_mode="sparse"), make_operator(d, pf_mode="generated")
+    c = torch.as_tensor(d["c"], device="cuda")
+    r = torch.as_tensor(d["r"], device="cuda")
+    assert torch.equal(a.direct(c), b.direct(c))
+    assert torch.equal(a.adjoint(r), b.adjoint(r))
+
+
+def test_numpy_streaming_equals_device_and_is_reproducible(golden):
+    d = golden("ti8_small")
+    op = make_operator(d)
+    c_dev = op.direct(torch.as_tensor(d["c"], device="cuda")).cpu().numpy()
+    assert np.array_equal(op.direct(d["c"]), c_dev)
+    a_dev = op.adjoint(torch.as_tensor(d["r"], device="cuda")).cpu().numpy()
+    assert np.array_equal(op.adjoint(d["r"]), a_dev)
+    assert np.array_equal(op.direct(d["c"]), c_dev)          # same bits every call
+
+
+def test_argument_errors(golden):
+    d = golden("diff_midpoint_hat")
+    op = make_operator(d)
+    with pytest.raises(TypeError):
+        op.direct_cl(np.zeros(op.coeff_shape, np.float32), torch.empty(op.data_shape, device="cuda"))
+    with pytest.raises(ValueError):
+        op.direct_cl(torch.zeros((1, 2, 3), device="cuda"), torch.empty(op.data_shape, device="cuda"))
+    with pytest.raises(TypeError):
+        op.direct_cl(torch.zeros(op.coeff_shape, device="cuda", dtype=torch.float64),
+                     torch.empty(op.data_shape, device="cuda"))
+    with pytest.raises(ValueError):
+        op.zero_subset_rows(torch.empty(op.data_shape, device="cuda"), 0)     # no subsets yet
+    with pytest.raises(ValueError):
+        op.set_omega_subsets([np.array([0, op.N_Omega])])
