@@ -49,7 +49,7 @@ WORKLOADS = {
                                 hkl_list=[[1, 0, 0], [0, 0, 2], [1, 0, 1], [1, 0, 2], [1, 1, 0], [1, 0, 3],
                                           [2, 0, 0], [1, 1, 2]]),
                   K=20000, sigma_deg=2.0, grains=200, background=0.10, mean_counts=50.0, subsets=20, epochs=30,
-                  max_gb=8.0),
+                  max_gb=4.0),
     "al99": dict(cfg=dict(Nx=99, Ny=99, My=103, N_Omega=180, angle_range=[0, 180], cor_offset=0.0, N_eta=180,
                           eta_angle_range=[0, 360], energy=12.398 / 0.3, k_direction_0=[0, 0, 1],
                           p_direction_0=[1, 0, 0], detector_direction_origin=[0, -1, 0],

@@ -56,6 +56,15 @@ SIGNATURES = {
     "dfx_poisson_value_grad": ([P, P, P, L, P, L, P, L, F, I, I, F, L, P, P, c_size_t, S], c_int),
     "dfx_mean_counted": ([P, P, L, L, P, P, c_size_t, S], c_int),
     "dfx_dot_f64": ([P, P, L, P, P, c_size_t, S], c_int),
+    "dfx_times_curvature": ([P, P, P, P, L, P, L, P, L, F, I, L, P, P, c_size_t, S], c_int),
+    "dfx_support_sum": ([P, P, L, L, P, P, c_size_t, S], c_int),
+    "dfx_weighted_sums": ([P, P, P, L, L, P, P, c_size_t, S], c_int),
+    "dfx_step_sums": ([P, P, P, P, L, P, P, c_size_t, S], c_int),
+    "dfx_invert_metric": ([P, P, P, L, L, S], c_int),
+    "dfx_metric_step": ([P, P, P, P, F, F, L, S], c_int),
+    "dfx_extrapolate": ([P, P, P, F, L, S], c_int),
+    "dfx_copy_f32": ([P, P, L, S], c_int),
+    "dfx_scale_f32": ([P, F, L, S], c_int),
 }
 
 _lib = None

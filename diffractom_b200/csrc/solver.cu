@@ -218,6 +218,119 @@ __global__ void __launch_bounds__(RED_THREADS) dot_kernel(const float *__restric
     block_sum<1>(v, part + blockIdx.x);
 }
 
+// ---- FISTAPoisson (fista_poisson.py:115-282) ----
+__global__ void __launch_bounds__(RED_THREADS) times_curvature_kernel(
+    float *__restrict__ u, const float *__restrict__ mu, const float *__restrict__ b, const float *__restrict__ w,
+    int64_t pw, const float *__restrict__ g, int64_t pg, const float *__restrict__ bg, int64_t pbg, float floor_counts,
+    int mode, int64_t n, double *__restrict__ part)
+{
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float wi = periodic(w, pw, i, 1.0f);
+        const float gi = periodic(g, pg, i, 1.0f);
+        const float r = u[i];
+        float c;
+        if (mode == 0) {
+            const float m = fmaxf(__fadd_rn(fmaxf(mu[i], 0.0f), periodic(bg, pbg, i, 0.0f)), __fmul_rn(floor_counts, gi));
+            c = wi != 0.0f ? __fmul_rn(__fdiv_rn(wi, gi), __fdiv_rn(fmaxf(b[i], m), __fmul_rn(m, m))) : 0.0f;
+        } else {
+            c = wi != 0.0f ? __fdiv_rn(wi, __fmul_rn(gi, fmaxf(b[i], __fmul_rn(floor_counts, gi)))) : 0.0f;
+        }
+        u[i] = __fmul_rn(r, c);
+        v[0] += (double)c * (double)r * (double)r;
+    }
+    block_sum<1>(v, part + blockIdx.x);
+}
+
+__global__ void __launch_bounds__(RED_THREADS) support_sum_kernel(const float *__restrict__ x,
+                                                                  const uint8_t *__restrict__ supp, int64_t npix,
+                                                                  int64_t n, double *__restrict__ part)
+{
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (!supp || __ldg(supp + (i % npix))) v[0] += (double)x[i];
+    block_sum<1>(v, part + blockIdx.x);
+}
+
+__global__ void __launch_bounds__(RED_THREADS) weighted_sums_kernel(const float *__restrict__ mu,
+                                                                    const float *__restrict__ b,
+                                                                    const float *__restrict__ w, int64_t pw, int64_t n,
+                                                                    double *__restrict__ part)
+{
+    double v[2] = {0.0, 0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float wi = periodic(w, pw, i, 1.0f);
+        v[0] += (double)wi * b[i];
+        v[1] += (double)wi * mu[i];
+    }
+    block_sum<2>(v, part + 2 * blockIdx.x);
+}
+
+__global__ void invert_metric_kernel(float *__restrict__ D, const float *__restrict__ d,
+                                     const uint8_t *__restrict__ supp, int64_t npix, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const bool inside = supp ? __ldg(supp + (i % npix)) != 0 : true;
+        const float di = d[i];
+        D[i] = (inside && di > 0.0f) ? __frcp_rn(di) : 0.0f;
+    }
+}
+
+__global__ void metric_step_kernel(float *__restrict__ xn, const float *__restrict__ y,
+                                   const float *__restrict__ grad, const float *__restrict__ D, float th, float lam,
+                                   int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float Di = D[i];
+        xn[i] = Di > 0.0f ? fmaxf(0.0f, __fsub_rn(y[i], __fmul_rn(__fmul_rn(th, Di), __fadd_rn(grad[i], lam)))) : 0.0f;
+    }
+}
+
+__global__ void __launch_bounds__(RED_THREADS) step_sums_kernel(const float *__restrict__ xn,
+                                                                const float *__restrict__ y,
+                                                                const float *__restrict__ grad,
+                                                                const float *__restrict__ D, int64_t n,
+                                                                double *__restrict__ part)
+{
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double d = (double)xn[i] - (double)y[i];
+        v[0] += (double)grad[i] * d;
+        const float Di = D[i];
+        if (Di > 0.0f) v[1] += d * d / (double)Di;
+        v[2] += (double)xn[i];
+    }
+    block_sum<3>(v, part + 3 * blockIdx.x);
+}
+
+__global__ void extrapolate_kernel(float *__restrict__ out, const float *__restrict__ a, const float *__restrict__ c,
+                                   float beta, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float ai = a[i];
+        out[i] = __fadd_rn(ai, __fmul_rn(beta, __fsub_rn(ai, c[i])));
+    }
+}
+
+__global__ void copy_kernel(const float *__restrict__ src, float *__restrict__ dst, int64_t n)
+{
+    // float4 body (both arrays 16-byte aligned, checked by the caller) and a scalar tail
+    const int64_t n4 = n / 4;
+    const float4 *s4 = reinterpret_cast<const float4 *>(src);
+    float4 *d4 = reinterpret_cast<float4 *>(dst);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x)
+        d4[i] = s4[i];
+    for (int64_t i = 4 * n4 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+__global__ void scale_kernel(float *__restrict__ x, float a, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = __fmul_rn(x[i], a);
+}
+
 static int check_scratch(void *scratch, size_t bytes, int64_t n, int ns)
 {
     const size_t need = (size_t)red_blocks(n) * ns * sizeof(double);
@@ -364,4 +477,99 @@ extern "C" int dfx_dot_f64(const float *x, const float *y, int64_t n, double *ou
     if (st) return st;
     finish_sums<1><<<1, RED_THREADS, 0, s>>>((const double *)scratch, nb, out);
     return launch_status("finish_sums");
+}
+
+// ---- FISTAPoisson entry points ----
+template <int NS, typename Launch>
+static int reduce_launch(int64_t n, void *scratch, size_t bytes, double *out, void *stream, const char *what,
+                         Launch launch)
+{
+    int st = check_scratch(scratch, bytes, n, NS);
+    if (st) return st;
+    const int nb = red_blocks(n);
+    cudaStream_t s = (cudaStream_t)stream;
+    launch(nb, s, (double *)scratch);
+    st = launch_status(what);
+    if (st) return st;
+    finish_sums<NS><<<1, RED_THREADS, 0, s>>>((const double *)scratch, nb, out);
+    return launch_status("finish_sums");
+}
+
+extern "C" int dfx_times_curvature(float *u, const float *mu, const float *b, const float *w, int64_t pw,
+                                   const float *g, int64_t pg, const float *bg, int64_t pbg, float floor_counts,
+                                   int mode, int64_t n, double *out, void *scratch, size_t scratch_bytes, void *stream)
+{
+    DFX_REQUIRE(u && mu && b && out && n >= 0 && (!pw || w) && (!pg || g) && (!pbg || bg), "times_curvature: bad args");
+    return reduce_launch<1>(n, scratch, scratch_bytes, out, stream, "times_curvature",
+                            [&](int nb, cudaStream_t s, double *part) {
+                                times_curvature_kernel<<<nb, RED_THREADS, 0, s>>>(u, mu, b, w, pw, g, pg, bg, pbg,
+                                                                                  floor_counts, mode, n, part);
+                            });
+}
+
+extern "C" int dfx_support_sum(const float *x, const uint8_t *supp, int64_t npix, int64_t n, double *out,
+                               void *scratch, size_t scratch_bytes, void *stream)
+{
+    DFX_REQUIRE(x && out && n >= 0 && (!supp || npix > 0), "support_sum: bad arguments");
+    return reduce_launch<1>(n, scratch, scratch_bytes, out, stream, "support_sum",
+                            [&](int nb, cudaStream_t s, double *part) {
+                                support_sum_kernel<<<nb, RED_THREADS, 0, s>>>(x, supp, npix, n, part);
+                            });
+}
+
+extern "C" int dfx_weighted_sums(const float *mu, const float *b, const float *w, int64_t pw, int64_t n, double *out,
+                                 void *scratch, size_t scratch_bytes, void *stream)
+{
+    DFX_REQUIRE(mu && b && out && n >= 0 && (!pw || w), "weighted_sums: bad arguments");
+    return reduce_launch<2>(n, scratch, scratch_bytes, out, stream, "weighted_sums",
+                            [&](int nb, cudaStream_t s, double *part) {
+                                weighted_sums_kernel<<<nb, RED_THREADS, 0, s>>>(mu, b, w, pw, n, part);
+                            });
+}
+
+extern "C" int dfx_step_sums(const float *xn, const float *y, const float *grad, const float *D, int64_t n,
+                             double *out, void *scratch, size_t scratch_bytes, void *stream)
+{
+    DFX_REQUIRE(xn && y && grad && D && out && n >= 0, "step_sums: bad arguments");
+    return reduce_launch<3>(n, scratch, scratch_bytes, out, stream, "step_sums",
+                            [&](int nb, cudaStream_t s, double *part) {
+                                step_sums_kernel<<<nb, RED_THREADS, 0, s>>>(xn, y, grad, D, n, part);
+                            });
+}
+
+extern "C" int dfx_invert_metric(float *D, const float *d, const uint8_t *supp, int64_t npix, int64_t n, void *stream)
+{
+    DFX_REQUIRE(D && d && n >= 0 && (!supp || npix > 0), "invert_metric: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(invert_metric_kernel, n, stream, D, d, supp, npix, n);
+}
+
+extern "C" int dfx_metric_step(float *xn, const float *y, const float *grad, const float *D, float th, float lam,
+                               int64_t n, void *stream)
+{
+    DFX_REQUIRE(xn && y && grad && D && n >= 0, "metric_step: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(metric_step_kernel, n, stream, xn, y, grad, D, th, lam, n);
+}
+
+extern "C" int dfx_extrapolate(float *out, const float *a, const float *c, float beta, int64_t n, void *stream)
+{
+    DFX_REQUIRE(out && a && c && n >= 0, "extrapolate: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(extrapolate_kernel, n, stream, out, a, c, beta, n);
+}
+
+extern "C" int dfx_copy_f32(const float *src, float *dst, int64_t n, void *stream)
+{
+    DFX_REQUIRE(src && dst && n >= 0, "copy: bad arguments");
+    DFX_REQUIRE(((uintptr_t)src % 16) == 0 && ((uintptr_t)dst % 16) == 0, "copy: 16-byte aligned arrays");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(copy_kernel, cdiv(n, 4), stream, src, dst, n);
+}
+
+extern "C" int dfx_scale_f32(float *x, float a, int64_t n, void *stream)
+{
+    DFX_REQUIRE(x && n >= 0, "scale: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(scale_kernel, n, stream, x, a, n);
 }

@@ -172,6 +172,32 @@ int dfx_mean_counted(const float *b, const float *w, int64_t pw, int64_t n, doub
 int dfx_dot_f64(const float *x, const float *y, int64_t n, double *out, void *scratch, size_t scratch_bytes,
                 void *stream);
 
+/* FISTAPoisson (optimization/fista_poisson.py), all float32 element-wise with float64 sums:
+ * replaces times_curvature (:115-144): u <- u * c, c the curvature of the data term at mu (mode 0 Poisson, 1 the
+ * weighted least squares of the start); out[0] = sum c u_old^2. */
+int dfx_times_curvature(float *u, const float *mu, const float *b, const float *w, int64_t pw, const float *g,
+                        int64_t pg, const float *bg, int64_t pbg, float floor_counts, int mode, int64_t n, double *out,
+                        void *scratch, size_t scratch_bytes, void *stream);
+/* replaces support_sum (:146-159): out[0] = sum of x over the support (supp (npix) uint8 or NULL). */
+int dfx_support_sum(const float *x, const uint8_t *supp, int64_t npix, int64_t n, double *out, void *scratch,
+                    size_t scratch_bytes, void *stream);
+/* replaces weighted_sums (:161-180): out = (sum w b, sum w mu). */
+int dfx_weighted_sums(const float *mu, const float *b, const float *w, int64_t pw, int64_t n, double *out,
+                      void *scratch, size_t scratch_bytes, void *stream);
+/* replaces step_sums (:230-258): out = (<grad, xn - y>, sum (xn - y)^2 / D over D > 0, sum xn). */
+int dfx_step_sums(const float *xn, const float *y, const float *grad, const float *D, int64_t n, double *out,
+                  void *scratch, size_t scratch_bytes, void *stream);
+/* replaces invert_metric (:201-209): D = inside && d > 0 ? 1 / d : 0. */
+int dfx_invert_metric(float *D, const float *d, const uint8_t *supp, int64_t npix, int64_t n, void *stream);
+/* replaces metric_step (:219-225): xn = D > 0 ? max(0, y - th D (grad + lam)) : 0. */
+int dfx_metric_step(float *xn, const float *y, const float *grad, const float *D, float th, float lam, int64_t n,
+                    void *stream);
+/* replaces extrapolate (:260-266): out = a + beta (a - c). */
+int dfx_extrapolate(float *out, const float *a, const float *c, float beta, int64_t n, void *stream);
+/* replaces copy_buf / scale_buf (:268-275, :195-198): dst = src (both 16-byte aligned); x *= a. */
+int dfx_copy_f32(const float *src, float *dst, int64_t n, void *stream);
+int dfx_scale_f32(float *x, float a, int64_t n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
