@@ -157,11 +157,10 @@ def cpu_sample(op, w, sp_seed=0):
     sub_a, sub_f = subsets[0], subsets[1]
     orc = OracleOperator.from_operator(op, precision="f32", batches=[(0, kb)])
     rows = np.union1d(sub_a, sub_f)
-    # the PF matrix of the sample's angles only (a subset of the rows of the batch's CSR)
-    keep = np.zeros(op.N_Omega, bool)
-    keep[rows] = True
-    orc_rows = OracleOperator(coords=orc.coords[rows], poles=orc.poles, axis_start=orc.axis_start,
-                              axis_count=orc.axis_count, inv_sigma2=orc.inv_sigma2, norm=orc.norm, quad_w=orc.quad_w,
+    # the PF matrix of the sample's angles and orientations only (rows of the first batch's CSR)
+    orc_rows = OracleOperator(coords=orc.coords[rows], poles=orc.poles[:kb], axis_start=orc.axis_start,
+                              axis_count=orc.axis_count, inv_sigma2=orc.inv_sigma2[:kb], norm=orc.norm[:kb],
+                              quad_w=orc.quad_w,
                               geo=orc.geo[rows], scale=orc.scale, n_taps=orc.n_taps, kernel=orc.kernel, Nx=op.Nx,
                               Ny=op.Ny, My=op.My, cut=orc.cut, batches=[(0, kb)], precision="f32")
     ia = np.searchsorted(rows, sub_a)
