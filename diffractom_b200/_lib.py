@@ -39,6 +39,7 @@ SIGNATURES = {
     "dfx_pf_csr_fill": ([POINTER(PFGeometry), P, I, I, I, I, P, P, P, S], c_int),
     "dfx_scan_scratch_bytes": ([L], c_size_t),
     "dfx_scan_exclusive_i32": ([P, P, L, P, c_size_t, S], c_int),
+    "dfx_scan_exclusive_i32_static": ([P, P, L, S], c_int),
     "dfx_spmm_pf_forward": ([P, P, P, P, P, P, I, I, I, I, I, I, S], c_int),
     "dfx_spmm_pf_adjoint": ([P, P, P, P, P, P, I, I, I, I, I, F, I, S], c_int),
     "dfx_zero_rows": ([P, P, I, L, S], c_int),

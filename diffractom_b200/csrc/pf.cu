@@ -10,6 +10,8 @@
 // the block (TY lines of the sinogram or of the data) is staged in shared memory a chunk of columns at a time,
 // transposed so that the TY values of one column are contiguous (float4 reads); every CSR entry is read once per
 // block and used TY times from a register.
+#include <mutex>
+
 #include "dfx_common.cuh"
 
 namespace dfx {
@@ -393,6 +395,61 @@ extern "C" int dfx_scan_exclusive_i32(const int32_t *in, int32_t *out, int64_t n
     if (n == 0) return DFX_OK;
     scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, sums, out);
     return launch_status("scan_tiles");
+}
+
+// ---- the exclusive scan without caller scratch ----
+// Its tile sums live in this array, which the CUDA runtime places in the memory of every device that loads this
+// library and keeps there until the process exits. Host code only knows a stand-in for its name: the device address
+// comes from cudaGetSymbolAddress, looked up once per device (with that device current) and cached.
+static __device__ __align__(256) int32_t g_scan_tile_sums[DFX_SCAN_STATIC_MAX_N / SCAN_TILE + 1];
+
+namespace dfx {
+constexpr int MAX_DEVICES = 64;
+static std::mutex g_scan_mu;
+static int32_t *g_scan_ptr[MAX_DEVICES] = {nullptr};
+}  // namespace dfx
+
+extern "C" int dfx_scan_exclusive_i32_static(const int32_t *in, int32_t *out, int64_t n, void *stream)
+{
+    static_assert(DFX_SCAN_STATIC_MAX_N % SCAN_TILE == 0, "the maximum is a whole number of tiles");
+    DFX_REQUIRE(in && out, "scan_static: null pointer");
+    DFX_REQUIRE(n >= 0 && n <= DFX_SCAN_STATIC_MAX_N,
+                "scan_static: n = %lld is beyond the %lld elements its built-in scratch covers; use "
+                "dfx_scan_exclusive_i32 with scratch of dfx_scan_scratch_bytes(n) bytes", (long long)n,
+                (long long)DFX_SCAN_STATIC_MAX_N);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        set_error("scan_static: cudaGetDevice: %s", cudaGetErrorString(e));
+        return DFX_ECUDA;
+    }
+    DFX_REQUIRE(dev >= 0 && dev < MAX_DEVICES, "scan_static: device %d beyond the %d supported", dev, MAX_DEVICES);
+    int32_t *sums = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_scan_mu);
+        if (!g_scan_ptr[dev]) {            // once per device, with that device current (the caller's)
+            void *p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_scan_tile_sums);
+            if (e != cudaSuccess) {
+                set_error("scan_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+                return DFX_ECUDA;
+            }
+            g_scan_ptr[dev] = static_cast<int32_t *>(p);
+        }
+        sums = g_scan_ptr[dev];
+    }
+    // every slot the later passes read is written by the first pass of this call: nothing to clear
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t tiles = cdiv(n > 0 ? n : 1, SCAN_TILE);
+    scan_tile_sums<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, sums);
+    int st = launch_status("scan_static_tile_sums");
+    if (st) return st;
+    scan_sums<<<1, SCAN_THREADS, 0, s>>>(sums, tiles, out + n);
+    st = launch_status("scan_static_sums");
+    if (st) return st;
+    if (n == 0) return DFX_OK;
+    scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, sums, out);
+    return launch_status("scan_static_tiles");
 }
 
 extern "C" int dfx_spmm_pf_forward(const float *sino, const int32_t *row_ptr, const uint16_t *col_k, const float *val,

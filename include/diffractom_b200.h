@@ -102,6 +102,21 @@ size_t dfx_scan_scratch_bytes(int64_t n);
 int dfx_scan_exclusive_i32(const int32_t *in, int32_t *out, int64_t n, void *scratch, size_t scratch_bytes,
                            void *stream);
 
+/* The same exclusive scan for callers that cannot allocate device memory; it has no counterpart in the reference.
+ * Some callers own every byte of the GPU through their own pool or budget and may not call cudaMalloc (a host
+ * application that hands this library fixed buffers, or a loop that must not synchronise the device on an
+ * allocation); they cannot provide dfx_scan_exclusive_i32's scratch. This entry point takes inputs and outputs only:
+ * its scratch (one int32 per 2048 elements) is a fixed array inside the library, present on every GPU that loads it
+ * until the process exits (256 KiB per device). Limits and rules:
+ *   n <= DFX_SCAN_STATIC_MAX_N, else DFX_EINVAL with a message (the other entry point has no such limit);
+ *   the first call on a device looks up the array's address on that device (the calling thread's current device),
+ *   so make that first call before any stream capture;
+ *   all calls on a device share the array: calls that overlap on the GPU (other streams, other threads) race and
+ *   corrupt each other's result; serialise them. Nothing has to be cleared between calls (each call writes every
+ *   slot it later reads). */
+#define DFX_SCAN_STATIC_MAX_N (65536LL * 2048LL)
+int dfx_scan_exclusive_i32_static(const int32_t *in, int32_t *out, int64_t n, void *stream);
+
 /* replaces spmm_pf_forward_c / spmm_pf_forward_sub (pf_kernels.cl:597-641, SPFO:38-80): for the n_sub angles
  * omegas (NULL: all, n_sub = R): data[omegas[s], y, j] += sum_k val * sino[s, y, k] over the forward CSR; rows of the
  * CSR are s * CP + j if compact, else omegas[s] * CP + j. Empty CSR rows leave data untouched. */
