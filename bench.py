@@ -49,7 +49,7 @@ WORKLOADS = {
                                 hkl_list=[[1, 0, 0], [0, 0, 2], [1, 0, 1], [1, 0, 2], [1, 1, 0], [1, 0, 3],
                                           [2, 0, 0], [1, 1, 2]]),
                   K=20000, sigma_deg=2.0, grains=200, background=0.10, mean_counts=50.0, subsets=20, epochs=30,
-                  max_gb=4.0),
+                  max_gb=3.9),
     "al99": dict(cfg=dict(Nx=99, Ny=99, My=103, N_Omega=180, angle_range=[0, 180], cor_offset=0.0, N_eta=180,
                           eta_angle_range=[0, 360], energy=12.398 / 0.3, k_direction_0=[0, 0, 1],
                           p_direction_0=[1, 0, 0], detector_direction_origin=[0, -1, 0],
@@ -263,10 +263,10 @@ def main():
         dist.barrier()
     value = world * a.steps / (t_max / 1e3)
     # deviance of the iterate after warm-up + timed epochs (float64 reduction)
+    sp._finish()
     D = torch.empty(op.data_shape, dtype=torch.float32, device=op.device)
     op.direct_cl(sp.x, D)
     f_final = sp._deviance(D)
-    sp._finish()
     roof = timers.roofline(op)
 
     e2e = None
@@ -299,35 +299,36 @@ def main():
 class KernelTimers:
     """CUDA events around the launches of chosen kernels inside the timed region (same stream), for the roofline."""
 
-    NAMES = ("dfx_radon_forward", "dfx_radon_backward", "dfx_spmm_pf_forward", "dfx_spmm_pf_adjoint",
-             "dfx_gather_channels", "dfx_scatter_channels", "dfx_spdhg_primal_update", "dfx_spdhg_dual_update")
-
     def __init__(self, op):
+        from diffractom_b200 import _lib
         self.op = op
-        self.events = {n: [] for n in self.NAMES}
-        self.args = {n: [] for n in self.NAMES}
+        self._lib = _lib
+        self.events, self.args = {}, {}
         self.n_extra = 0
-        self._orig = op._call
+        self._orig_op, self._orig_lib = op._call, _lib.call
 
-    def on(self):
+    def _wrap(self, orig):
         import torch
         op = self.op
 
         def call(name, *args):
-            if name in self.events:
-                s = op.stream()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(s)
-                self._orig(name, *args)
-                e1.record(s)
-                self.events[name].append((e0, e1))
-                self.args[name].append(args)
-            else:
-                self._orig(name, *args)
-        op._call = call
+            s = op.stream()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            orig(name, *args)
+            e1.record(s)
+            self.events.setdefault(name, []).append((e0, e1))
+            self.args.setdefault(name, []).append(args)
+        return call
+
+    def on(self):
+        """Every entry point the operator or the solvers call (all launch on the operator's stream) is timed."""
+        self.op._call = self._wrap(self._orig_op)
+        self._lib.call = self._wrap(self._orig_lib)
 
     def off(self):
-        self.op._call = self._orig
+        self.op._call = self._orig_op
+        self._lib.call = self._orig_lib
 
     def roofline(self, op):
         import torch
@@ -374,11 +375,18 @@ def algorithmic_work(op, name, args_list):
         elif name in ("dfx_gather_channels", "dfx_scatter_channels"):
             nb.append(2 * 4 * npix * args[4])
             nf.append(0)
+        elif name == "dfx_radon_backward_spdhg":
+            n_ang, kstride, kb = args[2], args[6], args[7]
+            nb.append(4 * kb * n_ang * op.My + 4 * 5 * npix * kstride)      # sino; x, z, T read; x, z written
+            nf.append(2 * 2 * npix * n_ang * kb)
         elif name == "dfx_spdhg_primal_update":
             nb.append(4 * 6 * args[6])
             nf.append(0)
-        else:
+        elif name == "dfx_spdhg_dual_update":
             nb.append(4 * 7 * args[12] * args[13])
+            nf.append(0)
+        else:
+            nb.append(0)
             nf.append(0)
     return float(np.mean(nb)), float(np.mean(nf))
 

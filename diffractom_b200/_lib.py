@@ -34,6 +34,8 @@ SIGNATURES = {
     "dfx_scatter_channels": ([P, P, L, I, I, I, S], c_int),
     "dfx_radon_forward": ([P, P, P, I, I, I, I, I, I, I, F, S], c_int),
     "dfx_radon_backward": ([P, P, P, I, I, I, I, I, I, I, I, S], c_int),
+    "dfx_radon_backward_spdhg": ([P, P, I, I, I, I, I, I, I, I, P, P, P, F, F, S], c_int),
+    "dfx_batch_support": ([P, P, P, L, I, I, F, I, S], c_int),
     "dfx_pf_dense": ([POINTER(PFGeometry), I, I, P, S], c_int),
     "dfx_pf_csr_count": ([POINTER(PFGeometry), P, I, I, I, I, P, S], c_int),
     "dfx_pf_csr_fill": ([POINTER(PFGeometry), P, I, I, I, I, P, P, P, S], c_int),

@@ -50,6 +50,34 @@ __device__ __forceinline__ AngleGeo load_geo(const float4 *geo, int a) {
     return o;
 }
 
+// The per-angle constants packed for shared memory: (A, B, T0, w) and (hw, top, iw, rows_are_y).
+struct __align__(16) AngleParams {
+    float4 abtw;
+    float4 htir;
+};
+
+__device__ __forceinline__ AngleParams pack_geo(const AngleGeo &g)
+{
+    AngleParams p;
+    p.abtw = make_float4(g.A, g.B, g.T0, g.w);
+    p.htir = make_float4(g.hw, g.top, g.iw, g.rows_are_y ? 1.0f : 0.0f);
+    return p;
+}
+
+__device__ __forceinline__ AngleGeo unpack_geo(const AngleParams &p)
+{
+    AngleGeo g;
+    g.A = p.abtw.x;
+    g.B = p.abtw.y;
+    g.T0 = p.abtw.z;
+    g.w = p.abtw.w;
+    g.hw = p.htir.x;
+    g.top = p.htir.y;
+    g.iw = p.htir.z;
+    g.rows_are_y = p.htir.w != 0.0f;
+    return g;
+}
+
 // K(d) for d = t - s: trapezoid (kernel 1) or hat (kernel 0).
 template <int KERNEL>
 __device__ __forceinline__ float tap_weight(const AngleGeo &g, float d) {

@@ -1,15 +1,11 @@
-// Pole-figure (PF) matrix of the single-phase operator on sm_100a: entry evaluation, CSR construction, and the two
-// sparse products with the channel-fastest sinogram batch (FP32).
+// Pole-figure (PF) matrix of the single-phase operator on sm_100a: entry evaluation and CSR construction (the sparse
+// products with the channel-fastest sinogram batch are in spmm.cu).
 //
 // CSR construction: one warp per CSR row. The lanes evaluate the row's 32 next entries in column order, a ballot
 // orders the non-zeros, so every row is written in ascending column order and the structure is a pure function of
 // the float32 entry values: the CSR of the dense batch, bit for bit, with no sort and no atomics. Adjoint rows
 // (angle, orientation) run over the segments j = c * P + p; forward rows (angle, segment) over the orientations.
-//
-// Products: a block owns one angle, TY detector positions and 128 CSR rows (one per thread). The dense operand of
-// the block (TY lines of the sinogram or of the data) is staged in shared memory a chunk of columns at a time,
-// transposed so that the TY values of one column are contiguous (float4 reads); every CSR entry is read once per
-// block and used TY times from a register.
+
 #include <mutex>
 
 #include "dfx_common.cuh"
@@ -183,116 +179,6 @@ __global__ void __launch_bounds__(SCAN_THREADS) scan_tiles(const int32_t *in, in
     }
 }
 
-// ---- sparse products ----
-constexpr int SP_THREADS = 128;   // CSR rows per block
-constexpr int TY = 16;            // detector positions per block
-constexpr int TYP = TY + 4;       // padded column of the staged tile (keeps float4 alignment)
-constexpr int CHUNK = 512;        // columns staged per pass (CHUNK * TYP * 4 = 40 KB)
-
-__global__ void __launch_bounds__(SP_THREADS) spmm_forward_kernel(
-    const float *__restrict__ sino, const int32_t *__restrict__ row_ptr, const uint16_t *__restrict__ col_k,
-    const float *__restrict__ val, float *__restrict__ data, const int32_t *__restrict__ omegas, int my, int cp,
-    int kstride, int kb, int compact)
-{
-    __shared__ __align__(16) float lz[CHUNK * TYP];
-    const int j = blockIdx.x * SP_THREADS + threadIdx.x;
-    const int y0 = blockIdx.y * TY;
-    const int s = blockIdx.z;
-    const int r = omegas ? __ldg(omegas + s) : s;
-    const int ny = min(TY, my - y0);
-    const int64_t rr = (int64_t)(compact ? s : r) * cp + j;
-    int i = 0, e = 0;
-    if (j < cp) { i = __ldg(row_ptr + rr); e = __ldg(row_ptr + rr + 1); }
-    const bool nonempty = i < e;
-    float acc[TY];
-#pragma unroll
-    for (int t = 0; t < TY; ++t) acc[t] = 0.0f;
-    const float *zl = sino + ((int64_t)s * my + y0) * kstride;
-    for (int k0 = 0; k0 < kb; k0 += CHUNK) {
-        const int kn = min(CHUNK, kb - k0);
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < TY * kn; idx += SP_THREADS) {
-            const int t = idx / kn, kk = idx - t * kn;
-            lz[kk * TYP + t] = t < ny ? __ldg(zl + (int64_t)t * kstride + k0 + kk) : 0.0f;
-        }
-        __syncthreads();
-        const int k1 = k0 + kn;
-        for (; i < e; ++i) {
-            const int k = __ldg(col_k + i);
-            if (k >= k1) break;
-            const float v = __ldg(val + i);
-            const float4 *z4 = reinterpret_cast<const float4 *>(lz + (k - k0) * TYP);
-#pragma unroll
-            for (int q = 0; q < TY / 4; ++q) {
-                const float4 z = z4[q];
-                acc[4 * q + 0] = __fmaf_rn(v, z.x, acc[4 * q + 0]);
-                acc[4 * q + 1] = __fmaf_rn(v, z.y, acc[4 * q + 1]);
-                acc[4 * q + 2] = __fmaf_rn(v, z.z, acc[4 * q + 2]);
-                acc[4 * q + 3] = __fmaf_rn(v, z.w, acc[4 * q + 3]);
-            }
-        }
-    }
-    if (j < cp && nonempty) {
-        float *dl = data + ((int64_t)r * my + y0) * cp + j;
-#pragma unroll
-        for (int t = 0; t < TY; ++t)
-            if (t < ny) dl[(int64_t)t * cp] += acc[t];
-    }
-}
-
-__global__ void __launch_bounds__(SP_THREADS) spmm_adjoint_kernel(
-    const float *__restrict__ data, const int32_t *__restrict__ row_ptr, const uint16_t *__restrict__ col_j,
-    const float *__restrict__ val, float *__restrict__ sino, const int32_t *__restrict__ omegas, int my, int kb,
-    int cp, int kstride, float alpha, int compact)
-{
-    __shared__ __align__(16) float ld[CHUNK * TYP];
-    const int k = blockIdx.x * SP_THREADS + threadIdx.x;
-    const int y0 = blockIdx.y * TY;
-    const int s = blockIdx.z;
-    const int r = omegas ? __ldg(omegas + s) : s;
-    const int ny = min(TY, my - y0);
-    int i = 0, e = 0;
-    if (k < kb) {
-        const int64_t rr = (int64_t)(compact ? s : r) * kb + k;
-        i = __ldg(row_ptr + rr);
-        e = __ldg(row_ptr + rr + 1);
-    }
-    float acc[TY];
-#pragma unroll
-    for (int t = 0; t < TY; ++t) acc[t] = 0.0f;
-    const float *dl = data + ((int64_t)r * my + y0) * cp;
-    for (int j0 = 0; j0 < cp; j0 += CHUNK) {
-        const int jn = min(CHUNK, cp - j0);
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < TY * jn; idx += SP_THREADS) {
-            const int t = idx / jn, jj = idx - t * jn;
-            ld[jj * TYP + t] = t < ny ? __ldg(dl + (int64_t)t * cp + j0 + jj) : 0.0f;
-        }
-        __syncthreads();
-        const int j1 = j0 + jn;
-        for (; i < e; ++i) {
-            const int j = __ldg(col_j + i);
-            if (j >= j1) break;
-            const float v = __ldg(val + i);
-            const float4 *d4 = reinterpret_cast<const float4 *>(ld + (j - j0) * TYP);
-#pragma unroll
-            for (int q = 0; q < TY / 4; ++q) {
-                const float4 d = d4[q];
-                acc[4 * q + 0] = __fmaf_rn(v, d.x, acc[4 * q + 0]);
-                acc[4 * q + 1] = __fmaf_rn(v, d.y, acc[4 * q + 1]);
-                acc[4 * q + 2] = __fmaf_rn(v, d.z, acc[4 * q + 2]);
-                acc[4 * q + 3] = __fmaf_rn(v, d.w, acc[4 * q + 3]);
-            }
-        }
-    }
-    if (k < kstride) {
-        float *zl = sino + ((int64_t)s * my + y0) * kstride + k;
-#pragma unroll
-        for (int t = 0; t < TY; ++t)
-            if (t < ny) zl[(int64_t)t * kstride] = k < kb ? alpha * acc[t] : 0.0f;
-    }
-}
-
 __global__ void zero_rows_kernel(float *__restrict__ data, const int32_t *__restrict__ omegas, int n_sub,
                                  int64_t row_len)
 {
@@ -450,32 +336,6 @@ extern "C" int dfx_scan_exclusive_i32_static(const int32_t *in, int32_t *out, in
     if (n == 0) return DFX_OK;
     scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, sums, out);
     return launch_status("scan_static_tiles");
-}
-
-extern "C" int dfx_spmm_pf_forward(const float *sino, const int32_t *row_ptr, const uint16_t *col_k, const float *val,
-                                   float *data, const int32_t *omegas, int n_sub, int my, int cp, int kstride, int kb,
-                                   int compact, void *stream)
-{
-    DFX_REQUIRE(sino && row_ptr && col_k && val && data, "spmm_forward: null pointer");
-    DFX_REQUIRE(n_sub > 0 && my > 0 && cp > 0 && kb > 0 && kb <= kstride, "spmm_forward: bad sizes");
-    DFX_REQUIRE(n_sub <= 65535 && cdiv(my, TY) <= 65535, "spmm_forward: grid too large");
-    dim3 grid((unsigned)cdiv(cp, SP_THREADS), (unsigned)cdiv(my, TY), (unsigned)n_sub);
-    spmm_forward_kernel<<<grid, SP_THREADS, 0, (cudaStream_t)stream>>>(sino, row_ptr, col_k, val, data, omegas, my, cp,
-                                                                       kstride, kb, compact);
-    return launch_status("spmm_pf_forward");
-}
-
-extern "C" int dfx_spmm_pf_adjoint(const float *data, const int32_t *row_ptr, const uint16_t *col_j, const float *val,
-                                   float *sino, const int32_t *omegas, int n_sub, int my, int kb, int cp, int kstride,
-                                   float alpha, int compact, void *stream)
-{
-    DFX_REQUIRE(sino && row_ptr && col_j && val && data, "spmm_adjoint: null pointer");
-    DFX_REQUIRE(n_sub > 0 && my > 0 && cp > 0 && kb > 0 && kb <= kstride, "spmm_adjoint: bad sizes");
-    DFX_REQUIRE(n_sub <= 65535 && cdiv(my, TY) <= 65535, "spmm_adjoint: grid too large");
-    dim3 grid((unsigned)cdiv(kstride, SP_THREADS), (unsigned)cdiv(my, TY), (unsigned)n_sub);
-    spmm_adjoint_kernel<<<grid, SP_THREADS, 0, (cudaStream_t)stream>>>(data, row_ptr, col_j, val, sino, omegas, my,
-                                                                       kb, cp, kstride, alpha, compact);
-    return launch_status("spmm_pf_adjoint");
 }
 
 extern "C" int dfx_zero_rows(float *data, const int32_t *omegas, int n_sub, int64_t row_len, void *stream)

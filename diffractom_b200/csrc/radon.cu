@@ -1,136 +1,249 @@
 // Parallel-beam Radon transform of a batch of channel-fastest images (the orientations of a batch are the channels),
-// sm_100a, FP32. Semantics: operators/radon_kernels.cl of diffractom (ParallelRadon), tap weights as in
-// dfx_common.cuh (and the CPU oracle, oracle/oracle_core.h).
+// sm_100a, FP32. Semantics: operators/radon_kernels.cl of diffractom (ParallelRadon); tap weights as in
+// dfx_common.cuh, which the CPU oracle (oracle/oracle_core.h) restates bit for bit.
 //
-// Forward (ray-driven): a thread owns NB neighbouring detector bins of one angle and 8 channels (two float4), loops
-// over the image rows and over the pixels of each row whose footprint reaches its bins, and accumulates in
-// registers; no atomics, each output written once. Backward (pixel-driven): a thread owns one pixel and 8 channels
-// and loops over the angles and the taps of its footprint. Both read the image / sinogram through L1 (__ldg).
+// Work split: the 32 lanes of a warp own 8 channels each (256 channels per warp), so everything that depends on the
+// geometry only (detector coordinate, tap bins and weights) is the same for the whole warp: one warp instruction
+// serves 256 channels, and a zero weight skips its FMAs with a branch all lanes take.
+//
+// Forward (ray-driven, no atomics): a block owns NB_F bins of one angle and 256 channels; its 8 warps split the image
+// rows (warp w takes rows w, w + 8, ...), each accumulating all NB_F bins in registers, and sum their partial
+// projections through shared memory in a fixed order at the end (deterministic). Per row a warp walks the pixels
+// whose footprint reaches the block's bins; a pixel's non-zero taps go to their bin's accumulator through a switch
+// on the warp-uniform bin offset.
+//
+// Backward (pixel-driven, no atomics): a warp owns one pixel. The per-angle constants are computed once per block
+// into shared memory; per angle the warp evaluates the pixel's taps and reads 8 channels of each tap's sinogram bin
+// per lane. A fused variant applies SPDHG's primal step in the epilogue (no dz array).
 #include "dfx_common.cuh"
 
 namespace dfx {
 
-constexpr int CPT = 8;              // channels per thread (two float4)
-constexpr int FWD_CG = 16;          // channel groups per forward block (128 channels)
-constexpr int FWD_BG = 8;           // bin groups per forward block
-constexpr int BWD_CG = 16;          // channel groups per backward block
-constexpr int BWD_PX = 16;          // pixels per backward block
+constexpr int WARPS = 8;        // warps per block
+constexpr int CPL = 8;          // channels per lane
+constexpr int CPW = 32 * CPL;   // channels per warp
+constexpr int NB_F = 8;         // bins per forward block
 
-__device__ __forceinline__ void ld8(const float *p, float4 &a, float4 &b) {
+__device__ __forceinline__ void ld8(const float *p, float4 &a, float4 &b)
+{
     a = __ldg(reinterpret_cast<const float4 *>(p));
     b = __ldg(reinterpret_cast<const float4 *>(p) + 1);
 }
 
-template <int KERNEL, int NB>
-__global__ void __launch_bounds__(FWD_CG *FWD_BG) radon_forward_kernel(
-    const float *__restrict__ img, float *__restrict__ sino, const float4 *__restrict__ geo, int nx, int ny, int ns,
-    int kstride, int kb, float scale)
+__device__ __forceinline__ void acc8(float (&a)[CPL], float w, const float4 &p0, const float4 &p1)
 {
+    a[0] = __fmaf_rn(w, p0.x, a[0]);
+    a[1] = __fmaf_rn(w, p0.y, a[1]);
+    a[2] = __fmaf_rn(w, p0.z, a[2]);
+    a[3] = __fmaf_rn(w, p0.w, a[3]);
+    a[4] = __fmaf_rn(w, p1.x, a[4]);
+    a[5] = __fmaf_rn(w, p1.y, a[5]);
+    a[6] = __fmaf_rn(w, p1.z, a[6]);
+    a[7] = __fmaf_rn(w, p1.w, a[7]);
+}
+
+// bins strictly inside a pixel's footprint (t - hw, t + hw) at this angle: at most ceil(1 + |A|) for the trapezoid
+// (2 for the hat), never more than the caller's bound n_taps
+__device__ __forceinline__ int taps_of(const AngleGeo &g, int kernel, int n_taps)
+{
+    if (kernel != 1) return 2;
+    const int t = max(2, (int)ceilf(1.0f + fabsf(g.A) - 1e-6f));
+    return min(t, n_taps);
+}
+
+// first bin that can get a non-zero weight from a pixel at detector coordinate t
+template <int KERNEL>
+__device__ __forceinline__ int first_tap(const AngleGeo &g, float t)
+{
+    return KERNEL == 1 ? (int)floorf(__fsub_rn(t, g.hw)) + 1 : (int)floorf(t);
+}
+
+// ------------------------------------------------------------------------------------------------ forward
+template <int KERNEL>
+__global__ void __launch_bounds__(32 * WARPS) radon_forward_v3(
+    const float *__restrict__ img, float *__restrict__ sino, const float4 *__restrict__ geo, int nx, int ny, int ns,
+    int kstride, int kb, float scale, int n_taps)
+{
+    extern __shared__ __align__(16) float red[];          // [WARPS][NB_F][CPW] partial projections
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int a = blockIdx.z;
-    const int k = (blockIdx.y * FWD_CG + threadIdx.x) * CPT;
-    const int s0 = (blockIdx.x * FWD_BG + threadIdx.y) * NB;
-    if (k >= kstride || s0 >= ns) return;
+    const int k = blockIdx.y * CPW + lane * CPL;
+    const int s0 = blockIdx.x * NB_F;
+    const bool live = k < kstride;
     const AngleGeo g = load_geo(geo, a);
     const int nu = g.rows_are_y ? nx : ny, nv = g.rows_are_y ? ny : nx;
-    const int64_t du = g.rows_are_y ? 1 : nx, dv = g.rows_are_y ? nx : 1;   // pixel strides of u, v
-    const bool live = k < kb;             // kb is a multiple of 8 or the tail group is fully masked below
-    float acc[NB][CPT];
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) acc[j][c] = 0.0f;
-
+    const int64_t du = (g.rows_are_y ? 1 : (int64_t)nx) * kstride, dv = (g.rows_are_y ? (int64_t)nx : 1) * kstride;
     const float half = KERNEL == 1 ? g.hw : 1.0f;
     const float inv = __frcp_rn(g.A);
-    const float *base = img + k;
-    if (live) {
-        for (int v = 0; v < nv; ++v) {
-            const float c = __fmaf_rn(g.B, (float)v, g.T0);
-            // pixels whose t lies in (s0 - half, s0 + NB - 1 + half): u between these, in either order
-            const float e1 = (s0 - half - c) * inv, e2 = (s0 + NB - 1 + half - c) * inv;
-            // (a margin of 1e-3 pixel covers the rounding of e1, e2; the tap weights decide membership)
-            const int u0 = max((int)floorf(fminf(e1, e2) - 1e-3f), 0);
-            const int u1 = min((int)ceilf(fmaxf(e1, e2) + 1e-3f), nu - 1);
-            const float *row = base + (int64_t)v * dv * kstride;
-            for (int u = u0; u <= u1; ++u) {
-                const float t = __fmaf_rn(g.A, (float)u, c);
-                float4 p0, p1;
-                ld8(row + (int64_t)u * du * kstride, p0, p1);
+    const int ntap = taps_of(g, KERNEL, n_taps);
+    float acc[NB_F][CPL];
 #pragma unroll
-                for (int j = 0; j < NB; ++j) {
-                    const float w = tap_weight<KERNEL>(g, __fsub_rn(t, (float)(s0 + j)));
-                    acc[j][0] = __fmaf_rn(w, p0.x, acc[j][0]);
-                    acc[j][1] = __fmaf_rn(w, p0.y, acc[j][1]);
-                    acc[j][2] = __fmaf_rn(w, p0.z, acc[j][2]);
-                    acc[j][3] = __fmaf_rn(w, p0.w, acc[j][3]);
-                    acc[j][4] = __fmaf_rn(w, p1.x, acc[j][4]);
-                    acc[j][5] = __fmaf_rn(w, p1.y, acc[j][5]);
-                    acc[j][6] = __fmaf_rn(w, p1.z, acc[j][6]);
-                    acc[j][7] = __fmaf_rn(w, p1.w, acc[j][7]);
+    for (int j = 0; j < NB_F; ++j)
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) acc[j][c] = 0.0f;
+    const float *base = img + (live ? k : 0);
+    for (int v = warp; v < nv; v += WARPS) {
+        const float c = __fmaf_rn(g.B, (float)v, g.T0);
+        const float e1 = (s0 - half - c) * inv, e2 = (s0 + NB_F - 1 + half - c) * inv;
+        // a margin of 1e-3 pixel covers the rounding of e1, e2; the tap weights decide membership
+        const int u0 = max((int)floorf(fminf(e1, e2) - 1e-3f), 0);
+        const int u1 = min((int)ceilf(fmaxf(e1, e2) + 1e-3f), nu - 1);
+        const float *row = base + (int64_t)v * dv;
+        for (int u = u0; u <= u1; ++u) {
+            const float t = __fmaf_rn(g.A, (float)u, c);
+            float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
+            if (live) ld8(row + (int64_t)u * du, p0, p1);
+            const int sf = first_tap<KERNEL>(g, t);
+            for (int i = 0; i < ntap; ++i) {
+                const int j = sf + i - s0;
+                if (j < 0 || j >= NB_F) continue;
+                const float w = tap_weight<KERNEL>(g, __fsub_rn(t, (float)(sf + i)));
+                if (w == 0.0f) continue;
+                switch (j) {
+                    case 0: acc8(acc[0], w, p0, p1); break;
+                    case 1: acc8(acc[1], w, p0, p1); break;
+                    case 2: acc8(acc[2], w, p0, p1); break;
+                    case 3: acc8(acc[3], w, p0, p1); break;
+                    case 4: acc8(acc[4], w, p0, p1); break;
+                    case 5: acc8(acc[5], w, p0, p1); break;
+                    case 6: acc8(acc[6], w, p0, p1); break;
+                    default: acc8(acc[7], w, p0, p1); break;
                 }
             }
         }
     }
+    // partial projections of the 8 row classes -> shared memory -> warp j sums bin j over them in a fixed order
 #pragma unroll
-    for (int j = 0; j < NB; ++j) {
-        if (s0 + j >= ns) break;
-        float *o = sino + ((int64_t)a * ns + s0 + j) * kstride + k;
-        float4 r0, r1;
-        float r[CPT];
+    for (int j = 0; j < NB_F; ++j) {
+        float4 *d = reinterpret_cast<float4 *>(red + ((warp * NB_F + j) * CPW + lane * CPL));
+        d[0] = make_float4(acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+        d[1] = make_float4(acc[j][4], acc[j][5], acc[j][6], acc[j][7]);
+    }
+    __syncthreads();
+    const int j = warp;
+    if (!live || s0 + j >= ns) return;
+    float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) r[c] = (k + c < kb) ? scale * acc[j][c] : 0.0f;   // padding channels: 0
-        r0 = make_float4(r[0], r[1], r[2], r[3]);
-        r1 = make_float4(r[4], r[5], r[6], r[7]);
-        reinterpret_cast<float4 *>(o)[0] = r0;
-        reinterpret_cast<float4 *>(o)[1] = r1;
+    for (int w = 0; w < WARPS; ++w) {
+        const float4 *q = reinterpret_cast<const float4 *>(red + ((w * NB_F + j) * CPW + lane * CPL));
+        const float4 q0 = q[0], q1 = q[1];
+        r0.x = __fadd_rn(r0.x, q0.x); r0.y = __fadd_rn(r0.y, q0.y); r0.z = __fadd_rn(r0.z, q0.z);
+        r0.w = __fadd_rn(r0.w, q0.w); r1.x = __fadd_rn(r1.x, q1.x); r1.y = __fadd_rn(r1.y, q1.y);
+        r1.z = __fadd_rn(r1.z, q1.z); r1.w = __fadd_rn(r1.w, q1.w);
+    }
+    float r[CPL] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) r[q] = (k + q < kb) ? __fmul_rn(scale, r[q]) : 0.0f;   // padding channels: 0
+    float4 *o = reinterpret_cast<float4 *>(sino + ((int64_t)a * ns + s0 + j) * kstride + k);
+    o[0] = make_float4(r[0], r[1], r[2], r[3]);
+    o[1] = make_float4(r[4], r[5], r[6], r[7]);
+}
+
+// ------------------------------------------------------------------------------------------------ backward
+// SPDHG primal step of one coefficient: the operations of primal_update_kernel (solver.cu), bitwise
+__device__ __forceinline__ void primal_step(float &x, float &z, float t, float dz, float inv_p, float lam)
+{
+    const float zi = __fadd_rn(z, dz);
+    z = zi;
+    const float zb = __fadd_rn(zi, __fmul_rn(inv_p, dz));
+    x = t > 0.0f ? fmaxf(0.0f, __fsub_rn(x, __fmul_rn(t, __fadd_rn(zb, lam)))) : 0.0f;
+}
+
+// MODE 0: img (npix, kstride) = backprojection; MODE 1: the backprojection dz is applied to x, z (T the steps):
+// z += dz; x = T > 0 ? max(0, x - T (z + inv_p dz + lam)) : 0.
+template <int KERNEL, int MODE>
+__global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
+    const float *__restrict__ sino, float *__restrict__ img, const float4 *__restrict__ geo, int n_angles, int nx,
+    int ny, int ns, int kstride, int kb, int n_taps, float *__restrict__ z, const float *__restrict__ T, float inv_p,
+    float lam)
+{
+    extern __shared__ AngleParams prm[];                   // the constants of every angle
+    for (int i = threadIdx.x; i < n_angles; i += blockDim.x) prm[i] = pack_geo(load_geo(geo, i));
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t p = (int64_t)blockIdx.x * WARPS + warp;
+    const int k = blockIdx.y * CPW + lane * CPL;
+    if (p >= (int64_t)nx * ny || k >= kstride) return;
+    const int px = (int)(p % nx), py = (int)(p / nx);
+    const float fx = (float)px, fy = (float)py;
+    float acc[CPL];
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) acc[c] = 0.0f;
+    const float *col = sino + k;
+    const int64_t angle_stride = (int64_t)ns * kstride;
+    for (int a = 0; a < n_angles; ++a, col += angle_stride) {
+        const AngleGeo g = unpack_geo(prm[a]);
+        const float t = __fmaf_rn(g.A, g.rows_are_y ? fx : fy, __fmaf_rn(g.B, g.rows_are_y ? fy : fx, g.T0));
+        const int sf = first_tap<KERNEL>(g, t);
+        const int ntap = taps_of(g, KERNEL, n_taps);
+        if (ntap == 2 && sf >= 0 && sf + 1 < ns) {        // the common case: two taps inside the detector
+            const float w0 = __fmul_rn(g.w, tap_weight<KERNEL>(g, __fsub_rn(t, (float)sf)));
+            const float w1 = __fmul_rn(g.w, tap_weight<KERNEL>(g, __fsub_rn(t, (float)(sf + 1))));
+            float4 a0, a1, b0, b1;
+            ld8(col + (int64_t)sf * kstride, a0, a1);
+            ld8(col + (int64_t)(sf + 1) * kstride, b0, b1);
+            acc8(acc, w0, a0, a1);
+            acc8(acc, w1, b0, b1);
+            continue;
+        }
+        for (int i = 0; i < ntap; ++i) {
+            const int s = sf + i;
+            if (s < 0 || s >= ns) continue;
+            const float w = tap_weight<KERNEL>(g, __fsub_rn(t, (float)s));
+            if (w == 0.0f) continue;
+            float4 q0, q1;
+            ld8(col + (int64_t)s * kstride, q0, q1);
+            acc8(acc, __fmul_rn(g.w, w), q0, q1);
+        }
+    }
+    const int64_t o = p * kstride + k;
+    if (MODE == 0) {
+        float r[CPL];
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) r[c] = (k + c < kb) ? acc[c] : 0.0f;      // padding channels: 0
+        float4 *d = reinterpret_cast<float4 *>(img + o);
+        d[0] = make_float4(r[0], r[1], r[2], r[3]);
+        d[1] = make_float4(r[4], r[5], r[6], r[7]);
+    } else {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            float4 *xp = reinterpret_cast<float4 *>(img + o) + h;
+            float4 *zp = reinterpret_cast<float4 *>(z + o) + h;
+            float4 xv = *xp, zv = *zp;
+            const float4 tv = __ldg(reinterpret_cast<const float4 *>(T + o) + h);
+            primal_step(xv.x, zv.x, tv.x, (k + 4 * h + 0 < kb) ? acc[4 * h + 0] : 0.0f, inv_p, lam);
+            primal_step(xv.y, zv.y, tv.y, (k + 4 * h + 1 < kb) ? acc[4 * h + 1] : 0.0f, inv_p, lam);
+            primal_step(xv.z, zv.z, tv.z, (k + 4 * h + 2 < kb) ? acc[4 * h + 2] : 0.0f, inv_p, lam);
+            primal_step(xv.w, zv.w, tv.w, (k + 4 * h + 3 < kb) ? acc[4 * h + 3] : 0.0f, inv_p, lam);
+            *xp = xv;
+            *zp = zv;
+        }
     }
 }
 
-template <int KERNEL>
-__global__ void __launch_bounds__(BWD_CG *BWD_PX) radon_backward_kernel(
-    const float *__restrict__ sino, float *__restrict__ img, const float4 *__restrict__ geo, int n_angles, int nx,
-    int ny, int ns, int kstride, int kb, int n_taps)
+// ------------------------------------------------------------------------------------------------ batch helpers
+// Element-wise on channel-fastest batches (npix, kstride) whose channels kb .. kstride-1 are padding:
+// mode 0: x = 1 inside the support on live channels, else 0 (support_ones); mode 1: x = 0 outside the support, on
+// padding channels or where negative (project_support); mode 2: T = min(T, c / colsum) inside the support where
+// colsum > 0 (tmin).
+__global__ void batch_support_kernel(float *__restrict__ x, const float *__restrict__ colsum,
+                                     const uint8_t *__restrict__ supp, int64_t npix, int kstride, int kb, float c,
+                                     int mode)
 {
-    const int k = (blockIdx.y * BWD_CG + threadIdx.x) * CPT;
-    const int64_t p = (int64_t)blockIdx.x * BWD_PX + threadIdx.y;
-    if (k >= kstride || p >= (int64_t)nx * ny) return;
-    const int x = (int)(p % nx), y = (int)(p / nx);
-    float acc[CPT];
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) acc[c] = 0.0f;
-    if (k < kb) {
-        const float *col = sino + k;
-        for (int a = 0; a < n_angles; ++a) {
-            const AngleGeo g = load_geo(geo, a);
-            const float u = (float)(g.rows_are_y ? x : y), v = (float)(g.rows_are_y ? y : x);
-            const float t = __fmaf_rn(g.A, u, __fmaf_rn(g.B, v, g.T0));
-            const int s_lo = KERNEL == 1 ? (int)floorf(__fsub_rn(t, g.hw)) : (int)floorf(t);
-            const int n = KERNEL == 1 ? n_taps + 1 : 2;
-            for (int i = 0; i < n; ++i) {
-                const int s = s_lo + i;
-                if (s < 0 || s >= ns) continue;
-                const float w = tap_weight<KERNEL>(g, __fsub_rn(t, (float)s));
-                if (w == 0.0f) continue;
-                const float ww = __fmul_rn(g.w, w);
-                float4 q0, q1;
-                ld8(col + ((int64_t)a * ns + s) * kstride, q0, q1);
-                acc[0] = __fmaf_rn(ww, q0.x, acc[0]);
-                acc[1] = __fmaf_rn(ww, q0.y, acc[1]);
-                acc[2] = __fmaf_rn(ww, q0.z, acc[2]);
-                acc[3] = __fmaf_rn(ww, q0.w, acc[3]);
-                acc[4] = __fmaf_rn(ww, q1.x, acc[4]);
-                acc[5] = __fmaf_rn(ww, q1.y, acc[5]);
-                acc[6] = __fmaf_rn(ww, q1.z, acc[6]);
-                acc[7] = __fmaf_rn(ww, q1.w, acc[7]);
-            }
+    const int64_t n = npix * kstride;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = i / kstride;
+        const int k = (int)(i - p * kstride);
+        const bool inside = (supp ? __ldg(supp + p) != 0 : true) && k < kb;
+        if (mode == 0) {
+            x[i] = inside ? 1.0f : 0.0f;
+        } else if (mode == 1) {
+            if (!inside || x[i] < 0.0f) x[i] = 0.0f;
+        } else {
+            const float cs = colsum[i];
+            if (inside && cs > 0.0f) x[i] = fminf(x[i], __fdiv_rn(c, cs));
         }
     }
-#pragma unroll
-    for (int c = 0; c < CPT; ++c)
-        if (k + c >= kb) acc[c] = 0.0f;                     // padding channels: 0
-    float4 *o = reinterpret_cast<float4 *>(img + p * kstride + k);
-    o[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
-    o[1] = make_float4(acc[4], acc[5], acc[6], acc[7]);
 }
 
 // (Ktot, npix) <-> (npix, kstride) channel transposes through a 32 x 33 shared tile.
@@ -180,13 +293,43 @@ static int check_radon_args(const void *in, const void *out, const void *geo, in
     DFX_REQUIRE(in && out && geo, "radon: null pointer");
     DFX_REQUIRE(n_angles >= 0 && nx > 0 && ny > 0 && n_det > 0, "radon: bad sizes (angles %d, %d x %d, %d bins)",
                 n_angles, nx, ny, n_det);
-    DFX_REQUIRE(kstride > 0 && kstride % CPT == 0 && kb >= 0 && kb <= kstride,
-                "radon: kstride (%d) must be a positive multiple of %d and kb (%d) <= kstride", kstride, CPT, kb);
+    DFX_REQUIRE(kstride > 0 && kstride % CPL == 0 && kb >= 0 && kb <= kstride,
+                "radon: kstride (%d) must be a positive multiple of %d and kb (%d) <= kstride", kstride, CPL, kb);
     DFX_REQUIRE(kernel == 0 || kernel == 1, "radon: kernel must be 0 (hat) or 1 (trapezoid)");
     DFX_REQUIRE(((uintptr_t)in % 16) == 0 && ((uintptr_t)out % 16) == 0 && ((uintptr_t)geo % 16) == 0,
                 "radon: arrays must be 16-byte aligned");
     DFX_REQUIRE((int64_t)nx * ny * kstride < ((int64_t)1 << 40), "radon: image batch too large");
     return DFX_OK;
+}
+
+template <typename Kernel>
+static int allow_smem(Kernel kernel, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return DFX_OK;
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) {
+        set_error("radon: %zu bytes of shared memory: %s", bytes, cudaGetErrorString(e));
+        return DFX_ECUDA;
+    }
+    return DFX_OK;
+}
+
+template <int KERNEL, int MODE>
+static int launch_backward(const float *sino, float *img, const float *geo, int n_angles, int nx, int ny, int n_det,
+                           int kstride, int kb, int n_taps, float *z, const float *T, float inv_p, float lam,
+                           void *stream)
+{
+    const int64_t npix = (int64_t)nx * ny;
+    dim3 grid((unsigned)cdiv(npix, WARPS), (unsigned)cdiv(kstride, CPW));
+    DFX_REQUIRE(grid.x < 2147483647u && grid.y <= 65535u, "radon: batch too large for one launch");
+    const size_t smem = sizeof(AngleParams) * (size_t)(n_angles > 0 ? n_angles : 1);
+    DFX_REQUIRE(smem <= 200 * 1024, "radon: %d angles exceed the shared memory of one launch", n_angles);
+    int st = allow_smem(radon_backward_v3<KERNEL, MODE>, smem);
+    if (st) return st;
+    radon_backward_v3<KERNEL, MODE><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
+        sino, img, reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, kstride, kb, n_taps, z, T, inv_p,
+        lam);
+    return launch_status(MODE ? "radon_backward_spdhg" : "radon_backward");
 }
 
 }  // namespace dfx
@@ -199,16 +342,19 @@ extern "C" int dfx_radon_forward(const float *img_k, float *sino_k, const float 
     int st = check_radon_args(img_k, sino_k, geo, n_angles, nx, ny, n_det, kstride, kb, kernel);
     if (st) return st;
     if (n_angles == 0) return DFX_OK;
-    constexpr int NB = 2;
     DFX_REQUIRE(n_angles <= 65535, "radon: at most 65535 angles per launch");
-    dim3 block(FWD_CG, FWD_BG);
-    dim3 grid((unsigned)cdiv(n_det, FWD_BG * NB), (unsigned)cdiv(kstride, FWD_CG * CPT), (unsigned)n_angles);
-    cudaStream_t s = (cudaStream_t)stream;
-    const float4 *g4 = reinterpret_cast<const float4 *>(geo);
-    if (kernel == 1)
-        radon_forward_kernel<1, NB><<<grid, block, 0, s>>>(img_k, sino_k, g4, nx, ny, n_det, kstride, kb, scale);
-    else
-        radon_forward_kernel<0, NB><<<grid, block, 0, s>>>(img_k, sino_k, g4, nx, ny, n_det, kstride, kb, scale);
+    dim3 grid((unsigned)cdiv(n_det, NB_F), (unsigned)cdiv(kstride, CPW), (unsigned)n_angles);
+    const size_t smem = sizeof(float) * WARPS * NB_F * CPW;      // 64 KB of partial projections
+    const int max_taps = 64;                                      // per angle: ceil(1 + |A|)
+    if (kernel == 1) {
+        if ((st = allow_smem(radon_forward_v3<1>, smem))) return st;
+        radon_forward_v3<1><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
+            img_k, sino_k, reinterpret_cast<const float4 *>(geo), nx, ny, n_det, kstride, kb, scale, max_taps);
+    } else {
+        if ((st = allow_smem(radon_forward_v3<0>, smem))) return st;
+        radon_forward_v3<0><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
+            img_k, sino_k, reinterpret_cast<const float4 *>(geo), nx, ny, n_det, kstride, kb, scale, max_taps);
+    }
     return launch_status("radon_forward");
 }
 
@@ -218,17 +364,39 @@ extern "C" int dfx_radon_backward(const float *sino_k, float *img_k, const float
     int st = check_radon_args(sino_k, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, kernel);
     if (st) return st;
     DFX_REQUIRE(n_taps >= 2 && n_taps <= 64, "radon: n_taps (%d) out of range", n_taps);
-    const int64_t npix = (int64_t)nx * ny;
-    dim3 block(BWD_CG, BWD_PX);
-    dim3 grid((unsigned)cdiv(npix, BWD_PX), (unsigned)cdiv(kstride, BWD_CG * CPT));
-    DFX_REQUIRE(grid.x < 2147483647u && grid.y <= 65535u, "radon: batch too large for one launch");
-    cudaStream_t s = (cudaStream_t)stream;
-    const float4 *g4 = reinterpret_cast<const float4 *>(geo);
     if (kernel == 1)
-        radon_backward_kernel<1><<<grid, block, 0, s>>>(sino_k, img_k, g4, n_angles, nx, ny, n_det, kstride, kb, n_taps);
-    else
-        radon_backward_kernel<0><<<grid, block, 0, s>>>(sino_k, img_k, g4, n_angles, nx, ny, n_det, kstride, kb, n_taps);
-    return launch_status("radon_backward");
+        return launch_backward<1, 0>(sino_k, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, n_taps, nullptr,
+                                     nullptr, 0.0f, 0.0f, stream);
+    return launch_backward<0, 0>(sino_k, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, n_taps, nullptr, nullptr,
+                                 0.0f, 0.0f, stream);
+}
+
+extern "C" int dfx_radon_backward_spdhg(const float *sino_k, const float *geo, int n_angles, int nx, int ny, int n_det,
+                                        int kstride, int kb, int kernel, int n_taps, float *x_k, float *z_k,
+                                        const float *T_k, float inv_p, float lam, void *stream)
+{
+    int st = check_radon_args(sino_k, x_k, geo, n_angles, nx, ny, n_det, kstride, kb, kernel);
+    if (st) return st;
+    DFX_REQUIRE(z_k && T_k && ((uintptr_t)z_k % 16) == 0 && ((uintptr_t)T_k % 16) == 0,
+                "radon_backward_spdhg: z and T must be 16-byte aligned device arrays");
+    DFX_REQUIRE(n_taps >= 2 && n_taps <= 64, "radon: n_taps (%d) out of range", n_taps);
+    if (kernel == 1)
+        return launch_backward<1, 1>(sino_k, x_k, geo, n_angles, nx, ny, n_det, kstride, kb, n_taps, z_k, T_k, inv_p,
+                                     lam, stream);
+    return launch_backward<0, 1>(sino_k, x_k, geo, n_angles, nx, ny, n_det, kstride, kb, n_taps, z_k, T_k, inv_p, lam,
+                                 stream);
+}
+
+extern "C" int dfx_batch_support(float *x_k, const float *colsum_k, const uint8_t *supp, int64_t npix, int kstride,
+                                 int kb, float c, int mode, void *stream)
+{
+    DFX_REQUIRE(x_k && npix > 0 && kstride > 0 && kb >= 0 && kb <= kstride && mode >= 0 && mode <= 2,
+                "batch_support: bad arguments");
+    DFX_REQUIRE(mode != 2 || colsum_k, "batch_support: tmin needs the column sums");
+    const int64_t blocks = cdiv(npix * kstride, 256);
+    batch_support_kernel<<<(unsigned)(blocks < 148 * 32 ? blocks : 148 * 32), 256, 0, (cudaStream_t)stream>>>(
+        x_k, colsum_k, supp, npix, kstride, kb, c, mode);
+    return launch_status("batch_support");
 }
 
 extern "C" int dfx_gather_channels(const float *coeffs, float *img_k, int64_t npix, int k0, int kb, int kstride,
@@ -247,8 +415,8 @@ extern "C" int dfx_scatter_channels(const float *img_k, float *coeffs, int64_t n
 {
     DFX_REQUIRE(coeffs && img_k, "scatter: null pointer");
     DFX_REQUIRE(npix > 0 && k0 >= 0 && kb >= 0 && kb <= kstride, "scatter: bad sizes");
-    dim3 grid((unsigned)cdiv(npix, TT), (unsigned)cdiv(kb, TT));
     if (kb == 0) return DFX_OK;
+    dim3 grid((unsigned)cdiv(npix, TT), (unsigned)cdiv(kb, TT));
     DFX_REQUIRE(grid.y <= 65535u, "scatter: kb too large");
     scatter_kernel<<<grid, dim3(TT, 8), 0, (cudaStream_t)stream>>>(img_k, coeffs, npix, k0, kb, kstride);
     return launch_status("scatter_channels");

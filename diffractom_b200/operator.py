@@ -438,6 +438,68 @@ class SinglePhaseForwardOperator:
         self._call("dfx_scatter_channels", self._img_k.data_ptr(), target.data_ptr(), self.npix, k_target, Kb,
                    self.Kstride, s)
 
+    # ---- channel-fastest batches: the solvers keep their coefficient state in the layout the kernels use, batch ib
+    # at element offset ib * npix * Kstride of a flat array (no gather / scatter pass per iteration)
+    def batch_elems(self) -> int:
+        return self.npix * self.Kstride
+
+    def _geo_of(self, subset):
+        if subset is None:
+            return self.geo_gpu, self.N_Omega, None, None
+        m = self._subset(subset)
+        e = self._sub[m]
+        return e["geo"], e["n"], e["omegas"], m
+
+    def _direct_batch_k(self, src_ptr, ib, data, subset=None):
+        """Add the forward projection of batch ib, given channel-fastest at device address src_ptr, to data."""
+        Kb = self.batches[ib]["K_batch"]
+        s = self._s()
+        geo, n_ang, om, m = self._geo_of(subset)
+        self._call("dfx_radon_forward", src_ptr, self.coeffs_sino_C.data_ptr(), geo.data_ptr(), n_ang, self.Nx,
+                   self.Ny, self.My, self.Kstride, Kb, self._kernel_id, float(self.radon_geo.scale), s)
+        rp, col, val, compact = self._pf_batch(ib, True, m)
+        self._call("dfx_spmm_pf_forward", self.coeffs_sino_C.data_ptr(), rp.data_ptr(), col.data_ptr(),
+                   val.data_ptr(), data.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My,
+                   self.N_seg, self.Kstride, Kb, compact, s)
+
+    def _pf_adjoint_to_sino(self, data, ib, subset):
+        Kb = self.batches[ib]["K_batch"]
+        geo, n_ang, om, m = self._geo_of(subset)
+        alpha = float(np.float32(self.N_Omega / np.pi))
+        rp, col, val, compact = self._pf_batch(ib, False, m)
+        self._call("dfx_spmm_pf_adjoint", data.data_ptr(), rp.data_ptr(), col.data_ptr(), val.data_ptr(),
+                   self.coeffs_sino_C.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My, Kb,
+                   self.N_seg, self.Kstride, alpha, compact, self._s())
+        return geo, n_ang, Kb
+
+    def _adjoint_batch_k(self, data, ib, out_ptr, subset=None):
+        """A^T data of batch ib into a channel-fastest batch at device address out_ptr."""
+        geo, n_ang, Kb = self._pf_adjoint_to_sino(data, ib, subset)
+        self._call("dfx_radon_backward", self.coeffs_sino_C.data_ptr(), out_ptr, geo.data_ptr(), n_ang, self.Nx,
+                   self.Ny, self.My, self.Kstride, Kb, self._kernel_id, int(self.radon_geo.n_taps), self._s())
+
+    def _adjoint_update_batch(self, data, ib, subset, x_ptr, z_ptr, T_ptr, inv_p, lam):
+        """SPDHG's update of batch ib: dz = A_m^T data (batch ib), z += dz, x = max(0, x - T (z + inv_p dz + lam)),
+        on channel-fastest batches, the primal step fused into the backprojection."""
+        geo, n_ang, Kb = self._pf_adjoint_to_sino(data, ib, subset)
+        self._call("dfx_radon_backward_spdhg", self.coeffs_sino_C.data_ptr(), geo.data_ptr(), n_ang, self.Nx,
+                   self.Ny, self.My, self.Kstride, Kb, self._kernel_id, int(self.radon_geo.n_taps), x_ptr, z_ptr,
+                   T_ptr, float(inv_p), float(lam), self._s())
+
+    def to_batches(self, coeffs, out_k):
+        """coeffs (K, Ny, Nx) -> channel-fastest batches (flat, batch ib at ib * npix * Kstride)."""
+        s = self._s()
+        for ib, b in enumerate(self.batches):
+            self._call("dfx_gather_channels", coeffs.data_ptr(), out_k.data_ptr() + 4 * ib * self.batch_elems(),
+                       self.npix, b["k_start"], b["K_batch"], self.Kstride, s)
+
+    def from_batches(self, in_k, coeffs):
+        """Channel-fastest batches -> coeffs (K, Ny, Nx)."""
+        s = self._s()
+        for ib, b in enumerate(self.batches):
+            self._call("dfx_scatter_channels", in_k.data_ptr() + 4 * ib * self.batch_elems(), coeffs.data_ptr(),
+                       self.npix, b["k_start"], b["K_batch"], self.Kstride, s)
+
     def adjoint_batches_cl(self, data, out_batch, update):
         """The adjoint one batch at a time into the first Kb * Ny * Nx elements of out_batch, then update(k0, Kb)
         (SPFO:1819-1838)."""

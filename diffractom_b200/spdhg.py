@@ -10,8 +10,10 @@ forward of the next subset) and the same state dict.
 Iteration, for the next subset m (p_m = 1 / M):
     y_m'  <- prox_{S F_m*}(y_m + S A_m x)            rows of subset m, closed form in float64
     dz    <- A_m^T (y_m' - y_m);  z <- z + dz;  x <- max(0, x - T (z + dz / p_m + lam))
-Device arrays: x, z, T (coefficient-sized), y, S, D (data-sized; D holds A_m x of the next subset and the dual
-change of the current one) and one batch-sized dz.
+Device arrays: x, z, T (coefficient-sized, kept for the whole run in the operator's channel-fastest batch layout, so
+that an iteration needs no gather / scatter and the primal step runs in the backprojection's epilogue), y, S, D
+(data-sized; D holds A_m x of the next subset and the dual change of the current one) and one batch-sized scratch.
+x is converted back to the (K, Ny, Nx) layout for callbacks and at the end; z for the state.
 """
 from __future__ import annotations
 
@@ -83,19 +85,15 @@ class SPDHGPoisson:
         """One pass over the batches: adjoint of subset adj's dual change (in D), z and x updated; then the forward
         of the new x for subset fwd ("full": all rows) added to D (spdhg_poisson.py:430-484)."""
         op = self.op
-        npix, kmax = op.npix, op.K_batch_max
-        s = op._s()
+        be = op.batch_elems()
         sub = None if fwd == "full" else fwd
-        for ib, b in enumerate(op.batches):
-            k0, kb = b["k_start"], b["K_batch"]
-            off = k0 * npix * 4
-            n = kb * npix
-            if adj is not None:
-                op._adjoint_batch(self.D, ib, self.dz, 0, kmax, subset=adj)
-                _lib.call("dfx_spdhg_primal_update", self.x.data_ptr() + off, self.z.data_ptr() + off,
-                          self.T.data_ptr() + off, self.dz.data_ptr(), float(self._inv_p_data), self.lam, n, s)
+        for ib in range(len(op.batches)):
+            off = 4 * ib * be
+            if adj is not None:       # A_m^T of the dual change, z and x updated in the backprojection's epilogue
+                op._adjoint_update_batch(self.D, ib, adj, self.xk.data_ptr() + off, self.zk.data_ptr() + off,
+                                         self.Tk.data_ptr() + off, self._inv_p_data, self.lam)
             if fwd is not None:
-                op._direct_batch(self.x, k0, op.K, ib, self.D, sub)
+                op._direct_batch_k(self.xk.data_ptr() + off, ib, self.D, sub)
 
     def _deviance(self, mu):
         return self.red.deviance(mu, self.b, self.w, self.pw, self.g, self.pg, self.bg, self.pbg, self.eps_counts)
@@ -130,7 +128,6 @@ class SPDHGPoisson:
         self.y = torch.zeros(dshape, dtype=torch.float32, device=dev)
         self.sig = torch.empty(dshape, dtype=torch.float32, device=dev)
         self.D = torch.empty(dshape, dtype=torch.float32, device=dev)
-        self.dz = torch.empty(npix * op.K_batch_max, dtype=torch.float32, device=dev)
         supp = self.support_gpu
         sp = None if supp is None else supp.data_ptr()
         npx = 0 if supp is None else npix
@@ -144,16 +141,24 @@ class SPDHGPoisson:
         gamma = np.sqrt(rho)
         p = self._p_data
         self.resident_used = NAMES
-        self.z = torch.zeros(cshape, dtype=torch.float32, device=dev)
+        # x, z, T live in the operator's channel-fastest batch layout for the whole run (batch ib at ib * be)
+        be = op.batch_elems()
+        nbt = len(op.batches)
+        self.xk = torch.empty(nbt * be, dtype=torch.float32, device=dev)
+        self.zk = torch.empty(nbt * be, dtype=torch.float32, device=dev)
+        self.Tk = torch.empty(nbt * be, dtype=torch.float32, device=dev)
+        self.dzk = torch.empty(be, dtype=torch.float32, device=dev)
+        op.to_batches(self.x, self.xk)
         if state is not None and state.get("z") is not None:
-            self.z.copy_(torch.as_tensor(as_host(state["z"], cshape, "state['z']")))
-        self.T = torch.empty(cshape, dtype=torch.float32, device=dev)
+            op.to_batches(torch.as_tensor(as_host(state["z"], cshape, "state['z']"), device=dev), self.zk)
+        else:
+            op._fill(self.zk, 0.0)
 
         # S from the row sums A 1_S (spdhg_poisson.py:621-629)
         op._fill(self.D, 0.0)
         for ib, bt in enumerate(op.batches):
-            _lib.call("dfx_support_ones", self.dz.data_ptr(), sp, npx, npix * bt["K_batch"], s)
-            op._direct_batch(self.dz, 0, op.K_batch_max, ib, self.D)
+            _lib.call("dfx_batch_support", self.dzk.data_ptr(), None, sp, npix, op.Kstride, bt["K_batch"], 0.0, 0, s)
+            op._direct_batch_k(self.dzk.data_ptr(), ib, self.D)
         rs, rn = self.red.mean_counted(self.D, self.w, self.pw)
         bs, bn = self.red.mean_counted(self.b, self.w, self.pw)
         self.scales = {"row_sum_mean": rs / max(rn, 1.0), "b_mean": bs / max(bn, 1.0),
@@ -164,19 +169,20 @@ class SPDHGPoisson:
         _lib.call("dfx_set_mask_ones", self.D.data_ptr(), _ptr(self.w), self.pw, self.D.numel(), s)
         c = float(np.float32(p / gamma))
         for ib, bt in enumerate(op.batches):
-            off = bt["k_start"] * npix * 4
-            n = bt["K_batch"] * npix
-            tb = self.T.data_ptr() + off
-            _lib.call("dfx_tinit", tb, n, s)
+            tb = self.Tk.data_ptr() + 4 * ib * be
+            _lib.call("dfx_tinit", tb, be, s)
             for m in range(self.M):
-                op._adjoint_batch(self.D, ib, self.dz, 0, op.K_batch_max, subset=m)
-                _lib.call("dfx_tmin", tb, self.dz.data_ptr(), sp, npx, c, n, s)
-            _lib.call("dfx_tfinal", tb, n, s)
-        _lib.call("dfx_project_support", self.x.data_ptr(), sp, npx, self.x.numel(), s)
+                op._adjoint_batch_k(self.D, ib, self.dzk.data_ptr(), subset=m)
+                _lib.call("dfx_batch_support", tb, self.dzk.data_ptr(), sp, npix, op.Kstride, bt["K_batch"], c, 2, s)
+            _lib.call("dfx_tfinal", tb, be, s)           # padding channels were never reached: T = 0 there
+        for ib, bt in enumerate(op.batches):            # x on the support, >= 0, padding 0
+            _lib.call("dfx_batch_support", self.xk.data_ptr() + 4 * ib * be, None, sp, npix, op.Kstride,
+                      bt["K_batch"], 0.0, 1, s)
         if state is not None:
             self.y.copy_(torch.as_tensor(as_host(state["y"], dshape, "state['y']")))
             if state.get("z") is None:
-                op.adjoint_cl(self.y, self.z)
+                for ib in range(nbt):
+                    op._adjoint_batch_k(self.y, ib, self.zk.data_ptr() + 4 * ib * be)
         self._t_setup = time.perf_counter() - self._t_start
         self._ep0 = int(state["epoch"]) if state is not None else 0
         self.iter_stats = []
@@ -226,6 +232,7 @@ class SPDHGPoisson:
             self.iter_stats.append(stats)
             stop = False
             if callback is not None:
+                op.from_batches(self.xk, self.x)
                 if not self._x_on_gpu:
                     self._host_x[...] = self.x.cpu().numpy()
                 stop = bool(callback(ep, self.x if self._x_on_gpu else self._host_x, stats))
@@ -236,7 +243,12 @@ class SPDHGPoisson:
                 break
 
     def _finish(self):
-        self.state = {"epoch": self._ep0 + len(self.iter_stats), "z": self.z.cpu().numpy(), "y": self.y.cpu().numpy()}
+        op = self.op
+        op.from_batches(self.xk, self.x)
+        z = torch.empty(op.coeff_shape, dtype=torch.float32, device=op.device)
+        op.from_batches(self.zk, z)
+        self.state = {"epoch": self._ep0 + len(self.iter_stats), "z": z.cpu().numpy(), "y": self.y.cpu().numpy()}
+        del z
         self.final_stats = {"epochs": len(self.iter_stats), "final_f": self._f, "setup_s": self._t_setup,
                             "rho": self.rho_used, "subsets": self.M, "resident": self.resident_used,
                             "time": time.perf_counter() - self._t_start, "tv": 0.0, "tv_prob": 0.0, **self.scales}
@@ -244,7 +256,8 @@ class SPDHGPoisson:
         if not self._x_on_gpu:
             self._host_x[...] = x.cpu().numpy()
         out = x if self._x_on_gpu else self._host_x
-        self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = self.dz = self.z = self.T = None
+        self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = None
+        self.xk = self.zk = self.Tk = self.dzk = None
         self.x = None
         return out
 

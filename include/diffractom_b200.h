@@ -63,6 +63,21 @@ int dfx_radon_forward(const float *img_k, float *sino_k, const float *geo, int n
 int dfx_radon_backward(const float *sino_k, float *img_k, const float *geo, int n_angles, int nx, int ny, int n_det,
                        int kstride, int kb, int kernel, int n_taps, void *stream);
 
+/* replaces, in one kernel, radon_backward_k + scatter_channels_k_fastest + spdhg_update (radon_kernels.cl:106-141,
+ * 192-215; spdhg_poisson.py:95-106) for the fused SPDHG pass (spdhg_poisson.py:430-484): the backprojection dz of
+ * sino_k is applied to channel-fastest coefficient batches x_k, z_k, T_k (npix, kstride):
+ * z += dz; x = T > 0 ? max(0, x - T (z + inv_p dz + lam)) : 0 (dz = 0 on padding channels kb .. kstride-1). */
+int dfx_radon_backward_spdhg(const float *sino_k, const float *geo, int n_angles, int nx, int ny, int n_det,
+                             int kstride, int kb, int kernel, int n_taps, float *x_k, float *z_k, const float *T_k,
+                             float inv_p, float lam, void *stream);
+
+/* replaces support_ones / project_support / tmin (fista_poisson.py:256-263, 277-281; spdhg_poisson.py:259-265) on a
+ * channel-fastest batch (npix, kstride) with padding channels kb .. kstride-1 (supp (npix) uint8 or NULL):
+ * mode 0: x = 1 on live channels of support pixels, else 0; mode 1: x = 0 outside them or where negative;
+ * mode 2: x = min(x, c / colsum) on live channels of support pixels where colsum > 0. */
+int dfx_batch_support(float *x_k, const float *colsum_k, const uint8_t *supp, int64_t npix, int kstride, int kb,
+                      float c, int mode, void *stream);
+
 /* ---------------------------------------------------------------- pole-figure matrix
  * The PF entry of (angle r, orientation k, eta bin c, ring p) is pf_entry of operators/pf_generate.cl:62-140
  * (== pfmatrix_eval_poles, operators/create_pfo_matrix.py:108-199), times the ring intensity unless normalized. */

@@ -127,6 +127,37 @@ def test_numpy_streaming_equals_device_and_is_reproducible(golden):
     assert np.array_equal(op.direct(d["c"]), c_dev)          # same bits every call
 
 
+def test_fused_backprojection_update_equals_unfused(golden):
+    """dfx_radon_backward_spdhg (backprojection + SPDHG primal step in one kernel) gives bitwise the result of the
+    backprojection followed by dfx_spdhg_primal_update; channel-fastest batches round-trip through the gathers."""
+    from diffractom_b200 import _lib
+    d = golden("al5_small")
+    op = make_operator(d)
+    op.set_omega_subsets(3)
+    rng = np.random.default_rng(4)
+    be = op.batch_elems()
+    data = torch.as_tensor(rng.random(op.data_shape).astype(np.float32), device="cuda")
+    coeffs = torch.as_tensor(rng.random(op.coeff_shape).astype(np.float32), device="cuda")
+    xk = torch.empty(len(op.batches) * be, device="cuda")
+    op.to_batches(coeffs, xk)
+    back = torch.empty(op.coeff_shape, device="cuda")
+    op.from_batches(xk, back)
+    assert torch.equal(back, coeffs)
+    zk = torch.as_tensor(rng.normal(0, 1, xk.numel()).astype(np.float32), device="cuda")
+    Tk = torch.as_tensor((rng.random(xk.numel()) * (rng.random(xk.numel()) < 0.8)).astype(np.float32),
+                         device="cuda")
+    x1, z1 = xk.clone(), zk.clone()
+    dz = torch.empty(be, device="cuda")
+    for ib in range(len(op.batches)):
+        off = ib * be
+        op._adjoint_batch_k(data, ib, dz.data_ptr(), subset=1)
+        _lib.call("dfx_spdhg_primal_update", x1.data_ptr() + 4 * off, z1.data_ptr() + 4 * off,
+                  Tk.data_ptr() + 4 * off, dz.data_ptr(), 3.0, 0.25, be, op._s())
+        op._adjoint_update_batch(data, ib, 1, xk.data_ptr() + 4 * off, zk.data_ptr() + 4 * off,
+                                 Tk.data_ptr() + 4 * off, 3.0, 0.25)
+    assert torch.equal(x1, xk) and torch.equal(z1, zk)
+
+
 def test_argument_errors(golden):
     d = golden("diff_midpoint_hat")
     op = make_operator(d)
