@@ -68,6 +68,11 @@ SIGNATURES = {
     "dfx_extrapolate": ([P, P, P, F, L, S], c_int),
     "dfx_copy_f32": ([P, P, L, S], c_int),
     "dfx_scale_f32": ([P, F, L, S], c_int),
+    "dfx_pf_dense_bf16": ([POINTER(PFGeometry), I, I, L, L, I, P, S], c_int),
+    "dfx_pf_tc_forward": ([P, L, I, I, I, P, P, I, I, P, I, S], c_int),
+    "dfx_pf_tc_adjoint": ([P, L, I, I, I, P, P, I, I, F, P, S], c_int),
+    "dfx_tc_status": ([POINTER(ctypes.c_uint), I], c_int),
+    "dfx_rows_to_bf16": ([P, P, P, I, I, I, I, S], c_int),
 }
 
 _lib = None

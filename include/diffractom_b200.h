@@ -202,6 +202,34 @@ int dfx_mean_counted(const float *b, const float *w, int64_t pw, int64_t n, doub
 int dfx_dot_f64(const float *x, const float *y, int64_t n, double *out, void *scratch, size_t scratch_bytes,
                 void *stream);
 
+/* ---------------------------------------------------------------- BF16 tensor-core precision path
+ * Dense BF16 PF (R, ktot, cp_pad), segments fastest: the batch k0 .. k0+kb-1 fills rows koff .. koff+kb-1 of every
+ * angle (columns CP .. cp_pad-1 and rows outside the batch are left as they are: zero them once). The entries are the
+ * float32 pf_entry values (dfx_pf_dense) rounded to nearest-even BF16. */
+int dfx_pf_dense_bf16(const dfx_pf_geometry *g, int k0, int kb, int64_t koff, int64_t ktot, int cp_pad, void *out,
+                      void *stream);
+
+/* replaces batched_gemm_clblast (SPFO:2063-2098) and, in the BF16 path, spmm_pf_forward_c (pf_kernels.cl:597-641):
+ * for the n_sub angles r = omegas[s] (omegas NULL: r = s), data[r, y, j] (+)= sum_k PF[r, k, j] Z[s, y, k] over all
+ * ktot orientations, with tcgen05 BF16 MMAs and float32 accumulation. pf_bf16 (n_omega, ktot, cp_pad), z_bf16
+ * (n_sub, my, ktot) BF16, data (n_omega, my, cp) float32; accumulate = 0 overwrites the rows. ktot and cp_pad
+ * multiples of 8, both BF16 arrays 16-byte aligned. */
+int dfx_pf_tc_forward(const void *pf_bf16, int64_t ktot, int cp, int cp_pad, int n_omega, const void *z_bf16,
+                      const int32_t *omegas, int n_sub, int my, float *data, int accumulate, void *stream);
+/* replaces batched_gemm_clblast_adj (SPFO:2100-2127) and, in the BF16 path, spmm_pf_adjoint_c (pf_kernels.cl:644-687):
+ * Z[s, y, k] = alpha sum_j PF[r, k, j] D[r, y, j] (BF16 out, float32 accumulation), d_bf16 (n_omega, my, cp_pad). */
+int dfx_pf_tc_adjoint(const void *pf_bf16, int64_t ktot, int cp, int cp_pad, int n_omega, const void *d_bf16,
+                      const int32_t *omegas, int n_sub, int my, float alpha, void *z_bf16, void *stream);
+/* Bits of device-side waits of the tensor-core kernels that ran out since the last reset (DFX_TC_TIMEOUT); the
+ * kernels return early on expiry and leave their outputs undefined. Synchronous; no reference counterpart. */
+#define DFX_TC_TIMEOUT 1u
+int dfx_tc_status(unsigned int *flags, int reset);
+
+/* BF16 copy of the data rows of the n_sub angles omegas[s] (omegas NULL: all n_omega rows): out (n_omega, my, cp_pad)
+ * = in (n_omega, my, cp) rounded to nearest-even, padding columns set to 0. The data side of the adjoint product. */
+int dfx_rows_to_bf16(const float *in, void *out, const int32_t *omegas, int n_sub, int my, int cp, int cp_pad,
+                     void *stream);
+
 /* FISTAPoisson (optimization/fista_poisson.py), all float32 element-wise with float64 sums:
  * replaces times_curvature (:115-144): u <- u * c, c the curvature of the data term at mu (mode 0 Poisson, 1 the
  * weighted least squares of the start); out[0] = sum c u_old^2. */
