@@ -205,6 +205,8 @@ def main():
     ap.add_argument("--workload", default="ti256", choices=sorted(WORKLOADS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["both", "bf16", "fp32"],
+                    help="both: the BF16 tensor-core path (the value) and the float32 path (for the ratio)")
     a = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -221,18 +223,72 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
 
-    from diffractom_b200 import SPDHGPoisson, SinglePhaseForwardOperator
-    from diffractom_b200 import _lib
+    from diffractom_b200 import SinglePhaseForwardOperator
     cfg, mat, grid, w = make_problem(a.workload)
     t_build = time.perf_counter()
-    op = SinglePhaseForwardOperator(cfg, mat, grid, w["max_gb"], normalized=True)
+    op = SinglePhaseForwardOperator(cfg, mat, grid, w["max_gb"], normalized=True,
+                                    precision="bf16" if a.precision in ("bf16", "both") else "fp32")
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
+    op.precision = "fp32"
     x_true = phantom(op, w)
     b = counts(op, x_true, w["mean_counts"])
     del x_true
     torch.cuda.empty_cache()
 
+    arms = {}
+    for prec in (("fp32", "bf16") if a.precision == "both" else (a.precision,)):
+        arms[prec] = timed_epochs(op, w, b, a, prec, dist, local, world)
+    head = arms["bf16" if "bf16" in arms else "fp32"]
+
+    e2e = None
+    if not a.no_e2e:
+        op.precision = "bf16" if "bf16" in arms else "fp32"
+        e2e = measure_e2e(op, w, b, a.steps)
+        op.precision = "fp32"
+    cpu = None
+    if rank == 0 and not a.no_cpu:
+        per_epoch, threads, desc, took = cpu_sample(op, w)
+        cpu = {"value": 1.0 / per_epoch, "unit": "epochs/s", "cores": threads, "kind": "port",
+               "sample": desc + f" ({took:.1f} s of CPU time)"}
+    if rank == 0:
+        cfg_line = {"workload": a.workload, "K": op.K, "pixels": f"{op.Nx}x{op.Ny}", "N_Omega": op.N_Omega,
+                    "My": op.My, "N_eta": op.N_eta, "rings": op.N_peaks, "subsets": w["subsets"],
+                    "batches": len(op.batches), "K_batch_max": op.K_batch_max, "pf_mode": op.pf_mode,
+                    "pf_nnz": op.sparse_nnz, "precision_path": "bf16-tc" if "bf16" in arms else "fp32",
+                    "l2": "inputs larger than L2, no flush", "parallelism": f"replicas x{world}",
+                    "operator_build_s": round(t_build, 2)}
+        for prec, r in arms.items():
+            cfg_line[f"{prec}_epochs_per_s"] = r["value"]
+            cfg_line[f"{prec}_final_deviance_f64"] = r["f"]
+        if len(arms) == 2:
+            xf, xb = arms["fp32"]["x"], arms["bf16"]["x"]
+            cfg_line["bf16_speedup_vs_fp32"] = arms["bf16"]["value"] / arms["fp32"]["value"]
+            cfg_line["deviance_rel_err_bf16_vs_fp32"] = abs(arms["bf16"]["f"] - arms["fp32"]["f"]) / arms["fp32"]["f"]
+            cfg_line["coef_rel_err_bf16_vs_fp32"] = float((xb - xf).double().norm() / xf.double().norm())
+            cfg_line["deviance_note"] = ("deviance of each run's final iterate: float32 forward, float64 sum; the "
+                                         "float32 path matches the float64 oracle to 1e-5 (tests)")
+            cfg_line["fp32_roofline"] = arms["fp32"]["roof"]
+        line = {
+            "metric": METRIC, "value": head["value"], "unit": "epochs/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": head["t_max"] / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16" if "bf16" in arms else "f32",
+            "data": "synthetic (seeded phantom, Poisson counts)", "config": cfg_line,
+            "roofline": head["roof"], "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(head["launches"]),
+            "clocks": head["clk"],
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def timed_epochs(op, w, b, a, precision, dist, local, world):
+    """warmup untimed + steps timed SPDHG epochs with the operator in the given precision; the deviance of the final
+    iterate with the float32 operator (float64 sum)."""
+    import torch
+    from diffractom_b200 import SPDHGPoisson, _lib
+    op.precision = precision
     sp = SPDHGPoisson(op, subsets=w["subsets"], seed=0)
     x0 = torch.zeros(op.coeff_shape, dtype=torch.float32, device=op.device)
     sp._setup(x0, b)
@@ -262,38 +318,16 @@ def main():
         t_max = float(tt.item())
         dist.barrier()
     value = world * a.steps / (t_max / 1e3)
-    # deviance of the iterate after warm-up + timed epochs (float64 reduction)
+    x = sp.x
     sp._finish()
+    op.precision = "fp32"
     D = torch.empty(op.data_shape, dtype=torch.float32, device=op.device)
-    op.direct_cl(sp.x, D)
+    op.direct_cl(x, D)
+    sp.b, sp.w, sp.pw, sp.g, sp.pg, sp.bg, sp.pbg = b, None, 0, None, 0, None, 0
     f_final = sp._deviance(D)
+    del D
     roof = timers.roofline(op)
-
-    e2e = None
-    if not a.no_e2e:
-        e2e = measure_e2e(op, w, b, a.steps)
-    cpu = None
-    if rank == 0 and not a.no_cpu:
-        per_epoch, threads, desc, took = cpu_sample(op, w)
-        cpu = {"value": 1.0 / per_epoch, "unit": "epochs/s", "cores": threads, "kind": "port",
-               "sample": desc + f" ({took:.1f} s of CPU time)"}
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": "epochs/s", "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson counts)",
-            "config": {"workload": a.workload, "K": op.K, "pixels": f"{op.Nx}x{op.Ny}", "N_Omega": op.N_Omega,
-                       "My": op.My, "N_eta": op.N_eta, "rings": op.N_peaks, "subsets": w["subsets"],
-                       "batches": len(op.batches), "K_batch_max": op.K_batch_max, "pf_mode": op.pf_mode,
-                       "pf_nnz": op.sparse_nnz, "precision_path": "fp32", "l2": "inputs larger than L2, no flush",
-                       "parallelism": f"replicas x{world}", "operator_build_s": round(t_build, 2),
-                       "final_deviance_f64": f_final},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
-        }
-        print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    return {"value": value, "t_max": t_max, "f": f_final, "x": x, "roof": roof, "launches": launches, "clk": clk}
 
 
 class KernelTimers:
@@ -331,54 +365,103 @@ class KernelTimers:
         self._lib.call = self._orig_lib
 
     def roofline(self, op):
+        """The dominant kernel (largest share of the timed kernels' device time) against its roofline: tensor-core
+        products against the measured sustained BF16 GEMM rate (they run inside a seconds-long loop), the rest
+        against the measured HBM copy bandwidth; every kernel's share and achieved rates under "kernels"."""
         import torch
         torch.cuda.synchronize()
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() \
             else {}
         hbm = float(peaks.get("hbm_gbs", 6650.0))
-        per = {}
-        for n, evs in self.events.items():
-            if evs:
-                per[n] = [e0.elapsed_time(e1) for e0, e1 in evs]
+        tc = float(peaks.get("bf16_tflops_sustained", 1400.0))
+        src = "MEASURED_PEAKS.json" if peaks else "fallback"
+        fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12          # FP32 FMA lanes x 2 flops x max SM clock (TFLOP/s)
+        per = {n: [e0.elapsed_time(e1) for e0, e1 in evs] for n, evs in self.events.items() if evs}
         tot = {n: sum(v) for n, v in per.items()}
+        total = sum(tot.values())
+        kernels = {}
+        for n in sorted(tot, key=lambda n: -tot[n]):
+            ms = float(np.mean(per[n]))
+            nbytes, flops = algorithmic_work(op, n, self.args[n])
+            entry = {"share": round(tot[n] / total, 4), "launches": len(per[n]), "mean_ms": round(ms, 4),
+                     "gbs": round(nbytes / (ms / 1e3) / 1e9, 1)}
+            if flops:
+                entry["tflops"] = round(flops / (ms / 1e3) / 1e12, 2)
+            kernels[n] = entry
         dom = max(tot, key=tot.get)
         ms = float(np.mean(per[dom]))
         nbytes, flops = algorithmic_work(op, dom, self.args[dom])
-        achieved = nbytes / (ms / 1e3) / 1e9
-        share = {n: round(t / sum(tot.values()), 4) for n, t in sorted(tot.items(), key=lambda t: -t[1])}
-        fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12          # FP32 FMA lanes x 2 flops x max SM clock (TFLOP/s)
-        return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
-                "mean_launch_ms": ms, "launches": len(per[dom]),
-                "fp32_tflops": flops / (ms / 1e3) / 1e12 if flops else None, "fp32_peak_tflops_nominal": fp32_peak,
-                "fp32_frac_of_nominal": (flops / (ms / 1e3) / 1e12) / fp32_peak if flops else None,
-                "time_share_of_timed_kernels": share}
+        if dom.startswith("dfx_pf_tc"):
+            achieved = flops / (ms / 1e3) / 1e12
+            out = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": tc, "unit": "TFLOP/s",
+                   "frac": achieved / tc, "peak_source": f"{src} bf16_tflops_sustained (of measured)"}
+        else:
+            achieved = nbytes / (ms / 1e3) / 1e9
+            out = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                   "frac": achieved / hbm, "peak_source": f"{src} hbm_gbs (of measured)"}
+            if flops:
+                out["fp32_tflops"] = flops / (ms / 1e3) / 1e12
+                out["fp32_frac_of_nominal"] = out["fp32_tflops"] / fp32_peak
+        out.update({"traffic": profiled_traffic(dom), "mean_launch_ms": ms, "launches": len(per[dom]),
+                    "kernels": kernels})
+        return out
+
+
+def profiled_traffic(kernel):
+    """DRAM bytes per launch of a kernel from the committed ncu summary of this workload (profiles/traffic.json),
+    or None when none was captured."""
+    f = ROOT / "profiles" / "traffic.json"
+    if not f.exists():
+        return None
+    return json.loads(f.read_text()).get(kernel, {}).get("dram_bytes_per_launch")
 
 
 def algorithmic_work(op, name, args_list):
     """(bytes, flops) per launch (mean over the recorded launches) of a kernel: its own inputs + outputs once, and the
-    multiply-adds of its non-zero taps / entries (an FMA = 2 flops)."""
+    multiply-adds of its non-zero taps / entries (an FMA = 2 flops); the tensor-core products count the dense
+    multiply-adds they perform."""
     nb, nf = [], []
     npix = op.Nx * op.Ny
+    My = op.My
     for args in args_list:
         if name in ("dfx_radon_forward", "dfx_radon_backward"):
             n_ang, kb = args[3], args[8]
-            nb.append(4 * kb * (npix + n_ang * op.My))
+            nb.append(4 * kb * (npix + n_ang * My))
             nf.append(2 * 2 * npix * n_ang * kb)            # ~2 taps per pixel and angle
+        elif name == "dfx_radon_forward_bf16":
+            n_ang, kb = args[4], args[9]
+            nb.append(4 * kb * npix + 2 * kb * n_ang * My)
+            nf.append(2 * 2 * npix * n_ang * kb)
+        elif name == "dfx_radon_backward_spdhg":
+            n_ang, kstride, kb = args[2], args[6], args[7]
+            nb.append(4 * kb * n_ang * My + 4 * 5 * npix * kstride)      # sino; x, z, T read; x, z written
+            nf.append(2 * 2 * npix * n_ang * kb)
+        elif name == "dfx_radon_backward_spdhg_bf16":
+            n_ang, kstride, kb = args[3], args[7], args[8]
+            nb.append(2 * kb * n_ang * My + 4 * 5 * npix * kstride)
+            nf.append(2 * 2 * npix * n_ang * kb)
         elif name in ("dfx_spmm_pf_forward", "dfx_spmm_pf_adjoint"):
             n_sub = args[6]
             kb = args[10] if name == "dfx_spmm_pf_forward" else args[8]
             frac = n_sub / op.N_Omega
             nnz = sum(sb["nnz"] for sb in op.sparse_batches) / len(op.sparse_batches) * frac
-            nb.append(4 * n_sub * op.My * (kb + 2 * op.N_seg) + 6 * nnz)
-            nf.append(2 * nnz * op.My)
+            nb.append(4 * n_sub * My * (kb + 2 * op.N_seg) + 6 * nnz)
+            nf.append(2 * nnz * My)
+        elif name == "dfx_pf_tc_forward":
+            kn, cp, cp_pad, n_sub, my, acc = args[3], args[4], args[5], args[9], args[10], args[12]
+            nb.append(2 * n_sub * kn * cp_pad + 2 * n_sub * my * kn + 4 * n_sub * my * cp * (2 if acc else 1))
+            nf.append(2 * n_sub * my * kn * cp)
+        elif name == "dfx_pf_tc_adjoint":
+            kn, cp, cp_pad, n_sub, my = args[3], args[4], args[5], args[9], args[10]
+            nb.append(2 * n_sub * kn * cp_pad + 2 * n_sub * my * cp_pad + 2 * n_sub * my * kn)
+            nf.append(2 * n_sub * my * kn * cp)
+        elif name == "dfx_rows_to_bf16":
+            n_sub, my, cp, cp_pad = args[3], args[4], args[5], args[6]
+            nb.append(n_sub * my * (4 * cp + 2 * cp_pad))
+            nf.append(0)
         elif name in ("dfx_gather_channels", "dfx_scatter_channels"):
             nb.append(2 * 4 * npix * args[4])
             nf.append(0)
-        elif name == "dfx_radon_backward_spdhg":
-            n_ang, kstride, kb = args[2], args[6], args[7]
-            nb.append(4 * kb * n_ang * op.My + 4 * 5 * npix * kstride)      # sino; x, z, T read; x, z written
-            nf.append(2 * 2 * npix * n_ang * kb)
         elif name == "dfx_spdhg_primal_update":
             nb.append(4 * 6 * args[6])
             nf.append(0)

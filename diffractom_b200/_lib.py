@@ -35,6 +35,9 @@ SIGNATURES = {
     "dfx_radon_forward": ([P, P, P, I, I, I, I, I, I, I, F, S], c_int),
     "dfx_radon_backward": ([P, P, P, I, I, I, I, I, I, I, I, S], c_int),
     "dfx_radon_backward_spdhg": ([P, P, I, I, I, I, I, I, I, I, P, P, P, F, F, S], c_int),
+    "dfx_radon_forward_bf16": ([P, P, L, P, I, I, I, I, I, I, I, F, S], c_int),
+    "dfx_radon_backward_bf16": ([P, L, P, P, I, I, I, I, I, I, I, I, S], c_int),
+    "dfx_radon_backward_spdhg_bf16": ([P, L, P, I, I, I, I, I, I, I, I, P, P, P, F, F, S], c_int),
     "dfx_batch_support": ([P, P, P, L, I, I, F, I, S], c_int),
     "dfx_pf_dense": ([POINTER(PFGeometry), I, I, P, S], c_int),
     "dfx_pf_csr_count": ([POINTER(PFGeometry), P, I, I, I, I, P, S], c_int),
@@ -69,8 +72,8 @@ SIGNATURES = {
     "dfx_copy_f32": ([P, P, L, S], c_int),
     "dfx_scale_f32": ([P, F, L, S], c_int),
     "dfx_pf_dense_bf16": ([POINTER(PFGeometry), I, I, L, L, I, P, S], c_int),
-    "dfx_pf_tc_forward": ([P, L, I, I, I, P, P, I, I, P, I, S], c_int),
-    "dfx_pf_tc_adjoint": ([P, L, I, I, I, P, P, I, I, F, P, S], c_int),
+    "dfx_pf_tc_forward": ([P, L, L, L, I, I, I, P, P, I, I, P, I, S], c_int),
+    "dfx_pf_tc_adjoint": ([P, L, L, L, I, I, I, P, P, I, I, F, P, S], c_int),
     "dfx_tc_status": ([POINTER(ctypes.c_uint), I], c_int),
     "dfx_rows_to_bf16": ([P, P, P, I, I, I, I, S], c_int),
 }

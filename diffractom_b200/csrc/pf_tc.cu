@@ -318,16 +318,17 @@ EncodeTiledFn encoder()
     return fn;
 }
 
-// 3-D BF16 tensor (d0 fastest) with a box of (b0, b1, 1), 128-byte swizzle, zero fill out of bounds.
-int make_map(CUtensorMap *map, const void *base, uint64_t d0, uint64_t d1, uint64_t d2, uint32_t b0, uint32_t b1,
-             const char *what)
+// 3-D BF16 tensor (d0 fastest; s1, s2 the element strides of dimensions 1 and 2) with a box of (b0, b1, 1),
+// 128-byte swizzle, zero fill out of bounds (so a view of rows k0 .. k0+kn-1 reads zeros past its last row).
+int make_map(CUtensorMap *map, const void *base, uint64_t d0, uint64_t d1, uint64_t d2, uint64_t s1, uint64_t s2,
+             uint32_t b0, uint32_t b1, const char *what)
 {
     EncodeTiledFn enc = encoder();
     DFX_REQUIRE(enc != nullptr, "pf_tc: cuTensorMapEncodeTiled is not available from the driver");
-    DFX_REQUIRE(((uintptr_t)base % 16) == 0 && (d0 * 2) % 16 == 0, "pf_tc: %s must be 16-byte aligned with rows of a "
-                "multiple of 8 elements", what);
+    DFX_REQUIRE(((uintptr_t)base % 16) == 0 && (s1 * 2) % 16 == 0 && (s2 * 2) % 16 == 0,
+                "pf_tc: %s must be 16-byte aligned with rows of a multiple of 8 elements", what);
     const cuuint64_t dims[3] = {d0, d1, d2};
-    const cuuint64_t strides[2] = {d0 * 2, d0 * d1 * 2};
+    const cuuint64_t strides[2] = {s1 * 2, s2 * 2};
     const cuuint32_t box[3] = {b0, b1, 1};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult rc = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void *>(base), dims, strides, box,
@@ -372,11 +373,14 @@ int launch(const CUtensorMap &ma, const CUtensorMap &mb, TcArgs a, int m_tiles, 
     return launch_status(DIR == 0 ? "pf_tc_forward" : "pf_tc_adjoint");
 }
 
-int check_common(const void *pf, int64_t ktot, int cp, int cp_pad, int n_sub, int my, int n_omega)
+int check_common(const void *pf, int64_t ktot, int64_t k0, int64_t kn, int cp, int cp_pad, int n_sub, int my,
+                 int n_omega)
 {
     DFX_REQUIRE(pf != nullptr, "pf_tc: null PF");
     DFX_REQUIRE(ktot > 0 && ktot % 8 == 0 && ktot <= 2147483647LL, "pf_tc: Ktot (%lld) must be a positive multiple "
                 "of 8", (long long)ktot);
+    DFX_REQUIRE(k0 >= 0 && k0 % 8 == 0 && kn > 0 && k0 + kn <= ktot, "pf_tc: orientation range %lld + %lld outside "
+                "Ktot %lld (start a multiple of 8)", (long long)k0, (long long)kn, (long long)ktot);
     DFX_REQUIRE(cp > 0 && cp_pad >= cp && cp_pad % 8 == 0, "pf_tc: CPpad (%d) must be a multiple of 8 >= CP (%d)",
                 cp_pad, cp);
     DFX_REQUIRE(n_sub > 0 && n_sub <= 65535 && n_omega > 0, "pf_tc: bad angle counts");
@@ -389,55 +393,64 @@ int check_common(const void *pf, int64_t ktot, int cp, int cp_pad, int n_sub, in
 
 using namespace dfx;
 
-extern "C" int dfx_pf_tc_forward(const void *pf_bf16, int64_t ktot, int cp, int cp_pad, int n_omega,
-                                 const void *z_bf16, const int32_t *omegas, int n_sub, int my, float *data,
+extern "C" int dfx_pf_tc_forward(const void *pf_bf16, int64_t ktot, int64_t k0, int64_t kn, int cp, int cp_pad,
+                                 int n_omega, const void *z_bf16, const int32_t *omegas, int n_sub, int my, float *data,
                                  int accumulate, void *stream)
 {
-    int st = check_common(pf_bf16, ktot, cp, cp_pad, n_sub, my, n_omega);
+    int st = check_common(pf_bf16, ktot, k0, kn, cp, cp_pad, n_sub, my, n_omega);
     if (st) return st;
     DFX_REQUIRE(z_bf16 && data, "pf_tc_forward: null pointer");
+    const __nv_bfloat16 *pf = reinterpret_cast<const __nv_bfloat16 *>(pf_bf16) + k0 * cp_pad;
+    const __nv_bfloat16 *z = reinterpret_cast<const __nv_bfloat16 *>(z_bf16) + k0;
     CUtensorMap ma, mb;
-    if ((st = make_map(&ma, pf_bf16, (uint64_t)cp_pad, (uint64_t)ktot, (uint64_t)n_omega, 64, 64, "PF"))) return st;
     TcArgs a{};
     a.omegas = omegas;
     a.n_sub = n_sub;
     a.m_extent = cp;
     a.n_extent = my;
     a.nt = n_tile(my);
-    a.k_chunks = (int)cdiv(ktot, TC_BK);
+    a.k_chunks = (int)cdiv(kn, TC_BK);
     a.stages = pick_stages(a.nt);
     a.out_f32 = data;
     a.out_ld = cp;
     a.alpha = 1.0f;
     a.accumulate = accumulate != 0;
-    if ((st = make_map(&mb, z_bf16, (uint64_t)ktot, (uint64_t)my, (uint64_t)n_sub, 64, (uint32_t)a.nt, "Z")))
+    if ((st = make_map(&ma, pf, (uint64_t)cp_pad, (uint64_t)kn, (uint64_t)n_omega, (uint64_t)cp_pad,
+                       (uint64_t)ktot * cp_pad, 64, 64, "PF")))
+        return st;
+    if ((st = make_map(&mb, z, (uint64_t)kn, (uint64_t)my, (uint64_t)n_sub, (uint64_t)ktot, (uint64_t)ktot * my, 64,
+                       (uint32_t)a.nt, "Z")))
         return st;
     return launch<0>(ma, mb, a, (int)cdiv(cp, TC_M), (cudaStream_t)stream);
 }
 
-extern "C" int dfx_pf_tc_adjoint(const void *pf_bf16, int64_t ktot, int cp, int cp_pad, int n_omega,
-                                 const void *d_bf16, const int32_t *omegas, int n_sub, int my, float alpha,
-                                 void *z_bf16, void *stream)
+extern "C" int dfx_pf_tc_adjoint(const void *pf_bf16, int64_t ktot, int64_t k0, int64_t kn, int cp, int cp_pad,
+                                 int n_omega, const void *d_bf16, const int32_t *omegas, int n_sub, int my,
+                                 float alpha, void *z_bf16, void *stream)
 {
-    int st = check_common(pf_bf16, ktot, cp, cp_pad, n_sub, my, n_omega);
+    int st = check_common(pf_bf16, ktot, k0, kn, cp, cp_pad, n_sub, my, n_omega);
     if (st) return st;
     DFX_REQUIRE(z_bf16 && d_bf16, "pf_tc_adjoint: null pointer");
+    const __nv_bfloat16 *pf = reinterpret_cast<const __nv_bfloat16 *>(pf_bf16) + k0 * cp_pad;
     CUtensorMap ma, mb;
-    if ((st = make_map(&ma, pf_bf16, (uint64_t)cp_pad, (uint64_t)ktot, (uint64_t)n_omega, 64, TC_M, "PF"))) return st;
     TcArgs a{};
     a.omegas = omegas;
     a.n_sub = n_sub;
-    a.m_extent = (int)ktot;
+    a.m_extent = (int)kn;
     a.n_extent = my;
     a.nt = n_tile(my);
     a.k_chunks = (int)cdiv(cp_pad, TC_BK);
     a.stages = pick_stages(a.nt);
-    a.out_bf16 = reinterpret_cast<__nv_bfloat16 *>(z_bf16);
+    a.out_bf16 = reinterpret_cast<__nv_bfloat16 *>(z_bf16) + k0;
     a.out_ld = ktot;
     a.alpha = alpha;
-    if ((st = make_map(&mb, d_bf16, (uint64_t)cp_pad, (uint64_t)my, (uint64_t)n_omega, 64, (uint32_t)a.nt, "D")))
+    if ((st = make_map(&ma, pf, (uint64_t)cp_pad, (uint64_t)kn, (uint64_t)n_omega, (uint64_t)cp_pad,
+                       (uint64_t)ktot * cp_pad, 64, TC_M, "PF")))
         return st;
-    return launch<1>(ma, mb, a, (int)cdiv(ktot, TC_M), (cudaStream_t)stream);
+    if ((st = make_map(&mb, d_bf16, (uint64_t)cp_pad, (uint64_t)my, (uint64_t)n_omega, (uint64_t)cp_pad,
+                       (uint64_t)cp_pad * my, 64, (uint32_t)a.nt, "D")))
+        return st;
+    return launch<1>(ma, mb, a, (int)cdiv(kn, TC_M), (cudaStream_t)stream);
 }
 
 extern "C" int dfx_tc_status(unsigned int *flags, int reset)

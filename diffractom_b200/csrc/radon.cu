@@ -15,6 +15,11 @@
 // Backward (pixel-driven, no atomics): a warp owns one pixel. The per-angle constants are computed once per block
 // into shared memory; per angle the warp evaluates the pixel's taps and reads 8 channels of each tap's sinogram bin
 // per lane. A fused variant applies SPDHG's primal step in the epilogue (no dz array).
+//
+// The sinogram is float32 or, in the BF16 precision path, BF16 with its own row stride (bins of all orientation
+// batches side by side): loads widen BF16 to float32 exactly, the forward rounds its float32 sums once on store.
+#include <cuda_bf16.h>
+
 #include "dfx_common.cuh"
 
 namespace dfx {
@@ -28,6 +33,34 @@ __device__ __forceinline__ void ld8(const float *p, float4 &a, float4 &b)
 {
     a = __ldg(reinterpret_cast<const float4 *>(p));
     b = __ldg(reinterpret_cast<const float4 *>(p) + 1);
+}
+
+__device__ __forceinline__ float bf_lo(uint32_t u) { return __uint_as_float(u << 16); }
+__device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 0xFFFF0000u); }
+
+__device__ __forceinline__ void ld8(const __nv_bfloat16 *p, float4 &a, float4 &b)
+{
+    const uint4 u = __ldg(reinterpret_cast<const uint4 *>(p));
+    a = make_float4(bf_lo(u.x), bf_hi(u.x), bf_lo(u.y), bf_hi(u.y));
+    b = make_float4(bf_lo(u.z), bf_hi(u.z), bf_lo(u.w), bf_hi(u.w));
+}
+
+__device__ __forceinline__ void st8(float *p, const float (&r)[CPL])
+{
+    reinterpret_cast<float4 *>(p)[0] = make_float4(r[0], r[1], r[2], r[3]);
+    reinterpret_cast<float4 *>(p)[1] = make_float4(r[4], r[5], r[6], r[7]);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+__device__ __forceinline__ void st8(__nv_bfloat16 *p, const float (&r)[CPL])
+{
+    *reinterpret_cast<uint4 *>(p) = make_uint4(pack_bf16(r[0], r[1]), pack_bf16(r[2], r[3]), pack_bf16(r[4], r[5]),
+                                               pack_bf16(r[6], r[7]));
 }
 
 __device__ __forceinline__ void acc8(float (&a)[CPL], float w, const float4 &p0, const float4 &p1)
@@ -59,10 +92,10 @@ __device__ __forceinline__ int first_tap(const AngleGeo &g, float t)
 }
 
 // ------------------------------------------------------------------------------------------------ forward
-template <int KERNEL>
+template <int KERNEL, typename ST>
 __global__ void __launch_bounds__(32 * WARPS) radon_forward_v3(
-    const float *__restrict__ img, float *__restrict__ sino, const float4 *__restrict__ geo, int nx, int ny, int ns,
-    int kstride, int kb, float scale, int n_taps)
+    const float *__restrict__ img, ST *__restrict__ sino, int64_t sld, const float4 *__restrict__ geo, int nx, int ny,
+    int ns, int kstride, int kb, float scale, int n_taps)
 {
     extern __shared__ __align__(16) float red[];          // [WARPS][NB_F][CPW] partial projections
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -134,9 +167,7 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_v3(
     float r[CPL] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
 #pragma unroll
     for (int q = 0; q < CPL; ++q) r[q] = (k + q < kb) ? __fmul_rn(scale, r[q]) : 0.0f;   // padding channels: 0
-    float4 *o = reinterpret_cast<float4 *>(sino + ((int64_t)a * ns + s0 + j) * kstride + k);
-    o[0] = make_float4(r[0], r[1], r[2], r[3]);
-    o[1] = make_float4(r[4], r[5], r[6], r[7]);
+    st8(sino + ((int64_t)a * ns + s0 + j) * sld + k, r);
 }
 
 // ------------------------------------------------------------------------------------------------ backward
@@ -151,9 +182,9 @@ __device__ __forceinline__ void primal_step(float &x, float &z, float t, float d
 
 // MODE 0: img (npix, kstride) = backprojection; MODE 1: the backprojection dz is applied to x, z (T the steps):
 // z += dz; x = T > 0 ? max(0, x - T (z + inv_p dz + lam)) : 0.
-template <int KERNEL, int MODE>
+template <int KERNEL, int MODE, typename ST>
 __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
-    const float *__restrict__ sino, float *__restrict__ img, const float4 *__restrict__ geo, int n_angles, int nx,
+    const ST *__restrict__ sino, int64_t sld, float *__restrict__ img, const float4 *__restrict__ geo, int n_angles, int nx,
     int ny, int ns, int kstride, int kb, int n_taps, float *__restrict__ z, const float *__restrict__ T, float inv_p,
     float lam)
 {
@@ -169,8 +200,8 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
     float acc[CPL];
 #pragma unroll
     for (int c = 0; c < CPL; ++c) acc[c] = 0.0f;
-    const float *col = sino + k;
-    const int64_t angle_stride = (int64_t)ns * kstride;
+    const ST *col = sino + k;
+    const int64_t angle_stride = (int64_t)ns * sld;
     for (int a = 0; a < n_angles; ++a, col += angle_stride) {
         const AngleGeo g = unpack_geo(prm[a]);
         const float t = __fmaf_rn(g.A, g.rows_are_y ? fx : fy, __fmaf_rn(g.B, g.rows_are_y ? fy : fx, g.T0));
@@ -180,8 +211,8 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
             const float w0 = __fmul_rn(g.w, tap_weight<KERNEL>(g, __fsub_rn(t, (float)sf)));
             const float w1 = __fmul_rn(g.w, tap_weight<KERNEL>(g, __fsub_rn(t, (float)(sf + 1))));
             float4 a0, a1, b0, b1;
-            ld8(col + (int64_t)sf * kstride, a0, a1);
-            ld8(col + (int64_t)(sf + 1) * kstride, b0, b1);
+            ld8(col + (int64_t)sf * sld, a0, a1);
+            ld8(col + (int64_t)(sf + 1) * sld, b0, b1);
             acc8(acc, w0, a0, a1);
             acc8(acc, w1, b0, b1);
             continue;
@@ -192,7 +223,7 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
             const float w = tap_weight<KERNEL>(g, __fsub_rn(t, (float)s));
             if (w == 0.0f) continue;
             float4 q0, q1;
-            ld8(col + (int64_t)s * kstride, q0, q1);
+            ld8(col + (int64_t)s * sld, q0, q1);
             acc8(acc, __fmul_rn(g.w, w), q0, q1);
         }
     }
@@ -314,8 +345,8 @@ static int allow_smem(Kernel kernel, size_t bytes)
     return DFX_OK;
 }
 
-template <int KERNEL, int MODE>
-static int launch_backward(const float *sino, float *img, const float *geo, int n_angles, int nx, int ny, int n_det,
+template <int KERNEL, int MODE, typename ST>
+static int launch_backward(const ST *sino, int64_t sld, float *img, const float *geo, int n_angles, int nx, int ny, int n_det,
                            int kstride, int kb, int n_taps, float *z, const float *T, float inv_p, float lam,
                            void *stream)
 {
@@ -324,10 +355,10 @@ static int launch_backward(const float *sino, float *img, const float *geo, int 
     DFX_REQUIRE(grid.x < 2147483647u && grid.y <= 65535u, "radon: batch too large for one launch");
     const size_t smem = sizeof(AngleParams) * (size_t)(n_angles > 0 ? n_angles : 1);
     DFX_REQUIRE(smem <= 200 * 1024, "radon: %d angles exceed the shared memory of one launch", n_angles);
-    int st = allow_smem(radon_backward_v3<KERNEL, MODE>, smem);
+    int st = allow_smem(radon_backward_v3<KERNEL, MODE, ST>, smem);
     if (st) return st;
-    radon_backward_v3<KERNEL, MODE><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
-        sino, img, reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, kstride, kb, n_taps, z, T, inv_p,
+    radon_backward_v3<KERNEL, MODE, ST><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
+        sino, sld, img, reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, kstride, kb, n_taps, z, T, inv_p,
         lam);
     return launch_status(MODE ? "radon_backward_spdhg" : "radon_backward");
 }
@@ -336,55 +367,95 @@ static int launch_backward(const float *sino, float *img, const float *geo, int 
 
 using namespace dfx;
 
-extern "C" int dfx_radon_forward(const float *img_k, float *sino_k, const float *geo, int n_angles, int nx, int ny,
-                                 int n_det, int kstride, int kb, int kernel, float scale, void *stream)
+template <typename ST>
+static int radon_forward_any(const float *img_k, ST *sino, int64_t sld, const float *geo, int n_angles, int nx, int ny,
+                             int n_det, int kstride, int kb, int kernel, float scale, void *stream)
 {
-    int st = check_radon_args(img_k, sino_k, geo, n_angles, nx, ny, n_det, kstride, kb, kernel);
+    int st = check_radon_args(img_k, sino, geo, n_angles, nx, ny, n_det, kstride, kb, kernel);
     if (st) return st;
+    DFX_REQUIRE(sld >= kstride && sld % CPL == 0, "radon: sinogram row stride (%lld) must be a multiple of %d >= "
+                "kstride", (long long)sld, CPL);
     if (n_angles == 0) return DFX_OK;
     DFX_REQUIRE(n_angles <= 65535, "radon: at most 65535 angles per launch");
     dim3 grid((unsigned)cdiv(n_det, NB_F), (unsigned)cdiv(kstride, CPW), (unsigned)n_angles);
     const size_t smem = sizeof(float) * WARPS * NB_F * CPW;      // 64 KB of partial projections
     const int max_taps = 64;                                      // per angle: ceil(1 + |A|)
     if (kernel == 1) {
-        if ((st = allow_smem(radon_forward_v3<1>, smem))) return st;
-        radon_forward_v3<1><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
-            img_k, sino_k, reinterpret_cast<const float4 *>(geo), nx, ny, n_det, kstride, kb, scale, max_taps);
+        if ((st = allow_smem(radon_forward_v3<1, ST>, smem))) return st;
+        radon_forward_v3<1, ST><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
+            img_k, sino, sld, reinterpret_cast<const float4 *>(geo), nx, ny, n_det, kstride, kb, scale, max_taps);
     } else {
-        if ((st = allow_smem(radon_forward_v3<0>, smem))) return st;
-        radon_forward_v3<0><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
-            img_k, sino_k, reinterpret_cast<const float4 *>(geo), nx, ny, n_det, kstride, kb, scale, max_taps);
+        if ((st = allow_smem(radon_forward_v3<0, ST>, smem))) return st;
+        radon_forward_v3<0, ST><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
+            img_k, sino, sld, reinterpret_cast<const float4 *>(geo), nx, ny, n_det, kstride, kb, scale, max_taps);
     }
     return launch_status("radon_forward");
+}
+
+template <int MODE, typename ST>
+static int radon_backward_any(const ST *sino, int64_t sld, float *img_k, const float *geo, int n_angles, int nx,
+                              int ny, int n_det, int kstride, int kb, int kernel, int n_taps, float *z_k,
+                              const float *T_k, float inv_p, float lam, void *stream)
+{
+    int st = check_radon_args(sino, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, kernel);
+    if (st) return st;
+    DFX_REQUIRE(sld >= kstride && sld % CPL == 0, "radon: sinogram row stride (%lld) must be a multiple of %d >= "
+                "kstride", (long long)sld, CPL);
+    DFX_REQUIRE(MODE == 0 || (z_k && T_k && ((uintptr_t)z_k % 16) == 0 && ((uintptr_t)T_k % 16) == 0),
+                "radon_backward_spdhg: z and T must be 16-byte aligned device arrays");
+    DFX_REQUIRE(n_taps >= 2 && n_taps <= 64, "radon: n_taps (%d) out of range", n_taps);
+    if (kernel == 1)
+        return launch_backward<1, MODE, ST>(sino, sld, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, n_taps, z_k,
+                                            T_k, inv_p, lam, stream);
+    return launch_backward<0, MODE, ST>(sino, sld, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, n_taps, z_k, T_k,
+                                        inv_p, lam, stream);
+}
+
+extern "C" int dfx_radon_forward(const float *img_k, float *sino_k, const float *geo, int n_angles, int nx, int ny,
+                                 int n_det, int kstride, int kb, int kernel, float scale, void *stream)
+{
+    return radon_forward_any(img_k, sino_k, (int64_t)kstride, geo, n_angles, nx, ny, n_det, kstride, kb, kernel,
+                             scale, stream);
+}
+
+extern "C" int dfx_radon_forward_bf16(const float *img_k, void *sino_bf16, int64_t sino_ld, const float *geo,
+                                      int n_angles, int nx, int ny, int n_det, int kstride, int kb, int kernel,
+                                      float scale, void *stream)
+{
+    return radon_forward_any(img_k, reinterpret_cast<__nv_bfloat16 *>(sino_bf16), sino_ld, geo, n_angles, nx, ny,
+                             n_det, kstride, kb, kernel, scale, stream);
 }
 
 extern "C" int dfx_radon_backward(const float *sino_k, float *img_k, const float *geo, int n_angles, int nx, int ny,
                                   int n_det, int kstride, int kb, int kernel, int n_taps, void *stream)
 {
-    int st = check_radon_args(sino_k, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, kernel);
-    if (st) return st;
-    DFX_REQUIRE(n_taps >= 2 && n_taps <= 64, "radon: n_taps (%d) out of range", n_taps);
-    if (kernel == 1)
-        return launch_backward<1, 0>(sino_k, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, n_taps, nullptr,
-                                     nullptr, 0.0f, 0.0f, stream);
-    return launch_backward<0, 0>(sino_k, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, n_taps, nullptr, nullptr,
-                                 0.0f, 0.0f, stream);
+    return radon_backward_any<0>(sino_k, (int64_t)kstride, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, kernel,
+                                 n_taps, nullptr, nullptr, 0.0f, 0.0f, stream);
+}
+
+extern "C" int dfx_radon_backward_bf16(const void *sino_bf16, int64_t sino_ld, float *img_k, const float *geo,
+                                       int n_angles, int nx, int ny, int n_det, int kstride, int kb, int kernel,
+                                       int n_taps, void *stream)
+{
+    return radon_backward_any<0>(reinterpret_cast<const __nv_bfloat16 *>(sino_bf16), sino_ld, img_k, geo, n_angles, nx,
+                                 ny, n_det, kstride, kb, kernel, n_taps, nullptr, nullptr, 0.0f, 0.0f, stream);
 }
 
 extern "C" int dfx_radon_backward_spdhg(const float *sino_k, const float *geo, int n_angles, int nx, int ny, int n_det,
                                         int kstride, int kb, int kernel, int n_taps, float *x_k, float *z_k,
                                         const float *T_k, float inv_p, float lam, void *stream)
 {
-    int st = check_radon_args(sino_k, x_k, geo, n_angles, nx, ny, n_det, kstride, kb, kernel);
-    if (st) return st;
-    DFX_REQUIRE(z_k && T_k && ((uintptr_t)z_k % 16) == 0 && ((uintptr_t)T_k % 16) == 0,
-                "radon_backward_spdhg: z and T must be 16-byte aligned device arrays");
-    DFX_REQUIRE(n_taps >= 2 && n_taps <= 64, "radon: n_taps (%d) out of range", n_taps);
-    if (kernel == 1)
-        return launch_backward<1, 1>(sino_k, x_k, geo, n_angles, nx, ny, n_det, kstride, kb, n_taps, z_k, T_k, inv_p,
-                                     lam, stream);
-    return launch_backward<0, 1>(sino_k, x_k, geo, n_angles, nx, ny, n_det, kstride, kb, n_taps, z_k, T_k, inv_p, lam,
-                                 stream);
+    return radon_backward_any<1>(sino_k, (int64_t)kstride, x_k, geo, n_angles, nx, ny, n_det, kstride, kb, kernel,
+                                 n_taps, z_k, T_k, inv_p, lam, stream);
+}
+
+extern "C" int dfx_radon_backward_spdhg_bf16(const void *sino_bf16, int64_t sino_ld, const float *geo, int n_angles,
+                                             int nx, int ny, int n_det, int kstride, int kb, int kernel, int n_taps,
+                                             float *x_k, float *z_k, const float *T_k, float inv_p, float lam,
+                                             void *stream)
+{
+    return radon_backward_any<1>(reinterpret_cast<const __nv_bfloat16 *>(sino_bf16), sino_ld, x_k, geo, n_angles, nx,
+                                 ny, n_det, kstride, kb, kernel, n_taps, z_k, T_k, inv_p, lam, stream);
 }
 
 extern "C" int dfx_batch_support(float *x_k, const float *colsum_k, const uint8_t *supp, int64_t npix, int kstride,

@@ -54,11 +54,17 @@ class SinglePhaseForwardOperator:
                  radon_kernel: str | None = None, fft_max_gb: float = 1.5, reserve_coefficient_arrays: int = 3,
                  pf_cutoff_sigma: float | None = 4.0, quadrature="auto", quadrature_tol: float = DEFAULT_TOL,
                  intensity_model=None, sparse_batch_max: int = SPARSE_BATCH_MAX, rings=None, ring_two_theta=None,
-                 reflection_two_theta: bool = False, window_parallax=None, ring_intensities=None, **kwargs):
+                 reflection_two_theta: bool = False, window_parallax=None, ring_intensities=None,
+                 precision: str = "fp32", **kwargs):
         """Arguments as diffractom's (SPFO:169-197). ctx: None, a torch.device or a CUDA device index (the GPU);
         queue: None (the current torch stream at every call) or a torch.cuda.Stream. ring_intensities: with
         normalized=False, the integrated intensity of every ring (diffractom computes them from structure factors,
         which this package does not model); fft_max_gb is accepted for compatibility.
+
+        precision: "fp32" (the reference's arithmetic) or "bf16": direct_cl / adjoint_cl on device tensors then run
+        the Radon output through BF16 and the pole-figure products on the tensor cores (dense BF16 PF of all
+        orientations, float32 accumulation); the float32 sparse PF stays available (the solvers use it for set-up
+        and for their once-per-epoch residual), NumPy (streamed) calls stay float32.
 
         Not provided (NotImplementedError): projector "fft" / "gratopy", pf_mode "dense" (the sparse products give
         the same operator), reflection_two_theta, window_parallax, custom rings with overlap weights other than 1."""
@@ -138,6 +144,12 @@ class SinglePhaseForwardOperator:
         self._pf_build = dict(mode=pf_mode, max_fill=sparse_max_fill, max_gb=sparse_max_gb,
                               max_fill_partial=sparse_max_fill_partial)
         self.build_sparse_pf(**self._pf_build)
+        if precision not in ("fp32", "bf16"):
+            raise ValueError(f"precision must be 'fp32' or 'bf16', not {precision!r}")
+        self.precision = precision
+        self.pf_bf16 = None
+        if precision == "bf16":
+            self.build_dense_bf16_pf()
 
     # ------------------------------------------------------------------ small helpers
     def stream(self) -> torch.cuda.Stream:
@@ -321,6 +333,133 @@ class SinglePhaseForwardOperator:
         self._csr(b["k_start"], b["K_batch"], forward, rows, row_ptr=rp, out=(self._gen_col, self._gen_val))
         return rp, self._gen_col, self._gen_val, compact
 
+    # ------------------------------------------------------------------ BF16 tensor-core path
+    def build_dense_bf16_pf(self, max_z_gb: float = 2.0):
+        """The dense BF16 PF of all orientation batches, (N_Omega, Ktot, CPpad) with batch ib at rows ib * Kstride
+        (padding rows and columns 0), and the BF16 work buffers of the tensor-core products: Z (angles, My, Ktot),
+        the Radon output of all batches side by side, for up to max_z_gb of angles at a time, and D's BF16 copy."""
+        R, CP = self.N_Omega, self.N_seg
+        self.Ktot = len(self.batches) * self.Kstride
+        self.cp_pad = -(-CP // 8) * 8
+        nbytes = 2 * R * self.Ktot * self.cp_pad
+        free, _ = torch.cuda.mem_get_info(self.device)
+        if nbytes > 0.9 * free:
+            raise MemoryError(f"dense BF16 PF of {nbytes / 1024 ** 3:.1f} GB does not fit in the free device memory "
+                              f"({free / 1024 ** 3:.1f} GB)")
+        t0 = time.perf_counter()
+        self.pf_bf16 = torch.zeros((R, self.Ktot, self.cp_pad), dtype=torch.bfloat16, device=self.device)
+        for ib, b in enumerate(self.batches):
+            self._call("dfx_pf_dense_bf16", ctypes.byref(self._pfg), b["k_start"], b["K_batch"], ib * self.Kstride,
+                       self.Ktot, self.cp_pad, self.pf_bf16.data_ptr(), self._s())
+        self._d_bf16 = torch.zeros((R, self.My, self.cp_pad), dtype=torch.bfloat16, device=self.device)
+        self._z_bf16 = torch.empty(0, dtype=torch.bfloat16, device=self.device)
+        per_angle = 2 * self.My * self.Ktot
+        self._bf16_chunk = max(1, min(R, int(max_z_gb * 1024 ** 3 // per_angle)))
+        self._all_omegas = torch.arange(R, dtype=torch.int32, device=self.device)
+        self.pf_bf16_setup_s = time.perf_counter() - t0
+
+    def _z(self, n):
+        """The BF16 Radon output buffer for n angles, (n, My, Ktot)."""
+        need = n * self.My * self.Ktot
+        if self._z_bf16.numel() < need:
+            self._z_bf16 = torch.empty(need, dtype=torch.bfloat16, device=self.device)
+        return self._z_bf16[:need].view(n, self.My, self.Ktot)
+
+    def _bf16_chunks(self, subset):
+        """(geo, n, omegas) pieces of the angles of subset m (or of all angles), each at most the Z buffer's size."""
+        if subset is None:
+            geo, om = self.geo_gpu, self._all_omegas
+        else:
+            e = self._sub[self._subset(subset)]
+            geo, om = e["geo"], e["omegas"]
+        n = om.numel()
+        c = max(self._bf16_chunk, self._max_subset()) if subset is not None else self._bf16_chunk
+        return [(geo[a:a + c], min(c, n - a), om[a:a + c]) for a in range(0, n, c)]
+
+    def _max_subset(self):
+        return max((e["n"] for e in self._sub), default=1)
+
+    def _radon_forward_bf16(self, src_ptr, ib, z, geo, n):
+        """Radon transform of channel-fastest batch ib (float32 at src_ptr) into its columns of Z (BF16)."""
+        self._call("dfx_radon_forward_bf16", src_ptr, z.data_ptr() + 2 * ib * self.Kstride, self.Ktot,
+                   geo.data_ptr(), n, self.Nx, self.Ny, self.My, self.Kstride, self.batches[ib]["K_batch"],
+                   self._kernel_id, float(self.radon_geo.scale), self._s())
+
+    def _pf_tc_forward(self, z, om, n, data, k0=0, kn=None, accumulate=0):
+        self._call("dfx_pf_tc_forward", self.pf_bf16.data_ptr(), self.Ktot, k0, self.Ktot if kn is None else kn,
+                   self.N_seg, self.cp_pad, self.N_Omega, z.data_ptr(), om.data_ptr(), n, self.My, data.data_ptr(),
+                   accumulate, self._s())
+
+    def _pf_tc_adjoint(self, om, n, z, k0=0, kn=None):
+        """Z = alpha PF^T D for the angles om (D's BF16 copy must hold their rows)."""
+        alpha = float(np.float32(self.N_Omega / np.pi))
+        self._call("dfx_pf_tc_adjoint", self.pf_bf16.data_ptr(), self.Ktot, k0, self.Ktot if kn is None else kn,
+                   self.N_seg, self.cp_pad, self.N_Omega, self._d_bf16.data_ptr(), om.data_ptr(), n, self.My, alpha,
+                   z.data_ptr(), self._s())
+
+    def _rows_to_bf16(self, data, om, n):
+        self._call("dfx_rows_to_bf16", data.data_ptr(), self._d_bf16.data_ptr(), om.data_ptr(), n, self.My,
+                   self.N_seg, self.cp_pad, self._s())
+
+    def _direct_bf16(self, coeffs, data, subset):
+        for geo, n, om in self._bf16_chunks(subset):
+            z = self._z(n)
+            for ib, b in enumerate(self.batches):
+                self._call("dfx_gather_channels", coeffs.data_ptr(), self._img_k.data_ptr(), self.npix, b["k_start"],
+                           b["K_batch"], self.Kstride, self._s())
+                self._radon_forward_bf16(self._img_k.data_ptr(), ib, z, geo, n)
+            self._pf_tc_forward(z, om, n, data)
+
+    def _adjoint_bf16(self, data, coeffs, subset):
+        chunks = self._bf16_chunks(subset)
+        for geo, n, om in chunks:
+            self._rows_to_bf16(data, om, n)
+        for ib, b in enumerate(self.batches):
+            k0, kb = ib * self.Kstride, b["K_batch"]
+            for ic, (geo, n, om) in enumerate(chunks):
+                z = self._z(n)
+                self._pf_tc_adjoint(om, n, z, k0, self.Kstride)
+                # over several angle chunks the backprojections of the chunks are summed in the batch buffer
+                dst = self._img_k if ic == 0 else self._img_acc()
+                self._call("dfx_radon_backward_bf16", z.data_ptr() + 2 * k0, self.Ktot, dst.data_ptr(),
+                           geo.data_ptr(), n, self.Nx, self.Ny, self.My, self.Kstride, kb, self._kernel_id,
+                           int(self.radon_geo.n_taps), self._s())
+                if ic > 0:
+                    with torch.cuda.stream(self.stream()):
+                        self._img_k.add_(dst)
+            self._call("dfx_scatter_channels", self._img_k.data_ptr(), coeffs.data_ptr(), self.npix, b["k_start"],
+                       kb, self.Kstride, self._s())
+
+    def _img_acc(self):
+        if getattr(self, "_img_k2", None) is None:
+            self._img_k2 = torch.empty_like(self._img_k)
+        return self._img_k2
+
+    # ---- BF16 SPDHG pass pieces (channel-fastest batches)
+    def _bf16_adjoint_sino(self, data, subset):
+        """Z = alpha PF^T data for the angles of subset m, all batches (one tensor-core launch); returns (geo, n, z)."""
+        e = self._sub[self._subset(subset)]
+        z = self._z(e["n"])
+        self._rows_to_bf16(data, e["omegas"], e["n"])
+        self._pf_tc_adjoint(e["omegas"], e["n"], z)
+        return e["geo"], e["n"], z
+
+    def _bf16_update_batch(self, ib, geo, n, z, x_ptr, z_ptr, T_ptr, inv_p, lam):
+        """SPDHG's update of batch ib from its columns of Z: the backprojection with the primal step fused."""
+        self._call("dfx_radon_backward_spdhg_bf16", z.data_ptr() + 2 * ib * self.Kstride, self.Ktot, geo.data_ptr(),
+                   n, self.Nx, self.Ny, self.My, self.Kstride, self.batches[ib]["K_batch"], self._kernel_id,
+                   int(self.radon_geo.n_taps), x_ptr, z_ptr, T_ptr, float(inv_p), float(lam), self._s())
+
+    def _bf16_forward_sino(self, subset, ib, src_ptr):
+        """Radon transform of batch ib (channel-fastest at src_ptr) for the angles of subset m into Z."""
+        e = self._sub[self._subset(subset)]
+        self._radon_forward_bf16(src_ptr, ib, self._z(e["n"]), e["geo"], e["n"])
+
+    def _bf16_forward_rows(self, subset, data):
+        """data rows of subset m = PF Z over all orientations (the rows are overwritten)."""
+        e = self._sub[self._subset(subset)]
+        self._pf_tc_forward(self._z(e["n"]), e["omegas"], e["n"], data)
+
     # ------------------------------------------------------------------ omega subsets
     def set_omega_subsets(self, subsets):
         """Subsets of the rotation angles for the subset forms direct_cl / adjoint_cl(subset=m) (SPFO:1541-1599):
@@ -383,6 +522,9 @@ class SinglePhaseForwardOperator:
         of subset m are written (the other rows are left as they are)."""
         check_device(coeffs, self.coeff_shape, "coeffs")
         check_device(data, self.data_shape, "data")
+        if self.precision == "bf16":
+            self._direct_bf16(coeffs, data, subset)
+            return
         if subset is None:
             self._fill(data, 0.0)
         else:
@@ -414,6 +556,9 @@ class SinglePhaseForwardOperator:
         """In-place adjoint coeffs = A^T data (SPFO:1800-1817); subset=m: A_m^T (rows of subset m only)."""
         check_device(data, self.data_shape, "data")
         check_device(coeffs, self.coeff_shape, "coeffs")
+        if self.precision == "bf16":
+            self._adjoint_bf16(data, coeffs, subset)
+            return
         for ib, b in enumerate(self.batches):
             self._adjoint_batch(data, ib, coeffs, b["k_start"], self.K, subset)
 
@@ -543,7 +688,8 @@ class SinglePhaseForwardOperator:
             n += t.numel() * t.element_size()
         for sb in self.sparse_batches or []:
             n += sum(v.numel() * v.element_size() for v in sb.values() if isinstance(v, torch.Tensor))
-        for t in (getattr(self, "_gen_col", None), getattr(self, "_gen_val", None)):
+        for t in (getattr(self, "_gen_col", None), getattr(self, "_gen_val", None), self.pf_bf16,
+                  getattr(self, "_d_bf16", None), getattr(self, "_z_bf16", None), getattr(self, "_img_k2", None)):
             if t is not None:
                 n += t.numel() * t.element_size()
         return n
@@ -560,6 +706,7 @@ class SinglePhaseForwardOperator:
         self.sparse_batches = None
         self.coeffs_sino_C = self._img_k = None
         self._gen_col = self._gen_val = None
+        self.pf_bf16 = self._d_bf16 = self._z_bf16 = self._img_k2 = None
         self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
         torch.cuda.synchronize(self.device)
 

@@ -86,6 +86,9 @@ class SPDHGPoisson:
         of the new x for subset fwd ("full": all rows) added to D (spdhg_poisson.py:430-484)."""
         op = self.op
         be = op.batch_elems()
+        if op.precision == "bf16" and fwd != "full":
+            self._pass_bf16(adj, fwd)
+            return
         sub = None if fwd == "full" else fwd
         for ib in range(len(op.batches)):
             off = 4 * ib * be
@@ -94,6 +97,25 @@ class SPDHGPoisson:
                                          self.Tk.data_ptr() + off, self._inv_p_data, self.lam)
             if fwd is not None:
                 op._direct_batch_k(self.xk.data_ptr() + off, ib, self.D, sub)
+
+    def _pass_bf16(self, adj, fwd):
+        """The pass of an operator with precision "bf16": one tensor-core launch takes the dual change of subset adj
+        to the BF16 Radon output of all batches, each batch's backprojection applies the primal step and projects the
+        new x for subset fwd into its columns of that output, and one tensor-core launch overwrites subset fwd's data
+        rows. Full forward passes (the residual of the diagnostics) stay float32."""
+        op = self.op
+        be = op.batch_elems()
+        if adj is not None:
+            geo, n, zb = op._bf16_adjoint_sino(self.D, adj)
+        for ib in range(len(op.batches)):
+            off = 4 * ib * be
+            if adj is not None:
+                op._bf16_update_batch(ib, geo, n, zb, self.xk.data_ptr() + off, self.zk.data_ptr() + off,
+                                      self.Tk.data_ptr() + off, self._inv_p_data, self.lam)
+            if fwd is not None:
+                op._bf16_forward_sino(fwd, ib, self.xk.data_ptr() + off)
+        if fwd is not None:
+            op._bf16_forward_rows(fwd, self.D)
 
     def _deviance(self, mu):
         return self.red.deviance(mu, self.b, self.w, self.pw, self.g, self.pg, self.bg, self.pbg, self.eps_counts)

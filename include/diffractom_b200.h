@@ -71,6 +71,18 @@ int dfx_radon_backward_spdhg(const float *sino_k, const float *geo, int n_angles
                              int kstride, int kb, int kernel, int n_taps, float *x_k, float *z_k, const float *T_k,
                              float inv_p, float lam, void *stream);
 
+/* The three Radon entry points above for the BF16 precision path: the sinogram is BF16 with sino_ld elements between
+ * consecutive bins (sino_ld >= kstride, a multiple of 8: the batches of all orientations side by side, the layout of
+ * the Z operand of dfx_pf_tc_forward / dfx_pf_tc_adjoint). The forward accumulates in float32 and rounds to BF16 on
+ * store; the backward widens BF16 exactly and accumulates in float32. Same references as above. */
+int dfx_radon_forward_bf16(const float *img_k, void *sino_bf16, int64_t sino_ld, const float *geo, int n_angles,
+                           int nx, int ny, int n_det, int kstride, int kb, int kernel, float scale, void *stream);
+int dfx_radon_backward_bf16(const void *sino_bf16, int64_t sino_ld, float *img_k, const float *geo, int n_angles,
+                            int nx, int ny, int n_det, int kstride, int kb, int kernel, int n_taps, void *stream);
+int dfx_radon_backward_spdhg_bf16(const void *sino_bf16, int64_t sino_ld, const float *geo, int n_angles, int nx,
+                                  int ny, int n_det, int kstride, int kb, int kernel, int n_taps, float *x_k,
+                                  float *z_k, const float *T_k, float inv_p, float lam, void *stream);
+
 /* replaces support_ones / project_support / tmin (fista_poisson.py:256-263, 277-281; spdhg_poisson.py:259-265) on a
  * channel-fastest batch (npix, kstride) with padding channels kb .. kstride-1 (supp (npix) uint8 or NULL):
  * mode 0: x = 1 on live channels of support pixels, else 0; mode 1: x = 0 outside them or where negative;
@@ -210,16 +222,19 @@ int dfx_pf_dense_bf16(const dfx_pf_geometry *g, int k0, int kb, int64_t koff, in
                       void *stream);
 
 /* replaces batched_gemm_clblast (SPFO:2063-2098) and, in the BF16 path, spmm_pf_forward_c (pf_kernels.cl:597-641):
- * for the n_sub angles r = omegas[s] (omegas NULL: r = s), data[r, y, j] (+)= sum_k PF[r, k, j] Z[s, y, k] over all
- * ktot orientations, with tcgen05 BF16 MMAs and float32 accumulation. pf_bf16 (n_omega, ktot, cp_pad), z_bf16
- * (n_sub, my, ktot) BF16, data (n_omega, my, cp) float32; accumulate = 0 overwrites the rows. ktot and cp_pad
- * multiples of 8, both BF16 arrays 16-byte aligned. */
-int dfx_pf_tc_forward(const void *pf_bf16, int64_t ktot, int cp, int cp_pad, int n_omega, const void *z_bf16,
-                      const int32_t *omegas, int n_sub, int my, float *data, int accumulate, void *stream);
+ * for the n_sub angles r = omegas[s] (omegas NULL: r = s), data[r, y, j] (+)= sum_k PF[r, k, j] Z[s, y, k] over the
+ * orientations k = k0 .. k0+kn-1 of the ktot, with tcgen05 BF16 MMAs and float32 accumulation. pf_bf16 (n_omega,
+ * ktot, cp_pad), z_bf16 (n_sub, my, ktot) BF16, data (n_omega, my, cp) float32; accumulate = 0 overwrites the rows.
+ * ktot, k0 and cp_pad multiples of 8, both BF16 arrays 16-byte aligned. */
+int dfx_pf_tc_forward(const void *pf_bf16, int64_t ktot, int64_t k0, int64_t kn, int cp, int cp_pad, int n_omega,
+                      const void *z_bf16, const int32_t *omegas, int n_sub, int my, float *data, int accumulate,
+                      void *stream);
 /* replaces batched_gemm_clblast_adj (SPFO:2100-2127) and, in the BF16 path, spmm_pf_adjoint_c (pf_kernels.cl:644-687):
- * Z[s, y, k] = alpha sum_j PF[r, k, j] D[r, y, j] (BF16 out, float32 accumulation), d_bf16 (n_omega, my, cp_pad). */
-int dfx_pf_tc_adjoint(const void *pf_bf16, int64_t ktot, int cp, int cp_pad, int n_omega, const void *d_bf16,
-                      const int32_t *omegas, int n_sub, int my, float alpha, void *z_bf16, void *stream);
+ * Z[s, y, k] = alpha sum_j PF[r, k, j] D[r, y, j] for k = k0 .. k0+kn-1 (BF16 out, float32 accumulation), d_bf16
+ * (n_omega, my, cp_pad); the other orientations of Z are left as they are. */
+int dfx_pf_tc_adjoint(const void *pf_bf16, int64_t ktot, int64_t k0, int64_t kn, int cp, int cp_pad, int n_omega,
+                      const void *d_bf16, const int32_t *omegas, int n_sub, int my, float alpha, void *z_bf16,
+                      void *stream);
 /* Bits of device-side waits of the tensor-core kernels that ran out since the last reset (DFX_TC_TIMEOUT); the
  * kernels return early on expiry and leave their outputs undefined. Synchronous; no reference counterpart. */
 #define DFX_TC_TIMEOUT 1u

@@ -1,0 +1,97 @@
+"""The BF16 tensor-core precision path of the operator and of SPDHGPoisson against the float64 oracle: operator
+values within the BF16 bound, subset rows, angle-chunked products, and the SPDHG deviance within 1e-3 relative of
+the float64 run of the same loop (same subsets, schedule and step sizes)."""
+import numpy as np
+import pytest
+
+from conftest import case_inputs
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+# BF16 operands (8-bit significands) with float32 accumulation: the operator's values stay within a few 2^-9 of the
+# largest value; this bound is checked, not assumed
+OP_TOL = 1e-2
+DEV_TOL = 1e-3
+
+
+def make_operator(d, **kw):
+    from diffractom_b200 import SinglePhaseForwardOperator
+    cfg, mat, grid = case_inputs(d)
+    kw.setdefault("max_gb", 1e-5)
+    return SinglePhaseForwardOperator(cfg, mat, grid, normalized=True, quadrature=d["quadrature"],
+                                      radon_kernel=d["kernel"], **kw)
+
+
+def rel(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - b).max() / np.abs(b).max())
+
+
+@pytest.mark.parametrize("name", ["al5_small", "ti8_small", "adj_0_360"])
+def test_bf16_operator_matches_oracle(golden, name):
+    from oracle.oracle import OracleOperator
+    d = golden(name)
+    op = make_operator(d, precision="bf16")
+    assert op.precision == "bf16" and len(op.batches) > 1
+    orc = OracleOperator.from_operator(op, precision="f64")
+    c = torch.as_tensor(d["c"], device="cuda")
+    r = torch.as_tensor(d["r"], device="cuda")
+    fwd = op.direct(c).cpu().numpy()
+    adj = op.adjoint(r).cpu().numpy()
+    ef, ea = rel(fwd, orc.forward(d["c"])), rel(adj, orc.adjoint(d["r"]))
+    assert ef < OP_TOL and ea < OP_TOL, (ef, ea)
+    # the float32 operator of the same object is untouched by the precision switch
+    op.precision = "fp32"
+    assert rel(op.direct(c).cpu().numpy(), orc.forward(d["c"])) < 1e-5
+
+
+def test_bf16_subsets_and_angle_chunks(golden):
+    d = golden("adj_0_360")
+    op = make_operator(d, precision="bf16")
+    R = op.N_Omega
+    subs = op.set_omega_subsets(4)
+    rng = np.random.default_rng(2)
+    x = torch.as_tensor((rng.random(op.coeff_shape) * op.support_mask()[None]).astype(np.float32), device="cuda")
+    y = torch.as_tensor(rng.random(op.data_shape).astype(np.float32), device="cuda")
+    full = op.direct(x)
+    adj = op.adjoint(y)
+    for m, s in enumerate(subs):
+        dd = torch.full(op.data_shape, -7.0, device="cuda")
+        op.direct_cl(x, dd, subset=m)
+        sel = torch.as_tensor(s, device="cuda")
+        assert torch.equal(dd[sel], full[sel])                      # same tensor-core sums row by row
+        rest = torch.as_tensor(np.setdiff1d(np.arange(R), s), device="cuda")
+        assert torch.all(dd[rest] == -7.0)
+    # angles in several chunks of the Z buffer: the same rows, and the backprojections summed over the chunks
+    op.build_dense_bf16_pf(max_z_gb=3 * 2 * op.My * op.Ktot / 1024 ** 3)
+    assert op._bf16_chunk == 3 < R
+    assert torch.equal(op.direct(x), full)
+    a2 = op.adjoint(y)
+    assert rel(a2.cpu().numpy(), adj.cpu().numpy().astype(np.float64)) < 1e-5
+
+
+def test_bf16_spdhg_deviance_within_1e3_of_float64(golden):
+    from diffractom_b200 import SinglePhaseForwardOperator, SPDHGPoisson
+    from oracle.oracle import OracleOperator, spdhg_reference
+    d = golden("al5_small")
+    cfg, mat, grid = case_inputs(d)
+    op = SinglePhaseForwardOperator(cfg, mat, grid, 1e-5, normalized=True, quadrature=d["quadrature"],
+                                    precision="bf16")
+    rng = np.random.default_rng(11)
+    x_true = (rng.random(op.coeff_shape) * (rng.random(op.coeff_shape) < 0.2) * op.support_mask()[None]
+              ).astype(np.float32)
+    op.precision = "fp32"
+    b = rng.poisson(op.direct(x_true) * 50).astype(np.float32)
+    op.precision = "bf16"
+    n_ep = 6
+    sp = SPDHGPoisson(op, subsets=3, seed=1)
+    x = sp.run(torch.zeros(op.coeff_shape, device="cuda"), b, n_ep, diagnostics_interval=n_ep).cpu().numpy()
+    f_bf16 = sp.iter_stats[-1]["f"]
+    orc = OracleOperator.from_operator(op, precision="f64")
+    xr, yr, zr, devs, rho = spdhg_reference(orc, op.omega_subsets, b, n_ep, support=op.support_mask(), seed=1,
+                                            diagnostics_interval=n_ep)
+    f64 = devs[-1]
+    dev_err = abs(f_bf16 - f64) / f64
+    coef_err = float(np.linalg.norm(x - xr) / np.linalg.norm(xr))
+    assert dev_err <= DEV_TOL, (dev_err, coef_err)
+    assert coef_err < 5e-2, coef_err

@@ -43,26 +43,39 @@ def test_pf_tc_products_match_fp32_gemm(my):
     tc_flags()
     s = torch.cuda.current_stream().cuda_stream
     data = torch.full((R, my, CP), 7.0, device="cuda")
-    lib.call("dfx_pf_tc_forward", pf.data_ptr(), ktot, CP, cp_pad, R, z.data_ptr(), omegas.data_ptr(), n_sub, my,
-             data.data_ptr(), 0, s)
+    lib.call("dfx_pf_tc_forward", pf.data_ptr(), ktot, 0, ktot, CP, cp_pad, R, z.data_ptr(), omegas.data_ptr(),
+             n_sub, my, data.data_ptr(), 0, s)
     ref = torch.stack([z[i].float() @ pf[int(r), :, :CP].float() for i, r in enumerate(omegas.tolist())])
     got = data[omegas.long()]
     assert float((got - ref).abs().max() / ref.abs().max()) < 1e-5
     assert torch.all(data[[1, 2]] == 7.0)
-    lib.call("dfx_pf_tc_forward", pf.data_ptr(), ktot, CP, cp_pad, R, z.data_ptr(), omegas.data_ptr(), n_sub, my,
-             data.data_ptr(), 1, s)
+    lib.call("dfx_pf_tc_forward", pf.data_ptr(), ktot, 0, ktot, CP, cp_pad, R, z.data_ptr(), omegas.data_ptr(),
+             n_sub, my, data.data_ptr(), 1, s)
     assert float((data[omegas.long()] - 2 * ref).abs().max() / ref.abs().max()) < 1e-5
+    # a range of orientations (one batch of a wider Z): rows k0 .. k0+kn-1 only, nothing read past them
+    k0, kn = 104, 200
+    lib.call("dfx_pf_tc_forward", pf.data_ptr(), ktot, k0, kn, CP, cp_pad, R, z.data_ptr(), omegas.data_ptr(),
+             n_sub, my, data.data_ptr(), 0, s)
+    ref = torch.stack([z[i, :, k0:k0 + kn].float() @ pf[int(r), k0:k0 + kn, :CP].float()
+                       for i, r in enumerate(omegas.tolist())])
+    assert float((data[omegas.long()] - ref).abs().max() / ref.abs().max()) < 1e-5
 
     d = rand_bf16((R, my, cp_pad), gen)
     d[:, :, CP:] = 0
     zo = torch.zeros((n_sub, my, ktot), dtype=torch.bfloat16, device="cuda")
     alpha = 57.29
-    lib.call("dfx_pf_tc_adjoint", pf.data_ptr(), ktot, CP, cp_pad, R, d.data_ptr(), omegas.data_ptr(), n_sub, my,
-             alpha, zo.data_ptr(), s)
+    lib.call("dfx_pf_tc_adjoint", pf.data_ptr(), ktot, 0, ktot, CP, cp_pad, R, d.data_ptr(), omegas.data_ptr(),
+             n_sub, my, alpha, zo.data_ptr(), s)
     ref = torch.stack([alpha * (d[int(r)].float() @ pf[int(r)].float().T) for r in omegas.tolist()])
     # the output is rounded to BF16 once: within half a BF16 ulp of the float32 value (2^-9 relative)
     err = (zo.float() - ref).abs()
     assert bool(torch.all(err <= ref.abs() * 2.0 ** -8 + 1e-6 * float(ref.abs().max())))
+    zo.fill_(3.0)
+    lib.call("dfx_pf_tc_adjoint", pf.data_ptr(), ktot, k0, kn, CP, cp_pad, R, d.data_ptr(), omegas.data_ptr(),
+             n_sub, my, alpha, zo.data_ptr(), s)
+    err = (zo[:, :, k0:k0 + kn].float() - ref[:, :, k0:k0 + kn]).abs()
+    assert bool(torch.all(err <= ref[:, :, k0:k0 + kn].abs() * 2.0 ** -8 + 1e-6 * float(ref.abs().max())))
+    assert torch.all(zo[:, :, :k0] == 3.0) and torch.all(zo[:, :, k0 + kn:] == 3.0)
     torch.cuda.synchronize()
     assert tc_flags() == 0
 
@@ -89,9 +102,17 @@ def test_tc_argument_errors():
     data = torch.zeros((2, 3, 16), device="cuda")
     s = torch.cuda.current_stream().cuda_stream
     with pytest.raises(ValueError):      # Ktot not a multiple of 8
-        lib.call("dfx_pf_tc_forward", pf.data_ptr(), 12, 16, 16, 2, z.data_ptr(), None, 2, 3, data.data_ptr(), 0, s)
-    with pytest.raises(ValueError):      # cp_pad < cp
-        lib.call("dfx_pf_tc_forward", pf.data_ptr(), 16, 16, 8, 2, z.data_ptr(), None, 2, 3, data.data_ptr(), 0, s)
-    with pytest.raises(ValueError):      # misaligned operand
-        lib.call("dfx_pf_tc_forward", pf.data_ptr() + 2, 16, 16, 16, 2, z.data_ptr(), None, 2, 3, data.data_ptr(),
+        lib.call("dfx_pf_tc_forward", pf.data_ptr(), 12, 0, 12, 16, 16, 2, z.data_ptr(), None, 2, 3, data.data_ptr(),
                  0, s)
+    with pytest.raises(ValueError):      # cp_pad < cp
+        lib.call("dfx_pf_tc_forward", pf.data_ptr(), 16, 0, 16, 16, 8, 2, z.data_ptr(), None, 2, 3, data.data_ptr(),
+                 0, s)
+    with pytest.raises(ValueError):      # orientation range start not a multiple of 8 / past Ktot
+        lib.call("dfx_pf_tc_forward", pf.data_ptr(), 16, 4, 8, 16, 16, 2, z.data_ptr(), None, 2, 3, data.data_ptr(),
+                 0, s)
+    with pytest.raises(ValueError):
+        lib.call("dfx_pf_tc_forward", pf.data_ptr(), 16, 8, 16, 16, 16, 2, z.data_ptr(), None, 2, 3, data.data_ptr(),
+                 0, s)
+    with pytest.raises(ValueError):      # misaligned operand
+        lib.call("dfx_pf_tc_forward", pf.data_ptr() + 2, 16, 0, 16, 16, 16, 2, z.data_ptr(), None, 2, 3,
+                 data.data_ptr(), 0, s)
