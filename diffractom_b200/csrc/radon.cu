@@ -6,11 +6,9 @@
 // geometry only (detector coordinate, tap bins and weights) is the same for the whole warp: one warp instruction
 // serves 256 channels, and a zero weight skips its FMAs with a branch all lanes take.
 //
-// Forward (ray-driven, no atomics): a block owns NB_F bins of one angle and 256 channels; its 8 warps split the image
-// rows (warp w takes rows w, w + 8, ...), each accumulating all NB_F bins in registers, and sum their partial
-// projections through shared memory in a fixed order at the end (deterministic). Per row a warp walks the pixels
-// whose footprint reaches the block's bins; a pixel's non-zero taps go to their bin's accumulator through a switch
-// on the warp-uniform bin offset.
+// Forward (ray-driven gather, no atomics): a warp owns one bin of one angle; per image row it reads the two to four
+// pixels whose footprint reaches the bin. The grid is ordered so that one channel block of the image stays in L2
+// while all angles and bins of the launch read it.
 //
 // Backward (pixel-driven, no atomics): a warp owns one pixel. The per-angle constants are computed once per block
 // into shared memory; per angle the warp evaluates the pixel's taps and reads 8 channels of each tap's sinogram bin
@@ -27,7 +25,6 @@ namespace dfx {
 constexpr int WARPS = 8;        // warps per block
 constexpr int CPL = 8;          // channels per lane
 constexpr int CPW = 32 * CPL;   // channels per warp
-constexpr int NB_F = 8;         // bins per forward block
 
 __device__ __forceinline__ void ld8(const float *p, float4 &a, float4 &b)
 {
@@ -92,82 +89,53 @@ __device__ __forceinline__ int first_tap(const AngleGeo &g, float t)
 }
 
 // ------------------------------------------------------------------------------------------------ forward
+// Ray-driven gather: a warp owns one bin s of one angle and 256 channels. Per image row it evaluates the pixels whose
+// footprint can reach s (two to four), skips zero weights (a branch the whole warp takes) and accumulates the
+// weighted channels in registers: no shared memory, no atomics, a fixed summation order. The grid runs
+// channel-block-major (blockIdx.z), so the columns of one channel block (npix x 256) are read from L2 by every
+// angle and bin while they are resident.
 template <int KERNEL, typename ST>
-__global__ void __launch_bounds__(32 * WARPS) radon_forward_v3(
+__global__ void __launch_bounds__(32 * WARPS) radon_forward_v4(
     const float *__restrict__ img, ST *__restrict__ sino, int64_t sld, const float4 *__restrict__ geo, int nx, int ny,
-    int ns, int kstride, int kb, float scale, int n_taps)
+    int ns, int kstride, int kb, float scale)
 {
-    extern __shared__ __align__(16) float red[];          // [WARPS][NB_F][CPW] partial projections
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int a = blockIdx.z;
-    const int k = blockIdx.y * CPW + lane * CPL;
-    const int s0 = blockIdx.x * NB_F;
+    const int s = blockIdx.x * WARPS + warp;
+    const int a = blockIdx.y;
+    const int k = blockIdx.z * CPW + lane * CPL;
+    if (s >= ns) return;                                   // whole warps
     const bool live = k < kstride;
     const AngleGeo g = load_geo(geo, a);
     const int nu = g.rows_are_y ? nx : ny, nv = g.rows_are_y ? ny : nx;
     const int64_t du = (g.rows_are_y ? 1 : (int64_t)nx) * kstride, dv = (g.rows_are_y ? (int64_t)nx : 1) * kstride;
     const float half = KERNEL == 1 ? g.hw : 1.0f;
     const float inv = __frcp_rn(g.A);
-    const int ntap = taps_of(g, KERNEL, n_taps);
-    float acc[NB_F][CPL];
+    const float fs = (float)s;
+    float acc[CPL];
 #pragma unroll
-    for (int j = 0; j < NB_F; ++j)
-#pragma unroll
-        for (int c = 0; c < CPL; ++c) acc[j][c] = 0.0f;
+    for (int c = 0; c < CPL; ++c) acc[c] = 0.0f;
     const float *base = img + (live ? k : 0);
-    for (int v = warp; v < nv; v += WARPS) {
+#pragma unroll 2
+    for (int v = 0; v < nv; ++v) {
         const float c = __fmaf_rn(g.B, (float)v, g.T0);
-        const float e1 = (s0 - half - c) * inv, e2 = (s0 + NB_F - 1 + half - c) * inv;
+        const float e1 = (fs - half - c) * inv, e2 = (fs + half - c) * inv;
         // a margin of 1e-3 pixel covers the rounding of e1, e2; the tap weights decide membership
         const int u0 = max((int)floorf(fminf(e1, e2) - 1e-3f), 0);
         const int u1 = min((int)ceilf(fmaxf(e1, e2) + 1e-3f), nu - 1);
         const float *row = base + (int64_t)v * dv;
         for (int u = u0; u <= u1; ++u) {
-            const float t = __fmaf_rn(g.A, (float)u, c);
+            const float w = tap_weight<KERNEL>(g, __fsub_rn(__fmaf_rn(g.A, (float)u, c), fs));
+            if (w == 0.0f) continue;
             float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
             if (live) ld8(row + (int64_t)u * du, p0, p1);
-            const int sf = first_tap<KERNEL>(g, t);
-            for (int i = 0; i < ntap; ++i) {
-                const int j = sf + i - s0;
-                if (j < 0 || j >= NB_F) continue;
-                const float w = tap_weight<KERNEL>(g, __fsub_rn(t, (float)(sf + i)));
-                if (w == 0.0f) continue;
-                switch (j) {
-                    case 0: acc8(acc[0], w, p0, p1); break;
-                    case 1: acc8(acc[1], w, p0, p1); break;
-                    case 2: acc8(acc[2], w, p0, p1); break;
-                    case 3: acc8(acc[3], w, p0, p1); break;
-                    case 4: acc8(acc[4], w, p0, p1); break;
-                    case 5: acc8(acc[5], w, p0, p1); break;
-                    case 6: acc8(acc[6], w, p0, p1); break;
-                    default: acc8(acc[7], w, p0, p1); break;
-                }
-            }
+            acc8(acc, w, p0, p1);
         }
     }
-    // partial projections of the 8 row classes -> shared memory -> warp j sums bin j over them in a fixed order
+    if (!live) return;
+    float r[CPL];
 #pragma unroll
-    for (int j = 0; j < NB_F; ++j) {
-        float4 *d = reinterpret_cast<float4 *>(red + ((warp * NB_F + j) * CPW + lane * CPL));
-        d[0] = make_float4(acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
-        d[1] = make_float4(acc[j][4], acc[j][5], acc[j][6], acc[j][7]);
-    }
-    __syncthreads();
-    const int j = warp;
-    if (!live || s0 + j >= ns) return;
-    float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
-#pragma unroll
-    for (int w = 0; w < WARPS; ++w) {
-        const float4 *q = reinterpret_cast<const float4 *>(red + ((w * NB_F + j) * CPW + lane * CPL));
-        const float4 q0 = q[0], q1 = q[1];
-        r0.x = __fadd_rn(r0.x, q0.x); r0.y = __fadd_rn(r0.y, q0.y); r0.z = __fadd_rn(r0.z, q0.z);
-        r0.w = __fadd_rn(r0.w, q0.w); r1.x = __fadd_rn(r1.x, q1.x); r1.y = __fadd_rn(r1.y, q1.y);
-        r1.z = __fadd_rn(r1.z, q1.z); r1.w = __fadd_rn(r1.w, q1.w);
-    }
-    float r[CPL] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
-#pragma unroll
-    for (int q = 0; q < CPL; ++q) r[q] = (k + q < kb) ? __fmul_rn(scale, r[q]) : 0.0f;   // padding channels: 0
-    st8(sino + ((int64_t)a * ns + s0 + j) * sld + k, r);
+    for (int q = 0; q < CPL; ++q) r[q] = (k + q < kb) ? __fmul_rn(scale, acc[q]) : 0.0f;   // padding channels: 0
+    st8(sino + ((int64_t)a * ns + s) * sld + k, r);
 }
 
 // ------------------------------------------------------------------------------------------------ backward
@@ -377,18 +345,14 @@ static int radon_forward_any(const float *img_k, ST *sino, int64_t sld, const fl
                 "kstride", (long long)sld, CPL);
     if (n_angles == 0) return DFX_OK;
     DFX_REQUIRE(n_angles <= 65535, "radon: at most 65535 angles per launch");
-    dim3 grid((unsigned)cdiv(n_det, NB_F), (unsigned)cdiv(kstride, CPW), (unsigned)n_angles);
-    const size_t smem = sizeof(float) * WARPS * NB_F * CPW;      // 64 KB of partial projections
-    const int max_taps = 64;                                      // per angle: ceil(1 + |A|)
-    if (kernel == 1) {
-        if ((st = allow_smem(radon_forward_v3<1, ST>, smem))) return st;
-        radon_forward_v3<1, ST><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
-            img_k, sino, sld, reinterpret_cast<const float4 *>(geo), nx, ny, n_det, kstride, kb, scale, max_taps);
-    } else {
-        if ((st = allow_smem(radon_forward_v3<0, ST>, smem))) return st;
-        radon_forward_v3<0, ST><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
-            img_k, sino, sld, reinterpret_cast<const float4 *>(geo), nx, ny, n_det, kstride, kb, scale, max_taps);
-    }
+    DFX_REQUIRE(cdiv(kstride, CPW) <= 65535, "radon: kstride too large for one launch");
+    dim3 grid((unsigned)cdiv(n_det, WARPS), (unsigned)n_angles, (unsigned)cdiv(kstride, CPW));
+    if (kernel == 1)
+        radon_forward_v4<1, ST><<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
+            img_k, sino, sld, reinterpret_cast<const float4 *>(geo), nx, ny, n_det, kstride, kb, scale);
+    else
+        radon_forward_v4<0, ST><<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
+            img_k, sino, sld, reinterpret_cast<const float4 *>(geo), nx, ny, n_det, kstride, kb, scale);
     return launch_status("radon_forward");
 }
 
