@@ -62,10 +62,14 @@ WORKLOADS = {
 
 
 # ----------------------------------------------------------------------------------------------- workload
-def make_problem(name, seed=0):
-    """(cfg, Material, Grid, workload dict): seeded orientations."""
+def make_problem(name, seed=0, K=None):
+    """(cfg, Material, Grid, workload dict): seeded orientations (K: fewer orientations than the workload's, for
+    profiling captures of the same geometry on a few GB)."""
     from diffractom_b200 import Grid, Material
-    w = WORKLOADS[name]
+    w = dict(WORKLOADS[name])
+    if K:
+        w["K"] = int(K)
+        w["grains"] = min(w["grains"], w["K"])
     mat = Material.from_lattice_parameters(**w["material"])
     grid = Grid.from_random_fundamental_zone(w["K"], mat.crystal_system, np.deg2rad(w["sigma_deg"]), seed=seed)
     return dict(w["cfg"]), mat, grid, w
@@ -205,6 +209,7 @@ def main():
     ap.add_argument("--workload", default="ti256", choices=sorted(WORKLOADS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--K", type=int, default=None, help="orientations (default: the workload's)")
     ap.add_argument("--precision", default="both", choices=["both", "bf16", "fp32"],
                     help="both: the BF16 tensor-core path (the value) and the float32 path (for the ratio)")
     a = ap.parse_args()
@@ -224,7 +229,7 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     from diffractom_b200 import SinglePhaseForwardOperator
-    cfg, mat, grid, w = make_problem(a.workload)
+    cfg, mat, grid, w = make_problem(a.workload, K=a.K)
     t_build = time.perf_counter()
     op = SinglePhaseForwardOperator(cfg, mat, grid, w["max_gb"], normalized=True,
                                     precision="bf16" if a.precision in ("bf16", "both") else "fp32")
@@ -252,7 +257,8 @@ def main():
         cpu = {"value": 1.0 / per_epoch, "unit": "epochs/s", "cores": threads, "kind": "port",
                "sample": desc + f" ({took:.1f} s of CPU time)"}
     if rank == 0:
-        cfg_line = {"workload": a.workload, "K": op.K, "pixels": f"{op.Nx}x{op.Ny}", "N_Omega": op.N_Omega,
+        cfg_line = {"workload": a.workload + (f" (K {a.K})" if a.K else ""), "K": op.K,
+                    "pixels": f"{op.Nx}x{op.Ny}", "N_Omega": op.N_Omega,
                     "My": op.My, "N_eta": op.N_eta, "rings": op.N_peaks, "subsets": w["subsets"],
                     "batches": len(op.batches), "K_batch_max": op.K_batch_max, "pf_mode": op.pf_mode,
                     "pf_nnz": op.sparse_nnz, "precision_path": "bf16-tc" if "bf16" in arms else "fp32",
@@ -430,6 +436,14 @@ def algorithmic_work(op, name, args_list):
             nf.append(2 * 2 * npix * n_ang * kb)            # ~2 taps per pixel and angle
         elif name == "dfx_radon_forward_bf16":
             n_ang, kb = args[4], args[9]
+            nb.append(4 * kb * npix + 2 * kb * n_ang * My)
+            nf.append(2 * 2 * npix * n_ang * kb)
+        elif name == "dfx_radon_forward_table":
+            n_ang, kb = args[5], args[8]
+            nb.append(4 * kb * (npix + n_ang * My))
+            nf.append(2 * 2 * npix * n_ang * kb)
+        elif name == "dfx_radon_forward_table_bf16":
+            n_ang, kb = args[6], args[9]
             nb.append(4 * kb * npix + 2 * kb * n_ang * My)
             nf.append(2 * 2 * npix * n_ang * kb)
         elif name == "dfx_radon_backward_spdhg":

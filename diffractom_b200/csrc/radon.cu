@@ -105,6 +105,12 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_v4(
     const int k = blockIdx.z * CPW + lane * CPL;
     if (s >= ns) return;                                   // whole warps
     const bool live = k < kstride;
+    if (blockIdx.z * CPW >= kb) {                          // padding channels only
+        const float zero[CPL] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (live) st8(sino + ((int64_t)a * ns + s) * sld + k, zero);
+        return;
+    }
+    const bool load = k < kb;
     const AngleGeo g = load_geo(geo, a);
     const int nu = g.rows_are_y ? nx : ny, nv = g.rows_are_y ? ny : nx;
     const int64_t du = (g.rows_are_y ? 1 : (int64_t)nx) * kstride, dv = (g.rows_are_y ? (int64_t)nx : 1) * kstride;
@@ -127,7 +133,7 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_v4(
             const float w = tap_weight<KERNEL>(g, __fsub_rn(__fmaf_rn(g.A, (float)u, c), fs));
             if (w == 0.0f) continue;
             float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
-            if (live) ld8(row + (int64_t)u * du, p0, p1);
+            if (load) ld8(row + (int64_t)u * du, p0, p1);
             acc8(acc, w, p0, p1);
         }
     }
@@ -136,6 +142,96 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_v4(
 #pragma unroll
     for (int q = 0; q < CPL; ++q) r[q] = (k + q < kb) ? __fmul_rn(scale, acc[q]) : 0.0f;   // padding channels: 0
     st8(sino + ((int64_t)a * ns + s) * sld + k, r);
+}
+
+// ---- ray table: the non-zero taps of every (angle, bin) in the order radon_forward_v4 visits them (rows v, then
+// pixels u ascending), as (pixel index, weight bits). The geometry of an operator is fixed, so the table is built
+// once; the table-driven forward then spends its instructions on loads and FMAs only, with four taps in flight.
+template <int KERNEL>
+__global__ void ray_table_kernel(const float4 *__restrict__ geo, int n_angles, int nx, int ny, int ns,
+                                 int32_t *__restrict__ counts, const int32_t *__restrict__ row_ptr,
+                                 int2 *__restrict__ entries)
+{
+    const int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;      // a * ns + s
+    if (row >= (int64_t)n_angles * ns) return;
+    const int a = (int)(row / ns), s = (int)(row % ns);
+    const AngleGeo g = load_geo(geo, a);
+    const int nu = g.rows_are_y ? nx : ny, nv = g.rows_are_y ? ny : nx;
+    const float half = KERNEL == 1 ? g.hw : 1.0f;
+    const float inv = __frcp_rn(g.A);
+    const float fs = (float)s;
+    int n = 0;
+    int64_t pos = row_ptr ? row_ptr[row] : 0;
+    for (int v = 0; v < nv; ++v) {
+        const float c = __fmaf_rn(g.B, (float)v, g.T0);
+        const float e1 = (fs - half - c) * inv, e2 = (fs + half - c) * inv;
+        const int u0 = max((int)floorf(fminf(e1, e2) - 1e-3f), 0);
+        const int u1 = min((int)ceilf(fmaxf(e1, e2) + 1e-3f), nu - 1);
+        for (int u = u0; u <= u1; ++u) {
+            const float w = tap_weight<KERNEL>(g, __fsub_rn(__fmaf_rn(g.A, (float)u, c), fs));
+            if (w == 0.0f) continue;
+            if (row_ptr) {
+                const int pix = g.rows_are_y ? u + nx * v : v + nx * u;
+                entries[pos++] = make_int2(pix, __float_as_int(w));
+            }
+            ++n;
+        }
+    }
+    if (!row_ptr) counts[row] = n;
+}
+
+// Table-driven forward: warp per (angle, bin, 256 channels), angle a of the launch = angles[a] of the table (angles
+// NULL: a); the same taps, weights and summation order as radon_forward_v4, so the same bits.
+template <typename ST>
+__global__ void __launch_bounds__(32 * WARPS) radon_forward_table(
+    const float *__restrict__ img, ST *__restrict__ sino, int64_t sld, const int32_t *__restrict__ row_ptr,
+    const int2 *__restrict__ entries, const int32_t *__restrict__ angles, int ns, int kstride, int kb, float scale)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int s = blockIdx.x * WARPS + warp;
+    const int al = blockIdx.y;
+    const int k = blockIdx.z * CPW + lane * CPL;
+    if (s >= ns) return;
+    const bool live = k < kstride;
+    ST *out = sino + ((int64_t)al * ns + s) * sld + k;
+    if (blockIdx.z * CPW >= kb) {
+        const float zero[CPL] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (live) st8(out, zero);
+        return;
+    }
+    const bool load = k < kb;
+    const int a = angles ? __ldg(angles + al) : al;
+    const int64_t r = (int64_t)a * ns + s;
+    int e = __ldg(row_ptr + r);
+    const int e1 = __ldg(row_ptr + r + 1);
+    const float *base = img + (load ? k : 0);
+    float acc[CPL];
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) acc[c] = 0.0f;
+    for (; e + 4 <= e1; e += 4) {
+        int2 t[4];
+        float4 q[4][2];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) t[i] = __ldg(entries + e + i);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            q[i][0] = q[i][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (load) ld8(base + (int64_t)t[i].x * kstride, q[i][0], q[i][1]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc8(acc, __int_as_float(t[i].y), q[i][0], q[i][1]);
+    }
+    for (; e < e1; ++e) {
+        const int2 t = __ldg(entries + e);
+        float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = q0;
+        if (load) ld8(base + (int64_t)t.x * kstride, q0, q1);
+        acc8(acc, __int_as_float(t.y), q0, q1);
+    }
+    if (!live) return;
+    float o[CPL];
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) o[q] = (k + q < kb) ? __fmul_rn(scale, acc[q]) : 0.0f;
+    st8(out, o);
 }
 
 // ------------------------------------------------------------------------------------------------ backward
@@ -163,6 +259,13 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
     const int64_t p = (int64_t)blockIdx.x * WARPS + warp;
     const int k = blockIdx.y * CPW + lane * CPL;
     if (p >= (int64_t)nx * ny || k >= kstride) return;
+    if (blockIdx.y * CPW >= kb) {          // a block of padding channels only: the backprojection is 0 there
+        if (MODE == 0) {
+            const float zero[CPL] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            st8(img + p * kstride + k, zero);
+        }
+        return;                            // MODE 1: dz = 0 leaves z, and x (0 on padding channels), unchanged
+    }
     const int px = (int)(p % nx), py = (int)(p / nx);
     const float fx = (float)px, fy = (float)py;
     float acc[CPL];
@@ -356,6 +459,27 @@ static int radon_forward_any(const float *img_k, ST *sino, int64_t sld, const fl
     return launch_status("radon_forward");
 }
 
+template <typename ST>
+static int radon_forward_table_any(const float *img_k, ST *sino, int64_t sld, const int32_t *row_ptr,
+                                   const int32_t *entries, const int32_t *angles, int n_angles, int n_det,
+                                   int kstride, int kb, float scale, void *stream)
+{
+    DFX_REQUIRE(img_k && sino && row_ptr && entries, "radon_forward_table: null pointer");
+    DFX_REQUIRE(((uintptr_t)img_k % 16) == 0 && ((uintptr_t)sino % 16) == 0 && ((uintptr_t)entries % 8) == 0,
+                "radon_forward_table: misaligned arrays");
+    DFX_REQUIRE(n_angles >= 0 && n_angles <= 65535 && n_det > 0, "radon_forward_table: bad sizes");
+    DFX_REQUIRE(kstride > 0 && kstride % CPL == 0 && kb >= 0 && kb <= kstride && cdiv(kstride, CPW) <= 65535,
+                "radon_forward_table: kstride (%d) must be a positive multiple of %d and kb (%d) <= kstride",
+                kstride, CPL, kb);
+    DFX_REQUIRE(sld >= kstride && sld % CPL == 0, "radon_forward_table: sinogram row stride (%lld) must be a "
+                "multiple of %d >= kstride", (long long)sld, CPL);
+    if (n_angles == 0) return DFX_OK;
+    dim3 grid((unsigned)cdiv(n_det, WARPS), (unsigned)n_angles, (unsigned)cdiv(kstride, CPW));
+    radon_forward_table<ST><<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
+        img_k, sino, sld, row_ptr, reinterpret_cast<const int2 *>(entries), angles, n_det, kstride, kb, scale);
+    return launch_status("radon_forward_table");
+}
+
 template <int MODE, typename ST>
 static int radon_backward_any(const ST *sino, int64_t sld, float *img_k, const float *geo, int n_angles, int nx,
                               int ny, int n_det, int kstride, int kb, int kernel, int n_taps, float *z_k,
@@ -420,6 +544,57 @@ extern "C" int dfx_radon_backward_spdhg_bf16(const void *sino_bf16, int64_t sino
 {
     return radon_backward_any<1>(reinterpret_cast<const __nv_bfloat16 *>(sino_bf16), sino_ld, x_k, geo, n_angles, nx,
                                  ny, n_det, kstride, kb, kernel, n_taps, z_k, T_k, inv_p, lam, stream);
+}
+
+extern "C" int dfx_radon_table_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
+                                     int32_t *counts, void *stream)
+{
+    DFX_REQUIRE(geo && counts && ((uintptr_t)geo % 16) == 0, "radon_table: null or misaligned pointer");
+    DFX_REQUIRE(n_angles > 0 && nx > 0 && ny > 0 && n_det > 0 && (kernel == 0 || kernel == 1),
+                "radon_table: bad sizes or kernel");
+    const int64_t rows = (int64_t)n_angles * n_det;
+    DFX_REQUIRE(cdiv(rows, 128) < 2147483647LL, "radon_table: too many rows");
+    if (kernel == 1)
+        ray_table_kernel<1><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, counts, nullptr, nullptr);
+    else
+        ray_table_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, counts, nullptr, nullptr);
+    return launch_status("radon_table_count");
+}
+
+extern "C" int dfx_radon_table_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
+                                    const int32_t *row_ptr, int32_t *entries, void *stream)
+{
+    DFX_REQUIRE(geo && row_ptr && entries && ((uintptr_t)geo % 16) == 0 && ((uintptr_t)entries % 8) == 0,
+                "radon_table: null or misaligned pointer");
+    DFX_REQUIRE(n_angles > 0 && nx > 0 && ny > 0 && n_det > 0 && (kernel == 0 || kernel == 1),
+                "radon_table: bad sizes or kernel");
+    const int64_t rows = (int64_t)n_angles * n_det;
+    int2 *e = reinterpret_cast<int2 *>(entries);
+    if (kernel == 1)
+        ray_table_kernel<1><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, nullptr, row_ptr, e);
+    else
+        ray_table_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, nullptr, row_ptr, e);
+    return launch_status("radon_table_fill");
+}
+
+extern "C" int dfx_radon_forward_table(const float *img_k, float *sino_k, const int32_t *row_ptr,
+                                       const int32_t *entries, const int32_t *angles, int n_angles, int n_det,
+                                       int kstride, int kb, float scale, void *stream)
+{
+    return radon_forward_table_any(img_k, sino_k, (int64_t)kstride, row_ptr, entries, angles, n_angles, n_det,
+                                   kstride, kb, scale, stream);
+}
+
+extern "C" int dfx_radon_forward_table_bf16(const float *img_k, void *sino_bf16, int64_t sino_ld,
+                                            const int32_t *row_ptr, const int32_t *entries, const int32_t *angles,
+                                            int n_angles, int n_det, int kstride, int kb, float scale, void *stream)
+{
+    return radon_forward_table_any(img_k, reinterpret_cast<__nv_bfloat16 *>(sino_bf16), sino_ld, row_ptr, entries,
+                                   angles, n_angles, n_det, kstride, kb, scale, stream);
 }
 
 extern "C" int dfx_batch_support(float *x_k, const float *colsum_k, const uint8_t *supp, int64_t npix, int kstride,

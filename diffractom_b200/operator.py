@@ -130,6 +130,7 @@ class SinglePhaseForwardOperator:
             self.N_Omega, self.N_eta, self.N_peaks, self.N_axes, self.N_Omega_subdivisions, self.N_eta_subdivisions,
             self.K, float(self.pf_cut))
         self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
+        self._build_ray_table()
         self.omega_subsets = None
         self._sub = []
         self._streamer = None
@@ -169,6 +170,40 @@ class SinglePhaseForwardOperator:
 
     def detector_shifts(self):
         return self.geometry.detector_shifts()
+
+    def _build_ray_table(self):
+        """The projector's non-zero taps per (angle, bin) (dfx_radon_table_*): the forward projection then reads
+        (pixel, weight) pairs instead of evaluating the footprint of every candidate pixel in every call."""
+        R, ns = self.N_Omega, self.My
+        n = R * ns
+        s = self._s()
+        rp = torch.empty(n + 1, dtype=torch.int32, device=self.device)
+        self._call("dfx_radon_table_count", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id,
+                   rp.data_ptr(), s)
+        self.stream().synchronize()
+        cnt64 = rp[:n].to(torch.int64).sum()
+        total = int(cnt64.item())
+        if total >= 2 ** 31:
+            raise ValueError(f"the projector has {total} taps, more than 2^31 - 1")
+        nb = self._lib.dfx_scan_scratch_bytes(n)
+        scr = self.scratch(nb)
+        self._call("dfx_scan_exclusive_i32", rp.data_ptr(), rp.data_ptr(), n, scr.data_ptr(), nb, s)
+        ent = torch.empty(2 * max(total, 1), dtype=torch.int32, device=self.device)
+        self._call("dfx_radon_table_fill", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id,
+                   rp.data_ptr(), ent.data_ptr(), s)
+        self._ray_rp, self._ray_ent, self.ray_taps = rp, ent, total
+
+    def _radon_fwd(self, src_ptr, dst_ptr, om, n_ang, kb, sld=None):
+        """Forward projection of a channel-fastest batch through the ray table: angles om (int32 device tensor of
+        angle indices, None: all) into float32 (sld None) or BF16 (row stride sld) sinogram rows."""
+        om_ptr = None if om is None else om.data_ptr()
+        if sld is None:
+            self._call("dfx_radon_forward_table", src_ptr, dst_ptr, self._ray_rp.data_ptr(), self._ray_ent.data_ptr(),
+                       om_ptr, n_ang, self.My, self.Kstride, kb, float(self.radon_geo.scale), self._s())
+        else:
+            self._call("dfx_radon_forward_table_bf16", src_ptr, dst_ptr, sld, self._ray_rp.data_ptr(),
+                       self._ray_ent.data_ptr(), om_ptr, n_ang, self.My, self.Kstride, kb,
+                       float(self.radon_geo.scale), self._s())
 
     @property
     def coeff_shape(self):
@@ -379,11 +414,10 @@ class SinglePhaseForwardOperator:
     def _max_subset(self):
         return max((e["n"] for e in self._sub), default=1)
 
-    def _radon_forward_bf16(self, src_ptr, ib, z, geo, n):
+    def _radon_forward_bf16(self, src_ptr, ib, z, om, n):
         """Radon transform of channel-fastest batch ib (float32 at src_ptr) into its columns of Z (BF16)."""
-        self._call("dfx_radon_forward_bf16", src_ptr, z.data_ptr() + 2 * ib * self.Kstride, self.Ktot,
-                   geo.data_ptr(), n, self.Nx, self.Ny, self.My, self.Kstride, self.batches[ib]["K_batch"],
-                   self._kernel_id, float(self.radon_geo.scale), self._s())
+        self._radon_fwd(src_ptr, z.data_ptr() + 2 * ib * self.Kstride, om, n, self.batches[ib]["K_batch"],
+                        sld=self.Ktot)
 
     def _pf_tc_forward(self, z, om, n, data, k0=0, kn=None, accumulate=0):
         self._call("dfx_pf_tc_forward", self.pf_bf16.data_ptr(), self.Ktot, k0, self.Ktot if kn is None else kn,
@@ -407,7 +441,7 @@ class SinglePhaseForwardOperator:
             for ib, b in enumerate(self.batches):
                 self._call("dfx_gather_channels", coeffs.data_ptr(), self._img_k.data_ptr(), self.npix, b["k_start"],
                            b["K_batch"], self.Kstride, self._s())
-                self._radon_forward_bf16(self._img_k.data_ptr(), ib, z, geo, n)
+                self._radon_forward_bf16(self._img_k.data_ptr(), ib, z, om, n)
             self._pf_tc_forward(z, om, n, data)
 
     def _adjoint_bf16(self, data, coeffs, subset):
@@ -453,7 +487,7 @@ class SinglePhaseForwardOperator:
     def _bf16_forward_sino(self, subset, ib, src_ptr):
         """Radon transform of batch ib (channel-fastest at src_ptr) for the angles of subset m into Z."""
         e = self._sub[self._subset(subset)]
-        self._radon_forward_bf16(src_ptr, ib, self._z(e["n"]), e["geo"], e["n"])
+        self._radon_forward_bf16(src_ptr, ib, self._z(e["n"]), e["omegas"], e["n"])
 
     def _bf16_forward_rows(self, subset, data):
         """data rows of subset m = PF Z over all orientations (the rows are overwritten)."""
@@ -545,8 +579,7 @@ class SinglePhaseForwardOperator:
             e = self._sub[m]
             geo, n_ang, om = e["geo"], e["n"], e["omegas"]
         self._call("dfx_gather_channels", src.data_ptr(), self._img_k.data_ptr(), self.npix, k_src, Kb, self.Kstride, s)
-        self._call("dfx_radon_forward", self._img_k.data_ptr(), self.coeffs_sino_C.data_ptr(), geo.data_ptr(), n_ang,
-                   self.Nx, self.Ny, self.My, self.Kstride, Kb, self._kernel_id, float(self.radon_geo.scale), s)
+        self._radon_fwd(self._img_k.data_ptr(), self.coeffs_sino_C.data_ptr(), om, n_ang, Kb)
         rp, col, val, compact = self._pf_batch(ib, True, m)
         self._call("dfx_spmm_pf_forward", self.coeffs_sino_C.data_ptr(), rp.data_ptr(), col.data_ptr(),
                    val.data_ptr(), data.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My,
@@ -600,8 +633,7 @@ class SinglePhaseForwardOperator:
         Kb = self.batches[ib]["K_batch"]
         s = self._s()
         geo, n_ang, om, m = self._geo_of(subset)
-        self._call("dfx_radon_forward", src_ptr, self.coeffs_sino_C.data_ptr(), geo.data_ptr(), n_ang, self.Nx,
-                   self.Ny, self.My, self.Kstride, Kb, self._kernel_id, float(self.radon_geo.scale), s)
+        self._radon_fwd(src_ptr, self.coeffs_sino_C.data_ptr(), om, n_ang, Kb)
         rp, col, val, compact = self._pf_batch(ib, True, m)
         self._call("dfx_spmm_pf_forward", self.coeffs_sino_C.data_ptr(), rp.data_ptr(), col.data_ptr(),
                    val.data_ptr(), data.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My,

@@ -83,6 +83,23 @@ int dfx_radon_backward_spdhg_bf16(const void *sino_bf16, int64_t sino_ld, const 
                                   int ny, int n_det, int kstride, int kb, int kernel, int n_taps, float *x_k,
                                   float *z_k, const float *T_k, float inv_p, float lam, void *stream);
 
+/* Ray table of a projector geometry (no reference counterpart: the reference evaluates the taps in every call): the
+ * non-zero taps of every (angle a, bin s), row a * n_det + s, as int32 pairs (pixel index, float32 weight bits) in
+ * the order the forward projection sums them. count: counts[row] = taps of the row (row_ptr = exclusive scan, at
+ * most 2^31 - 1 in total); fill: entries (2 int32 per tap, 8-byte aligned) at row_ptr[row] .. row_ptr[row + 1]. */
+int dfx_radon_table_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel, int32_t *counts,
+                          void *stream);
+int dfx_radon_table_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
+                         const int32_t *row_ptr, int32_t *entries, void *stream);
+/* dfx_radon_forward / dfx_radon_forward_bf16 through the ray table (same references): angle a of the launch is row
+ * block angles[a] of the table (angles NULL: a); the same taps, weights and summation order, hence the same bits. */
+int dfx_radon_forward_table(const float *img_k, float *sino_k, const int32_t *row_ptr, const int32_t *entries,
+                            const int32_t *angles, int n_angles, int n_det, int kstride, int kb, float scale,
+                            void *stream);
+int dfx_radon_forward_table_bf16(const float *img_k, void *sino_bf16, int64_t sino_ld, const int32_t *row_ptr,
+                                 const int32_t *entries, const int32_t *angles, int n_angles, int n_det, int kstride,
+                                 int kb, float scale, void *stream);
+
 /* replaces support_ones / project_support / tmin (fista_poisson.py:256-263, 277-281; spdhg_poisson.py:259-265) on a
  * channel-fastest batch (npix, kstride) with padding channels kb .. kstride-1 (supp (npix) uint8 or NULL):
  * mode 0: x = 1 on live channels of support pixels, else 0; mode 1: x = 0 outside them or where negative;

@@ -172,3 +172,32 @@ def test_argument_errors(golden):
         op.zero_subset_rows(torch.empty(op.data_shape, device="cuda"), 0)     # no subsets yet
     with pytest.raises(ValueError):
         op.set_omega_subsets([np.array([0, op.N_Omega])])
+
+
+@pytest.mark.parametrize("name", ["ti8_small", "adj_0_90", "diff_midpoint_hat"])
+def test_ray_table_forward_equals_footprint_forward(golden, name):
+    """The table-driven forward projection (the operator's) gives the bits of the footprint-evaluating one, for all
+    angles and for a subset's angle list, in float32 and BF16 sinograms."""
+    from diffractom_b200 import _lib
+    d = golden(name)
+    op = make_operator(d)
+    rng = np.random.default_rng(5)
+    kb = op.batches[0]["K_batch"]
+    img = torch.as_tensor(rng.random((op.npix, op.Kstride)).astype(np.float32), device="cuda")
+    img[:, kb:] = 0
+    s = op._s()
+    R, ns, ks = op.N_Omega, op.My, op.Kstride
+    a = torch.empty((R, ns, ks), device="cuda")
+    b = torch.empty((R, ns, ks), device="cuda")
+    _lib.call("dfx_radon_forward", img.data_ptr(), a.data_ptr(), op.geo_gpu.data_ptr(), R, op.Nx, op.Ny, ns, ks, kb,
+              op._kernel_id, float(op.radon_geo.scale), s)
+    op._radon_fwd(img.data_ptr(), b.data_ptr(), None, R, kb)
+    assert torch.equal(a, b)
+    om = torch.arange(1, R, 3, dtype=torch.int32, device="cuda")
+    c = torch.empty((om.numel(), ns, ks), device="cuda")
+    op._radon_fwd(img.data_ptr(), c.data_ptr(), om, om.numel(), kb)
+    assert torch.equal(c, a[om.long()])
+    zb = torch.empty((R, ns, ks + 8), dtype=torch.bfloat16, device="cuda")
+    op._radon_fwd(img.data_ptr(), zb.data_ptr(), None, R, kb, sld=ks + 8)
+    assert torch.equal(zb[:, :, :ks], a.to(torch.bfloat16))
+    assert op.ray_taps == int(op._ray_rp[-1].item()) > 0
