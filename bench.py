@@ -446,13 +446,17 @@ def algorithmic_work(op, name, args_list):
             n_ang, kb = args[6], args[9]
             nb.append(4 * kb * npix + 2 * kb * n_ang * My)
             nf.append(2 * 2 * npix * n_ang * kb)
+        elif name == "dfx_radon_forward_table_bf16_bf16":
+            n_ang, kb = args[6], args[9]
+            nb.append(2 * kb * npix + 2 * kb * n_ang * My)
+            nf.append(2 * 2 * npix * n_ang * kb)
         elif name == "dfx_radon_backward_spdhg":
             n_ang, kstride, kb = args[2], args[6], args[7]
             nb.append(4 * kb * n_ang * My + 4 * 5 * npix * kstride)      # sino; x, z, T read; x, z written
             nf.append(2 * 2 * npix * n_ang * kb)
         elif name == "dfx_radon_backward_spdhg_bf16":
             n_ang, kstride, kb = args[3], args[7], args[8]
-            nb.append(2 * kb * n_ang * My + 4 * 5 * npix * kstride)
+            nb.append(2 * kb * n_ang * My + (4 * 5 + (2 if args[16] else 0)) * npix * kstride)   # + BF16 x copy
             nf.append(2 * 2 * npix * n_ang * kb)
         elif name in ("dfx_spmm_pf_forward", "dfx_spmm_pf_adjoint"):
             n_sub = args[6]

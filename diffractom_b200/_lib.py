@@ -37,11 +37,12 @@ SIGNATURES = {
     "dfx_radon_backward_spdhg": ([P, P, I, I, I, I, I, I, I, I, P, P, P, F, F, S], c_int),
     "dfx_radon_forward_bf16": ([P, P, L, P, I, I, I, I, I, I, I, F, S], c_int),
     "dfx_radon_backward_bf16": ([P, L, P, P, I, I, I, I, I, I, I, I, S], c_int),
-    "dfx_radon_backward_spdhg_bf16": ([P, L, P, I, I, I, I, I, I, I, I, P, P, P, F, F, S], c_int),
+    "dfx_radon_backward_spdhg_bf16": ([P, L, P, I, I, I, I, I, I, I, I, P, P, P, F, F, P, S], c_int),
     "dfx_radon_table_count": ([P, I, I, I, I, I, P, S], c_int),
     "dfx_radon_table_fill": ([P, I, I, I, I, I, P, P, S], c_int),
     "dfx_radon_forward_table": ([P, P, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_radon_forward_table_bf16": ([P, P, L, P, P, P, I, I, I, I, F, S], c_int),
+    "dfx_radon_forward_table_bf16_bf16": ([P, P, L, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_batch_support": ([P, P, P, L, I, I, F, I, S], c_int),
     "dfx_pf_dense": ([POINTER(PFGeometry), I, I, P, S], c_int),
     "dfx_pf_csr_count": ([POINTER(PFGeometry), P, I, I, I, I, P, S], c_int),
@@ -80,6 +81,7 @@ SIGNATURES = {
     "dfx_pf_tc_adjoint": ([P, L, L, L, I, I, I, P, P, I, I, F, P, S], c_int),
     "dfx_tc_status": ([POINTER(ctypes.c_uint), I], c_int),
     "dfx_rows_to_bf16": ([P, P, P, I, I, I, I, S], c_int),
+    "dfx_f32_to_bf16": ([P, P, L, S], c_int),
 }
 
 _lib = None

@@ -299,6 +299,15 @@ __global__ void rows_to_bf16_kernel(const float *__restrict__ in, __nv_bfloat16 
     }
 }
 
+__global__ void f32_to_bf16_kernel(const float4 *__restrict__ in, uint2 *__restrict__ out, int64_t n4)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+        const float4 v = __ldg(in + i);
+        const __nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), b = __floats2bfloat162_rn(v.z, v.w);
+        out[i] = make_uint2(*reinterpret_cast<const uint32_t *>(&a), *reinterpret_cast<const uint32_t *>(&b));
+    }
+}
+
 // ---------------------------------------------------------------------------------------------- host side
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -478,4 +487,15 @@ extern "C" int dfx_rows_to_bf16(const float *in, void *out, const int32_t *omega
     rows_to_bf16_kernel<<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, (cudaStream_t)stream>>>(
         in, reinterpret_cast<__nv_bfloat16 *>(out), omegas, n_sub, my, cp, cp_pad);
     return launch_status("rows_to_bf16");
+}
+
+extern "C" int dfx_f32_to_bf16(const float *in, void *out, int64_t n, void *stream)
+{
+    DFX_REQUIRE(in && out && n >= 0 && n % 4 == 0, "f32_to_bf16: null pointer or n not a multiple of 4");
+    DFX_REQUIRE(((uintptr_t)in % 16) == 0 && ((uintptr_t)out % 8) == 0, "f32_to_bf16: misaligned arrays");
+    if (n == 0) return DFX_OK;
+    const int64_t blocks = cdiv(n / 4, 256);
+    f32_to_bf16_kernel<<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<const float4 *>(in), reinterpret_cast<uint2 *>(out), n / 4);
+    return launch_status("f32_to_bf16");
 }

@@ -60,16 +60,16 @@ __device__ __forceinline__ void st8(__nv_bfloat16 *p, const float (&r)[CPL])
                                                pack_bf16(r[6], r[7]));
 }
 
+// a += w p on 8 channels: four paired FMAs (FFMA2, sm_100), each lane of a pair rounded once as fmaf does
 __device__ __forceinline__ void acc8(float (&a)[CPL], float w, const float4 &p0, const float4 &p1)
 {
-    a[0] = __fmaf_rn(w, p0.x, a[0]);
-    a[1] = __fmaf_rn(w, p0.y, a[1]);
-    a[2] = __fmaf_rn(w, p0.z, a[2]);
-    a[3] = __fmaf_rn(w, p0.w, a[3]);
-    a[4] = __fmaf_rn(w, p1.x, a[4]);
-    a[5] = __fmaf_rn(w, p1.y, a[5]);
-    a[6] = __fmaf_rn(w, p1.z, a[6]);
-    a[7] = __fmaf_rn(w, p1.w, a[7]);
+    const float2 ww = make_float2(w, w);
+    float2 r0 = __ffma2_rn(ww, make_float2(p0.x, p0.y), make_float2(a[0], a[1]));
+    float2 r1 = __ffma2_rn(ww, make_float2(p0.z, p0.w), make_float2(a[2], a[3]));
+    float2 r2 = __ffma2_rn(ww, make_float2(p1.x, p1.y), make_float2(a[4], a[5]));
+    float2 r3 = __ffma2_rn(ww, make_float2(p1.z, p1.w), make_float2(a[6], a[7]));
+    a[0] = r0.x; a[1] = r0.y; a[2] = r1.x; a[3] = r1.y;
+    a[4] = r2.x; a[5] = r2.y; a[6] = r3.x; a[7] = r3.y;
 }
 
 // bins strictly inside a pixel's footprint (t - hw, t + hw) at this angle: at most ceil(1 + |A|) for the trapezoid
@@ -182,9 +182,9 @@ __global__ void ray_table_kernel(const float4 *__restrict__ geo, int n_angles, i
 
 // Table-driven forward: warp per (angle, bin, 256 channels), angle a of the launch = angles[a] of the table (angles
 // NULL: a); the same taps, weights and summation order as radon_forward_v4, so the same bits.
-template <typename ST>
+template <typename ST, typename IT>
 __global__ void __launch_bounds__(32 * WARPS) radon_forward_table(
-    const float *__restrict__ img, ST *__restrict__ sino, int64_t sld, const int32_t *__restrict__ row_ptr,
+    const IT *__restrict__ img, ST *__restrict__ sino, int64_t sld, const int32_t *__restrict__ row_ptr,
     const int2 *__restrict__ entries, const int32_t *__restrict__ angles, int ns, int kstride, int kb, float scale)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_table(
     const int64_t r = (int64_t)a * ns + s;
     int e = __ldg(row_ptr + r);
     const int e1 = __ldg(row_ptr + r + 1);
-    const float *base = img + (load ? k : 0);
+    const IT *base = img + (load ? k : 0);
     float acc[CPL];
 #pragma unroll
     for (int c = 0; c < CPL; ++c) acc[c] = 0.0f;
@@ -250,7 +250,7 @@ template <int KERNEL, int MODE, typename ST>
 __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
     const ST *__restrict__ sino, int64_t sld, float *__restrict__ img, const float4 *__restrict__ geo, int n_angles, int nx,
     int ny, int ns, int kstride, int kb, int n_taps, float *__restrict__ z, const float *__restrict__ T, float inv_p,
-    float lam)
+    float lam, __nv_bfloat16 *__restrict__ xb)
 {
     extern __shared__ AngleParams prm[];                   // the constants of every angle
     for (int i = threadIdx.x; i < n_angles; i += blockDim.x) prm[i] = pack_geo(load_geo(geo, i));
@@ -307,6 +307,7 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
         d[0] = make_float4(r[0], r[1], r[2], r[3]);
         d[1] = make_float4(r[4], r[5], r[6], r[7]);
     } else {
+        float xn[CPL];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             float4 *xp = reinterpret_cast<float4 *>(img + o) + h;
@@ -319,7 +320,9 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
             primal_step(xv.w, zv.w, tv.w, (k + 4 * h + 3 < kb) ? acc[4 * h + 3] : 0.0f, inv_p, lam);
             *xp = xv;
             *zp = zv;
+            xn[4 * h] = xv.x; xn[4 * h + 1] = xv.y; xn[4 * h + 2] = xv.z; xn[4 * h + 3] = xv.w;
         }
+        if (xb) st8(xb + o, xn);           // the BF16 copy of x the next forward projection reads
     }
 }
 
@@ -417,9 +420,9 @@ static int allow_smem(Kernel kernel, size_t bytes)
 }
 
 template <int KERNEL, int MODE, typename ST>
-static int launch_backward(const ST *sino, int64_t sld, float *img, const float *geo, int n_angles, int nx, int ny, int n_det,
-                           int kstride, int kb, int n_taps, float *z, const float *T, float inv_p, float lam,
-                           void *stream)
+static int launch_backward(const ST *sino, int64_t sld, float *img, const float *geo, int n_angles, int nx, int ny,
+                           int n_det, int kstride, int kb, int n_taps, float *z, const float *T, float inv_p, float lam,
+                           __nv_bfloat16 *xb, void *stream)
 {
     const int64_t npix = (int64_t)nx * ny;
     dim3 grid((unsigned)cdiv(npix, WARPS), (unsigned)cdiv(kstride, CPW));
@@ -430,7 +433,7 @@ static int launch_backward(const ST *sino, int64_t sld, float *img, const float 
     if (st) return st;
     radon_backward_v3<KERNEL, MODE, ST><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
         sino, sld, img, reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, kstride, kb, n_taps, z, T, inv_p,
-        lam);
+        lam, xb);
     return launch_status(MODE ? "radon_backward_spdhg" : "radon_backward");
 }
 
@@ -459,8 +462,8 @@ static int radon_forward_any(const float *img_k, ST *sino, int64_t sld, const fl
     return launch_status("radon_forward");
 }
 
-template <typename ST>
-static int radon_forward_table_any(const float *img_k, ST *sino, int64_t sld, const int32_t *row_ptr,
+template <typename ST, typename IT>
+static int radon_forward_table_any(const IT *img_k, ST *sino, int64_t sld, const int32_t *row_ptr,
                                    const int32_t *entries, const int32_t *angles, int n_angles, int n_det,
                                    int kstride, int kb, float scale, void *stream)
 {
@@ -475,7 +478,7 @@ static int radon_forward_table_any(const float *img_k, ST *sino, int64_t sld, co
                 "multiple of %d >= kstride", (long long)sld, CPL);
     if (n_angles == 0) return DFX_OK;
     dim3 grid((unsigned)cdiv(n_det, WARPS), (unsigned)n_angles, (unsigned)cdiv(kstride, CPW));
-    radon_forward_table<ST><<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
+    radon_forward_table<ST, IT><<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
         img_k, sino, sld, row_ptr, reinterpret_cast<const int2 *>(entries), angles, n_det, kstride, kb, scale);
     return launch_status("radon_forward_table");
 }
@@ -483,7 +486,8 @@ static int radon_forward_table_any(const float *img_k, ST *sino, int64_t sld, co
 template <int MODE, typename ST>
 static int radon_backward_any(const ST *sino, int64_t sld, float *img_k, const float *geo, int n_angles, int nx,
                               int ny, int n_det, int kstride, int kb, int kernel, int n_taps, float *z_k,
-                              const float *T_k, float inv_p, float lam, void *stream)
+                              const float *T_k, float inv_p, float lam, void *stream,
+                              __nv_bfloat16 *xb = nullptr)
 {
     int st = check_radon_args(sino, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, kernel);
     if (st) return st;
@@ -494,9 +498,9 @@ static int radon_backward_any(const ST *sino, int64_t sld, float *img_k, const f
     DFX_REQUIRE(n_taps >= 2 && n_taps <= 64, "radon: n_taps (%d) out of range", n_taps);
     if (kernel == 1)
         return launch_backward<1, MODE, ST>(sino, sld, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, n_taps, z_k,
-                                            T_k, inv_p, lam, stream);
+                                            T_k, inv_p, lam, xb, stream);
     return launch_backward<0, MODE, ST>(sino, sld, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, n_taps, z_k, T_k,
-                                        inv_p, lam, stream);
+                                        inv_p, lam, xb, stream);
 }
 
 extern "C" int dfx_radon_forward(const float *img_k, float *sino_k, const float *geo, int n_angles, int nx, int ny,
@@ -540,10 +544,12 @@ extern "C" int dfx_radon_backward_spdhg(const float *sino_k, const float *geo, i
 extern "C" int dfx_radon_backward_spdhg_bf16(const void *sino_bf16, int64_t sino_ld, const float *geo, int n_angles,
                                              int nx, int ny, int n_det, int kstride, int kb, int kernel, int n_taps,
                                              float *x_k, float *z_k, const float *T_k, float inv_p, float lam,
-                                             void *stream)
+                                             void *x_bf16, void *stream)
 {
+    DFX_REQUIRE(((uintptr_t)x_bf16 % 16) == 0, "radon_backward_spdhg_bf16: x_bf16 must be 16-byte aligned");
     return radon_backward_any<1>(reinterpret_cast<const __nv_bfloat16 *>(sino_bf16), sino_ld, x_k, geo, n_angles, nx,
-                                 ny, n_det, kstride, kb, kernel, n_taps, z_k, T_k, inv_p, lam, stream);
+                                 ny, n_det, kstride, kb, kernel, n_taps, z_k, T_k, inv_p, lam, stream,
+                                 reinterpret_cast<__nv_bfloat16 *>(x_bf16));
 }
 
 extern "C" int dfx_radon_table_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
@@ -595,6 +601,15 @@ extern "C" int dfx_radon_forward_table_bf16(const float *img_k, void *sino_bf16,
 {
     return radon_forward_table_any(img_k, reinterpret_cast<__nv_bfloat16 *>(sino_bf16), sino_ld, row_ptr, entries,
                                    angles, n_angles, n_det, kstride, kb, scale, stream);
+}
+
+extern "C" int dfx_radon_forward_table_bf16_bf16(const void *img_bf16, void *sino_bf16, int64_t sino_ld,
+                                                 const int32_t *row_ptr, const int32_t *entries, const int32_t *angles,
+                                                 int n_angles, int n_det, int kstride, int kb, float scale, void *stream)
+{
+    return radon_forward_table_any(reinterpret_cast<const __nv_bfloat16 *>(img_bf16),
+                                   reinterpret_cast<__nv_bfloat16 *>(sino_bf16), sino_ld, row_ptr, entries, angles,
+                                   n_angles, n_det, kstride, kb, scale, stream);
 }
 
 extern "C" int dfx_batch_support(float *x_k, const float *colsum_k, const uint8_t *supp, int64_t npix, int kstride,

@@ -478,16 +478,24 @@ class SinglePhaseForwardOperator:
         self._pf_tc_adjoint(e["omegas"], e["n"], z)
         return e["geo"], e["n"], z
 
-    def _bf16_update_batch(self, ib, geo, n, z, x_ptr, z_ptr, T_ptr, inv_p, lam):
-        """SPDHG's update of batch ib from its columns of Z: the backprojection with the primal step fused."""
+    def _bf16_update_batch(self, ib, geo, n, z, x_ptr, z_ptr, T_ptr, inv_p, lam, xb_ptr=None):
+        """SPDHG's update of batch ib from its columns of Z: the backprojection with the primal step fused (and the
+        BF16 copy of the new x written to xb_ptr)."""
         self._call("dfx_radon_backward_spdhg_bf16", z.data_ptr() + 2 * ib * self.Kstride, self.Ktot, geo.data_ptr(),
                    n, self.Nx, self.Ny, self.My, self.Kstride, self.batches[ib]["K_batch"], self._kernel_id,
-                   int(self.radon_geo.n_taps), x_ptr, z_ptr, T_ptr, float(inv_p), float(lam), self._s())
+                   int(self.radon_geo.n_taps), x_ptr, z_ptr, T_ptr, float(inv_p), float(lam), xb_ptr, self._s())
 
-    def _bf16_forward_sino(self, subset, ib, src_ptr):
-        """Radon transform of batch ib (channel-fastest at src_ptr) for the angles of subset m into Z."""
+    def _bf16_forward_sino(self, subset, ib, src_ptr, src_bf16=False):
+        """Radon transform of batch ib (channel-fastest at src_ptr, float32 or BF16) for the angles of subset m into
+        Z."""
         e = self._sub[self._subset(subset)]
-        self._radon_forward_bf16(src_ptr, ib, self._z(e["n"]), e["omegas"], e["n"])
+        if not src_bf16:
+            self._radon_forward_bf16(src_ptr, ib, self._z(e["n"]), e["omegas"], e["n"])
+            return
+        z = self._z(e["n"])
+        self._call("dfx_radon_forward_table_bf16_bf16", src_ptr, z.data_ptr() + 2 * ib * self.Kstride, self.Ktot,
+                   self._ray_rp.data_ptr(), self._ray_ent.data_ptr(), e["omegas"].data_ptr(), e["n"], self.My,
+                   self.Kstride, self.batches[ib]["K_batch"], float(self.radon_geo.scale), self._s())
 
     def _bf16_forward_rows(self, subset, data):
         """data rows of subset m = PF Z over all orientations (the rows are overwritten)."""

@@ -109,11 +109,12 @@ class SPDHGPoisson:
             geo, n, zb = op._bf16_adjoint_sino(self.D, adj)
         for ib in range(len(op.batches)):
             off = 4 * ib * be
+            xb = self.xkb.data_ptr() + 2 * ib * be
             if adj is not None:
                 op._bf16_update_batch(ib, geo, n, zb, self.xk.data_ptr() + off, self.zk.data_ptr() + off,
-                                      self.Tk.data_ptr() + off, self._inv_p_data, self.lam)
+                                      self.Tk.data_ptr() + off, self._inv_p_data, self.lam, xb)
             if fwd is not None:
-                op._bf16_forward_sino(fwd, ib, self.xk.data_ptr() + off)
+                op._bf16_forward_sino(fwd, ib, xb, src_bf16=True)
         if fwd is not None:
             op._bf16_forward_rows(fwd, self.D)
 
@@ -210,6 +211,10 @@ class SPDHGPoisson:
         self.iter_stats = []
         self._f = float("nan")
         self._seq = self._epoch_sequence()
+        self.xkb = None
+        if op.precision == "bf16":       # the BF16 copy of x that the forward projections read
+            self.xkb = torch.empty(nbt * be, dtype=torch.bfloat16, device=dev)
+            _lib.call("dfx_f32_to_bf16", self.xk.data_ptr(), self.xkb.data_ptr(), nbt * be, s)
         op.zero_subset_rows(self.D, self._seq[0])
         self._pass(None, self._seq[0])
 
@@ -279,7 +284,7 @@ class SPDHGPoisson:
             self._host_x[...] = x.cpu().numpy()
         out = x if self._x_on_gpu else self._host_x
         self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = None
-        self.xk = self.zk = self.Tk = self.dzk = None
+        self.xk = self.zk = self.Tk = self.dzk = self.xkb = None
         self.x = None
         return out
 

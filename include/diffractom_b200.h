@@ -79,9 +79,11 @@ int dfx_radon_forward_bf16(const float *img_k, void *sino_bf16, int64_t sino_ld,
                            int nx, int ny, int n_det, int kstride, int kb, int kernel, float scale, void *stream);
 int dfx_radon_backward_bf16(const void *sino_bf16, int64_t sino_ld, float *img_k, const float *geo, int n_angles,
                             int nx, int ny, int n_det, int kstride, int kb, int kernel, int n_taps, void *stream);
+/* x_bf16 (or NULL): also writes the new x rounded to BF16 there (same layout as x_k), the input of
+ * dfx_radon_forward_table_bf16_bf16 for the next forward projection. */
 int dfx_radon_backward_spdhg_bf16(const void *sino_bf16, int64_t sino_ld, const float *geo, int n_angles, int nx,
                                   int ny, int n_det, int kstride, int kb, int kernel, int n_taps, float *x_k,
-                                  float *z_k, const float *T_k, float inv_p, float lam, void *stream);
+                                  float *z_k, const float *T_k, float inv_p, float lam, void *x_bf16, void *stream);
 
 /* Ray table of a projector geometry (no reference counterpart: the reference evaluates the taps in every call): the
  * non-zero taps of every (angle a, bin s), row a * n_det + s, as int32 pairs (pixel index, float32 weight bits) in
@@ -99,6 +101,10 @@ int dfx_radon_forward_table(const float *img_k, float *sino_k, const int32_t *ro
 int dfx_radon_forward_table_bf16(const float *img_k, void *sino_bf16, int64_t sino_ld, const int32_t *row_ptr,
                                  const int32_t *entries, const int32_t *angles, int n_angles, int n_det, int kstride,
                                  int kb, float scale, void *stream);
+/* The same with a BF16 image batch (the BF16 copy of the coefficients), widened exactly; float32 sums. */
+int dfx_radon_forward_table_bf16_bf16(const void *img_bf16, void *sino_bf16, int64_t sino_ld, const int32_t *row_ptr,
+                                      const int32_t *entries, const int32_t *angles, int n_angles, int n_det,
+                                      int kstride, int kb, float scale, void *stream);
 
 /* replaces support_ones / project_support / tmin (fista_poisson.py:256-263, 277-281; spdhg_poisson.py:259-265) on a
  * channel-fastest batch (npix, kstride) with padding channels kb .. kstride-1 (supp (npix) uint8 or NULL):
@@ -261,6 +267,10 @@ int dfx_tc_status(unsigned int *flags, int reset);
  * = in (n_omega, my, cp) rounded to nearest-even, padding columns set to 0. The data side of the adjoint product. */
 int dfx_rows_to_bf16(const float *in, void *out, const int32_t *omegas, int n_sub, int my, int cp, int cp_pad,
                      void *stream);
+
+/* out = in rounded to nearest-even BF16, n a multiple of 4 (in 16-byte, out 8-byte aligned); no reference
+ * counterpart (the BF16 copies of the precision path). */
+int dfx_f32_to_bf16(const float *in, void *out, int64_t n, void *stream);
 
 /* FISTAPoisson (optimization/fista_poisson.py), all float32 element-wise with float64 sums:
  * replaces times_curvature (:115-144): u <- u * c, c the curvature of the data term at mu (mode 0 Poisson, 1 the
