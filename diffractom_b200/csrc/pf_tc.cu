@@ -21,16 +21,17 @@
 
 #include <mutex>
 
-#include "dfx_common.cuh"
+#include "tc_common.cuh"
 
 namespace dfx {
 namespace {
+
+using namespace tc;
 
 constexpr int TC_M = 128;              // tile rows = tensor-memory lanes
 constexpr int TC_BK = 64;              // K elements per stage: one 128-byte swizzle row of BF16
 constexpr int TC_THREADS = 128;
 constexpr int A_STAGE_BYTES = TC_M * TC_BK * 2;
-constexpr unsigned long long WAIT_NS = 2000000000ull;     // 2 s
 
 __device__ unsigned int g_tc_flags;    // DFX_TC_* bits of expired waits since the last dfx_tc_status reset
 
@@ -43,115 +44,6 @@ struct TcArgs {
     float alpha;
     int accumulate;
 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ unsigned long long now_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Wait for the phase of the given parity to complete, for at most WAIT_NS; false (and the flag set) on expiry.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned int flag)
-{
-    if (mbar_try_wait(bar, parity)) return true;
-    const unsigned long long t0 = now_ns();
-    while (!mbar_try_wait(bar, parity)) {
-        if (now_ns() - t0 > WAIT_NS) {
-            atomicOr(&g_tc_flags, flag);
-            return false;
-        }
-    }
-    return true;
-}
-
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1, int c2)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
-        "[%2];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
-}
-
-// Shared-memory matrix descriptor of a 128-byte-swizzled operand tile (sm_100 layout: start, leading and stride byte
-// offsets in 16-byte units, version 1, swizzle mode 2 = 128B).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
-{
-    uint64_t d = (uint64_t)((addr >> 4) & 0x3FFF);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-    d |= (uint64_t)1 << 46;
-    d |= (uint64_t)2 << 61;
-    return d;
-}
-
-// Instruction descriptor of kind::f16: BF16 A and B, float32 accumulator, M = 128, N = n, A K- or MN-major, B K-major.
-__host__ __device__ constexpr uint32_t instr_desc(int n, int a_mn_major)
-{
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn_major << 15) | ((uint32_t)(n >> 3) << 17) |
-           ((uint32_t)(TC_M >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
-{
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t bar)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
-{
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
 
 constexpr uint32_t TMEM_COLS = 256;    // NT <= 256 float32 columns
 
@@ -206,7 +98,7 @@ __global__ void __launch_bounds__(TC_THREADS) pf_tc_kernel(const __grid_constant
         int kc = 0;
         for (; kc < p.k_chunks; ++kc) {
             const int s = kc % S;
-            if (kc >= S && !mbar_wait(empty0 + 8 * s, ((kc / S) & 1) ^ 1, DFX_TC_TIMEOUT)) break;
+            if (kc >= S && !mbar_wait(empty0 + 8 * s, ((kc / S) & 1) ^ 1, DFX_TC_TIMEOUT, &g_tc_flags)) break;
             const uint32_t fb = full0 + 8 * s;
             mbar_expect_tx(fb, tx);
             const uint32_t a_dst = smem_u32(a_tiles + (size_t)s * A_STAGE_BYTES);
@@ -227,7 +119,7 @@ __global__ void __launch_bounds__(TC_THREADS) pf_tc_kernel(const __grid_constant
         int kc = 0;
         for (; kc < p.k_chunks; ++kc) {
             const int s = kc % S;
-            if (!mbar_wait(full0 + 8 * s, (kc / S) & 1, DFX_TC_TIMEOUT)) break;
+            if (!mbar_wait(full0 + 8 * s, (kc / S) & 1, DFX_TC_TIMEOUT, &g_tc_flags)) break;
             tc_fence_after();
             const uint32_t a_base = smem_u32(a_tiles + (size_t)s * A_STAGE_BYTES);
             const uint32_t b_base = smem_u32(b_tiles + (size_t)s * b_stage_bytes);
@@ -247,7 +139,7 @@ __global__ void __launch_bounds__(TC_THREADS) pf_tc_kernel(const __grid_constant
     __syncwarp();
 
     // epilogue: lane i of warp w holds row m0 + 32 w + i of the tile
-    const bool ok = mbar_wait(done, 0, DFX_TC_TIMEOUT);
+    const bool ok = mbar_wait(done, 0, DFX_TC_TIMEOUT, &g_tc_flags);
     tc_fence_after();
     const int m = m0 + 32 * warp + lane;
     const bool row_live = m < p.m_extent;
@@ -275,7 +167,7 @@ __global__ void __launch_bounds__(TC_THREADS) pf_tc_kernel(const __grid_constant
     if (threadIdx.x == 0) {
         // copies issued but never consumed (only after an expired wait): let them land before the CTA exits
         for (int kc = progress[1]; kc < progress[0]; ++kc)
-            if (!mbar_wait(full0 + 8 * (kc % S), (kc / S) & 1, DFX_TC_TIMEOUT)) break;
+            if (!mbar_wait(full0 + 8 * (kc % S), (kc / S) & 1, DFX_TC_TIMEOUT, &g_tc_flags)) break;
     }
     __syncthreads();
     if (warp == 0) {
@@ -309,44 +201,6 @@ __global__ void f32_to_bf16_kernel(const float4 *__restrict__ in, uint2 *__restr
 }
 
 // ---------------------------------------------------------------------------------------------- host side
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encoder()
-{
-    static std::once_flag once;
-    static EncodeTiledFn fn = nullptr;
-    std::call_once(once, [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    });
-    return fn;
-}
-
-// 3-D BF16 tensor (d0 fastest; s1, s2 the element strides of dimensions 1 and 2) with a box of (b0, b1, 1),
-// 128-byte swizzle, zero fill out of bounds (so a view of rows k0 .. k0+kn-1 reads zeros past its last row).
-int make_map(CUtensorMap *map, const void *base, uint64_t d0, uint64_t d1, uint64_t d2, uint64_t s1, uint64_t s2,
-             uint32_t b0, uint32_t b1, const char *what)
-{
-    EncodeTiledFn enc = encoder();
-    DFX_REQUIRE(enc != nullptr, "pf_tc: cuTensorMapEncodeTiled is not available from the driver");
-    DFX_REQUIRE(((uintptr_t)base % 16) == 0 && (s1 * 2) % 16 == 0 && (s2 * 2) % 16 == 0,
-                "pf_tc: %s must be 16-byte aligned with rows of a multiple of 8 elements", what);
-    const cuuint64_t dims[3] = {d0, d1, d2};
-    const cuuint64_t strides[2] = {s1 * 2, s2 * 2};
-    const cuuint32_t box[3] = {b0, b1, 1};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    const CUresult rc = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void *>(base), dims, strides, box,
-                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    DFX_REQUIRE(rc == CUDA_SUCCESS, "pf_tc: tensor map of %s rejected (CUresult %d)", what, (int)rc);
-    return DFX_OK;
-}
-
 // N tile: the translations split into the fewest tiles of at most 256, each a multiple of 16.
 int n_tile(int my)
 {
@@ -462,10 +316,15 @@ extern "C" int dfx_pf_tc_adjoint(const void *pf_bf16, int64_t ktot, int64_t k0, 
     return launch<1>(ma, mb, a, (int)cdiv(kn, TC_M), (cudaStream_t)stream);
 }
 
+namespace dfx {
+unsigned int tcb_status(unsigned int reset);    // the flags of the tensor-core backprojection (radon_tc.cu)
+}
+
 extern "C" int dfx_tc_status(unsigned int *flags, int reset)
 {
     DFX_REQUIRE(flags != nullptr, "tc_status: null output");
     cudaError_t e = cudaMemcpyFromSymbol(flags, g_tc_flags, sizeof(unsigned int));
+    *flags |= dfx::tcb_status(reset ? 1u : 0u);
     if (e == cudaSuccess && reset) {
         const unsigned int zero = 0;
         e = cudaMemcpyToSymbol(g_tc_flags, &zero, sizeof(unsigned int));

@@ -1,0 +1,366 @@
+// Backprojection on the tensor cores (tcgen05, sm_100a) for the BF16 precision path, with SPDHG's primal step in the
+// epilogue.
+//
+// For a tile of 128 pixels (16 x 8) and 256 channels the backprojection img[p, k] = sum_a w_a sum_s K(t_a(p) - s)
+// Z[a, s, k] is a sum over the launch's angles of GEMMs  D (128 x 256) += W_a (128 x 32) . Z_a (32 x 256):  W_a holds
+// the tap weights of the tile's pixels on a window of 32 bins that covers all of them at angle a (two or three
+// non-zeros per row, float32 weights split into BF16 hi + lo parts, two MMAs, so the weights keep float32 accuracy),
+// Z_a the window's rows of the BF16 Radon output, fetched by TMA (128-byte swizzle, channels fastest). Per angle the
+// four warps write W_a into shared memory (interleaved 8 x 16-byte core matrices) while the tensor core works on the
+// previous angle; the Z windows run up to two angles ahead in a four-stage ring. The float32 accumulator lives in
+// tensor memory (256 columns); the epilogue (eight warps) moves it through shared memory, half the channels at a
+// time, and walks the pixel rows with channel-contiguous loads and stores, applying
+//     z += dz;  x = T > 0 ? max(0, x - T (z + inv_p dz + lam)) : 0;  x_bf16 = bf16(x)
+// exactly as the SIMT kernel radon_backward_v3<MODE 1> does. Replaces, like dfx_radon_backward_spdhg_bf16,
+// radon_backward_k + spdhg_update (radon_kernels.cl:106-141; spdhg_poisson.py:95-106).
+//
+// Every mbarrier wait is bounded (2 s); on expiry the CTA records DFX_TC_TIMEOUT, stops issuing work, lets its copies
+// in flight land, frees its tensor memory and returns without touching x and z. A tap outside the 32-bin window
+// (a geometry whose 16 x 8 tile spans more bins; the host checks this before launching) records DFX_TC_WINDOW.
+
+#include "tc_common.cuh"
+
+namespace dfx {
+
+unsigned int tcb_status(unsigned int reset);
+
+namespace {
+
+using namespace tc;
+
+constexpr int TB_TX = 16, TB_TY = 8;           // pixel tile: 128 pixels = tensor-memory lanes
+constexpr int TB_KW = 32;                      // bins per angle window
+constexpr int TB_N = 256;                      // channels per CTA = accumulator columns
+constexpr int TB_STAGES = 4;                   // Z windows in the ring
+constexpr int TB_AHEAD = 2;                    // angles the Z loads run ahead of the MMAs
+constexpr int TB_A_BYTES = 128 * TB_KW * 2;    // one weight tile (hi or lo): 8 KB
+constexpr int TB_B_BYTES = TB_KW * TB_N * 2;   // one Z window: 16 KB (four 64-channel boxes of 4 KB)
+
+__device__ unsigned int g_tcb_flags;
+
+struct TbArgs {
+    int n_angles, nx, ny, ns, kstride, kb, n_taps, tiles_x;
+    float *x, *z;
+    const float *T;
+    __nv_bfloat16 *xb;
+    float inv_p, lam;
+};
+
+__device__ __forceinline__ uint32_t a_offset(int m, int j)      // interleaved K-major core matrices
+{
+    return (uint32_t)((m >> 3) * 512 + (j >> 3) * 128 + (m & 7) * 16 + (j & 7) * 2);
+}
+
+__device__ __forceinline__ void primal_step_tc(float &x, float &z, float t, float dz, float inv_p, float lam)
+{
+    const float zi = __fadd_rn(z, dz);
+    z = zi;
+    const float zb = __fadd_rn(zi, __fmul_rn(inv_p, dz));
+    x = t > 0.0f ? fmaxf(0.0f, __fsub_rn(x, __fmul_rn(t, __fadd_rn(zb, lam)))) : 0.0f;
+}
+
+__device__ __forceinline__ uint32_t pack2(float lo, float hi)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+template <int KERNEL>
+__device__ __forceinline__ int window_start(const AngleGeo &g, int px0, int py0, int ns)
+{
+    // the tile's smallest detector coordinate is at a corner; its first tap is the tile's first tap
+    float tmin = 3.0e38f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float fx = (float)(px0 + (c & 1) * (TB_TX - 1)), fy = (float)(py0 + (c >> 1) * (TB_TY - 1));
+        const float t = __fmaf_rn(g.A, g.rows_are_y ? fx : fy, __fmaf_rn(g.B, g.rows_are_y ? fy : fx, g.T0));
+        tmin = fminf(tmin, t);
+    }
+    const int sf = KERNEL == 1 ? (int)floorf(__fsub_rn(tmin, g.hw)) + 1 : (int)floorf(tmin);
+    // taps outside the detector get no weight, so the window may start at bin 0 (or the last bin) instead
+    return min(max(sf, 0), ns - 1);
+}
+
+template <int KERNEL>
+__global__ void __launch_bounds__(256) tc_backproject_spdhg(const __grid_constant__ CUtensorMap zmap,
+                                                            const float4 *__restrict__ geo, TbArgs p)
+{
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+    uint8_t *btile = smem;                                        // [TB_STAGES][16 KB]
+    uint8_t *atile = smem + TB_STAGES * TB_B_BYTES;               // [2][hi 8 KB | lo 8 KB]
+    AngleParams *prm = reinterpret_cast<AngleParams *>(atile + 4 * TB_A_BYTES);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(prm + p.n_angles);   // full[S], empty[S], done
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * TB_STAGES + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+    int *n_issued = reinterpret_cast<int *>(tmem_slot + 2), *n_used = reinterpret_cast<int *>(tmem_slot + 3);
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tx = blockIdx.x % p.tiles_x, ty = blockIdx.x / p.tiles_x;
+    const int px0 = tx * TB_TX, py0 = ty * TB_TY;
+    const int k0 = blockIdx.y * TB_N;
+    const int m = tid & 127;                                      // tile row = tensor-memory lane (builders)
+    const int px = px0 + (m & (TB_TX - 1)), py = py0 + (m / TB_TX);
+    const bool valid = px < p.nx && py < p.ny;
+    const int n_ang = p.n_angles;
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + TB_STAGES), done = smem_u32(bars + 2 * TB_STAGES);
+
+    for (int i = tid; i < n_ang; i += blockDim.x) prm[i] = pack_geo(load_geo(geo, i));
+    if (tid == 0) {
+        for (int s = 0; s < TB_STAGES; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        *n_issued = *n_used = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&zmap)) : "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(256));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    // Z window loads: four 64-channel boxes of 32 bins; boxes wholly past the batch's channels are not loaded (their
+    // accumulator columns are never read)
+    int issued = 0;
+    auto load_window = [&](int a) {
+        const AngleGeo g = unpack_geo(prm[a]);
+        const int sw = window_start<KERNEL>(g, px0, py0, p.ns);
+        const int st = a % TB_STAGES;
+        int boxes = 0;
+        for (int i = 0; i < TB_N / 64; ++i) boxes += (k0 + 64 * i < p.kstride);
+        const uint32_t fb = full0 + 8 * st;
+        mbar_expect_tx(fb, (uint32_t)boxes * 4096u);
+        for (int i = 0; i < boxes; ++i)
+            tma_load_3d(smem_u32(btile + st * TB_B_BYTES + 4096 * i), &zmap, fb, k0 + 64 * i, sw, a);
+        issued = a + 1;
+    };
+    if (tid == 0)
+        for (int a = 0; a < n_ang && a < TB_AHEAD; ++a) load_window(a);
+
+    const uint32_t idesc = instr_desc(TB_N, 0, 1);               // A (weights) K-major, B (Z) channels-major
+    for (int a = 0; a < n_ang; ++a) {
+        const int st = a % TB_STAGES;
+        const AngleGeo g = unpack_geo(prm[a]);
+        const int sw = window_start<KERNEL>(g, px0, py0, p.ns);
+        if (a >= 2 && !mbar_wait(empty0 + 8 * ((a - 2) % TB_STAGES), ((a - 2) / TB_STAGES) & 1, DFX_TC_TIMEOUT,
+                                 &g_tcb_flags))
+            *abort_flag = 1;                                      // the MMAs of angle a - 2 have not finished
+        if (tid == 0 && a + TB_AHEAD < n_ang && !*abort_flag) load_window(a + TB_AHEAD);
+
+        // weights of row m on the window (zero row, then its non-zero taps)
+        uint8_t *ah = atile + (a & 1) * 2 * TB_A_BYTES, *al = ah + TB_A_BYTES;
+#pragma unroll
+        for (int c = 0; c < TB_KW / 8; ++c) {
+            if (tid >= 128) break;
+            const uint32_t off = (uint32_t)((m >> 3) * 512 + c * 128 + (m & 7) * 16);
+            *reinterpret_cast<uint4 *>(ah + off) = make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4 *>(al + off) = make_uint4(0, 0, 0, 0);
+        }
+        if (valid && tid < 128) {
+            const float fx = (float)px, fy = (float)py;
+            const float t = __fmaf_rn(g.A, g.rows_are_y ? fx : fy, __fmaf_rn(g.B, g.rows_are_y ? fy : fx, g.T0));
+            const int sf = KERNEL == 1 ? (int)floorf(__fsub_rn(t, g.hw)) + 1 : (int)floorf(t);
+            const int nt = KERNEL == 1 ? min(max(2, (int)ceilf(1.0f + fabsf(g.A) - 1e-6f)), p.n_taps) : 2;
+            for (int i = 0; i < nt; ++i) {
+                const int s = sf + i;
+                if (s < 0 || s >= p.ns) continue;
+                const float w = __fmul_rn(g.w, tap_weight<KERNEL>(g, __fsub_rn(t, (float)s)));
+                if (w == 0.0f) continue;
+                const int j = s - sw;
+                if (j < 0 || j >= TB_KW) {
+                    atomicOr(&g_tcb_flags, DFX_TC_WINDOW);
+                    continue;
+                }
+                const __nv_bfloat16 hi = __float2bfloat16_rn(w);
+                const __nv_bfloat16 lo = __float2bfloat16_rn(__fsub_rn(w, __bfloat162float(hi)));
+                *reinterpret_cast<__nv_bfloat16 *>(ah + a_offset(m, j)) = hi;
+                *reinterpret_cast<__nv_bfloat16 *>(al + a_offset(m, j)) = lo;
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic-proxy writes -> tensor core
+        __syncthreads();
+        if (*abort_flag) break;                                   // the same decision in every thread
+        if (tid == 32) {
+            if (!mbar_wait(full0 + 8 * st, (a / TB_STAGES) & 1, DFX_TC_TIMEOUT, &g_tcb_flags)) {
+                *abort_flag = 1;
+            } else {
+                *n_used = a + 1;
+                tc_fence_after();
+                const uint32_t b_base = smem_u32(btile + st * TB_B_BYTES);
+                const uint32_t ah_base = smem_u32(ah), al_base = smem_u32(al);
+#pragma unroll
+                for (int kk = 0; kk < TB_KW / 16; ++kk) {
+                    const uint64_t bd = smem_desc(b_base + kk * 2048, 4096, 1024, SW_128B);
+                    mma_bf16(tmem, smem_desc(ah_base + kk * 256, 128, 512, SW_NONE), bd, idesc, (a | kk) != 0);
+                    mma_bf16(tmem, smem_desc(al_base + kk * 256, 128, 512, SW_NONE), bd, idesc, 1);
+                }
+                mma_commit(empty0 + 8 * st);                      // weights and window free once these are done
+            }
+        }
+    }
+    if (tid == 0) *n_issued = issued;
+    if (tid == 32) mma_commit(done);
+    __syncwarp();
+    const bool fin = mbar_wait(done, 0, DFX_TC_TIMEOUT, &g_tcb_flags);
+    const bool ok = __syncthreads_and(fin && !*abort_flag) != 0;
+    tc_fence_after();
+
+    // epilogue, per half of the 256 channels: the accumulator goes through shared memory (the freed window ring and
+    // weight tiles) so that each warp then walks pixel rows with coalesced, channel-contiguous loads and stores of
+    // x, z, T and the BF16 copy of x (lane l: channels 4 l .. 4 l + 3 of the half)
+    if (ok) {
+        float *S = reinterpret_cast<float *>(smem);               // 128 rows x 129 floats (padded: no bank conflicts)
+        const int lane = tid & 31, lg = warp & 3, cw = (warp >> 2) * 64;
+        for (int h = 0; h < TB_N / 128; ++h) {
+            if (k0 + h * 128 >= p.kb) break;                      // the same in every thread
+            for (int c = 0; c < 64; c += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(32 * lg) << 16) + (uint32_t)(h * 128 + cw + c), v);
+                float *row = S + (32 * lg + lane) * 129 + cw + c;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) row[i] = v[i];
+            }
+            __syncthreads();
+            const int k = k0 + h * 128 + 4 * lane;
+            if (k < p.kb) {
+#pragma unroll 1
+                for (int r0 = 0; r0 < 16; r0 += 4) {
+                    float4 xv[4], zv[4], tv[4];
+                    int64_t o[4];
+                    bool pv[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int mm = warp * 16 + r0 + u;
+                        const int qx = px0 + (mm & (TB_TX - 1)), qy = py0 + mm / TB_TX;
+                        pv[u] = qx < p.nx && qy < p.ny;
+                        o[u] = ((int64_t)qy * p.nx + qx) * p.kstride + k;
+                        if (pv[u]) {
+                            xv[u] = *reinterpret_cast<const float4 *>(p.x + o[u]);
+                            zv[u] = *reinterpret_cast<const float4 *>(p.z + o[u]);
+                            tv[u] = __ldg(reinterpret_cast<const float4 *>(p.T + o[u]));
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        if (!pv[u]) continue;
+                        const float *d = S + (warp * 16 + r0 + u) * 129 + 4 * lane;
+                        primal_step_tc(xv[u].x, zv[u].x, tv[u].x, (k + 0 < p.kb) ? d[0] : 0.0f, p.inv_p, p.lam);
+                        primal_step_tc(xv[u].y, zv[u].y, tv[u].y, (k + 1 < p.kb) ? d[1] : 0.0f, p.inv_p, p.lam);
+                        primal_step_tc(xv[u].z, zv[u].z, tv[u].z, (k + 2 < p.kb) ? d[2] : 0.0f, p.inv_p, p.lam);
+                        primal_step_tc(xv[u].w, zv[u].w, tv[u].w, (k + 3 < p.kb) ? d[3] : 0.0f, p.inv_p, p.lam);
+                        *reinterpret_cast<float4 *>(p.x + o[u]) = xv[u];
+                        *reinterpret_cast<float4 *>(p.z + o[u]) = zv[u];
+                        if (p.xb)
+                            *reinterpret_cast<uint2 *>(p.xb + o[u]) =
+                                make_uint2(pack2(xv[u].x, xv[u].y), pack2(xv[u].z, xv[u].w));
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+        // windows loaded but never consumed (only after an expired wait): let them land before the CTA exits
+        for (int a = *n_used; a < *n_issued; ++a)
+            if (!mbar_wait(full0 + 8 * (a % TB_STAGES), (a / TB_STAGES) & 1, DFX_TC_TIMEOUT, &g_tcb_flags)) break;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
+    }
+}
+
+size_t tb_smem_bytes(int n_angles)
+{
+    return 1024 + (size_t)TB_STAGES * TB_B_BYTES + 4 * TB_A_BYTES + sizeof(AngleParams) * (size_t)n_angles +
+           (2 * TB_STAGES + 1) * 8 + 16;
+}
+
+}  // namespace
+
+unsigned int tcb_status(unsigned int reset)
+{
+    unsigned int f = 0;
+    cudaMemcpyFromSymbol(&f, g_tcb_flags, sizeof(f));
+    if (reset) {
+        const unsigned int zero = 0;
+        cudaMemcpyToSymbol(g_tcb_flags, &zero, sizeof(zero));
+    }
+    return f;
+}
+
+}  // namespace dfx
+
+using namespace dfx;
+
+extern "C" int dfx_radon_backward_spdhg_tc(const void *sino_bf16, int64_t sino_ld, const float *geo, int n_angles,
+                                           int nx, int ny, int n_det, int kstride, int kb, int kernel, int n_taps,
+                                           float *x_k, float *z_k, const float *T_k, float inv_p, float lam,
+                                           void *x_bf16, void *stream)
+{
+    DFX_REQUIRE(sino_bf16 && geo && x_k && z_k && T_k, "radon_backward_spdhg_tc: null pointer");
+    DFX_REQUIRE(((uintptr_t)sino_bf16 % 16) == 0 && ((uintptr_t)geo % 16) == 0 && ((uintptr_t)x_k % 16) == 0 &&
+                    ((uintptr_t)z_k % 16) == 0 && ((uintptr_t)T_k % 16) == 0 && ((uintptr_t)x_bf16 % 16) == 0,
+                "radon_backward_spdhg_tc: arrays must be 16-byte aligned");
+    DFX_REQUIRE(n_angles >= 0 && n_angles <= 1024 && nx > 0 && ny > 0 && n_det > 0,
+                "radon_backward_spdhg_tc: bad sizes (angles %d, %d x %d, %d bins)", n_angles, nx, ny, n_det);
+    DFX_REQUIRE(kstride > 0 && kstride % 16 == 0 && kb >= 0 && kb <= kstride,
+                "radon_backward_spdhg_tc: kstride (%d) must be a positive multiple of 16 and kb (%d) <= kstride",
+                kstride, kb);
+    DFX_REQUIRE(sino_ld >= kstride && sino_ld % 8 == 0, "radon_backward_spdhg_tc: bad sinogram row stride");
+    DFX_REQUIRE(kernel == 0 || kernel == 1, "radon_backward_spdhg_tc: kernel must be 0 or 1");
+    DFX_REQUIRE(n_taps >= 2 && n_taps <= 64, "radon_backward_spdhg_tc: n_taps (%d) out of range", n_taps);
+    if (n_angles == 0 || kb == 0) return DFX_OK;
+    CUtensorMap zmap;
+    int st = tc::make_map(&zmap, sino_bf16, (uint64_t)kstride, (uint64_t)n_det, (uint64_t)n_angles,
+                          (uint64_t)sino_ld, (uint64_t)sino_ld * n_det, 64, TB_KW, "Z");
+    if (st) return st;
+    TbArgs a{};
+    a.n_angles = n_angles;
+    a.nx = nx;
+    a.ny = ny;
+    a.ns = n_det;
+    a.kstride = kstride;
+    a.kb = kb;
+    a.n_taps = n_taps;
+    a.tiles_x = (int)cdiv(nx, TB_TX);
+    a.x = x_k;
+    a.z = z_k;
+    a.T = T_k;
+    a.xb = reinterpret_cast<__nv_bfloat16 *>(x_bf16);
+    a.inv_p = inv_p;
+    a.lam = lam;
+    const int64_t tiles = (int64_t)a.tiles_x * cdiv(ny, TB_TY);
+    DFX_REQUIRE(tiles < 2147483647LL && cdiv(kb, TB_N) <= 65535, "radon_backward_spdhg_tc: batch too large");
+    const size_t smem = tb_smem_bytes(n_angles);
+    DFX_REQUIRE(smem <= 227 * 1024, "radon_backward_spdhg_tc: %d angles exceed the shared memory of one launch",
+                n_angles);
+    dim3 grid((unsigned)tiles, (unsigned)cdiv(kb, TB_N));
+    cudaError_t e;
+    if (kernel == 1) {
+        e = cudaFuncSetAttribute(tc_backproject_spdhg<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            tc_backproject_spdhg<1><<<grid, 256, smem, (cudaStream_t)stream>>>(zmap, (const float4 *)geo, a);
+    } else {
+        e = cudaFuncSetAttribute(tc_backproject_spdhg<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            tc_backproject_spdhg<0><<<grid, 256, smem, (cudaStream_t)stream>>>(zmap, (const float4 *)geo, a);
+    }
+    if (e != cudaSuccess) {
+        set_error("radon_backward_spdhg_tc: shared memory attribute: %s", cudaGetErrorString(e));
+        return DFX_ELAUNCH;
+    }
+    return launch_status("radon_backward_spdhg_tc");
+}

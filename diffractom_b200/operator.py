@@ -35,7 +35,7 @@ SPARSE_BATCH_MAX = 1024   # largest orientation batch of the sparse modes (SPFO:
 SPARSE_MIN_BATCHES = 4    # sparse modes: at least this many batches (SPFO:135)
 CAND_BYTES = 2 + 4 + 4 + 4 + 4          # per candidate / non-zero scratch of the reference's generator
 NNZ_BYTES = 2 + 4 + 4 + 2 + 4 + 2 + 4   # (pf_generate.py:29-30), used by the batch-size rule
-KSTRIDE_ALIGN = 8                        # channel stride of the batch buffers (two float4 per thread)
+KSTRIDE_ALIGN = 16                       # channel stride of the batch buffers (16 channels per tensor-memory load)
 
 
 def _stream_handle(stream) -> ctypes.c_void_p:
@@ -391,6 +391,11 @@ class SinglePhaseForwardOperator:
         per_angle = 2 * self.My * self.Ktot
         self._bf16_chunk = max(1, min(R, int(max_z_gb * 1024 ** 3 // per_angle)))
         self._all_omegas = torch.arange(R, dtype=torch.int32, device=self.device)
+        # the tensor-core backprojection covers a 16 x 8 pixel tile with a 32-bin window per angle
+        g = np.abs(np.asarray(self.radon_geo.geo, np.float64))
+        hw = (1.0 + np.maximum(g[:, 0], g[:, 1])) / 2.0 if self._kernel_id == 1 else np.ones(R)
+        span = 15.0 * g[:, 0] + 7.0 * g[:, 1] + 2.0 * hw + 2.0
+        self.tc_backprojection = bool(np.all(span <= 32.0)) and self.Kstride % 16 == 0
         self.pf_bf16_setup_s = time.perf_counter() - t0
 
     def _z(self, n):
@@ -481,9 +486,10 @@ class SinglePhaseForwardOperator:
     def _bf16_update_batch(self, ib, geo, n, z, x_ptr, z_ptr, T_ptr, inv_p, lam, xb_ptr=None):
         """SPDHG's update of batch ib from its columns of Z: the backprojection with the primal step fused (and the
         BF16 copy of the new x written to xb_ptr)."""
-        self._call("dfx_radon_backward_spdhg_bf16", z.data_ptr() + 2 * ib * self.Kstride, self.Ktot, geo.data_ptr(),
-                   n, self.Nx, self.Ny, self.My, self.Kstride, self.batches[ib]["K_batch"], self._kernel_id,
-                   int(self.radon_geo.n_taps), x_ptr, z_ptr, T_ptr, float(inv_p), float(lam), xb_ptr, self._s())
+        name = "dfx_radon_backward_spdhg_tc" if self.tc_backprojection else "dfx_radon_backward_spdhg_bf16"
+        self._call(name, z.data_ptr() + 2 * ib * self.Kstride, self.Ktot, geo.data_ptr(), n, self.Nx, self.Ny,
+                   self.My, self.Kstride, self.batches[ib]["K_batch"], self._kernel_id, int(self.radon_geo.n_taps),
+                   x_ptr, z_ptr, T_ptr, float(inv_p), float(lam), xb_ptr, self._s())
 
     def _bf16_forward_sino(self, subset, ib, src_ptr, src_bf16=False):
         """Radon transform of batch ib (channel-fastest at src_ptr, float32 or BF16) for the angles of subset m into

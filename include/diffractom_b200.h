@@ -85,6 +85,15 @@ int dfx_radon_backward_spdhg_bf16(const void *sino_bf16, int64_t sino_ld, const 
                                   int ny, int n_det, int kstride, int kb, int kernel, int n_taps, float *x_k,
                                   float *z_k, const float *T_k, float inv_p, float lam, void *x_bf16, void *stream);
 
+/* dfx_radon_backward_spdhg_bf16 on the tensor cores (same arguments, same references; kstride a multiple of 16):
+ * per 16 x 8 pixel tile and angle, the tap weights on a 32-bin window (float32 weights as BF16 hi + lo) times the
+ * window's BF16 rows, float32 accumulation in tensor memory; the primal step as in the SIMT kernel. The geometry must
+ * keep a tile within the window: |X| * 15 + |Y| * 7 + 2 hw + 2 <= 32 for every angle (X, Y the first two columns of
+ * geo, hw the footprint half width, 1 for the hat); taps outside it are skipped and flagged (DFX_TC_WINDOW). */
+int dfx_radon_backward_spdhg_tc(const void *sino_bf16, int64_t sino_ld, const float *geo, int n_angles, int nx,
+                                int ny, int n_det, int kstride, int kb, int kernel, int n_taps, float *x_k, float *z_k,
+                                const float *T_k, float inv_p, float lam, void *x_bf16, void *stream);
+
 /* Ray table of a projector geometry (no reference counterpart: the reference evaluates the taps in every call): the
  * non-zero taps of every (angle a, bin s), row a * n_det + s, as int32 pairs (pixel index, float32 weight bits) in
  * the order the forward projection sums them. count: counts[row] = taps of the row (row_ptr = exclusive scan, at
@@ -261,6 +270,7 @@ int dfx_pf_tc_adjoint(const void *pf_bf16, int64_t ktot, int64_t k0, int64_t kn,
 /* Bits of device-side waits of the tensor-core kernels that ran out since the last reset (DFX_TC_TIMEOUT); the
  * kernels return early on expiry and leave their outputs undefined. Synchronous; no reference counterpart. */
 #define DFX_TC_TIMEOUT 1u
+#define DFX_TC_WINDOW 2u   /* a tap outside the tensor-core backprojection's 32-bin window (skipped) */
 int dfx_tc_status(unsigned int *flags, int reset);
 
 /* BF16 copy of the data rows of the n_sub angles omegas[s] (omegas NULL: all n_omega rows): out (n_omega, my, cp_pad)
