@@ -7,7 +7,7 @@
 // non-zeros per row, float32 weights split into BF16 hi + lo parts, two MMAs, so the weights keep float32 accuracy),
 // Z_a the window's rows of the BF16 Radon output, fetched by TMA (128-byte swizzle, channels fastest). Per angle the
 // four warps write W_a into shared memory (interleaved 8 x 16-byte core matrices) while the tensor core works on the
-// previous angle; the Z windows run up to two angles ahead in a four-stage ring. The float32 accumulator lives in
+// previous angle; a fifth warp streams the Z windows up to four angles ahead (a four-stage ring). The float32 accumulator lives in
 // tensor memory (256 columns); the epilogue (eight warps) moves it through shared memory, half the channels at a
 // time, and walks the pixel rows with channel-contiguous loads and stores, applying
 //     z += dz;  x = T > 0 ? max(0, x - T (z + inv_p dz + lam)) : 0;  x_bf16 = bf16(x)
@@ -32,7 +32,6 @@ constexpr int TB_TX = 16, TB_TY = 8;           // pixel tile: 128 pixels = tenso
 constexpr int TB_KW = 32;                      // bins per angle window
 constexpr int TB_N = 256;                      // channels per CTA = accumulator columns
 constexpr int TB_STAGES = 4;                   // Z windows in the ring
-constexpr int TB_AHEAD = 2;                    // angles the Z loads run ahead of the MMAs
 constexpr int TB_A_BYTES = 128 * TB_KW * 2;    // one weight tile (hi or lo): 8 KB
 constexpr int TB_B_BYTES = TB_KW * TB_N * 2;   // one Z window: 16 KB (four 64-channel boxes of 4 KB)
 
@@ -65,6 +64,18 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi)
     return *reinterpret_cast<const uint32_t *>(&h);
 }
 
+// OR of v over the 128 threads of warps 0-3 (named barrier 1), which also orders their shared-memory writes
+__device__ __forceinline__ bool builders_or(bool v)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 1, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v)
+        : "memory");
+    return r != 0;
+}
+
 template <int KERNEL>
 __device__ __forceinline__ int window_start(const AngleGeo &g, int px0, int py0, int ns)
 {
@@ -93,7 +104,6 @@ __global__ void __launch_bounds__(256) tc_backproject_spdhg(const __grid_constan
     AngleParams *prm = reinterpret_cast<AngleParams *>(atile + 4 * TB_A_BYTES);
     uint64_t *bars = reinterpret_cast<uint64_t *>(prm + p.n_angles);   // full[S], empty[S], done
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * TB_STAGES + 1);
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
     int *n_issued = reinterpret_cast<int *>(tmem_slot + 2), *n_used = reinterpret_cast<int *>(tmem_slot + 3);
 
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -113,7 +123,6 @@ __global__ void __launch_bounds__(256) tc_backproject_spdhg(const __grid_constan
             mbar_init(empty0 + 8 * s, 1);
         }
         mbar_init(done, 1);
-        *abort_flag = 0;
         *n_issued = *n_used = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&zmap)) : "memory");
@@ -143,75 +152,88 @@ __global__ void __launch_bounds__(256) tc_backproject_spdhg(const __grid_constan
             tma_load_3d(smem_u32(btile + st * TB_B_BYTES + 4096 * i), &zmap, fb, k0 + 64 * i, sw, a);
         issued = a + 1;
     };
-    if (tid == 0)
-        for (int a = 0; a < n_ang && a < TB_AHEAD; ++a) load_window(a);
-
+    // warp 4 lane 0 streams the Z windows, up to TB_STAGES angles ahead of the MMAs; warps 0-3 build the weights
+    // (thread m: row m) and warp 1 lane 0 issues the MMAs; warps 5-7 wait for the epilogue
     const uint32_t idesc = instr_desc(TB_N, 0, 1);               // A (weights) K-major, B (Z) channels-major
-    for (int a = 0; a < n_ang; ++a) {
-        const int st = a % TB_STAGES;
-        const AngleGeo g = unpack_geo(prm[a]);
-        const int sw = window_start<KERNEL>(g, px0, py0, p.ns);
-        if (a >= 2 && !mbar_wait(empty0 + 8 * ((a - 2) % TB_STAGES), ((a - 2) / TB_STAGES) & 1, DFX_TC_TIMEOUT,
-                                 &g_tcb_flags))
-            *abort_flag = 1;                                      // the MMAs of angle a - 2 have not finished
-        if (tid == 0 && a + TB_AHEAD < n_ang && !*abort_flag) load_window(a + TB_AHEAD);
+    bool failed = false;
+    if (tid == 128) {
+        for (int a = 0; a < n_ang; ++a) {
+            const int st = a % TB_STAGES;
+            if (a >= TB_STAGES && !mbar_wait(empty0 + 8 * st, ((a - TB_STAGES) / TB_STAGES) & 1, DFX_TC_TIMEOUT,
+                                             &g_tcb_flags)) {
+                failed = true;
+                break;
+            }
+            load_window(a);
+        }
+        *n_issued = issued;
+    } else if (tid < 128) {
+        for (int a = 0; a < n_ang; ++a) {
+            const int st = a % TB_STAGES;
+            const AngleGeo g = unpack_geo(prm[a]);
+            const int sw = window_start<KERNEL>(g, px0, py0, p.ns);
+            bool bad = failed;                                    // the MMA thread's wait of the last step
+            if (a >= 2 && !mbar_wait(empty0 + 8 * ((a - 2) % TB_STAGES), ((a - 2) / TB_STAGES) & 1, DFX_TC_TIMEOUT,
+                                     &g_tcb_flags))
+                bad = true;                                       // the MMAs of angle a - 2 have not finished
 
-        // weights of row m on the window (zero row, then its non-zero taps)
-        uint8_t *ah = atile + (a & 1) * 2 * TB_A_BYTES, *al = ah + TB_A_BYTES;
+            // weights of row m on the window (zero row, then its non-zero taps)
+            uint8_t *ah = atile + (a & 1) * 2 * TB_A_BYTES, *al = ah + TB_A_BYTES;
 #pragma unroll
-        for (int c = 0; c < TB_KW / 8; ++c) {
-            if (tid >= 128) break;
-            const uint32_t off = (uint32_t)((m >> 3) * 512 + c * 128 + (m & 7) * 16);
-            *reinterpret_cast<uint4 *>(ah + off) = make_uint4(0, 0, 0, 0);
-            *reinterpret_cast<uint4 *>(al + off) = make_uint4(0, 0, 0, 0);
-        }
-        if (valid && tid < 128) {
-            const float fx = (float)px, fy = (float)py;
-            const float t = __fmaf_rn(g.A, g.rows_are_y ? fx : fy, __fmaf_rn(g.B, g.rows_are_y ? fy : fx, g.T0));
-            const int sf = KERNEL == 1 ? (int)floorf(__fsub_rn(t, g.hw)) + 1 : (int)floorf(t);
-            const int nt = KERNEL == 1 ? min(max(2, (int)ceilf(1.0f + fabsf(g.A) - 1e-6f)), p.n_taps) : 2;
-            for (int i = 0; i < nt; ++i) {
-                const int s = sf + i;
-                if (s < 0 || s >= p.ns) continue;
-                const float w = __fmul_rn(g.w, tap_weight<KERNEL>(g, __fsub_rn(t, (float)s)));
-                if (w == 0.0f) continue;
-                const int j = s - sw;
-                if (j < 0 || j >= TB_KW) {
-                    atomicOr(&g_tcb_flags, DFX_TC_WINDOW);
-                    continue;
+            for (int c = 0; c < TB_KW / 8; ++c) {
+                const uint32_t off = (uint32_t)((m >> 3) * 512 + c * 128 + (m & 7) * 16);
+                *reinterpret_cast<uint4 *>(ah + off) = make_uint4(0, 0, 0, 0);
+                *reinterpret_cast<uint4 *>(al + off) = make_uint4(0, 0, 0, 0);
+            }
+            if (valid) {
+                const float fx = (float)px, fy = (float)py;
+                const float t = __fmaf_rn(g.A, g.rows_are_y ? fx : fy, __fmaf_rn(g.B, g.rows_are_y ? fy : fx, g.T0));
+                const int sf = KERNEL == 1 ? (int)floorf(__fsub_rn(t, g.hw)) + 1 : (int)floorf(t);
+                const int nt = KERNEL == 1 ? min(max(2, (int)ceilf(1.0f + fabsf(g.A) - 1e-6f)), p.n_taps) : 2;
+                for (int i = 0; i < nt; ++i) {
+                    const int s = sf + i;
+                    if (s < 0 || s >= p.ns) continue;
+                    const float w = __fmul_rn(g.w, tap_weight<KERNEL>(g, __fsub_rn(t, (float)s)));
+                    if (w == 0.0f) continue;
+                    const int j = s - sw;
+                    if (j < 0 || j >= TB_KW) {
+                        atomicOr(&g_tcb_flags, DFX_TC_WINDOW);
+                        continue;
+                    }
+                    const __nv_bfloat16 hi = __float2bfloat16_rn(w);
+                    const __nv_bfloat16 lo = __float2bfloat16_rn(__fsub_rn(w, __bfloat162float(hi)));
+                    *reinterpret_cast<__nv_bfloat16 *>(ah + a_offset(m, j)) = hi;
+                    *reinterpret_cast<__nv_bfloat16 *>(al + a_offset(m, j)) = lo;
                 }
-                const __nv_bfloat16 hi = __float2bfloat16_rn(w);
-                const __nv_bfloat16 lo = __float2bfloat16_rn(__fsub_rn(w, __bfloat162float(hi)));
-                *reinterpret_cast<__nv_bfloat16 *>(ah + a_offset(m, j)) = hi;
-                *reinterpret_cast<__nv_bfloat16 *>(al + a_offset(m, j)) = lo;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic-proxy writes -> tensor core
+            if (builders_or(bad)) {                               // the same decision in all 128 builder threads
+                failed = true;
+                break;
+            }
+            if (tid == 32) {
+                if (!mbar_wait(full0 + 8 * st, (a / TB_STAGES) & 1, DFX_TC_TIMEOUT, &g_tcb_flags)) {
+                    failed = true;                                // seen by the builders at the next step
+                } else {
+                    *n_used = a + 1;
+                    tc_fence_after();
+                    const uint32_t b_base = smem_u32(btile + st * TB_B_BYTES);
+                    const uint32_t ah_base = smem_u32(ah), al_base = smem_u32(al);
+#pragma unroll
+                    for (int kk = 0; kk < TB_KW / 16; ++kk) {
+                        const uint64_t bd = smem_desc(b_base + kk * 2048, 4096, 1024, SW_128B);
+                        mma_bf16(tmem, smem_desc(ah_base + kk * 256, 128, 512, SW_NONE), bd, idesc, (a | kk) != 0);
+                        mma_bf16(tmem, smem_desc(al_base + kk * 256, 128, 512, SW_NONE), bd, idesc, 1);
+                    }
+                    mma_commit(empty0 + 8 * st);                  // weights and window free once these are done
+                }
             }
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic-proxy writes -> tensor core
-        __syncthreads();
-        if (*abort_flag) break;                                   // the same decision in every thread
-        if (tid == 32) {
-            if (!mbar_wait(full0 + 8 * st, (a / TB_STAGES) & 1, DFX_TC_TIMEOUT, &g_tcb_flags)) {
-                *abort_flag = 1;
-            } else {
-                *n_used = a + 1;
-                tc_fence_after();
-                const uint32_t b_base = smem_u32(btile + st * TB_B_BYTES);
-                const uint32_t ah_base = smem_u32(ah), al_base = smem_u32(al);
-#pragma unroll
-                for (int kk = 0; kk < TB_KW / 16; ++kk) {
-                    const uint64_t bd = smem_desc(b_base + kk * 2048, 4096, 1024, SW_128B);
-                    mma_bf16(tmem, smem_desc(ah_base + kk * 256, 128, 512, SW_NONE), bd, idesc, (a | kk) != 0);
-                    mma_bf16(tmem, smem_desc(al_base + kk * 256, 128, 512, SW_NONE), bd, idesc, 1);
-                }
-                mma_commit(empty0 + 8 * st);                      // weights and window free once these are done
-            }
-        }
+        if (tid == 32) mma_commit(done);
     }
-    if (tid == 0) *n_issued = issued;
-    if (tid == 32) mma_commit(done);
-    __syncwarp();
+    __syncthreads();
     const bool fin = mbar_wait(done, 0, DFX_TC_TIMEOUT, &g_tcb_flags);
-    const bool ok = __syncthreads_and(fin && !*abort_flag) != 0;
+    const bool ok = __syncthreads_and(fin && !failed) != 0;
     tc_fence_after();
 
     // epilogue, per half of the 256 channels: the accumulator goes through shared memory (the freed window ring and
@@ -270,7 +292,7 @@ __global__ void __launch_bounds__(256) tc_backproject_spdhg(const __grid_constan
     }
     tc_fence_before();
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 128) {
         // windows loaded but never consumed (only after an expired wait): let them land before the CTA exits
         for (int a = *n_used; a < *n_issued; ++a)
             if (!mbar_wait(full0 + 8 * (a % TB_STAGES), (a / TB_STAGES) & 1, DFX_TC_TIMEOUT, &g_tcb_flags)) break;
