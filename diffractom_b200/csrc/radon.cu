@@ -180,13 +180,35 @@ __global__ void ray_table_kernel(const float4 *__restrict__ geo, int n_angles, i
     if (!row_ptr) counts[row] = n;
 }
 
+// Raw channel loads of the table-driven forward: 8 channels kept as loaded (2 x float4, or 8 BF16 in a uint4) until
+// their FMAs, so that a warp can hold many taps' loads in flight in few registers.
+template <typename IT> struct Raw8;
+template <> struct Raw8<float> { float4 a, b; };
+template <> struct Raw8<__nv_bfloat16> { uint4 u; };
+
+__device__ __forceinline__ void ldraw(const float *p, Raw8<float> &r) { ld8(p, r.a, r.b); }
+__device__ __forceinline__ void ldraw(const __nv_bfloat16 *p, Raw8<__nv_bfloat16> &r)
+{
+    r.u = __ldg(reinterpret_cast<const uint4 *>(p));
+}
+__device__ __forceinline__ void zraw(Raw8<float> &r) { r.a = r.b = make_float4(0.f, 0.f, 0.f, 0.f); }
+__device__ __forceinline__ void zraw(Raw8<__nv_bfloat16> &r) { r.u = make_uint4(0, 0, 0, 0); }
+__device__ __forceinline__ void accraw(float (&a)[CPL], float w, const Raw8<float> &r) { acc8(a, w, r.a, r.b); }
+__device__ __forceinline__ void accraw(float (&a)[CPL], float w, const Raw8<__nv_bfloat16> &r)
+{
+    acc8(a, w, make_float4(bf_lo(r.u.x), bf_hi(r.u.x), bf_lo(r.u.y), bf_hi(r.u.y)),
+         make_float4(bf_lo(r.u.z), bf_hi(r.u.z), bf_lo(r.u.w), bf_hi(r.u.w)));
+}
+
 // Table-driven forward: warp per (angle, bin, 256 channels), angle a of the launch = angles[a] of the table (angles
-// NULL: a); the same taps, weights and summation order as radon_forward_v4, so the same bits.
+// NULL: a); the same taps, weights and summation order as radon_forward_v4, so the same bits. U taps are loaded
+// before their FMAs (8 for a BF16 image, 4 for float32).
 template <typename ST, typename IT>
 __global__ void __launch_bounds__(32 * WARPS) radon_forward_table(
     const IT *__restrict__ img, ST *__restrict__ sino, int64_t sld, const int32_t *__restrict__ row_ptr,
     const int2 *__restrict__ entries, const int32_t *__restrict__ angles, int ns, int kstride, int kb, float scale)
 {
+    constexpr int U = sizeof(IT) == 2 ? 8 : 4;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = blockIdx.x * WARPS + warp;
     const int al = blockIdx.y;
@@ -208,24 +230,25 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_table(
     float acc[CPL];
 #pragma unroll
     for (int c = 0; c < CPL; ++c) acc[c] = 0.0f;
-    for (; e + 4 <= e1; e += 4) {
-        int2 t[4];
-        float4 q[4][2];
+    for (; e + U <= e1; e += U) {
+        int2 t[U];
+        Raw8<IT> q[U];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) t[i] = __ldg(entries + e + i);
+        for (int i = 0; i < U; ++i) t[i] = __ldg(entries + e + i);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            q[i][0] = q[i][1] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (load) ld8(base + (int64_t)t[i].x * kstride, q[i][0], q[i][1]);
+        for (int i = 0; i < U; ++i) {
+            zraw(q[i]);
+            if (load) ldraw(base + (int64_t)t[i].x * kstride, q[i]);
         }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) acc8(acc, __int_as_float(t[i].y), q[i][0], q[i][1]);
+        for (int i = 0; i < U; ++i) accraw(acc, __int_as_float(t[i].y), q[i]);
     }
     for (; e < e1; ++e) {
         const int2 t = __ldg(entries + e);
-        float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = q0;
-        if (load) ld8(base + (int64_t)t.x * kstride, q0, q1);
-        acc8(acc, __int_as_float(t.y), q0, q1);
+        Raw8<IT> q;
+        zraw(q);
+        if (load) ldraw(base + (int64_t)t.x * kstride, q);
+        accraw(acc, __int_as_float(t.y), q);
     }
     if (!live) return;
     float o[CPL];
