@@ -11,7 +11,7 @@ from .material import Material, group_reflections_into_rings
 from .quadrature import QuadratureRule
 
 __all__ = ["Grid", "MatrixGrid", "Material", "QuadratureRule", "group_reflections_into_rings",
-           "SinglePhaseForwardOperator", "SPDHGPoisson", "estimate_L_power"]
+           "SinglePhaseForwardOperator", "SPDHGPoisson", "FISTAPoisson", "estimate_L_power", "forward_operator"]
 
 
 def __getattr__(name):
@@ -22,4 +22,10 @@ def __getattr__(name):
     if name == "SPDHGPoisson":
         from .spdhg import SPDHGPoisson
         return SPDHGPoisson
+    if name == "FISTAPoisson":
+        from .fista import FISTAPoisson
+        return FISTAPoisson
+    if name == "forward_operator":
+        from .autograd import forward_operator
+        return forward_operator
     raise AttributeError(name)

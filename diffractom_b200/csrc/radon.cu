@@ -202,13 +202,13 @@ __device__ __forceinline__ void accraw(float (&a)[CPL], float w, const Raw8<__nv
 
 // Table-driven forward: warp per (angle, bin, 256 channels), angle a of the launch = angles[a] of the table (angles
 // NULL: a); the same taps, weights and summation order as radon_forward_v4, so the same bits. U taps are loaded
-// before their FMAs (8 for a BF16 image, 4 for float32).
+// before their FMAs.
 template <typename ST, typename IT>
 __global__ void __launch_bounds__(32 * WARPS) radon_forward_table(
     const IT *__restrict__ img, ST *__restrict__ sino, int64_t sld, const int32_t *__restrict__ row_ptr,
     const int2 *__restrict__ entries, const int32_t *__restrict__ angles, int ns, int kstride, int kb, float scale)
 {
-    constexpr int U = sizeof(IT) == 2 ? 8 : 4;
+    constexpr int U = 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = blockIdx.x * WARPS + warp;
     const int al = blockIdx.y;

@@ -21,6 +21,14 @@
 #include "oracle_core.h"
 #undef ACC
 #undef SUFFIX
+#undef IO
+#define ACC double
+#define IO double
+#define SUFFIX _f64io
+#include "oracle_core.h"
+#undef ACC
+#undef IO
+#undef SUFFIX
 
 /* One pole-figure entry, pf_generate.cl:62-140 (pf_entry) == create_pfo_matrix.py:108-199 (pfmatrix_eval_poles):
  * PF[r, k, c, p] = norm_k * mean over the (omega, eta) quadrature nodes of

@@ -41,7 +41,7 @@ def lib():
             build()
         h = ctypes.CDLL(str(LIB))
         P, I, F = c_void_p, c_int, c_float
-        for suf in ("_f64", "_f32"):
+        for suf in ("_f64", "_f32", "_f64io"):
             getattr(h, "orc_radon_forward" + suf).argtypes = [P, P, P, I, I, I, I, I, I, I, F]
             getattr(h, "orc_radon_backward" + suf).argtypes = [P, P, P, I, I, I, I, I, I, I]
             getattr(h, "orc_spmm_forward" + suf).argtypes = [P, P, P, P, P, P, I, I, I, I, I]
@@ -89,6 +89,7 @@ class OracleOperator:
         self.CP = self.C * self.P
         self.batches = [(int(k0), int(kb)) for k0, kb in batches]
         self.suffix = "_" + precision
+        self.io = np.float64 if precision == "f64io" else np.float32   # image / data arrays
         self._csr = {}
 
     @classmethod
@@ -136,20 +137,20 @@ class OracleOperator:
     def forward(self, x, subset=None, data=None):
         """data (R, My, CP) = A x; subset (angle indices): only those rows are written (the others kept from data,
         default zeros)."""
-        x = _c(x, np.float32).reshape(self.K, -1)
+        x = _c(x, self.io).reshape(self.K, -1)
         npix = self.Nx * self.Ny
         if data is None:
-            data = np.zeros((self.R, self.My, self.CP), np.float32)
+            data = np.zeros((self.R, self.My, self.CP), self.io)
         else:
-            data = _c(data, np.float32)
+            data = _c(data, self.io)
         angles = np.arange(self.R) if subset is None else np.asarray(subset, np.int64)
         data[angles] = 0.0
         om = _c(angles, np.int32)
         geo = _c(self.geo[angles], np.float32)
         L = lib()
         for k0, kb in self.batches:
-            img = _c(x[k0:k0 + kb].T, np.float32)                    # (npix, kb) channel-fastest
-            sino = np.empty((len(angles), self.My, kb), np.float32)
+            img = _c(x[k0:k0 + kb].T, self.io)                    # (npix, kb) channel-fastest
+            sino = np.empty((len(angles), self.My, kb), self.io)
             getattr(L, "orc_radon_forward" + self.suffix)(_p(img), _p(sino), _p(geo), len(angles), self.Nx, self.Ny,
                                                           self.My, kb, kb, self.kernel, self.scale)
             c = self.csr(k0, kb)
@@ -159,21 +160,21 @@ class OracleOperator:
 
     def adjoint(self, data, subset=None):
         """coeffs (K, Ny, Nx) = A^T data (subset: the rows of those angles only)."""
-        data = _c(data, np.float32)
+        data = _c(data, self.io)
         npix = self.Nx * self.Ny
         angles = np.arange(self.R) if subset is None else np.asarray(subset, np.int64)
         om = _c(angles, np.int32)
         geo = _c(self.geo[angles], np.float32)
-        out = np.empty((self.K, npix), np.float32)
+        out = np.empty((self.K, npix), self.io)
         alpha = float(np.float32(self.R / np.pi))
         L = lib()
         for k0, kb in self.batches:
             c = self.csr(k0, kb)
-            sino = np.empty((len(angles), self.My, kb), np.float32)
+            sino = np.empty((len(angles), self.My, kb), self.io)
             getattr(L, "orc_spmm_adjoint" + self.suffix)(_p(data), _p(c["row_ptr_a"]), _p(c["col_j"]),
                                                          _p(c["val_a"]), _p(sino), _p(om), len(angles), self.My, kb,
                                                          self.CP, kb, alpha, 0)
-            img = np.empty((npix, kb), np.float32)
+            img = np.empty((npix, kb), self.io)
             getattr(L, "orc_radon_backward" + self.suffix)(_p(sino), _p(img), _p(geo), len(angles), self.Nx, self.Ny,
                                                            self.My, kb, kb, self.kernel)
             out[k0:k0 + kb] = img.T

@@ -9,9 +9,9 @@ from conftest import CASES, case_geometry
 from oracle.oracle import OracleOperator, deviance, lib
 
 
-def _oracle(d, batches=None):
+def _oracle(d, batches=None, precision="f64"):
     g = case_geometry(d)
-    return OracleOperator.from_operator(g, batches=batches), g
+    return OracleOperator.from_operator(g, batches=batches, precision=precision), g
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -140,3 +140,23 @@ def test_dual_update_and_deviance_match_numpy():
     bd = b.astype(np.float64)
     ref = np.sum(m - bd + np.where(bd > 0, bd * np.log(np.where(bd > 0, bd, 1) / m), 0))
     assert abs(deviance(mu, b) / ref - 1) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["al5_small", "ti8_small"])
+def test_float64_io_variant_and_finite_differences(golden, name):
+    """The float64-I/O oracle (the model of the finite-difference checks) equals the float32-I/O checker to float32
+    rounding, matches the reference's float64 model, and its central differences with step 1e-6 give A d."""
+    d = golden(name)
+    f64, _ = _oracle(d)
+    io, _ = _oracle(d, precision="f64io")
+    c = d["c"].astype(np.float64)
+    a = io.forward(c)
+    assert a.dtype == np.float64
+    assert np.abs(a - f64.forward(d["c"])).max() <= 1e-6 * np.abs(a).max()
+    assert np.abs(a - d["fwd"]).max() < 2e-5 * np.abs(d["fwd"]).max()
+    rng = np.random.default_rng(0)
+    dr = rng.standard_normal(c.shape)
+    h = 1e-6
+    fd = (io.forward(c + h * dr) - io.forward(c - h * dr)) / (2 * h)
+    ad = io.forward(dr)
+    assert np.abs(fd - ad).max() <= 1e-7 * np.abs(ad).max()
