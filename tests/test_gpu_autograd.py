@@ -66,7 +66,7 @@ def test_adjoint_identity_100_pairs_and_slice_batch():
         x = (torch.rand(op.coeff_shape, generator=g, device="cuda") < 0.05) * supp * \
             torch.rand(op.coeff_shape, generator=g, device="cuda")
         x.requires_grad_(True)
-        yv = torch.randn(op.data_shape, generator=g, device="cuda")
+        yv = torch.rand(op.data_shape, generator=g, device="cuda")   # non-negative, as the reference's test
         ax = forward_operator(op, x)
         (aty,) = torch.autograd.grad(ax, x, grad_outputs=yv)
         lhs = float((ax.double() * yv.double()).sum())
