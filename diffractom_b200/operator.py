@@ -754,7 +754,7 @@ class SinglePhaseForwardOperator:
         self._gen_col = self._gen_val = None
         self.pf_bf16 = self._d_bf16 = self._z_bf16 = self._img_k2 = None
         self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
-        torch.cuda.synchronize(self.device)
+        self.stream().synchronize()          # this operator's work only (other streams keep running)
 
 
 def estimate_L_power(op, niter: int = 20, seed: int = 0, eps: float = 1e-30, verbose: int = 1) -> float:
