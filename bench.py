@@ -209,6 +209,9 @@ def main():
     ap.add_argument("--workload", default="ti256", choices=sorted(WORKLOADS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the short serving run of the default line")
+    ap.add_argument("--serve", action="store_true", help="only the serving benchmark (64 requests, Poisson "
+                    "arrivals at 2/s, sizes of the serving configuration); its own JSON line")
     ap.add_argument("--K", type=int, default=None, help="orientations (default: the workload's)")
     ap.add_argument("--precision", default="both", choices=["both", "bf16", "fp32"],
                     help="both: the BF16 tensor-core path (the value) and the float32 path (for the ratio)")
@@ -221,6 +224,13 @@ def main():
     if a.impl == "reference":
         return run_reference(a, rank)
     torch.cuda.set_device(local)
+    if a.serve:
+        if rank == 0:
+            st = serving_run(**SERVE_FULL)
+            print(json.dumps({"metric": "serving latency p50/p99 (SPDHG to 1e-3 relative deviance change)",
+                              "value": st["p99_s"], "unit": "s", "higher_is_better": False, "n_gpus": 1,
+                              "data": "synthetic", "serve": st}), flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -275,13 +285,20 @@ def main():
             cfg_line["deviance_note"] = ("deviance of each run's final iterate: float32 forward, float64 sum; the "
                                          "float32 path matches the float64 oracle to 1e-5 (tests)")
             cfg_line["fp32_roofline"] = arms["fp32"]["roof"]
+    serve = None
+    if not a.no_serve and rank == 0:
+        op.free_memory()
+        del op, b
+        torch.cuda.empty_cache()
+        serve = serving_run(**SERVE_SHORT)
+    if rank == 0:
         line = {
             "metric": METRIC, "value": head["value"], "unit": "epochs/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": head["t_max"] / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16" if "bf16" in arms else "f32",
             "data": "synthetic (seeded phantom, Poisson counts)", "config": cfg_line,
             "roofline": head["roof"], "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(head["launches"]),
-            "clocks": head["clk"],
+            "clocks": head["clk"], "serve": serve,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -490,6 +507,71 @@ def algorithmic_work(op, name, args_list):
             nb.append(0)
             nf.append(0)
     return float(np.mean(nb)), float(np.mean(nf))
+
+
+SERVE_FULL = dict(n=64, rate=2.0, px=(48, 200), omega=(90, 360), eta=(90, 360), rings=(3, 8), K=(500, 10000),
+                  slots=8, budget_gb=120.0, max_epochs=100, seed=0,
+                  scenario="64 requests, Poisson arrivals 2/s, pixels 48^2-200^2, omega 90-360, eta 90-360, rings 3-8, "
+                           "K 500-10000, cubic or hexagonal, SPDHG to 1e-3 relative deviance change, 120 GB budget")
+SERVE_SHORT = dict(n=12, rate=2.0, px=(48, 128), omega=(90, 240), eta=(90, 240), rings=(3, 8), K=(500, 2000),
+                   slots=8, budget_gb=120.0, max_epochs=150, seed=0,
+                   scenario="12 requests, Poisson arrivals 2/s, pixels 48^2-128^2, omega 90-240, eta 90-240, rings "
+                            "3-8, K 500-2000 (the serving configuration's ranges, capped to keep the run short), "
+                            "SPDHG to 1e-3 relative deviance change, 120 GB budget")
+
+
+def serving_run(n, rate, px, omega, eta, rings, K, slots, budget_gb, max_epochs, seed, scenario):
+    """Requests of random size drawn uniformly from the ranges (cubic Al or hexagonal Ti, the first `rings`
+    reflections), seeded phantoms and Poisson counts made beforehand, then submitted to a ReconstructionServer at
+    Poisson arrival times; returns its latency statistics."""
+    import torch
+    from diffractom_b200 import Grid, Material, SinglePhaseForwardOperator
+    from diffractom_b200.serving import ReconstructionServer, Request
+    rng = np.random.default_rng(seed)
+    cub = [[1, 1, 1], [2, 0, 0], [2, 2, 0], [3, 1, 1], [2, 2, 2], [4, 0, 0], [3, 3, 1], [4, 2, 0]]
+    reqs = []
+    t_prep = time.perf_counter()
+    for i in range(n):
+        p = int(rng.integers(px[0], px[1] + 1))
+        cfg = dict(Nx=p, Ny=p, My=p + 4 + p // 40, N_Omega=int(rng.integers(omega[0], omega[1] + 1)),
+                   angle_range=[0, 180], cor_offset=0.0, N_eta=int(rng.integers(eta[0], eta[1] + 1)),
+                   eta_angle_range=[0, 360], energy=12.398 / 0.3, k_direction_0=[0, 0, 1], p_direction_0=[1, 0, 0],
+                   detector_direction_origin=[0, -1, 0], detector_direction_positive_90=[0, 0, -1])
+        nr = int(rng.integers(rings[0], rings[1] + 1))
+        if rng.random() < 0.5:
+            mat = Material.from_lattice_parameters(a=4.05, symmetry_group="cubic", wavelength_A=0.3,
+                                                   hkl_list=cub[:nr])
+        else:
+            mat = Material.from_lattice_parameters(**{**WORKLOADS["ti256"]["material"],
+                                                      "hkl_list": WORKLOADS["ti256"]["material"]["hkl_list"][:nr]})
+        k = int(rng.integers(K[0], K[1] + 1))
+        grid = Grid.from_random_fundamental_zone(k, mat.crystal_system, np.deg2rad(3.0), seed=seed + i)
+        op = SinglePhaseForwardOperator(cfg, mat, grid, 1.0, normalized=True)
+        x = phantom(op, {"grains": 10, "background": 0.0}, seed=seed + i)
+        b = counts(op, x, 50.0, seed=seed + i).cpu().numpy()
+        op.free_memory()
+        del op, x
+        reqs.append(Request(cfg, mat, grid, b, subsets=8, max_epochs=max_epochs, tol=1e-3))
+    torch.cuda.empty_cache()
+    t_prep = time.perf_counter() - t_prep
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    srv = ReconstructionServer(device=torch.cuda.current_device(), max_slots=slots, hbm_budget_gb=budget_gb).start()
+    t0 = time.perf_counter()
+    for r, t in zip(reqs, arrivals):
+        delay = t - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        srv.submit(r)
+    finished = srv.wait_all(timeout=1800)
+    srv.stop()
+    st = srv.stats()
+    st.update({"scenario": scenario, "slots": slots, "all_finished": bool(finished),
+               "input_preparation_s": round(t_prep, 1),
+               "converged": int(sum(1 for r in reqs if r.error is None and r.epochs < max_epochs)),
+               "epochs_p50": float(np.median([r.epochs for r in reqs])),
+               "deviance_first_request": [float("%.6g" % f) for f in reqs[0].deviance[:12]],
+               "errors": [r.error for r in reqs if r.error][:3]})
+    return st
 
 
 def measure_e2e(op, w, b_dev, steps):
