@@ -475,6 +475,11 @@ def algorithmic_work(op, name, args_list):
             n_ang, kstride, kb = args[3], args[7], args[8]
             nb.append(2 * kb * n_ang * My + (4 * 5 + (2 if args[16] else 0)) * npix * kstride)   # + BF16 x copy
             nf.append(2 * 2 * npix * n_ang * kb)
+        elif name == "dfx_radon_backward_spdhg_tc":
+            # BF16 Z rows of the batch's channels; x, z, T read, x, z written (float32) and the BF16 copy of x
+            n_ang, kb = args[3], args[8]
+            nb.append(2 * kb * n_ang * My + (4 * 5 + (2 if args[16] else 0)) * npix * kb)
+            nf.append(2 * 2 * npix * n_ang * kb)
         elif name in ("dfx_spmm_pf_forward", "dfx_spmm_pf_adjoint"):
             n_sub = args[6]
             kb = args[10] if name == "dfx_spmm_pf_forward" else args[8]

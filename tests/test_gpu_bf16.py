@@ -97,19 +97,14 @@ def test_bf16_spdhg_deviance_within_1e3_of_float64(golden):
     assert coef_err < 5e-2, coef_err
 
 
-@pytest.mark.parametrize("name", ["al5_small", "adj_0_360", "diff_midpoint_hat"])
-def test_tc_backprojection_update_matches_simt(golden, name):
-    """The tensor-core backprojection with the fused SPDHG step against the SIMT one on the same BF16 sinogram:
-    z (= the backprojection, from z = 0) within 2e-5 of its maximum, x from the same formula, and the BF16 copy of x
-    exactly x rounded."""
+def _tc_vs_simt(geo, R, nx, ny, ns, kb, kernel_id, n_taps, seed=8):
+    """Runs the SIMT and the tensor-core backprojection with the fused SPDHG step on the same BF16 sinogram and
+    state and checks: z (= the backprojection, from z = 0) within 2e-5 of its maximum, x from the same formula, and
+    the BF16 copy of x exactly x rounded."""
     import ctypes
     from diffractom_b200 import _lib
-    d = golden(name)
-    op = make_operator(d)
-    assert op.Kstride > 0
-    rng = np.random.default_rng(8)
-    npix, R, ns = op.npix, op.N_Omega, op.My
-    kb = op.batches[0]["K_batch"]
+    rng = np.random.default_rng(seed)
+    npix = nx * ny
     ks = -(-max(kb, 16) // 16) * 16
     sld = ks + 16
     sino = torch.as_tensor(rng.standard_normal((R, ns, sld)).astype(np.float32), device="cuda").to(torch.bfloat16)
@@ -117,14 +112,15 @@ def test_tc_backprojection_update_matches_simt(golden, name):
     T[:, kb:] = 0
     x0 = torch.full((npix, ks), 50.0, device="cuda")
     x0[:, kb:] = 0
+    stream = torch.cuda.current_stream().cuda_stream
     out = {}
     for name_fn in ("dfx_radon_backward_spdhg_bf16", "dfx_radon_backward_spdhg_tc"):
         x, z = x0.clone(), torch.zeros((npix, ks), device="cuda")
         xb = torch.zeros((npix, ks), dtype=torch.bfloat16, device="cuda")
-        _lib.call(name_fn, sino.data_ptr(), sld, op.geo_gpu.data_ptr(), R, op.Nx, op.Ny, ns, ks, kb, op._kernel_id,
-                  int(op.radon_geo.n_taps), x.data_ptr(), z.data_ptr(), T.data_ptr(), 3.0, 0.1, xb.data_ptr(),
-                  op._s())
+        _lib.call(name_fn, sino.data_ptr(), sld, geo.data_ptr(), R, nx, ny, ns, ks, kb, kernel_id, n_taps,
+                  x.data_ptr(), z.data_ptr(), T.data_ptr(), 3.0, 0.1, xb.data_ptr(), stream)
         out[name_fn] = (x, z, xb)
+    torch.cuda.synchronize()
     xs, zs, xbs = out["dfx_radon_backward_spdhg_bf16"]
     xt, zt, xbt = out["dfx_radon_backward_spdhg_tc"]
     zmax = float(zs.abs().max())
@@ -133,6 +129,32 @@ def test_tc_backprojection_update_matches_simt(golden, name):
     assert float((xt - xs).abs().max()) <= 1e-4 * float(xs.abs().max())
     assert torch.equal(xbt[:, :kb], xt[:, :kb].to(torch.bfloat16))
     assert torch.equal(xbs[:, :kb], xs[:, :kb].to(torch.bfloat16))
+    # channels past the batch are left alone
+    assert torch.equal(xt[:, kb:], x0[:, kb:]) and not bool(zt[:, kb:].any())
     f = ctypes.c_uint(0)
     _lib.check(_lib.lib().dfx_tc_status(ctypes.byref(f), 1))
     assert f.value == 0
+
+
+@pytest.mark.parametrize("name", ["al5_small", "adj_0_360", "diff_midpoint_hat"])
+def test_tc_backprojection_update_matches_simt(golden, name):
+    """The tensor-core backprojection with the fused SPDHG step against the SIMT one on the reference's test
+    geometries (one tile per CTA)."""
+    d = golden(name)
+    op = make_operator(d)
+    assert op.Kstride > 0
+    _tc_vs_simt(op.geo_gpu, op.N_Omega, op.Nx, op.Ny, op.My, op.batches[0]["K_batch"], op._kernel_id,
+                int(op.radon_geo.n_taps))
+
+
+@pytest.mark.parametrize("kernel", ["trapezoid", "hat"])
+def test_tc_backprojection_many_tiles_per_cta(kernel):
+    """A ragged image (130 x 124 pixels: partial 16 x 8 tiles on both edges) and 1200 channels (a partial last
+    256-channel block): 720 tiles, so each persistent CTA walks several tiles and both tensor-memory accumulators
+    go through several phases."""
+    from diffractom_b200.geometry import radon_geometry
+    nx, ny, ns, R = 130, 124, 190, 30
+    ang = np.linspace(0.0, np.pi, R, endpoint=False) + 0.013
+    g = radon_geometry(ang, nx, ny, ns, float(max(nx, ny)), float(ns), 0.37, np.pi / R, kernel=kernel)
+    geo = torch.as_tensor(g.geo, device="cuda")
+    _tc_vs_simt(geo, R, nx, ny, ns, 1200, 1 if kernel == "trapezoid" else 0, int(g.n_taps), seed=3)
