@@ -10,10 +10,13 @@ forward of the next subset) and the same state dict.
 Iteration, for the next subset m (p_m = 1 / M):
     y_m'  <- prox_{S F_m*}(y_m + S A_m x)            rows of subset m, closed form in float64
     dz    <- A_m^T (y_m' - y_m);  z <- z + dz;  x <- max(0, x - T (z + dz / p_m + lam))
-Device arrays: x, z, T (coefficient-sized, kept for the whole run in the operator's channel-fastest batch layout, so
-that an iteration needs no gather / scatter and the primal step runs in the backprojection's epilogue), y, S, D
+State: x, z, T (coefficient-sized, kept for the whole run in the operator's channel-fastest batch layout, so that
+an iteration needs no gather / scatter and the primal step runs in the backprojection's epilogue), y, S, D
 (data-sized; D holds A_m x of the next subset and the dual change of the current one) and one batch-sized scratch.
-x is converted back to the (K, Ny, Nx) layout for callbacks and at the end; z for the state.
+With a NumPy x0, each of x, z, T that does not fit on the device (resident="auto") or is not asked to stay there
+(resident="none" or a list of names) lives in pinned host memory in the same batch layout and is streamed through two
+device slots on side streams during every pass (spdhg_poisson.py:411-428); the iterates are the same bits either
+way. x is converted back to the (K, Ny, Nx) layout for callbacks and at the end; z for the state.
 """
 from __future__ import annotations
 
@@ -25,9 +28,11 @@ import torch
 from . import _lib
 from .arrays import as_host, check_device, is_device
 from .solvers import Reducer, as_device_data, periodic, support_mask_to_device
+from .streaming import BatchPipeline, CoeffArray, KMajorStaging
 
 RHO_AUTO = 3e4
 NAMES = ("x", "z", "T")
+MARGIN_GB = 1.5          # resident="auto": device memory left free (spdhg_poisson.py:278)
 
 
 class SPDHGPoisson:
@@ -35,9 +40,10 @@ class SPDHGPoisson:
 
     def __init__(self, operator, subsets=8, prox_kind="nonneg", lam=0.0, support="fov", eps_counts=1e-3, rho="auto",
                  seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None):
-        """Arguments as diffractom's SPDHGPoisson (spdhg_poisson.py:301-302). resident: accepted; the coefficient
-        arrays of a NumPy x0 are kept on the device when they fit (this package's streaming of solver state is the
-        operator's direct / adjoint streaming). tv > 0 (the TV block) is not provided."""
+        """Arguments as diffractom's SPDHGPoisson (spdhg_poisson.py:301-302). resident ("auto", "all", "none" or a
+        list of names from ("x", "z", "T")): which coefficient arrays of a run with a NumPy x0 stay on the device;
+        the others are streamed from pinned host memory (a CUDA x0 keeps all three on the device). tv > 0 (the TV
+        block) is not provided."""
         if prox_kind not in ("nonneg", "nonneg_l1"):
             raise ValueError("SPDHGPoisson supports prox_kind 'nonneg' and 'nonneg_l1'")
         if not (resident in ("auto", "all", "none") or set(resident) <= set(NAMES + ("qx", "qy"))):
@@ -85,36 +91,47 @@ class SPDHGPoisson:
         """One pass over the batches: adjoint of subset adj's dual change (in D), z and x updated; then the forward
         of the new x for subset fwd ("full": all rows) added to D (spdhg_poisson.py:430-484)."""
         op = self.op
-        be = op.batch_elems()
         if op.precision == "bf16" and fwd != "full":
             self._pass_bf16(adj, fwd)
             return
         sub = None if fwd == "full" else fwd
-        for ib in range(len(op.batches)):
-            off = 4 * ib * be
+        X, Z, T = self.X, self.Z, self.T
+
+        def compute(ib, s):
+            xp = X.ptr(ib, s)
             if adj is not None:       # A_m^T of the dual change, z and x updated in the backprojection's epilogue
-                op._adjoint_update_batch(self.D, ib, adj, self.xk.data_ptr() + off, self.zk.data_ptr() + off,
-                                         self.Tk.data_ptr() + off, self._inv_p_data, self.lam)
+                op._adjoint_update_batch(self.D, ib, adj, xp, Z.ptr(ib, s), T.ptr(ib, s), self._inv_p_data,
+                                         self.lam)
             if fwd is not None:
-                op._direct_batch_k(self.xk.data_ptr() + off, ib, self.D, sub)
+                op._direct_batch_k(xp, ib, self.D, sub)
+
+        upd = adj is not None
+        self.pipe.run([X, Z, T] if upd else [X], [X, Z] if upd else [], compute)
 
     def _pass_bf16(self, adj, fwd):
         """The pass of an operator with precision "bf16": one tensor-core launch takes the dual change of subset adj
         to the BF16 Radon output of all batches, each batch's backprojection applies the primal step and projects the
         new x for subset fwd into its columns of that output, and one tensor-core launch overwrites subset fwd's data
-        rows. Full forward passes (the residual of the diagnostics) stay float32."""
+        rows. Full forward passes (the residual of the diagnostics) stay float32. The BF16 copy of x that the forward
+        reads is kept for all batches when x is resident, else made per batch (one buffer)."""
         op = self.op
         be = op.batch_elems()
+        X, Z, T = self.X, self.Z, self.T
         if adj is not None:
             geo, n, zb = op._bf16_adjoint_sino(self.D, adj)
-        for ib in range(len(op.batches)):
-            off = 4 * ib * be
-            xb = self.xkb.data_ptr() + 2 * ib * be
+
+        def compute(ib, s):
+            xb = self.xkb.data_ptr() + (2 * ib * be if X.resident else 0)
             if adj is not None:
-                op._bf16_update_batch(ib, geo, n, zb, self.xk.data_ptr() + off, self.zk.data_ptr() + off,
-                                      self.Tk.data_ptr() + off, self._inv_p_data, self.lam, xb)
+                op._bf16_update_batch(ib, geo, n, zb, X.ptr(ib, s), Z.ptr(ib, s), T.ptr(ib, s), self._inv_p_data,
+                                      self.lam, xb)
+            elif not X.resident:
+                _lib.call("dfx_f32_to_bf16", X.ptr(ib, s), xb, be, op._s())
             if fwd is not None:
                 op._bf16_forward_sino(fwd, ib, xb, src_bf16=True)
+
+        upd = adj is not None
+        self.pipe.run([X, Z, T] if upd else [X], [X, Z] if upd else [], compute)
         if fwd is not None:
             op._bf16_forward_rows(fwd, self.D)
 
@@ -140,7 +157,6 @@ class SPDHGPoisson:
         s = op._s()
         self._x_on_gpu = is_device(x0)
         self._host_x = None if self._x_on_gpu else as_host(x0, cshape, "x0")
-        self.x = check_device(x0, cshape, "x0") if self._x_on_gpu else torch.as_tensor(self._host_x, device=dev)
         self.b = as_device_data(b, dshape, dev)
         self.w, self.pw = periodic(weights, dshape, "weights", dev)
         self.g, self.pg = periodic(gain, dshape, "gain", dev)
@@ -163,19 +179,32 @@ class SPDHGPoisson:
         self.rho_used = float(rho)
         gamma = np.sqrt(rho)
         p = self._p_data
-        self.resident_used = NAMES
-        # x, z, T live in the operator's channel-fastest batch layout for the whole run (batch ib at ib * be)
+        # x, z, T in the operator's channel-fastest batch layout for the whole run (batch ib at ib * be): on the device,
+        # or in pinned host memory streamed through two device slots
         be = op.batch_elems()
         nbt = len(op.batches)
-        self.xk = torch.empty(nbt * be, dtype=torch.float32, device=dev)
-        self.zk = torch.empty(nbt * be, dtype=torch.float32, device=dev)
-        self.Tk = torch.empty(nbt * be, dtype=torch.float32, device=dev)
+        resident = self._choose_resident()
+        self.resident_used = tuple(nm for nm in NAMES if nm in resident)
+        self.X, self.Z, self.T = (CoeffArray(op, nm, nm in resident) for nm in NAMES)
+        self.pipe = BatchPipeline(op)
+        self._stage = None if len(resident) == len(NAMES) else KMajorStaging(op)
         self.dzk = torch.empty(be, dtype=torch.float32, device=dev)
-        op.to_batches(self.x, self.xk)
-        if state is not None and state.get("z") is not None:
-            op.to_batches(torch.as_tensor(as_host(state["z"], cshape, "state['z']"), device=dev), self.zk)
+        self.x = None
+        if self.X.resident:
+            self.x = x0 if self._x_on_gpu else torch.as_tensor(self._host_x, device=dev)
+            op.to_batches(self.x, self.X.dev)
         else:
-            op._fill(self.zk, 0.0)
+            self._stage.load(self._host_x.reshape(-1), self.X, self.pipe)
+        if state is not None and state.get("z") is not None:
+            z0 = as_host(state["z"], cshape, "state['z']")
+            if self.Z.resident:
+                op.to_batches(torch.as_tensor(z0, device=dev), self.Z.dev)
+            else:
+                self._stage.load(z0.reshape(-1), self.Z, self.pipe)
+        elif self.Z.resident:
+            op._fill(self.Z.dev, 0.0)
+        else:
+            self.Z.host.zero_()
 
         # S from the row sums A 1_S (spdhg_poisson.py:621-629)
         op._fill(self.D, 0.0)
@@ -191,21 +220,27 @@ class SPDHGPoisson:
         # T from the subsets' column sums over the counted points (spdhg_poisson.py:630-643)
         _lib.call("dfx_set_mask_ones", self.D.data_ptr(), _ptr(self.w), self.pw, self.D.numel(), s)
         c = float(np.float32(p / gamma))
-        for ib, bt in enumerate(op.batches):
-            tb = self.Tk.data_ptr() + 4 * ib * be
+        T = self.T
+
+        def t_batch(ib, s_):
+            tb, kb = T.ptr(ib, s_), op.batches[ib]["K_batch"]
             _lib.call("dfx_tinit", tb, be, s)
             for m in range(self.M):
                 op._adjoint_batch_k(self.D, ib, self.dzk.data_ptr(), subset=m)
-                _lib.call("dfx_batch_support", tb, self.dzk.data_ptr(), sp, npix, op.Kstride, bt["K_batch"], c, 2, s)
+                _lib.call("dfx_batch_support", tb, self.dzk.data_ptr(), sp, npix, op.Kstride, kb, c, 2, s)
             _lib.call("dfx_tfinal", tb, be, s)           # padding channels were never reached: T = 0 there
-        for ib, bt in enumerate(op.batches):            # x on the support, >= 0, padding 0
-            _lib.call("dfx_batch_support", self.xk.data_ptr() + 4 * ib * be, None, sp, npix, op.Kstride,
-                      bt["K_batch"], 0.0, 1, s)
+
+        self.pipe.run([], [T], t_batch)
+
+        def project_x(ib, s_):                          # x on the support, >= 0, padding 0
+            _lib.call("dfx_batch_support", self.X.ptr(ib, s_), None, sp, npix, op.Kstride,
+                      op.batches[ib]["K_batch"], 0.0, 1, s)
+
+        self.pipe.run([self.X], [self.X], project_x)
         if state is not None:
             self.y.copy_(torch.as_tensor(as_host(state["y"], dshape, "state['y']")))
             if state.get("z") is None:
-                for ib in range(nbt):
-                    op._adjoint_batch_k(self.y, ib, self.zk.data_ptr() + 4 * ib * be)
+                self.pipe.run([], [self.Z], lambda ib, s_: op._adjoint_batch_k(self.y, ib, self.Z.ptr(ib, s_)))
         self._t_setup = time.perf_counter() - self._t_start
         self._ep0 = int(state["epoch"]) if state is not None else 0
         self.iter_stats = []
@@ -213,8 +248,11 @@ class SPDHGPoisson:
         self._seq = self._epoch_sequence()
         self.xkb = None
         if op.precision == "bf16":       # the BF16 copy of x that the forward projections read
-            self.xkb = torch.empty(nbt * be, dtype=torch.bfloat16, device=dev)
-            _lib.call("dfx_f32_to_bf16", self.xk.data_ptr(), self.xkb.data_ptr(), nbt * be, s)
+            if self.X.resident:
+                self.xkb = torch.empty(nbt * be, dtype=torch.bfloat16, device=dev)
+                _lib.call("dfx_f32_to_bf16", self.X.dev.data_ptr(), self.xkb.data_ptr(), nbt * be, s)
+            else:
+                self.xkb = torch.empty(be, dtype=torch.bfloat16, device=dev)
         op.zero_subset_rows(self.D, self._seq[0])
         self._pass(None, self._seq[0])
 
@@ -259,9 +297,7 @@ class SPDHGPoisson:
             self.iter_stats.append(stats)
             stop = False
             if callback is not None:
-                op.from_batches(self.xk, self.x)
-                if not self._x_on_gpu:
-                    self._host_x[...] = self.x.cpu().numpy()
+                self._x_out()
                 stop = bool(callback(ep, self.x if self._x_on_gpu else self._host_x, stats))
             if verbose and want_f:
                 print(f"[spdhg epoch {ep:4d}] f={self._f:.8e} {time.perf_counter() - self._t_start:.1f} s",
@@ -269,22 +305,54 @@ class SPDHGPoisson:
             if stop:
                 break
 
+    def _x_out(self):
+        """x in the (K, Ny, Nx) layout of the caller's array (the CUDA x0, or the NumPy x0's device copy and x0)."""
+        op = self.op
+        if self.X.resident:
+            op.from_batches(self.X.dev, self.x)
+            if not self._x_on_gpu:
+                self._host_x[...] = self.x.cpu().numpy()
+        else:
+            self._stage.store(self.X, self._host_x.reshape(-1), self.pipe)
+
+    def _choose_resident(self):
+        """The coefficient arrays kept on the device (spdhg_poisson.py:411-428): all of them for a CUDA x0 or
+        resident="all"; for "auto" as many of x, z, T (in this order) as fit into the free device memory less the
+        streaming buffers and a margin."""
+        if self._x_on_gpu or self.resident == "all":
+            return set(NAMES)
+        if self.resident == "none":
+            return set()
+        if self.resident != "auto":
+            return set(self.resident) & set(NAMES)
+        op = self.op
+        be = op.batch_elems()
+        nbytes = 4 * be * len(op.batches)
+        free, _ = torch.cuda.mem_get_info(op.device)
+        # two slots per streamed array, the k-major staging buffer, the batch scratch and a BF16 batch of x
+        staging = (4 * 2 * len(NAMES) + 4 + 4 + 2) * be
+        n = int(max(0, free - staging - MARGIN_GB * 1024 ** 3) // nbytes)
+        return set(NAMES[:min(n, len(NAMES))])
+
     def _finish(self):
         op = self.op
-        op.from_batches(self.xk, self.x)
-        z = torch.empty(op.coeff_shape, dtype=torch.float32, device=op.device)
-        op.from_batches(self.zk, z)
-        self.state = {"epoch": self._ep0 + len(self.iter_stats), "z": z.cpu().numpy(), "y": self.y.cpu().numpy()}
-        del z
+        self._x_out()
+        if self.Z.resident:
+            z = torch.empty(op.coeff_shape, dtype=torch.float32, device=op.device)
+            op.from_batches(self.Z.dev, z)
+            z_host = z.cpu().numpy()
+            del z
+        else:
+            z_host = np.empty(op.coeff_shape, np.float32)
+            self._stage.store(self.Z, z_host.reshape(-1), self.pipe)
+        self.pipe.synchronize()
+        self.state = {"epoch": self._ep0 + len(self.iter_stats), "z": z_host, "y": self.y.cpu().numpy()}
         self.final_stats = {"epochs": len(self.iter_stats), "final_f": self._f, "setup_s": self._t_setup,
                             "rho": self.rho_used, "subsets": self.M, "resident": self.resident_used,
                             "time": time.perf_counter() - self._t_start, "tv": 0.0, "tv_prob": 0.0, **self.scales}
-        x = self.x
-        if not self._x_on_gpu:
-            self._host_x[...] = x.cpu().numpy()
-        out = x if self._x_on_gpu else self._host_x
+        out = self.x if self._x_on_gpu else self._host_x
         self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = None
-        self.xk = self.zk = self.Tk = self.dzk = self.xkb = None
+        self.X = self.Z = self.T = self.dzk = self.xkb = self._stage = None
         self.x = None
         return out
 

@@ -104,3 +104,167 @@ def streamer_for(op) -> Streamer:
     if op._streamer is None:
         op._streamer = Streamer(op)
     return op._streamer
+
+
+# ---------------------------------------------------------------------------------------------- solver state
+# A solver's coefficient-sized state (x, z, T of SPDHG) is kept in the operator's channel-fastest batch layout, batch
+# ib at element ib * npix * Kstride. An array that does not stay on the device lives in pinned host memory in that
+# same layout, so a batch crosses the host link as one contiguous copy in each direction, and two device slots hold
+# the batches in use (spdhg_poisson.py:287-296, streaming.py:255-309 of diffractom).
+
+class CoeffArray:
+    """One coefficient-sized state array: resident (one flat device array) or streamed (pinned host array + two
+    device slots). ptr(ib, s) is the device address of batch ib while it sits in slot s."""
+
+    def __init__(self, op, name, resident, dtype=torch.float32):
+        self.name = name
+        self.be = op.batch_elems()
+        self.n_batches = len(op.batches)
+        self.esize = torch.empty(0, dtype=dtype).element_size()
+        n = self.n_batches * self.be
+        if resident:
+            self.dev = torch.empty(n, dtype=dtype, device=op.device)
+            self.host = self.slots = None
+        else:
+            self.dev = None
+            self.host = torch.empty(n, dtype=dtype, pin_memory=True)
+            self.slots = [torch.empty(self.be, dtype=dtype, device=op.device) for _ in range(2)]
+        self.host_ready = [None] * self.n_batches    # event: the last download of batch ib into host has finished
+
+    @property
+    def resident(self):
+        return self.dev is not None
+
+    def ptr(self, ib, s):
+        if self.dev is not None:
+            return self.dev.data_ptr() + self.esize * ib * self.be
+        return self.slots[s].data_ptr()
+
+    def host_batch(self, ib):
+        return self.host[ib * self.be:(ib + 1) * self.be]
+
+    def nbytes_device(self):
+        t = [self.dev] if self.dev is not None else self.slots
+        return sum(x.numel() * x.element_size() for x in t)
+
+
+class BatchPipeline:
+    """Runs a pass over the orientation batches with the streamed state arrays moving through their two slots:
+    batch ib + 1 is uploaded (upload stream) while batch ib is computed (the operator's stream), and the updated
+    arrays of batch ib go back to host memory on the download stream. Ordering is by CUDA events only: an upload into
+    a slot waits for the compute and the download of the batch that used it before, and the upload of a batch waits
+    for the previous download of that batch's host memory; the host never waits."""
+
+    def __init__(self, op):
+        self.op = op
+        self.up = torch.cuda.Stream(op.device)
+        self.dn = torch.cuda.Stream(op.device)
+        self.slot_free = [None, None]
+
+    def _upload(self, arrays, ib):
+        s = ib % 2
+        if not arrays:
+            return None
+        with torch.cuda.stream(self.up):
+            if self.slot_free[s] is not None:
+                self.up.wait_event(self.slot_free[s])
+            for c in arrays:
+                if c.host_ready[ib] is not None:
+                    self.up.wait_event(c.host_ready[ib])
+                c.slots[s].copy_(c.host_batch(ib), non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(self.up)
+        return ev
+
+    def run(self, ups, dns, compute):
+        """compute(ib, s) launches batch ib's work on the operator's stream with the arrays of ups in slot s; the
+        arrays of dns are written back to host memory afterwards. Resident arrays in ups / dns are ignored."""
+        ups = [c for c in ups if not c.resident]
+        dns = [c for c in dns if not c.resident]
+        nbt = len(self.op.batches)
+        if not ups and not dns:
+            for ib in range(nbt):
+                compute(ib, ib % 2)
+            return
+        comp = self.op.stream()
+        ev = self._upload(ups, 0)
+        for ib in range(nbt):
+            s = ib % 2
+            nxt = self._upload(ups, ib + 1) if ib + 1 < nbt else None
+            if ev is not None:
+                comp.wait_event(ev)
+            elif self.slot_free[s] is not None:
+                comp.wait_event(self.slot_free[s])
+            compute(ib, s)
+            done = torch.cuda.Event()
+            done.record(comp)
+            if dns:
+                with torch.cuda.stream(self.dn):
+                    self.dn.wait_event(done)
+                    for c in dns:
+                        c.host_batch(ib).copy_(c.slots[s], non_blocking=True)
+                    done = torch.cuda.Event()
+                    done.record(self.dn)
+                for c in dns:
+                    c.host_ready[ib] = done
+            self.slot_free[s] = done
+            ev = nxt
+
+    def synchronize(self):
+        """Waits for every copy issued so far (before the host reads or writes a streamed array)."""
+        self.op.stream().synchronize()
+        self.up.synchronize()
+        self.dn.synchronize()
+
+
+class KMajorStaging:
+    """Conversions between a host (K, Ny, Nx) float32 array and a state array in the batch layout, one batch at a
+    time through a pinned buffer and a device buffer (set-up and results only)."""
+
+    def __init__(self, op):
+        self.op = op
+        n = op.npix * op.K_batch_max
+        self.pin = torch.empty(n, dtype=torch.float32, pin_memory=True)
+        self.dev = torch.empty(n, dtype=torch.float32, device=op.device)
+
+    def load(self, host_k, coeff, pipe, post=None):
+        """coeff <- host_k (flattened (K, Ny, Nx)); post(ib, ptr) runs on the batch on the device before it is
+        stored (e.g. the support projection)."""
+        op = self.op
+        comp = op.stream()
+        pipe.synchronize()
+        for ib, b in enumerate(op.batches):
+            n = op.npix * b["K_batch"]
+            k0 = op.npix * b["k_start"]
+            np.copyto(self.pin.numpy()[:n], host_k[k0:k0 + n])
+            with torch.cuda.stream(comp):
+                self.dev[:n].copy_(self.pin[:n], non_blocking=True)
+            dst = coeff.ptr(ib, 0)
+            op._call("dfx_gather_channels", self.dev.data_ptr(), dst, op.npix, 0, b["K_batch"], op.Kstride, op._s())
+            if post is not None:
+                post(ib, dst)
+            if not coeff.resident:
+                with torch.cuda.stream(comp):
+                    coeff.host_batch(ib).copy_(coeff.slots[0], non_blocking=True)
+            comp.synchronize()          # the pinned buffer and slot 0 are reused by the next batch
+        pipe.slot_free = [None, None]
+        coeff.host_ready = [None] * coeff.n_batches
+
+    def store(self, coeff, host_k, pipe):
+        """host_k (flattened (K, Ny, Nx)) <- coeff."""
+        op = self.op
+        comp = op.stream()
+        pipe.synchronize()
+        for ib, b in enumerate(op.batches):
+            n = op.npix * b["K_batch"]
+            k0 = op.npix * b["k_start"]
+            if not coeff.resident:
+                with torch.cuda.stream(comp):
+                    coeff.slots[0].copy_(coeff.host_batch(ib), non_blocking=True)
+            op._call("dfx_scatter_channels", coeff.ptr(ib, 0), self.dev.data_ptr(), op.npix, 0, b["K_batch"],
+                     op.Kstride, op._s())
+            with torch.cuda.stream(comp):
+                self.pin[:n].copy_(self.dev[:n], non_blocking=True)
+            comp.synchronize()
+            np.copyto(host_k[k0:k0 + n], self.pin.numpy()[:n])
+        pipe.slot_free = [None, None]

@@ -53,3 +53,53 @@ def test_spdhg_reproducible_resumed_and_numpy(golden):
     x = two.run(x, b, 2, diagnostics_interval=2, state=two.state)
     assert two.state["epoch"] == 6
     np.testing.assert_allclose(x, x_ref, rtol=1e-5, atol=1e-6 * np.abs(x_ref).max())
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+def test_spdhg_streamed_state_equals_resident(golden, precision):
+    """x, z, T streamed from pinned host memory through two device slots (any mix, resident= as in the reference's
+    test_spdhg_streamed_and_resumed) give the iterates, deviances and state of the device-resident run bit for bit;
+    a callback sees the same x; a run resumed from the state of a streamed run matches too."""
+    from diffractom_b200 import SinglePhaseForwardOperator, SPDHGPoisson
+    d = golden("al5_small")
+    cfg, mat, grid = case_inputs(d)
+    kw = {} if precision == "fp32" else {"precision": "bf16"}
+    op = SinglePhaseForwardOperator(cfg, mat, grid, 1e-5, normalized=True, quadrature=d["quadrature"], **kw)
+    assert len(op.batches) > 2
+    rng = np.random.default_rng(9)
+    x_true = (rng.random(op.coeff_shape) * (rng.random(op.coeff_shape) < 0.2) * op.support_mask()[None]
+              ).astype(np.float32)
+    b = rng.poisson(op.direct(torch.as_tensor(x_true, device="cuda")).cpu().numpy() * 50).astype(np.float32)
+    seen = {}
+
+    def cb(key):
+        def f(ep, x, stats):
+            seen.setdefault(key, []).append(np.array(x.cpu().numpy() if torch.is_tensor(x) else x, copy=True))
+        return f
+
+    ref = SPDHGPoisson(op, subsets=3, seed=1)
+    x_ref = ref.run(torch.zeros(op.coeff_shape, device="cuda"), b, 5, diagnostics_interval=2,
+                    callback=cb("ref")).cpu().numpy()
+    f_ref = [s["f"] for s in ref.iter_stats]
+    assert ref.resident_used == ("x", "z", "T")
+    for resident in ("none", ["x"], ["z", "T"], ["T"], "all"):
+        sp = SPDHGPoisson(op, subsets=3, seed=1, resident=resident)
+        x = sp.run(np.zeros(op.coeff_shape, np.float32), b, 5, diagnostics_interval=2, callback=cb(str(resident)))
+        want = {"none": (), "all": ("x", "z", "T")}.get(resident) if isinstance(resident, str) else \
+            tuple(n for n in ("x", "z", "T") if n in resident)
+        assert sp.final_stats["resident"] == want
+        assert np.array_equal(x, x_ref), resident
+        assert [s["f"] for s in sp.iter_stats] == f_ref, resident
+        assert np.array_equal(sp.state["z"], ref.state["z"]) and np.array_equal(sp.state["y"], ref.state["y"])
+        assert all(np.array_equal(a, r) for a, r in zip(seen[str(resident)], seen["ref"]))
+
+    def resumed(resident):
+        sp = SPDHGPoisson(op, subsets=3, seed=1, resident=resident)
+        x1 = sp.run(np.zeros(op.coeff_shape, np.float32), b, 3, diagnostics_interval=3)
+        x1 = sp.run(x1, b, 2, diagnostics_interval=2, state=sp.state)
+        assert sp.state["epoch"] == 5
+        return x1, sp.state
+
+    xa, sa = resumed("all")
+    xn, sn = resumed("none")
+    assert np.array_equal(xa, xn) and np.array_equal(sa["z"], sn["z"]) and np.array_equal(sa["y"], sn["y"])
