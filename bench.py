@@ -19,8 +19,10 @@ metric through the public API (SPDHGPoisson.run on NumPy arrays: uploads, set-up
 dominant kernel from CUDA events around its launches inside the timed region; cpu_baseline = the CPU oracle
 (oracle/oracle.c, float32, all host threads) on a bounded sample of the same epoch.
 
-With --gpus N > 1 (torchrun) every rank runs the whole reconstruction on its GPU (independent replicas, weak
-scaling); value is the sum over ranks of epochs / (max over ranks of the time).
+With --gpus N > 1 (torchrun, NCCL) the orientations are sharded: the grid holds N x K orientations and each rank
+builds the operator of its K (weak scaling: per-GPU work fixed); the only exchange is the all-reduce of the data rows
+each forward pass writes (diffractom_b200.sharding). value = N x epochs / (max over ranks of the time), i.e. epochs
+of K orientations per second summed over the GPUs, as at N = 1.
 """
 from __future__ import annotations
 
@@ -99,14 +101,20 @@ def phantom(op, w, seed=1):
     return x.reshape(op.coeff_shape)
 
 
-def counts(op, x_true, mean, seed=2):
-    """Poisson counts with the given mean of the prediction A x_true (scaled)."""
+def counts(op, x_true, mean, seed=2, dist=None):
+    """Poisson counts with the given mean of the prediction A x_true (scaled); with orientation shards the prediction
+    is summed over the ranks and rank 0's counts are broadcast."""
     import torch
     ax = op.direct(x_true)
+    if dist is not None:
+        dist.all_reduce(ax)
     lam = ax * (mean / float(ax.double().mean().item()))
     g = torch.Generator(device=op.device)
     g.manual_seed(seed)
-    return torch.poisson(lam, generator=g)
+    b = torch.poisson(lam, generator=g)
+    if dist is not None:
+        dist.broadcast(b, 0)
+    return b
 
 
 # ----------------------------------------------------------------------------------------------- clocks
@@ -235,31 +243,37 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
     from diffractom_b200 import SinglePhaseForwardOperator
-    cfg, mat, grid, w = make_problem(a.workload, K=a.K)
+    from diffractom_b200.sharding import ShardSum, shard_grid
+    k_per = a.K or WORKLOADS[a.workload]["K"]
+    cfg, mat, grid, w = make_problem(a.workload, K=k_per * world if world > 1 else a.K)
+    shards = None
+    if world > 1:
+        grid = shard_grid(grid, rank, world)
+        shards = ShardSum()
     t_build = time.perf_counter()
     op = SinglePhaseForwardOperator(cfg, mat, grid, w["max_gb"], normalized=True,
                                     precision="bf16" if a.precision in ("bf16", "both") else "fp32")
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
     op.precision = "fp32"
-    x_true = phantom(op, w)
-    b = counts(op, x_true, w["mean_counts"])
+    x_true = phantom(op, dict(w, grains=min(w["grains"], op.K)), seed=1 + rank)
+    b = counts(op, x_true, w["mean_counts"], dist=dist)
     del x_true
     torch.cuda.empty_cache()
 
     arms = {}
     for prec in (("fp32", "bf16") if a.precision == "both" else (a.precision,)):
-        arms[prec] = timed_epochs(op, w, b, a, prec, dist, local, world)
+        arms[prec] = timed_epochs(op, w, b, a, prec, dist, local, world, shards)
     head = arms["bf16" if "bf16" in arms else "fp32"]
 
     e2e = None
     if not a.no_e2e:
         op.precision = "bf16" if "bf16" in arms else "fp32"
-        e2e = measure_e2e(op, w, b, a.steps)
+        e2e = measure_e2e(op, w, b, a.steps, dist, world, shards)
         op.precision = "fp32"
     cpu = None
     if rank == 0 and not a.no_cpu:
@@ -267,12 +281,14 @@ def main():
         cpu = {"value": 1.0 / per_epoch, "unit": "epochs/s", "cores": threads, "kind": "port",
                "sample": desc + f" ({took:.1f} s of CPU time)"}
     if rank == 0:
-        cfg_line = {"workload": a.workload + (f" (K {a.K})" if a.K else ""), "K": op.K,
+        cfg_line = {"workload": a.workload + (f" (K {a.K})" if a.K else ""), "K": op.K * world, "K_per_gpu": op.K,
                     "pixels": f"{op.Nx}x{op.Ny}", "N_Omega": op.N_Omega,
                     "My": op.My, "N_eta": op.N_eta, "rings": op.N_peaks, "subsets": w["subsets"],
                     "batches": len(op.batches), "K_batch_max": op.K_batch_max, "pf_mode": op.pf_mode,
                     "pf_nnz": op.sparse_nnz, "precision_path": "bf16-tc" if "bf16" in arms else "fp32",
-                    "l2": "inputs larger than L2, no flush", "parallelism": f"replicas x{world}",
+                    "l2": "inputs larger than L2, no flush",
+                    "parallelism": "single GPU" if world == 1 else
+                    f"orientation shards x{world} (NCCL all-reduce of the forward's data rows)",
                     "operator_build_s": round(t_build, 2)}
         for prec, r in arms.items():
             cfg_line[f"{prec}_epochs_per_s"] = r["value"]
@@ -306,13 +322,13 @@ def main():
         dist.destroy_process_group()
 
 
-def timed_epochs(op, w, b, a, precision, dist, local, world):
+def timed_epochs(op, w, b, a, precision, dist, local, world, shards=None):
     """warmup untimed + steps timed SPDHG epochs with the operator in the given precision; the deviance of the final
     iterate with the float32 operator (float64 sum)."""
     import torch
     from diffractom_b200 import SPDHGPoisson, _lib
     op.precision = precision
-    sp = SPDHGPoisson(op, subsets=w["subsets"], seed=0)
+    sp = SPDHGPoisson(op, subsets=w["subsets"], seed=0, shards=shards)
     x0 = torch.zeros(op.coeff_shape, dtype=torch.float32, device=op.device)
     sp._setup(x0, b)
     never = 1 << 30
@@ -346,6 +362,8 @@ def timed_epochs(op, w, b, a, precision, dist, local, world):
     op.precision = "fp32"
     D = torch.empty(op.data_shape, dtype=torch.float32, device=op.device)
     op.direct_cl(x, D)
+    if shards is not None:
+        shards.all(D, op.stream())
     sp.b, sp.w, sp.pw, sp.g, sp.pg, sp.bg, sp.pbg = b, None, 0, None, 0, None, 0
     f_final = sp._deviance(D)
     del D
@@ -579,23 +597,30 @@ def serving_run(n, rate, px, omega, eta, rings, K, slots, budget_gb, max_epochs,
     return st
 
 
-def measure_e2e(op, w, b_dev, steps):
-    """The metric through the public API on host arrays: SPDHGPoisson.run(NumPy x0, NumPy b, steps epochs)."""
+def measure_e2e(op, w, b_dev, steps, dist=None, world=1, shards=None):
+    """The metric through the public API on host arrays: SPDHGPoisson.run(NumPy x0, NumPy b, steps epochs); with
+    orientation shards every rank runs it on its shard, the time is the maximum over the ranks."""
     import torch
     from diffractom_b200 import SPDHGPoisson
     b_host = torch.empty(b_dev.shape, dtype=torch.float32, pin_memory=True)
     b_host.copy_(b_dev)
     b_np = b_host.numpy()
     x0 = np.zeros(op.coeff_shape, np.float32)
-    sp = SPDHGPoisson(op, subsets=w["subsets"], seed=0)
+    sp = SPDHGPoisson(op, subsets=w["subsets"], seed=0, shards=shards)
     torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
     t0 = time.perf_counter()
     x = sp.run(x0, b_np, steps, diagnostics_interval=steps)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
+    if dist is not None:
+        tt = torch.tensor([dt], dtype=torch.float64, device=op.device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dt = float(tt.item())
     h2d = b_np.nbytes + x0.nbytes
     d2h = x.nbytes + sp.state["y"].nbytes + sp.state["z"].nbytes
-    return {"value": steps / dt, "unit": "epochs/s", "h2d_bytes_per_step": h2d // steps,
+    return {"value": world * steps / dt, "unit": "epochs/s", "h2d_bytes_per_step": h2d // steps,
             "d2h_bytes_per_step": d2h // steps,
             "includes": "upload of x0 and b, step sizes S and T (1 forward + M subset adjoints), epochs, final "
                         "deviance, download of x, y, z"}

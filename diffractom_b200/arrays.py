@@ -41,3 +41,47 @@ def as_host(a, shape, name):
 def ptr(t) -> int | None:
     """Device address of a tensor (None for None)."""
     return None if t is None else t.data_ptr()
+
+
+class stream_scope:
+    """Runs a block with an operator's stream current (operators built with queue=<torch.cuda.Stream>). The stream
+    first waits for the caller's current stream (inputs written there), and the caller's stream waits for it at the
+    end (results visible there), so torch work and the operator's kernels stay ordered whichever stream the caller
+    uses. Without a queue, or when the queue is already current, nothing changes."""
+
+    def __init__(self, op):
+        self.q = getattr(op, "queue", None)
+        self.dev = op.device
+        self.cur = None
+        self.ctx = None
+
+    def __enter__(self):
+        if self.q is None:
+            return self
+        cur = torch.cuda.current_stream(self.dev)
+        if cur == self.q:
+            return self
+        self.cur = cur
+        self.q.wait_stream(cur)
+        self.ctx = torch.cuda.stream(self.q)
+        self.ctx.__enter__()
+        return self
+
+    def __exit__(self, *exc):
+        if self.ctx is not None:
+            self.ctx.__exit__(*exc)
+            self.cur.wait_stream(self.q)
+            self.ctx = self.cur = None
+        return False
+
+
+def on_op_stream(method):
+    """Decorator: the method of an operator (self) or of a solver (self.op) runs inside stream_scope."""
+    import functools
+
+    @functools.wraps(method)
+    def wrapper(self, *args, **kwargs):
+        op = self.op if hasattr(self, "op") and not hasattr(self, "batches") else self
+        with stream_scope(op):
+            return method(self, *args, **kwargs)
+    return wrapper

@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .arrays import as_host, check_device, is_device
+from .arrays import as_host, check_device, is_device, on_op_stream
 from .solvers import Reducer, as_device_data, periodic, support_mask_to_device
 
 DEFAULT_REFRESH = (5, 10, 20, 40, 80, 160, 320, 640, 1280, 2560, 5120)
@@ -92,6 +92,7 @@ class FISTAPoisson:
         _lib.call("dfx_invert_metric", D.data_ptr(), x_tmp.data_ptr(), sp, npx, D.numel(), self.op._s())
 
     # ---- run
+    @on_op_stream
     def run(self, x0, b, niter, weights=None, gain=None, background=None, verbose=0, diagnostics_interval=10,
             state=None, callback=None):
         """As diffractom's FISTAPoisson.run (fista_poisson.py:414-...) for a CUDA x0 (updated in place) or a NumPy

@@ -27,7 +27,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .arrays import as_host, check_device, is_device
+from .arrays import as_host, check_device, is_device, on_op_stream, stream_scope
 from .geometry import OperatorGeometry, interleaved_subsets
 from .quadrature import DEFAULT_TOL
 
@@ -111,46 +111,47 @@ class SinglePhaseForwardOperator:
         self.pf_batch_max_gb = float(max_gb)
         self._kernel_id = 1 if radon_kernel == "trapezoid" else 0
 
-        # ---- device copies
-        dev = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=self.device)
-        self.coords_gpu = dev(self.coords_cpu)
-        self.poles_gpu = dev(self.poles_cpu)
-        self.axis_start_gpu = dev(self.axis_start_cpu, torch.int32)
-        self.axis_count_gpu = dev(self.axis_count_cpu)
-        self.inv_sigma2_gpu = dev(self.inv_sigma2_cpu)
-        self.norm_factor_gpu = dev(self.norm_factor_cpu)
-        self.quad_weights_gpu = None if self.quad_weights_cpu is None else dev(self.quad_weights_cpu)
-        self.intens_gpu = None if self.normalized else dev(self.intens_cpu)
-        self.geo_gpu = dev(self.radon_geo.geo)
-        self._pfg = _lib.PFGeometry(
-            self.coords_gpu.data_ptr(), self.poles_gpu.data_ptr(), self.axis_start_gpu.data_ptr(),
-            self.axis_count_gpu.data_ptr(), self.inv_sigma2_gpu.data_ptr(), self.norm_factor_gpu.data_ptr(),
-            None if self.quad_weights_gpu is None else self.quad_weights_gpu.data_ptr(),
-            None if self.intens_gpu is None else self.intens_gpu.data_ptr(),
-            self.N_Omega, self.N_eta, self.N_peaks, self.N_axes, self.N_Omega_subdivisions, self.N_eta_subdivisions,
-            self.K, float(self.pf_cut))
-        self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
-        self._build_ray_table()
-        self.omega_subsets = None
-        self._sub = []
-        self._streamer = None
+        with stream_scope(self):          # device work of the build on the operator's stream
+            # ---- device copies
+            dev = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=self.device)
+            self.coords_gpu = dev(self.coords_cpu)
+            self.poles_gpu = dev(self.poles_cpu)
+            self.axis_start_gpu = dev(self.axis_start_cpu, torch.int32)
+            self.axis_count_gpu = dev(self.axis_count_cpu)
+            self.inv_sigma2_gpu = dev(self.inv_sigma2_cpu)
+            self.norm_factor_gpu = dev(self.norm_factor_cpu)
+            self.quad_weights_gpu = None if self.quad_weights_cpu is None else dev(self.quad_weights_cpu)
+            self.intens_gpu = None if self.normalized else dev(self.intens_cpu)
+            self.geo_gpu = dev(self.radon_geo.geo)
+            self._pfg = _lib.PFGeometry(
+                self.coords_gpu.data_ptr(), self.poles_gpu.data_ptr(), self.axis_start_gpu.data_ptr(),
+                self.axis_count_gpu.data_ptr(), self.inv_sigma2_gpu.data_ptr(), self.norm_factor_gpu.data_ptr(),
+                None if self.quad_weights_gpu is None else self.quad_weights_gpu.data_ptr(),
+                None if self.intens_gpu is None else self.intens_gpu.data_ptr(),
+                self.N_Omega, self.N_eta, self.N_peaks, self.N_axes, self.N_Omega_subdivisions, self.N_eta_subdivisions,
+                self.K, float(self.pf_cut))
+            self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
+            self._build_ray_table()
+            self.omega_subsets = None
+            self._sub = []
+            self._streamer = None
 
-        # ---- batches and the sparse PF matrix (SPFO:1026-1094, 1207-1373)
-        self.get_pf_batches_for_material()
-        self.pf_mode = pf_mode
-        self.sparse_batches = None
-        self.pf_storage = None
-        if sparse_max_gb is None:
-            sparse_max_gb = self.default_sparse_budget_gb()
-        self._pf_build = dict(mode=pf_mode, max_fill=sparse_max_fill, max_gb=sparse_max_gb,
-                              max_fill_partial=sparse_max_fill_partial)
-        self.build_sparse_pf(**self._pf_build)
-        if precision not in ("fp32", "bf16"):
-            raise ValueError(f"precision must be 'fp32' or 'bf16', not {precision!r}")
-        self.precision = precision
-        self.pf_bf16 = None
-        if precision == "bf16":
-            self.build_dense_bf16_pf()
+            # ---- batches and the sparse PF matrix (SPFO:1026-1094, 1207-1373)
+            self.get_pf_batches_for_material()
+            self.pf_mode = pf_mode
+            self.sparse_batches = None
+            self.pf_storage = None
+            if sparse_max_gb is None:
+                sparse_max_gb = self.default_sparse_budget_gb()
+            self._pf_build = dict(mode=pf_mode, max_fill=sparse_max_fill, max_gb=sparse_max_gb,
+                                  max_fill_partial=sparse_max_fill_partial)
+            self.build_sparse_pf(**self._pf_build)
+            if precision not in ("fp32", "bf16"):
+                raise ValueError(f"precision must be 'fp32' or 'bf16', not {precision!r}")
+            self.precision = precision
+            self.pf_bf16 = None
+            if precision == "bf16":
+                self.build_dense_bf16_pf()
 
     # ------------------------------------------------------------------ small helpers
     def stream(self) -> torch.cuda.Stream:
@@ -509,6 +510,7 @@ class SinglePhaseForwardOperator:
         self._pf_tc_forward(self._z(e["n"]), e["omegas"], e["n"], data)
 
     # ------------------------------------------------------------------ omega subsets
+    @on_op_stream
     def set_omega_subsets(self, subsets):
         """Subsets of the rotation angles for the subset forms direct_cl / adjoint_cl(subset=m) (SPFO:1541-1599):
         an int M (angle i in subset i % M) or a list of index arrays; returns the sorted index arrays."""
@@ -555,6 +557,7 @@ class SinglePhaseForwardOperator:
             raise ValueError("no omega subsets defined: call set_omega_subsets first")
         return int(subset)
 
+    @on_op_stream
     def zero_subset_rows(self, data, subset):
         """data rows of the angles of subset m <- 0 (SPFO:1638-1644)."""
         m = self._subset(subset)
@@ -565,6 +568,7 @@ class SinglePhaseForwardOperator:
         self._call("dfx_fill_f32", t.data_ptr(), float(value), t.numel(), self._s())
 
     # ------------------------------------------------------------------ forward / adjoint
+    @on_op_stream
     def direct_cl(self, coeffs, data, subset=None):
         """In-place forward operator data = PF @ Radon(coeffs) (SPFO:1646-1662); subset=m: only the rows of the angles
         of subset m are written (the other rows are left as they are)."""
@@ -599,6 +603,7 @@ class SinglePhaseForwardOperator:
                    val.data_ptr(), data.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My,
                    self.N_seg, self.Kstride, Kb, compact, s)
 
+    @on_op_stream
     def adjoint_cl(self, data, coeffs, subset=None):
         """In-place adjoint coeffs = A^T data (SPFO:1800-1817); subset=m: A_m^T (rows of subset m only)."""
         check_device(data, self.data_shape, "data")
@@ -691,6 +696,7 @@ class SinglePhaseForwardOperator:
             self._call("dfx_scatter_channels", in_k.data_ptr() + 4 * ib * self.batch_elems(), coeffs.data_ptr(),
                        self.npix, b["k_start"], b["K_batch"], self.Kstride, s)
 
+    @on_op_stream
     def adjoint_batches_cl(self, data, out_batch, update):
         """The adjoint one batch at a time into the first Kb * Ny * Nx elements of out_batch, then update(k0, Kb)
         (SPFO:1819-1838)."""
@@ -700,6 +706,7 @@ class SinglePhaseForwardOperator:
             self._adjoint_batch(data, ib, out_batch, 0, self.K_batch_max)
             update(b["k_start"], b["K_batch"])
 
+    @on_op_stream
     def direct(self, coeffs):
         """Forward operator allocating its output: a CUDA tensor for a CUDA tensor; for a NumPy array (K, Ny, Nx) the
         coefficients are streamed to the GPU batch by batch and a NumPy array is returned (SPFO:1107-1127)."""
@@ -713,6 +720,7 @@ class SinglePhaseForwardOperator:
         streamer_for(self).forward(x.reshape(-1), data)
         return data.cpu().numpy()
 
+    @on_op_stream
     def adjoint(self, data):
         """Adjoint allocating its output (SPFO:1777-1796): CUDA tensor in, CUDA tensor out; NumPy in, NumPy out with
         the coefficients streamed to the host batch by batch."""
@@ -745,6 +753,7 @@ class SinglePhaseForwardOperator:
             self._streamer.release()
             self._streamer = None
 
+    @on_op_stream
     def free_memory(self):
         """Release the operator's device buffers (SPFO:957-1020)."""
         self.release_omega_subsets()
@@ -760,6 +769,11 @@ class SinglePhaseForwardOperator:
 def estimate_L_power(op, niter: int = 20, seed: int = 0, eps: float = 1e-30, verbose: int = 1) -> float:
     """Lipschitz constant ||A^T A|| by power iteration (SPFO:2136-2206); the start vector is the reference's
     (a standard normal (Nx, Ny, K) draw stored pixel-fastest) and the dot products are float64 (dfx_dot_f64)."""
+    with stream_scope(op):
+        return _estimate_L_power(op, niter, seed, eps, verbose)
+
+
+def _estimate_L_power(op, niter, seed, eps, verbose):
     if niter < 1:
         raise ValueError("niter must be >= 1")
     rng = np.random.default_rng(seed)

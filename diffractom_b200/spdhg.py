@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .arrays import as_host, check_device, is_device
+from .arrays import as_host, check_device, is_device, on_op_stream
 from .solvers import Reducer, as_device_data, periodic, support_mask_to_device
 from .streaming import BatchPipeline, CoeffArray, KMajorStaging
 
@@ -39,11 +39,13 @@ class SPDHGPoisson:
     """SPDHG over omega subsets for the Poisson deviance (module docstring)."""
 
     def __init__(self, operator, subsets=8, prox_kind="nonneg", lam=0.0, support="fov", eps_counts=1e-3, rho="auto",
-                 seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None):
+                 seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None, shards=None):
         """Arguments as diffractom's SPDHGPoisson (spdhg_poisson.py:301-302). resident ("auto", "all", "none" or a
         list of names from ("x", "z", "T")): which coefficient arrays of a run with a NumPy x0 stay on the device;
         the others are streamed from pinned host memory (a CUDA x0 keeps all three on the device). tv > 0 (the TV
-        block) is not provided."""
+        block) is not provided. shards (this package's extension; a sharding.ShardSum): the operator holds one
+        orientation shard of a process group, and the forward's data rows are summed over the shards after each
+        pass; every rank passes the same seed and subsets."""
         if prox_kind not in ("nonneg", "nonneg_l1"):
             raise ValueError("SPDHGPoisson supports prox_kind 'nonneg' and 'nonneg_l1'")
         if not (resident in ("auto", "all", "none") or set(resident) <= set(NAMES + ("qx", "qy"))):
@@ -64,6 +66,7 @@ class SPDHGPoisson:
         self._inv_p_data = float(self.M)
         self._last = None
         self.support_gpu = support_mask_to_device(operator, support, operator.device)
+        self.shards = shards
         self.state = None
 
     # ---------------------------------------------------------------- schedule
@@ -107,6 +110,18 @@ class SPDHGPoisson:
 
         upd = adj is not None
         self.pipe.run([X, Z, T] if upd else [X], [X, Z] if upd else [], compute)
+        if fwd is not None:
+            self._sum_shards(fwd)
+
+    def _sum_shards(self, fwd):
+        """The forward rows just written, summed over the orientation shards (the pass's only exchange)."""
+        if self.shards is None:
+            return
+        op = self.op
+        if fwd == "full":
+            self.shards.all(self.D, op.stream())
+        else:
+            self.shards.rows(self.D, op._sub[op._subset(fwd)]["omegas"], op.stream())
 
     def _pass_bf16(self, adj, fwd):
         """The pass of an operator with precision "bf16": one tensor-core launch takes the dual change of subset adj
@@ -134,11 +149,13 @@ class SPDHGPoisson:
         self.pipe.run([X, Z, T] if upd else [X], [X, Z] if upd else [], compute)
         if fwd is not None:
             op._bf16_forward_rows(fwd, self.D)
+            self._sum_shards(fwd)
 
     def _deviance(self, mu):
         return self.red.deviance(mu, self.b, self.w, self.pw, self.g, self.pg, self.bg, self.pbg, self.eps_counts)
 
     # ---------------------------------------------------------------- run
+    @on_op_stream
     def run(self, x0, b, n_epochs, weights=None, gain=None, background=None, verbose=0, diagnostics_interval=1,
             callback=None, state=None):
         """As diffractom's SPDHGPoisson.run (spdhg_poisson.py:513-751). x0: a CUDA tensor (updated in place and
@@ -147,6 +164,7 @@ class SPDHGPoisson:
         self._iterate(n_epochs, verbose, diagnostics_interval, callback)
         return self._finish()
 
+    @on_op_stream
     def _setup(self, x0, b, weights=None, gain=None, background=None, state=None):
         """Upload, step sizes S and T, support projection, warm start (spdhg_poisson.py:520-662)."""
         self._t_start = time.perf_counter()
@@ -211,6 +229,7 @@ class SPDHGPoisson:
         for ib, bt in enumerate(op.batches):
             _lib.call("dfx_batch_support", self.dzk.data_ptr(), None, sp, npix, op.Kstride, bt["K_batch"], 0.0, 0, s)
             op._direct_batch_k(self.dzk.data_ptr(), ib, self.D)
+        self._sum_shards("full")
         rs, rn = self.red.mean_counted(self.D, self.w, self.pw)
         bs, bn = self.red.mean_counted(self.b, self.w, self.pw)
         self.scales = {"row_sum_mean": rs / max(rn, 1.0), "b_mean": bs / max(bn, 1.0),
@@ -256,6 +275,7 @@ class SPDHGPoisson:
         op.zero_subset_rows(self.D, self._seq[0])
         self._pass(None, self._seq[0])
 
+    @on_op_stream
     def _iterate(self, n_epochs, verbose=0, diagnostics_interval=1, callback=None, final=True):
         """n_epochs epochs (spdhg_poisson.py:664-719). final=False: the last of them is not the run's last (no
         closing full forward unless diagnostics fall there), so that epochs can be run in several calls."""
@@ -334,6 +354,7 @@ class SPDHGPoisson:
         n = int(max(0, free - staging - MARGIN_GB * 1024 ** 3) // nbytes)
         return set(NAMES[:min(n, len(NAMES))])
 
+    @on_op_stream
     def _finish(self):
         op = self.op
         self._x_out()

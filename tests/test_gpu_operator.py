@@ -201,3 +201,25 @@ def test_ray_table_forward_equals_footprint_forward(golden, name):
     op._radon_fwd(img.data_ptr(), zb.data_ptr(), None, R, kb, sld=ks + 8)
     assert torch.equal(zb[:, :, :ks], a.to(torch.bfloat16))
     assert op.ray_taps == int(op._ray_rp[-1].item()) > 0
+
+
+def test_operator_on_its_own_queue_equals_current_stream(golden):
+    """An operator built with queue=<a stream that is not current> gives the bits of one on the current stream: its
+    build, forward, adjoint (device and NumPy) and an SPDHG run order themselves against the caller's stream."""
+    from diffractom_b200 import SPDHGPoisson
+    d = golden("al5_small")
+    op = make_operator(d)
+    opq = make_operator(d, queue=torch.cuda.Stream())
+    assert opq.stream() != torch.cuda.current_stream()
+    rng = np.random.default_rng(4)
+    c = torch.as_tensor(rng.random(op.coeff_shape).astype(np.float32), device="cuda")
+    fwd, fwdq = op.direct(c), opq.direct(c)
+    assert torch.equal(fwd, fwdq)
+    assert torch.equal(op.adjoint(fwd), opq.adjoint(fwdq))
+    assert np.array_equal(op.direct(c.cpu().numpy()), opq.direct(c.cpu().numpy()))
+    b = np.random.default_rng(5).poisson(fwd.cpu().numpy() * 20).astype(np.float32)
+    xs = []
+    for o in (op, opq):
+        sp = SPDHGPoisson(o, subsets=3, seed=2)
+        xs.append(sp.run(torch.zeros(o.coeff_shape, device="cuda"), b, 2, diagnostics_interval=1).cpu().numpy())
+    assert np.array_equal(xs[0], xs[1])
