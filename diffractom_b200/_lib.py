@@ -39,8 +39,8 @@ SIGNATURES = {
     "dfx_radon_backward_bf16": ([P, L, P, P, I, I, I, I, I, I, I, I, S], c_int),
     "dfx_radon_backward_spdhg_bf16": ([P, L, P, I, I, I, I, I, I, I, I, P, P, P, F, F, P, S], c_int),
     "dfx_radon_backward_spdhg_tc": ([P, L, P, I, I, I, I, I, I, I, I, P, P, P, F, F, P, S], c_int),
-    "dfx_radon_table_count": ([P, I, I, I, I, I, P, S], c_int),
-    "dfx_radon_table_fill": ([P, I, I, I, I, I, P, P, S], c_int),
+    "dfx_radon_table_count": ([P, I, I, I, I, I, P, P, S], c_int),
+    "dfx_radon_table_fill": ([P, I, I, I, I, I, P, P, P, S], c_int),
     "dfx_radon_forward_table": ([P, P, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_radon_forward_table_bf16": ([P, P, L, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_radon_forward_table_bf16_bf16": ([P, P, L, P, P, P, I, I, I, I, F, S], c_int),

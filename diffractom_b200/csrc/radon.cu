@@ -146,11 +146,14 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_v4(
 
 // ---- ray table: the non-zero taps of every (angle, bin) in the order radon_forward_v4 visits them (rows v, then
 // pixels u ascending), as (pixel index, weight bits). The geometry of an operator is fixed, so the table is built
-// once; the table-driven forward then spends its instructions on loads and FMAs only, with four taps in flight.
+// once; the table-driven forward then spends its instructions on loads and FMAs only, with many taps in flight.
+// supp (optional, one byte per pixel): only the taps of pixels inside the support; for images that are zero outside
+// it (a solver's iterates projected onto the support) the forward through this table adds exactly the same terms
+// minus zeros, so it gives the same bits.
 template <int KERNEL>
 __global__ void ray_table_kernel(const float4 *__restrict__ geo, int n_angles, int nx, int ny, int ns,
-                                 int32_t *__restrict__ counts, const int32_t *__restrict__ row_ptr,
-                                 int2 *__restrict__ entries)
+                                 const uint8_t *__restrict__ supp, int32_t *__restrict__ counts,
+                                 const int32_t *__restrict__ row_ptr, int2 *__restrict__ entries)
 {
     const int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;      // a * ns + s
     if (row >= (int64_t)n_angles * ns) return;
@@ -170,10 +173,9 @@ __global__ void ray_table_kernel(const float4 *__restrict__ geo, int n_angles, i
         for (int u = u0; u <= u1; ++u) {
             const float w = tap_weight<KERNEL>(g, __fsub_rn(__fmaf_rn(g.A, (float)u, c), fs));
             if (w == 0.0f) continue;
-            if (row_ptr) {
-                const int pix = g.rows_are_y ? u + nx * v : v + nx * u;
-                entries[pos++] = make_int2(pix, __float_as_int(w));
-            }
+            const int pix = g.rows_are_y ? u + nx * v : v + nx * u;
+            if (supp && !supp[pix]) continue;
+            if (row_ptr) entries[pos++] = make_int2(pix, __float_as_int(w));
             ++n;
         }
     }
@@ -202,13 +204,13 @@ __device__ __forceinline__ void accraw(float (&a)[CPL], float w, const Raw8<__nv
 
 // Table-driven forward: warp per (angle, bin, 256 channels), angle a of the launch = angles[a] of the table (angles
 // NULL: a); the same taps, weights and summation order as radon_forward_v4, so the same bits. U taps are loaded
-// before their FMAs.
+// before their FMAs (16 for a BF16 image: 0.32 -> 0.28 ms per ti256 launch of 18 angles x 1012 channels).
 template <typename ST, typename IT>
 __global__ void __launch_bounds__(32 * WARPS) radon_forward_table(
     const IT *__restrict__ img, ST *__restrict__ sino, int64_t sld, const int32_t *__restrict__ row_ptr,
     const int2 *__restrict__ entries, const int32_t *__restrict__ angles, int ns, int kstride, int kb, float scale)
 {
-    constexpr int U = 8;
+    constexpr int U = sizeof(IT) == 2 ? 16 : 8;   // taps in flight: 16 x 16 bytes (BF16), 8 x 32 bytes (float32)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = blockIdx.x * WARPS + warp;
     const int al = blockIdx.y;
@@ -576,7 +578,7 @@ extern "C" int dfx_radon_backward_spdhg_bf16(const void *sino_bf16, int64_t sino
 }
 
 extern "C" int dfx_radon_table_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
-                                     int32_t *counts, void *stream)
+                                     const uint8_t *supp, int32_t *counts, void *stream)
 {
     DFX_REQUIRE(geo && counts && ((uintptr_t)geo % 16) == 0, "radon_table: null or misaligned pointer");
     DFX_REQUIRE(n_angles > 0 && nx > 0 && ny > 0 && n_det > 0 && (kernel == 0 || kernel == 1),
@@ -585,15 +587,15 @@ extern "C" int dfx_radon_table_count(const float *geo, int n_angles, int nx, int
     DFX_REQUIRE(cdiv(rows, 128) < 2147483647LL, "radon_table: too many rows");
     if (kernel == 1)
         ray_table_kernel<1><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
-            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, counts, nullptr, nullptr);
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, counts, nullptr, nullptr);
     else
         ray_table_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
-            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, counts, nullptr, nullptr);
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, counts, nullptr, nullptr);
     return launch_status("radon_table_count");
 }
 
 extern "C" int dfx_radon_table_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
-                                    const int32_t *row_ptr, int32_t *entries, void *stream)
+                                    const uint8_t *supp, const int32_t *row_ptr, int32_t *entries, void *stream)
 {
     DFX_REQUIRE(geo && row_ptr && entries && ((uintptr_t)geo % 16) == 0 && ((uintptr_t)entries % 8) == 0,
                 "radon_table: null or misaligned pointer");
@@ -603,10 +605,10 @@ extern "C" int dfx_radon_table_fill(const float *geo, int n_angles, int nx, int 
     int2 *e = reinterpret_cast<int2 *>(entries);
     if (kernel == 1)
         ray_table_kernel<1><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
-            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, nullptr, row_ptr, e);
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, nullptr, row_ptr, e);
     else
         ray_table_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
-            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, nullptr, row_ptr, e);
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, nullptr, row_ptr, e);
     return launch_status("radon_table_fill");
 }
 

@@ -131,7 +131,8 @@ class SinglePhaseForwardOperator:
                 self.N_Omega, self.N_eta, self.N_peaks, self.N_axes, self.N_Omega_subdivisions, self.N_eta_subdivisions,
                 self.K, float(self.pf_cut))
             self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
-            self._build_ray_table()
+            self._ray_rp, self._ray_ent, self.ray_taps = self._build_ray_table()
+            self._ray_supp = {}
             self.omega_subsets = None
             self._sub = []
             self._streamer = None
@@ -172,14 +173,16 @@ class SinglePhaseForwardOperator:
     def detector_shifts(self):
         return self.geometry.detector_shifts()
 
-    def _build_ray_table(self):
+    def _build_ray_table(self, supp=None):
         """The projector's non-zero taps per (angle, bin) (dfx_radon_table_*): the forward projection then reads
-        (pixel, weight) pairs instead of evaluating the footprint of every candidate pixel in every call."""
+        (pixel, weight) pairs instead of evaluating the footprint of every candidate pixel in every call. supp (a
+        uint8 (Ny * Nx) device mask): the taps of the support's pixels only. Returns (row_ptr, entries, taps)."""
         R, ns = self.N_Omega, self.My
         n = R * ns
         s = self._s()
+        sp = None if supp is None else supp.data_ptr()
         rp = torch.empty(n + 1, dtype=torch.int32, device=self.device)
-        self._call("dfx_radon_table_count", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id,
+        self._call("dfx_radon_table_count", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id, sp,
                    rp.data_ptr(), s)
         self.stream().synchronize()
         cnt64 = rp[:n].to(torch.int64).sum()
@@ -190,20 +193,34 @@ class SinglePhaseForwardOperator:
         scr = self.scratch(nb)
         self._call("dfx_scan_exclusive_i32", rp.data_ptr(), rp.data_ptr(), n, scr.data_ptr(), nb, s)
         ent = torch.empty(2 * max(total, 1), dtype=torch.int32, device=self.device)
-        self._call("dfx_radon_table_fill", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id,
+        self._call("dfx_radon_table_fill", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id, sp,
                    rp.data_ptr(), ent.data_ptr(), s)
-        self._ray_rp, self._ray_ent, self.ray_taps = rp, ent, total
+        return rp, ent, total
 
-    def _radon_fwd(self, src_ptr, dst_ptr, om, n_ang, kb, sld=None):
-        """Forward projection of a channel-fastest batch through the ray table: angles om (int32 device tensor of
-        angle indices, None: all) into float32 (sld None) or BF16 (row stride sld) sinogram rows."""
+    @on_op_stream
+    def support_ray_table(self, supp):
+        """The ray table restricted to a support mask (uint8 (Ny * Nx) device tensor), built once per mask content
+        and kept: the solvers' forward projections of iterates that are zero outside the support read it (same
+        bits, fewer taps)."""
+        key = bytes(supp.cpu().numpy())
+        hit = self._ray_supp.get(key)
+        if hit is None:
+            hit = self._build_ray_table(supp)
+            self._ray_supp[key] = hit
+        return hit
+
+    def _radon_fwd(self, src_ptr, dst_ptr, om, n_ang, kb, sld=None, ray=None):
+        """Forward projection of a channel-fastest batch through the ray table (ray: (row_ptr, entries, taps) of a
+        support table, None: the full one): angles om (int32 device tensor of angle indices, None: all) into float32
+        (sld None) or BF16 (row stride sld) sinogram rows."""
         om_ptr = None if om is None else om.data_ptr()
+        rp, ent = (self._ray_rp, self._ray_ent) if ray is None else ray[:2]
         if sld is None:
-            self._call("dfx_radon_forward_table", src_ptr, dst_ptr, self._ray_rp.data_ptr(), self._ray_ent.data_ptr(),
+            self._call("dfx_radon_forward_table", src_ptr, dst_ptr, rp.data_ptr(), ent.data_ptr(),
                        om_ptr, n_ang, self.My, self.Kstride, kb, float(self.radon_geo.scale), self._s())
         else:
-            self._call("dfx_radon_forward_table_bf16", src_ptr, dst_ptr, sld, self._ray_rp.data_ptr(),
-                       self._ray_ent.data_ptr(), om_ptr, n_ang, self.My, self.Kstride, kb,
+            self._call("dfx_radon_forward_table_bf16", src_ptr, dst_ptr, sld, rp.data_ptr(),
+                       ent.data_ptr(), om_ptr, n_ang, self.My, self.Kstride, kb,
                        float(self.radon_geo.scale), self._s())
 
     @property
@@ -492,16 +509,17 @@ class SinglePhaseForwardOperator:
                    self.My, self.Kstride, self.batches[ib]["K_batch"], self._kernel_id, int(self.radon_geo.n_taps),
                    x_ptr, z_ptr, T_ptr, float(inv_p), float(lam), xb_ptr, self._s())
 
-    def _bf16_forward_sino(self, subset, ib, src_ptr, src_bf16=False):
+    def _bf16_forward_sino(self, subset, ib, src_ptr, src_bf16=False, ray=None):
         """Radon transform of batch ib (channel-fastest at src_ptr, float32 or BF16) for the angles of subset m into
-        Z."""
+        Z (ray: a support ray table for images that are zero outside the support)."""
         e = self._sub[self._subset(subset)]
         if not src_bf16:
             self._radon_forward_bf16(src_ptr, ib, self._z(e["n"]), e["omegas"], e["n"])
             return
         z = self._z(e["n"])
+        rp, ent = (self._ray_rp, self._ray_ent) if ray is None else ray[:2]
         self._call("dfx_radon_forward_table_bf16_bf16", src_ptr, z.data_ptr() + 2 * ib * self.Kstride, self.Ktot,
-                   self._ray_rp.data_ptr(), self._ray_ent.data_ptr(), e["omegas"].data_ptr(), e["n"], self.My,
+                   rp.data_ptr(), ent.data_ptr(), e["omegas"].data_ptr(), e["n"], self.My,
                    self.Kstride, self.batches[ib]["K_batch"], float(self.radon_geo.scale), self._s())
 
     def _bf16_forward_rows(self, subset, data):
@@ -647,12 +665,13 @@ class SinglePhaseForwardOperator:
         e = self._sub[m]
         return e["geo"], e["n"], e["omegas"], m
 
-    def _direct_batch_k(self, src_ptr, ib, data, subset=None):
-        """Add the forward projection of batch ib, given channel-fastest at device address src_ptr, to data."""
+    def _direct_batch_k(self, src_ptr, ib, data, subset=None, ray=None):
+        """Add the forward projection of batch ib, given channel-fastest at device address src_ptr, to data (ray: a
+        support ray table for images that are zero outside the support)."""
         Kb = self.batches[ib]["K_batch"]
         s = self._s()
         geo, n_ang, om, m = self._geo_of(subset)
-        self._radon_fwd(src_ptr, self.coeffs_sino_C.data_ptr(), om, n_ang, Kb)
+        self._radon_fwd(src_ptr, self.coeffs_sino_C.data_ptr(), om, n_ang, Kb, ray=ray)
         rp, col, val, compact = self._pf_batch(ib, True, m)
         self._call("dfx_spmm_pf_forward", self.coeffs_sino_C.data_ptr(), rp.data_ptr(), col.data_ptr(),
                    val.data_ptr(), data.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My,
@@ -758,6 +777,7 @@ class SinglePhaseForwardOperator:
         """Release the operator's device buffers (SPFO:957-1020)."""
         self.release_omega_subsets()
         self.release_streamer()
+        self._ray_supp = {}
         self.sparse_batches = None
         self.coeffs_sino_C = self._img_k = None
         self._gen_col = self._gen_val = None

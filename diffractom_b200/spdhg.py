@@ -38,6 +38,10 @@ MARGIN_GB = 1.5          # resident="auto": device memory left free (spdhg_poiss
 class SPDHGPoisson:
     """SPDHG over omega subsets for the Poisson deviance (module docstring)."""
 
+    # the iterates are zero outside the support (projected at set-up, T = 0 there), so the forward projections read
+    # the operator's ray table restricted to the support: the same sums without the zero terms
+    use_support_table = True
+
     def __init__(self, operator, subsets=8, prox_kind="nonneg", lam=0.0, support="fov", eps_counts=1e-3, rho="auto",
                  seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None, shards=None):
         """Arguments as diffractom's SPDHGPoisson (spdhg_poisson.py:301-302). resident ("auto", "all", "none" or a
@@ -106,7 +110,7 @@ class SPDHGPoisson:
                 op._adjoint_update_batch(self.D, ib, adj, xp, Z.ptr(ib, s), T.ptr(ib, s), self._inv_p_data,
                                          self.lam)
             if fwd is not None:
-                op._direct_batch_k(xp, ib, self.D, sub)
+                op._direct_batch_k(xp, ib, self.D, sub, ray=self._ray)
 
         upd = adj is not None
         self.pipe.run([X, Z, T] if upd else [X], [X, Z] if upd else [], compute)
@@ -143,7 +147,7 @@ class SPDHGPoisson:
             elif not X.resident:
                 _lib.call("dfx_f32_to_bf16", X.ptr(ib, s), xb, be, op._s())
             if fwd is not None:
-                op._bf16_forward_sino(fwd, ib, xb, src_bf16=True)
+                op._bf16_forward_sino(fwd, ib, xb, src_bf16=True, ray=self._ray)
 
         upd = adj is not None
         self.pipe.run([X, Z, T] if upd else [X], [X, Z] if upd else [], compute)
@@ -224,11 +228,12 @@ class SPDHGPoisson:
         else:
             self.Z.host.zero_()
 
+        self._ray = op.support_ray_table(supp) if supp is not None and self.use_support_table else None
         # S from the row sums A 1_S (spdhg_poisson.py:621-629)
         op._fill(self.D, 0.0)
         for ib, bt in enumerate(op.batches):
             _lib.call("dfx_batch_support", self.dzk.data_ptr(), None, sp, npix, op.Kstride, bt["K_batch"], 0.0, 0, s)
-            op._direct_batch_k(self.dzk.data_ptr(), ib, self.D)
+            op._direct_batch_k(self.dzk.data_ptr(), ib, self.D, ray=self._ray)
         self._sum_shards("full")
         rs, rn = self.red.mean_counted(self.D, self.w, self.pw)
         bs, bn = self.red.mean_counted(self.b, self.w, self.pw)
@@ -373,7 +378,7 @@ class SPDHGPoisson:
                             "time": time.perf_counter() - self._t_start, "tv": 0.0, "tv_prob": 0.0, **self.scales}
         out = self.x if self._x_on_gpu else self._host_x
         self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = None
-        self.X = self.Z = self.T = self.dzk = self.xkb = self._stage = None
+        self.X = self.Z = self.T = self.dzk = self.xkb = self._stage = self._ray = None
         self.x = None
         return out
 

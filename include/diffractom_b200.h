@@ -97,10 +97,12 @@ int dfx_radon_backward_spdhg_tc(const void *sino_bf16, int64_t sino_ld, const fl
 /* Ray table of a projector geometry (no reference counterpart: the reference evaluates the taps in every call): the
  * non-zero taps of every (angle a, bin s), row a * n_det + s, as int32 pairs (pixel index, float32 weight bits) in
  * the order the forward projection sums them. count: counts[row] = taps of the row (row_ptr = exclusive scan, at
- * most 2^31 - 1 in total); fill: entries (2 int32 per tap, 8-byte aligned) at row_ptr[row] .. row_ptr[row + 1]. */
-int dfx_radon_table_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel, int32_t *counts,
-                          void *stream);
-int dfx_radon_table_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
+ * most 2^31 - 1 in total); fill: entries (2 int32 per tap, 8-byte aligned) at row_ptr[row] .. row_ptr[row + 1].
+ * supp (NULL: all pixels): one byte per pixel (index x + nx y); only the taps of pixels with supp != 0 are listed, so
+ * that the forward of an image that is zero outside the support skips terms that are exactly zero. */
+int dfx_radon_table_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel, const uint8_t *supp,
+                          int32_t *counts, void *stream);
+int dfx_radon_table_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel, const uint8_t *supp,
                          const int32_t *row_ptr, int32_t *entries, void *stream);
 /* dfx_radon_forward / dfx_radon_forward_bf16 through the ray table (same references): angle a of the launch is row
  * block angles[a] of the table (angles NULL: a); the same taps, weights and summation order, hence the same bits. */

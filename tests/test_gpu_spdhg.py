@@ -103,3 +103,30 @@ def test_spdhg_streamed_state_equals_resident(golden, precision):
     xa, sa = resumed("all")
     xn, sn = resumed("none")
     assert np.array_equal(xa, xn) and np.array_equal(sa["z"], sn["z"]) and np.array_equal(sa["y"], sn["y"])
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+def test_support_ray_table_gives_the_same_iterates(golden, precision):
+    """The forward projections of SPDHG read the ray table restricted to the support (the iterates are zero outside
+    it): fewer taps, the iterates and deviances of the full table bit for bit."""
+    from diffractom_b200 import SinglePhaseForwardOperator, SPDHGPoisson
+    d = golden("al5_small")
+    cfg, mat, grid = case_inputs(d)
+    kw = {} if precision == "fp32" else {"precision": "bf16"}
+    op = SinglePhaseForwardOperator(cfg, mat, grid, 1e-5, normalized=True, quadrature=d["quadrature"], **kw)
+    rng = np.random.default_rng(2)
+    x_true = (rng.random(op.coeff_shape) * (rng.random(op.coeff_shape) < 0.3) * op.support_mask()[None]
+              ).astype(np.float32)
+    b = rng.poisson(op.direct(torch.as_tensor(x_true, device="cuda")).cpu().numpy() * 40).astype(np.float32)
+    runs = []
+    for use in (False, True):
+        sp = SPDHGPoisson(op, subsets=3, seed=4)
+        sp.use_support_table = use
+        x0 = torch.as_tensor(rng.random(op.coeff_shape).astype(np.float32), device="cuda")   # non-zero outside
+        x0.copy_(torch.as_tensor(np.random.default_rng(7).random(op.coeff_shape).astype(np.float32)))
+        x = sp.run(x0, b, 3, diagnostics_interval=1).cpu().numpy()
+        runs.append((x, [s["f"] for s in sp.iter_stats], sp.state["y"]))
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert runs[0][1] == runs[1][1] and np.array_equal(runs[0][2], runs[1][2])
+    supp = torch.as_tensor(op.support_mask().astype(np.uint8).ravel(), device="cuda")
+    assert op.support_ray_table(supp)[2] < op.ray_taps
