@@ -17,6 +17,7 @@ import torch
 
 from . import _lib
 from .arrays import as_host, check_device, is_device, on_op_stream
+from .streaming import host_copier
 from .solvers import Reducer, as_device_data, periodic, support_mask_to_device
 
 DEFAULT_REFRESH = (5, 10, 20, 40, 80, 160, 320, 640, 1280, 2560, 5120)
@@ -107,7 +108,8 @@ class FISTAPoisson:
             x = check_device(x0, cshape, "x0")
         else:
             host_x0 = as_host(x0, cshape, "x0")
-            x = torch.as_tensor(host_x0, device=dev)
+            x = torch.empty(cshape, dtype=torch.float32, device=dev)
+            host_copier().to_device(host_x0, x)
         self.b = as_device_data(b, dshape, dev)
         self.w, self.pw = periodic(weights, dshape, "weights", dev)
         self.g, self.pg = periodic(gain, dshape, "gain", dev)
@@ -224,12 +226,14 @@ class FISTAPoisson:
             if stop:
                 break
         done = len(self.iter_stats)
-        self.state = {"it": it0 + done, "t": t_mom, "theta": theta, "y": y.cpu().numpy(), "wls_until": wls_until}
+        y_host = np.empty(tuple(y.shape), np.float32)
+        host_copier().to_host(y, y_host)
+        self.state = {"it": it0 + done, "t": t_mom, "theta": theta, "y": y_host, "wls_until": wls_until}
         self.final_stats = {"niter": done, "final_f": f_x, "final_obj": F_x, "backtracks": n_bt_total,
                             "metric_updates_on_failure": n_metric, "adjoint_scale": self.adjoint_scale,
                             "restarts": n_restart, "metric_setup_s": t_metric, "time": time.perf_counter() - t_start}
         self.b = self.w = self.g = self.bg = None
         if host_x0 is not None:
-            host_x0[...] = x.cpu().numpy()
+            host_copier().to_host(x, host_x0)
             return host_x0
         return x

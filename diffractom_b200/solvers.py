@@ -91,4 +91,7 @@ def as_device_data(b, dshape, device):
     h = np.ascontiguousarray(b, dtype=np.float32)
     if h.shape != tuple(dshape):
         raise ValueError(f"b must have shape {tuple(dshape)}, not {h.shape}")
-    return torch.as_tensor(h, device=device)
+    from .streaming import host_copier
+    out = torch.empty(tuple(dshape), dtype=torch.float32, device=device)
+    host_copier().to_device(h, out)
+    return out

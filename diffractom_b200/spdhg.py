@@ -28,7 +28,7 @@ import torch
 from . import _lib
 from .arrays import as_host, check_device, is_device, on_op_stream
 from .solvers import Reducer, as_device_data, periodic, support_mask_to_device
-from .streaming import BatchPipeline, CoeffArray, KMajorStaging
+from .streaming import BatchPipeline, CoeffArray, KMajorStaging, host_copier
 
 RHO_AUTO = 3e4
 NAMES = ("x", "z", "T")
@@ -213,7 +213,11 @@ class SPDHGPoisson:
         self.dzk = torch.empty(be, dtype=torch.float32, device=dev)
         self.x = None
         if self.X.resident:
-            self.x = x0 if self._x_on_gpu else torch.as_tensor(self._host_x, device=dev)
+            if self._x_on_gpu:
+                self.x = x0
+            else:
+                self.x = torch.empty(cshape, dtype=torch.float32, device=dev)
+                host_copier().to_device(self._host_x, self.x)
             op.to_batches(self.x, self.X.dev)
         else:
             self._stage.load(self._host_x.reshape(-1), self.X, self.pipe)
@@ -262,7 +266,7 @@ class SPDHGPoisson:
 
         self.pipe.run([self.X], [self.X], project_x)
         if state is not None:
-            self.y.copy_(torch.as_tensor(as_host(state["y"], dshape, "state['y']")))
+            host_copier().to_device(as_host(state["y"], dshape, "state['y']"), self.y)
             if state.get("z") is None:
                 self.pipe.run([], [self.Z], lambda ib, s_: op._adjoint_batch_k(self.y, ib, self.Z.ptr(ib, s_)))
         self._t_setup = time.perf_counter() - self._t_start
@@ -336,7 +340,7 @@ class SPDHGPoisson:
         if self.X.resident:
             op.from_batches(self.X.dev, self.x)
             if not self._x_on_gpu:
-                self._host_x[...] = self.x.cpu().numpy()
+                host_copier().to_host(self.x, self._host_x)
         else:
             self._stage.store(self.X, self._host_x.reshape(-1), self.pipe)
 
@@ -366,13 +370,16 @@ class SPDHGPoisson:
         if self.Z.resident:
             z = torch.empty(op.coeff_shape, dtype=torch.float32, device=op.device)
             op.from_batches(self.Z.dev, z)
-            z_host = z.cpu().numpy()
+            z_host = np.empty(op.coeff_shape, np.float32)
+            host_copier().to_host(z, z_host)
             del z
         else:
             z_host = np.empty(op.coeff_shape, np.float32)
             self._stage.store(self.Z, z_host.reshape(-1), self.pipe)
         self.pipe.synchronize()
-        self.state = {"epoch": self._ep0 + len(self.iter_stats), "z": z_host, "y": self.y.cpu().numpy()}
+        y_host = np.empty(op.data_shape, np.float32)
+        host_copier().to_host(self.y, y_host)
+        self.state = {"epoch": self._ep0 + len(self.iter_stats), "z": z_host, "y": y_host}
         self.final_stats = {"epochs": len(self.iter_stats), "final_f": self._f, "setup_s": self._t_setup,
                             "rho": self.rho_used, "subsets": self.M, "resident": self.resident_used,
                             "time": time.perf_counter() - self._t_start, "tv": 0.0, "tv_prob": 0.0, **self.scales}

@@ -268,3 +268,113 @@ class KMajorStaging:
             comp.synchronize()
             np.copyto(host_k[k0:k0 + n], self.pin.numpy()[:n])
         pipe.slot_free = [None, None]
+
+
+# ---------------------------------------------------------------------------------------------- host copies
+# Host arrays of the public API (NumPy x0, b, and the returned x, y, z) are pageable memory: a plain copy from or to
+# the device runs at a few GB/s there. These copies go through pinned chunks instead: the DMA of one chunk overlaps
+# the CPU copies of others, which run on a few threads (NumPy's copy releases the GIL).
+
+_COPY_CHUNK = 64 << 20          # bytes per pinned chunk
+_COPY_BUFS = 4                  # pinned chunks in flight = host threads
+
+
+class HostCopier:
+    """Chunked, pipelined copies between pageable NumPy arrays and contiguous device tensors (float32 or any dtype
+    of equal size on both sides)."""
+
+    def __init__(self):
+        import threading
+        from concurrent.futures import ThreadPoolExecutor
+        self.lock = threading.Lock()        # one copy at a time per process (the pinned chunks are shared)
+        self.pool = ThreadPoolExecutor(_COPY_BUFS, thread_name_prefix="dfx-copy")
+        self.pins = [torch.empty(_COPY_CHUNK, dtype=torch.uint8, pin_memory=True) for _ in range(_COPY_BUFS)]
+
+    @staticmethod
+    def _bytes(a: np.ndarray):
+        return a.reshape(-1).view(np.uint8)
+
+    def to_device(self, host: np.ndarray, dev: torch.Tensor, stream=None):
+        """dev <- host (C-contiguous, same number of bytes); returns after the copies are enqueued on stream (the
+        pinned buffers are not reused before their DMA has finished)."""
+        with self.lock:
+            self._to_device(host, dev, stream)
+
+    def _to_device(self, host, dev, stream):
+        src = self._bytes(np.ascontiguousarray(host))
+        dst = dev.view(-1).view(torch.uint8)
+        assert src.size == dst.numel()
+        stream = stream or torch.cuda.current_stream(dev.device)
+        n, nb = src.size, len(self.pins)
+        starts = list(range(0, n, _COPY_CHUNK))
+        done = [None] * nb
+        staged = {}
+
+        def stage(i):
+            o = starts[i]
+            m = min(_COPY_CHUNK, n - o)
+            np.copyto(self.pins[i % nb].numpy()[:m], src[o:o + m])
+            return m
+
+        for i in range(min(nb, len(starts))):
+            staged[i] = self.pool.submit(stage, i)
+        for i, o in enumerate(starts):
+            m = staged.pop(i).result()
+            b = i % nb
+            with torch.cuda.stream(stream):
+                dst[o:o + m].copy_(self.pins[b][:m], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+            done[b] = ev
+            j = i + nb
+            if j < len(starts):
+                def restage(j=j, ev=ev):
+                    ev.synchronize()          # the DMA out of this pinned buffer has finished
+                    return stage(j)
+                staged[j] = self.pool.submit(restage)
+        for ev in done:
+            if ev is not None:
+                ev.synchronize()
+
+    def to_host(self, dev: torch.Tensor, host: np.ndarray, stream=None):
+        """host (C-contiguous, same number of bytes) <- dev, after the work queued on stream; returns when host
+        holds the data."""
+        with self.lock:
+            self._to_host(dev, host, stream)
+
+    def _to_host(self, dev, host, stream):
+        dst = self._bytes(host)
+        src = dev.reshape(-1).view(torch.uint8)
+        assert dst.size == src.numel()
+        stream = stream or torch.cuda.current_stream(dev.device)
+        n, nb = dst.size, len(self.pins)
+        starts = list(range(0, n, _COPY_CHUNK))
+        futs = [None] * nb
+        for i, o in enumerate(starts):
+            m = min(_COPY_CHUNK, n - o)
+            b = i % nb
+            if futs[b] is not None:
+                futs[b].result()              # the CPU copy out of this pinned buffer has finished
+            with torch.cuda.stream(stream):
+                self.pins[b][:m].copy_(src[o:o + m], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+
+            def unstage(o=o, m=m, b=b, ev=ev):
+                ev.synchronize()
+                np.copyto(dst[o:o + m], self.pins[b].numpy()[:m])
+            futs[b] = self.pool.submit(unstage)
+        for f in futs:
+            if f is not None:
+                f.result()
+
+
+_copier = None
+
+
+def host_copier() -> HostCopier:
+    """The process's copier (made on first use: a few pinned chunks and threads)."""
+    global _copier
+    if _copier is None:
+        _copier = HostCopier()
+    return _copier
