@@ -1,5 +1,5 @@
 """diffractom_b200: diffractom's reconstruction hot path (the single-phase forward operator, its adjoint and the
-SPDHG / FISTA Poisson solvers) as hand-written sm_100a CUDA kernels behind a C ABI, with diffractom's Python API.
+SPDHG / FISTA Poisson, FISTA least-squares / Huber solvers) as hand-written sm_100a CUDA kernels behind a C ABI, with diffractom's Python API.
 
     from diffractom_b200 import Material, Grid, SinglePhaseForwardOperator, SPDHGPoisson
 
@@ -11,7 +11,8 @@ from .material import Material, group_reflections_into_rings
 from .quadrature import QuadratureRule
 
 __all__ = ["Grid", "MatrixGrid", "Material", "QuadratureRule", "group_reflections_into_rings",
-           "SinglePhaseForwardOperator", "SPDHGPoisson", "FISTAPoisson", "estimate_L_power", "forward_operator"]
+           "SinglePhaseForwardOperator", "SPDHGPoisson", "FISTAPoisson", "FISTAHuber", "FISTAL2", "estimate_L_power",
+           "forward_operator"]
 
 
 def __getattr__(name):
@@ -25,6 +26,9 @@ def __getattr__(name):
     if name == "FISTAPoisson":
         from .fista import FISTAPoisson
         return FISTAPoisson
+    if name in ("FISTAHuber", "FISTAL2"):
+        from . import fista_ls
+        return getattr(fista_ls, name)
     if name == "forward_operator":
         from .autograd import forward_operator
         return forward_operator

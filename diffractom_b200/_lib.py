@@ -68,6 +68,10 @@ SIGNATURES = {
     "dfx_poisson_value_grad": ([P, P, P, L, P, L, P, L, F, I, I, F, L, P, P, c_size_t, S], c_int),
     "dfx_mean_counted": ([P, P, L, L, P, P, c_size_t, S], c_int),
     "dfx_dot_f64": ([P, P, L, P, P, c_size_t, S], c_int),
+    "dfx_ls_residual": ([P, P, P, L, I, F, L, P, P, c_size_t, S], c_int),
+    "dfx_fista_ls_blocks": ([], c_int),
+    "dfx_fista_ls_update": ([P, P, P, P, L, I, I, F, F, F, I, P, S], c_int),
+    "dfx_sum_partials": ([P, I, I, P, S], c_int),
     "dfx_times_curvature": ([P, P, P, P, L, P, L, P, L, F, I, L, P, P, c_size_t, S], c_int),
     "dfx_support_sum": ([P, P, L, L, P, P, c_size_t, S], c_int),
     "dfx_weighted_sums": ([P, P, P, L, L, P, P, c_size_t, S], c_int),

@@ -369,6 +369,8 @@ __global__ void batch_support_kernel(float *__restrict__ x, const float *__restr
             x[i] = inside ? 1.0f : 0.0f;
         } else if (mode == 1) {
             if (!inside || x[i] < 0.0f) x[i] = 0.0f;
+        } else if (mode == 3) {
+            if (!inside) x[i] = 0.0f;
         } else {
             const float cs = colsum[i];
             if (inside && cs > 0.0f) x[i] = fminf(x[i], __fdiv_rn(c, cs));
@@ -640,7 +642,7 @@ extern "C" int dfx_radon_forward_table_bf16_bf16(const void *img_bf16, void *sin
 extern "C" int dfx_batch_support(float *x_k, const float *colsum_k, const uint8_t *supp, int64_t npix, int kstride,
                                  int kb, float c, int mode, void *stream)
 {
-    DFX_REQUIRE(x_k && npix > 0 && kstride > 0 && kb >= 0 && kb <= kstride && mode >= 0 && mode <= 2,
+    DFX_REQUIRE(x_k && npix > 0 && kstride > 0 && kb >= 0 && kb <= kstride && mode >= 0 && mode <= 3,
                 "batch_support: bad arguments");
     DFX_REQUIRE(mode != 2 || colsum_k, "batch_support: tmin needs the column sums");
     const int64_t blocks = cdiv(npix * kstride, 256);

@@ -67,15 +67,79 @@ __global__ void __launch_bounds__(RED_THREADS) finish_sums(const double *__restr
     block_sum<NS>(v, out);
 }
 
+
+// ---- FISTA for least squares and Huber (FISTAL2 / FISTAHuber) ----
+constexpr int FU_BLOCKS = 148 * 4;    // blocks of one fused update launch = its partial sums
+
+// r = w (Ax - b) (w periodic, pw = 0: 1) in place, clipped to [-delta, delta] if clip; partial sums of r^2 before
+// the clip (fista_huber.py / fista_l2.py residual_sumsq)
+__global__ void __launch_bounds__(RED_THREADS) ls_residual_kernel(float *__restrict__ ax, const float *__restrict__ b,
+                                                                  const float *__restrict__ w, int64_t pw, int clip,
+                                                                  float delta, int64_t n, double *part)
+{
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float r = __fsub_rn(ax[i], b[i]);
+        if (pw) r = __fmul_rn(periodic(w, pw, i, 1.0f), r);
+        v[0] += (double)r * (double)r;
+        if (clip) r = fminf(fmaxf(r, -delta), delta);
+        ax[i] = r;
+    }
+    block_sum<1>(v, part + blockIdx.x);
+}
+
+// The FISTA step of one orientation batch in the channel-fastest layout (npix x kstride, kb live channels), from its
+// gradient g: v = prox(y - tau g) (0: max(v, 0); 1: soft threshold lt; 2: max(v - lt, 0)), 0 outside the support and
+// on padding channels; y = v + beta (v - x); x = v (fused_update.py:22-49). Per-block partials of g^2, v^2, |v|.
+__global__ void __launch_bounds__(RED_THREADS) fista_ls_update_kernel(
+    const float4 *__restrict__ g, float4 *__restrict__ x, float4 *__restrict__ y, const uint8_t *__restrict__ supp,
+    int64_t npix, int kq, int kb, float tau, float beta, float lt, int prox, double *part)
+{
+    double acc[3] = {0.0, 0.0, 0.0};
+    const int64_t n4 = npix * kq;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n4; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pix = t / kq;
+        const int k = (int)(t - pix * kq) * 4;
+        const bool in = supp == nullptr || supp[pix] != 0;
+        const float4 gv = g[t], xv = x[t], yv = y[t];
+        const float gg[4] = {gv.x, gv.y, gv.z, gv.w}, xo[4] = {xv.x, xv.y, xv.z, xv.w};
+        const float yy[4] = {yv.x, yv.y, yv.z, yv.w};
+        float xn[4], yn[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float v = __fsub_rn(yy[c], __fmul_rn(tau, gg[c]));
+            if (prox == 0) {
+                v = v < 0.0f ? 0.0f : v;
+            } else if (prox == 1) {
+                const float a = __fsub_rn(fabsf(v), lt);
+                v = a > 0.0f ? copysignf(a, v) : 0.0f;
+            } else {
+                const float d = __fsub_rn(v, lt);
+                v = d > 0.0f ? d : 0.0f;
+            }
+            if (!in || k + c >= kb) v = 0.0f;
+            xn[c] = v;
+            yn[c] = __fadd_rn(v, __fmul_rn(beta, __fsub_rn(v, xo[c])));
+            acc[0] += (double)gg[c] * (double)gg[c];
+            acc[1] += (double)v * (double)v;
+            acc[2] += (double)fabsf(v);
+        }
+        x[t] = make_float4(xn[0], xn[1], xn[2], xn[3]);
+        y[t] = make_float4(yn[0], yn[1], yn[2], yn[3]);
+    }
+    block_sum<3>(acc, part + 3 * (int64_t)blockIdx.x);
+}
+
 // ---- SPDHG ----
 __global__ void dual_update_kernel(float *__restrict__ y, float *__restrict__ d, const float *__restrict__ sig,
                                    const float *__restrict__ b, const float *__restrict__ w, int64_t pw,
                                    const float *__restrict__ g, int64_t pg, const float *__restrict__ bg, int64_t pbg,
-                                   float eps, const int32_t *__restrict__ omegas, int64_t row, int64_t n)
+                                   float eps, const int32_t *__restrict__ omegas, int64_t row)
 {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t s = t / row;
-        const int64_t i = (int64_t)__ldg(omegas + s) * row + (t - s * row);
+    // blockIdx.y: the subset's angle (one data row of row elements), no division per element
+    const int64_t base = (int64_t)__ldg(omegas + blockIdx.y) * row;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < row; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + j;
         const float wi = periodic(w, pw, i, 1.0f), si = sig[i];
         const float yo = y[i];
         float yn = 0.0f;
@@ -357,9 +421,12 @@ extern "C" int dfx_spdhg_dual_update(float *y, float *d, const float *sig, const
 {
     DFX_REQUIRE(y && d && sig && b && omegas && n_sub >= 0 && row_len > 0, "dual_update: bad arguments");
     DFX_REQUIRE((!pw || w) && (!pg || g) && (!pbg || bg), "dual_update: periodic array missing");
-    const int64_t n = (int64_t)n_sub * row_len;
-    if (n == 0) return DFX_OK;
-    EW_LAUNCH(dual_update_kernel, n, stream, y, d, sig, b, w, pw, g, pg, bg, pbg, eps, omegas, row_len, n);
+    DFX_REQUIRE(n_sub <= 65535, "dual_update: at most 65535 angles per call");
+    if (n_sub == 0) return DFX_OK;
+    const dim3 grid((unsigned)std::min<int64_t>(cdiv(row_len, (int64_t)EW_THREADS * 4), 65535), (unsigned)n_sub);
+    dual_update_kernel<<<grid, EW_THREADS, 0, (cudaStream_t)stream>>>(y, d, sig, b, w, pw, g, pg, bg, pbg, eps,
+                                                                      omegas, row_len);
+    return launch_status("dual_update_kernel");
 }
 
 extern "C" int dfx_spdhg_primal_update(float *x, float *z, const float *T, const float *dz, float inv_p, float lam,
@@ -572,4 +639,47 @@ extern "C" int dfx_scale_f32(float *x, float a, int64_t n, void *stream)
     DFX_REQUIRE(x && n >= 0, "scale: bad arguments");
     if (n == 0) return DFX_OK;
     EW_LAUNCH(scale_kernel, n, stream, x, a, n);
+}
+
+
+// ---- FISTAL2 / FISTAHuber entry points ----
+extern "C" int dfx_ls_residual(float *ax, const float *b, const float *w, int64_t pw, int clip, float delta,
+                               int64_t n, double *out, void *scratch, size_t scratch_bytes, void *stream)
+{
+    DFX_REQUIRE(ax && b && out && n >= 0 && (!pw || w) && pw >= 0, "ls_residual: bad arguments");
+    DFX_REQUIRE(!clip || delta >= 0.0f, "ls_residual: the Huber delta must be >= 0");
+    return reduce_launch<1>(n, scratch, scratch_bytes, out, stream, "ls_residual", [&](int nb, cudaStream_t s,
+                                                                                         double *part) {
+        ls_residual_kernel<<<nb, RED_THREADS, 0, s>>>(ax, b, w, pw, clip, delta, n, part);
+    });
+}
+
+extern "C" int dfx_fista_ls_blocks(void) { return FU_BLOCKS; }
+
+extern "C" int dfx_fista_ls_update(const float *g, float *x, float *y, const uint8_t *supp, int64_t npix, int kstride,
+                                   int kb, float tau, float beta, float lt, int prox, double *part, void *stream)
+{
+    DFX_REQUIRE(g && x && y && part && npix > 0, "fista_ls_update: bad arguments");
+    DFX_REQUIRE(kstride > 0 && kstride % 4 == 0 && kb >= 0 && kb <= kstride,
+                "fista_ls_update: kstride (%d) must be a positive multiple of 4 and kb (%d) <= kstride", kstride, kb);
+    DFX_REQUIRE(prox >= 0 && prox <= 2, "fista_ls_update: prox must be 0 (nonneg), 1 (l1) or 2 (nonneg_l1)");
+    DFX_REQUIRE(((uintptr_t)g % 16) == 0 && ((uintptr_t)x % 16) == 0 && ((uintptr_t)y % 16) == 0,
+                "fista_ls_update: arrays must be 16-byte aligned");
+    fista_ls_update_kernel<<<FU_BLOCKS, RED_THREADS, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<const float4 *>(g), reinterpret_cast<float4 *>(x), reinterpret_cast<float4 *>(y), supp,
+        npix, kstride / 4, kb, tau, beta, lt, prox, part);
+    return launch_status("fista_ls_update");
+}
+
+extern "C" int dfx_sum_partials(const double *part, int n_part, int n_sums, double *out, void *stream)
+{
+    DFX_REQUIRE(part && out && n_part > 0 && n_sums >= 1 && n_sums <= 3, "sum_partials: bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n_sums == 1)
+        finish_sums<1><<<1, RED_THREADS, 0, s>>>(part, n_part, out);
+    else if (n_sums == 2)
+        finish_sums<2><<<1, RED_THREADS, 0, s>>>(part, n_part, out);
+    else
+        finish_sums<3><<<1, RED_THREADS, 0, s>>>(part, n_part, out);
+    return launch_status("finish_sums");
 }

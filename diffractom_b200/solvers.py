@@ -74,6 +74,14 @@ class Reducer:
         s, n = self.out[:2].tolist()
         return s, n
 
+    def ls_residual(self, ax, b, w, pw, clip, delta):
+        """ax <- w (ax - b) (clipped to [-delta, delta] if clip) in place; returns the sum of squares before the
+        clip (float64)."""
+        scr, nb = self._scr(ax.numel())
+        _lib.call("dfx_ls_residual", ax.data_ptr(), b.data_ptr(), _p(w), pw, int(clip), float(delta), ax.numel(),
+                  self.out.data_ptr(), scr.data_ptr(), nb, self.op._s())
+        return float(self.out[0].item())
+
     def dot(self, x, y=None):
         scr, nb = self._scr(x.numel())
         _lib.call("dfx_dot_f64", x.data_ptr(), _p(y), x.numel(), self.out.data_ptr(), scr.data_ptr(), nb,

@@ -120,7 +120,8 @@ int dfx_radon_forward_table_bf16_bf16(const void *img_bf16, void *sino_bf16, int
 /* replaces support_ones / project_support / tmin (fista_poisson.py:256-263, 277-281; spdhg_poisson.py:259-265) on a
  * channel-fastest batch (npix, kstride) with padding channels kb .. kstride-1 (supp (npix) uint8 or NULL):
  * mode 0: x = 1 on live channels of support pixels, else 0; mode 1: x = 0 outside them or where negative;
- * mode 2: x = min(x, c / colsum) on live channels of support pixels where colsum > 0. */
+ * mode 2: x = min(x, c / colsum) on live channels of support pixels where colsum > 0; mode 3: x = 0 outside them
+ * (apply_support, prox.py:75-99). */
 int dfx_batch_support(float *x_k, const float *colsum_k, const uint8_t *supp, int64_t npix, int kstride, int kb,
                       float c, int mode, void *stream);
 
@@ -309,6 +310,21 @@ int dfx_extrapolate(float *out, const float *a, const float *c, float beta, int6
 /* replaces copy_buf / scale_buf (:268-275, :195-198): dst = src (both 16-byte aligned); x *= a. */
 int dfx_copy_f32(const float *src, float *dst, int64_t n, void *stream);
 int dfx_scale_f32(float *x, float a, int64_t n, void *stream);
+
+/* FISTAL2 / FISTAHuber (optimization/fista_l2.py, fista_huber.py, fused_update.py), float32 element-wise with float64
+ * sums. replaces residual_sumsq (fista_huber.py:80-105): r = w (Ax - b) in place (w periodic with period pw, pw = 0:
+ * unweighted), then clipped to [-delta, delta] if clip; out[0] = sum r^2 before the clip. */
+int dfx_ls_residual(float *ax, const float *b, const float *w, int64_t pw, int clip, float delta, int64_t n,
+                    double *out, void *scratch, size_t scratch_bytes, void *stream);
+/* replaces fista_fused_update (fused_update.py:22-49) for one orientation batch in the channel-fastest layout
+ * (npix x kstride, kb live channels): v = prox(y - tau g) (prox 0 nonneg, 1 soft threshold lt, 2 nonneg soft
+ * threshold), v = 0 outside supp (NULL: no support) and on padding channels, y = v + beta (v - x), x = v. Writes
+ * dfx_fista_ls_blocks() x 3 float64 partial sums (sum g^2, sum v^2, sum |v|) to part; dfx_sum_partials adds the
+ * partials of several launches in a fixed order (n_sums of 1, 2 or 3 per partial). */
+int dfx_fista_ls_blocks(void);
+int dfx_fista_ls_update(const float *g, float *x, float *y, const uint8_t *supp, int64_t npix, int kstride, int kb,
+                        float tau, float beta, float lt, int prox, double *part, void *stream);
+int dfx_sum_partials(const double *part, int n_part, int n_sums, double *out, void *stream);
 
 #ifdef __cplusplus
 }

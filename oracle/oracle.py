@@ -285,3 +285,45 @@ def spdhg_reference(op: OracleOperator, subsets, b, n_epochs, x0=None, weights=N
         if nseq is not None:
             seq = nseq
     return x.reshape(K, op.Ny, op.Nx), y, z.reshape(K, op.Ny, op.Nx), devs, rho
+
+
+def fista_ls_reference(op: OracleOperator, b, niter, tau, x0=None, prox="nonneg", lam=0.0, support=None, clip=False,
+                       delta=1e-2, weights=None):
+    """FISTAL2 / FISTAHuber (fista_l2.py, fista_huber.py with fused_update.py:22-49) in float64 on the oracle
+    operator: r = w (A y - b), f = 0.5 sum r^2, r clipped to [-delta, delta] (Huber); x' = prox(y - tau A^T r),
+    0 outside the support; y = x' + beta (x' - x); t' = (1 + sqrt(1 + 4 t^2)) / 2, beta = (t - 1) / t'. op should
+    be a float64-I/O oracle (precision "f64io"). Returns (x, [f per iteration], [||grad|| per iteration])."""
+    K, npix = op.K, op.Nx * op.Ny
+    dshape = (op.R, op.My, op.CP)
+    b = np.asarray(b, np.float64).reshape(dshape)
+    w = None if weights is None else np.resize(np.asarray(weights, np.float64).ravel(), b.size).reshape(dshape)
+    supp = np.ones(npix, bool) if support is None else np.asarray(support, bool).ravel()
+    x = np.zeros((K, npix)) if x0 is None else np.asarray(x0, np.float64).reshape(K, npix).copy()
+    x[:, ~supp] = 0.0
+    y = x.copy()
+    t = 1.0
+    lt = lam * tau
+    fs, gs = [], []
+    for _ in range(niter):
+        r = op.forward(y.reshape(K, op.Ny, op.Nx)).astype(np.float64) - b
+        if w is not None:
+            r = w * r
+        fs.append(0.5 * float(np.sum(r * r)))
+        if clip:
+            r = np.clip(r, -delta, delta)
+        g = op.adjoint(r).reshape(K, npix).astype(np.float64)
+        gs.append(float(np.sqrt(np.sum(g * g))))
+        t_new = 0.5 * (1.0 + np.sqrt(1.0 + 4.0 * t * t))
+        beta = (t - 1.0) / t_new
+        v = y - tau * g
+        if prox == "nonneg":
+            v = np.maximum(v, 0.0)
+        elif prox == "l1":
+            v = np.sign(v) * np.maximum(np.abs(v) - lt, 0.0)
+        else:
+            v = np.maximum(v - lt, 0.0)
+        v[:, ~supp] = 0.0
+        y = v + beta * (v - x)
+        x = v
+        t = t_new
+    return x.reshape(K, op.Ny, op.Nx), fs, gs
