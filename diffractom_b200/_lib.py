@@ -72,6 +72,9 @@ SIGNATURES = {
     "dfx_fista_ls_blocks": ([], c_int),
     "dfx_fista_ls_update": ([P, P, P, P, L, I, I, F, F, F, I, P, S], c_int),
     "dfx_sum_partials": ([P, I, I, P, S], c_int),
+    "dfx_fr_scratch_bytes": ([P, I], c_size_t),
+    "dfx_fr_forward": ([P, P, P, I, I, I, P, c_size_t, S], c_int),
+    "dfx_fr_backward": ([P, P, P, I, I, I, P, c_size_t, S], c_int),
     "dfx_times_curvature": ([P, P, P, P, L, P, L, P, L, F, I, L, P, P, c_size_t, S], c_int),
     "dfx_support_sum": ([P, P, L, L, P, P, c_size_t, S], c_int),
     "dfx_weighted_sums": ([P, P, P, L, L, P, P, c_size_t, S], c_int),

@@ -32,6 +32,7 @@ from .geometry import OperatorGeometry, interleaved_subsets
 from .quadrature import DEFAULT_TOL
 
 SPARSE_BATCH_MAX = 1024   # largest orientation batch of the sparse modes (SPFO:134)
+AUTO_FFT_PIXELS = 400 * 400   # projector="auto": the Fourier-slice projector for grids of more pixels (SPFO:27)
 SPARSE_MIN_BATCHES = 4    # sparse modes: at least this many batches (SPFO:135)
 CAND_BYTES = 2 + 4 + 4 + 4 + 4          # per candidate / non-zero scratch of the reference's generator
 NNZ_BYTES = 2 + 4 + 4 + 2 + 4 + 2 + 4   # (pf_generate.py:29-30), used by the batch-size rule
@@ -59,15 +60,18 @@ class SinglePhaseForwardOperator:
         """Arguments as diffractom's (SPFO:169-197). ctx: None, a torch.device or a CUDA device index (the GPU);
         queue: None (the current torch stream at every call) or a torch.cuda.Stream. ring_intensities: with
         normalized=False, the integrated intensity of every ring (diffractom computes them from structure factors,
-        which this package does not model); fft_max_gb is accepted for compatibility.
+        which this package does not model). projector: "native" (the ray-driven / pixel-driven pair), "fft" (the
+        Fourier-slice projector, fourier.py; fft_max_gb bounds its scratch per channel slice) or "auto" (the
+        Fourier-slice one for grids of more than 400 x 400 pixels at float32 precision, SPFO:448-449).
 
         precision: "fp32" (the reference's arithmetic) or "bf16": direct_cl / adjoint_cl on device tensors then run
         the Radon output through BF16 and the pole-figure products on the tensor cores (dense BF16 PF of all
         orientations, float32 accumulation); the float32 sparse PF stays available (the solvers use it for set-up
         and for their once-per-epoch residual), NumPy (streamed) calls stay float32.
 
-        Not provided (NotImplementedError): projector "fft" / "gratopy", pf_mode "dense" (the sparse products give
-        the same operator), reflection_two_theta, window_parallax, custom rings with overlap weights other than 1."""
+        Not provided (NotImplementedError): projector "gratopy", the BF16 path with the Fourier-slice projector,
+        pf_mode "dense" (the sparse products give the same operator), reflection_two_theta, window_parallax, custom
+        rings with overlap weights other than 1."""
         lib = _lib.lib()                                    # fails loudly without the CUDA library
         if not torch.cuda.is_available():
             raise RuntimeError("SinglePhaseForwardOperator needs a CUDA device")
@@ -90,26 +94,36 @@ class SinglePhaseForwardOperator:
             raise NotImplementedError("reflection_two_theta and window_parallax are not provided by this operator")
         if projector not in ("auto", "native", "fft", "gratopy"):
             raise ValueError(f"projector must be 'auto', 'native', 'fft' or 'gratopy', not {projector!r}")
-        if projector in ("fft", "gratopy"):
-            raise NotImplementedError(f"projector {projector!r} is not provided (the native projector is)")
+        if projector == "gratopy":
+            raise NotImplementedError("projector 'gratopy' is not provided (the native and 'fft' projectors are)")
         if pf_mode not in ("dense", "sparse", "generated", "auto"):
             raise ValueError(f"pf_mode must be 'dense', 'sparse', 'generated' or 'auto', not {pf_mode!r}")
         if pf_mode == "dense":
             raise NotImplementedError("pf_mode='dense' is not provided: 'sparse' applies the same matrix")
-        if radon_kernel is None:
-            radon_kernel = "trapezoid"
-        self.projector = "native"
-        self.radon_kernel = radon_kernel
+        # the native projector's geometry is made in any case (the Fourier-slice projector shares its conventions)
+        geom_kernel = "trapezoid" if projector == "fft" or radon_kernel is None else radon_kernel
 
         # ---- host set-up (SPFO:376-494): rings, quadrature, probed directions, poles, projector geometry
         geom = OperatorGeometry(self.cfg, material, grid, normalized=normalized, quadrature=quadrature,
                                 quadrature_tol=quadrature_tol, pf_cutoff_sigma=pf_cutoff_sigma,
-                                radon_kernel=radon_kernel, rings=rings, ring_two_theta=ring_two_theta,
+                                radon_kernel=geom_kernel, rings=rings, ring_two_theta=ring_two_theta,
                                 ring_intensities=ring_intensities)
         self.__dict__.update({k: v for k, v in vars(geom).items() if k != "cfg"})
         self.geometry = geom
         self.pf_batch_max_gb = float(max_gb)
-        self._kernel_id = 1 if radon_kernel == "trapezoid" else 0
+        if projector == "auto":
+            projector = ("fft" if self.Nx * self.Ny > AUTO_FFT_PIXELS and precision == "fp32"
+                         and radon_kernel in (None, "hat") else "native")
+        if radon_kernel is None:
+            radon_kernel = "trapezoid" if projector == "native" else "hat"
+        if radon_kernel != "hat" and projector != "native":
+            raise ValueError(f"radon_kernel={radon_kernel!r} needs the native projector (projector is {projector!r})")
+        if projector == "fft" and precision == "bf16":
+            raise NotImplementedError("the BF16 precision path needs the native projector")
+        self.projector = projector
+        self.radon_kernel = radon_kernel
+        self._kernel_id = 1 if geom_kernel == "trapezoid" else 0
+        self.fft_max_gb = float(fft_max_gb)
 
         with stream_scope(self):          # device work of the build on the operator's stream
             # ---- device copies
@@ -131,8 +145,14 @@ class SinglePhaseForwardOperator:
                 self.N_Omega, self.N_eta, self.N_peaks, self.N_axes, self.N_Omega_subdivisions, self.N_eta_subdivisions,
                 self.K, float(self.pf_cut))
             self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
-            self._ray_rp, self._ray_ent, self.ray_taps = self._build_ray_table()
             self._ray_supp = {}
+            self._fft = None
+            if self.projector == "fft":
+                self._ray_rp = self._ray_ent = None
+                self.ray_taps = 0
+                self._build_fourier()
+            else:
+                self._ray_rp, self._ray_ent, self.ray_taps = self._build_ray_table()
             self.omega_subsets = None
             self._sub = []
             self._streamer = None
@@ -202,6 +222,8 @@ class SinglePhaseForwardOperator:
         """The ray table restricted to a support mask (uint8 (Ny * Nx) device tensor), built once per mask content
         and kept: the solvers' forward projections of iterates that are zero outside the support read it (same
         bits, fewer taps)."""
+        if self.projector == "fft":
+            return None                     # the Fourier-slice projector reads every pixel in any case
         key = bytes(supp.cpu().numpy())
         hit = self._ray_supp.get(key)
         if hit is None:
@@ -209,10 +231,44 @@ class SinglePhaseForwardOperator:
             self._ray_supp[key] = hit
         return hit
 
-    def _radon_fwd(self, src_ptr, dst_ptr, om, n_ang, kb, sld=None, ray=None):
+    def _build_fourier(self):
+        """The Fourier-slice projector of the geometry (fourier.py) and its channel slice: as many channels as fit
+        fft_max_gb of scratch (at most 256, at least 1), SPFO:469-481."""
+        from .fourier import FourierHost, FourierProjector
+        host = FourierHost(self.angles, self.Nx, self.Ny, self.My, self.image_width, self.My, self.detector_shifts(),
+                           self.angle_weight)
+        self._fft = FourierProjector(host, self.device)
+        per = self._fft.scratch_bytes(1)
+        self._fft_channels = int(max(1, min(256, self.fft_max_gb * 1024 ** 3 // per)))
+
+    def _fft_of(self, m):
+        return self._fft if m is None else self._sub[m]["fft"]
+
+    def _fft_run(self, forward, m, src_ptr, dst_ptr, kb):
+        fp = self._fft_of(m)
+        ch = self._fft_channels
+        nb = fp.scratch_bytes(min(ch, max(kb, 1)))
+        scr = self.scratch(nb)
+        (fp.forward if forward else fp.backward)(src_ptr, dst_ptr, self.Kstride, kb, ch, scr.data_ptr(), nb, self._s())
+
+    def _radon_bwd(self, sino_ptr, out_ptr, geo, n_ang, kb, m):
+        """Backward projection of a (n_ang, My, Kstride) sinogram into a channel-fastest batch (angles of subset m,
+        None: all)."""
+        if self.projector == "fft":
+            self._fft_run(False, m, sino_ptr, out_ptr, kb)
+            return
+        self._call("dfx_radon_backward", sino_ptr, out_ptr, geo.data_ptr(), n_ang, self.Nx, self.Ny, self.My,
+                   self.Kstride, kb, self._kernel_id, int(self.radon_geo.n_taps), self._s())
+
+    def _radon_fwd(self, src_ptr, dst_ptr, om, n_ang, kb, sld=None, ray=None, m=None):
         """Forward projection of a channel-fastest batch through the ray table (ray: (row_ptr, entries, taps) of a
         support table, None: the full one): angles om (int32 device tensor of angle indices, None: all) into float32
         (sld None) or BF16 (row stride sld) sinogram rows."""
+        if self.projector == "fft":
+            if sld is not None:
+                raise NotImplementedError("BF16 sinograms need the native projector")
+            self._fft_run(True, m, src_ptr, dst_ptr, kb)
+            return
         om_ptr = None if om is None else om.data_ptr()
         rp, ent = (self._ray_rp, self._ray_ent) if ray is None else ray[:2]
         if sld is None:
@@ -553,6 +609,8 @@ class SinglePhaseForwardOperator:
             om = torch.as_tensor(s.astype(np.int32), device=self.device)
             geo = self.geo_gpu[torch.as_tensor(s, device=self.device)].contiguous()
             entry = dict(omegas=om, geo=geo, n=len(s), row_ptr=None)
+            if self.projector == "fft":
+                entry["fft"] = self._fft.subset(s)
             if any(sb.get("generated") for sb in self.sparse_batches):
                 entry["row_ptr"] = []
                 for b in self.batches:
@@ -615,7 +673,7 @@ class SinglePhaseForwardOperator:
             e = self._sub[m]
             geo, n_ang, om = e["geo"], e["n"], e["omegas"]
         self._call("dfx_gather_channels", src.data_ptr(), self._img_k.data_ptr(), self.npix, k_src, Kb, self.Kstride, s)
-        self._radon_fwd(self._img_k.data_ptr(), self.coeffs_sino_C.data_ptr(), om, n_ang, Kb)
+        self._radon_fwd(self._img_k.data_ptr(), self.coeffs_sino_C.data_ptr(), om, n_ang, Kb, m=m)
         rp, col, val, compact = self._pf_batch(ib, True, m)
         self._call("dfx_spmm_pf_forward", self.coeffs_sino_C.data_ptr(), rp.data_ptr(), col.data_ptr(),
                    val.data_ptr(), data.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My,
@@ -648,8 +706,7 @@ class SinglePhaseForwardOperator:
         self._call("dfx_spmm_pf_adjoint", data.data_ptr(), rp.data_ptr(), col.data_ptr(), val.data_ptr(),
                    self.coeffs_sino_C.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My, Kb,
                    self.N_seg, self.Kstride, alpha, compact, s)
-        self._call("dfx_radon_backward", self.coeffs_sino_C.data_ptr(), self._img_k.data_ptr(), geo.data_ptr(), n_ang,
-                   self.Nx, self.Ny, self.My, self.Kstride, Kb, self._kernel_id, int(self.radon_geo.n_taps), s)
+        self._radon_bwd(self.coeffs_sino_C.data_ptr(), self._img_k.data_ptr(), geo, n_ang, Kb, m)
         self._call("dfx_scatter_channels", self._img_k.data_ptr(), target.data_ptr(), self.npix, k_target, Kb,
                    self.Kstride, s)
 
@@ -671,7 +728,7 @@ class SinglePhaseForwardOperator:
         Kb = self.batches[ib]["K_batch"]
         s = self._s()
         geo, n_ang, om, m = self._geo_of(subset)
-        self._radon_fwd(src_ptr, self.coeffs_sino_C.data_ptr(), om, n_ang, Kb, ray=ray)
+        self._radon_fwd(src_ptr, self.coeffs_sino_C.data_ptr(), om, n_ang, Kb, ray=ray, m=m)
         rp, col, val, compact = self._pf_batch(ib, True, m)
         self._call("dfx_spmm_pf_forward", self.coeffs_sino_C.data_ptr(), rp.data_ptr(), col.data_ptr(),
                    val.data_ptr(), data.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My,
@@ -690,13 +747,19 @@ class SinglePhaseForwardOperator:
     def _adjoint_batch_k(self, data, ib, out_ptr, subset=None):
         """A^T data of batch ib into a channel-fastest batch at device address out_ptr."""
         geo, n_ang, Kb = self._pf_adjoint_to_sino(data, ib, subset)
-        self._call("dfx_radon_backward", self.coeffs_sino_C.data_ptr(), out_ptr, geo.data_ptr(), n_ang, self.Nx,
-                   self.Ny, self.My, self.Kstride, Kb, self._kernel_id, int(self.radon_geo.n_taps), self._s())
+        self._radon_bwd(self.coeffs_sino_C.data_ptr(), out_ptr, geo, n_ang, Kb,
+                        None if subset is None else self._subset(subset))
 
     def _adjoint_update_batch(self, data, ib, subset, x_ptr, z_ptr, T_ptr, inv_p, lam):
         """SPDHG's update of batch ib: dz = A_m^T data (batch ib), z += dz, x = max(0, x - T (z + inv_p dz + lam)),
         on channel-fastest batches, the primal step fused into the backprojection."""
         geo, n_ang, Kb = self._pf_adjoint_to_sino(data, ib, subset)
+        if self.projector == "fft":         # backprojection into the batch buffer, then the primal step
+            self._radon_bwd(self.coeffs_sino_C.data_ptr(), self._img_k.data_ptr(), geo, n_ang, Kb,
+                            None if subset is None else self._subset(subset))
+            self._call("dfx_spdhg_primal_update", x_ptr, z_ptr, T_ptr, self._img_k.data_ptr(), float(inv_p),
+                       float(lam), self.batch_elems(), self._s())
+            return
         self._call("dfx_radon_backward_spdhg", self.coeffs_sino_C.data_ptr(), geo.data_ptr(), n_ang, self.Nx,
                    self.Ny, self.My, self.Kstride, Kb, self._kernel_id, int(self.radon_geo.n_taps), x_ptr, z_ptr,
                    T_ptr, float(inv_p), float(lam), self._s())
@@ -778,6 +841,7 @@ class SinglePhaseForwardOperator:
         self.release_omega_subsets()
         self.release_streamer()
         self._ray_supp = {}
+        self._fft = None
         self.sparse_batches = None
         self.coeffs_sino_C = self._img_k = None
         self._gen_col = self._gen_val = None

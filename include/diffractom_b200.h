@@ -326,6 +326,35 @@ int dfx_fista_ls_update(const float *g, float *x, float *y, const uint8_t *supp,
                         float tau, float beta, float lt, int prox, double *part, void *stream);
 int dfx_sum_partials(const double *part, int n_part, int n_sums, double *out, void *stream);
 
+/* Fourier-slice projector (replaces FourierRadon.forward / backward, operators/fourier_radon.py:248-297, with their
+ * OpenCL kernels fourier_radon.cl:10-217 around the VkFFT transforms). The tables of one angle set (the full scan or
+ * a subset), built on the host: deapodisation inv_dx (Nx), inv_dy (Ny); per polar sample (angle a, frequency
+ * j < H = L/2 + 1; R*H samples): filt (2 floats: phase, bin response, 1/L), kb (2 int32: the first tap on the
+ * oversampled Mx x My grid), w1 and w2 (W floats each); the spreading tiles of the half grid (16 x 16 cells,
+ * n_tx per row of tiles): tile_ptr (n_tiles + 1) and tile_smp (sample, or -(sample + 1) through the Hermitian
+ * mirror); wa (R) the angle weights; scale the forward factor. */
+typedef struct dfx_fr_geometry {
+    const float *inv_dx, *inv_dy;
+    const void *filt;
+    const int32_t *kb;
+    const float *w1, *w2;
+    const int32_t *tile_ptr, *tile_smp;
+    const float *wa;
+    int32_t Nx, Ny, Ns, R, L, H, Mx, My, W, cx, cy, n_tx, n_tiles;
+    float scale;
+} dfx_fr_geometry;
+/* Scratch for channel slices of at most `channels` (grid, spectrum, lines and the cuFFT work area); 0 on bad input
+ * (dfx_last_error says why). cuFFT plans are made on first use per size and kept by the library. */
+size_t dfx_fr_scratch_bytes(const dfx_fr_geometry *g, int channels);
+/* sino (R, Ns, kstride): channels 0 .. kb-1 = scale x the projections of the channel-fastest batch img_k
+ * (Nx*Ny, kstride), channels kb .. kstride-1 = 0; the batch goes through in equal slices of at most `channels`. */
+int dfx_fr_forward(const dfx_fr_geometry *g, const float *img_k, float *sino, int kstride, int kb, int channels,
+                   void *scratch, size_t scratch_bytes, void *stream);
+/* img_k channels 0 .. kb-1 = the transpose of the unscaled projection applied to sino, weighted by wa; padding
+ * channels 0. */
+int dfx_fr_backward(const dfx_fr_geometry *g, const float *sino, float *img_k, int kstride, int kb, int channels,
+                    void *scratch, size_t scratch_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
