@@ -26,7 +26,7 @@ namespace {
 
 constexpr int FR_TS = 16;     // spreading tile (cells per side)
 constexpr int FR_SB = 64;     // samples staged per round of the spread
-constexpr int FR_CCS = 8;     // channels per spreading block
+constexpr int FR_CCS = 16;    // channels per spreading block
 
 __device__ __forceinline__ int wrap(int v, int m)
 {
@@ -157,36 +157,41 @@ __global__ void fr_unfilter_kernel(float2 *__restrict__ spec, const float2 *__re
     }
 }
 
-// The transposed interpolation as a gather over the half grid: the block owns a FR_TS x FR_TS tile (rows k2, columns
-// k1 <= Mx/2) and FR_CCS channels; every thread adds, for its cell q, half * w2[l] w1[i] * spec (conjugated through
-// the mirror) of each tap of each listed sample that lands on q, in the list's order. half = 1/2 for the
-// frequencies 0 and L/2 (counted once by the real line), else 1.
+// The transposed interpolation as a gather over the half grid. A block owns one piece of a FR_TS x FR_TS tile's
+// sample list (rows k2, columns k1 <= Mx/2) and FR_CCS channels; every thread adds, for its cell q, half * w2[l]
+// w1[i] * spec (conjugated through the mirror) of each tap of each listed sample that lands on q, in the list's
+// order (half = 1/2 for the frequencies 0 and L/2, counted once by the real line). The tap offsets need no division:
+// each staged sample carries its first tap reduced modulo the grid (or its mirror's), so d = q - b (or b - q) is one
+// conditional wrap away. A tile's first piece writes the spectrum, its later pieces their own partial tiles, which
+// fr_spread_finish adds in order: deterministic.
 template <int W>
 __global__ void __launch_bounds__(FR_TS *FR_TS) fr_spread_kernel(
-    const float2 *__restrict__ spec, const int32_t *__restrict__ tile_ptr, const int32_t *__restrict__ tile_smp,
+    const float2 *__restrict__ spec, const int4 *__restrict__ pieces, const int32_t *__restrict__ tile_smp,
     const int2 *__restrict__ kb, const float *__restrict__ w1s, const float *__restrict__ w2s, float2 *__restrict__ Q,
-    int Mx, int My, int RH, int H, int n_tx, int C)
+    float2 *__restrict__ part, int Mx, int My, int RH, int H, int n_tx, int C)
 {
-    __shared__ int2 lkb[FR_SB];
+    __shared__ int lb1[FR_SB], lb2[FR_SB], lmir[FR_SB];
     __shared__ float lw1[FR_SB][W], lw2[FR_SB][W], lhalf[FR_SB];
-    __shared__ int lmir[FR_SB];
     __shared__ float2 lv[FR_CCS][FR_SB];
-    const int tile = blockIdx.x, cg = blockIdx.y * FR_CCS;
+    const int4 pc = __ldg(pieces + blockIdx.x);                   // tile, first entry, end entry, slot
+    const int tile = pc.x, cg = blockIdx.y * FR_CCS;
     const int lx = threadIdx.x, ly = threadIdx.y, lid = ly * FR_TS + lx;
     const int Hx = Mx / 2 + 1;
     const int q1 = (tile % n_tx) * FR_TS + lx, q2 = (tile / n_tx) * FR_TS + ly;
     float2 acc[FR_CCS];
 #pragma unroll
     for (int c = 0; c < FR_CCS; ++c) acc[c] = make_float2(0.0f, 0.0f);
-    const int e0 = __ldg(tile_ptr + tile), e1 = __ldg(tile_ptr + tile + 1);
-    for (int b0 = e0; b0 < e1; b0 += FR_SB) {
-        const int nb = min(FR_SB, e1 - b0);
+    for (int b0 = pc.y; b0 < pc.z; b0 += FR_SB) {
+        const int nb = min(FR_SB, pc.z - b0);
         __syncthreads();
         if (lid < nb) {
             const int sm = __ldg(tile_smp + b0 + lid);
             const int smp = sm >= 0 ? sm : -sm - 1;
-            lmir[lid] = sm < 0;
-            lkb[lid] = __ldg(kb + smp);
+            const bool mir = sm < 0;
+            const int2 b = __ldg(kb + smp);
+            lmir[lid] = mir;
+            lb1[lid] = wrap(mir ? -b.x : b.x, Mx);                // tap offset d = q - b, or b - q through the mirror
+            lb2[lid] = wrap(mir ? -b.y : b.y, My);
             const int j = smp % H;
             lhalf[lid] = (j == 0 || j == H - 1) ? 0.5f : 1.0f;
 #pragma unroll
@@ -194,16 +199,20 @@ __global__ void __launch_bounds__(FR_TS *FR_TS) fr_spread_kernel(
                 lw1[lid][i] = __ldg(w1s + (int64_t)smp * W + i);
                 lw2[lid][i] = __ldg(w2s + (int64_t)smp * W + i);
             }
-#pragma unroll
-            for (int c = 0; c < FR_CCS; ++c)
-                lv[c][lid] = cg + c < C ? spec[(int64_t)(cg + c) * RH + smp] : make_float2(0.0f, 0.0f);
+        }
+        for (int i = lid; i < nb * FR_CCS; i += FR_TS * FR_TS) {
+            const int t = i % nb, c = i / nb;                     // consecutive threads: consecutive samples
+            const int sm = __ldg(tile_smp + b0 + t);
+            lv[c][t] = cg + c < C ? spec[(int64_t)(cg + c) * RH + (sm >= 0 ? sm : -sm - 1)] : make_float2(0.0f, 0.0f);
         }
         __syncthreads();
         if (q1 < Hx && q2 < My) {
             for (int t = 0; t < nb; ++t) {
-                const int2 b = lkb[t];
                 const bool mir = lmir[t] != 0;
-                const int d1 = wrap((mir ? -q1 : q1) - b.x, Mx), d2 = wrap((mir ? -q2 : q2) - b.y, My);
+                int d1 = mir ? lb1[t] - q1 : q1 - lb1[t];
+                int d2 = mir ? lb2[t] - q2 : q2 - lb2[t];
+                d1 += d1 < 0 ? Mx : 0;
+                d2 += d2 < 0 ? My : 0;
                 if (d1 < W && d2 < W) {
                     const float w = __fmul_rn(__fmul_rn(lw2[t][d2], lw1[t][d1]), lhalf[t]);
 #pragma unroll
@@ -217,8 +226,37 @@ __global__ void __launch_bounds__(FR_TS *FR_TS) fr_spread_kernel(
     }
     if (q1 < Hx && q2 < My) {
 #pragma unroll
-        for (int c = 0; c < FR_CCS; ++c)
-            if (cg + c < C) Q[((int64_t)(cg + c) * My + q2) * Hx + q1] = acc[c];
+        for (int c = 0; c < FR_CCS; ++c) {
+            if (cg + c >= C) break;
+            if (pc.w < 0)
+                Q[((int64_t)(cg + c) * My + q2) * Hx + q1] = acc[c];
+            else
+                part[((int64_t)pc.w * C + cg + c) * (FR_TS * FR_TS) + lid] = acc[c];
+        }
+    }
+}
+
+// Q += the partial tiles of a tile's later pieces, in their order (one block per tile, thread = cell)
+__global__ void __launch_bounds__(FR_TS *FR_TS) fr_spread_finish_kernel(float2 *__restrict__ Q,
+                                                                        const float2 *__restrict__ part,
+                                                                        const int32_t *__restrict__ tile_xptr, int Mx,
+                                                                        int My, int n_tx, int C)
+{
+    const int tile = blockIdx.x;
+    const int s0 = __ldg(tile_xptr + tile), s1 = __ldg(tile_xptr + tile + 1);
+    if (s0 == s1) return;
+    const int lid = threadIdx.y * FR_TS + threadIdx.x, Hx = Mx / 2 + 1;
+    const int q1 = (tile % n_tx) * FR_TS + threadIdx.x, q2 = (tile / n_tx) * FR_TS + threadIdx.y;
+    if (q1 >= Hx || q2 >= My) return;
+    for (int c = 0; c < C; ++c) {
+        float2 *q = Q + ((int64_t)c * My + q2) * Hx + q1;
+        float2 v = *q;
+        for (int sl = s0; sl < s1; ++sl) {
+            const float2 pv = part[((int64_t)sl * C + c) * (FR_TS * FR_TS) + lid];
+            v.x = __fadd_rn(v.x, pv.x);
+            v.y = __fadd_rn(v.y, pv.y);
+        }
+        *q = v;
     }
 }
 
@@ -326,7 +364,7 @@ int run_plan(int type, int n0, int n1, int batch, void *in, void *outp, void *wo
 }
 
 struct Layout {
-    size_t grid, G, spec, lines, work, total;
+    size_t grid, G, spec, lines, part, work, total;
 };
 
 size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -338,7 +376,8 @@ int layout(const dfx_fr_geometry *g, int C, Layout *L)
     L->G = L->grid + al256((size_t)C * g->My * g->Mx * 4);
     L->spec = L->G + al256((size_t)C * g->My * Hx * 8);
     L->lines = L->spec + al256((size_t)C * g->R * g->H * 8);
-    L->work = L->lines + al256((size_t)C * g->R * g->L * 4);
+    L->part = L->lines + al256((size_t)C * g->R * g->L * 4);
+    L->work = L->part + al256((size_t)g->n_slots * C * FR_TS * FR_TS * 8);
     size_t w = 0;
     std::lock_guard<std::mutex> lk(g_plan_lock);
     const int kinds[4][4] = {{CUFFT_R2C, g->My, g->Mx, C},
@@ -365,6 +404,8 @@ int check_geometry(const dfx_fr_geometry *g, const char *what)
                     g->n_tx > 0 && g->n_tiles > 0,
                 "%s: bad geometry sizes", what);
     DFX_REQUIRE((int64_t)g->R * g->H < 2147483647LL, "%s: too many polar samples", what);
+    DFX_REQUIRE(g->pieces && g->tile_xptr && g->n_pieces >= g->n_tiles && g->n_slots >= 0,
+                "%s: bad spreading pieces", what);
     return DFX_OK;
 }
 
@@ -469,17 +510,23 @@ extern "C" int dfx_fr_backward(const dfx_fr_geometry *g, const float *sino, floa
             fr_unfilter_kernel<<<(unsigned)std::min<int64_t>(cdiv(nsp, 256), 148 * 32), 256, 0, s>>>(
                 spec, (const float2 *)g->filt, RH, nsp);
             if ((st = launch_status("fr_unfilter"))) return st;
-            const dim3 sg((unsigned)g->n_tiles, (unsigned)cdiv(cs, FR_CCS));
+            const dim3 sg((unsigned)g->n_pieces, (unsigned)cdiv(cs, FR_CCS));
             DFX_REQUIRE(sg.y <= 65535u, "fr_backward: too many channels per slice");
+            float2 *part = (float2 *)(base + L.part);
             if (g->W == 7)
-                fr_spread_kernel<7><<<sg, dim3(FR_TS, FR_TS), 0, s>>>(spec, g->tile_ptr, g->tile_smp,
-                                                                     (const int2 *)g->kb, g->w1, g->w2, Q, g->Mx,
-                                                                     g->My, RH, g->H, g->n_tx, cs);
+                fr_spread_kernel<7><<<sg, dim3(FR_TS, FR_TS), 0, s>>>(spec, (const int4 *)g->pieces, g->tile_smp,
+                                                                     (const int2 *)g->kb, g->w1, g->w2, Q, part,
+                                                                     g->Mx, g->My, RH, g->H, g->n_tx, cs);
             else
-                fr_spread_kernel<6><<<sg, dim3(FR_TS, FR_TS), 0, s>>>(spec, g->tile_ptr, g->tile_smp,
-                                                                     (const int2 *)g->kb, g->w1, g->w2, Q, g->Mx,
-                                                                     g->My, RH, g->H, g->n_tx, cs);
+                fr_spread_kernel<6><<<sg, dim3(FR_TS, FR_TS), 0, s>>>(spec, (const int4 *)g->pieces, g->tile_smp,
+                                                                     (const int2 *)g->kb, g->w1, g->w2, Q, part,
+                                                                     g->Mx, g->My, RH, g->H, g->n_tx, cs);
             if ((st = launch_status("fr_spread"))) return st;
+            if (g->n_slots > 0) {
+                fr_spread_finish_kernel<<<(unsigned)g->n_tiles, dim3(FR_TS, FR_TS), 0, s>>>(Q, part, g->tile_xptr,
+                                                                                             g->Mx, g->My, g->n_tx, cs);
+                if ((st = launch_status("fr_spread_finish"))) return st;
+            }
             if ((st = run_plan(CUFFT_C2R, g->My, g->Mx, cs, Q, grid, base + L.work, scratch_bytes - L.work, s)))
                 return st;
             fr_crop_kernel<<<dim3((unsigned)cdiv(g->Nx, 32), (unsigned)g->Ny, (unsigned)cdiv(cb, 32)), dim3(32, 8), 0,

@@ -30,7 +30,7 @@ import torch
 
 from . import _lib
 
-SIGMA, W_TAPS, L_FACTOR, TILE = 1.5, 7, 1.25, 16
+SIGMA, W_TAPS, L_FACTOR, TILE, PIECE = 1.5, 7, 1.25, 16, 512
 
 
 def smooth_length(n, even=True):
@@ -110,6 +110,21 @@ class FourierTables:
             raise ValueError("too many spreading entries for 32-bit indices")
         self.tile_ptr = tile_ptr.astype(np.int32)
         self.tile_smp = np.where(mir == 1, -s - 1, s).astype(np.int32)
+        # the lists are very uneven (the tiles at the origin collect the low frequencies of every angle): a list is
+        # cut into pieces of at most PIECE samples, one block each; a tile's first piece writes the spectrum, the
+        # others partial tiles (slots) that are added to it afterwards in the pieces' order
+        cnt = np.diff(tile_ptr)
+        n_pc = np.maximum(1, -(-cnt // PIECE))
+        first = np.concatenate([[0], np.cumsum(n_pc)[:-1]])
+        tile_of = np.repeat(np.arange(self.n_tiles), n_pc)
+        k = np.arange(len(tile_of)) - first[tile_of]                 # piece number within its tile
+        e0 = tile_ptr[tile_of] + k * PIECE
+        e1 = np.minimum(e0 + PIECE, tile_ptr[tile_of + 1])
+        extra = np.maximum(0, n_pc - 1)
+        self.tile_xptr = np.concatenate([[0], np.cumsum(extra)]).astype(np.int32)
+        slot = np.where(k == 0, -1, self.tile_xptr[tile_of] + k - 1)
+        self.pieces = np.ascontiguousarray(np.stack([tile_of, e0, e1, slot], 1), np.int32)
+        self.n_slots = int(self.tile_xptr[-1])
         self.wa = np.ascontiguousarray(np.broadcast_to(np.asarray(angle_weights, np.float64), (R,)), np.float32)
 
 
@@ -118,10 +133,12 @@ class FRGeometry(ctypes.Structure):
     _fields_ = [("inv_dx", ctypes.c_void_p), ("inv_dy", ctypes.c_void_p), ("filt", ctypes.c_void_p),
                 ("kb", ctypes.c_void_p), ("w1", ctypes.c_void_p), ("w2", ctypes.c_void_p),
                 ("tile_ptr", ctypes.c_void_p), ("tile_smp", ctypes.c_void_p), ("wa", ctypes.c_void_p),
+                ("pieces", ctypes.c_void_p), ("tile_xptr", ctypes.c_void_p),
                 ("Nx", ctypes.c_int32), ("Ny", ctypes.c_int32), ("Ns", ctypes.c_int32), ("R", ctypes.c_int32),
                 ("L", ctypes.c_int32), ("H", ctypes.c_int32), ("Mx", ctypes.c_int32), ("My", ctypes.c_int32),
                 ("W", ctypes.c_int32), ("cx", ctypes.c_int32), ("cy", ctypes.c_int32), ("n_tx", ctypes.c_int32),
-                ("n_tiles", ctypes.c_int32), ("scale", ctypes.c_float)]
+                ("n_tiles", ctypes.c_int32), ("n_pieces", ctypes.c_int32), ("n_slots", ctypes.c_int32),
+                ("scale", ctypes.c_float)]
 
 
 class FourierHost:
@@ -179,18 +196,20 @@ class FourierProjector:
         self.w1, self.w2 = dev(tab.w1), dev(tab.w2)
         self.tile_ptr, self.tile_smp = dev(tab.tile_ptr), dev(tab.tile_smp)
         self.wa = dev(tab.wa)
+        self.pieces, self.tile_xptr = dev(tab.pieces), dev(tab.tile_xptr)
         self.geom = FRGeometry(self.inv_dx.data_ptr(), self.inv_dy.data_ptr(), self.filt.data_ptr(),
                                self.kb.data_ptr(), self.w1.data_ptr(), self.w2.data_ptr(), self.tile_ptr.data_ptr(),
-                               self.tile_smp.data_ptr(), self.wa.data_ptr(), self.Nx, self.Ny, self.Ns, self.R,
-                               self.L, self.H, self.Mx, self.My, self.W, self.cx, self.cy, tab.n_tx, tab.n_tiles,
-                               float(self.scale))
+                               self.tile_smp.data_ptr(), self.wa.data_ptr(), self.pieces.data_ptr(),
+                               self.tile_xptr.data_ptr(), self.Nx, self.Ny, self.Ns, self.R, self.L, self.H, self.Mx,
+                               self.My, self.W, self.cx, self.cy, tab.n_tx, tab.n_tiles, len(tab.pieces),
+                               tab.n_slots, float(self.scale))
 
     def subset(self, idx):
         return FourierProjector(self.host, self.device, idx, _inv=(self.inv_dx, self.inv_dy))
 
     def nbytes(self):
         return sum(t.numel() * t.element_size() for t in (self.filt, self.kb, self.w1, self.w2, self.tile_ptr,
-                                                           self.tile_smp, self.wa))
+                                                           self.tile_smp, self.wa, self.pieces, self.tile_xptr))
 
     def scratch_bytes(self, channels):
         n = int(_lib.lib().dfx_fr_scratch_bytes(ctypes.byref(self.geom), int(channels)))

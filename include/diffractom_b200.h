@@ -332,7 +332,9 @@ int dfx_sum_partials(const double *part, int n_part, int n_sums, double *out, vo
  * j < H = L/2 + 1; R*H samples): filt (2 floats: phase, bin response, 1/L), kb (2 int32: the first tap on the
  * oversampled Mx x My grid), w1 and w2 (W floats each); the spreading tiles of the half grid (16 x 16 cells,
  * n_tx per row of tiles): tile_ptr (n_tiles + 1) and tile_smp (sample, or -(sample + 1) through the Hermitian
- * mirror); wa (R) the angle weights; scale the forward factor. */
+ * mirror); wa (R) the angle weights; the lists cut into n_pieces pieces (4 int32 each: tile, first and end entry,
+ * partial slot or -1 for a tile's first piece) with tile_xptr (n_tiles + 1) the slots of each tile's later pieces
+ * (n_slots in all); scale the forward factor. */
 typedef struct dfx_fr_geometry {
     const float *inv_dx, *inv_dy;
     const void *filt;
@@ -340,7 +342,8 @@ typedef struct dfx_fr_geometry {
     const float *w1, *w2;
     const int32_t *tile_ptr, *tile_smp;
     const float *wa;
-    int32_t Nx, Ny, Ns, R, L, H, Mx, My, W, cx, cy, n_tx, n_tiles;
+    const int32_t *pieces, *tile_xptr;
+    int32_t Nx, Ny, Ns, R, L, H, Mx, My, W, cx, cy, n_tx, n_tiles, n_pieces, n_slots;
     float scale;
 } dfx_fr_geometry;
 /* Scratch for channel slices of at most `channels` (grid, spectrum, lines and the cuFFT work area); 0 on bad input

@@ -118,3 +118,20 @@ def test_exact_projection_is_close_to_the_native_hat_projector():
     native = scale * (hat * img[None, None, :]).sum(-1)
     rel = np.linalg.norm(fs - native) / np.linalg.norm(native)
     assert rel <= 0.03, rel
+
+
+def test_spreading_pieces_partition_every_tile_list():
+    """Every tile's sample list is cut into pieces in order (at most PIECE samples each); a tile's first piece has
+    no slot, its later pieces the consecutive slots tile_xptr[t] ..; empty lists keep one (empty) piece."""
+    from diffractom_b200.fourier import PIECE
+    g = dict(Nx=64, Ny=60, Ns=90, R=90, shift=0.1, width=64.0)
+    h, _ = _host(g)
+    tab = h.tables()
+    pc = tab.pieces
+    assert np.diff(tab.tile_ptr).max() > PIECE                    # some lists need several pieces
+    for t in range(tab.n_tiles):
+        mine = pc[pc[:, 0] == t]
+        assert mine[0, 1] == tab.tile_ptr[t] and mine[-1, 2] == tab.tile_ptr[t + 1]
+        assert np.array_equal(mine[1:, 1], mine[:-1, 2]) and np.all(mine[:, 2] - mine[:, 1] <= PIECE)
+        assert mine[0, 3] == -1 and np.array_equal(mine[1:, 3], np.arange(tab.tile_xptr[t], tab.tile_xptr[t + 1]))
+    assert tab.n_slots == len(pc) - tab.n_tiles
