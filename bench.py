@@ -220,6 +220,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the short serving run of the default line")
     ap.add_argument("--serve", action="store_true", help="only the serving benchmark (64 requests, Poisson "
                     "arrivals at 2/s, sizes of the serving configuration); its own JSON line")
+    ap.add_argument("--projectors", action="store_true", help="only the projector comparison (native vs "
+                    "Fourier-slice) at the large-slice geometry; its own JSON line")
     ap.add_argument("--K", type=int, default=None, help="orientations (default: the workload's)")
     ap.add_argument("--precision", default="both", choices=["both", "bf16", "fp32"],
                     help="both: the BF16 tensor-core path (the value) and the float32 path (for the ratio)")
@@ -232,6 +234,10 @@ def main():
     if a.impl == "reference":
         return run_reference(a, rank)
     torch.cuda.set_device(local)
+    if a.projectors:
+        if rank == 0:
+            print(json.dumps(projector_run(a.K or 256, a.steps, a.warmup)), flush=True)
+        return 0
     if a.serve:
         if rank == 0:
             st = serving_run(**SERVE_FULL)
@@ -541,6 +547,60 @@ SERVE_SHORT = dict(n=12, rate=2.0, px=(48, 128), omega=(90, 240), eta=(90, 240),
                    scenario="12 requests, Poisson arrivals 2/s, pixels 48^2-128^2, omega 90-240, eta 90-240, rings "
                             "3-8, K 500-2000 (the serving configuration's ranges, capped to keep the run short), "
                             "SPDHG to 1e-3 relative deviance change, 120 GB budget")
+
+
+LARGE_SLICE = dict(cfg=dict(Nx=512, Ny=512, My=520, N_Omega=720, angle_range=[0, 180], cor_offset=0.0, N_eta=360,
+                             eta_angle_range=[0, 360], energy=12.398 / 0.3, k_direction_0=[0, 0, 1],
+                             p_direction_0=[1, 0, 0], detector_direction_origin=[0, -1, 0],
+                             detector_direction_positive_90=[0, 0, -1]),
+                   material=dict(a=3.52, symmetry_group="cubic", wavelength_A=0.3,
+                                 hkl_list=[[1, 1, 1], [2, 0, 0], [2, 2, 0], [3, 1, 1], [2, 2, 2], [4, 0, 0]]),
+                   sigma_deg=1.0, subsets=36)
+
+
+def projector_run(K, steps, warmup):
+    """The native and the Fourier-slice projector at the large-slice geometry (512 x 512 pixels, 720 angles over 180
+    deg, 520 bins, cubic Ni): forward and backward projection of one batch of K orientations, for the full scan and
+    for one of 36 subsets; CUDA events, mean over `steps` launches after `warmup`."""
+    import torch
+    from diffractom_b200 import Grid, Material, SinglePhaseForwardOperator
+    w = LARGE_SLICE
+    mat = Material.from_lattice_parameters(**w["material"])
+    grid = Grid.from_random_fundamental_zone(K, mat.crystal_system, np.deg2rad(w["sigma_deg"]), seed=0)
+    out = {}
+    for proj in ("native", "fft"):
+        op = SinglePhaseForwardOperator(dict(w["cfg"]), mat, grid, 2.0, normalized=True, projector=proj,
+                                        pf_mode="generated")
+        op.set_omega_subsets(w["subsets"])
+        kb = op.batches[0]["K_batch"]
+        img = torch.rand(op.npix * op.Kstride, device=op.device)
+        res = torch.empty_like(img)
+        st = op.stream()
+        for tag, m in (("full", None), ("subset", 0)):
+            om, n = (None, op.N_Omega) if m is None else (op._sub[m]["omegas"], op._sub[m]["n"])
+            geo = op.geo_gpu if m is None else op._sub[m]["geo"]
+            calls = {"forward": lambda: op._radon_fwd(img.data_ptr(), op.coeffs_sino_C.data_ptr(), om, n, kb, m=m),
+                     "backward": lambda: op._radon_bwd(op.coeffs_sino_C.data_ptr(), res.data_ptr(), geo, n, kb, m)}
+            for name, f in calls.items():
+                for _ in range(max(1, warmup)):
+                    f()
+                st.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                for _ in range(steps):
+                    f()
+                e1.record(st)
+                e1.synchronize()
+                out[f"{proj}_{tag}_{name}_us_per_orientation"] = round(1000 * e0.elapsed_time(e1) / steps / kb, 2)
+        if proj == "fft":
+            out["fft_channels_per_slice"] = op._fft_channels
+        op.free_memory()
+        del op
+        torch.cuda.empty_cache()
+    return {"metric": "projector time per orientation (us)", "unit": "us", "higher_is_better": False,
+            "config": {"workload": "large slice 512x512, 720 angles over 180 deg, 520 bins, 36 subsets",
+                       "K_batch": K}, "steps": steps, "warmup": warmup, "data": "synthetic (random images)",
+            "projectors": out}
 
 
 def serving_run(n, rate, px, omega, eta, rings, K, slots, budget_gb, max_epochs, seed, scenario):
