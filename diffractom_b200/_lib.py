@@ -34,6 +34,7 @@ SIGNATURES = {
     "dfx_scatter_channels": ([P, P, L, I, I, I, S], c_int),
     "dfx_radon_forward": ([P, P, P, I, I, I, I, I, I, I, F, S], c_int),
     "dfx_radon_backward": ([P, P, P, I, I, I, I, I, I, I, I, S], c_int),
+    "dfx_radon_backward_pixels": ([P, P, P, I, I, I, I, I, I, I, I, P, L, S], c_int),
     "dfx_radon_backward_spdhg": ([P, P, I, I, I, I, I, I, I, I, P, P, P, F, F, S], c_int),
     "dfx_radon_forward_bf16": ([P, P, L, P, I, I, I, I, I, I, I, F, S], c_int),
     "dfx_radon_backward_bf16": ([P, L, P, P, I, I, I, I, I, I, I, I, S], c_int),
@@ -72,6 +73,7 @@ SIGNATURES = {
     "dfx_fista_ls_blocks": ([], c_int),
     "dfx_fista_ls_update": ([P, P, P, P, L, I, I, F, F, F, I, P, S], c_int),
     "dfx_sum_partials": ([P, I, I, P, S], c_int),
+    "dfx_score_z": ([P, P, P, L, S], c_int),
     "dfx_fr_scratch_bytes": ([P, I], c_size_t),
     "dfx_fr_forward": ([P, P, P, I, I, I, P, c_size_t, S], c_int),
     "dfx_fr_backward": ([P, P, P, I, I, I, P, c_size_t, S], c_int),

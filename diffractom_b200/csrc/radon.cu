@@ -270,20 +270,21 @@ __device__ __forceinline__ void primal_step(float &x, float &z, float t, float d
 }
 
 // MODE 0: img (npix, kstride) = backprojection; MODE 1: the backprojection dz is applied to x, z (T the steps):
-// z += dz; x = T > 0 ? max(0, x - T (z + inv_p dz + lam)) : 0.
+// z += dz; x = T > 0 ? max(0, x - T (z + inv_p dz + lam)) : 0. plist (MODE 0, optional): only the pixels plist[0 ..
+// n_out-1], output row r for pixel plist[r] (the same arithmetic per pixel as the whole image).
 template <int KERNEL, int MODE, typename ST>
 __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
     const ST *__restrict__ sino, int64_t sld, float *__restrict__ img, const float4 *__restrict__ geo, int n_angles, int nx,
     int ny, int ns, int kstride, int kb, int n_taps, float *__restrict__ z, const float *__restrict__ T, float inv_p,
-    float lam, __nv_bfloat16 *__restrict__ xb)
+    float lam, __nv_bfloat16 *__restrict__ xb, const int32_t *__restrict__ plist, int64_t n_out)
 {
     extern __shared__ AngleParams prm[];                   // the constants of every angle
     for (int i = threadIdx.x; i < n_angles; i += blockDim.x) prm[i] = pack_geo(load_geo(geo, i));
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t p = (int64_t)blockIdx.x * WARPS + warp;
+    const int64_t p = (int64_t)blockIdx.x * WARPS + warp;     // output row
     const int k = blockIdx.y * CPW + lane * CPL;
-    if (p >= (int64_t)nx * ny || k >= kstride) return;
+    if (p >= n_out || k >= kstride) return;
     if (blockIdx.y * CPW >= kb) {          // a block of padding channels only: the backprojection is 0 there
         if (MODE == 0) {
             const float zero[CPL] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -291,7 +292,8 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
         }
         return;                            // MODE 1: dz = 0 leaves z, and x (0 on padding channels), unchanged
     }
-    const int px = (int)(p % nx), py = (int)(p / nx);
+    const int64_t pix = plist ? (int64_t)__ldg(plist + p) : p;
+    const int px = (int)(pix % nx), py = (int)(pix / nx);
     const float fx = (float)px, fy = (float)py;
     float acc[CPL];
 #pragma unroll
@@ -449,9 +451,9 @@ static int allow_smem(Kernel kernel, size_t bytes)
 template <int KERNEL, int MODE, typename ST>
 static int launch_backward(const ST *sino, int64_t sld, float *img, const float *geo, int n_angles, int nx, int ny,
                            int n_det, int kstride, int kb, int n_taps, float *z, const float *T, float inv_p, float lam,
-                           __nv_bfloat16 *xb, void *stream)
+                           __nv_bfloat16 *xb, void *stream, const int32_t *plist = nullptr, int64_t n_list = 0)
 {
-    const int64_t npix = (int64_t)nx * ny;
+    const int64_t npix = plist ? n_list : (int64_t)nx * ny;
     dim3 grid((unsigned)cdiv(npix, WARPS), (unsigned)cdiv(kstride, CPW));
     DFX_REQUIRE(grid.x < 2147483647u && grid.y <= 65535u, "radon: batch too large for one launch");
     const size_t smem = sizeof(AngleParams) * (size_t)(n_angles > 0 ? n_angles : 1);
@@ -460,7 +462,7 @@ static int launch_backward(const ST *sino, int64_t sld, float *img, const float 
     if (st) return st;
     radon_backward_v3<KERNEL, MODE, ST><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
         sino, sld, img, reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, kstride, kb, n_taps, z, T, inv_p,
-        lam, xb);
+        lam, xb, plist, npix);
     return launch_status(MODE ? "radon_backward_spdhg" : "radon_backward");
 }
 
@@ -543,6 +545,21 @@ extern "C" int dfx_radon_forward_bf16(const float *img_k, void *sino_bf16, int64
 {
     return radon_forward_any(img_k, reinterpret_cast<__nv_bfloat16 *>(sino_bf16), sino_ld, geo, n_angles, nx, ny,
                              n_det, kstride, kb, kernel, scale, stream);
+}
+
+extern "C" int dfx_radon_backward_pixels(const float *sino_k, float *img_k, const float *geo, int n_angles, int nx,
+                                         int ny, int n_det, int kstride, int kb, int kernel, int n_taps,
+                                         const int32_t *pixels, int64_t n_pix, void *stream)
+{
+    int st = check_radon_args(sino_k, img_k, geo, n_angles, nx, ny, n_det, kstride, kb, kernel);
+    if (st) return st;
+    DFX_REQUIRE(pixels && n_pix > 0 && n_pix <= (int64_t)nx * ny, "radon_backward_pixels: bad pixel list");
+    DFX_REQUIRE(n_taps >= 2 && n_taps <= 64, "radon: n_taps (%d) out of range", n_taps);
+    if (kernel == 1)
+        return launch_backward<1, 0, float>(sino_k, (int64_t)kstride, img_k, geo, n_angles, nx, ny, n_det, kstride, kb,
+                                            n_taps, nullptr, nullptr, 0.0f, 0.0f, nullptr, stream, pixels, n_pix);
+    return launch_backward<0, 0, float>(sino_k, (int64_t)kstride, img_k, geo, n_angles, nx, ny, n_det, kstride, kb,
+                                        n_taps, nullptr, nullptr, 0.0f, 0.0f, nullptr, stream, pixels, n_pix);
 }
 
 extern "C" int dfx_radon_backward(const float *sino_k, float *img_k, const float *geo, int n_angles, int nx, int ny,

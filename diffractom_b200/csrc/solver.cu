@@ -130,6 +130,20 @@ __global__ void __launch_bounds__(RED_THREADS) fista_ls_update_kernel(
     block_sum<3>(acc, part + 3 * (int64_t)blockIdx.x);
 }
 
+
+// ---- orientation search: z = E / sqrt(max(D, 1e-30)) (NaN kept), 0 where D <= 0, with correctly rounded division
+// and square root: the float32 NumPy expression of the reference's host path, bitwise (orientation_search.py:41-54)
+__global__ void score_z_kernel(const float *__restrict__ E, const float *__restrict__ D, float *__restrict__ Z,
+                               int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float d = D[i];
+        const float m = d != d ? d : fmaxf(d, 1e-30f);
+        const float z = __fdiv_rn(E[i], __fsqrt_rn(m));
+        Z[i] = d <= 0.0f ? 0.0f : z;
+    }
+}
+
 // ---- SPDHG ----
 __global__ void dual_update_kernel(float *__restrict__ y, float *__restrict__ d, const float *__restrict__ sig,
                                    const float *__restrict__ b, const float *__restrict__ w, int64_t pw,
@@ -682,4 +696,11 @@ extern "C" int dfx_sum_partials(const double *part, int n_part, int n_sums, doub
     else
         finish_sums<3><<<1, RED_THREADS, 0, s>>>(part, n_part, out);
     return launch_status("finish_sums");
+}
+
+extern "C" int dfx_score_z(const float *E, const float *D, float *Z, int64_t n, void *stream)
+{
+    DFX_REQUIRE(E && D && Z && n >= 0, "score_z: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(score_z_kernel, n, stream, E, D, Z, n);
 }

@@ -789,6 +789,84 @@ class SinglePhaseForwardOperator:
             update(b["k_start"], b["K_batch"])
 
     @on_op_stream
+    def adjoint_multi_cl(self, datas, consume, row_masks=(None,), batch_done=None, pixels=None, nrhs=4,
+                         rows_per_group=12):
+        """Several adjoints in one pass over the orientation batches, sharing each batch's PF matrix (SPFO:1840-1964).
+
+        For every batch the PF matrix is made once (stored, or generated once) and its transpose applied to every
+        array of ``datas`` for the rows of every entry of ``row_masks`` (None: all rows, else an (N_Omega,) bool array
+        of the rows that count); each product is back-projected over those rows and handed to
+        ``consume(i, s, k0, Kb, block)`` (data array i, row mask s); ``batch_done(k0, Kb)`` follows every batch.
+
+        pixels None: block = the batch image, a (Nx*Ny, Kstride) view of the operator's batch buffer (block[p, k],
+        pixel p = x + Nx*y; columns k < Kb valid). pixels = (npix,) flat pixel indices: only these pixels are
+        back-projected, block = (K_batch_max, npix) orientation-major (rows k < Kb valid). Blocks are overwritten by
+        later calls of consume. The values are those adjoint_cl gives for datas[i] with the rows outside mask s set to
+        zero, bitwise: the product of an angle row depends on that row only, and the skipped rows would add exact
+        zeros to the backprojection. nrhs: data arrays per group of blocks (each group member keeps its own blocks
+        while the group is consumed); rows_per_group is accepted (a launch-shape option of the reference).
+
+        Needs pf_mode "sparse" or "generated" and the native projector."""
+        if self.pf_mode not in ("sparse", "generated") or self.projector != "native":
+            raise NotImplementedError("adjoint_multi_cl needs pf_mode 'sparse' or 'generated' and the native projector")
+        for d in datas:
+            check_device(d, self.data_shape, "data")
+        R = self.N_Omega
+        sets = []
+        for m in row_masks:
+            if m is None:
+                sets.append((None, self.geo_gpu, R))
+                continue
+            m = np.asarray(m, dtype=bool).reshape(-1)
+            if m.size != R:
+                raise ValueError(f"a row mask needs {R} entries (one per rotation angle), not {m.size}")
+            rows = np.nonzero(m)[0]
+            sets.append((torch.as_tensor(rows.astype(np.int32), device=self.device),
+                         self.geo_gpu[torch.as_tensor(rows, device=self.device)].contiguous(), len(rows)))
+        nrhs = max(1, min(int(nrhs), len(datas))) if datas else 1
+        s = self._s()
+        alpha = float(np.float32(self.N_Omega / np.pi))
+        Kmax, npix_img = self.K_batch_max, self.npix
+        if pixels is not None:
+            pix_h = np.asarray(pixels, dtype=np.int64).reshape(-1)
+            if pix_h.size == 0 or pix_h.min() < 0 or pix_h.max() >= npix_img:
+                raise ValueError(f"pixels must be flat indices in 0 .. {npix_img - 1}")
+            pix = torch.as_tensor(pix_h.astype(np.int32), device=self.device)
+            npl = int(pix_h.size)
+            tmp = torch.empty(npl * self.Kstride, dtype=torch.float32, device=self.device)
+            blocks = [[torch.empty((Kmax, npl), dtype=torch.float32, device=self.device) for _ in sets]
+                      for _ in range(nrhs)]
+        image = self._img_k.view(npix_img, self.Kstride)
+        for ib, b in enumerate(self.batches):
+            k0, Kb = b["k_start"], b["K_batch"]
+            rp, col, val, compact = self._pf_batch(ib, False, None)       # once for every data array and mask
+            for g0 in range(0, len(datas), nrhs):
+                for n, i in enumerate(range(g0, min(g0 + nrhs, len(datas)))):
+                    for si, (om, geo, n_ang) in enumerate(sets):
+                        if n_ang == 0:              # no rows count: the adjoint is zero
+                            blk = blocks[n][si] if pixels is not None else image
+                            self._fill(blk, 0.0)
+                            consume(i, si, k0, Kb, blk)
+                            continue
+                        self._call("dfx_spmm_pf_adjoint", datas[i].data_ptr(), rp.data_ptr(), col.data_ptr(),
+                                   val.data_ptr(), self.coeffs_sino_C.data_ptr(), None if om is None else om.data_ptr(),
+                                   n_ang, self.My, Kb, self.N_seg, self.Kstride, alpha, compact, s)
+                        if pixels is None:
+                            self._call("dfx_radon_backward", self.coeffs_sino_C.data_ptr(), self._img_k.data_ptr(),
+                                       geo.data_ptr(), n_ang, self.Nx, self.Ny, self.My, self.Kstride, Kb,
+                                       self._kernel_id, int(self.radon_geo.n_taps), s)
+                            consume(i, si, k0, Kb, image)
+                        else:
+                            self._call("dfx_radon_backward_pixels", self.coeffs_sino_C.data_ptr(), tmp.data_ptr(),
+                                       geo.data_ptr(), n_ang, self.Nx, self.Ny, self.My, self.Kstride, Kb,
+                                       self._kernel_id, int(self.radon_geo.n_taps), pix.data_ptr(), npl, s)
+                            self._call("dfx_scatter_channels", tmp.data_ptr(), blocks[n][si].data_ptr(), npl, 0, Kb,
+                                       self.Kstride, s)
+                            consume(i, si, k0, Kb, blocks[n][si])
+            if batch_done is not None:
+                batch_done(k0, Kb)
+
+    @on_op_stream
     def direct(self, coeffs):
         """Forward operator allocating its output: a CUDA tensor for a CUDA tensor; for a NumPy array (K, Ny, Nx) the
         coefficients are streamed to the GPU batch by batch and a NumPy array is returned (SPFO:1107-1127)."""

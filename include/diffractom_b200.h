@@ -62,6 +62,13 @@ int dfx_radon_forward(const float *img_k, float *sino_k, const float *geo, int n
  * atomics. n_taps: the most bins a pixel touches (ParallelRadon.n_taps). */
 int dfx_radon_backward(const float *sino_k, float *img_k, const float *geo, int n_angles, int nx, int ny, int n_det,
                        int kstride, int kb, int kernel, int n_taps, void *stream);
+/* dfx_radon_backward for the pixels pixels[0 .. n_pix-1] (flat indices x + nx y, each checked by the caller to lie in
+ * the image) only: img_k row r (n_pix rows of kstride) = the backprojection at pixel pixels[r], the same arithmetic
+ * as the whole-image call (replaces ParallelRadon.backward_list, operators/parallel_radon.py:320-340, used by
+ * adjoint_multi_cl with pixels, SPFO:1840-1964). */
+int dfx_radon_backward_pixels(const float *sino_k, float *img_k, const float *geo, int n_angles, int nx, int ny,
+                              int n_det, int kstride, int kb, int kernel, int n_taps, const int32_t *pixels,
+                              int64_t n_pix, void *stream);
 
 /* replaces, in one kernel, radon_backward_k + scatter_channels_k_fastest + spdhg_update (radon_kernels.cl:106-141,
  * 192-215; spdhg_poisson.py:95-106) for the fused SPDHG pass (spdhg_poisson.py:430-484): the backprojection dz of
@@ -357,6 +364,10 @@ int dfx_fr_forward(const dfx_fr_geometry *g, const float *img_k, float *sino, in
  * channels 0. */
 int dfx_fr_backward(const dfx_fr_geometry *g, const float *sino, float *img_k, int kstride, int kb, int channels,
                     void *scratch, size_t scratch_bytes, void *stream);
+
+/* replaces score_z (orientation_search.py:41-54): Z = E / sqrt(max(D, 1e-30)) (a NaN D kept), 0 where D <= 0, with
+ * correctly rounded division and square root (the float32 NumPy values, bitwise). */
+int dfx_score_z(const float *E, const float *D, float *Z, int64_t n, void *stream);
 
 #ifdef __cplusplus
 }
