@@ -46,6 +46,7 @@ class Request:
     max_gb: float = 2.0
     seed: int = 0
     id: int = 0
+    graphs: bool = True          # replay the SPDHG iterations as CUDA graphs from the second epoch on
     # filled in by the server
     arrival: float = 0.0
     admitted: float = 0.0
@@ -226,6 +227,7 @@ def run_request(req: Request, device, stream):
                                     queue=stream, precision=req.precision)
     try:
         sp = SPDHGPoisson(op, subsets=req.subsets, seed=req.seed)
+        sp.use_graphs = req.graphs
         x0 = torch.zeros(op.coeff_shape, dtype=torch.float32, device=device)
         sp._setup(x0, req.counts)
         devs = []

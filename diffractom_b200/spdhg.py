@@ -41,6 +41,12 @@ class SPDHGPoisson:
     # the iterates are zero outside the support (projected at set-up, T = 0 there), so the forward projections read
     # the operator's ray table restricted to the support: the same sums without the zero terms
     use_support_table = True
+    # CUDA graphs (an operator on its own stream, x on the device, no orientation shards): from the second epoch on, an
+    # iteration "dual step of m, then the pass (m, nb)" is replayed as two graphs captured once per subset: the update
+    # of m (dual step, adjoint with the primal step) and the forward of nb (row zeroing, forward projections and
+    # products). The pass's per-batch interleaving of the two becomes all updates, then all forwards: every batch's
+    # forward still reads its updated x and adds into the rows of nb in batch order, so the values are the same bits.
+    use_graphs = False
 
     def __init__(self, operator, subsets=8, prox_kind="nonneg", lam=0.0, support="fov", eps_counts=1e-3, rho="auto",
                  seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None, shards=None):
@@ -269,6 +275,8 @@ class SPDHGPoisson:
             host_copier().to_device(as_host(state["y"], dshape, "state['y']"), self.y)
             if state.get("z") is None:
                 self.pipe.run([], [self.Z], lambda ib, s_: op._adjoint_batch_k(self.y, ib, self.Z.ptr(ib, s_)))
+        self._graphs = {}
+        self.graph_replays = 0
         self._t_setup = time.perf_counter() - self._t_start
         self._ep0 = int(state["epoch"]) if state is not None else 0
         self.iter_stats = []
@@ -305,7 +313,9 @@ class SPDHGPoisson:
                     nb = nseq[0]
                 else:
                     nb = None
-                self._dual(m)
+                graphed = not ((end_of_epoch and want_f) or nb is None or nb == m) and self._graphs_on()
+                if not graphed:
+                    self._dual(m)
                 if (end_of_epoch and want_f) or nb is None or nb == m:
                     self._pass(m, None)
                     if (end_of_epoch and want_f) or nb is not None:
@@ -313,6 +323,10 @@ class SPDHGPoisson:
                         self._pass(None, "full")
                         if end_of_epoch and want_f:
                             self._f = self._deviance(self.D)
+                elif graphed:
+                    self._replay(("update", m), lambda m=m: (self._dual(m), self._pass(m, None)))
+                    self._replay(("forward", nb), lambda nb=nb: (op.zero_subset_rows(self.D, nb),
+                                                                 self._pass(None, nb)))
                 else:
                     op.zero_subset_rows(self.D, nb)
                     self._pass(m, nb)
@@ -333,6 +347,25 @@ class SPDHGPoisson:
                       flush=True)
             if stop:
                 break
+
+    def _graphs_on(self):
+        op = self.op
+        return (self.use_graphs and len(self.iter_stats) >= 1 and self.shards is None and self.X.resident
+                and torch.cuda.current_stream(op.device) != torch.cuda.default_stream(op.device))
+
+    def _replay(self, key, fn):
+        """Replay the graph of key, capturing fn on the current (the operator's) stream the first time."""
+        g = self._graphs.get(key)
+        if g is None:
+            g = torch.cuda.CUDAGraph()
+            g.capture_begin(capture_error_mode="thread_local")
+            try:
+                fn()
+            finally:
+                g.capture_end()
+            self._graphs[key] = g
+        g.replay()
+        self.graph_replays += 1
 
     def _x_out(self):
         """x in the (K, Ny, Nx) layout of the caller's array (the CUDA x0, or the NumPy x0's device copy and x0)."""
@@ -382,10 +415,12 @@ class SPDHGPoisson:
         self.state = {"epoch": self._ep0 + len(self.iter_stats), "z": z_host, "y": y_host}
         self.final_stats = {"epochs": len(self.iter_stats), "final_f": self._f, "setup_s": self._t_setup,
                             "rho": self.rho_used, "subsets": self.M, "resident": self.resident_used,
-                            "time": time.perf_counter() - self._t_start, "tv": 0.0, "tv_prob": 0.0, **self.scales}
+                            "time": time.perf_counter() - self._t_start, "tv": 0.0, "tv_prob": 0.0,
+                            "graph_replays": self.graph_replays, **self.scales}
         out = self.x if self._x_on_gpu else self._host_x
         self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = None
         self.X = self.Z = self.T = self.dzk = self.xkb = self._stage = self._ray = None
+        self._graphs = {}
         self.x = None
         return out
 

@@ -130,3 +130,29 @@ def test_support_ray_table_gives_the_same_iterates(golden, precision):
     assert runs[0][1] == runs[1][1] and np.array_equal(runs[0][2], runs[1][2])
     supp = torch.as_tensor(op.support_mask().astype(np.uint8).ravel(), device="cuda")
     assert op.support_ray_table(supp)[2] < op.ray_taps
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+def test_spdhg_cuda_graphs_equal_plain_iterations(golden, precision):
+    """use_graphs: from the second epoch on the iterations replay captured CUDA graphs (update of subset m, forward of
+    subset nb); iterates, deviances and state equal the plain run bit for bit, and the graphs were replayed."""
+    from diffractom_b200 import SinglePhaseForwardOperator, SPDHGPoisson
+    d = golden("al5_small")
+    cfg, mat, grid = case_inputs(d)
+    kw = {} if precision == "fp32" else {"precision": "bf16"}
+    op = SinglePhaseForwardOperator(cfg, mat, grid, 1e-5, normalized=True, quadrature=d["quadrature"],
+                                    queue=torch.cuda.Stream(), **kw)
+    rng = np.random.default_rng(3)
+    x_true = (rng.random(op.coeff_shape) * (rng.random(op.coeff_shape) < 0.2) * op.support_mask()[None]
+              ).astype(np.float32)
+    b = rng.poisson(op.direct(torch.as_tensor(x_true, device="cuda")).cpu().numpy() * 50).astype(np.float32)
+    runs = []
+    for graphs in (False, True):
+        sp = SPDHGPoisson(op, subsets=4, seed=2)
+        sp.use_graphs = graphs
+        x = sp.run(torch.zeros(op.coeff_shape, device="cuda"), b, 5, diagnostics_interval=2).cpu().numpy()
+        runs.append((x, [s["f"] for s in sp.iter_stats], sp.state["z"], sp.state["y"],
+                     sp.final_stats["graph_replays"]))
+    (x0, f0, z0, y0, n0), (x1, f1, z1, y1, n1) = runs
+    assert n0 == 0 and n1 > 0
+    assert np.array_equal(x0, x1) and f0 == f1 and np.array_equal(z0, z1) and np.array_equal(y0, y1)
