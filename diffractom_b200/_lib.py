@@ -74,6 +74,8 @@ SIGNATURES = {
     "dfx_fista_ls_update": ([P, P, P, P, L, I, I, F, F, F, I, P, S], c_int),
     "dfx_sum_partials": ([P, I, I, P, S], c_int),
     "dfx_score_z": ([P, P, P, L, S], c_int),
+    "dfx_local_scatter": ([P, P, P, P, P, I, I, I, I, P, S], c_int),
+    "dfx_local_gather": ([P, P, P, P, P, I, I, I, I, P, S], c_int),
     "dfx_fr_scratch_bytes": ([P, I], c_size_t),
     "dfx_fr_forward": ([P, P, P, I, I, I, P, c_size_t, S], c_int),
     "dfx_fr_backward": ([P, P, P, I, I, I, P, c_size_t, S], c_int),

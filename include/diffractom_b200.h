@@ -369,6 +369,18 @@ int dfx_fr_backward(const dfx_fr_geometry *g, const float *sino, float *img_k, i
  * correctly rounded division and square root (the float32 NumPy values, bitwise). */
 int dfx_score_z(const float *E, const float *D, float *Z, int64_t n, void *stream);
 
+/* Local basis (replaces the strip kernels local_radon_forward / local_radon_backward of
+ * operators/local_kernels.cl:38-181 around the dense projections): the patches of one orientation batch, box
+ * (y0, x0, h, w) int32 x 4 per patch (16-byte aligned), coff int64 (offset of its coefficients, row-major), chan
+ * int32 (its orientation's channel in the batch, < kstride), mask (uint8 per coefficient: 1 where the voxel is
+ * allowed). scatter: img_k (Nx*Ny, kstride) channel-fastest, at the patches' voxels = coeffs where allowed, 0 at
+ * their other voxels (the caller zeroes the rest of the batch image first); gather: coeffs of the patches = img_k at
+ * the allowed voxels, 0 at the others. */
+int dfx_local_scatter(const float *coeffs, const uint8_t *mask, const int32_t *box, const int64_t *coff,
+                      const int32_t *chan, int n_patches, int nx, int ny, int kstride, float *img_k, void *stream);
+int dfx_local_gather(const float *img_k, const uint8_t *mask, const int32_t *box, const int64_t *coff,
+                     const int32_t *chan, int n_patches, int nx, int ny, int kstride, float *coeffs, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
