@@ -930,7 +930,8 @@ class SinglePhaseForwardOperator:
 
 def estimate_L_power(op, niter: int = 20, seed: int = 0, eps: float = 1e-30, verbose: int = 1) -> float:
     """Lipschitz constant ||A^T A|| by power iteration (SPFO:2136-2206); the start vector is the reference's
-    (a standard normal (Nx, Ny, K) draw stored pixel-fastest) and the dot products are float64 (dfx_dot_f64)."""
+    (a standard normal (Nx, Ny, K) draw stored pixel-fastest; a draw of the coefficient shape for a local-basis
+    operator) and the dot products are float64 (dfx_dot_f64)."""
     with stream_scope(op):
         return _estimate_L_power(op, niter, seed, eps, verbose)
 
@@ -939,7 +940,10 @@ def _estimate_L_power(op, niter, seed, eps, verbose):
     if niter < 1:
         raise ValueError("niter must be >= 1")
     rng = np.random.default_rng(seed)
-    x_host = np.ascontiguousarray(rng.standard_normal((op.Nx, op.Ny, op.K)).astype(np.float32).transpose(2, 1, 0))
+    if getattr(op, "coefficient_layout", "dense") == "dense":
+        x_host = np.ascontiguousarray(rng.standard_normal((op.Nx, op.Ny, op.K)).astype(np.float32).transpose(2, 1, 0))
+    else:                                       # flat coefficients (local basis): drawn in their own shape
+        x_host = rng.standard_normal(tuple(op.coeff_shape)).astype(np.float32)
     x = torch.as_tensor(x_host, device=op.device)
     Ax = torch.empty(op.data_shape, dtype=torch.float32, device=op.device)
     z = torch.empty(op.coeff_shape, dtype=torch.float32, device=op.device)

@@ -38,6 +38,12 @@ def support_mask_to_device(operator, support, device):
     (diffractom/optimization/prox.py:75-99)."""
     if support is None or support is False:
         return None
+    if getattr(operator, "coefficient_layout", "dense") != "dense":
+        # a local-basis operator: its support (field of view included) is part of the operator
+        if isinstance(support, str) and support == "fov":
+            return None
+        raise ValueError("a support mask cannot be applied to this operator's coefficients; restrict the "
+                         "operator's LocalSupport instead (LocalSupport.restrict)")
     if isinstance(support, str):
         if support != "fov":
             raise ValueError(f"support must be 'fov', None or an (Ny, Nx) array, not {support!r}")

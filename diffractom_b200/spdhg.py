@@ -17,6 +17,10 @@ With a NumPy x0, each of x, z, T that does not fit on the device (resident="auto
 (resident="none" or a list of names) lives in pinned host memory in the same batch layout and is streamed through two
 device slots on side streams during every pass (spdhg_poisson.py:411-428); the iterates are the same bits either
 way. x is converted back to the (K, Ny, Nx) layout for callbacks and at the end; z for the state.
+
+On a local-basis operator (flat coefficients, LocalSinglePhaseForwardOperator) x, z, T are whole vectors on the device
+(they scale with the support) and an iteration is the dual step, the subset adjoint, the primal step of the whole
+vector and the next subset's forward (spdhg_poisson.py:753-945): the same steps as the fused pass, in four calls.
 """
 from __future__ import annotations
 
@@ -170,9 +174,137 @@ class SPDHGPoisson:
             callback=None, state=None):
         """As diffractom's SPDHGPoisson.run (spdhg_poisson.py:513-751). x0: a CUDA tensor (updated in place and
         returned) or a NumPy array (updated in place if C-contiguous float32, else converted; returned)."""
+        if getattr(self.op, "coefficient_layout", "dense") == "local":
+            return self._run_local(x0, b, n_epochs, weights, gain, background, verbose, diagnostics_interval,
+                                   callback, state)
         self._setup(x0, b, weights, gain, background, state)
         self._iterate(n_epochs, verbose, diagnostics_interval, callback)
         return self._finish()
+
+    def _setup_data(self, b, weights, gain, background):
+        """The data, weights, gain and background on the device, y = 0, the data-sized buffers; returns gamma."""
+        op = self.op
+        dev, dshape = op.device, tuple(op.data_shape)
+        self.b = as_device_data(b, dshape, dev)
+        self.w, self.pw = periodic(weights, dshape, "weights", dev)
+        self.g, self.pg = periodic(gain, dshape, "gain", dev)
+        self.bg, self.pbg = periodic(background, dshape, "background", dev)
+        if self.pg and float(self.g.min().item()) <= 0:
+            raise ValueError("the gain must be positive everywhere")
+        self.red = Reducer(op)
+        self.y = torch.zeros(dshape, dtype=torch.float32, device=dev)
+        self.sig = torch.empty(dshape, dtype=torch.float32, device=dev)
+        self.D = torch.empty(dshape, dtype=torch.float32, device=dev)
+        rho = self.rho
+        if rho == "auto":
+            sb, sn = self.red.mean_counted(self.b, self.w, self.pw)
+            mean_b = sb / max(sn, 1.0)
+            rho = RHO_AUTO / mean_b ** 2 if mean_b > 0 else 1.0
+        self.rho_used = float(rho)
+        return np.sqrt(rho)
+
+    def _dual_steps_from_rowsums(self, gamma):
+        """S = gamma / (A 1_S) from the row sums in D, the scales; then D = 1 on the counted points (for T)."""
+        s = self.op._s()
+        rs, rn = self.red.mean_counted(self.D, self.w, self.pw)
+        bs, bn = self.red.mean_counted(self.b, self.w, self.pw)
+        self.scales = {"row_sum_mean": rs / max(rn, 1.0), "b_mean": bs / max(bn, 1.0),
+                       "gain_mean": 1.0 if self.pg == 0 else float(self.g.double().mean().item())}
+        _lib.call("dfx_dual_steps", self.sig.data_ptr(), self.D.data_ptr(), _ptr(self.w), self.pw, float(gamma),
+                  self.D.numel(), s)
+        _lib.call("dfx_set_mask_ones", self.D.data_ptr(), _ptr(self.w), self.pw, self.D.numel(), s)
+
+    # ---------------------------------------------------------------- local basis
+    def _run_local(self, x0, b, n_epochs, weights, gain, background, verbose, diagnostics_interval, callback, state):
+        """run() on flat coefficients (module docstring); the schedule, steps and state are those of the dense run."""
+        t_start = time.perf_counter()
+        op = self.op
+        dev, s = op.device, op._s()
+        n = int(op.n_coef)
+        cshape, dshape = (n,), tuple(op.data_shape)
+        x_on_gpu = is_device(x0)
+        host_x = None if x_on_gpu else as_host(x0, cshape, "x0")
+        x = check_device(x0, cshape, "x0") if x_on_gpu else torch.as_tensor(host_x).to(dev)
+        gamma = self._setup_data(b, weights, gain, background)
+        # S from the row sums A 1 (1 on the allowed coefficients); T from the subsets' column sums over the counted
+        # points (spdhg_poisson.py:799-813)
+        ones = torch.as_tensor(np.ascontiguousarray(op.coefficient_mask(), np.float32), device=dev)
+        op.direct_cl(ones, self.D)
+        del ones
+        self._dual_steps_from_rowsums(gamma)
+        z = torch.zeros(n, dtype=torch.float32, device=dev)
+        T = torch.empty(n, dtype=torch.float32, device=dev)
+        dz = torch.empty(n, dtype=torch.float32, device=dev)
+        c = float(np.float32(self._p_data / gamma))
+        _lib.call("dfx_tinit", T.data_ptr(), n, s)
+        for m in range(self.M):
+            op.adjoint_cl(self.D, dz, subset=m)
+            _lib.call("dfx_tmin", T.data_ptr(), dz.data_ptr(), None, 0, c, n, s)
+        _lib.call("dfx_tfinal", T.data_ptr(), n, s)
+        _lib.call("dfx_project_support", x.data_ptr(), None, 0, n, s)
+        self.resident_used = NAMES
+        if state is not None:
+            host_copier().to_device(as_host(state["y"], dshape, "state['y']"), self.y)
+            if state.get("z") is not None:
+                z.copy_(torch.as_tensor(as_host(state["z"], cshape, "state['z']")))
+            else:                                       # z = A^T y of this operator
+                op.adjoint_cl(self.y, z)
+        t_setup = time.perf_counter() - t_start
+        inv_p = self._inv_p_data
+        ep0 = int(state["epoch"]) if state is not None else 0
+        self.iter_stats = []
+        f = float("nan")
+        seq = self._epoch_sequence()
+        op.direct_cl(x, self.D, subset=seq[0])
+        for e in range(int(n_epochs)):
+            ep = ep0 + e + 1
+            last = e + 1 == n_epochs
+            want_f = (e + 1) % max(1, diagnostics_interval) == 0 or last
+            nseq = None
+            for j, m in enumerate(seq):
+                self._dual(m)
+                op.adjoint_cl(self.D, dz, subset=m)
+                _lib.call("dfx_spdhg_primal_update", x.data_ptr(), z.data_ptr(), T.data_ptr(), dz.data_ptr(),
+                          inv_p, self.lam, n, s)
+                end_of_epoch = j + 1 == len(seq)
+                if not end_of_epoch:
+                    nb = seq[j + 1]
+                elif not last:
+                    nseq = self._epoch_sequence()
+                    nb = nseq[0]
+                else:
+                    nb = None
+                if end_of_epoch and want_f:
+                    op.direct_cl(x, self.D)                  # every row (the next subset's among them)
+                    f = self._deviance(self.D)
+                elif nb is not None:
+                    op.direct_cl(x, self.D, subset=nb)
+            if nseq is not None:
+                seq = nseq
+            if callback is not None or verbose:
+                op.stream().synchronize()
+            stats = {"epoch": ep, "f": f if want_f else None, "rho": self.rho_used,
+                     "time": time.perf_counter() - t_start}
+            self.iter_stats.append(stats)
+            stop = False
+            if callback is not None:
+                if not x_on_gpu:
+                    host_x[...] = x.cpu().numpy()
+                stop = bool(callback(ep, x if x_on_gpu else host_x, stats))
+            if verbose and want_f:
+                print(f"[spdhg epoch {ep:4d}] f={f:.8e} {time.perf_counter() - t_start:.1f} s", flush=True)
+            if stop:
+                break
+        z_host, y_host = z.cpu().numpy(), self.y.cpu().numpy()
+        self.state = {"epoch": ep0 + len(self.iter_stats), "z": z_host, "y": y_host}
+        self.final_stats = {"epochs": len(self.iter_stats), "final_f": f, "setup_s": t_setup, "rho": self.rho_used,
+                            "subsets": self.M, "resident": self.resident_used,
+                            "time": time.perf_counter() - t_start, "tv": 0.0, "tv_prob": 0.0, "graph_replays": 0,
+                            **self.scales}
+        if not x_on_gpu:
+            host_x[...] = x.cpu().numpy()
+        self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = None
+        return x if x_on_gpu else host_x
 
     @on_op_stream
     def _setup(self, x0, b, weights=None, gain=None, background=None, state=None):
@@ -185,27 +317,9 @@ class SPDHGPoisson:
         s = op._s()
         self._x_on_gpu = is_device(x0)
         self._host_x = None if self._x_on_gpu else as_host(x0, cshape, "x0")
-        self.b = as_device_data(b, dshape, dev)
-        self.w, self.pw = periodic(weights, dshape, "weights", dev)
-        self.g, self.pg = periodic(gain, dshape, "gain", dev)
-        self.bg, self.pbg = periodic(background, dshape, "background", dev)
-        if self.pg and float(self.g.min().item()) <= 0:
-            raise ValueError("the gain must be positive everywhere")
-        self.red = Reducer(op)
-        self.y = torch.zeros(dshape, dtype=torch.float32, device=dev)
-        self.sig = torch.empty(dshape, dtype=torch.float32, device=dev)
-        self.D = torch.empty(dshape, dtype=torch.float32, device=dev)
+        gamma = self._setup_data(b, weights, gain, background)
         supp = self.support_gpu
         sp = None if supp is None else supp.data_ptr()
-        npx = 0 if supp is None else npix
-
-        rho = self.rho
-        if rho == "auto":
-            sb, sn = self.red.mean_counted(self.b, self.w, self.pw)
-            mean_b = sb / max(sn, 1.0)
-            rho = RHO_AUTO / mean_b ** 2 if mean_b > 0 else 1.0
-        self.rho_used = float(rho)
-        gamma = np.sqrt(rho)
         p = self._p_data
         # x, z, T in the operator's channel-fastest batch layout for the whole run (batch ib at ib * be): on the device,
         # or in pinned host memory streamed through two device slots
@@ -245,14 +359,8 @@ class SPDHGPoisson:
             _lib.call("dfx_batch_support", self.dzk.data_ptr(), None, sp, npix, op.Kstride, bt["K_batch"], 0.0, 0, s)
             op._direct_batch_k(self.dzk.data_ptr(), ib, self.D, ray=self._ray)
         self._sum_shards("full")
-        rs, rn = self.red.mean_counted(self.D, self.w, self.pw)
-        bs, bn = self.red.mean_counted(self.b, self.w, self.pw)
-        self.scales = {"row_sum_mean": rs / max(rn, 1.0), "b_mean": bs / max(bn, 1.0),
-                       "gain_mean": 1.0 if self.pg == 0 else float(self.g.double().mean().item())}
-        _lib.call("dfx_dual_steps", self.sig.data_ptr(), self.D.data_ptr(), _ptr(self.w), self.pw, float(gamma),
-                  self.D.numel(), s)
+        self._dual_steps_from_rowsums(gamma)
         # T from the subsets' column sums over the counted points (spdhg_poisson.py:630-643)
-        _lib.call("dfx_set_mask_ones", self.D.data_ptr(), _ptr(self.w), self.pw, self.D.numel(), s)
         c = float(np.float32(p / gamma))
         T = self.T
 
