@@ -76,6 +76,11 @@ SIGNATURES = {
     "dfx_score_z": ([P, P, P, L, S], c_int),
     "dfx_local_scatter": ([P, P, P, P, P, I, I, I, I, P, S], c_int),
     "dfx_local_gather": ([P, P, P, P, P, I, I, I, I, P, S], c_int),
+    "dfx_pf_param_nq": ([I, I], c_int),
+    "dfx_pf_param_vjp": ([POINTER(PFGeometry), P, P, P, P, P, I, I, I, I, I, P, P, P, P, I, P, S], c_int),
+    "dfx_pf_rows_sum": ([P, I, I, I, P, S], c_int),
+    "dfx_radon_dtable_fill": ([P, I, I, I, I, I, P, P, S], c_int),
+    "dfx_angle_dot": ([P, P, I, I, I, I, P, S], c_int),
     "dfx_fr_scratch_bytes": ([P, I], c_size_t),
     "dfx_fr_forward": ([P, P, P, I, I, I, P, c_size_t, S], c_int),
     "dfx_fr_backward": ([P, P, P, I, I, I, P, c_size_t, S], c_int),

@@ -85,4 +85,15 @@ __device__ __forceinline__ float tap_weight(const AngleGeo &g, float d) {
     return fmaxf(__fsub_rn(1.0f, fabsf(d)), 0.0f);
 }
 
+// K'(d): the derivative of the tap weight with respect to the detector coordinate (0 at the kinks' outer side:
+// non-zero only where K is); the derivative of a projection with respect to a detector shift.
+template <int KERNEL>
+__device__ __forceinline__ float tap_dweight(const AngleGeo &g, float d) {
+    if (KERNEL == 1) {
+        const float q = __fsub_rn(g.hw, fabsf(d));
+        return (q > 0.0f && q < g.top) ? -copysignf(g.iw, d) : 0.0f;
+    }
+    return fabsf(d) < 1.0f ? -copysignf(1.0f, d) : 0.0f;
+}
+
 }  // namespace dfx

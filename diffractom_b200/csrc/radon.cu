@@ -150,7 +150,9 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_v4(
 // supp (optional, one byte per pixel): only the taps of pixels inside the support; for images that are zero outside
 // it (a solver's iterates projected onto the support) the forward through this table adds exactly the same terms
 // minus zeros, so it gives the same bits.
-template <int KERNEL>
+// DERIV: the same taps with the weights K'(t - s) (tap_dweight), the table of the projections' derivative with
+// respect to a detector shift of every angle.
+template <int KERNEL, bool DERIV = false>
 __global__ void ray_table_kernel(const float4 *__restrict__ geo, int n_angles, int nx, int ny, int ns,
                                  const uint8_t *__restrict__ supp, int32_t *__restrict__ counts,
                                  const int32_t *__restrict__ row_ptr, int2 *__restrict__ entries)
@@ -171,11 +173,12 @@ __global__ void ray_table_kernel(const float4 *__restrict__ geo, int n_angles, i
         const int u0 = max((int)floorf(fminf(e1, e2) - 1e-3f), 0);
         const int u1 = min((int)ceilf(fmaxf(e1, e2) + 1e-3f), nu - 1);
         for (int u = u0; u <= u1; ++u) {
-            const float w = tap_weight<KERNEL>(g, __fsub_rn(__fmaf_rn(g.A, (float)u, c), fs));
+            const float d = __fsub_rn(__fmaf_rn(g.A, (float)u, c), fs);
+            const float w = tap_weight<KERNEL>(g, d);
             if (w == 0.0f) continue;
             const int pix = g.rows_are_y ? u + nx * v : v + nx * u;
             if (supp && !supp[pix]) continue;
-            if (row_ptr) entries[pos++] = make_int2(pix, __float_as_int(w));
+            if (row_ptr) entries[pos++] = make_int2(pix, __float_as_int(DERIV ? tap_dweight<KERNEL>(g, d) : w));
             ++n;
         }
     }
@@ -629,6 +632,24 @@ extern "C" int dfx_radon_table_fill(const float *geo, int n_angles, int nx, int 
         ray_table_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
             reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, nullptr, row_ptr, e);
     return launch_status("radon_table_fill");
+}
+
+extern "C" int dfx_radon_dtable_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
+                                     const int32_t *row_ptr, int32_t *entries, void *stream)
+{
+    DFX_REQUIRE(geo && row_ptr && entries && ((uintptr_t)geo % 16) == 0 && ((uintptr_t)entries % 8) == 0,
+                "radon_dtable: null or misaligned pointer");
+    DFX_REQUIRE(n_angles > 0 && nx > 0 && ny > 0 && n_det > 0 && (kernel == 0 || kernel == 1),
+                "radon_dtable: bad sizes or kernel");
+    const int64_t rows = (int64_t)n_angles * n_det;
+    int2 *e = reinterpret_cast<int2 *>(entries);
+    if (kernel == 1)
+        ray_table_kernel<1, true><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, nullptr, nullptr, row_ptr, e);
+    else
+        ray_table_kernel<0, true><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, nullptr, nullptr, row_ptr, e);
+    return launch_status("radon_dtable_fill");
 }
 
 extern "C" int dfx_radon_forward_table(const float *img_k, float *sino_k, const int32_t *row_ptr,

@@ -137,13 +137,8 @@ class SinglePhaseForwardOperator:
             self.quad_weights_gpu = None if self.quad_weights_cpu is None else dev(self.quad_weights_cpu)
             self.intens_gpu = None if self.normalized else dev(self.intens_cpu)
             self.geo_gpu = dev(self.radon_geo.geo)
-            self._pfg = _lib.PFGeometry(
-                self.coords_gpu.data_ptr(), self.poles_gpu.data_ptr(), self.axis_start_gpu.data_ptr(),
-                self.axis_count_gpu.data_ptr(), self.inv_sigma2_gpu.data_ptr(), self.norm_factor_gpu.data_ptr(),
-                None if self.quad_weights_gpu is None else self.quad_weights_gpu.data_ptr(),
-                None if self.intens_gpu is None else self.intens_gpu.data_ptr(),
-                self.N_Omega, self.N_eta, self.N_peaks, self.N_axes, self.N_Omega_subdivisions, self.N_eta_subdivisions,
-                self.K, float(self.pf_cut))
+            self._pf_version = 0
+            self._make_pfg()
             self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
             self._ray_supp = {}
             self._fft = None
@@ -175,6 +170,16 @@ class SinglePhaseForwardOperator:
                 self.build_dense_bf16_pf()
 
     # ------------------------------------------------------------------ small helpers
+    def _make_pfg(self):
+        """The PF kernels' view of the device parameters (dfx_pf_geometry), made again after they change."""
+        self._pfg = _lib.PFGeometry(
+            self.coords_gpu.data_ptr(), self.poles_gpu.data_ptr(), self.axis_start_gpu.data_ptr(),
+            self.axis_count_gpu.data_ptr(), self.inv_sigma2_gpu.data_ptr(), self.norm_factor_gpu.data_ptr(),
+            None if self.quad_weights_gpu is None else self.quad_weights_gpu.data_ptr(),
+            None if self.intens_gpu is None else self.intens_gpu.data_ptr(),
+            self.N_Omega, self.N_eta, self.N_peaks, self.N_axes, self.N_Omega_subdivisions, self.N_eta_subdivisions,
+            self.K, float(self.pf_cut))
+
     def stream(self) -> torch.cuda.Stream:
         return self.queue if self.queue is not None else torch.cuda.current_stream(self.device)
 

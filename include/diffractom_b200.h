@@ -381,6 +381,33 @@ int dfx_local_scatter(const float *coeffs, const uint8_t *mask, const int32_t *b
 int dfx_local_gather(const float *img_k, const uint8_t *mask, const int32_t *box, const int64_t *coff,
                      const int32_t *chan, int n_patches, int nx, int ny, int kstride, float *coeffs, void *stream);
 
+/* ---------------------------------------------------------------- parameter gradients
+ * replaces pf_param_vjp (differentiable/pf_grad.cl:48-176, launched by PFGradient.__call__,
+ * differentiable/gradients.py:112-174): for every non-zero (r, k, j) of a batch's adjoint CSR (orientations
+ * k0 .. k0+kb-1), G = sum_y res[r, y, j] sino[r, y, k] times the derivative of the PF entry with respect to the
+ * rotation (3), the width (1), the eta offset, the axis tilt (2) and the ring's two-theta, summed per row r * kb + k
+ * into rows (R * kb, nq doubles; nq = dfx_pf_param_nq(P, hess); float32 entries, float64 sums); hess: also the
+ * upper triangle of
+ * sum_y curv S^2 q q^T (10 floats after the width), q the derivative of the entry with respect to (rot, sigma).
+ * flags: 1 eta offset, 2 axis tilt, 4 two-theta (each needs its probed directions' derivatives, coords-shaped).
+ * At most 16 rings; my floats + 2 nq doubles of shared memory (<= 48 KB). */
+int dfx_pf_param_nq(int n_rings, int hess);
+int dfx_pf_param_vjp(const dfx_pf_geometry *g, const int32_t *row_ptr, const uint16_t *col_j, const float *res,
+                     const float *curv, const float *sino, int my, int kstride, int k0, int kb, int flags,
+                     const float *dv_eta, const float *dv_t1, const float *dv_t2, const float *dv_tth, int hess,
+                     double *rows, void *stream);
+/* replaces rows_to_orientations (pf_grad.cl:179-187): out (kb, nq) = rows summed over the n_angles angles. */
+int dfx_pf_rows_sum(const double *rows, int n_angles, int kb, int nq, double *out, void *stream);
+
+/* replaces radon_dforward_k (differentiable/proj_grad.cl:12-63): the ray table (row pointers of
+ * dfx_radon_table_count without support) with the weights K'(t - s), the derivative of every tap with respect to a
+ * detector shift; dfx_radon_forward_table through it gives dS. */
+int dfx_radon_dtable_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
+                          const int32_t *row_ptr, int32_t *entries, void *stream);
+/* replaces shift_dot (proj_grad.cl:66-87): out[a] = sum_{y < n_det, k < kb} Z[a, y, k] dS[a, y, k]. */
+int dfx_angle_dot(const float *Z, const float *dS, int n_angles, int n_det, int kstride, int kb, float *out,
+                  void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,7 +15,9 @@ pole-figure matrix, the forward model and its transpose. What is recorded per ca
            rotated poles, 1/sigma^2, norm factors, ring two-theta and intensities, projector geometry (X, Y, T0,
            weights, scale, taps) and the field-of-view support mask
   outputs  ReferenceModel.pf (R, K, C, P) float64, forward(c) and the coefficient gradient of <r, forward(c)>
-           (= the adjoint applied to r)
+           (= the adjoint applied to r); the gradients of <r, forward(c)> with respect to the PF parameters (rot,
+           sigma, eta_offset, axis_tilt, two_theta) and the projector's (shift, cor), the probed directions'
+           derivatives, and the forward at moved PF and projector parameters (the checks of the parameter updates)
 
 Material fixtures record, for the materials of the benchmark configurations, the ring two-theta, the pole axes and
 their counts, which the package's own Material must reproduce.
@@ -109,7 +111,8 @@ def material_record(mat, cfg_energy):
                 h_first=np.asarray(op.h_cpu, np.float32))
 
 
-def case(name, cfg, mat_spec, n_orient, sigma_deg, grid_seed, quadrature="auto", kernel="trapezoid", seed=0):
+def case(name, cfg, mat_spec, n_orient, sigma_deg, grid_seed, quadrature="auto", kernel="trapezoid", seed=0,
+         probed=False, with_moved=True):
     mat = Material.from_lattice_parameters(**mat_spec)
     np.random.seed(grid_seed)
     grid = Grid.from_random_fundamental_zone(n_orient, mat_spec["symmetry_group"], np.deg2rad(sigma_deg))
@@ -125,6 +128,20 @@ def case(name, cfg, mat_spec, n_orient, sigma_deg, grid_seed, quadrature="auto",
     pf = ref.pf(prm)
     fwd = ref.forward(c, prm)
     adj = ref.vjp(c, prm, r, groups=("c",))["c"]
+    pf_groups = ("rot", "sigma", "eta_offset", "axis_tilt", "two_theta")
+    grads = ref.vjp(c, prm, r, groups=pf_groups + ("shift", "cor"))
+    dv = ref.probed_derivatives(prm)
+    moved = ref.params0()
+    moved["rot"] = rng.normal(0, 0.02, (K, 3))
+    moved["sigma"] = moved["sigma"] * 1.1
+    moved["two_theta"] = moved["two_theta"] + 0.001
+    moved["eta_offset"] = 0.01
+    moved["axis_tilt"] = np.array([0.01, -0.02])
+    fwd_pf_moved = ref.forward(c, moved)
+    proj = ref.params0()
+    proj["cor"] = proj["cor"] + 0.3
+    proj["shift"] = rng.normal(0, 0.4, op.N_Omega)
+    fwd_proj_moved = ref.forward(c, proj)
     geo, scale, n_taps = radon_geometry(op)
     rule = op.quadrature
     mat_json = {k: (v.tolist() if isinstance(v, np.ndarray) else v) for k, v in mat_spec.items()}
@@ -145,7 +162,17 @@ def case(name, cfg, mat_spec, n_orient, sigma_deg, grid_seed, quadrature="auto",
         intens=np.asarray(op.intens_cpu, np.float32),
         geo=geo, scale=np.float32(scale), n_taps=np.int32(n_taps), support=supp,
         pf=pf, fwd=fwd, adj=adj,
+        g_rot=grads["rot"], g_sigma=grads["sigma"], g_eta_offset=np.float64(grads["eta_offset"]),
+        g_axis_tilt=grads["axis_tilt"], g_two_theta=grads["two_theta"], g_shift=grads["shift"],
+        g_cor=np.float64(grads["cor"]),
     )
+    if with_moved:      # the forward at moved parameters, float32 (the checks' tolerance is 2e-5 of the maximum)
+        out.update(moved_rot=moved["rot"], moved_sigma=moved["sigma"], moved_two_theta=moved["two_theta"],
+                   fwd_pf_moved=fwd_pf_moved.astype(np.float32), moved_cor=np.float64(proj["cor"]),
+                   moved_shift=proj["shift"], fwd_proj_moved=fwd_proj_moved.astype(np.float32))
+    if probed:          # the probed directions' derivatives (coords-shaped), float32 as they reach the device
+        out.update(dv_eta=dv["eta_offset"].astype(np.float32), dv_tilt0=dv[("axis_tilt", 0)].astype(np.float32),
+                   dv_tilt1=dv[("axis_tilt", 1)].astype(np.float32), dv_tth=dv["two_theta"].astype(np.float32))
     np.savez_compressed(OUT / f"{name}.npz", **out)
     print(f"{name}: K={K} R={op.N_Omega} My={op.My} C={op.N_eta} P={op.N_peaks} rule={rule} "
           f"fill={np.mean(pf != 0):.3f}")
@@ -170,7 +197,7 @@ def main():
     # the geometry of the reference's tests/test_differentiable.py (two quadrature / kernel variants)
     diff = {**BASE, "Nx": 14, "Ny": 12, "My": 17, "N_Omega": 16, "angle_range": [0, 360], "cor_offset": 0.7,
             "N_eta": 24, "energy": 12.398 / 0.35}
-    case("diff_auto_trapezoid", diff, AL3, 12, 6.0, 5, "auto", "trapezoid", seed=0)
+    case("diff_auto_trapezoid", diff, AL3, 12, 6.0, 5, "auto", "trapezoid", seed=0, probed=True)
     case("diff_midpoint_hat", diff, AL3, 12, 6.0, 5, "midpoint", "hat", seed=0)
     # the geometry of tests/test_adjoint.py, every angle range it tests (a decreasing one too)
     for lo, hi in ((0, 180), (0, 360), (0, 90), (180, 0)):
@@ -180,11 +207,11 @@ def main():
     # a reduced version of the cubic-Al configuration (5 rings, half rotation, sigma 3 deg, midpoint rule)
     al = {**BASE, "Nx": 33, "Ny": 33, "My": 35, "N_Omega": 60, "angle_range": [0, 180], "cor_offset": 0.0,
           "N_eta": 60, "energy": 12.398 / 0.3}
-    case("al5_small", al, AL5, 16, 3.0, 3, "auto", "trapezoid", seed=2)
+    case("al5_small", al, AL5, 16, 3.0, 3, "auto", "trapezoid", seed=2, with_moved=False)
     # non-square image, hexagonal Ti, pixels smaller than the bins do not occur here (image width = Nx bins)
     ti = {**BASE, "Nx": 20, "Ny": 26, "My": 27, "N_Omega": 24, "angle_range": [0, 180], "cor_offset": -0.3,
           "N_eta": 48, "energy": 12.398 / 0.3}
-    case("ti8_small", ti, TI8, 10, 5.0, 4, "auto", "trapezoid", seed=3)
+    case("ti8_small", ti, TI8, 10, 5.0, 4, "auto", "trapezoid", seed=3, probed=True)
 
     mats = {}
     for name, spec in (("al5", AL5), ("ti8", TI8), ("fe5", FE5), ("ni6", NI6), ("al3", AL3)):
