@@ -76,6 +76,7 @@ SIGNATURES = {
     "dfx_score_z": ([P, P, P, L, S], c_int),
     "dfx_local_scatter": ([P, P, P, P, P, I, I, I, I, P, S], c_int),
     "dfx_local_gather": ([P, P, P, P, P, I, I, I, I, P, S], c_int),
+    "dfx_poisson_term": ([P, P, P, L, P, L, P, L, F, F, I, P, P, L, S], c_int),
     "dfx_pf_param_nq": ([I, I], c_int),
     "dfx_pf_param_vjp": ([POINTER(PFGeometry), P, P, P, P, P, I, I, I, I, I, P, P, P, P, I, P, S], c_int),
     "dfx_pf_rows_sum": ([P, I, I, I, P, S], c_int),

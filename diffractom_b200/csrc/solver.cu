@@ -131,6 +131,37 @@ __global__ void __launch_bounds__(RED_THREADS) fista_ls_update_kernel(
 }
 
 
+// ---- the Poisson data term of a prediction (optimization/poisson_term.py:36-58), mu = max(pred, 0) + bg + eps g, on
+// the points of weight != 0 (0 elsewhere; the fitted angles are the caller's weights):
+//   mode 0: r = w/g (1 - b/mu), c = w / (g max(mu, floor g))     (gradient and Fisher curvature; c may be NULL)
+//   mode 1: r = w/g b/mu                                          (the EM ratio)
+//   mode 2: r = w/g                                               (the EM sensitivity's data)
+__global__ void poisson_term_kernel(const float *__restrict__ pred, const float *__restrict__ b,
+                                    const float *__restrict__ w, int64_t pw, const float *__restrict__ g, int64_t pg,
+                                    const float *__restrict__ bg, int64_t pbg, float eps, float floor_counts, int mode,
+                                    float *__restrict__ r, float *__restrict__ c, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float wi = periodic(w, pw, i, 1.0f);
+        const float gi = periodic(g, pg, i, 1.0f);
+        float ri = 0.0f, ci = 0.0f;
+        if (wi != 0.0f) {
+            const float wg = __fdiv_rn(wi, gi);
+            if (mode == 2) {
+                ri = wg;
+            } else {
+                const float mu = __fadd_rn(__fadd_rn(fmaxf(pred[i], 0.0f), periodic(bg, pbg, i, 0.0f)),
+                                           __fmul_rn(eps, gi));
+                const float q = __fdiv_rn(b[i], mu);
+                ri = mode == 1 ? __fmul_rn(wg, q) : __fmul_rn(wg, __fsub_rn(1.0f, q));
+                ci = __fdiv_rn(wi, __fmul_rn(gi, fmaxf(mu, __fmul_rn(floor_counts, gi))));
+            }
+        }
+        r[i] = ri;
+        if (c) c[i] = ci;
+    }
+}
+
 // ---- orientation search: z = E / sqrt(max(D, 1e-30)) (NaN kept), 0 where D <= 0, with correctly rounded division
 // and square root: the float32 NumPy expression of the reference's host path, bitwise (orientation_search.py:41-54)
 __global__ void score_z_kernel(const float *__restrict__ E, const float *__restrict__ D, float *__restrict__ Z,
@@ -428,6 +459,17 @@ using namespace dfx;
         kernel<<<ew_grid(n), EW_THREADS, 0, (cudaStream_t)(stream)>>>(__VA_ARGS__);                         \
         return launch_status(#kernel);                                                                      \
     } while (0)
+
+extern "C" int dfx_poisson_term(const float *pred, const float *b, const float *w, int64_t pw, const float *g, int64_t pg,
+                                const float *bg, int64_t pbg, float eps, float floor_counts, int mode, float *r,
+                                float *c, int64_t n, void *stream)
+{
+    DFX_REQUIRE(b && r && n >= 0 && (mode == 2 || pred) && mode >= 0 && mode <= 2 && (!pw || w) && (!pg || g) &&
+                    (!pbg || bg),
+                "poisson_term: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(poisson_term_kernel, n, stream, pred, b, w, pw, g, pg, bg, pbg, eps, floor_counts, mode, r, c, n);
+}
 
 extern "C" int dfx_spdhg_dual_update(float *y, float *d, const float *sig, const float *b, const float *w, int64_t pw,
                                      const float *g, int64_t pg, const float *bg, int64_t pbg, float eps,

@@ -188,6 +188,54 @@ def build_patches(k, iy, ix, K, split=True, merge_gap=2, min_box_fill=0.5):
     return dict(pk=pk, y0=py0, x0=px0, h=ph, w=pw, coff=coff, n_coef=n_coef, mask=mask, pair_index=pair_index)
 
 
+def split_regions(mats, sigmas, support: LocalSupport, mode: str = "components", tile: int = 8, min_pairs: int = 1):
+    """Copies of the orientations, one per region of their support (differentiable/local_basis.py:17-61), so that a
+    refinement can turn every region's copy on its own (orientation gradients inside a grain).
+
+    mode "components": every 8-connected component of an orientation's voxels is a region; "tiles": the voxels are
+    grouped by tile x tile blocks of the grid; "components+tiles": components cut by the tiles. Regions of fewer
+    than min_pairs voxels are dropped. Returns (mats, sigmas, support, parent), parent[k'] the orientation that the new
+    orientation k' copies; the new orientations are numbered by parent, then region label."""
+    from scipy import ndimage
+    if mode not in ("components", "tiles", "components+tiles"):
+        raise ValueError(f"mode: 'components', 'tiles' or 'components+tiles', not {mode!r}")
+    Ny, Nx = support.Ny, support.Nx
+    n_tx = -(-Nx // tile)
+    order = np.argsort(support.k, kind="stable")
+    k, iy, ix = support.k[order], support.iy[order], support.ix[order]
+    bounds = np.searchsorted(k, np.arange(support.K + 1))
+    out_k, out_y, out_x, parent = [], [], [], []
+    for kk in range(support.K):
+        a, b = bounds[kk], bounds[kk + 1]
+        if a == b:
+            continue
+        y, x = iy[a:b], ix[a:b]
+        tiles = (y // tile) * n_tx + x // tile
+        if mode == "tiles":
+            lab = tiles
+        else:
+            y0, x0 = y.min(), x.min()
+            img = np.zeros((y.max() - y0 + 1, x.max() - x0 + 1), bool)
+            img[y - y0, x - x0] = True
+            comp, _ = ndimage.label(img, structure=np.ones((3, 3), bool))
+            lab = comp[y - y0, x - x0].astype(np.int64)
+            if mode == "components+tiles":
+                lab = lab * (Ny * Nx) + tiles
+        uniq, inv = np.unique(lab, return_inverse=True)
+        keep = np.bincount(inv, minlength=len(uniq)) >= min_pairs
+        new_id = np.full(len(uniq), -1, np.int64)
+        new_id[keep] = len(parent) + np.arange(int(keep.sum()))
+        sel = new_id[inv] >= 0
+        out_k.append(new_id[inv][sel])
+        out_y.append(y[sel])
+        out_x.append(x[sel])
+        parent.extend([kk] * int(keep.sum()))
+    parent = np.asarray(parent, np.int64)
+    cat = lambda parts: np.concatenate(parts) if parts else np.zeros(0, np.int64)
+    sup = LocalSupport(cat(out_k), cat(out_y), cat(out_x), len(parent), (Ny, Nx))
+    return np.asarray(mats)[parent], np.asarray(sigmas)[parent], sup, parent
+
+
 def _morton(y, x):
     """Z-order code of non-negative integer coordinates below 2^16 (bits of y and x interleaved)."""
     def spread(v):

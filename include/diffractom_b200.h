@@ -381,6 +381,13 @@ int dfx_local_scatter(const float *coeffs, const uint8_t *mask, const int32_t *b
 int dfx_local_gather(const float *img_k, const uint8_t *mask, const int32_t *box, const int64_t *coff,
                      const int32_t *chan, int n_patches, int nx, int ny, int kstride, float *coeffs, void *stream);
 
+/* replaces PoissonTerm's pt_grad_curv / pt_ratio / pt_wg (optimization/poisson_term.py:52-58), mu = max(pred, 0) +
+ * bg + eps g, on points of weight != 0 (0 elsewhere): mode 0 r = w/g (1 - b/mu), c = w / (g max(mu, floor g)) (c may
+ * be NULL); mode 1 r = w b / (g mu); mode 2 r = w / g (pred unused). */
+int dfx_poisson_term(const float *pred, const float *b, const float *w, int64_t pw, const float *g, int64_t pg,
+                     const float *bg, int64_t pbg, float eps, float floor_counts, int mode, float *r, float *c,
+                     int64_t n, void *stream);
+
 /* ---------------------------------------------------------------- parameter gradients
  * replaces pf_param_vjp (differentiable/pf_grad.cl:48-176, launched by PFGradient.__call__,
  * differentiable/gradients.py:112-174): for every non-zero (r, k, j) of a batch's adjoint CSR (orientations

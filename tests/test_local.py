@@ -48,3 +48,34 @@ def test_patches_cover_the_pairs_once():
 def test_merge_boxes_merges_overlaps():
     out = sorted(_merge_boxes([[0, 4, 0, 4], [3, 8, 3, 8], [20, 21, 20, 21], [7, 9, 0, 1]]))
     assert out == [[0, 9, 0, 8], [20, 21, 20, 21]]
+
+
+def test_split_regions():
+    """Components, tiles and both: every region of an orientation becomes a copy (parent), the copies' voxels are
+    exactly the original pairs, regions below min_pairs are dropped."""
+    from diffractom_b200.local import LocalSupport, split_regions
+    K, Ny, Nx = 3, 12, 10
+    m = np.zeros((K, Ny, Nx), bool)
+    m[0, 1:3, 1:3] = True          # two 8-connected components
+    m[0, 7:10, 6:9] = True
+    m[1, 2, 2] = m[1, 3, 3] = True  # diagonal neighbours: one component
+    m[2, 0:12, 4] = True           # a column crossing tiles
+    sup = LocalSupport.from_mask(m)
+    mats = np.stack([np.eye(3) * (i + 1) for i in range(K)])
+    sig = np.arange(K, dtype=np.float64) + 0.1
+    m2, s2, sp, parent = split_regions(mats, sig, sup, mode="components")
+    assert list(parent) == [0, 0, 1, 2] and np.array_equal(m2, mats[parent]) and np.array_equal(s2, sig[parent])
+    back = np.zeros_like(m)
+    for k2, y, x in zip(sp.k, sp.iy, sp.ix):
+        back[parent[k2], y, x] = True
+    assert np.array_equal(back, m)
+    # 4 x 4 tiles: orientation 0's blobs cover tile (0, 0) and tiles (1..2, 1..2); orientation 2's column 3 tiles
+    _, _, sp_t, par_t = split_regions(mats, sig, sup, mode="tiles", tile=4)
+    assert list(par_t) == [0] * 5 + [1] + [2] * 3
+    _, _, sp_c, par_c = split_regions(mats, sig, sup, mode="components+tiles", tile=4)
+    assert list(par_c) == [0] * 5 + [1] + [2] * 3
+    assert sp_c.n_pairs == sup.n_pairs
+    _, _, sp_m, par_m = split_regions(mats, sig, sup, mode="components", min_pairs=3)
+    assert list(par_m) == [0, 0, 2]
+    with pytest.raises(ValueError):
+        split_regions(mats, sig, sup, mode="rings")
