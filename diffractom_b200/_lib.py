@@ -77,6 +77,9 @@ SIGNATURES = {
     "dfx_local_scatter": ([P, P, P, P, P, I, I, I, I, P, S], c_int),
     "dfx_local_gather": ([P, P, P, P, P, I, I, I, I, P, S], c_int),
     "dfx_poisson_term": ([P, P, P, L, P, L, P, L, F, F, I, P, P, L, S], c_int),
+    "dfx_tv_dual": ([P, P, P, P, P, P, I, I, I, F, F, S], c_int),
+    "dfx_tv_adjoint_update": ([P, P, P, P, P, I, I, I, F, F, S], c_int),
+    "dfx_tv_value": ([P, P, I, I, I, P, P, c_size_t, S], c_int),
     "dfx_pf_param_nq": ([I, I], c_int),
     "dfx_pf_param_vjp": ([POINTER(PFGeometry), P, P, P, P, P, I, I, I, I, I, P, P, P, P, I, P, S], c_int),
     "dfx_pf_rows_sum": ([P, I, I, I, P, S], c_int),

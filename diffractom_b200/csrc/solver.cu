@@ -131,6 +131,95 @@ __global__ void __launch_bounds__(RED_THREADS) fista_ls_update_kernel(
 }
 
 
+// ---- SPDHG's total-variation block on a channel-fastest batch (npix x kstride, kb live channels): forward
+// differences to the right (+1 pixel) and down (+nx pixels) between free coefficients (T > 0 at both ends), the dual
+// q = (qx, qy) per coefficient projected onto |q| <= lam after the step s = ps / (4 max(T_j + T_right, T_j + T_down))
+// (spdhg_poisson.py:110-165). The float32 operations are correctly rounded, in the reference's order.
+__device__ __forceinline__ void tv_dual_core(float tj, float tr, float td, bool vr0, bool vd0, float xj, float xr,
+                                             float xd, float ox, float oy, float lam, float ps, float &nx, float &ny)
+{
+    const bool vr = vr0 && tj > 0.0f && tr > 0.0f;
+    const bool vd = vd0 && tj > 0.0f && td > 0.0f;
+    float m = 0.0f;
+    if (vr) m = fmaxf(m, __fadd_rn(tj, tr));
+    if (vd) m = fmaxf(m, __fadd_rn(tj, td));
+    float ax = 0.0f, ay = 0.0f;
+    if (m > 0.0f) {
+        const float st = __fdiv_rn(ps, __fmul_rn(4.0f, m));
+        if (vr) ax = __fadd_rn(ox, __fmul_rn(st, __fsub_rn(xr, xj)));
+        if (vd) ay = __fadd_rn(oy, __fmul_rn(st, __fsub_rn(xd, xj)));
+        const float nrm = __fsqrt_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)));
+        if (nrm > lam) {
+            const float c = __fdiv_rn(lam, nrm);
+            ax = __fmul_rn(ax, c);
+            ay = __fmul_rn(ay, c);
+        }
+    }
+    nx = ax;
+    ny = ay;
+}
+
+// q <- proj(q + s D x), dq = q' - q (dq batch-sized)
+__global__ void tv_dual_kernel(const float *__restrict__ x, const float *__restrict__ T, float *__restrict__ qx,
+                               float *__restrict__ qy, float *__restrict__ dqx, float *__restrict__ dqy, int nx, int ny,
+                               int kstride, float lam, float ps, int64_t n)
+{
+    const int64_t row = (int64_t)nx * kstride;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pix = i / kstride;
+        const int ix = (int)(pix % nx), iy = (int)(pix / nx);
+        const bool vr0 = ix + 1 < nx, vd0 = iy + 1 < ny;
+        const float tr = vr0 ? T[i + kstride] : 0.0f, td = vd0 ? T[i + row] : 0.0f;
+        const float xr = vr0 ? x[i + kstride] : 0.0f, xd = vd0 ? x[i + row] : 0.0f;
+        const float ox = qx[i], oy = qy[i];
+        float nxv, nyv;
+        tv_dual_core(T[i], tr, td, vr0, vd0, x[i], xr, xd, ox, oy, lam, ps, nxv, nyv);
+        qx[i] = nxv;
+        qy[i] = nyv;
+        dqx[i] = __fsub_rn(nxv, ox);
+        dqy[i] = __fsub_rn(nyv, oy);
+    }
+}
+
+// dz = D^T dq, then the primal step of SPDHG with it: z += dz; x = T > 0 ? max(0, x - T (z + inv_p dz + lam)) : 0
+__global__ void tv_adjoint_update_kernel(const float *__restrict__ dqx, const float *__restrict__ dqy,
+                                         float *__restrict__ x, float *__restrict__ z, const float *__restrict__ T,
+                                         int nx, int kstride, float inv_p, float lam, int64_t n)
+{
+    const int64_t row = (int64_t)nx * kstride;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pix = i / kstride;
+        const int ix = (int)(pix % nx);
+        float v = __fsub_rn(-dqx[i], dqy[i]);
+        if (ix > 0) v = __fadd_rn(v, dqx[i - kstride]);
+        if (pix >= nx) v = __fadd_rn(v, dqy[i - row]);
+        const float zi = __fadd_rn(z[i], v);
+        z[i] = zi;
+        const float zb = __fadd_rn(zi, __fmul_rn(inv_p, v));
+        const float t = T[i];
+        x[i] = t > 0.0f ? fmaxf(0.0f, __fsub_rn(x[i], __fmul_rn(t, __fadd_rn(zb, lam)))) : 0.0f;
+    }
+}
+
+// sum of |D x| over the coefficients (float32 norms, float64 sum)
+__global__ void __launch_bounds__(RED_THREADS) tv_value_kernel(const float *__restrict__ x,
+                                                               const float *__restrict__ T, int nx, int ny,
+                                                               int kstride, int64_t n, double *__restrict__ part)
+{
+    const int64_t row = (int64_t)nx * kstride;
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pix = i / kstride;
+        const int ix = (int)(pix % nx), iy = (int)(pix / nx);
+        const bool vr0 = ix + 1 < nx, vd0 = iy + 1 < ny;
+        const float tj = T[i];
+        const float gx = (vr0 && tj > 0.0f && T[i + kstride] > 0.0f) ? __fsub_rn(x[i + kstride], x[i]) : 0.0f;
+        const float gy = (vd0 && tj > 0.0f && T[i + row] > 0.0f) ? __fsub_rn(x[i + row], x[i]) : 0.0f;
+        v[0] += (double)__fsqrt_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)));
+    }
+    block_sum<1>(v, part + blockIdx.x);
+}
+
 // ---- the Poisson data term of a prediction (optimization/poisson_term.py:36-58), mu = max(pred, 0) + bg + eps g, on
 // the points of weight != 0 (0 elsewhere; the fitted angles are the caller's weights):
 //   mode 0: r = w/g (1 - b/mu), c = w / (g max(mu, floor g))     (gradient and Fisher curvature; c may be NULL)
@@ -459,6 +548,38 @@ using namespace dfx;
         kernel<<<ew_grid(n), EW_THREADS, 0, (cudaStream_t)(stream)>>>(__VA_ARGS__);                         \
         return launch_status(#kernel);                                                                      \
     } while (0)
+
+extern "C" int dfx_tv_dual(const float *x, const float *T, float *qx, float *qy, float *dqx, float *dqy, int nx,
+                           int ny, int kstride, float lam, float ps, void *stream)
+{
+    DFX_REQUIRE(x && T && qx && qy && dqx && dqy && nx > 0 && ny > 0 && kstride > 0, "tv_dual: bad arguments");
+    const int64_t n = (int64_t)nx * ny * kstride;
+    EW_LAUNCH(tv_dual_kernel, n, stream, x, T, qx, qy, dqx, dqy, nx, ny, kstride, lam, ps, n);
+}
+
+extern "C" int dfx_tv_adjoint_update(const float *dqx, const float *dqy, float *x, float *z, const float *T, int nx,
+                                     int ny, int kstride, float inv_p, float lam, void *stream)
+{
+    DFX_REQUIRE(dqx && dqy && x && z && T && nx > 0 && ny > 0 && kstride > 0, "tv_adjoint_update: bad arguments");
+    const int64_t n = (int64_t)nx * ny * kstride;
+    EW_LAUNCH(tv_adjoint_update_kernel, n, stream, dqx, dqy, x, z, T, nx, kstride, inv_p, lam, n);
+}
+
+extern "C" int dfx_tv_value(const float *x, const float *T, int nx, int ny, int kstride, double *out, void *scratch,
+                            size_t scratch_bytes, void *stream)
+{
+    DFX_REQUIRE(x && T && out && nx > 0 && ny > 0 && kstride > 0, "tv_value: bad arguments");
+    const int64_t n = (int64_t)nx * ny * kstride;
+    int st = check_scratch(scratch, scratch_bytes, n, 1);
+    if (st) return st;
+    const int nb = red_blocks(n);
+    cudaStream_t s = (cudaStream_t)stream;
+    tv_value_kernel<<<nb, RED_THREADS, 0, s>>>(x, T, nx, ny, kstride, n, (double *)scratch);
+    st = launch_status("tv_value");
+    if (st) return st;
+    finish_sums<1><<<1, RED_THREADS, 0, s>>>((const double *)scratch, nb, out);
+    return launch_status("finish_sums");
+}
 
 extern "C" int dfx_poisson_term(const float *pred, const float *b, const float *w, int64_t pw, const float *g, int64_t pg,
                                 const float *bg, int64_t pbg, float eps, float floor_counts, int mode, float *r,

@@ -1,7 +1,7 @@
 """SPDHGPoisson: stochastic primal-dual hybrid gradient over omega subsets for the Poisson deviance, on a B200.
 
-Drop-in for diffractom's SPDHGPoisson (optimization/spdhg_poisson.py) without the total-variation block: the same
-arguments, subset schedule (numpy default_rng(seed) permutations, an epoch never starting with the subset that ended
+Drop-in for diffractom's SPDHGPoisson (optimization/spdhg_poisson.py), with the dense total-variation block: the
+same arguments, subset schedule (numpy default_rng(seed) permutations, an epoch never starting with the subset that ended
 the previous one), step sizes (diagonal preconditioning: S_i = gamma / (A 1_S)_i, T_j = min_m p_m / (gamma (A_m^T
 1_counted)_j), gamma = sqrt(rho), rho = 3e4 / mean(b)^2 by default), the same pass structure (one pass over the
 orientation batches per iteration: the adjoint of the current subset's dual change, the update of z and x, the
@@ -36,6 +36,8 @@ from .streaming import BatchPipeline, CoeffArray, KMajorStaging, host_copier
 
 RHO_AUTO = 3e4
 NAMES = ("x", "z", "T")
+TV_NAMES = ("qx", "qy")  # the TV dual (tv > 0), after x, z, T
+TV_SAFETY = 0.99         # the TV dual step: this fraction of its bound (spdhg_poisson.py:277)
 MARGIN_GB = 1.5          # resident="auto": device memory left free (spdhg_poisson.py:278)
 
 
@@ -56,16 +58,26 @@ class SPDHGPoisson:
                  seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None, shards=None):
         """Arguments as diffractom's SPDHGPoisson (spdhg_poisson.py:301-302). resident ("auto", "all", "none" or a
         list of names from ("x", "z", "T")): which coefficient arrays of a run with a NumPy x0 stay on the device;
-        the others are streamed from pinned host memory (a CUDA x0 keeps all three on the device). tv > 0 (the TV
-        block) is not provided. shards (this package's extension; a sharding.ShardSum): the operator holds one
-        orientation shard of a process group, and the forward's data rows are summed over the shards after each
-        pass; every rank passes the same seed and subsets."""
+        the others are streamed from pinned host memory (a CUDA x0 keeps all three on the device). tv > 0: the total
+        variation of every orientation's image as one more block of the serial sampling, chosen with probability
+        tv_prob (default 1 / (M + 1)); its dual (qx, qy) is two more coefficient arrays, resident or streamed as x, z,
+        T (spdhg_poisson.py:20-40, 320-324); not with the local basis, the hierarchical tv_tree or shards. shards
+        (this package's extension; a sharding.ShardSum): the operator holds one orientation shard of a process
+        group, and the forward's data rows are summed over the shards after each pass; every rank passes the same
+        seed and subsets."""
         if prox_kind not in ("nonneg", "nonneg_l1"):
             raise ValueError("SPDHGPoisson supports prox_kind 'nonneg' and 'nonneg_l1'")
-        if not (resident in ("auto", "all", "none") or set(resident) <= set(NAMES + ("qx", "qy"))):
-            raise ValueError(f"resident must be 'auto', 'all', 'none' or a list of names from {NAMES}")
-        if float(tv) != 0.0 or tv_tree is not None:
-            raise NotImplementedError("the total-variation block of SPDHGPoisson is not provided")
+        if not (resident in ("auto", "all", "none") or set(resident) <= set(NAMES + TV_NAMES)):
+            raise ValueError(f"resident must be 'auto', 'all', 'none' or a list of names from {NAMES + TV_NAMES}")
+        tv = float(tv)
+        if tv < 0:
+            raise ValueError("tv must be >= 0")
+        if tv_tree is not None:
+            if tv <= 0:
+                raise ValueError("tv_tree needs tv > 0")
+            raise NotImplementedError("the hierarchical total variation (tv_tree) is not provided")
+        if tv > 0 and (shards is not None or getattr(operator, "coefficient_layout", "dense") != "dense"):
+            raise NotImplementedError("the total-variation block needs the (K, Ny, Nx) layout on one device")
         self.op = operator
         self.ctx, self.queue = operator.ctx, operator.queue
         self.subsets = operator.set_omega_subsets(subsets)
@@ -75,9 +87,15 @@ class SPDHGPoisson:
         self.rho = rho if rho == "auto" else float(rho)
         self.rng = np.random.default_rng(seed)
         self.resident = resident
-        self.tv, self.tv_prob = 0.0, 0.0
-        self._p_data = 1.0 / self.M
-        self._inv_p_data = float(self.M)
+        self.tv = tv
+        self.tv_prob = (1.0 / (self.M + 1) if tv_prob is None else float(tv_prob)) if tv > 0 else 0.0
+        if tv > 0 and not 0 < self.tv_prob < 1:
+            raise ValueError("tv_prob must be in (0, 1)")
+        self._n_tv = max(1, int(round(self.M * self.tv_prob / (1 - self.tv_prob)))) if tv > 0 else 0
+        self._names = NAMES + (TV_NAMES if tv > 0 else ())
+        # step probabilities: the data subsets (1 - p_tv) / M each, the TV block p_tv (spdhg_poisson.py:349-352)
+        self._p_data = (1.0 - self.tv_prob) / self.M
+        self._inv_p_data = float(self.M) if tv == 0 else 1.0 / self._p_data
         self._last = None
         self.support_gpu = support_mask_to_device(operator, support, operator.device)
         self.shards = shards
@@ -94,7 +112,15 @@ class SPDHGPoisson:
         return [int(m) for m in perm]
 
     def _epoch_sequence(self):
-        return self._epoch_order()
+        """The blocks of the next epoch: the subsets and, with tv, the TV block (-1) inserted _n_tv times at random
+        places (spdhg_poisson.py:373-381; without tv the random numbers drawn are those of _epoch_order alone)."""
+        order = self._epoch_order()
+        if self.tv <= 0:
+            return order
+        n = len(order) + self._n_tv
+        tv_at = set(int(i) for i in self.rng.choice(n, self._n_tv, replace=False))
+        it = iter(order)
+        return [-1 if i in tv_at else next(it) for i in range(n)]
 
     # ---------------------------------------------------------------- device steps
     def _dual(self, m):
@@ -104,26 +130,45 @@ class SPDHGPoisson:
                   self.b.data_ptr(), _ptr(self.w), self.pw, _ptr(self.g), self.pg, _ptr(self.bg), self.pbg,
                   self.eps_counts, e["omegas"].data_ptr(), e["n"], op.My * op.N_seg, op._s())
 
-    def _pass(self, adj, fwd):
-        """One pass over the batches: adjoint of subset adj's dual change (in D), z and x updated; then the forward
-        of the new x for subset fwd ("full": all rows) added to D (spdhg_poisson.py:430-484)."""
+    def _tv_batch(self, ib, s):
+        """The TV block on batch ib: its dual step (qx, qy) and D^T of the dual change with the primal step."""
+        op = self.op
+        Q, R_ = self.QX, self.QY
+        _lib.call("dfx_tv_dual", self.X.ptr(ib, s), self.T.ptr(ib, s), Q.ptr(ib, s), R_.ptr(ib, s),
+                  self.dqx.data_ptr(), self.dqy.data_ptr(), op.Nx, op.Ny, op.Kstride, float(self.tv),
+                  float(TV_SAFETY * self.tv_prob), op._s())
+        _lib.call("dfx_tv_adjoint_update", self.dqx.data_ptr(), self.dqy.data_ptr(), self.X.ptr(ib, s),
+                  self.Z.ptr(ib, s), self.T.ptr(ib, s), op.Nx, op.Ny, op.Kstride, float(1.0 / self.tv_prob),
+                  self.lam, op._s())
+
+    def _arrays(self, upd, tv):
+        """(loaded, stored) state arrays of a pass."""
+        if tv:
+            return [self.X, self.Z, self.T, self.QX, self.QY], [self.X, self.Z, self.QX, self.QY]
+        return ([self.X, self.Z, self.T] if upd else [self.X]), ([self.X, self.Z] if upd else [])
+
+    def _pass(self, adj, fwd, tv=False):
+        """One pass over the batches: adjoint of subset adj's dual change (in D), z and x updated (tv: the TV block's
+        dual step and update instead); then the forward of the new x for subset fwd ("full": all rows) added to D
+        (spdhg_poisson.py:430-484)."""
         op = self.op
         if op.precision == "bf16" and fwd != "full":
-            self._pass_bf16(adj, fwd)
+            self._pass_bf16(adj, fwd, tv)
             return
         sub = None if fwd == "full" else fwd
         X, Z, T = self.X, self.Z, self.T
 
         def compute(ib, s):
             xp = X.ptr(ib, s)
-            if adj is not None:       # A_m^T of the dual change, z and x updated in the backprojection's epilogue
+            if tv:
+                self._tv_batch(ib, s)
+            elif adj is not None:       # A_m^T of the dual change, z and x updated in the backprojection's epilogue
                 op._adjoint_update_batch(self.D, ib, adj, xp, Z.ptr(ib, s), T.ptr(ib, s), self._inv_p_data,
                                          self.lam)
             if fwd is not None:
                 op._direct_batch_k(xp, ib, self.D, sub, ray=self._ray)
 
-        upd = adj is not None
-        self.pipe.run([X, Z, T] if upd else [X], [X, Z] if upd else [], compute)
+        self.pipe.run(*self._arrays(adj is not None, tv), compute)
         if fwd is not None:
             self._sum_shards(fwd)
 
@@ -137,7 +182,7 @@ class SPDHGPoisson:
         else:
             self.shards.rows(self.D, op._sub[op._subset(fwd)]["omegas"], op.stream())
 
-    def _pass_bf16(self, adj, fwd):
+    def _pass_bf16(self, adj, fwd, tv=False):
         """The pass of an operator with precision "bf16": one tensor-core launch takes the dual change of subset adj
         to the BF16 Radon output of all batches, each batch's backprojection applies the primal step and projects the
         new x for subset fwd into its columns of that output, and one tensor-core launch overwrites subset fwd's data
@@ -151,7 +196,10 @@ class SPDHGPoisson:
 
         def compute(ib, s):
             xb = self.xkb.data_ptr() + (2 * ib * be if X.resident else 0)
-            if adj is not None:
+            if tv:                          # the TV block, then the BF16 copy of the new x
+                self._tv_batch(ib, s)
+                _lib.call("dfx_f32_to_bf16", X.ptr(ib, s), xb, be, op._s())
+            elif adj is not None:
                 op._bf16_update_batch(ib, geo, n, zb, X.ptr(ib, s), Z.ptr(ib, s), T.ptr(ib, s), self._inv_p_data,
                                       self.lam, xb)
             elif not X.resident:
@@ -159,14 +207,27 @@ class SPDHGPoisson:
             if fwd is not None:
                 op._bf16_forward_sino(fwd, ib, xb, src_bf16=True, ray=self._ray)
 
-        upd = adj is not None
-        self.pipe.run([X, Z, T] if upd else [X], [X, Z] if upd else [], compute)
+        self.pipe.run(*self._arrays(adj is not None, tv), compute)
         if fwd is not None:
             op._bf16_forward_rows(fwd, self.D)
             self._sum_shards(fwd)
 
     def _deviance(self, mu):
         return self.red.deviance(mu, self.b, self.w, self.pw, self.g, self.pg, self.bg, self.pbg, self.eps_counts)
+
+    def _tv_value(self):
+        """sum_k TV(x_k) (a pass over the batches; float64)."""
+        op = self.op
+        nb = op._lib.dfx_reduce_scratch_bytes(op.batch_elems())
+        total = torch.zeros(len(op.batches), dtype=torch.float64, device=op.device)
+
+        def compute(ib, s):
+            scr = op.scratch(nb)
+            _lib.call("dfx_tv_value", self.X.ptr(ib, s), self.T.ptr(ib, s), op.Nx, op.Ny, op.Kstride,
+                      total.data_ptr() + 8 * ib, scr.data_ptr(), nb, op._s())
+
+        self.pipe.run([self.X, self.T], [], compute)
+        return float(total.sum().item())
 
     # ---------------------------------------------------------------- run
     @on_op_stream
@@ -325,11 +386,13 @@ class SPDHGPoisson:
         # or in pinned host memory streamed through two device slots
         be = op.batch_elems()
         nbt = len(op.batches)
+        if state is not None and self.tv > 0 and state.get("z") is None:
+            raise ValueError("continuing a TV run needs the state's z")
         resident = self._choose_resident()
-        self.resident_used = tuple(nm for nm in NAMES if nm in resident)
+        self.resident_used = tuple(nm for nm in self._names if nm in resident)
         self.X, self.Z, self.T = (CoeffArray(op, nm, nm in resident) for nm in NAMES)
         self.pipe = BatchPipeline(op)
-        self._stage = None if len(resident) == len(NAMES) else KMajorStaging(op)
+        self._stage = None if len(resident) == len(self._names) else KMajorStaging(op)
         self.dzk = torch.empty(be, dtype=torch.float32, device=dev)
         self.x = None
         if self.X.resident:
@@ -351,6 +414,22 @@ class SPDHGPoisson:
             op._fill(self.Z.dev, 0.0)
         else:
             self.Z.host.zero_()
+        self.QX = self.QY = self.dqx = self.dqy = None
+        if self.tv > 0:                                 # the TV dual (state or 0) and its change per batch
+            self.QX, self.QY = (CoeffArray(op, nm, nm in resident) for nm in TV_NAMES)
+            for arr, nm in ((self.QX, "qx"), (self.QY, "qy")):
+                q0 = None if state is None or state.get(nm) is None else as_host(state[nm], cshape, f"state['{nm}']")
+                if q0 is None:
+                    if arr.resident:
+                        op._fill(arr.dev, 0.0)
+                    else:
+                        arr.host.zero_()
+                elif arr.resident:
+                    op.to_batches(torch.as_tensor(q0, device=dev), arr.dev)
+                else:
+                    self._stage.load(q0.reshape(-1), arr, self.pipe)
+            self.dqx = torch.empty(be, dtype=torch.float32, device=dev)
+            self.dqy = torch.empty(be, dtype=torch.float32, device=dev)
 
         self._ray = op.support_ray_table(supp) if supp is not None and self.use_support_table else None
         # S from the row sums A 1_S (spdhg_poisson.py:621-629)
@@ -397,8 +476,9 @@ class SPDHGPoisson:
                 _lib.call("dfx_f32_to_bf16", self.X.dev.data_ptr(), self.xkb.data_ptr(), nbt * be, s)
             else:
                 self.xkb = torch.empty(be, dtype=torch.bfloat16, device=dev)
-        op.zero_subset_rows(self.D, self._seq[0])
-        self._pass(None, self._seq[0])
+        if self._seq[0] >= 0:
+            op.zero_subset_rows(self.D, self._seq[0])
+            self._pass(None, self._seq[0])
 
     @on_op_stream
     def _iterate(self, n_epochs, verbose=0, diagnostics_interval=1, callback=None, final=True):
@@ -412,7 +492,7 @@ class SPDHGPoisson:
             last = final and e + 1 == n_epochs
             want_f = (len(self.iter_stats) + 1) % max(1, diagnostics_interval) == 0 or last
             nseq = None
-            for j, m in enumerate(seq):
+            for j, blk in enumerate(seq):
                 end_of_epoch = j + 1 == len(seq)
                 if not end_of_epoch:
                     nb = seq[j + 1]
@@ -421,23 +501,30 @@ class SPDHGPoisson:
                     nb = nseq[0]
                 else:
                     nb = None
-                graphed = not ((end_of_epoch and want_f) or nb is None or nb == m) and self._graphs_on()
-                if not graphed:
-                    self._dual(m)
-                if (end_of_epoch and want_f) or nb is None or nb == m:
-                    self._pass(m, None)
-                    if (end_of_epoch and want_f) or nb is not None:
+                adj = blk if blk >= 0 else None          # a data subset, or the TV block (-1)
+                tvb = adj is None
+                m_next = nb if nb is not None and nb >= 0 else None
+                full = (end_of_epoch and want_f) or nb is None or (m_next is not None and m_next == adj)
+                graphed = not full and not tvb and m_next is not None and self._graphs_on()
+                if adj is not None and not graphed:
+                    self._dual(adj)
+                if full:
+                    self._pass(adj, None, tv=tvb)
+                    if (end_of_epoch and want_f) or m_next is not None:
                         op._fill(self.D, 0.0)
                         self._pass(None, "full")
                         if end_of_epoch and want_f:
                             self._f = self._deviance(self.D)
+                            if self.tv > 0:
+                                self._f += self.tv * self._tv_value()
                 elif graphed:
-                    self._replay(("update", m), lambda m=m: (self._dual(m), self._pass(m, None)))
-                    self._replay(("forward", nb), lambda nb=nb: (op.zero_subset_rows(self.D, nb),
-                                                                 self._pass(None, nb)))
+                    self._replay(("update", adj), lambda m=adj: (self._dual(m), self._pass(m, None)))
+                    self._replay(("forward", m_next), lambda nb=m_next: (op.zero_subset_rows(self.D, nb),
+                                                                         self._pass(None, nb)))
                 else:
-                    op.zero_subset_rows(self.D, nb)
-                    self._pass(m, nb)
+                    if m_next is not None:
+                        op.zero_subset_rows(self.D, m_next)
+                    self._pass(adj, m_next, tv=tvb)
             if nseq is not None:
                 seq = nseq
             self._seq = seq
@@ -459,6 +546,7 @@ class SPDHGPoisson:
     def _graphs_on(self):
         op = self.op
         return (self.use_graphs and len(self.iter_stats) >= 1 and self.shards is None and self.X.resident
+                and self.tv == 0
                 and torch.cuda.current_stream(op.device) != torch.cuda.default_stream(op.device))
 
     def _replay(self, key, fn):
@@ -489,20 +577,21 @@ class SPDHGPoisson:
         """The coefficient arrays kept on the device (spdhg_poisson.py:411-428): all of them for a CUDA x0 or
         resident="all"; for "auto" as many of x, z, T (in this order) as fit into the free device memory less the
         streaming buffers and a margin."""
+        names = self._names
         if self._x_on_gpu or self.resident == "all":
-            return set(NAMES)
+            return set(names)
         if self.resident == "none":
             return set()
         if self.resident != "auto":
-            return set(self.resident) & set(NAMES)
+            return set(self.resident) & set(names)
         op = self.op
         be = op.batch_elems()
         nbytes = 4 * be * len(op.batches)
         free, _ = torch.cuda.mem_get_info(op.device)
         # two slots per streamed array, the k-major staging buffer, the batch scratch and a BF16 batch of x
-        staging = (4 * 2 * len(NAMES) + 4 + 4 + 2) * be
+        staging = (4 * 2 * len(names) + 4 + 4 + 2 + (8 if self.tv > 0 else 0)) * be
         n = int(max(0, free - staging - MARGIN_GB * 1024 ** 3) // nbytes)
-        return set(NAMES[:min(n, len(NAMES))])
+        return set(names[:min(n, len(names))])
 
     @on_op_stream
     def _finish(self):
@@ -517,17 +606,30 @@ class SPDHGPoisson:
         else:
             z_host = np.empty(op.coeff_shape, np.float32)
             self._stage.store(self.Z, z_host.reshape(-1), self.pipe)
+        tv_state = {}
+        for arr, nm in ((self.QX, "qx"), (self.QY, "qy")):
+            if arr is None:
+                continue
+            h = np.empty(op.coeff_shape, np.float32)
+            if arr.resident:
+                q = torch.empty(op.coeff_shape, dtype=torch.float32, device=op.device)
+                op.from_batches(arr.dev, q)
+                host_copier().to_host(q, h)
+            else:
+                self._stage.store(arr, h.reshape(-1), self.pipe)
+            tv_state[nm] = h
         self.pipe.synchronize()
         y_host = np.empty(op.data_shape, np.float32)
         host_copier().to_host(self.y, y_host)
-        self.state = {"epoch": self._ep0 + len(self.iter_stats), "z": z_host, "y": y_host}
+        self.state = {"epoch": self._ep0 + len(self.iter_stats), "z": z_host, "y": y_host, **tv_state}
         self.final_stats = {"epochs": len(self.iter_stats), "final_f": self._f, "setup_s": self._t_setup,
                             "rho": self.rho_used, "subsets": self.M, "resident": self.resident_used,
-                            "time": time.perf_counter() - self._t_start, "tv": 0.0, "tv_prob": 0.0,
+                            "time": time.perf_counter() - self._t_start, "tv": self.tv, "tv_prob": self.tv_prob,
                             "graph_replays": self.graph_replays, **self.scales}
         out = self.x if self._x_on_gpu else self._host_x
         self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = None
         self.X = self.Z = self.T = self.dzk = self.xkb = self._stage = self._ray = None
+        self.QX = self.QY = self.dqx = self.dqy = None
         self._graphs = {}
         self.x = None
         return out

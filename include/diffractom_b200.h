@@ -381,6 +381,19 @@ int dfx_local_scatter(const float *coeffs, const uint8_t *mask, const int32_t *b
 int dfx_local_gather(const float *img_k, const uint8_t *mask, const int32_t *box, const int64_t *coff,
                      const int32_t *chan, int n_patches, int nx, int ny, int kstride, float *coeffs, void *stream);
 
+/* replaces tv_dual_dense / tv_adjoint_dense + spdhg_update / tv_value_dense (optimization/spdhg_poisson.py:110-186)
+ * on one channel-fastest batch (nx * ny pixels x kstride channels; T = 0 on padding channels): SPDHG's total-variation
+ * block. dfx_tv_dual: q <- proj_{|q| <= lam}(q + s D x) with forward differences to the right and down between
+ * coefficients with T > 0, s = ps / (4 max(T_j + T_neighbour)), dq = q' - q (batch-sized). dfx_tv_adjoint_update:
+ * dz = D^T dq, z += dz, x = T > 0 ? max(0, x - T (z + inv_p dz + lam)) : 0. dfx_tv_value: out[0] = sum |D x| (float64
+ * sum; scratch of dfx_reduce_scratch_bytes(nx * ny * kstride)). */
+int dfx_tv_dual(const float *x, const float *T, float *qx, float *qy, float *dqx, float *dqy, int nx, int ny,
+                int kstride, float lam, float ps, void *stream);
+int dfx_tv_adjoint_update(const float *dqx, const float *dqy, float *x, float *z, const float *T, int nx, int ny,
+                          int kstride, float inv_p, float lam, void *stream);
+int dfx_tv_value(const float *x, const float *T, int nx, int ny, int kstride, double *out, void *scratch,
+                 size_t scratch_bytes, void *stream);
+
 /* replaces PoissonTerm's pt_grad_curv / pt_ratio / pt_wg (optimization/poisson_term.py:52-58), mu = max(pred, 0) +
  * bg + eps g, on points of weight != 0 (0 elsewhere): mode 0 r = w/g (1 - b/mu), c = w / (g max(mu, floor g)) (c may
  * be NULL); mode 1 r = w b / (g mu); mode 2 r = w / g (pred unused). */

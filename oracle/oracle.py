@@ -208,11 +208,83 @@ def epoch_order(rng, M, last):
     return [int(m) for m in perm], int(perm[-1])
 
 
+def epoch_sequence(rng, M, last, n_tv):
+    """SPDHGPoisson._epoch_sequence (spdhg_poisson.py:373-381): the epoch's subsets with the TV block (-1) inserted
+    n_tv times at random places."""
+    order, last = epoch_order(rng, M, last)
+    if n_tv == 0:
+        return order, last
+    n = M + n_tv
+    tv_at = set(int(i) for i in rng.choice(n, n_tv, replace=False))
+    it = iter(order)
+    return [-1 if i in tv_at else next(it) for i in range(n)], last
+
+
+def _shifted(a, axis):
+    """The right (axis 2) or lower (axis 1) neighbour of every pixel of (K, Ny, Nx) a, 0 past the edge."""
+    out = np.zeros_like(a)
+    if axis == 2:
+        out[:, :, :-1] = a[:, :, 1:]
+    else:
+        out[:, :-1, :] = a[:, 1:, :]
+    return out
+
+
+def tv_dual(x, T, qx, qy, lam, ps):
+    """tv_dual_dense (spdhg_poisson.py:110-151) on (K, Ny, Nx) float32 arrays, float32 arithmetic in the kernel's
+    order: returns (qx', qy', dqx, dqy)."""
+    f = np.float32
+    x, T, qx, qy = (np.asarray(a, f) for a in (x, T, qx, qy))
+    K, Ny, Nx = x.shape
+    vr0 = np.broadcast_to(np.arange(Nx) + 1 < Nx, x.shape)
+    vd0 = np.broadcast_to((np.arange(Ny) + 1 < Ny)[:, None], x.shape)
+    tr, td, xr, xd = _shifted(T, 2), _shifted(T, 1), _shifted(x, 2), _shifted(x, 1)
+    vr = vr0 & (T > 0) & (tr > 0)
+    vd = vd0 & (T > 0) & (td > 0)
+    m = np.zeros_like(x)
+    m = np.where(vr, np.maximum(m, T + tr), m)
+    m = np.where(vd, np.maximum(m, T + td), m)
+    pos = m > 0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        st = np.where(pos, f(ps) / (f(4) * m), f(0))
+    ax = np.where(vr & pos, qx + st * (xr - x), f(0)).astype(f)
+    ay = np.where(vd & pos, qy + st * (xd - x), f(0)).astype(f)
+    nrm = np.sqrt(ax * ax + ay * ay)
+    big = nrm > f(lam)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        c = np.where(big, f(lam) / nrm, f(1))
+    ax = np.where(big, ax * c, ax).astype(f)
+    ay = np.where(big, ay * c, ay).astype(f)
+    return ax, ay, (ax - qx).astype(f), (ay - qy).astype(f)
+
+
+def tv_adjoint(dqx, dqy):
+    """tv_adjoint_dense (spdhg_poisson.py:153-165): dz = D^T dq."""
+    v = (-dqx - dqy).astype(np.float32)
+    v[:, :, 1:] += dqx[:, :, :-1]
+    v[:, 1:, :] += dqy[:, :-1, :]
+    return v
+
+
+def tv_value(x, T):
+    """tv_value_dense (spdhg_poisson.py:167-181): sum of the float32 gradient norms, float64 sum."""
+    f = np.float32
+    x, T = np.asarray(x, f), np.asarray(T, f)
+    K, Ny, Nx = x.shape
+    vr = np.broadcast_to(np.arange(Nx) + 1 < Nx, x.shape) & (T > 0) & (_shifted(T, 2) > 0)
+    vd = np.broadcast_to((np.arange(Ny) + 1 < Ny)[:, None], x.shape) & (T > 0) & (_shifted(T, 1) > 0)
+    gx = np.where(vr, _shifted(x, 2) - x, f(0)).astype(f)
+    gy = np.where(vd, _shifted(x, 1) - x, f(0)).astype(f)
+    return float(np.sum(np.sqrt(gx * gx + gy * gy), dtype=np.float64))
+
+
 def spdhg_reference(op: OracleOperator, subsets, b, n_epochs, x0=None, weights=None, gain=None, background=None,
-                    support=None, eps_counts=1e-3, rho="auto", seed=0, lam=0.0, diagnostics_interval=1):
-    """SPDHGPoisson.run without TV for arrays on the device (spdhg_poisson.py:513-719, setup 558-662): returns
-    (x, y, z, [deviance per diagnostics epoch], rho). The float64 parts (dual prox, deviance, mean) are float64
-    here as in the reference; the operator is the oracle's."""
+                    support=None, eps_counts=1e-3, rho="auto", seed=0, lam=0.0, diagnostics_interval=1, tv=0.0,
+                    tv_prob=None):
+    """SPDHGPoisson.run for arrays on the device (spdhg_poisson.py:513-719, setup 558-662), with the dense
+    total-variation block when tv > 0 (spdhg_poisson.py:296-381, 430-484): returns (x, y, z, [deviance per
+    diagnostics epoch], rho). The float64 parts (dual prox, deviance, mean) are float64 here as in the reference; the
+    operator is the oracle's."""
     L = lib()
     R, My, CP = op.R, op.My, op.CP
     dshape = (R, My, CP)
@@ -224,7 +296,9 @@ def spdhg_reference(op: OracleOperator, subsets, b, n_epochs, x0=None, weights=N
     bg, pbg = periodic(background, n, dshape)
     M = len(subsets)
     subsets = [np.asarray(s, np.int64) for s in subsets]
-    p = 1.0 / M
+    p_tv = (1.0 / (M + 1) if tv_prob is None else float(tv_prob)) if tv > 0 else 0.0
+    n_tv = max(1, int(round(M * p_tv / (1 - p_tv)))) if tv > 0 else 0
+    p = (1.0 - p_tv) / M
     K, npix = op.K, op.Nx * op.Ny
     supp = np.ones(npix, bool) if support is None else np.asarray(support, bool).ravel()
     wv = np.ones(n, np.float32) if w is None else np.resize(w, n)
@@ -254,9 +328,13 @@ def spdhg_reference(op: OracleOperator, subsets, b, n_epochs, x0=None, weights=N
     rng = np.random.default_rng(seed)
     last = None
     devs = []
-    seq, last = epoch_order(rng, M, last)
-    D = op.forward(x, subset=subsets[seq[0]], data=D)
-    inv_p = np.float32(M)
+    seq, last = epoch_sequence(rng, M, last, n_tv)
+    if seq[0] >= 0:
+        D = op.forward(x, subset=subsets[seq[0]], data=D)
+    inv_p = np.float32(M) if tv <= 0 else np.float32(1.0 / p)
+    qx = np.zeros((K, op.Ny, op.Nx), np.float32)
+    qy = np.zeros_like(qx)
+    T3 = T.reshape(K, op.Ny, op.Nx)
     for e in range(n_epochs):
         final = e + 1 == n_epochs
         want = (e + 1) % max(1, diagnostics_interval) == 0 or final
@@ -266,22 +344,32 @@ def spdhg_reference(op: OracleOperator, subsets, b, n_epochs, x0=None, weights=N
             if not eoe:
                 nb = seq[j + 1]
             elif not final:
-                nseq, last = epoch_order(rng, M, last)
+                nseq, last = epoch_sequence(rng, M, last, n_tv)
                 nb = nseq[0]
             else:
                 nb = None
-            om = _c(subsets[m], np.int32)
-            L.orc_dual_update_sub(_p(y), _p(D), _p(sig), _p(b), _p(w), pw, _p(g), pg, _p(bg), pbg, eps_counts,
-                                  _p(om), row, len(om) * row)
-            dz = op.adjoint(D, subset=subsets[m]).reshape(K, npix)
-            L.orc_spdhg_update(_p(x), _p(z), _p(T), _p(_c(dz, np.float32)), float(inv_p), float(lam), x.size)
-            if (eoe and want) or nb is None or nb == m:
-                if (eoe and want) or nb is not None:
+            if m >= 0:
+                om = _c(subsets[m], np.int32)
+                L.orc_dual_update_sub(_p(y), _p(D), _p(sig), _p(b), _p(w), pw, _p(g), pg, _p(bg), pbg, eps_counts,
+                                      _p(om), row, len(om) * row)
+                dz = op.adjoint(D, subset=subsets[m]).reshape(K, npix)
+                ip = inv_p
+            else:                                   # the TV block
+                qx, qy, dqx, dqy = tv_dual(x.reshape(K, op.Ny, op.Nx), T3, qx, qy, tv, np.float32(0.99 * p_tv))
+                dz = tv_adjoint(dqx, dqy).reshape(K, npix)
+                ip = np.float32(1.0 / p_tv)
+            L.orc_spdhg_update(_p(x), _p(z), _p(T), _p(_c(dz, np.float32)), float(ip), float(lam), x.size)
+            m_next = nb if nb is not None and nb >= 0 else None
+            if (eoe and want) or nb is None or (m_next is not None and m_next == m):
+                if (eoe and want) or m_next is not None:
                     D = op.forward(x)
                     if eoe and want:
-                        devs.append(deviance(D, b, w, g, bg, eps_counts))
-            else:
-                D = op.forward(x, subset=subsets[nb], data=D)
+                        f = deviance(D, b, w, g, bg, eps_counts)
+                        if tv > 0:
+                            f += tv * tv_value(x.reshape(K, op.Ny, op.Nx), T3)
+                        devs.append(f)
+            elif m_next is not None:
+                D = op.forward(x, subset=subsets[m_next], data=D)
         if nseq is not None:
             seq = nseq
     return x.reshape(K, op.Ny, op.Nx), y, z.reshape(K, op.Ny, op.Nx), devs, rho
