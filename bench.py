@@ -222,6 +222,8 @@ def main():
                     "arrivals at 2/s, sizes of the serving configuration); its own JSON line")
     ap.add_argument("--projectors", action="store_true", help="only the projector comparison (native vs "
                     "Fourier-slice) at the large-slice geometry; its own JSON line")
+    ap.add_argument("--local", action="store_true", help="only the local-basis comparison (local vs dense operator "
+                    "over the same orientations) at the ti256 geometry; its own JSON line")
     ap.add_argument("--K", type=int, default=None, help="orientations (default: the workload's)")
     ap.add_argument("--precision", default="both", choices=["both", "bf16", "fp32"],
                     help="both: the BF16 tensor-core path (the value) and the float32 path (for the ratio)")
@@ -237,6 +239,10 @@ def main():
     if a.projectors:
         if rank == 0:
             print(json.dumps(projector_run(a.K or 256, a.steps, a.warmup)), flush=True)
+        return 0
+    if a.local:
+        if rank == 0:
+            print(json.dumps(local_run(a.K or 2000, a.steps, a.warmup)), flush=True)
         return 0
     if a.serve:
         if rank == 0:
@@ -601,6 +607,73 @@ def projector_run(K, steps, warmup):
             "config": {"workload": "large slice 512x512, 720 angles over 180 deg, 520 bins, 36 subsets",
                        "K_batch": K}, "steps": steps, "warmup": warmup, "data": "synthetic (random images)",
             "projectors": out}
+
+
+def local_run(K, steps, warmup, blob=12):
+    """The local basis against the dense operator over the same orientations, at the ti256 geometry (256 x 256
+    pixels, 360 angles, 263 bins, 360 eta bins, 8 Ti rings): K orientations, each allowed in a seeded disc of radius
+    blob pixels (inside the field of view). direct_cl / adjoint_cl of the full scan and of one of 20 subsets (CUDA
+    events, mean over `steps` after `warmup`), and one SPDHG epoch (20 subsets; wall clock of a run of 1 + steps / 2
+    epochs less that of a 1-epoch run)."""
+    import torch
+    from diffractom_b200 import SinglePhaseForwardOperator, SPDHGPoisson
+    from diffractom_b200.grid import MatrixGrid
+    from diffractom_b200.local import LocalSinglePhaseForwardOperator, LocalSupport
+    cfg, mat, grid, w = make_problem("ti256", K=K)
+    rng = np.random.default_rng(5)
+    Ny, Nx = cfg["Ny"], cfg["Nx"]
+    yy, xx = np.mgrid[:Ny, :Nx]
+    cy, cx = rng.uniform(blob, Ny - blob, K), rng.uniform(blob, Nx - blob, K)
+    mask = (yy[None] - cy[:, None, None]) ** 2 + (xx[None] - cx[:, None, None]) ** 2 <= blob ** 2
+    loc = LocalSinglePhaseForwardOperator(cfg, mat, grid, w["max_gb"], LocalSupport.from_mask(mask), normalized=True)
+    mats, sig = grid.leaf_arrays()
+    oi = loc.orientation_index
+    dense = SinglePhaseForwardOperator(cfg, mat, MatrixGrid(mats[oi], sig[oi]), w["max_gb"], normalized=True,
+                                       pf_mode=loc.pf_mode)
+    x = torch.as_tensor(rng.random(loc.n_coef).astype(np.float32) * loc.coefficient_mask(), device="cuda")
+    xd = torch.as_tensor(loc.to_dense(x.cpu().numpy())[oi], device="cuda")
+    out = {"fill": loc.n_coef / (loc.K * Nx * Ny), "n_coef": loc.n_coef, "patches": loc.n_patches,
+           "batches": len(loc.batches), "K_batch_max": loc.K_batch_max}
+    for op in (loc, dense):
+        op.set_omega_subsets(20)
+    data = torch.empty(loc.data_shape, device="cuda")
+
+    def timed(op, f):
+        st = op.stream()
+        for _ in range(max(1, warmup)):
+            f()
+        st.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            f()
+        e1.record(st)
+        e1.synchronize()
+        return round(e0.elapsed_time(e1) / steps, 3)
+
+    for name, op, c in (("local", loc, x), ("dense", dense, xd)):
+        g = torch.empty_like(c)
+        out[f"{name}_direct_ms"] = timed(op, lambda: op.direct_cl(c, data))
+        out[f"{name}_adjoint_ms"] = timed(op, lambda: op.adjoint_cl(data, g))
+        out[f"{name}_direct_subset_ms"] = timed(op, lambda: op.direct_cl(c, data, subset=3))
+        out[f"{name}_adjoint_subset_ms"] = timed(op, lambda: op.adjoint_cl(data, g, subset=3))
+    b = torch.poisson(torch.clamp(dense.direct(xd) * 20.0, min=0.0)).contiguous()
+    n_ep = max(1, steps // 2)
+
+    def run_time(op, c, epochs):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        SPDHGPoisson(op, subsets=20, seed=0).run(torch.zeros_like(c), b, epochs, diagnostics_interval=epochs)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    for name, op, c in (("local", loc, x), ("dense", dense, xd)):
+        run_time(op, c, 1)
+        # an epoch: the difference of two runs (set-up, final deviance and state download cancel)
+        out[f"{name}_spdhg_epoch_ms"] = round(1000 * (run_time(op, c, 1 + n_ep) - run_time(op, c, 1)) / n_ep, 2)
+    return {"metric": "local basis vs dense operator (ms per call)", "unit": "ms", "higher_is_better": False,
+            "config": {"workload": f"ti256 geometry, {K} orientations, each in a disc of radius {blob} px",
+                       "subsets": 20}, "steps": steps, "warmup": warmup, "data": "synthetic", "local": out}
 
 
 def serving_run(n, rate, px, omega, eta, rings, K, slots, budget_gb, max_epochs, seed, scenario):

@@ -74,8 +74,8 @@ SIGNATURES = {
     "dfx_fista_ls_update": ([P, P, P, P, L, I, I, F, F, F, I, P, S], c_int),
     "dfx_sum_partials": ([P, I, I, P, S], c_int),
     "dfx_score_z": ([P, P, P, L, S], c_int),
-    "dfx_local_scatter": ([P, P, P, P, P, I, I, I, I, P, S], c_int),
-    "dfx_local_gather": ([P, P, P, P, P, I, I, I, I, P, S], c_int),
+    "dfx_local_scatter": ([P, P, P, P, P, I, I, I, I, P, P, S], c_int),
+    "dfx_local_gather": ([P, P, P, P, P, I, I, I, I, P, P, S], c_int),
     "dfx_poisson_term": ([P, P, P, L, P, L, P, L, F, F, I, P, P, L, S], c_int),
     "dfx_tv_dual": ([P, P, P, P, P, P, I, I, I, F, F, S], c_int),
     "dfx_tv_adjoint_update": ([P, P, P, P, P, I, I, I, F, F, S], c_int),

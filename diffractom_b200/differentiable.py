@@ -180,10 +180,17 @@ class PFGradient:
             flags = (1 if "eta_offset" in groups else 0) | (2 if "axis_tilt" in groups else 0) | \
                 (4 if "two_theta" in groups else 0)
             R, My, nq, s = op.N_Omega, op.My, self.nq, op._s()
+            local = getattr(op, "coefficient_layout", "dense") == "local"
             for ib, b in enumerate(op.batches):
-                k0 = b["k_start"]
-                kb = _project_batch(op, c, ib)
-                op._radon_fwd(op._img_k.data_ptr(), op.coeffs_sino_C.data_ptr(), None, R, kb)
+                k0, kb = b["k_start"], b["K_batch"]
+                if local:
+                    if op.local_batches[ib] is None:       # no coefficients: zero gradients
+                        self.per_k[k0 * nq:(k0 + kb) * nq].zero_()
+                        continue
+                    op._project_local(c, ib)
+                else:
+                    _project_batch(op, c, ib)
+                    op._radon_fwd(op._img_k.data_ptr(), op.coeffs_sino_C.data_ptr(), None, R, kb)
                 rp, col, _, _ = op._pf_batch(ib, False)
                 op._call("dfx_pf_param_vjp", ctypes.byref(op._pfg), rp.data_ptr(), col.data_ptr(), r.data_ptr(),
                          None if cv is None else cv.data_ptr(), op.coeffs_sino_C.data_ptr(), My, op.Kstride, k0, kb,

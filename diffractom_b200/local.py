@@ -321,10 +321,19 @@ class LocalSinglePhaseForwardOperator(SinglePhaseForwardOperator):
         self._setup_local()
 
     def _setup_local(self):
+        """Per orientation batch: its patch table, and the compact image of the pixels where the batch has
+        coefficients (support pixels, ascending): the pixel -> row map, the pixel list for the backprojection and the
+        ray table restricted to those pixels with its pixel indices turned into rows. The projections of a batch then
+        cost its support, not the image."""
         P = self._patches
         bounds = np.searchsorted(P["pk"], [b["k_start"] for b in self.batches] + [self.K])
         dev = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a, dtype=dt), device=self.device)
+        _, iy, ix, pi = self._pairs()
+        pix_of_coef = np.full(self.n_coef, -1, np.int64)
+        pix_of_coef[pi] = iy * self.Nx + ix
+        npix = self.Nx * self.Ny
         self.local_batches = []
+        n_max = 0
         for ib, b in enumerate(self.batches):
             p0, p1 = int(bounds[ib]), int(bounds[ib + 1])
             if p1 == p0:
@@ -334,23 +343,52 @@ class LocalSinglePhaseForwardOperator(SinglePhaseForwardOperator):
             if chan.min() < 0 or chan.max() >= b["K_batch"]:
                 raise RuntimeError("a patch outside its batch")
             box = np.stack([P["y0"][p0:p1], P["x0"][p0:p1], P["h"][p0:p1], P["w"][p0:p1]], 1)
-            self.local_batches.append(dict(n=p1 - p0, box=dev(box, np.int32), coff=dev(P["coff"][p0:p1], np.int64),
-                                           chan=dev(chan, np.int32)))
+            c0, c1 = int(P["coff"][p0]), int(P["coff"][p1]) if p1 < len(P["coff"]) else self.n_coef
+            pix = np.unique(pix_of_coef[c0:c1])
+            pix = pix[pix >= 0]
+            row = np.full(npix, -1, np.int32)
+            row[pix] = np.arange(len(pix), dtype=np.int32)
+            lb = dict(n=p1 - p0, box=dev(box, np.int32), coff=dev(P["coff"][p0:p1], np.int64),
+                      chan=dev(chan, np.int32), n_pix=len(pix), plist=dev(pix, np.int32), pix_row=dev(row, np.int32))
+            if self.projector == "native":
+                supp = torch.zeros(npix, dtype=torch.uint8, device=self.device)
+                supp[lb["plist"].long()] = 1
+                rp, ent, taps = self._build_ray_table(supp)
+                e = ent[:2 * taps].view(-1, 2)
+                e[:, 0] = lb["pix_row"][e[:, 0].long()]
+                lb["ray"] = (rp, ent, taps)
+            n_max = max(n_max, len(pix))
+            self.local_batches.append(lb)
         self._mask = dev(P["mask"], np.uint8)
+        self._img_c = torch.empty(max(n_max, 1) * self.Kstride, dtype=torch.float32, device=self.device)
 
     @property
     def coeff_shape(self):
         return (self.n_coef,) if hasattr(self, "n_coef") and hasattr(self, "_mask") else super().coeff_shape
 
-    def _scatter(self, lb, coeffs, img):
+    def _scatter(self, lb, coeffs, img, compact=False):
+        """The batch's patches into a batch image (zero elsewhere: the caller clears it): the whole image, or the
+        compact image of the batch's support pixels."""
         self._call("dfx_local_scatter", coeffs.data_ptr(), self._mask.data_ptr(), lb["box"].data_ptr(),
                    lb["coff"].data_ptr(), lb["chan"].data_ptr(), lb["n"], self.Nx, self.Ny, self.Kstride,
-                   img.data_ptr(), self._s())
+                   lb["pix_row"].data_ptr() if compact else None, img.data_ptr(), self._s())
 
-    def _gather(self, lb, img, coeffs):
+    def _gather(self, lb, img, coeffs, compact=False):
         self._call("dfx_local_gather", img.data_ptr(), self._mask.data_ptr(), lb["box"].data_ptr(),
                    lb["coff"].data_ptr(), lb["chan"].data_ptr(), lb["n"], self.Nx, self.Ny, self.Kstride,
-                   coeffs.data_ptr(), self._s())
+                   lb["pix_row"].data_ptr() if compact else None, coeffs.data_ptr(), self._s())
+
+    def _project_local(self, coeffs, ib, subset=None):
+        """Radon of batch ib's patches into the batch sinogram (its support pixels only, through the batch's
+        compact image and restricted ray table); returns (om, n_ang, Kb, m) of the angles projected."""
+        lb = self.local_batches[ib]
+        Kb = self.batches[ib]["K_batch"]
+        img = self._img_c[:lb["n_pix"] * self.Kstride]
+        self._fill(img, 0.0)
+        self._scatter(lb, coeffs, img, compact=True)
+        geo, n_ang, om, m = self._geo_of(subset)
+        self._radon_fwd(img.data_ptr(), self.coeffs_sino_C.data_ptr(), om, n_ang, Kb, ray=lb["ray"], m=m)
+        return om, n_ang, Kb, m
 
     @on_op_stream
     def direct_cl(self, coeffs, data, subset=None):
@@ -364,9 +402,11 @@ class LocalSinglePhaseForwardOperator(SinglePhaseForwardOperator):
         for ib, lb in enumerate(self.local_batches):
             if lb is None:
                 continue
-            self._fill(self._img_k, 0.0)
-            self._scatter(lb, coeffs, self._img_k)
-            self._direct_batch_k(self._img_k.data_ptr(), ib, data, subset)
+            om, n_ang, Kb, m = self._project_local(coeffs, ib, subset)
+            rp, col, val, compact = self._pf_batch(ib, True, m)
+            self._call("dfx_spmm_pf_forward", self.coeffs_sino_C.data_ptr(), rp.data_ptr(), col.data_ptr(),
+                       val.data_ptr(), data.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My,
+                       self.N_seg, self.Kstride, Kb, compact, self._s())
 
     @on_op_stream
     def adjoint_cl(self, data, coeffs, subset=None):
@@ -376,8 +416,12 @@ class LocalSinglePhaseForwardOperator(SinglePhaseForwardOperator):
         for ib, lb in enumerate(self.local_batches):         # every patch is in one batch: all coefficients written
             if lb is None:
                 continue
-            self._adjoint_batch_k(data, ib, self._img_k.data_ptr(), subset)
-            self._gather(lb, self._img_k, coeffs)
+            geo, n_ang, Kb = self._pf_adjoint_to_sino(data, ib, subset)
+            img = self._img_c[:lb["n_pix"] * self.Kstride]
+            self._call("dfx_radon_backward_pixels", self.coeffs_sino_C.data_ptr(), img.data_ptr(), geo.data_ptr(),
+                       n_ang, self.Nx, self.Ny, self.My, self.Kstride, Kb, self._kernel_id,
+                       int(self.radon_geo.n_taps), lb["plist"].data_ptr(), lb["n_pix"], self._s())
+            self._gather(lb, img, coeffs, compact=True)
 
     @on_op_stream
     def direct(self, coeffs):
@@ -452,10 +496,12 @@ class LocalSinglePhaseForwardOperator(SinglePhaseForwardOperator):
         for lb in getattr(self, "local_batches", None) or []:
             if lb is not None:
                 n += sum(v.numel() * v.element_size() for v in lb.values() if isinstance(v, torch.Tensor))
-        m = getattr(self, "_mask", None)
-        return n + (0 if m is None else m.numel())
+                n += sum(t.numel() * t.element_size() for t in lb.get("ray", ())[:2])
+        for t in (getattr(self, "_mask", None), getattr(self, "_img_c", None)):
+            n += 0 if t is None else t.numel() * t.element_size()
+        return n
 
     def free_memory(self):
         self.local_batches = None
-        self._mask = None
+        self._mask = self._img_c = None
         super().free_memory()

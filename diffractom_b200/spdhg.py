@@ -285,7 +285,11 @@ class SPDHGPoisson:
         cshape, dshape = (n,), tuple(op.data_shape)
         x_on_gpu = is_device(x0)
         host_x = None if x_on_gpu else as_host(x0, cshape, "x0")
-        x = check_device(x0, cshape, "x0") if x_on_gpu else torch.as_tensor(host_x).to(dev)
+        if x_on_gpu:
+            x = check_device(x0, cshape, "x0")
+        else:
+            x = torch.empty(cshape, dtype=torch.float32, device=dev)
+            host_copier().to_device(host_x, x)
         gamma = self._setup_data(b, weights, gain, background)
         # S from the row sums A 1 (1 on the allowed coefficients); T from the subsets' column sums over the counted
         # points (spdhg_poisson.py:799-813)
@@ -350,20 +354,22 @@ class SPDHGPoisson:
             stop = False
             if callback is not None:
                 if not x_on_gpu:
-                    host_x[...] = x.cpu().numpy()
+                    host_copier().to_host(x, host_x)
                 stop = bool(callback(ep, x if x_on_gpu else host_x, stats))
             if verbose and want_f:
                 print(f"[spdhg epoch {ep:4d}] f={f:.8e} {time.perf_counter() - t_start:.1f} s", flush=True)
             if stop:
                 break
-        z_host, y_host = z.cpu().numpy(), self.y.cpu().numpy()
+        z_host, y_host = np.empty(cshape, np.float32), np.empty(dshape, np.float32)
+        host_copier().to_host(z, z_host)
+        host_copier().to_host(self.y, y_host)
         self.state = {"epoch": ep0 + len(self.iter_stats), "z": z_host, "y": y_host}
         self.final_stats = {"epochs": len(self.iter_stats), "final_f": f, "setup_s": t_setup, "rho": self.rho_used,
                             "subsets": self.M, "resident": self.resident_used,
                             "time": time.perf_counter() - t_start, "tv": 0.0, "tv_prob": 0.0, "graph_replays": 0,
                             **self.scales}
         if not x_on_gpu:
-            host_x[...] = x.cpu().numpy()
+            host_copier().to_host(x, host_x)
         self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = None
         return x if x_on_gpu else host_x
 

@@ -375,11 +375,14 @@ int dfx_score_z(const float *E, const float *D, float *Z, int64_t n, void *strea
  * int32 (its orientation's channel in the batch, < kstride), mask (uint8 per coefficient: 1 where the voxel is
  * allowed). scatter: img_k (Nx*Ny, kstride) channel-fastest, at the patches' voxels = coeffs where allowed, 0 at
  * their other voxels (the caller zeroes the rest of the batch image first); gather: coeffs of the patches = img_k at
- * the allowed voxels, 0 at the others. */
+ * the allowed voxels, 0 at the others. pix_row (NULL: whole images): the row of every pixel (nx * ny int32) in a
+ * compact batch image of the batch's support pixels, -1 for the others (cells there are skipped / read as 0). */
 int dfx_local_scatter(const float *coeffs, const uint8_t *mask, const int32_t *box, const int64_t *coff,
-                      const int32_t *chan, int n_patches, int nx, int ny, int kstride, float *img_k, void *stream);
+                      const int32_t *chan, int n_patches, int nx, int ny, int kstride, const int32_t *pix_row,
+                      float *img_k, void *stream);
 int dfx_local_gather(const float *img_k, const uint8_t *mask, const int32_t *box, const int64_t *coff,
-                     const int32_t *chan, int n_patches, int nx, int ny, int kstride, float *coeffs, void *stream);
+                     const int32_t *chan, int n_patches, int nx, int ny, int kstride, const int32_t *pix_row,
+                     float *coeffs, void *stream);
 
 /* replaces tv_dual_dense / tv_adjoint_dense + spdhg_update / tv_value_dense (optimization/spdhg_poisson.py:110-186)
  * on one channel-fastest batch (nx * ny pixels x kstride channels; T = 0 on padding channels): SPDHG's total-variation
