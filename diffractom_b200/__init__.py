@@ -11,7 +11,8 @@ from .material import Material, group_reflections_into_rings
 from .quadrature import QuadratureRule
 
 __all__ = ["Grid", "MatrixGrid", "Material", "QuadratureRule", "group_reflections_into_rings",
-           "SinglePhaseForwardOperator", "SPDHGPoisson", "FISTAPoisson", "FISTAHuber", "FISTAL2", "estimate_L_power",
+           "SinglePhaseForwardOperator", "SPDHGPoisson", "FISTAPoisson", "FISTAHuber", "FISTAL2", "OSEMPoisson",
+           "PDHGPoisson", "estimate_L_power",
            "forward_operator"]
 
 
@@ -26,6 +27,9 @@ def __getattr__(name):
     if name == "FISTAPoisson":
         from .fista import FISTAPoisson
         return FISTAPoisson
+    if name in ("OSEMPoisson", "PDHGPoisson"):
+        from . import osem_pdhg
+        return getattr(osem_pdhg, name)
     if name in ("FISTAHuber", "FISTAL2"):
         from . import fista_ls
         return getattr(fista_ls, name)

@@ -77,6 +77,11 @@ SIGNATURES = {
     "dfx_local_scatter": ([P, P, P, P, P, I, I, I, I, P, P, S], c_int),
     "dfx_local_gather": ([P, P, P, P, P, I, I, I, I, P, P, S], c_int),
     "dfx_poisson_term": ([P, P, P, L, P, L, P, L, F, F, I, P, P, L, S], c_int),
+    "dfx_osem_update": ([P, P, P, P, L, F, L, S], c_int),
+    "dfx_pdhg_dual_update": ([P, P, P, P, P, L, P, L, P, L, F, L, S], c_int),
+    "dfx_pdhg_primal_update": ([P, P, P, P, F, L, S], c_int),
+    "dfx_pdhg_average": ([P, P, L, S], c_int),
+    "dfx_pdhg_primal_steps": ([P, P, P, L, F, L, S], c_int),
     "dfx_tv_dual": ([P, P, P, P, P, P, I, I, I, F, F, S], c_int),
     "dfx_tv_adjoint_update": ([P, P, P, P, P, I, I, I, F, F, S], c_int),
     "dfx_tv_value": ([P, P, I, I, I, P, P, c_size_t, S], c_int),

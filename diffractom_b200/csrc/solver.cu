@@ -220,6 +220,74 @@ __global__ void __launch_bounds__(RED_THREADS) tv_value_kernel(const float *__re
     block_sum<1>(v, part + blockIdx.x);
 }
 
+// ---- OSEM's multiplicative update (optimization/osem_poisson.py:80-84): x = outside ? 0 : (s > 0 ? x back / (s + lam)
+// : x), the support mask periodic with period pm (0: none)
+__global__ void osem_update_kernel(float *__restrict__ x, const float *__restrict__ back,
+                                   const float *__restrict__ sens, const uint8_t *__restrict__ mask, int64_t pm,
+                                   float lam, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const bool ok = pm ? mask[i % pm] != 0 : true;
+        const float sv = sens[i];
+        x[i] = !ok ? 0.0f : (sv > 0.0f ? __fdiv_rn(__fmul_rn(x[i], back[i]), __fadd_rn(sv, lam)) : x[i]);
+    }
+}
+
+// ---- PDHG (optimization/pdhg_poisson.py:33-94). Dual: y <- prox_{sig F*}(y + sig Axb), F_i(z) = s (z + r - b log(z +
+// r)), s = w / g, r = bg + eps g: y = (v + s - sqrt((v - s)^2 + 4 sig s b)) / 2, v = y + sig Axb + sig r (float64);
+// 0 where w = 0 or sig = 0
+__global__ void pdhg_dual_kernel(float *__restrict__ y, const float *__restrict__ Axb, const float *__restrict__ sig,
+                                 const float *__restrict__ b, const float *__restrict__ w, int64_t pw,
+                                 const float *__restrict__ g, int64_t pg, const float *__restrict__ bg, int64_t pbg,
+                                 float eps, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float wi = periodic(w, pw, i, 1.0f);
+        const float si = sig[i];
+        if (wi == 0.0f || si == 0.0f) {
+            y[i] = 0.0f;
+            continue;
+        }
+        const float gi = periodic(g, pg, i, 1.0f);
+        const double sd = (double)wi / (double)gi;
+        const double r = (double)periodic(bg, pbg, i, 0.0f) + (double)eps * gi;
+        const double v = (double)y[i] + (double)si * Axb[i] + (double)si * r;
+        const double d = v - sd;
+        y[i] = (float)(0.5 * (v + sd - sqrt(d * d + 4.0 * (double)si * sd * (double)b[i])));
+    }
+}
+
+// primal: x_new = T > 0 ? max(0, x - T (grad + lam)) : 0; xb = 2 x_new - x; x = x_new
+__global__ void pdhg_primal_kernel(float *__restrict__ x, float *__restrict__ xb, const float *__restrict__ grad,
+                                   const float *__restrict__ T, float lam, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float t = T[i];
+        const float xo = x[i];
+        const float xn = t > 0.0f ? fmaxf(0.0f, __fsub_rn(xo, __fmul_rn(t, __fadd_rn(grad[i], lam)))) : 0.0f;
+        xb[i] = __fsub_rn(__fmul_rn(2.0f, xn), xo);
+        x[i] = xn;
+    }
+}
+
+// Ax <- (Axb + Ax) / 2 (A x_k from A x_bar_k = 2 A x_k - A x_(k-1))
+__global__ void pdhg_average_kernel(float *__restrict__ Ax, const float *__restrict__ Axb, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        Ax[i] = __fmul_rn(0.5f, __fadd_rn(Axb[i], Ax[i]));
+}
+
+// T = tau0 / colsum on the support (mask periodic with period npix, 0: none) where colsum > 0, else 0
+__global__ void pdhg_primal_steps_kernel(float *__restrict__ T, const float *__restrict__ colsum,
+                                         const uint8_t *__restrict__ supp, int64_t npix, float tau0, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const bool inside = npix ? supp[i % npix] != 0 : true;
+        const float c = colsum[i];
+        T[i] = (inside && c > 0.0f) ? __fdiv_rn(tau0, c) : 0.0f;
+    }
+}
+
 // ---- the Poisson data term of a prediction (optimization/poisson_term.py:36-58), mu = max(pred, 0) + bg + eps g, on
 // the points of weight != 0 (0 elsewhere; the fitted angles are the caller's weights):
 //   mode 0: r = w/g (1 - b/mu), c = w / (g max(mu, floor g))     (gradient and Fisher curvature; c may be NULL)
@@ -579,6 +647,47 @@ extern "C" int dfx_tv_value(const float *x, const float *T, int nx, int ny, int 
     if (st) return st;
     finish_sums<1><<<1, RED_THREADS, 0, s>>>((const double *)scratch, nb, out);
     return launch_status("finish_sums");
+}
+
+extern "C" int dfx_osem_update(float *x, const float *back, const float *sens, const uint8_t *mask, int64_t pm,
+                               float lam, int64_t n, void *stream)
+{
+    DFX_REQUIRE(x && back && sens && n >= 0 && (!pm || mask), "osem_update: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(osem_update_kernel, n, stream, x, back, sens, mask, pm, lam, n);
+}
+
+extern "C" int dfx_pdhg_dual_update(float *y, const float *Axb, const float *sig, const float *b, const float *w,
+                                    int64_t pw, const float *g, int64_t pg, const float *bg, int64_t pbg, float eps,
+                                    int64_t n, void *stream)
+{
+    DFX_REQUIRE(y && Axb && sig && b && n >= 0 && (!pw || w) && (!pg || g) && (!pbg || bg),
+                "pdhg_dual_update: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(pdhg_dual_kernel, n, stream, y, Axb, sig, b, w, pw, g, pg, bg, pbg, eps, n);
+}
+
+extern "C" int dfx_pdhg_primal_update(float *x, float *xb, const float *grad, const float *T, float lam, int64_t n,
+                                      void *stream)
+{
+    DFX_REQUIRE(x && xb && grad && T && n >= 0, "pdhg_primal_update: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(pdhg_primal_kernel, n, stream, x, xb, grad, T, lam, n);
+}
+
+extern "C" int dfx_pdhg_average(float *Ax, const float *Axb, int64_t n, void *stream)
+{
+    DFX_REQUIRE(Ax && Axb && n >= 0, "pdhg_average: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(pdhg_average_kernel, n, stream, Ax, Axb, n);
+}
+
+extern "C" int dfx_pdhg_primal_steps(float *T, const float *colsum, const uint8_t *supp, int64_t npix, float tau0,
+                                     int64_t n, void *stream)
+{
+    DFX_REQUIRE(T && colsum && n >= 0 && (!npix || supp), "pdhg_primal_steps: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(pdhg_primal_steps_kernel, n, stream, T, colsum, supp, npix, tau0, n);
 }
 
 extern "C" int dfx_poisson_term(const float *pred, const float *b, const float *w, int64_t pw, const float *g, int64_t pg,

@@ -397,6 +397,22 @@ int dfx_tv_adjoint_update(const float *dqx, const float *dqy, float *x, float *z
 int dfx_tv_value(const float *x, const float *T, int nx, int ny, int kstride, double *out, void *scratch,
                  size_t scratch_bytes, void *stream);
 
+/* replaces osem_update (optimization/osem_poisson.py:80-84): x = outside the support (mask periodic with period pm,
+ * 0: no mask) ? 0 : (sens > 0 ? x back / (sens + lam) : x). */
+int dfx_osem_update(float *x, const float *back, const float *sens, const uint8_t *mask, int64_t pm, float lam,
+                    int64_t n, void *stream);
+
+/* replaces PDHGPoisson's dual_update, primal_update, average, primal_steps (optimization/pdhg_poisson.py:33-94):
+ * y <- prox_{sig F*}(y + sig Axb) in float64 (0 where w = 0 or sig = 0); x_new = T > 0 ? max(0, x - T (grad + lam)) :
+ * 0, xb = 2 x_new - x, x = x_new; Ax = (Axb + Ax) / 2; T = tau0 / colsum inside the support (period npix) where
+ * colsum > 0, else 0. */
+int dfx_pdhg_dual_update(float *y, const float *Axb, const float *sig, const float *b, const float *w, int64_t pw,
+                         const float *g, int64_t pg, const float *bg, int64_t pbg, float eps, int64_t n, void *stream);
+int dfx_pdhg_primal_update(float *x, float *xb, const float *grad, const float *T, float lam, int64_t n, void *stream);
+int dfx_pdhg_average(float *Ax, const float *Axb, int64_t n, void *stream);
+int dfx_pdhg_primal_steps(float *T, const float *colsum, const uint8_t *supp, int64_t npix, float tau0, int64_t n,
+                          void *stream);
+
 /* replaces PoissonTerm's pt_grad_curv / pt_ratio / pt_wg (optimization/poisson_term.py:52-58), mu = max(pred, 0) +
  * bg + eps g, on points of weight != 0 (0 elsewhere): mode 0 r = w/g (1 - b/mu), c = w / (g max(mu, floor g)) (c may
  * be NULL); mode 1 r = w b / (g mu); mode 2 r = w / g (pred unused). */

@@ -415,3 +415,112 @@ def fista_ls_reference(op: OracleOperator, b, niter, tau, x0=None, prox="nonneg"
         x = v
         t = t_new
     return x.reshape(K, op.Ny, op.Nx), fs, gs
+
+
+def _data_terms(b, weights, gain, background, dshape, fit=None):
+    """Data-shaped float32 (w with unfitted rows 0, g, bg) as the solvers' periodic arrays expand them."""
+    n = int(np.prod(dshape))
+    w = np.ones(n, np.float32) if weights is None else np.resize(np.asarray(weights, np.float32).ravel(), n)
+    g = np.ones(n, np.float32) if gain is None else np.resize(np.asarray(gain, np.float32).ravel(), n)
+    bg = np.zeros(n, np.float32) if background is None else np.resize(np.asarray(background, np.float32).ravel(), n)
+    w, g, bg = (a.reshape(dshape).copy() for a in (w, g, bg))
+    if fit is not None:
+        w[~np.asarray(fit, bool)] = 0.0
+    return w, g, bg
+
+
+def osem_reference(op: OracleOperator, subsets, b, n_epochs, x0, weights=None, gain=None, background=None,
+                   support=None, eps_counts=1e-3, seed=0, lam=0.0, start_floor=0.01):
+    """OSEMPoisson.run (optimization/osem_poisson.py:95-185) on the oracle operator, float32 arithmetic in the
+    reference's order: returns (x, final deviance)."""
+    dshape = (op.R, op.My, op.CP)
+    K, npix = op.K, op.Nx * op.Ny
+    f = np.float32
+    b = _c(b, f).reshape(dshape)
+    M = 1 if subsets is None else len(subsets)
+    fit = None
+    if subsets is not None:
+        fit = np.zeros(op.R, bool)
+        for s_ in subsets:
+            fit[np.asarray(s_, np.int64)] = True
+    w, g, bg = _data_terms(b, weights, gain, background, dshape, fit)
+    eps = f(eps_counts)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        wg = np.where(w != 0, w / g, f(0)).astype(f)
+    sub = (lambda m: None) if subsets is None else (lambda m: subsets[m])
+    sens = [op.adjoint(wg, subset=sub(m)).reshape(K, npix).astype(f) for m in range(M)]
+    allowed = np.ones((K, npix), bool) if support is None else np.broadcast_to(np.asarray(support, bool).ravel(),
+                                                                               (K, npix))
+    x = np.where(allowed, _c(x0, f).reshape(K, npix), f(0)).astype(f)
+    if start_floor:
+        pos = x[x > 0]
+        if pos.size:
+            floor = float(start_floor) * float(np.median(pos.astype(np.float64)))
+        else:
+            st = sum(float(sm[allowed].sum(dtype=np.float64)) for sm in sens)
+            tot = float(np.sum(wg.astype(np.float64) * b)) - float(np.sum(wg.astype(np.float64) * bg))
+            floor = max(tot, 0.0) / st if st > 0 else 1.0
+        x = np.where(allowed, np.maximum(x.astype(np.float64), floor), 0.0).astype(f)
+    rng = np.random.default_rng(seed)
+    for _ in range(int(n_epochs)):
+        order = rng.permutation(M) if M > 1 else [0]
+        for m in order:
+            m = int(m)
+            pred = op.forward(x.reshape(K, op.Ny, op.Nx), subset=sub(m)).astype(f)
+            mu = (np.maximum(pred, f(0)) + bg) + eps * g
+            with np.errstate(divide="ignore", invalid="ignore"):
+                r = np.where(w != 0, (w / g) * (b / mu), f(0)).astype(f)
+            back = op.adjoint(r, subset=sub(m)).reshape(K, npix).astype(f)
+            s = sens[m]
+            with np.errstate(divide="ignore", invalid="ignore"):
+                upd = np.where(s > 0, (x * back) / (s + f(lam)), x).astype(f)
+            x = np.where(allowed, upd, f(0)).astype(f)
+    pred = op.forward(x.reshape(K, op.Ny, op.Nx))
+    return x.reshape(K, op.Ny, op.Nx), deviance(pred, b, w, g, bg, eps_counts)
+
+
+def pdhg_reference(op: OracleOperator, b, niter, x0=None, weights=None, gain=None, background=None, support=None,
+                   eps_counts=1e-3, rho="auto", lam=0.0):
+    """PDHGPoisson.run for device arrays (optimization/pdhg_poisson.py:159-262) on the oracle operator: float32 state,
+    the dual prox in float64; returns (x, [deviance per iteration], rho)."""
+    dshape = (op.R, op.My, op.CP)
+    K, npix = op.K, op.Nx * op.Ny
+    f = np.float32
+    b = _c(b, f).reshape(dshape)
+    w, g, bg = _data_terms(b, weights, gain, background, dshape)
+    counted = w != 0
+    if rho == "auto":
+        mean_b = float(np.sum(b[counted], dtype=np.float64)) / max(float(np.count_nonzero(counted)), 1.0)
+        rho = 3e4 / mean_b ** 2 if mean_b > 0 else 1.0
+    tau0, sigma0 = f(1.0 / np.sqrt(rho)), f(np.sqrt(rho))
+    supp = np.ones(npix, bool) if support is None else np.asarray(support, bool).ravel()
+    ones = np.broadcast_to(supp.astype(f), (K, npix)).reshape(K, op.Ny, op.Nx)
+    rowsum = op.forward(ones).astype(f)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        sig = np.where(counted & (rowsum > 0), sigma0 / rowsum, f(0)).astype(f)
+        colsum = op.adjoint(counted.astype(f)).reshape(K, npix).astype(f)
+        T = np.where(supp[None, :] & (colsum > 0), tau0 / colsum, f(0)).astype(f)
+    x = np.maximum(_c(x0 if x0 is not None else np.zeros((K, npix), f), f).reshape(K, npix), f(0))
+    x[:, ~supp] = 0.0
+    xb = x.copy()
+    y = np.zeros(dshape, f)
+    Ax = op.forward(x.reshape(K, op.Ny, op.Nx)).astype(f)
+    Axb = Ax.copy()
+    s64 = np.where(counted, w.astype(np.float64) / g, 0.0)
+    r64 = bg.astype(np.float64) + np.float64(f(eps_counts)) * g
+    devs = []
+    for it in range(1, int(niter) + 1):
+        v = y.astype(np.float64) + sig.astype(np.float64) * Axb + sig.astype(np.float64) * r64
+        d = v - s64
+        yn = 0.5 * (v + s64 - np.sqrt(d * d + 4.0 * sig.astype(np.float64) * s64 * b))
+        y = np.where(counted & (sig != 0), yn, 0.0).astype(f)
+        grad = op.adjoint(y).reshape(K, npix).astype(f)
+        xn = np.where(T > 0, np.maximum(f(0), x - T * (grad + f(lam))), f(0)).astype(f)
+        xb = (f(2) * xn - x).astype(f)
+        x = xn
+        Axb = op.forward(xb.reshape(K, op.Ny, op.Nx)).astype(f)
+        Ax = (f(0.5) * (Axb + Ax)).astype(f)
+        if it % 50 == 0:
+            Ax = op.forward(x.reshape(K, op.Ny, op.Nx)).astype(f)
+        devs.append(deviance(Ax, b, w, g, bg, eps_counts))
+    return x.reshape(K, op.Ny, op.Nx), devs, rho
