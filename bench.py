@@ -222,6 +222,8 @@ def main():
                     "arrivals at 2/s, sizes of the serving configuration); its own JSON line")
     ap.add_argument("--projectors", action="store_true", help="only the projector comparison (native vs "
                     "Fourier-slice) at the large-slice geometry; its own JSON line")
+    ap.add_argument("--extras", action="store_true", help="only the solvers and tools around the operator (FISTA, "
+                    "OSEM, PDHG, parameter gradients, orientation search) at the ti256 geometry; its own JSON line")
     ap.add_argument("--local", action="store_true", help="only the local-basis comparison (local vs dense operator "
                     "over the same orientations) at the ti256 geometry; its own JSON line")
     ap.add_argument("--K", type=int, default=None, help="orientations (default: the workload's)")
@@ -239,6 +241,10 @@ def main():
     if a.projectors:
         if rank == 0:
             print(json.dumps(projector_run(a.K or 256, a.steps, a.warmup)), flush=True)
+        return 0
+    if a.extras:
+        if rank == 0:
+            print(json.dumps(extras_run(a.K or 2000, a.steps, a.warmup)), flush=True)
         return 0
     if a.local:
         if rank == 0:
@@ -562,6 +568,84 @@ LARGE_SLICE = dict(cfg=dict(Nx=512, Ny=512, My=520, N_Omega=720, angle_range=[0,
                    material=dict(a=3.52, symmetry_group="cubic", wavelength_A=0.3,
                                  hkl_list=[[1, 1, 1], [2, 0, 0], [2, 2, 0], [3, 1, 1], [2, 2, 2], [4, 0, 0]]),
                    sigma_deg=1.0, subsets=36)
+
+
+def extras_run(K, steps, warmup):
+    """The solvers and tools around the operator at the ti256 geometry with K orientations (FP32, state on the
+    device): a FISTAL2 and a FISTAHuber iteration, an OSEM epoch (20 subsets), a PDHG iteration (each the difference
+    of a longer and a 1-iteration run), PFGradient (all parameter groups; with the Gauss-Newton blocks), ProjGradient
+    (the mean of `steps` synchronised calls after `warmup`), and the orientation search (score_candidates of 4 K
+    candidates, 2 input pairs x 2 angle-row sets, every 4th field-of-view pixel; one call). Wall clock."""
+    import torch
+    from diffractom_b200 import (FISTAHuber, FISTAL2, Grid, OSEMPoisson, PDHGPoisson, SinglePhaseForwardOperator,
+                                 estimate_L_power)
+    from diffractom_b200.differentiable import PFGradient, ProjGradient
+    from diffractom_b200.grid import MatrixGrid
+    from diffractom_b200.orientation_search import poisson_score_inputs, score_candidates
+    cfg, mat, grid, w = make_problem("ti256", K=K)
+    op = SinglePhaseForwardOperator(cfg, mat, grid, w["max_gb"], normalized=True)
+    x_true = phantom(op, dict(w, grains=min(w["grains"], op.K)), seed=1)
+    b = counts(op, x_true, w["mean_counts"])
+    del x_true
+    out = {}
+
+    def timed(f, n=steps, w_=warmup):
+        for _ in range(w_):
+            f()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            f()
+        torch.cuda.synchronize()
+        return round(1000 * (time.perf_counter() - t0) / n, 2)
+
+    x = torch.zeros(op.coeff_shape, device="cuda")
+    L = estimate_L_power(op, niter=5, verbose=0)
+
+    def per_iteration(run, n):
+        """(wall clock of run(1 + n) - that of run(1)) / n: the set-up and the closing work cancel."""
+        run(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run(1)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        run(1 + n)
+        torch.cuda.synchronize()
+        return round(1000 * ((time.perf_counter() - t1) - (t1 - t0)) / n, 2)
+
+    for name, cls in (("fista_l2", FISTAL2), ("fista_huber", FISTAHuber)):
+        out[f"{name}_iteration_ms"] = per_iteration(lambda it, cls=cls: cls(op, L=L).run(x, b, it), steps)
+    out["osem_epoch_ms"] = per_iteration(lambda it: OSEMPoisson(op, subsets=20, seed=0).run(
+        torch.full(op.coeff_shape, 0.01, device="cuda"), b, it, diagnostics_interval=0), max(1, steps // 2))
+    out["pdhg_iteration_ms"] = per_iteration(lambda it: PDHGPoisson(op).run(x, b, it), steps)
+    xs = torch.rand(op.coeff_shape, device="cuda")
+    r = torch.randn(op.data_shape, device="cuda")
+    pg, ph, pj = PFGradient(op), PFGradient(op, hessian=True), ProjGradient(op)
+    out["pf_gradient_ms"] = timed(lambda: pg(xs, r))
+    out["pf_gradient_hessian_ms"] = timed(lambda: ph(xs, r, groups=("rot", "sigma"), curv=torch.ones_like(r)))
+    out["proj_gradient_ms"] = timed(lambda: pj(xs, r))
+    mu = torch.clamp(op.direct(xs), min=0.1)
+    e, dd = poisson_score_inputs(b.cpu().numpy(), mu.cpu().numpy(), 1.0, np.ones(op.N_seg, np.float32))
+    inputs = [(torch.as_tensor(e, device="cuda"), torch.as_tensor(dd, device="cuda"))] * 2
+    held = np.zeros(op.N_Omega, bool)
+    held[::10] = True
+    pixels = np.flatnonzero(op.support_mask().ravel())[::4]
+    cand = Grid.from_random_fundamental_zone(4 * K, mat.crystal_system, np.deg2rad(w["sigma_deg"]), seed=9)
+    rots, sig = cand.leaf_arrays()
+    make = lambda rr: SinglePhaseForwardOperator(cfg, mat, MatrixGrid(rr, sig[:len(rr)]), w["max_gb"],
+                                                 normalized=True, pf_mode="generated")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    score_candidates(make, rots, inputs, [~held, held], pixels, top_k=16, chunk=K)
+    torch.cuda.synchronize()
+    out["search_s"] = round(time.perf_counter() - t0, 2)
+    out["search_candidates_per_s"] = round(4 * K / out["search_s"], 1)
+    return {"metric": "solvers and tools around the operator (ms per call)", "unit": "ms", "higher_is_better": False,
+            "config": {"workload": f"ti256 geometry, {K} orientations, FP32, state on the device",
+                       "search": f"{4 * K} candidates in chunks of {K}, 2 input pairs x 2 angle-row sets, "
+                                 f"{len(pixels)} pixels, top 16"},
+            "steps": steps, "warmup": warmup, "data": "synthetic (seeded phantom, Poisson counts)", "extras": out}
 
 
 def projector_run(K, steps, warmup):

@@ -107,30 +107,35 @@ class OSEMPoisson:
         if self.store_sensitivities:
             for m in range(self.M):
                 self._adj(wg, sens[m], m)
-        # start (osem_poisson.py:139-160)
+        # start (osem_poisson.py:139-160), on the device: the median of the positive allowed coefficients as NumPy's
+        # (the mean of the two middle values for an even count, in float64)
         n = int(np.prod(cshape))
-        xh = x.reshape(-1).cpu().numpy().astype(np.float64)
-        allowed = np.resize(self.mask.cpu().numpy().astype(bool), n) if self.pmask else np.ones(n, bool)
-        xh = np.where(allowed, xh, 0.0)
+        xf = x.reshape(-1)
+        allowed = (self.mask.reshape(-1).bool().repeat(n // self.pmask) if self.pmask
+                   else torch.ones(n, dtype=torch.bool, device=op.device))
+        xf.masked_fill_(~allowed, 0.0)
         if start_floor:
-            pos = xh[xh > 0]
-            if pos.size:
-                floor = float(start_floor) * float(np.median(pos))
+            pos = xf[xf > 0]
+            if pos.numel():
+                k = pos.numel()
+                lo = float(torch.kthvalue(pos, (k + 1) // 2).values.item())
+                hi = float(torch.kthvalue(pos, k // 2 + 1).values.item()) if k % 2 == 0 else lo
+                floor = float(start_floor) * (0.5 * (lo + hi) if k % 2 == 0 else lo)
             else:
                 st = 0.0
                 for m in range(self.M):
                     if not self.store_sensitivities:
                         self._adj(wg, sens[0], m)
                     sm = sens[m if self.store_sensitivities else 0]
-                    st += float(sm.reshape(-1).cpu().numpy()[allowed].sum(dtype=np.float64))
+                    st += float(sm.reshape(-1)[allowed].double().sum().item())
                 tot = float(torch.dot(wg.reshape(-1).double(), pt.b.reshape(-1).double()).item())
                 if pt.pbg:
-                    tot -= float((wg.reshape(-1).double().cpu().numpy()
-                                  * np.resize(pt.bg.cpu().numpy(), int(np.prod(dshape)))).sum())
+                    bgf = pt.bg.double().repeat(int(np.prod(dshape)) // pt.pbg)
+                    tot -= float(torch.dot(wg.reshape(-1).double(), bgf).item())
                 floor = max(tot, 0.0) / st if st > 0 else 1.0
-            xh = np.where(allowed, np.maximum(xh, floor), 0.0)
+            xf.copy_(torch.where(allowed, xf.double().clamp(min=floor), torch.zeros((), dtype=torch.float64,
+                                                                                      device=op.device)).float())
             self.start_floor_used = floor
-        x.copy_(torch.as_tensor(xh.astype(np.float32).reshape(cshape)))
         mp = None if self.mask is None else self.mask.data_ptr()
         self.iter_stats = []
         f = None
