@@ -12,13 +12,13 @@ from .quadrature import QuadratureRule
 
 __all__ = ["Grid", "MatrixGrid", "Material", "QuadratureRule", "group_reflections_into_rings",
            "SinglePhaseForwardOperator", "SPDHGPoisson", "FISTAPoisson", "FISTAHuber", "FISTAL2", "OSEMPoisson",
-           "PDHGPoisson", "estimate_L_power",
+           "PDHGPoisson", "estimate_L_power", "estimate_L_power_streamed",
            "forward_operator"]
 
 
 def __getattr__(name):
     # the device classes import torch and the CUDA library only when used
-    if name in ("SinglePhaseForwardOperator", "estimate_L_power"):
+    if name in ("SinglePhaseForwardOperator", "estimate_L_power", "estimate_L_power_streamed"):
         from . import operator
         return getattr(operator, name)
     if name == "SPDHGPoisson":

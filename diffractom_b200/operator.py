@@ -974,3 +974,50 @@ def _estimate_L_power(op, niter, seed, eps, verbose):
         if verbose:
             print(f"[power {it + 1:02d}] L_est={L_est:.6e}  ||z||={zn:.6e}")
     return float(L_est)
+
+
+def _host_dot(a, b, pool, chunk=1 << 24):
+    """float64 dot product of two float32 host vectors, chunk by chunk, the chunks' sums added in order."""
+    parts = [(i, min(i + chunk, a.size)) for i in range(0, a.size, chunk)]
+    return float(sum(pool.map(lambda c: float(np.dot(a[c[0]:c[1]].astype(np.float64), b[c[0]:c[1]])), parts)))
+
+
+def parallel_random_start(K, Ny, Nx, seed, threads=16):
+    """The parallel random start of estimate_L_power_streamed (streaming.py:363-372): x3 (K, Ny, Nx) float32 with column
+    ix (x3[:, :, ix]) the transposed (Ny, K) standard-normal draw of default_rng([seed, ix])."""
+    from concurrent.futures import ThreadPoolExecutor
+    x3 = np.empty((K, Ny, Nx), np.float32)
+
+    def col(ix):
+        x3[:, :, ix] = np.random.default_rng([seed, ix]).standard_normal((Ny, K)).astype(np.float32).T
+
+    with ThreadPoolExecutor(threads) as p:
+        list(p.map(col, range(Nx)))
+    return x3
+
+
+def estimate_L_power_streamed(op, niter: int = 20, seed: int = 0, eps: float = 1e-30, verbose: int = 1,
+                              parallel_start: bool = True) -> float:
+    """estimate_L_power with the two coefficient-sized vectors in host memory (streaming.py:398-432): the forward and
+    adjoint stream them through the device batch by batch (the operator's NumPy path), the dot products are float64
+    on the host. parallel_start (default): a column of the start from its own random stream (parallel_random_start),
+    fast, but not the numbers of estimate_L_power; False: the start of estimate_L_power, and its estimate (computed on
+    the device). Local-basis operators: estimate_L_power."""
+    if getattr(op, "coefficient_layout", "dense") != "dense" or not parallel_start:
+        return estimate_L_power(op, niter=niter, seed=seed, eps=eps, verbose=verbose)
+    if niter < 1:
+        raise ValueError("niter must be >= 1")
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(16) as pool:
+        x = parallel_random_start(op.K, op.Ny, op.Nx, seed).reshape(-1)
+        x *= np.float32(1.0 / (np.sqrt(_host_dot(x, x, pool)) + eps))
+        L_est = 0.0
+        for it in range(niter):
+            z = np.ascontiguousarray(op.adjoint(op.direct(x.reshape(op.coeff_shape))), np.float32).reshape(-1)
+            L_est = _host_dot(x, z, pool) / (_host_dot(x, x, pool) + eps)
+            zn = float(np.sqrt(_host_dot(z, z, pool))) + eps
+            z *= np.float32(1.0 / zn)
+            x = z
+            if verbose:
+                print(f"[power {it + 1:02d}] L_est={L_est:.6e}  ||z||={zn:.6e}")
+    return float(L_est)

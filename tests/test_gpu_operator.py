@@ -223,3 +223,14 @@ def test_operator_on_its_own_queue_equals_current_stream(golden):
         sp = SPDHGPoisson(o, subsets=3, seed=2)
         xs.append(sp.run(torch.zeros(o.coeff_shape, device="cuda"), b, 2, diagnostics_interval=1).cpu().numpy())
     assert np.array_equal(xs[0], xs[1])
+
+
+def test_estimate_L_power_streamed(golden):
+    """The streamed power iteration: with the serial start it is estimate_L_power; with the parallel start (other
+    random numbers) it converges to the same largest eigenvalue of A^T A."""
+    from diffractom_b200 import estimate_L_power, estimate_L_power_streamed
+    op = make_operator(golden("diff_auto_trapezoid"))
+    L = estimate_L_power(op, niter=40, verbose=0)
+    assert estimate_L_power_streamed(op, niter=40, verbose=0, parallel_start=False) == L
+    Lp = estimate_L_power_streamed(op, niter=40, verbose=0)
+    assert abs(Lp / L - 1) < 1e-2
