@@ -53,6 +53,9 @@ class SPDHGPoisson:
     # products). The pass's per-batch interleaving of the two becomes all updates, then all forwards: every batch's
     # forward still reads its updated x and adds into the rows of nb in batch order, so the values are the same bits.
     use_graphs = False
+    # with an operator of precision "bf16", the step sizes S and T come from the BF16 operator (the one the iterations
+    # apply); False: from the float32 operator, as the reference computes them
+    bf16_steps = True
 
     def __init__(self, operator, subsets=8, prox_kind="nonneg", lam=0.0, support="fov", eps_counts=1e-3, rho="auto",
                  seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None, shards=None):
@@ -438,22 +441,44 @@ class SPDHGPoisson:
             self.dqy = torch.empty(be, dtype=torch.float32, device=dev)
 
         self._ray = op.support_ray_table(supp) if supp is not None and self.use_support_table else None
-        # S from the row sums A 1_S (spdhg_poisson.py:621-629)
+        # S from the row sums A 1_S (spdhg_poisson.py:621-629); with a BF16 operator from the BF16 operator that the
+        # iterations apply (the step sizes of the operator in use, at a quarter of the float32 passes' time)
+        bf16 = op.precision == "bf16" and self.bf16_steps
         op._fill(self.D, 0.0)
-        for ib, bt in enumerate(op.batches):
-            _lib.call("dfx_batch_support", self.dzk.data_ptr(), None, sp, npix, op.Kstride, bt["K_batch"], 0.0, 0, s)
-            op._direct_batch_k(self.dzk.data_ptr(), ib, self.D, ray=self._ray)
+        if bf16:
+            for geo, n, om in op._bf16_chunks(None):
+                z = op._z(n)
+                for ib, bt in enumerate(op.batches):
+                    _lib.call("dfx_batch_support", self.dzk.data_ptr(), None, sp, npix, op.Kstride, bt["K_batch"],
+                              0.0, 0, s)
+                    op._radon_forward_bf16(self.dzk.data_ptr(), ib, z, om, n)
+                op._pf_tc_forward(z, om, n, self.D)
+        else:
+            for ib, bt in enumerate(op.batches):
+                _lib.call("dfx_batch_support", self.dzk.data_ptr(), None, sp, npix, op.Kstride, bt["K_batch"], 0.0,
+                          0, s)
+                op._direct_batch_k(self.dzk.data_ptr(), ib, self.D, ray=self._ray)
         self._sum_shards("full")
         self._dual_steps_from_rowsums(gamma)
         # T from the subsets' column sums over the counted points (spdhg_poisson.py:630-643)
         c = float(np.float32(p / gamma))
         T = self.T
+        if bf16:
+            op._rows_to_bf16(self.D, op._all_omegas, op.N_Omega)
 
         def t_batch(ib, s_):
             tb, kb = T.ptr(ib, s_), op.batches[ib]["K_batch"]
             _lib.call("dfx_tinit", tb, be, s)
             for m in range(self.M):
-                op._adjoint_batch_k(self.D, ib, self.dzk.data_ptr(), subset=m)
+                if bf16:                                   # this batch's columns of A_m^T 1_counted, BF16 operator
+                    e = op._sub[m]
+                    z = op._z(e["n"])
+                    op._pf_tc_adjoint(e["omegas"], e["n"], z, ib * op.Kstride, op.Kstride)
+                    _lib.call("dfx_radon_backward_bf16", z.data_ptr() + 2 * ib * op.Kstride, op.Ktot,
+                              self.dzk.data_ptr(), e["geo"].data_ptr(), e["n"], op.Nx, op.Ny, op.My, op.Kstride, kb,
+                              op._kernel_id, int(op.radon_geo.n_taps), s)
+                else:
+                    op._adjoint_batch_k(self.D, ib, self.dzk.data_ptr(), subset=m)
                 _lib.call("dfx_batch_support", tb, self.dzk.data_ptr(), sp, npix, op.Kstride, kb, c, 2, s)
             _lib.call("dfx_tfinal", tb, be, s)           # padding channels were never reached: T = 0 there
 
