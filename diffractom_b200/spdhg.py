@@ -56,6 +56,9 @@ class SPDHGPoisson:
     # with an operator of precision "bf16", the step sizes S and T come from the BF16 operator (the one the iterations
     # apply); False: from the float32 operator, as the reference computes them
     bf16_steps = True
+    # with an operator of precision "bf16", the full forward passes (the objective of the diagnostics epochs, whose
+    # rows also serve the next subset) run on the BF16 tensor-core path too; False: float32
+    bf16_diagnostics = True
 
     def __init__(self, operator, subsets=8, prox_kind="nonneg", lam=0.0, support="fov", eps_counts=1e-3, rho="auto",
                  seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None, shards=None):
@@ -155,6 +158,9 @@ class SPDHGPoisson:
         dual step and update instead); then the forward of the new x for subset fwd ("full": all rows) added to D
         (spdhg_poisson.py:430-484)."""
         op = self.op
+        if op.precision == "bf16" and fwd == "full" and adj is None and not tv and self.bf16_diagnostics:
+            self._full_forward_bf16()
+            return
         if op.precision == "bf16" and fwd != "full":
             self._pass_bf16(adj, fwd, tv)
             return
@@ -185,12 +191,34 @@ class SPDHGPoisson:
         else:
             self.shards.rows(self.D, op._sub[op._subset(fwd)]["omegas"], op.stream())
 
+    def _full_forward_bf16(self):
+        """D = A x on every row through the BF16 path: per angle chunk, the BF16 table forward of every batch's BF16
+        x into its columns of the Radon output, then one tensor-core PF product over all orientations."""
+        op = self.op
+        be = op.batch_elems()
+        X = self.X
+        rp, ent = (op._ray_rp, op._ray_ent) if self._ray is None else self._ray[:2]
+        for geo, n, om in op._bf16_chunks(None):
+            z = op._z(n)
+
+            def compute(ib, s, z=z, n=n, om=om):
+                xb = self.xkb.data_ptr() + (2 * ib * be if X.resident else 0)
+                if not X.resident:
+                    _lib.call("dfx_f32_to_bf16", X.ptr(ib, s), xb, be, op._s())
+                _lib.call("dfx_radon_forward_table_bf16_bf16", xb, z.data_ptr() + 2 * ib * op.Kstride, op.Ktot,
+                          rp.data_ptr(), ent.data_ptr(), om.data_ptr(), n, op.My, op.Kstride,
+                          op.batches[ib]["K_batch"], float(op.radon_geo.scale), op._s())
+
+            self.pipe.run([X], [], compute)
+            op._pf_tc_forward(z, om, n, self.D)
+        self._sum_shards("full")
+
     def _pass_bf16(self, adj, fwd, tv=False):
         """The pass of an operator with precision "bf16": one tensor-core launch takes the dual change of subset adj
         to the BF16 Radon output of all batches, each batch's backprojection applies the primal step and projects the
         new x for subset fwd into its columns of that output, and one tensor-core launch overwrites subset fwd's data
-        rows. Full forward passes (the residual of the diagnostics) stay float32. The BF16 copy of x that the forward
-        reads is kept for all batches when x is resident, else made per batch (one buffer)."""
+        rows (full forward passes: _full_forward_bf16). The BF16 copy of x that the forward reads is kept for all
+        batches when x is resident, else made per batch (one buffer)."""
         op = self.op
         be = op.batch_elems()
         X, Z, T = self.X, self.Z, self.T
