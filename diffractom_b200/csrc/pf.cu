@@ -20,14 +20,30 @@ __device__ __forceinline__ float pf_entry(const dfx_pf_geometry &g, int r, int k
     const float *pole = g.poles + (int64_t)kg * g.A * 3;
     const float inv = __ldg(g.inv_sigma2 + kg);
     float w_total = 0.0f;
+    const bool axis_theta = g.axis_w != nullptr;
     for (int s = 0; s < g.S; ++s)
         for (int se = 0; se < g.S_eta; ++se) {
-            const float *v = g.coords + ((((int64_t)(r * g.S + s) * g.C + c) * g.S_eta + se) * g.P + p) * 3;
+            const float *v = axis_theta
+                                 ? g.coords + (((int64_t)(r * g.S + s) * g.C + c) * g.S_eta + se) * 3
+                                 : g.coords + ((((int64_t)(r * g.S + s) * g.C + c) * g.S_eta + se) * g.P + p) * 3;
             const float vx = __ldg(v), vy = __ldg(v + 1), vz = __ldg(v + 2);
+            float wx = 0.0f, wy = 0.0f, wz = 0.0f;
+            if (axis_theta) {
+                const float *wv = g.axis_w + (int64_t)(r * g.S + s) * 3;
+                wx = __ldg(wv);
+                wy = __ldg(wv + 1);
+                wz = __ldg(wv + 2);
+            }
             float w_node = 0.0f;
             for (int a = a0; a < a1; ++a) {
                 const float nx = __ldg(pole + 3 * a), ny = __ldg(pole + 3 * a + 1), nz = __ldg(pole + 3 * a + 2);
-                const float d = fabsf(__fmaf_rn(nz, vz, __fmaf_rn(ny, vy, __fmul_rn(nx, vx))));
+                const float du = __fmaf_rn(nz, vz, __fmaf_rn(ny, vy, __fmul_rn(nx, vx)));
+                // reflection_two_theta: n . v = cos(theta_a) (n . u) - sin(theta_a) (n . w)
+                const float d = axis_theta
+                                    ? fabsf(__fsub_rn(__fmul_rn(__ldg(g.axis_cos + a), du),
+                                                      __fmul_rn(__ldg(g.axis_sin + a),
+                                                                __fmaf_rn(nz, wz, __fmaf_rn(ny, wy, __fmul_rn(nx, wx))))))
+                                    : fabsf(du);
                 float t = 0.0f;
                 const float e1 = __fmul_rn(__fsub_rn(1.0f, d), inv);
                 if (e1 < g.cut) t = __fadd_rn(t, expf(-e1));
@@ -212,6 +228,8 @@ static int check_geometry(const dfx_pf_geometry *g)
                 "pf: geometry has null pointers");
     DFX_REQUIRE(g->R > 0 && g->C > 0 && g->P > 0 && g->A > 0 && g->S > 0 && g->S_eta > 0 && g->K > 0,
                 "pf: bad geometry sizes");
+    DFX_REQUIRE((g->axis_w == nullptr) == (g->axis_sin == nullptr) && (g->axis_w == nullptr) == (g->axis_cos == nullptr),
+                "pf: reflection_two_theta needs axis_w, axis_sin and axis_cos together");
     return DFX_OK;
 }
 

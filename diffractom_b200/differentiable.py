@@ -24,7 +24,7 @@ import torch
 from scipy.spatial.transform import Rotation
 
 from .arrays import as_host, check_device, is_device, stream_scope
-from .geometry import kernel_factors, probed_directions, radon_geometry, rotate_axes
+from .geometry import axis_directions, kernel_factors, probed_directions, radon_geometry, rotate_axes
 
 PF_GROUPS = ("rot", "sigma", "eta_offset", "axis_tilt", "two_theta")
 
@@ -123,6 +123,8 @@ class PFGradient:
             raise NotImplementedError("PFGradient needs the (K, Ny, Nx) or the local coefficient layout")
         if int(op.N_peaks) > 16:
             raise NotImplementedError("PFGradient supports at most 16 rings")
+        if getattr(op, "reflection_two_theta", False):
+            raise NotImplementedError("PFGradient with reflection_two_theta is not provided")
         self.op = op
         self.hessian = bool(hessian)
         self.local_size = int(local_size)
@@ -365,10 +367,19 @@ def _rebuild(op, pf_changed, geo_changed):
             op.inv_sigma2_gpu = _f32_dev(inv_s2, dev)
             op.norm_factor_gpu = _f32_dev(norm, dev)
         if geo_changed:
-            coords = probed_directions(op.two_theta_peaks, op.angles_subdivided, op.eta_angles_subdivided,
-                                       op.N_Omega, op.N_eta, op.cfg)
-            _set(op, coords_cpu=coords)
-            op.coords_gpu = _f32_dev(coords, dev)
+            if getattr(op, "reflection_two_theta", False):
+                # u and w do not depend on the Bragg angles; the axes' angles follow their channels' two_theta
+                u, w = axis_directions(op.angles_subdivided, op.eta_angles_subdivided, op.N_Omega, op.N_eta, op.cfg)
+                _set(op, coords_cpu=u, w_cpu=w)
+                tth, sn, cs = op.geometry.axis_theta()
+                _set(op, axis_two_theta_cpu=tth, axis_sin_cpu=sn, axis_cos_cpu=cs)
+                op.coords_gpu = _f32_dev(u, dev)
+                op._upload_axis_theta()
+            else:
+                coords = probed_directions(op.two_theta_peaks, op.angles_subdivided, op.eta_angles_subdivided,
+                                           op.N_Omega, op.N_eta, op.cfg)
+                _set(op, coords_cpu=coords)
+                op.coords_gpu = _f32_dev(coords, dev)
         op._make_pfg()
         op.release_streamer()
         op.release_omega_subsets()

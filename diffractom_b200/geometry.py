@@ -41,23 +41,43 @@ def probed_directions(two_theta_f32, omega_nodes, eta_nodes, n_omega, n_eta, cfg
     return np.asarray(np.stack(per_ring, axis=-2), dtype=np.float32, order="C")
 
 
+def axis_directions(omega_nodes, eta_nodes, n_omega, n_eta, cfg):
+    """The probed directions of reflection_two_theta, stored once for all channels (SPFO:581-591): u (R, S, C, S_eta,
+    3) float32 = R(omega)^T (cos(eta) d0 + sin(eta) d90) and w (R * S, 3) float32 = R(omega)^T p0; a pole axis with
+    Bragg angle theta probes v = cos(theta) u - sin(theta) w."""
+    S = len(omega_nodes) // n_omega
+    Se = len(eta_nodes) // n_eta
+    eta2 = np.asarray(eta_nodes, np.float64).reshape(n_eta, Se)
+    d0 = np.array(cfg["detector_direction_origin"])
+    d90 = np.array(cfg["detector_direction_positive_90"])
+    p0 = np.array(cfg["p_direction_0"])
+    k0 = np.asarray(cfg["k_direction_0"])
+    rot = Rotation.from_rotvec(np.asarray(omega_nodes, np.float64)[:, None] * k0).as_matrix()
+    base = np.cos(eta2)[..., None] * d0[None, None, :] + np.sin(eta2)[..., None] * d90[None, None, :]
+    u = np.asarray(np.einsum("oij,esi->oesj", rot, base).reshape(n_omega, S, n_eta, Se, 3), np.float32, order="C")
+    w = np.asarray(np.einsum("oij,i->oj", rot, p0), np.float32, order="C")
+    return u, w
+
+
 @dataclass
 class PoleAxes:
     axes: np.ndarray        # (A, 3) float64 unit axes (crystal frame), rings one after the other
     counts: np.ndarray      # (A,) float32 images per axis (family-share weighted)
     start: np.ndarray       # (P + 1,) int32 first axis of every ring
     family_weights: list
+    two_theta: np.ndarray = None   # (A,) float64: the Bragg angle of every axis (its reflections' share-weighted mean)
 
 
-def pole_axes(material, ring_reflections, ring_overlap, shares=None) -> PoleAxes:
+def pole_axes(material, ring_reflections, ring_overlap, shares=None, refl_two_theta=None) -> PoleAxes:
     """The distinct symmetry images S_g h of every ring's reflections, up to sign, with their (share-weighted)
     counts (SPFO:742-825). shares: per ring the family shares before normalisation (default multiplicity x overlap:
     the normalized operator). Images are rounded to 6 decimals before they are merged, and the axes are the merged
-    rounded vectors normalised, as in the reference."""
+    rounded vectors normalised, as in the reference. refl_two_theta (per reflection, float64): also the Bragg angle
+    of every axis, the share-weighted mean of its images' (the plain mean where the shares are 0; SPFO:795-806)."""
     h = np.asarray(material.h_vecs_normed, dtype=np.float64)
     sym = np.asarray(material.point_group_matrices, dtype=np.float64).reshape(-1, 3, 3)
     mult = np.asarray(material.reflections["multiplicity"], dtype=np.float64)
-    axes, counts, start, fw = [], [], [0], []
+    axes, counts, start, fw, tths = [], [], [0], [], []
     for ip, (refl, overlap) in enumerate(zip(ring_reflections, ring_overlap)):
         refl = np.asarray(refl)
         share = (mult[refl] if shares is None else np.asarray(shares[ip], np.float64)) * overlap
@@ -67,13 +87,22 @@ def pole_axes(material, ring_reflections, ring_overlap, shares=None) -> PoleAxes
         fw.append(share)
         imgs = np.concatenate([sym @ h[f] for f in refl])
         wts = np.concatenate([np.full(len(sym), w) for w in share])
+        img_tth = None if refl_two_theta is None else np.repeat(np.asarray(refl_two_theta, np.float64)[refl], len(sym))
         lead = np.argmax(np.abs(imgs) > 1e-6, axis=1)
         imgs = imgs * np.sign(imgs[np.arange(len(imgs)), lead])[:, None]
         uniq, inv = np.unique(np.round(imgs, 6), axis=0, return_inverse=True)
-        counts.append(np.bincount(inv.ravel(), weights=wts, minlength=len(uniq)))
+        cnt = np.bincount(inv.ravel(), weights=wts, minlength=len(uniq))
+        counts.append(cnt)
+        if img_tth is not None:
+            nimg = np.bincount(inv.ravel(), minlength=len(uniq))
+            tth = np.bincount(inv.ravel(), weights=img_tth, minlength=len(uniq)) / nimg
+            has = cnt > 0
+            tth[has] = np.bincount(inv.ravel(), weights=wts * img_tth, minlength=len(uniq))[has] / cnt[has]
+            tths.append(tth)
         axes.append(uniq / np.linalg.norm(uniq, axis=1, keepdims=True))
         start.append(start[-1] + len(uniq))
-    return PoleAxes(np.concatenate(axes), np.concatenate(counts).astype(np.float32), np.asarray(start, np.int32), fw)
+    return PoleAxes(np.concatenate(axes), np.concatenate(counts).astype(np.float32), np.asarray(start, np.int32), fw,
+                    np.concatenate(tths) if tths else None)
 
 
 def rotate_axes(rot: np.ndarray, axes: np.ndarray, block: int = 4096) -> np.ndarray:
@@ -147,7 +176,7 @@ class OperatorGeometry:
 
     def __init__(self, cfg, material, grid, *, normalized=False, quadrature="auto", quadrature_tol=0.05,
                  pf_cutoff_sigma=4.0, radon_kernel="trapezoid", rings=None, ring_two_theta=None,
-                 ring_intensities=None):
+                 ring_intensities=None, reflection_two_theta=False):
         from .grid import grid_arrays, grid_sigma_min
         from .material import group_reflections_into_rings
         from .quadrature import pf_cut_value, setup_quadrature
@@ -191,6 +220,14 @@ class OperatorGeometry:
         self.two_theta_peaks = two_theta_of_rings(self.h_cpu, float(cfg["energy"]))
         if ring_two_theta is not None:
             self.two_theta_peaks = np.asarray(ring_two_theta, dtype=np.float32).copy()
+        elif rings is not None:
+            # a window: the overlap-weighted mean two-theta of its reflections, float32 as for one ring (SPFO:560-566)
+            lam = ENERGY_KEV_A / float(cfg["energy"])
+            hh = np.asarray(material.h_vecs, dtype=np.float32)
+            tth = (2.0 * np.arcsin(np.linalg.norm(hh, axis=1) / (4.0 * np.pi) * lam)).astype(np.float32)
+            self.two_theta_peaks = np.array([np.average(tth[ix], weights=w) if w.sum() > 0 else tth[ix[0]]
+                                             for ix, w in zip(self.ring_reflections, self.ring_overlap)],
+                                            dtype=np.float32)
         if self.normalized:
             self.intens_cpu = np.ones(self.N_peaks, np.float32)
         else:
@@ -201,12 +238,25 @@ class OperatorGeometry:
             if not np.all(np.isfinite(ri)) or np.any(ri <= 0):
                 raise ValueError("ring_intensities must be finite and positive")
             self.intens_cpu = ri.astype(np.float32)
-        self.coords_cpu = probed_directions(self.two_theta_peaks, self.angles_subdivided, self.eta_angles_subdivided,
-                                            self.N_Omega, self.N_eta, cfg)
+        self.reflection_two_theta = bool(reflection_two_theta)
+        if self.reflection_two_theta:
+            self.coords_cpu, self.w_cpu = axis_directions(self.angles_subdivided, self.eta_angles_subdivided,
+                                                          self.N_Omega, self.N_eta, cfg)
+        else:
+            self.coords_cpu = probed_directions(self.two_theta_peaks, self.angles_subdivided,
+                                                self.eta_angles_subdivided, self.N_Omega, self.N_eta, cfg)
+            self.w_cpu = None
         self.grid_rot_cpu, self.sigma_cpu = grid_arrays(grid)
         self.K = len(self.sigma_cpu)
-        pa = pole_axes(material, self.ring_reflections, self.ring_overlap)
+        lam = ENERGY_KEV_A / float(cfg["energy"])
+        refl_tth = 2.0 * np.arcsin(np.linalg.norm(np.asarray(material.h_vecs, np.float64), axis=1) / (4.0 * np.pi)
+                                   * lam)
+        pa = pole_axes(material, self.ring_reflections, self.ring_overlap,
+                       refl_two_theta=refl_tth if self.reflection_two_theta else None)
         self.pole_axes_cpu, self.axis_count_cpu, self.axis_start_cpu = pa.axes, pa.counts, pa.start
+        self.axis_two_theta_built = pa.two_theta
+        self._two_theta_built = np.asarray(self.two_theta_peaks, np.float64).copy()
+        self.axis_two_theta_cpu, self.axis_sin_cpu, self.axis_cos_cpu = self.axis_theta()
         self.ring_family_weights = pa.family_weights
         self.N_axes = len(pa.axes)
         self.poles_cpu = rotate_axes(self.grid_rot_cpu, pa.axes)
@@ -217,6 +267,19 @@ class OperatorGeometry:
         self.radon_kernel = radon_kernel
         self.radon_geo = radon_geometry(self.angles, self.Nx, self.Ny, self.My, self.image_width, self.My,
                                         self.detector_shifts(), self.angle_weight, radon_kernel)
+
+    def axis_theta(self):
+        """reflection_two_theta: the Bragg angle of every pole axis, its reflections' own, moved by its channel's
+        change of two_theta since the operator was built, with sin and cos of theta as float32 (SPFO:829-842);
+        (None, None, None) otherwise."""
+        if not self.reflection_two_theta:
+            return None, None, None
+        tth = np.asarray(self.axis_two_theta_built, np.float64).copy()
+        shift = np.asarray(self.two_theta_peaks, np.float64) - self._two_theta_built
+        for p, d in enumerate(shift):
+            tth[self.axis_start_cpu[p]:self.axis_start_cpu[p + 1]] += d
+        th = 0.5 * tth
+        return tth, np.sin(th).astype(np.float32), np.cos(th).astype(np.float32)
 
     def detector_shifts(self):
         """Detector shift of every projection angle: cor_offset minus per-angle shifts (SPFO:1616-1620)."""

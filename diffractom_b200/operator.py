@@ -66,12 +66,12 @@ class SinglePhaseForwardOperator:
 
         precision: "fp32" (the reference's arithmetic) or "bf16": direct_cl / adjoint_cl on device tensors then run
         the Radon output through BF16 and the pole-figure products on the tensor cores (dense BF16 PF of all
-        orientations, float32 accumulation); the float32 sparse PF stays available (the solvers use it for set-up
-        and for their once-per-epoch residual), NumPy (streamed) calls stay float32.
+        orientations, float32 accumulation); the float32 sparse PF stays available (NumPy (streamed) calls stay
+        float32). reflection_two_theta: every pole axis probes at its reflections' own Bragg angle (the windows of
+        rings= then hold reflections of different angles; SPFO:236-244).
 
         Not provided (NotImplementedError): projector "gratopy", the BF16 path with the Fourier-slice projector,
-        pf_mode "dense" (the sparse products give the same operator), reflection_two_theta, window_parallax, custom
-        rings with overlap weights other than 1."""
+        pf_mode "dense" (the sparse products give the same operator), window_parallax."""
         lib = _lib.lib()                                    # fails loudly without the CUDA library
         if not torch.cuda.is_available():
             raise RuntimeError("SinglePhaseForwardOperator needs a CUDA device")
@@ -90,8 +90,8 @@ class SinglePhaseForwardOperator:
         self.sparse_batch_max = int(sparse_batch_max)
         self.cfg = {**cfg, **kwargs}
         self.material, self.grid = material, grid
-        if reflection_two_theta or window_parallax is not None:
-            raise NotImplementedError("reflection_two_theta and window_parallax are not provided by this operator")
+        if window_parallax is not None:
+            raise NotImplementedError("window_parallax is not provided by this operator")
         if projector not in ("auto", "native", "fft", "gratopy"):
             raise ValueError(f"projector must be 'auto', 'native', 'fft' or 'gratopy', not {projector!r}")
         if projector == "gratopy":
@@ -107,7 +107,7 @@ class SinglePhaseForwardOperator:
         geom = OperatorGeometry(self.cfg, material, grid, normalized=normalized, quadrature=quadrature,
                                 quadrature_tol=quadrature_tol, pf_cutoff_sigma=pf_cutoff_sigma,
                                 radon_kernel=geom_kernel, rings=rings, ring_two_theta=ring_two_theta,
-                                ring_intensities=ring_intensities)
+                                ring_intensities=ring_intensities, reflection_two_theta=reflection_two_theta)
         self.__dict__.update({k: v for k, v in vars(geom).items() if k != "cfg"})
         self.geometry = geom
         self.pf_batch_max_gb = float(max_gb)
@@ -137,6 +137,7 @@ class SinglePhaseForwardOperator:
             self.quad_weights_gpu = None if self.quad_weights_cpu is None else dev(self.quad_weights_cpu)
             self.intens_gpu = None if self.normalized else dev(self.intens_cpu)
             self.geo_gpu = dev(self.radon_geo.geo)
+            self._upload_axis_theta()
             self._pf_version = 0
             self._make_pfg()
             self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
@@ -170,6 +171,15 @@ class SinglePhaseForwardOperator:
                 self.build_dense_bf16_pf()
 
     # ------------------------------------------------------------------ small helpers
+    def _upload_axis_theta(self):
+        """reflection_two_theta: the rotated p0 and every pole axis's sin / cos of theta on the device (None
+        otherwise)."""
+        if not self.reflection_two_theta:
+            self.w_gpu = self.axis_sin_gpu = self.axis_cos_gpu = None
+            return
+        dev = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=self.device)
+        self.w_gpu, self.axis_sin_gpu, self.axis_cos_gpu = dev(self.w_cpu), dev(self.axis_sin_cpu), dev(self.axis_cos_cpu)
+
     def _make_pfg(self):
         """The PF kernels' view of the device parameters (dfx_pf_geometry), made again after they change."""
         self._pfg = _lib.PFGeometry(
@@ -178,7 +188,9 @@ class SinglePhaseForwardOperator:
             None if self.quad_weights_gpu is None else self.quad_weights_gpu.data_ptr(),
             None if self.intens_gpu is None else self.intens_gpu.data_ptr(),
             self.N_Omega, self.N_eta, self.N_peaks, self.N_axes, self.N_Omega_subdivisions, self.N_eta_subdivisions,
-            self.K, float(self.pf_cut))
+            self.K, float(self.pf_cut),
+            *((None, None, None) if self.w_gpu is None else
+              (self.w_gpu.data_ptr(), self.axis_sin_gpu.data_ptr(), self.axis_cos_gpu.data_ptr())))
 
     def stream(self) -> torch.cuda.Stream:
         return self.queue if self.queue is not None else torch.cuda.current_stream(self.device)

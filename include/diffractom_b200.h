@@ -146,6 +146,12 @@ typedef struct dfx_pf_geometry {
     const float *intens;       /* (P) ring intensities, NULL: normalized (every ring weight 1) */
     int32_t R, C, P, A, S, S_eta, K;
     float cut;                 /* exponent at which the Gaussian is cut (pf_cutoff_sigma^2 / 2) */
+    /* reflection_two_theta (SPFO:581-591, pf_generate.cl:37-43, 82-100), all NULL otherwise: every pole axis has its
+     * own Bragg angle theta_a; coords then holds u (R, S, C, S_eta, 3), without the ring index, and the entry uses
+     * v = cos(theta_a) u - sin(theta_a) w. */
+    const float *axis_w;       /* (R * S, 3) the rotated p0 */
+    const float *axis_sin;     /* (A) sin(theta_a) */
+    const float *axis_cos;     /* (A) cos(theta_a) */
 } dfx_pf_geometry;
 
 /* replaces pfmatrix_eval_poles + SCALE_PF_BY_INTENSITY_INPLACE (create_pfo_matrix.py:108-199, pf_kernels.cl:450-465;

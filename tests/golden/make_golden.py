@@ -52,7 +52,8 @@ from diffractom.operators.single_phase_forward_operator import SinglePhaseForwar
 from diffractom.utils.support import fov_support_mask  # noqa: E402
 
 
-def host_operator(cfg, mat, grid, quadrature="auto", kernel="trapezoid", pf_cutoff_sigma=4.0):
+def host_operator(cfg, mat, grid, quadrature="auto", kernel="trapezoid", pf_cutoff_sigma=4.0, rings=None,
+                  reflection_two_theta=False):
     """A SinglePhaseForwardOperator with its host state only (the steps of __init__ that run on the host)."""
     op = SinglePhaseForwardOperator.__new__(SinglePhaseForwardOperator)
     op.reserve_coefficient_arrays = 3
@@ -66,9 +67,14 @@ def host_operator(cfg, mat, grid, quadrature="auto", kernel="trapezoid", pf_cuto
     op.intensity_model = as_intensity_model(None)
     op.material, op.grid, op.verbose = mat, grid, False
     op.N_eta = op.cfg["N_eta"]
-    op.ring_reflections = group_reflections_into_rings(mat)
-    op.ring_overlap = [np.ones(len(r)) for r in op.ring_reflections]
-    op._custom_rings, op._ring_two_theta, op.reflection_two_theta = False, None, False
+    if rings is None:
+        op.ring_reflections = group_reflections_into_rings(mat)
+        op.ring_overlap = [np.ones(len(r)) for r in op.ring_reflections]
+    else:
+        op.ring_reflections = [np.asarray(ix, dtype=np.int64) for ix, _ in rings]
+        op.ring_overlap = [np.asarray(w, dtype=np.float64) for _, w in rings]
+    op._custom_rings, op._ring_two_theta = rings is not None, None
+    op.reflection_two_theta = bool(reflection_two_theta)
     op.N_peaks = len(op.ring_reflections)
     op.N_seg = op.N_peaks * op.N_eta
     op.Nx, op.Ny, op.My, op.N_Omega = cfg["Nx"], cfg["Ny"], cfg["My"], cfg["N_Omega"]
@@ -222,5 +228,50 @@ def main():
     print("materials:", sorted({k.split("_")[0] for k in mats}))
 
 
+
+
+def axis_case(name="refl_windows"):
+    """reflection_two_theta with windows of reflections of different Bragg angles (the geometry and material of the
+    reference's tests/test_reflection_two_theta.py): the operator model's PF, forward and adjoint, and the probed
+    u, w and axis angles."""
+    from scipy.spatial.transform import Rotation
+    from diffractom import MatrixGrid
+    cfg = {**BASE, "Nx": 14, "Ny": 12, "My": 17, "N_Omega": 16, "angle_range": [0, 360], "cor_offset": 0.7,
+           "N_eta": 36, "energy": 12.398 / 0.35}
+    spec = dict(a=8.1, b=12.8, c=7.1, alpha=94, beta=116, gamma=88, crystal_system="triclinic", wavelength_A=0.35,
+                hkl_list=np.array([[1, 0, 0], [0, 1, 0], [1, 1, 0], [1, -1, 0], [0, 0, 1], [1, 0, 1]]))
+    windows = [([0, 1], [1.0, 0.6]), ([2, 3], [0.5, 1.0]), ([4], [1.0])]
+    mat = Material.from_lattice_parameters(**spec)
+    rot = Rotation.random(10, random_state=5).as_matrix()
+    grid = MatrixGrid(rot, np.full(10, np.deg2rad(3.0)))
+    op = host_operator(cfg, mat, grid, "auto", "trapezoid", rings=windows, reflection_two_theta=True)
+    ref = ReferenceModel(op)
+    prm = ref.params0()
+    rng = np.random.default_rng(7)
+    supp = fov_support_mask(op.Nx, op.Ny, op.My, angles=op.angles, image_width=op.image_width, detector_width=op.My,
+                            detector_shift=op.cor_offset)
+    c = (rng.random((op.K, op.Ny, op.Nx)) * supp[None]).astype(np.float32)
+    r = rng.random((op.N_Omega, op.My, op.N_seg)).astype(np.float32)
+    rule = op.quadrature
+    mat_json = {k: (v.tolist() if isinstance(v, np.ndarray) else v) for k, v in spec.items()}
+    out = dict(cfg=json.dumps(cfg), material=json.dumps(mat_json), rings=json.dumps(windows), kernel="trapezoid",
+               quadrature="auto", rot=np.asarray(op.grid_rot_cpu, np.float64), sigma=np.asarray(op.sigma_cpu, np.float32),
+               sigma64=np.full(10, np.deg2rad(3.0)), c=c, r=r,
+               rule=np.array([rule.p_omega, rule.k_omega, rule.p_eta, rule.k_eta], np.int32),
+               coords=np.asarray(op.coords_cpu, np.float32), w=np.asarray(op.w_cpu, np.float32),
+               two_theta=np.asarray(op.two_theta_peaks, np.float32),
+               axis_two_theta=np.asarray(op.axis_two_theta_cpu, np.float64),
+               axes=np.asarray(op.pole_axes_cpu, np.float64), counts=np.asarray(op.axis_count_cpu, np.float32),
+               start=np.asarray(op.axis_start_cpu, np.int32), support=supp,
+               pf=ref.pf(prm), fwd=ref.forward(c, prm), adj=ref.vjp(c, prm, r, groups=("c",))["c"])
+    np.savez_compressed(OUT / f"{name}.npz", **out)
+    print(f"{name}: K={op.K} R={op.N_Omega} C={op.N_eta} P={op.N_peaks} axes={op.N_axes}")
+
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 2 and sys.argv[2] == "axis":       # only the reflection_two_theta case
+        axis_case()
+    else:
+        main()
+        axis_case()

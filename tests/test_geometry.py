@@ -77,3 +77,23 @@ def test_interleaved_subsets_and_errors():
     assert [list(a) for a in s] == [[0, 3, 6, 9], [1, 4, 7], [2, 5, 8]]
     with pytest.raises(ValueError):
         interleaved_subsets(4, 5)
+
+
+def test_reflection_two_theta_geometry_matches_reference(golden):
+    """reflection_two_theta with windows of reflections at different Bragg angles: the probed u and w, every axis's
+    Bragg angle and the windows' mean two-theta equal the reference's."""
+    import json
+    from diffractom_b200.geometry import OperatorGeometry
+    from diffractom_b200.grid import MatrixGrid
+    from diffractom_b200.material import Material
+    d = golden("refl_windows")
+    rings = [(ix, w) for ix, w in json.loads(str(d["rings"]))]
+    mat = Material.from_lattice_parameters(**d["material"])
+    g = OperatorGeometry(d["cfg"], mat, MatrixGrid(d["rot"], d["sigma64"]), normalized=True,
+                         quadrature=d["quadrature"], radon_kernel=d["kernel"], rings=rings,
+                         reflection_two_theta=True)
+    assert np.array_equal(g.two_theta_peaks, d["two_theta"])
+    assert np.abs(g.coords_cpu - d["coords"]).max() <= 2e-7 and np.abs(g.w_cpu - d["w"]).max() <= 2e-7
+    assert np.array_equal(g.axis_start_cpu, d["start"]) and np.allclose(g.pole_axes_cpu, d["axes"], atol=1e-12)
+    assert np.allclose(g.axis_two_theta_cpu, d["axis_two_theta"], rtol=0, atol=1e-14)
+    assert len(np.unique(np.round(g.axis_two_theta_cpu[d["start"][0]:d["start"][1]], 9))) == 2   # two angles in a window
