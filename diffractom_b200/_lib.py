@@ -87,7 +87,7 @@ SIGNATURES = {
     "dfx_tv_adjoint_update": ([P, P, P, P, P, I, I, I, F, F, S], c_int),
     "dfx_tv_value": ([P, P, I, I, I, P, P, c_size_t, S], c_int),
     "dfx_pf_param_nq": ([I, I], c_int),
-    "dfx_pf_param_vjp": ([POINTER(PFGeometry), P, P, P, P, P, I, I, I, I, I, P, P, P, P, I, P, S], c_int),
+    "dfx_pf_param_vjp": ([POINTER(PFGeometry), P, P, P, P, P, I, I, I, I, I, P, P, P, P, P, P, I, P, S], c_int),
     "dfx_pf_rows_sum": ([P, I, I, I, P, S], c_int),
     "dfx_radon_dtable_fill": ([P, I, I, I, I, I, P, P, S], c_int),
     "dfx_angle_dot": ([P, P, I, I, I, I, P, S], c_int),

@@ -42,7 +42,8 @@ __global__ void __launch_bounds__(PG_THREADS) pf_param_vjp_kernel(
     dfx_pf_geometry g, const int32_t *__restrict__ row_ptr, const uint16_t *__restrict__ col_j,
     const float *__restrict__ res, const float *__restrict__ curv, const float *__restrict__ sino, int my,
     int kstride, int k0, int kb, int flags, const float *__restrict__ dv_eta, const float *__restrict__ dv_t1,
-    const float *__restrict__ dv_t2, const float *__restrict__ dv_tth, double *__restrict__ rows, int nq)
+    const float *__restrict__ dv_t2, const float *__restrict__ dv_tth, const float *__restrict__ dw_t1,
+    const float *__restrict__ dw_t2, double *__restrict__ rows, int nq)
 {
     using L = PGLayout<HESS>;
     extern __shared__ float lS[];                         // my floats, then the warps' partial sums
@@ -57,6 +58,9 @@ __global__ void __launch_bounds__(PG_THREADS) pf_param_vjp_kernel(
     const float fk = g.norm[kg];
     const float w_mid = 1.0f / (float)(S * Se);
     const bool w_eta = flags & 1, w_tilt = flags & 2, w_tth = flags & 4;
+    // reflection_two_theta: coords = u without the ring index, v = cos(theta_a) u - sin(theta_a) w per axis; the
+    // derivatives of u (dv_*) and of w (dw_*) are given, the Bragg angle's is formed here (pf_grad.cl:100-122)
+    const bool axis_theta = g.axis_w != nullptr;
     double acc[L::Q_TTH];
     double att[PG_PMAX];
 #pragma unroll
@@ -79,14 +83,26 @@ __global__ void __launch_bounds__(PG_THREADS) pf_param_vjp_kernel(
         for (int s = 0; s < S; ++s) {
             for (int se = 0; se < Se; ++se) {
                 const float w = g.quad_w ? g.quad_w[s * Se + se] : w_mid;
-                const int64_t cb = ((((int64_t)(r * S + s) * C + c) * Se + se) * P + p) * 3;
-                const float vx = g.coords[cb], vy = g.coords[cb + 1], vz = g.coords[cb + 2];
+                const int64_t cb = axis_theta ? (((int64_t)(r * S + s) * C + c) * Se + se) * 3
+                                              : ((((int64_t)(r * S + s) * C + c) * Se + se) * P + p) * 3;
+                const int64_t wb = (int64_t)(r * S + s) * 3;
+                const float ux = g.coords[cb], uy = g.coords[cb + 1], uz = g.coords[cb + 2];
+                const float wx = axis_theta ? g.axis_w[wb] : 0.0f, wy = axis_theta ? g.axis_w[wb + 1] : 0.0f,
+                            wz = axis_theta ? g.axis_w[wb + 2] : 0.0f;
                 for (int a = a0; a < a1; ++a) {
                     const float *n = g.poles + ((int64_t)kg * A + a) * 3;
                     const float nx = n[0], ny = n[1], nz = n[2];
+                    const float ct = axis_theta ? g.axis_cos[a] : 1.0f, st = axis_theta ? g.axis_sin[a] : 0.0f;
+                    const float vx = axis_theta ? ct * ux - st * wx : ux, vy = axis_theta ? ct * uy - st * wy : uy,
+                                vz = axis_theta ? ct * uz - st * wz : uz;
                     // n . v near 1 for the terms that count: formed in float64 so that 1 - |n . v| keeps its
                     // digits (in float32 the exponent (1 - |d|) / sigma^2 of a narrow kernel loses up to 1e-4)
-                    const double Dd = fma((double)nx, (double)vx, fma((double)ny, (double)vy, (double)nz * vz));
+                    const double du = fma((double)nx, (double)ux, fma((double)ny, (double)uy, (double)nz * uz));
+                    const double Dd = axis_theta
+                                          ? (double)ct * du -
+                                                (double)st * fma((double)nx, (double)wx,
+                                                                 fma((double)ny, (double)wy, (double)nz * wz))
+                                          : du;
                     const float D = (float)Dd;
                     const double add = fabs(Dd);
                     const float ad = (float)add;
@@ -100,12 +116,23 @@ __global__ void __launch_bounds__(PG_THREADS) pf_param_vjp_kernel(
                     dr2 = fmaf(gd, nx * vy - ny * vx, dr2);
                     gs = fmaf(cw, e1 + e2, gs);
                     dgs = fmaf(cw, -(1.0f - ad) * e1 - (1.0f + ad) * e2, dgs);
-                    if (w_eta) de = fmaf(gd, dot3(dv_eta + cb, nx, ny, nz), de);
-                    if (w_tilt) {
-                        dt1 = fmaf(gd, dot3(dv_t1 + cb, nx, ny, nz), dt1);
-                        dt2 = fmaf(gd, dot3(dv_t2 + cb, nx, ny, nz), dt2);
+                    if (axis_theta) {
+                        if (w_eta) de = fmaf(gd * ct, dot3(dv_eta + cb, nx, ny, nz), de);
+                        if (w_tilt) {
+                            dt1 = fmaf(gd, ct * dot3(dv_t1 + cb, nx, ny, nz) - st * dot3(dw_t1 + wb, nx, ny, nz), dt1);
+                            dt2 = fmaf(gd, ct * dot3(dv_t2 + cb, nx, ny, nz) - st * dot3(dw_t2 + wb, nx, ny, nz), dt2);
+                        }
+                        if (w_tth)
+                            dtt = fmaf(gd, 0.5f * (-st * dot3(g.coords + cb, nx, ny, nz) -
+                                                   ct * dot3(g.axis_w + wb, nx, ny, nz)), dtt);
+                    } else {
+                        if (w_eta) de = fmaf(gd, dot3(dv_eta + cb, nx, ny, nz), de);
+                        if (w_tilt) {
+                            dt1 = fmaf(gd, dot3(dv_t1 + cb, nx, ny, nz), dt1);
+                            dt2 = fmaf(gd, dot3(dv_t2 + cb, nx, ny, nz), dt2);
+                        }
+                        if (w_tth) dtt = fmaf(gd, dot3(dv_tth + cb, nx, ny, nz), dtt);
                     }
-                    if (w_tth) dtt = fmaf(gd, dot3(dv_tth + cb, nx, ny, nz), dtt);
                 }
             }
         }
@@ -202,7 +229,8 @@ extern "C" int dfx_pf_param_nq(int n_rings, int hess) { return 4 + (hess ? 10 : 
 extern "C" int dfx_pf_param_vjp(const dfx_pf_geometry *g, const int32_t *row_ptr, const uint16_t *col_j,
                                 const float *res, const float *curv, const float *sino, int my, int kstride, int k0,
                                 int kb, int flags, const float *dv_eta, const float *dv_t1, const float *dv_t2,
-                                const float *dv_tth, int hess, double *rows, void *stream)
+                                const float *dv_tth, const float *dw_t1, const float *dw_t2, int hess, double *rows,
+                                void *stream)
 {
     DFX_REQUIRE(g && row_ptr && col_j && res && sino && rows, "pf_param_vjp: null pointer");
     DFX_REQUIRE(g->coords && g->poles && g->axis_start && g->axis_count && g->inv_sigma2 && g->norm,
@@ -213,7 +241,11 @@ extern "C" int dfx_pf_param_vjp(const dfx_pf_geometry *g, const int32_t *row_ptr
     DFX_REQUIRE(!hess || curv, "pf_param_vjp: the Hessian blocks need curv");
     DFX_REQUIRE(!(flags & 1) || dv_eta, "pf_param_vjp: eta offset requested without its derivatives");
     DFX_REQUIRE(!(flags & 2) || (dv_t1 && dv_t2), "pf_param_vjp: axis tilt requested without its derivatives");
-    DFX_REQUIRE(!(flags & 4) || dv_tth, "pf_param_vjp: two-theta requested without its derivatives");
+    const bool axis_theta = g->axis_w != nullptr;
+    DFX_REQUIRE(!(flags & 4) || dv_tth || axis_theta, "pf_param_vjp: two-theta requested without its derivatives");
+    DFX_REQUIRE(!(flags & 2) || !axis_theta || (dw_t1 && dw_t2),
+                "pf_param_vjp: axis tilt with reflection_two_theta needs the derivatives of w");
+    DFX_REQUIRE(!axis_theta || (g->axis_sin && g->axis_cos), "pf_param_vjp: incomplete axis Bragg angles");
     const int64_t n_rows = (int64_t)g->R * kb;
     DFX_REQUIRE(n_rows < 2147483647LL, "pf_param_vjp: too many rows");
     const int nq = dfx_pf_param_nq(g->P, hess);
@@ -222,10 +254,12 @@ extern "C" int dfx_pf_param_vjp(const dfx_pf_geometry *g, const int32_t *row_ptr
     cudaStream_t s = (cudaStream_t)stream;
     if (hess)
         pf_param_vjp_kernel<1><<<(unsigned)n_rows, PG_THREADS, smem, s>>>(
-            *g, row_ptr, col_j, res, curv, sino, my, kstride, k0, kb, flags, dv_eta, dv_t1, dv_t2, dv_tth, rows, nq);
+            *g, row_ptr, col_j, res, curv, sino, my, kstride, k0, kb, flags, dv_eta, dv_t1, dv_t2, dv_tth, dw_t1,
+            dw_t2, rows, nq);
     else
         pf_param_vjp_kernel<0><<<(unsigned)n_rows, PG_THREADS, smem, s>>>(
-            *g, row_ptr, col_j, res, curv, sino, my, kstride, k0, kb, flags, dv_eta, dv_t1, dv_t2, dv_tth, rows, nq);
+            *g, row_ptr, col_j, res, curv, sino, my, kstride, k0, kb, flags, dv_eta, dv_t1, dv_t2, dv_tth, dw_t1,
+            dw_t2, rows, nq);
     return launch_status("pf_param_vjp");
 }
 

@@ -76,6 +76,31 @@ def probed_derivatives(op, groups=("eta_offset", "axis_tilt", "two_theta")):
     return out
 
 
+def probed_parts_derivatives(op, groups=("eta_offset", "axis_tilt")):
+    """reflection_two_theta: the derivatives of u (R, S, C, S_eta, 3) and w (R * S, 3), v = cos(theta) u - sin(theta) w,
+    float64 (reference.py:151-167): "eta_offset" (du), ("axis_tilt", i) (du), ("axis_tilt_w", i) (dw)."""
+    R, C = int(op.N_Omega), int(op.N_eta)
+    S, Se = int(op.N_Omega_subdivisions), int(op.N_eta_subdivisions)
+    vec = lambda key: np.asarray(op.cfg[key], np.float64)
+    k0, p0, d0, d90 = vec("k_direction_0"), vec("p_direction_0"), vec("detector_direction_origin"), \
+        vec("detector_direction_positive_90")
+    om = np.asarray(op.angles_subdivided, np.float64).reshape(R * S)
+    eta = np.asarray(op.eta_angles_subdivided, np.float64).reshape(C * Se)
+    rot = Rotation.from_rotvec(om[:, None] * k0).as_matrix()
+    e = np.cos(eta)[:, None] * d0 + np.sin(eta)[:, None] * d90
+    turn = lambda a: np.einsum("oij,qi->oqj", rot, a).reshape(R, S, C, Se, 3)
+    out = {}
+    if "eta_offset" in groups:
+        out["eta_offset"] = turn(-np.sin(eta)[:, None] * d0 + np.cos(eta)[:, None] * d90)
+    if "axis_tilt" in groups:
+        u = turn(e)
+        w = np.einsum("oij,i->oj", rot, p0)
+        for i, ei in enumerate(perp_basis(k0)):
+            out[("axis_tilt", i)] = np.cross(ei, u) - turn(np.cross(ei[None, :], e))
+            out[("axis_tilt_w", i)] = np.cross(ei, w) - np.einsum("oij,i->oj", rot, np.cross(ei, p0))
+    return out
+
+
 def _f32_dev(a, dev):
     return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device=dev)
 
@@ -123,8 +148,6 @@ class PFGradient:
             raise NotImplementedError("PFGradient needs the (K, Ny, Nx) or the local coefficient layout")
         if int(op.N_peaks) > 16:
             raise NotImplementedError("PFGradient supports at most 16 rings")
-        if getattr(op, "reflection_two_theta", False):
-            raise NotImplementedError("PFGradient with reflection_two_theta is not provided")
         self.op = op
         self.hessian = bool(hessian)
         self.local_size = int(local_size)
@@ -146,6 +169,8 @@ class PFGradient:
         self.dv = {}
 
     def _dv(self, groups):
+        if getattr(self.op, "reflection_two_theta", False):
+            return self._dv_axis(groups)
         need = [g for g in ("eta_offset", "axis_tilt", "two_theta") if g in groups and g not in self.dv]
         if need:
             d = probed_derivatives(self.op, need)
@@ -160,7 +185,24 @@ class PFGradient:
         tilt = self.dv.get("axis_tilt", (None, None))
         return (ptr(self.dv.get("eta_offset") if "eta_offset" in groups else None),
                 ptr(tilt[0] if "axis_tilt" in groups else None), ptr(tilt[1] if "axis_tilt" in groups else None),
-                ptr(self.dv.get("two_theta") if "two_theta" in groups else None))
+                ptr(self.dv.get("two_theta") if "two_theta" in groups else None), None, None)
+
+    def _dv_axis(self, groups):
+        """reflection_two_theta: du / d eta, du and dw / d tilt (the Bragg angle's derivative is formed on the
+        device)."""
+        need = [g for g in ("eta_offset", "axis_tilt") if g in groups and g not in self.dv]
+        if need:
+            d = probed_parts_derivatives(self.op, need)
+            dev = self.op.device
+            if "eta_offset" in d:
+                self.dv["eta_offset"] = _f32_dev(d["eta_offset"], dev)
+            if ("axis_tilt", 0) in d:
+                self.dv["axis_tilt"] = tuple(_f32_dev(d[key], dev) for key in
+                                             (("axis_tilt", 0), ("axis_tilt", 1), ("axis_tilt_w", 0), ("axis_tilt_w", 1)))
+        ptr = lambda t: None if t is None else t.data_ptr()
+        tilt = self.dv.get("axis_tilt", (None,) * 4) if "axis_tilt" in groups else (None,) * 4
+        return (ptr(self.dv.get("eta_offset") if "eta_offset" in groups else None), ptr(tilt[0]), ptr(tilt[1]), None,
+                ptr(tilt[2]), ptr(tilt[3]))
 
     def __call__(self, c, r, groups=PF_GROUPS, curv=None):
         """c: coefficients (the operator's coeff_shape), r: dL/d data (N_Omega, My, N_seg) (NumPy arrays are
@@ -178,7 +220,7 @@ class PFGradient:
             if self.hessian:
                 cv = torch.ones(op.data_shape, dtype=torch.float32, device=op.device) if curv is None \
                     else _data_in(op, curv, "curv")
-            dv_eta, dv_t1, dv_t2, dv_tth = self._dv(groups)
+            dv_eta, dv_t1, dv_t2, dv_tth, dw_t1, dw_t2 = self._dv(groups)
             flags = (1 if "eta_offset" in groups else 0) | (2 if "axis_tilt" in groups else 0) | \
                 (4 if "two_theta" in groups else 0)
             R, My, nq, s = op.N_Omega, op.My, self.nq, op._s()
@@ -196,7 +238,8 @@ class PFGradient:
                 rp, col, _, _ = op._pf_batch(ib, False)
                 op._call("dfx_pf_param_vjp", ctypes.byref(op._pfg), rp.data_ptr(), col.data_ptr(), r.data_ptr(),
                          None if cv is None else cv.data_ptr(), op.coeffs_sino_C.data_ptr(), My, op.Kstride, k0, kb,
-                         flags, dv_eta, dv_t1, dv_t2, dv_tth, int(self.hessian), self.rows.data_ptr(), s)
+                         flags, dv_eta, dv_t1, dv_t2, dv_tth, dw_t1, dw_t2, int(self.hessian), self.rows.data_ptr(),
+                         s)
                 op._call("dfx_pf_rows_sum", self.rows.data_ptr(), R, kb, nq,
                          self.per_k.data_ptr() + 8 * k0 * nq, s)
             per_k = self.per_k.view(op.K, nq).cpu().numpy()

@@ -435,12 +435,14 @@ int dfx_poisson_term(const float *pred, const float *b, const float *w, int64_t 
  * upper triangle of
  * sum_y curv S^2 q q^T (10 floats after the width), q the derivative of the entry with respect to (rot, sigma).
  * flags: 1 eta offset, 2 axis tilt, 4 two-theta (each needs its probed directions' derivatives, coords-shaped).
+ * With reflection_two_theta (g->axis_w set; pf_grad.cl AXIS_THETA) dv_* are the derivatives of u, dw_t1 / dw_t2 those
+ * of w ((R * S, 3)) for the tilt, and the Bragg angle's derivative needs none (dv_tth unused).
  * At most 16 rings; my floats + 2 nq doubles of shared memory (<= 48 KB). */
 int dfx_pf_param_nq(int n_rings, int hess);
 int dfx_pf_param_vjp(const dfx_pf_geometry *g, const int32_t *row_ptr, const uint16_t *col_j, const float *res,
                      const float *curv, const float *sino, int my, int kstride, int k0, int kb, int flags,
-                     const float *dv_eta, const float *dv_t1, const float *dv_t2, const float *dv_tth, int hess,
-                     double *rows, void *stream);
+                     const float *dv_eta, const float *dv_t1, const float *dv_t2, const float *dv_tth,
+                     const float *dw_t1, const float *dw_t2, int hess, double *rows, void *stream);
 /* replaces rows_to_orientations (pf_grad.cl:179-187): out (kb, nq) = rows summed over the n_angles angles. */
 int dfx_pf_rows_sum(const double *rows, int n_angles, int kb, int nq, double *out, void *stream);
 

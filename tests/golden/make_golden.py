@@ -264,6 +264,9 @@ def axis_case(name="refl_windows"):
                axes=np.asarray(op.pole_axes_cpu, np.float64), counts=np.asarray(op.axis_count_cpu, np.float32),
                start=np.asarray(op.axis_start_cpu, np.int32), support=supp,
                pf=ref.pf(prm), fwd=ref.forward(c, prm), adj=ref.vjp(c, prm, r, groups=("c",))["c"])
+    grads = ref.vjp(c, prm, r, groups=("rot", "sigma", "eta_offset", "axis_tilt", "two_theta"))
+    out.update(g_rot=grads["rot"], g_sigma=grads["sigma"], g_eta_offset=np.float64(grads["eta_offset"]),
+               g_axis_tilt=grads["axis_tilt"], g_two_theta=grads["two_theta"])
     np.savez_compressed(OUT / f"{name}.npz", **out)
     print(f"{name}: K={op.K} R={op.N_Omega} C={op.N_eta} P={op.N_peaks} axes={op.N_axes}")
 

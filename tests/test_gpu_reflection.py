@@ -71,3 +71,17 @@ def test_modes_agree_adjoint_and_two_theta_update(golden):
     s0, s1 = sp.axis_start_cpu[0], sp.axis_start_cpu[1]
     assert np.allclose(moved[s0:s1], 0.002, atol=2e-9) and np.allclose(moved[s1:], 0.0, atol=2e-9)
     assert not np.array_equal(sp.direct(c), a)
+
+
+def test_pf_gradients_equal_reference(golden):
+    """PFGradient with reflection_two_theta against the reference model's float64 gradients, also with the
+    Gauss-Newton blocks: 3e-4 of the largest. The operator's probed directions u, w are float32: rounding them alone
+    moves the model's float64 width gradient of this case (3 deg kernels) by 1.0e-4 of the largest."""
+    from diffractom_b200.differentiable import PF_GROUPS, PFGradient
+    d = golden("refl_windows")
+    op = _op(d)
+    for hess in (False, True):
+        g = PFGradient(op, hessian=hess)(d["c"], d["r"], groups=PF_GROUPS)
+        for key in PF_GROUPS:
+            a, b = np.atleast_1d(g[key]), np.atleast_1d(d["g_" + key])
+            assert np.abs(a - b).max() <= 3e-4 * np.abs(b).max(), (hess, key)
