@@ -23,7 +23,9 @@ class PFGeometry(ctypes.Structure):
                 ("inv_sigma2", c_void_p), ("norm", c_void_p), ("quad_w", c_void_p), ("intens", c_void_p),
                 ("R", c_int32), ("C", c_int32), ("P", c_int32), ("A", c_int32), ("S", c_int32),
                 ("S_eta", c_int32), ("K", c_int32), ("cut", c_float),
-                ("axis_w", c_void_p), ("axis_sin", c_void_p), ("axis_cos", c_void_p)]
+                ("axis_w", c_void_p), ("axis_sin", c_void_p), ("axis_cos", c_void_p),
+                ("wp_pos", c_void_p), ("wp_cov", c_void_p), ("wp_b", c_void_p), ("wp_ax", c_void_p),
+                ("wp_ch", c_void_p), ("wp_invD", c_float), ("wp_eta", c_float)]
 
 
 P, I, L, F, S = c_void_p, c_int, c_int64, c_float, c_void_p   # pointer, int, int64, float, stream

@@ -96,4 +96,27 @@ __device__ __forceinline__ float tap_dweight(const AngleGeo &g, float d) {
     return fabsf(d) < 1.0f ? -copysignf(1.0f, d) : 0.0f;
 }
 
+// window_parallax: the fraction of axis a's radial profile inside channel p's window at angle r for orientation kg
+// (pf_generate.cl:103-121); the caller checks g.wp_ax != nullptr
+__device__ __forceinline__ float wp_fraction(const dfx_pf_geometry &g, int r, int kg, int p, int a)
+{
+    const float bx = __ldg(g.wp_b + 2 * r), by = __ldg(g.wp_b + 2 * r + 1);
+    const float qx = __ldg(g.wp_pos + 2 * kg), qy = __ldg(g.wp_pos + 2 * kg + 1);
+    const float cxx = __ldg(g.wp_cov + 4 * kg), cxy = __ldg(g.wp_cov + 4 * kg + 1), cyy = __ldg(g.wp_cov + 4 * kg + 2);
+    const float wx = qx * bx + qy * by;                               // mean depth along the beam
+    const float wvar = cxx * bx * bx + 2.0f * cxy * bx * by + cyy * by * by;
+    const float lo = __ldg(g.wp_ch + 2 * p), hi = __ldg(g.wp_ch + 2 * p + 1);
+    const float tt = __ldg(g.wp_ax + 4 * a), scs = __ldg(g.wp_ax + 4 * a + 1), s2 = __ldg(g.wp_ax + 4 * a + 2),
+                gam = __ldg(g.wp_ax + 4 * a + 3);
+    const float sh = tt - wx * g.wp_invD * scs;                       // the shifted two-theta
+    const float gg = scs * g.wp_invD;
+    const float is = rsqrtf(2.0f * (s2 + gg * gg * wvar));
+    const float zh = (hi - sh) * is, zl = (lo - sh) * is;             // erfc in the tails
+    float fr = zl > 0.0f ? 0.5f * (erfcf(zl) - erfcf(zh))
+                         : (zh < 0.0f ? 0.5f * (erfcf(-zh) - erfcf(-zl)) : 0.5f * (erff(zh) - erff(zl)));
+    if (g.wp_eta > 0.0f)
+        fr = (1.0f - g.wp_eta) * fr + g.wp_eta * (atanf((hi - sh) / gam) - atanf((lo - sh) / gam)) * 0.31830988618f;
+    return fr;
+}
+
 }  // namespace dfx

@@ -21,6 +21,9 @@ __device__ __forceinline__ float pf_entry(const dfx_pf_geometry &g, int r, int k
     const float inv = __ldg(g.inv_sigma2 + kg);
     float w_total = 0.0f;
     const bool axis_theta = g.axis_w != nullptr;
+    const bool wp = g.wp_ax != nullptr;
+    int wp_last = -1;                                  // window_parallax: the fraction depends on the axis only here
+    float wp_fr = 1.0f;
     for (int s = 0; s < g.S; ++s)
         for (int se = 0; se < g.S_eta; ++se) {
             const float *v = axis_theta
@@ -49,6 +52,13 @@ __device__ __forceinline__ float pf_entry(const dfx_pf_geometry &g, int r, int k
                 if (e1 < g.cut) t = __fadd_rn(t, expf(-e1));
                 const float e2 = __fmul_rn(__fadd_rn(1.0f, d), inv);
                 if (e2 < g.cut) t = __fadd_rn(t, expf(-e2));
+                if (wp && t > 0.0f) {
+                    if (a != wp_last) {
+                        wp_fr = wp_fraction(g, r, kg, p, a);
+                        wp_last = a;
+                    }
+                    t = __fmul_rn(t, wp_fr);
+                }
                 w_node = __fmaf_rn(__ldg(g.axis_count + a), t, w_node);
             }
             if (g.quad_w) w_total = __fmaf_rn(__ldg(g.quad_w + s * g.S_eta + se), w_node, w_total);
@@ -230,6 +240,7 @@ static int check_geometry(const dfx_pf_geometry *g)
                 "pf: bad geometry sizes");
     DFX_REQUIRE((g->axis_w == nullptr) == (g->axis_sin == nullptr) && (g->axis_w == nullptr) == (g->axis_cos == nullptr),
                 "pf: reflection_two_theta needs axis_w, axis_sin and axis_cos together");
+    DFX_REQUIRE(!g->wp_ax || (g->wp_pos && g->wp_cov && g->wp_b && g->wp_ch), "pf: incomplete window_parallax arrays");
     return DFX_OK;
 }
 

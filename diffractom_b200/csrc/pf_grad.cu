@@ -109,7 +109,9 @@ __global__ void __launch_bounds__(PG_THREADS) pf_param_vjp_kernel(
                     const float x1 = (float)((1.0 - add) * sinv), x2 = (float)((1.0 + add) * sinv);
                     const float e1 = x1 < g.cut ? expf(-x1) : 0.0f;
                     const float e2 = x2 < g.cut ? expf(-x2) : 0.0f;
-                    const float cw = w * g.axis_count[a];
+                    // window_parallax: the weight carries the window fraction (its own derivatives are not taken)
+                    const float cw = w * g.axis_count[a] * (g.wp_ax && (e1 != 0.0f || e2 != 0.0f)
+                                                                ? wp_fraction(g, r, kg, p, a) : 1.0f);
                     const float gd = cw * copysignf(sinv, D) * (e1 - e2);
                     dr0 = fmaf(gd, ny * vz - nz * vy, dr0);
                     dr1 = fmaf(gd, nz * vx - nx * vz, dr1);

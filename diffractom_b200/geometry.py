@@ -59,6 +59,16 @@ def axis_directions(omega_nodes, eta_nodes, n_omega, n_eta, cfg):
     return u, w
 
 
+def image_direction(lab_xy, omega):
+    """A lab-frame in-plane direction at rotation omega in image coordinates (col, row): turned into the sample frame
+    (R(omega)^T about the rotation axis z), then (x, y) -> (-x, y), normalised (differentiable/absorption.py:107-114)."""
+    c, s = np.cos(omega), np.sin(omega)
+    x, y = lab_xy[..., 0], lab_xy[..., 1]
+    xs, ys = c * x + s * y, -s * x + c * y
+    d = np.stack([-xs, ys], -1)
+    return d / np.linalg.norm(d, axis=-1, keepdims=True)
+
+
 @dataclass
 class PoleAxes:
     axes: np.ndarray        # (A, 3) float64 unit axes (crystal frame), rings one after the other

@@ -236,6 +236,25 @@ def split_regions(mats, sigmas, support: LocalSupport, mode: str = "components",
     return np.asarray(mats)[parent], np.asarray(sigmas)[parent], sup, parent
 
 
+def spatial_moments(k, iy, ix, v, K):
+    """Per orientation (K of them) the weighted mean (col, row) and covariance (col-col, col-row, row-row) of its
+    voxels (v: weights, default 1; local_forward_operator.py:77-92): the positions of the window_parallax option.
+    Orientations without weight get the origin and no spread."""
+    k = np.asarray(k, np.int64)
+    x, y = np.asarray(ix, np.float64), np.asarray(iy, np.float64)
+    w = np.ones(len(k)) if v is None else np.clip(np.asarray(v, np.float64), 0, None)
+    W = np.bincount(k, w, minlength=K)
+    Wn = np.maximum(W, 1e-300)
+    mx, my = np.bincount(k, w * x, minlength=K) / Wn, np.bincount(k, w * y, minlength=K) / Wn
+    dx, dy = x - mx[k], y - my[k]
+    cov = np.stack([np.bincount(k, w * dx * dx, minlength=K), np.bincount(k, w * dx * dy, minlength=K),
+                    np.bincount(k, w * dy * dy, minlength=K)], 1) / Wn[:, None]
+    pos = np.stack([mx, my], 1)
+    pos[W <= 0] = 0.0
+    cov[W <= 0] = 0.0
+    return pos, cov
+
+
 def _morton(y, x):
     """Z-order code of non-negative integer coordinates below 2^16 (bits of y and x interleaved)."""
     def spread(v):
@@ -317,6 +336,15 @@ class LocalSinglePhaseForwardOperator(SinglePhaseForwardOperator):
         self.n_patches = len(P["pk"])
         self._pf_chunk = pf_chunk
         inner = MatrixGrid(mats[self.orientation_index], sig[self.orientation_index])
+        if kwargs.get("window_parallax") is not None:            # positions in grid order -> operator order
+            wp = dict(kwargs["window_parallax"])
+            if wp.get("positions") is None:                      # default: the support's centroid and spread
+                wp["positions"], wp["covariances"] = spatial_moments(support.k, support.iy, support.ix, None,
+                                                                     self.K_basis)
+            pos = np.asarray(wp["positions"], np.float64).reshape(self.K_basis, 2)[self.orientation_index]
+            cov = (None if wp.get("covariances") is None else
+                   np.asarray(wp["covariances"], np.float64).reshape(self.K_basis, 3)[self.orientation_index])
+            kwargs["window_parallax"] = {**wp, "positions": pos, "covariances": cov}
         super().__init__(cfg, material, inner, max_gb, verbose=verbose, projector="native", **kwargs)
         self._setup_local()
 

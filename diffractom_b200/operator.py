@@ -90,8 +90,6 @@ class SinglePhaseForwardOperator:
         self.sparse_batch_max = int(sparse_batch_max)
         self.cfg = {**cfg, **kwargs}
         self.material, self.grid = material, grid
-        if window_parallax is not None:
-            raise NotImplementedError("window_parallax is not provided by this operator")
         if projector not in ("auto", "native", "fft", "gratopy"):
             raise ValueError(f"projector must be 'auto', 'native', 'fft' or 'gratopy', not {projector!r}")
         if projector == "gratopy":
@@ -138,6 +136,10 @@ class SinglePhaseForwardOperator:
             self.intens_gpu = None if self.normalized else dev(self.intens_cpu)
             self.geo_gpu = dev(self.radon_geo.geo)
             self._upload_axis_theta()
+            self.window_parallax = None
+            self._wp = None
+            if window_parallax is not None:
+                self.set_window_parallax(**dict(window_parallax), _build=False)
             self._pf_version = 0
             self._make_pfg()
             self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
@@ -190,7 +192,51 @@ class SinglePhaseForwardOperator:
             self.N_Omega, self.N_eta, self.N_peaks, self.N_axes, self.N_Omega_subdivisions, self.N_eta_subdivisions,
             self.K, float(self.pf_cut),
             *((None, None, None) if self.w_gpu is None else
-              (self.w_gpu.data_ptr(), self.axis_sin_gpu.data_ptr(), self.axis_cos_gpu.data_ptr())))
+              (self.w_gpu.data_ptr(), self.axis_sin_gpu.data_ptr(), self.axis_cos_gpu.data_ptr())),
+            *((None,) * 5 + (0.0, 0.0) if self._wp is None else
+              tuple(self._wp[k].data_ptr() for k in ("pos", "cov", "b", "ax", "ch")) + (self._wp["invD"],
+                                                                                      self._wp["eta"])))
+
+    def set_window_parallax(self, windows, sigma, distance, positions=None, covariances=None, lorentz=0.0,
+                            gamma=None, _build=True):
+        """Window fractions with sample parallax (SPFO:704-734, the window_parallax option): channels are
+        integration windows (windows (P, 2) two-theta limits, rad) that cut the reflections' radial profiles (width
+        sigma, rad: scalar, per channel or per pole axis), and an orientation's depth x along the beam shifts its
+        rings by -(x / distance) sin 2t cos 2t (distance in translation steps); positions (K, 2) / covariances
+        (K, 3): the orientations' mean (col, row) and spatial covariance in pixels (default the image centre, no
+        spread); lorentz, gamma: a pseudo-Voigt profile's Lorentzian share and half width (default sigma
+        sqrt(2 ln 2)). The sparse PF matrix is rebuilt (a call after construction)."""
+        from .geometry import image_direction
+        P, A, K = self.N_peaks, self.N_axes, self.K
+        win = np.asarray(windows, np.float64).reshape(P, 2)
+        st = np.asarray(self.axis_start_cpu)
+        ch = np.repeat(np.arange(P), np.diff(st))
+        tth = (np.asarray(self.axis_two_theta_built, np.float64) if self.reflection_two_theta
+               else np.asarray(self.two_theta_peaks, np.float64)[ch])
+        sig = np.asarray(sigma, np.float64)
+        sig_a = (np.broadcast_to(sig, (A,)) if sig.ndim == 0 or (sig.size == A and sig.size != P)
+                 else sig.reshape(P)[ch])
+        px = self.image_width / max(self.Nx, self.Ny)
+        cxy = np.array([(self.Nx - 1) / 2, (self.Ny - 1) / 2])
+        pos = np.zeros((K, 2)) if positions is None else (np.asarray(positions, np.float64).reshape(K, 2) - cxy) * px
+        cov = np.zeros((K, 3)) if covariances is None else np.asarray(covariances, np.float64).reshape(K, 3) * px ** 2
+        b = image_direction(np.asarray(self.cfg["p_direction_0"], np.float64)[:2], np.asarray(self.angles))
+        gam = (np.sqrt(2 * np.log(2)) * sig_a if gamma is None
+               else np.broadcast_to(np.asarray(gamma, np.float64), (A,)))
+        dev = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32).reshape(-1), device=self.device)
+        self.window_parallax = dict(windows=win, sigma=sig_a, distance=float(distance), positions=positions,
+                                    covariances=covariances, lorentz=float(lorentz), gamma=gamma)
+        self._wp = {"pos": dev(pos), "cov": dev(np.concatenate([cov, np.zeros((K, 1))], 1)), "b": dev(b),
+                    "ax": dev(np.stack([tth, np.sin(tth) * np.cos(tth), sig_a ** 2, gam], 1)), "ch": dev(win),
+                    "invD": float(np.float32(1.0 / float(distance))), "eta": float(np.float32(lorentz))}
+        self._make_pfg()
+        if _build:
+            self.release_omega_subsets()
+            self.build_sparse_pf(**self._pf_build)
+            if self.precision == "bf16":
+                self.pf_bf16 = None
+                self.build_dense_bf16_pf()
+            self._pf_version += 1
 
     def stream(self) -> torch.cuda.Stream:
         return self.queue if self.queue is not None else torch.cuda.current_stream(self.device)

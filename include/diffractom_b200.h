@@ -152,6 +152,16 @@ typedef struct dfx_pf_geometry {
     const float *axis_w;       /* (R * S, 3) the rotated p0 */
     const float *axis_sin;     /* (A) sin(theta_a) */
     const float *axis_cos;     /* (A) cos(theta_a) */
+    /* window_parallax (SPFO:704-734, pf_generate.cl:45-57, 103-121), wp_ax NULL otherwise: every axis's weight times
+     * the fraction of its radial profile inside its channel's window at the parallax-shifted angle, for the
+     * orientation's mean depth at this rotation angle (a Gaussian of variance sigma^2 + (sin 2t cos 2t / D)^2 var(x),
+     * optionally a pseudo-Voigt with Lorentzian share wp_eta). */
+    const float *wp_pos;       /* (K, 2) mean (col, row) position relative to the rotation axis, translation steps */
+    const float *wp_cov;       /* (K, 4) covariance (cc, cr, rr, 0), steps^2 */
+    const float *wp_b;         /* (R, 2) the beam direction in the image plane per angle */
+    const float *wp_ax;        /* (A, 4) (2 theta, sin 2t cos 2t, sigma^2, Lorentzian half width) per axis */
+    const float *wp_ch;        /* (P, 2) the windows' (lo, hi) two-theta */
+    float wp_invD, wp_eta;     /* 1 / sample-detector distance (steps), Lorentzian share */
 } dfx_pf_geometry;
 
 /* replaces pfmatrix_eval_poles + SCALE_PF_BY_INTENSITY_INPLACE (create_pfo_matrix.py:108-199, pf_kernels.cl:450-465;
