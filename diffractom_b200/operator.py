@@ -70,8 +70,8 @@ class SinglePhaseForwardOperator:
         float32). reflection_two_theta: every pole axis probes at its reflections' own Bragg angle (the windows of
         rings= then hold reflections of different angles; SPFO:236-244).
 
-        Not provided (NotImplementedError): projector "gratopy", the BF16 path with the Fourier-slice projector,
-        pf_mode "dense" (the sparse products give the same operator), window_parallax."""
+        pf_mode "dense" runs the sparse products (the same PF matrix, its zeros skipped). Not provided
+        (NotImplementedError): projector "gratopy", the BF16 path with the Fourier-slice projector."""
         lib = _lib.lib()                                    # fails loudly without the CUDA library
         if not torch.cuda.is_available():
             raise RuntimeError("SinglePhaseForwardOperator needs a CUDA device")
@@ -97,7 +97,10 @@ class SinglePhaseForwardOperator:
         if pf_mode not in ("dense", "sparse", "generated", "auto"):
             raise ValueError(f"pf_mode must be 'dense', 'sparse', 'generated' or 'auto', not {pf_mode!r}")
         if pf_mode == "dense":
-            raise NotImplementedError("pf_mode='dense' is not provided: 'sparse' applies the same matrix")
+            # the reference's dense mode applies the float32 PF matrix by GEMMs; the stored sparse matrix is the same
+            # operator (its zeros skipped), so "dense" runs the sparse products (SPFO:1207-1373)
+            warnings.warn("pf_mode='dense': the sparse products apply the same PF matrix and are used", stacklevel=2)
+            pf_mode = "sparse"
         # the native projector's geometry is made in any case (the Fourier-slice projector shares its conventions)
         geom_kernel = "trapezoid" if projector == "fft" or radon_kernel is None else radon_kernel
 

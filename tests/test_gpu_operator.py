@@ -234,3 +234,13 @@ def test_estimate_L_power_streamed(golden):
     assert estimate_L_power_streamed(op, niter=40, verbose=0, parallel_start=False) == L
     Lp = estimate_L_power_streamed(op, niter=40, verbose=0)
     assert abs(Lp / L - 1) < 1e-2
+
+
+def test_dense_pf_mode_runs_the_sparse_products(golden):
+    """pf_mode="dense" (the reference's GEMM path) applies the same PF matrix: it runs the sparse products."""
+    d = golden("diff_auto_trapezoid")
+    with pytest.warns(UserWarning, match="dense"):
+        dense = make_operator(d, pf_mode="dense")
+    sparse = make_operator(d, pf_mode="sparse")
+    assert dense.pf_mode == "sparse"
+    assert np.array_equal(dense.direct(d["c"]), sparse.direct(d["c"]))
