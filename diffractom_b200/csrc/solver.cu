@@ -220,6 +220,62 @@ __global__ void __launch_bounds__(RED_THREADS) tv_value_kernel(const float *__re
     block_sum<1>(v, part + blockIdx.x);
 }
 
+// ---- the TV block on a local basis's flat coefficients (spdhg_poisson.py:188-230): the differences to the right and
+// down neighbours within a coefficient's patch (index arrays, -1: none); the same arithmetic as the dense kernels
+__global__ void tv_dual_local_kernel(const float *__restrict__ x, const float *__restrict__ T, float *__restrict__ qx,
+                                     float *__restrict__ qy, float *__restrict__ dqx, float *__restrict__ dqy,
+                                     const int32_t *__restrict__ right, const int32_t *__restrict__ down, float lam,
+                                     float ps, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int r = right[i], d = down[i];
+        const bool vr0 = r >= 0, vd0 = d >= 0;
+        const float ox = qx[i], oy = qy[i];
+        float nxv, nyv;
+        tv_dual_core(T[i], vr0 ? T[r] : 0.0f, vd0 ? T[d] : 0.0f, vr0, vd0, x[i], vr0 ? x[r] : 0.0f,
+                     vd0 ? x[d] : 0.0f, ox, oy, lam, ps, nxv, nyv);
+        qx[i] = nxv;
+        qy[i] = nyv;
+        dqx[i] = __fsub_rn(nxv, ox);
+        dqy[i] = __fsub_rn(nyv, oy);
+    }
+}
+
+__global__ void tv_adjoint_update_local_kernel(const float *__restrict__ dqx, const float *__restrict__ dqy,
+                                               float *__restrict__ x, float *__restrict__ z,
+                                               const float *__restrict__ T, const int32_t *__restrict__ left,
+                                               const int32_t *__restrict__ up, float inv_p, float lam, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float v = __fsub_rn(-dqx[i], dqy[i]);
+        const int l = left[i], u = up[i];
+        if (l >= 0) v = __fadd_rn(v, dqx[l]);
+        if (u >= 0) v = __fadd_rn(v, dqy[u]);
+        const float zi = __fadd_rn(z[i], v);
+        z[i] = zi;
+        const float zb = __fadd_rn(zi, __fmul_rn(inv_p, v));
+        const float t = T[i];
+        x[i] = t > 0.0f ? fmaxf(0.0f, __fsub_rn(x[i], __fmul_rn(t, __fadd_rn(zb, lam)))) : 0.0f;
+    }
+}
+
+__global__ void __launch_bounds__(RED_THREADS) tv_value_local_kernel(const float *__restrict__ x,
+                                                                     const float *__restrict__ T,
+                                                                     const int32_t *__restrict__ right,
+                                                                     const int32_t *__restrict__ down, int64_t n,
+                                                                     double *__restrict__ part)
+{
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int r = right[i], d = down[i];
+        const float tj = T[i];
+        const float gx = (r >= 0 && tj > 0.0f && T[r] > 0.0f) ? __fsub_rn(x[r], x[i]) : 0.0f;
+        const float gy = (d >= 0 && tj > 0.0f && T[d] > 0.0f) ? __fsub_rn(x[d], x[i]) : 0.0f;
+        v[0] += (double)__fsqrt_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)));
+    }
+    block_sum<1>(v, part + blockIdx.x);
+}
+
 // ---- OSEM's multiplicative update (optimization/osem_poisson.py:80-84): x = outside ? 0 : (s > 0 ? x back / (s + lam)
 // : x), the support mask periodic with period pm (0: none)
 __global__ void osem_update_kernel(float *__restrict__ x, const float *__restrict__ back,
@@ -644,6 +700,39 @@ extern "C" int dfx_tv_value(const float *x, const float *T, int nx, int ny, int 
     cudaStream_t s = (cudaStream_t)stream;
     tv_value_kernel<<<nb, RED_THREADS, 0, s>>>(x, T, nx, ny, kstride, n, (double *)scratch);
     st = launch_status("tv_value");
+    if (st) return st;
+    finish_sums<1><<<1, RED_THREADS, 0, s>>>((const double *)scratch, nb, out);
+    return launch_status("finish_sums");
+}
+
+extern "C" int dfx_tv_dual_local(const float *x, const float *T, float *qx, float *qy, float *dqx, float *dqy,
+                                 const int32_t *right, const int32_t *down, float lam, float ps, int64_t n,
+                                 void *stream)
+{
+    DFX_REQUIRE(x && T && qx && qy && dqx && dqy && right && down && n >= 0, "tv_dual_local: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(tv_dual_local_kernel, n, stream, x, T, qx, qy, dqx, dqy, right, down, lam, ps, n);
+}
+
+extern "C" int dfx_tv_adjoint_update_local(const float *dqx, const float *dqy, float *x, float *z, const float *T,
+                                           const int32_t *left, const int32_t *up, float inv_p, float lam, int64_t n,
+                                           void *stream)
+{
+    DFX_REQUIRE(dqx && dqy && x && z && T && left && up && n >= 0, "tv_adjoint_update_local: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(tv_adjoint_update_local_kernel, n, stream, dqx, dqy, x, z, T, left, up, inv_p, lam, n);
+}
+
+extern "C" int dfx_tv_value_local(const float *x, const float *T, const int32_t *right, const int32_t *down,
+                                  int64_t n, double *out, void *scratch, size_t scratch_bytes, void *stream)
+{
+    DFX_REQUIRE(x && T && right && down && out && n > 0, "tv_value_local: bad arguments");
+    int st = check_scratch(scratch, scratch_bytes, n, 1);
+    if (st) return st;
+    const int nb = red_blocks(n);
+    cudaStream_t s = (cudaStream_t)stream;
+    tv_value_local_kernel<<<nb, RED_THREADS, 0, s>>>(x, T, right, down, n, (double *)scratch);
+    st = launch_status("tv_value_local");
     if (st) return st;
     finish_sums<1><<<1, RED_THREADS, 0, s>>>((const double *)scratch, nb, out);
     return launch_status("finish_sums");

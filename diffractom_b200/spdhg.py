@@ -82,8 +82,8 @@ class SPDHGPoisson:
             if tv <= 0:
                 raise ValueError("tv_tree needs tv > 0")
             raise NotImplementedError("the hierarchical total variation (tv_tree) is not provided")
-        if tv > 0 and (shards is not None or getattr(operator, "coefficient_layout", "dense") != "dense"):
-            raise NotImplementedError("the total-variation block needs the (K, Ny, Nx) layout on one device")
+        if tv > 0 and shards is not None:
+            raise NotImplementedError("the total-variation block needs all orientations on one device")
         self.op = operator
         self.ctx, self.queue = operator.ctx, operator.queue
         self.subsets = operator.set_omega_subsets(subsets)
@@ -338,7 +338,17 @@ class SPDHGPoisson:
             _lib.call("dfx_tmin", T.data_ptr(), dz.data_ptr(), None, 0, c, n, s)
         _lib.call("dfx_tfinal", T.data_ptr(), n, s)
         _lib.call("dfx_project_support", x.data_ptr(), None, 0, n, s)
-        self.resident_used = NAMES
+        self.resident_used = self._names
+        tvq = None
+        if self.tv > 0:                 # the TV dual, its change, the patches' neighbour indices (spdhg_poisson.py:814-826)
+            f32 = lambda: torch.zeros(n, dtype=torch.float32, device=dev)
+            tvq = dict(qx=f32(), qy=f32(), dqx=f32(), dqy=f32(),
+                       nbr=[torch.as_tensor(a, device=dev) for a in _patch_neighbours(op)])
+            for nm in ("qx", "qy"):
+                if state is not None and state.get(nm) is not None:
+                    tvq[nm].copy_(torch.as_tensor(as_host(state[nm], cshape, f"state['{nm}']")))
+        if state is not None and self.tv > 0 and state.get("z") is None:
+            raise ValueError("continuing a TV run needs the state's z")
         if state is not None:
             host_copier().to_device(as_host(state["y"], dshape, "state['y']"), self.y)
             if state.get("z") is not None:
@@ -351,17 +361,27 @@ class SPDHGPoisson:
         self.iter_stats = []
         f = float("nan")
         seq = self._epoch_sequence()
-        op.direct_cl(x, self.D, subset=seq[0])
+        if seq[0] >= 0:
+            op.direct_cl(x, self.D, subset=seq[0])
         for e in range(int(n_epochs)):
             ep = ep0 + e + 1
             last = e + 1 == n_epochs
             want_f = (e + 1) % max(1, diagnostics_interval) == 0 or last
             nseq = None
             for j, m in enumerate(seq):
-                self._dual(m)
-                op.adjoint_cl(self.D, dz, subset=m)
-                _lib.call("dfx_spdhg_primal_update", x.data_ptr(), z.data_ptr(), T.data_ptr(), dz.data_ptr(),
-                          inv_p, self.lam, n, s)
+                if m >= 0:
+                    self._dual(m)
+                    op.adjoint_cl(self.D, dz, subset=m)
+                    _lib.call("dfx_spdhg_primal_update", x.data_ptr(), z.data_ptr(), T.data_ptr(), dz.data_ptr(),
+                              inv_p, self.lam, n, s)
+                else:                                        # the TV block
+                    nb_ = tvq["nbr"]
+                    _lib.call("dfx_tv_dual_local", x.data_ptr(), T.data_ptr(), tvq["qx"].data_ptr(),
+                              tvq["qy"].data_ptr(), tvq["dqx"].data_ptr(), tvq["dqy"].data_ptr(), nb_[0].data_ptr(),
+                              nb_[1].data_ptr(), float(self.tv), float(TV_SAFETY * self.tv_prob), n, s)
+                    _lib.call("dfx_tv_adjoint_update_local", tvq["dqx"].data_ptr(), tvq["dqy"].data_ptr(),
+                              x.data_ptr(), z.data_ptr(), T.data_ptr(), nb_[2].data_ptr(), nb_[3].data_ptr(),
+                              float(1.0 / self.tv_prob), self.lam, n, s)
                 end_of_epoch = j + 1 == len(seq)
                 if not end_of_epoch:
                     nb = seq[j + 1]
@@ -370,11 +390,20 @@ class SPDHGPoisson:
                     nb = nseq[0]
                 else:
                     nb = None
+                m_next = nb if nb is not None and nb >= 0 else None
                 if end_of_epoch and want_f:
                     op.direct_cl(x, self.D)                  # every row (the next subset's among them)
                     f = self._deviance(self.D)
-                elif nb is not None:
-                    op.direct_cl(x, self.D, subset=nb)
+                    if self.tv > 0:
+                        nb_ = tvq["nbr"]
+                        tvs = torch.zeros(1, dtype=torch.float64, device=dev)
+                        nbytes = op._lib.dfx_reduce_scratch_bytes(n)
+                        scr = op.scratch(nbytes)
+                        _lib.call("dfx_tv_value_local", x.data_ptr(), T.data_ptr(), nb_[0].data_ptr(),
+                                  nb_[1].data_ptr(), n, tvs.data_ptr(), scr.data_ptr(), nbytes, s)
+                        f += self.tv * float(tvs.item())
+                elif m_next is not None:
+                    op.direct_cl(x, self.D, subset=m_next)
             if nseq is not None:
                 seq = nseq
             if callback is not None or verbose:
@@ -395,10 +424,12 @@ class SPDHGPoisson:
         host_copier().to_host(z, z_host)
         host_copier().to_host(self.y, y_host)
         self.state = {"epoch": ep0 + len(self.iter_stats), "z": z_host, "y": y_host}
+        if tvq is not None:
+            self.state.update(qx=tvq["qx"].cpu().numpy(), qy=tvq["qy"].cpu().numpy())
         self.final_stats = {"epochs": len(self.iter_stats), "final_f": f, "setup_s": t_setup, "rho": self.rho_used,
                             "subsets": self.M, "resident": self.resident_used,
-                            "time": time.perf_counter() - t_start, "tv": 0.0, "tv_prob": 0.0, "graph_replays": 0,
-                            **self.scales}
+                            "time": time.perf_counter() - t_start, "tv": self.tv, "tv_prob": self.tv_prob,
+                            "graph_replays": 0, **self.scales}
         if not x_on_gpu:
             host_copier().to_host(x, host_x)
         self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = None
@@ -696,3 +727,21 @@ class SPDHGPoisson:
 
 def _ptr(t):
     return None if t is None else t.data_ptr()
+
+
+def _patch_neighbours(op):
+    """(right, down, left, up) int32 indices of every flat coefficient's neighbour within its patch (a row-major
+    h x w box at coff), -1 at the box edges (spdhg_poisson.py:981-999)."""
+    P = op._patches
+    coff = np.asarray(P["coff"], np.int64)
+    h, w = np.asarray(P["h"], np.int64), np.asarray(P["w"], np.int64)
+    sizes = h * w
+    nc = int(op.n_coef)
+    if not (np.array_equal(coff, np.r_[0, np.cumsum(sizes)[:-1]]) and int(sizes.sum()) == nc):
+        raise RuntimeError("the local operator's patches are not stored contiguously")
+    j = np.arange(nc, dtype=np.int64)
+    loc = j - np.repeat(coff, sizes)
+    ww, hh = np.repeat(w, sizes), np.repeat(h, sizes)
+    r, c = loc // ww, loc % ww
+    return [a.astype(np.int32) for a in (np.where(c < ww - 1, j + 1, -1), np.where(r < hh - 1, j + ww, -1),
+                                         np.where(c > 0, j - 1, -1), np.where(r > 0, j - ww, -1))]

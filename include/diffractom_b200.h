@@ -413,6 +413,17 @@ int dfx_tv_adjoint_update(const float *dqx, const float *dqy, float *x, float *z
 int dfx_tv_value(const float *x, const float *T, int nx, int ny, int kstride, double *out, void *scratch,
                  size_t scratch_bytes, void *stream);
 
+/* replaces tv_dual_local / tv_adjoint_local + spdhg_update / tv_value_local (spdhg_poisson.py:188-230): the TV block
+ * on a local basis's n flat coefficients, the differences to the right / down neighbours within each patch (index
+ * arrays right, down, left, up; -1: none), the arithmetic of dfx_tv_dual / dfx_tv_adjoint_update / dfx_tv_value. */
+int dfx_tv_dual_local(const float *x, const float *T, float *qx, float *qy, float *dqx, float *dqy,
+                      const int32_t *right, const int32_t *down, float lam, float ps, int64_t n, void *stream);
+int dfx_tv_adjoint_update_local(const float *dqx, const float *dqy, float *x, float *z, const float *T,
+                                const int32_t *left, const int32_t *up, float inv_p, float lam, int64_t n,
+                                void *stream);
+int dfx_tv_value_local(const float *x, const float *T, const int32_t *right, const int32_t *down, int64_t n,
+                       double *out, void *scratch, size_t scratch_bytes, void *stream);
+
 /* replaces osem_update (optimization/osem_poisson.py:80-84): x = outside the support (mask periodic with period pm,
  * 0: no mask) ? 0 : (sens > 0 ? x back / (sens + lam) : x). */
 int dfx_osem_update(float *x, const float *back, const float *sens, const uint8_t *mask, int64_t pm, float lam,

@@ -114,3 +114,26 @@ def test_spdhg_tv_streamed_equals_resident_and_resumes(golden, precision):
     assert np.isfinite(xc).all() and c.state["epoch"] == 3
     with pytest.raises(ValueError):
         SPDHGPoisson(op, **kw).run(np.zeros(op.coeff_shape, np.float32), b, 1, state={"y": a.state["y"], "epoch": 1})
+
+
+def test_local_basis_tv_equals_dense_tv(golden):
+    """The TV block on a local basis (neighbours within the patches) with every orientation allowed in the whole field
+    of view takes the dense TV run's steps bit for bit; the objective with tv TV(x) agrees to float64 rounding."""
+    from diffractom_b200 import SPDHGPoisson
+    from test_gpu_local import _everywhere_pair
+    loc, inner, oi = _everywhere_pair(golden)
+    rng = np.random.default_rng(8)
+    x0 = rng.random((loc.K_basis, loc.Ny, loc.Nx)).astype(np.float32)
+    mu = inner.direct(torch.as_tensor(x0[oi], device="cuda")).cpu().numpy()
+    b = rng.poisson(np.maximum(mu, 0) * 3 + 0.5).astype(np.float32)
+    xs = np.full((loc.K_basis, loc.Ny, loc.Nx), 0.5, np.float32)
+    kw = dict(subsets=3, seed=2, tv=0.05)
+    sl = SPDHGPoisson(loc, **kw)
+    xl = sl.run(torch.as_tensor(loc.from_dense(xs), device="cuda"), b, 3)
+    sd = SPDHGPoisson(inner, **kw)
+    xd = sd.run(torch.as_tensor(xs[oi], device="cuda"), b, 3)
+    assert np.array_equal(loc.to_dense(xl)[oi], xd.cpu().numpy())
+    assert np.array_equal(sl.state["y"], sd.state["y"])
+    np.testing.assert_allclose([s["f"] for s in sl.iter_stats], [s["f"] for s in sd.iter_stats], rtol=1e-12)
+    fov = inner.support_mask()
+    assert np.array_equal(loc.to_dense(sl.state["qx"])[oi][:, fov], sd.state["qx"][:, fov])
