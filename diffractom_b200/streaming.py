@@ -276,7 +276,8 @@ class KMajorStaging:
 # the CPU copies of others, which run on a few threads (NumPy's copy releases the GIL).
 
 _COPY_CHUNK = 64 << 20          # bytes per pinned chunk
-_COPY_BUFS = 4                  # pinned chunks in flight = host threads
+_COPY_BUFS = 16                 # pinned chunks in flight = host threads: on a 16-core B200 host, 4 -> 16 threads took
+                                # downloads into fresh (page-faulting) NumPy memory from 14 to 34 GB/s (warm 39 -> 51)
 
 
 class HostCopier:
