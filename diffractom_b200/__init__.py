@@ -7,10 +7,11 @@ Device arrays are CUDA torch tensors (float32, contiguous) in place of pyopencl 
 where diffractom accepts them. The CUDA library is built in-tree by `python -m diffractom_b200.build`.
 """
 from .grid import Grid, MatrixGrid
+from .orientation_tree import OrientationTree
 from .material import Material, group_reflections_into_rings
 from .quadrature import QuadratureRule
 
-__all__ = ["Grid", "MatrixGrid", "Material", "QuadratureRule", "group_reflections_into_rings",
+__all__ = ["Grid", "MatrixGrid", "Material", "QuadratureRule", "group_reflections_into_rings", "OrientationTree",
            "SinglePhaseForwardOperator", "SPDHGPoisson", "FISTAPoisson", "FISTAHuber", "FISTAL2", "OSEMPoisson",
            "PDHGPoisson", "estimate_L_power", "estimate_L_power_streamed",
            "forward_operator"]

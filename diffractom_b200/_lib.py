@@ -84,6 +84,9 @@ SIGNATURES = {
     "dfx_tv_dual_local": ([P, P, P, P, P, P, P, P, F, F, L, S], c_int),
     "dfx_tv_adjoint_update_local": ([P, P, P, P, P, P, P, F, F, L, S], c_int),
     "dfx_tv_value_local": ([P, P, P, P, L, P, P, c_size_t, S], c_int),
+    "dfx_tv_adjoint_local": ([P, P, P, P, P, L, S], c_int),
+    "dfx_tree_sums": ([P, P, P, P, L, S], c_int),
+    "dfx_tree_scatter": ([P, P, P, L, S], c_int),
     "dfx_pdhg_dual_update": ([P, P, P, P, P, L, P, L, P, L, F, L, S], c_int),
     "dfx_pdhg_primal_update": ([P, P, P, P, F, L, S], c_int),
     "dfx_pdhg_average": ([P, P, L, S], c_int),

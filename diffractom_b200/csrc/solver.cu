@@ -241,16 +241,25 @@ __global__ void tv_dual_local_kernel(const float *__restrict__ x, const float *_
     }
 }
 
+// (D^T dq)_i within the patches: -dqx_i - dqy_i + dqx_left + dqy_up
+__device__ __forceinline__ float tv_adjoint_local_at(const float *__restrict__ dqx, const float *__restrict__ dqy,
+                                                     const int32_t *__restrict__ left, const int32_t *__restrict__ up,
+                                                     int64_t i)
+{
+    float v = __fsub_rn(-dqx[i], dqy[i]);
+    const int l = left[i], u = up[i];
+    if (l >= 0) v = __fadd_rn(v, dqx[l]);
+    if (u >= 0) v = __fadd_rn(v, dqy[u]);
+    return v;
+}
+
 __global__ void tv_adjoint_update_local_kernel(const float *__restrict__ dqx, const float *__restrict__ dqy,
                                                float *__restrict__ x, float *__restrict__ z,
                                                const float *__restrict__ T, const int32_t *__restrict__ left,
                                                const int32_t *__restrict__ up, float inv_p, float lam, int64_t n)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        float v = __fsub_rn(-dqx[i], dqy[i]);
-        const int l = left[i], u = up[i];
-        if (l >= 0) v = __fadd_rn(v, dqx[l]);
-        if (u >= 0) v = __fadd_rn(v, dqy[u]);
+        const float v = tv_adjoint_local_at(dqx, dqy, left, up, i);
         const float zi = __fadd_rn(z[i], v);
         z[i] = zi;
         const float zb = __fadd_rn(zi, __fmul_rn(inv_p, v));
@@ -274,6 +283,37 @@ __global__ void __launch_bounds__(RED_THREADS) tv_value_local_kernel(const float
         v[0] += (double)__fsqrt_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)));
     }
     block_sum<1>(v, part + blockIdx.x);
+}
+
+// ---- the hierarchical total variation on a local basis (spdhg_poisson.py:232-249): the node-pixels of a level of the
+// orientation tree (a cell of orientations in one pixel), their sums s over the cell's coefficients (CSR ptr / idx
+// into the flat coefficients, float32 in the list's order), D^T dq on the node-pixels, and its scatter back onto the
+// coefficients (map: a coefficient's node-pixel, -1: none)
+__global__ void tree_sums_kernel(const float *__restrict__ x, const int32_t *__restrict__ ptr,
+                                 const int32_t *__restrict__ idx, float *__restrict__ s, int64_t n)
+{
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        float a = 0.0f;
+        for (int p = ptr[j], e = ptr[j + 1]; p < e; ++p) a = __fadd_rn(a, x[idx[p]]);
+        s[j] = a;
+    }
+}
+
+__global__ void tv_adjoint_local_kernel(const float *__restrict__ dqx, const float *__restrict__ dqy,
+                                        float *__restrict__ w, const int32_t *__restrict__ left,
+                                        const int32_t *__restrict__ up, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        w[i] = tv_adjoint_local_at(dqx, dqy, left, up, i);
+}
+
+__global__ void tree_scatter_kernel(const float *__restrict__ w, const int32_t *__restrict__ map,
+                                    float *__restrict__ dz, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int m = map[i];
+        if (m >= 0) dz[i] = __fadd_rn(dz[i], w[m]);
+    }
 }
 
 // ---- OSEM's multiplicative update (optimization/osem_poisson.py:80-84): x = outside ? 0 : (s > 0 ? x back / (s + lam)
@@ -721,6 +761,29 @@ extern "C" int dfx_tv_adjoint_update_local(const float *dqx, const float *dqy, f
     DFX_REQUIRE(dqx && dqy && x && z && T && left && up && n >= 0, "tv_adjoint_update_local: bad arguments");
     if (n == 0) return DFX_OK;
     EW_LAUNCH(tv_adjoint_update_local_kernel, n, stream, dqx, dqy, x, z, T, left, up, inv_p, lam, n);
+}
+
+extern "C" int dfx_tv_adjoint_local(const float *dqx, const float *dqy, float *w, const int32_t *left,
+                                    const int32_t *up, int64_t n, void *stream)
+{
+    DFX_REQUIRE(dqx && dqy && w && left && up && n >= 0, "tv_adjoint_local: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(tv_adjoint_local_kernel, n, stream, dqx, dqy, w, left, up, n);
+}
+
+extern "C" int dfx_tree_sums(const float *x, const int32_t *ptr, const int32_t *idx, float *s, int64_t n,
+                             void *stream)
+{
+    DFX_REQUIRE(x && ptr && idx && s && n >= 0, "tree_sums: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(tree_sums_kernel, n, stream, x, ptr, idx, s, n);
+}
+
+extern "C" int dfx_tree_scatter(const float *w, const int32_t *map, float *dz, int64_t n, void *stream)
+{
+    DFX_REQUIRE(w && map && dz && n >= 0, "tree_scatter: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(tree_scatter_kernel, n, stream, w, map, dz, n);
 }
 
 extern "C" int dfx_tv_value_local(const float *x, const float *T, const int32_t *right, const int32_t *down,

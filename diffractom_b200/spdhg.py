@@ -32,6 +32,7 @@ import torch
 from . import _lib
 from .arrays import as_host, check_device, is_device, on_op_stream
 from .solvers import Reducer, as_device_data, periodic, support_mask_to_device
+from .orientation_tree import tree_level_arrays
 from .streaming import BatchPipeline, CoeffArray, KMajorStaging, host_copier
 
 RHO_AUTO = 3e4
@@ -67,7 +68,10 @@ class SPDHGPoisson:
         the others are streamed from pinned host memory (a CUDA x0 keeps all three on the device). tv > 0: the total
         variation of every orientation's image as one more block of the serial sampling, chosen with probability
         tv_prob (default 1 / (M + 1)); its dual (qx, qy) is two more coefficient arrays, resident or streamed as x, z,
-        T (spdhg_poisson.py:20-40, 320-324); not with the local basis, the hierarchical tv_tree or shards. shards
+        T (spdhg_poisson.py:20-40, 320-324); not with shards. tv_tree (an orientation_tree.OrientationTree over the basis's
+        orientations in the grid's order; local basis only): the hierarchical total variation of its nested cells, the leaf
+        level with weight tv leaf_edge and every penalised level with tv edge, their dual steps sharing the TV
+        block's (spdhg_poisson.py:322-326, 819-862). shards
         (this package's extension; a sharding.ShardSum): the operator holds one orientation shard of a process
         group, and the forward's data rows are summed over the shards after each pass; every rank passes the same
         seed and subsets."""
@@ -78,10 +82,8 @@ class SPDHGPoisson:
         tv = float(tv)
         if tv < 0:
             raise ValueError("tv must be >= 0")
-        if tv_tree is not None:
-            if tv <= 0:
-                raise ValueError("tv_tree needs tv > 0")
-            raise NotImplementedError("the hierarchical total variation (tv_tree) is not provided")
+        if tv_tree is not None and tv <= 0:
+            raise ValueError("tv_tree needs tv > 0")
         if tv > 0 and shards is not None:
             raise NotImplementedError("the total-variation block needs all orientations on one device")
         self.op = operator
@@ -94,6 +96,7 @@ class SPDHGPoisson:
         self.rng = np.random.default_rng(seed)
         self.resident = resident
         self.tv = tv
+        self.tv_tree = tv_tree
         self.tv_prob = (1.0 / (self.M + 1) if tv_prob is None else float(tv_prob)) if tv > 0 else 0.0
         if tv > 0 and not 0 < self.tv_prob < 1:
             raise ValueError("tv_prob must be in (0, 1)")
@@ -269,6 +272,8 @@ class SPDHGPoisson:
         if getattr(self.op, "coefficient_layout", "dense") == "local":
             return self._run_local(x0, b, n_epochs, weights, gain, background, verbose, diagnostics_interval,
                                    callback, state)
+        if self.tv_tree is not None:
+            raise NotImplementedError("tv_tree needs an operator with the local coefficient layout")
         self._setup(x0, b, weights, gain, background, state)
         self._iterate(n_epochs, verbose, diagnostics_interval, callback)
         return self._finish()
@@ -347,6 +352,34 @@ class SPDHGPoisson:
             for nm in ("qx", "qy"):
                 if state is not None and state.get(nm) is not None:
                     tvq[nm].copy_(torch.as_tensor(as_host(state[nm], cshape, f"state['{nm}']")))
+            # the tree's levels: node-pixel arrays, their duals and scratch (spdhg_poisson.py:819-826, 946-978)
+            tvq["levels"] = []
+            tvq["leaf_edge"] = float(self.tv_tree.leaf_edge) if self.tv_tree is not None else 1.0
+            if self.tv_tree is not None:
+                if int(self.tv_tree.K) != int(op.K_basis):
+                    raise ValueError(f"tv_tree must cover the basis's {op.K_basis} orientations (in the grid's "
+                                     f"order), not {self.tv_tree.K}")
+                k_, iy_, ix_, pi_ = op._pairs()
+                host_levels = tree_level_arrays(k_, iy_, ix_, pi_, int(op.Ny), int(op.Nx), n, T.cpu().numpy(),
+                                                self.tv_tree)
+                saved = list(state.get("tree_q") or []) if state is not None else []
+                for li, hl in enumerate(host_levels):
+                    lev = {nm: torch.as_tensor(hl[nm], device=dev)
+                           for nm in ("ptr", "idx", "map", "right", "down", "left", "up", "A")}
+                    lev.update(n=hl["n"], edge=hl["edge"],
+                               qx=torch.zeros(hl["n"], dtype=torch.float32, device=dev),
+                               qy=torch.zeros(hl["n"], dtype=torch.float32, device=dev))
+                    if li < len(saved):
+                        lev["qx"].copy_(torch.as_tensor(as_host(saved[li][0], (hl["n"],), "state['tree_q']")))
+                        lev["qy"].copy_(torch.as_tensor(as_host(saved[li][1], (hl["n"],), "state['tree_q']")))
+                    tvq["levels"].append(lev)
+                if tvq["levels"]:
+                    nmax = max(lev["n"] for lev in tvq["levels"])
+                    tvq["scr"] = {nm: torch.empty(nmax, dtype=torch.float32, device=dev)
+                                  for nm in ("s", "w", "dqx", "dqy")}
+            # the leaf level's weight and the dual step shared among the levels
+            tvq["lam"] = float(self.tv * tvq["leaf_edge"])
+            tvq["ps"] = float(TV_SAFETY * self.tv_prob / (1 + len(tvq["levels"])))
         if state is not None and self.tv > 0 and state.get("z") is None:
             raise ValueError("continuing a TV run needs the state's z")
         if state is not None:
@@ -375,13 +408,7 @@ class SPDHGPoisson:
                     _lib.call("dfx_spdhg_primal_update", x.data_ptr(), z.data_ptr(), T.data_ptr(), dz.data_ptr(),
                               inv_p, self.lam, n, s)
                 else:                                        # the TV block
-                    nb_ = tvq["nbr"]
-                    _lib.call("dfx_tv_dual_local", x.data_ptr(), T.data_ptr(), tvq["qx"].data_ptr(),
-                              tvq["qy"].data_ptr(), tvq["dqx"].data_ptr(), tvq["dqy"].data_ptr(), nb_[0].data_ptr(),
-                              nb_[1].data_ptr(), float(self.tv), float(TV_SAFETY * self.tv_prob), n, s)
-                    _lib.call("dfx_tv_adjoint_update_local", tvq["dqx"].data_ptr(), tvq["dqy"].data_ptr(),
-                              x.data_ptr(), z.data_ptr(), T.data_ptr(), nb_[2].data_ptr(), nb_[3].data_ptr(),
-                              float(1.0 / self.tv_prob), self.lam, n, s)
+                    self._tv_block_local(tvq, x, z, T, dz, n, s)
                 end_of_epoch = j + 1 == len(seq)
                 if not end_of_epoch:
                     nb = seq[j + 1]
@@ -395,13 +422,7 @@ class SPDHGPoisson:
                     op.direct_cl(x, self.D)                  # every row (the next subset's among them)
                     f = self._deviance(self.D)
                     if self.tv > 0:
-                        nb_ = tvq["nbr"]
-                        tvs = torch.zeros(1, dtype=torch.float64, device=dev)
-                        nbytes = op._lib.dfx_reduce_scratch_bytes(n)
-                        scr = op.scratch(nbytes)
-                        _lib.call("dfx_tv_value_local", x.data_ptr(), T.data_ptr(), nb_[0].data_ptr(),
-                                  nb_[1].data_ptr(), n, tvs.data_ptr(), scr.data_ptr(), nbytes, s)
-                        f += self.tv * float(tvs.item())
+                        f += self.tv * self._tv_value_local(tvq, x, T, n, s)
                 elif m_next is not None:
                     op.direct_cl(x, self.D, subset=m_next)
             if nseq is not None:
@@ -426,6 +447,8 @@ class SPDHGPoisson:
         self.state = {"epoch": ep0 + len(self.iter_stats), "z": z_host, "y": y_host}
         if tvq is not None:
             self.state.update(qx=tvq["qx"].cpu().numpy(), qy=tvq["qy"].cpu().numpy())
+            if tvq["levels"]:
+                self.state["tree_q"] = [(lev["qx"].cpu().numpy(), lev["qy"].cpu().numpy()) for lev in tvq["levels"]]
         self.final_stats = {"epochs": len(self.iter_stats), "final_f": f, "setup_s": t_setup, "rho": self.rho_used,
                             "subsets": self.M, "resident": self.resident_used,
                             "time": time.perf_counter() - t_start, "tv": self.tv, "tv_prob": self.tv_prob,
@@ -434,6 +457,56 @@ class SPDHGPoisson:
             host_copier().to_host(x, host_x)
         self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = None
         return x if x_on_gpu else host_x
+
+    def _tv_block_local(self, tvq, x, z, T, dz, n, s):
+        """The TV block on flat coefficients: the leaf level's dual step and D^T dq, then per tree level the node-pixel
+        sums, their dual step and D^T dq scattered onto the coefficients, and the primal step with the sum
+        (spdhg_poisson.py:853-877). Without tree levels the adjoint and the primal step run fused."""
+        nb_ = tvq["nbr"]
+        inv_p = float(1.0 / self.tv_prob)
+        _lib.call("dfx_tv_dual_local", x.data_ptr(), T.data_ptr(), tvq["qx"].data_ptr(), tvq["qy"].data_ptr(),
+                  tvq["dqx"].data_ptr(), tvq["dqy"].data_ptr(), nb_[0].data_ptr(), nb_[1].data_ptr(), tvq["lam"],
+                  tvq["ps"], n, s)
+        if not tvq["levels"]:
+            _lib.call("dfx_tv_adjoint_update_local", tvq["dqx"].data_ptr(), tvq["dqy"].data_ptr(), x.data_ptr(),
+                      z.data_ptr(), T.data_ptr(), nb_[2].data_ptr(), nb_[3].data_ptr(), inv_p, self.lam, n, s)
+            return
+        _lib.call("dfx_tv_adjoint_local", tvq["dqx"].data_ptr(), tvq["dqy"].data_ptr(), dz.data_ptr(),
+                  nb_[2].data_ptr(), nb_[3].data_ptr(), n, s)
+        scr = tvq["scr"]
+        for lev in tvq["levels"]:
+            nn = lev["n"]
+            _lib.call("dfx_tree_sums", x.data_ptr(), lev["ptr"].data_ptr(), lev["idx"].data_ptr(),
+                      scr["s"].data_ptr(), nn, s)
+            _lib.call("dfx_tv_dual_local", scr["s"].data_ptr(), lev["A"].data_ptr(), lev["qx"].data_ptr(),
+                      lev["qy"].data_ptr(), scr["dqx"].data_ptr(), scr["dqy"].data_ptr(), lev["right"].data_ptr(),
+                      lev["down"].data_ptr(), float(self.tv * lev["edge"]), tvq["ps"], nn, s)
+            _lib.call("dfx_tv_adjoint_local", scr["dqx"].data_ptr(), scr["dqy"].data_ptr(), scr["w"].data_ptr(),
+                      lev["left"].data_ptr(), lev["up"].data_ptr(), nn, s)
+            _lib.call("dfx_tree_scatter", scr["w"].data_ptr(), lev["map"].data_ptr(), dz.data_ptr(), n, s)
+        _lib.call("dfx_spdhg_primal_update", x.data_ptr(), z.data_ptr(), T.data_ptr(), dz.data_ptr(), inv_p,
+                  self.lam, n, s)
+
+    def _tv_value_local(self, tvq, x, T, n, s):
+        """The penalty over tv: leaf_edge TV(x) + the levels' edge TV(node-pixel sums) (spdhg_poisson.py:842-851)."""
+        op = self.op
+        nb_ = tvq["nbr"]
+        tvs = torch.zeros(1, dtype=torch.float64, device=op.device)
+        nbytes = op._lib.dfx_reduce_scratch_bytes(n)
+        scr = op.scratch(nbytes)
+        _lib.call("dfx_tv_value_local", x.data_ptr(), T.data_ptr(), nb_[0].data_ptr(), nb_[1].data_ptr(), n,
+                  tvs.data_ptr(), scr.data_ptr(), nbytes, s)
+        v = float(tvs.item()) * tvq["leaf_edge"]
+        for lev in tvq["levels"]:
+            nn = lev["n"]
+            _lib.call("dfx_tree_sums", x.data_ptr(), lev["ptr"].data_ptr(), lev["idx"].data_ptr(),
+                      tvq["scr"]["s"].data_ptr(), nn, s)
+            nbytes = op._lib.dfx_reduce_scratch_bytes(nn)
+            scr = op.scratch(nbytes)
+            _lib.call("dfx_tv_value_local", tvq["scr"]["s"].data_ptr(), lev["A"].data_ptr(), lev["right"].data_ptr(),
+                      lev["down"].data_ptr(), nn, tvs.data_ptr(), scr.data_ptr(), nbytes, s)
+            v += float(tvs.item()) * lev["edge"]
+        return v
 
     @on_op_stream
     def _setup(self, x0, b, weights=None, gain=None, background=None, state=None):

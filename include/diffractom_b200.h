@@ -424,6 +424,15 @@ int dfx_tv_adjoint_update_local(const float *dqx, const float *dqy, float *x, fl
 int dfx_tv_value_local(const float *x, const float *T, const int32_t *right, const int32_t *down, int64_t n,
                        double *out, void *scratch, size_t scratch_bytes, void *stream);
 
+/* replaces tv_adjoint_local / tree_sums / tree_scatter (spdhg_poisson.py:188-249): the hierarchical total variation's
+ * pieces. dfx_tv_adjoint_local writes w = D^T dq (the adjoint of dfx_tv_dual_local's differences, no primal step);
+ * dfx_tree_sums writes s_j = the float32 sum of x[idx[p]], p in [ptr[j], ptr[j+1]) (a node-pixel's coefficients);
+ * dfx_tree_scatter adds w[map[i]] to dz[i] where map[i] >= 0. */
+int dfx_tv_adjoint_local(const float *dqx, const float *dqy, float *w, const int32_t *left, const int32_t *up,
+                         int64_t n, void *stream);
+int dfx_tree_sums(const float *x, const int32_t *ptr, const int32_t *idx, float *s, int64_t n, void *stream);
+int dfx_tree_scatter(const float *w, const int32_t *map, float *dz, int64_t n, void *stream);
+
 /* replaces osem_update (optimization/osem_poisson.py:80-84): x = outside the support (mask periodic with period pm,
  * 0: no mask) ? 0 : (sens > 0 ? x back / (sens + lam) : x). */
 int dfx_osem_update(float *x, const float *back, const float *sens, const uint8_t *mask, int64_t pm, float lam,

@@ -9,6 +9,8 @@ and the SPDHG iteration of the reference (functions cite the reference file:line
                     subset, batch by batch, with the PF matrix evaluated densely (create_pfo_matrix.py:108-199) and
                     compacted into the two CSR copies (pf_kernels.cl:482-548)
   spdhg_reference   SPDHGPoisson.run (optimization/spdhg_poisson.py:513-751) for GPU-resident arrays, without TV
+  chambolle_pock_poisson_tv   a float64 primal-dual solve of the Poisson + (hierarchical) TV problem on explicit
+                    matrices: the independent optimum the tree-TV tests compare SPDHG's objective with
 
 Parity pins (tests/test_oracle.py): OracleOperator against the reference's float64 ReferenceModel on the golden
 fixtures of tests/golden (forward and transpose within 2e-5 of the maximum, as the reference's own
@@ -524,3 +526,46 @@ def pdhg_reference(op: OracleOperator, b, niter, x0=None, weights=None, gain=Non
             Ax = op.forward(x.reshape(K, op.Ny, op.Nx)).astype(f)
         devs.append(deviance(Ax, b, w, g, bg, eps_counts))
     return x.reshape(K, op.Ny, op.Nx), devs, rho
+
+
+def chambolle_pock_poisson_tv(A, D, b, gain, tv, free, eps=1e-3, n_iter=20000):
+    """The minimiser of sum_i (mu_i - b_i log mu_i) / g + tv sum_p |(D x)_p| over x >= 0 (x_j = 0 where not free),
+    mu = A x + eps g, by the diagonally preconditioned primal-dual method of Pock and Chambolle (ICCV 2011, alpha = 1:
+    sigma_i = 1 / sum_j |K_ij|, tau_j = 1 / sum_i |K_ij|, K = [A; D]) in float64 on the explicit matrices. D: sparse,
+    two rows (right, down) per penalty term p, already scaled by the term's weight; the dual of the Poisson rows is
+    the prox of sigma F*, F(u) = (u + r - b log(u + r)) / g, r = eps g: the smaller root of
+    y^2 - (c + v') y + v' c - sigma c b = 0, c = 1 / g, v' = v + sigma r; the TV rows are projected onto |q_p| <= tv.
+    The independent check of the optimum the reference's tests/test_tree_tv.py:69-91 makes."""
+    import scipy.sparse as sp
+    K = sp.vstack([sp.csr_matrix(A), sp.csr_matrix(D)]).tocsr()
+    KT = K.T.tocsr()
+    absK = abs(K)
+    sig = 1.0 / np.maximum(np.asarray(absK.sum(axis=1)).ravel(), 1e-30)
+    tau = 1.0 / np.maximum(np.asarray(absK.sum(axis=0)).ravel(), 1e-30)
+    tau[~np.asarray(free, bool)] = 0.0
+    nA = A.shape[0]
+    b = np.asarray(b, np.float64).ravel()
+    c, r = 1.0 / gain, eps * gain
+    sa = sig[:nA]
+    x = np.zeros(A.shape[1])
+    xb = x.copy()
+    y = np.zeros(K.shape[0])
+    for _ in range(n_iter):
+        v = y + sig * (K @ xb)
+        vp = v[:nA] + sa * r
+        y[:nA] = 0.5 * ((c + vp) - np.sqrt((vp - c) ** 2 + 4.0 * sa * c * b))
+        q = v[nA:].reshape(-1, 2)
+        y[nA:] = (q / np.maximum(1.0, np.hypot(q[:, 0], q[:, 1]) / tv)[:, None]).ravel()
+        xn = np.maximum(0.0, x - tau * (KT @ y))
+        xb = 2.0 * xn - x
+        x = xn
+    return x
+
+
+def poisson_tv_objective(A, D, x, b, gain, tv, eps=1e-3):
+    """sum (mu - b + b log(b / mu)) / g + tv sum_p |(D x)_p|, mu = max(A x, 0) + eps g (the solver's objective)."""
+    b = np.asarray(b, np.float64).ravel()
+    mu = np.maximum(A @ x, 0.0) + eps * gain
+    dev = np.sum((mu - b + np.where(b > 0, b * np.log(np.where(b > 0, b, 1.0) / mu), 0.0)) / gain)
+    g = (D @ x).reshape(-1, 2)
+    return float(dev + tv * np.hypot(g[:, 0], g[:, 1]).sum())
