@@ -68,10 +68,10 @@ class SPDHGPoisson:
         the others are streamed from pinned host memory (a CUDA x0 keeps all three on the device). tv > 0: the total
         variation of every orientation's image as one more block of the serial sampling, chosen with probability
         tv_prob (default 1 / (M + 1)); its dual (qx, qy) is two more coefficient arrays, resident or streamed as x, z,
-        T (spdhg_poisson.py:20-40, 320-324); not with shards. tv_tree (an orientation_tree.OrientationTree over the basis's
-        orientations in the grid's order; local basis only): the hierarchical total variation of its nested cells, the leaf
-        level with weight tv leaf_edge and every penalised level with tv edge, their dual steps sharing the TV
-        block's (spdhg_poisson.py:322-326, 819-862). shards
+        T (spdhg_poisson.py:20-40, 320-324); not with shards. tv_tree (an orientation_tree.OrientationTree over the
+        basis's orientations in the grid's order; local basis only): the hierarchical total variation of its nested
+        cells, the leaf level with weight tv leaf_edge and every penalised level with tv edge, their dual steps
+        sharing the TV block's (spdhg_poisson.py:322-326, 819-862). shards
         (this package's extension; a sharding.ShardSum): the operator holds one orientation shard of a process
         group, and the forward's data rows are summed over the shards after each pass; every rank passes the same
         seed and subsets."""
