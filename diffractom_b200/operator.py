@@ -830,16 +830,17 @@ class SinglePhaseForwardOperator:
                    self.Ny, self.My, self.Kstride, Kb, self._kernel_id, int(self.radon_geo.n_taps), x_ptr, z_ptr,
                    T_ptr, float(inv_p), float(lam), self._s())
 
-    def to_batches(self, coeffs, out_k):
-        """coeffs (K, Ny, Nx) -> channel-fastest batches (flat, batch ib at ib * npix * Kstride)."""
-        s = self._s()
+    def to_batches(self, coeffs, out_k, stream=None):
+        """coeffs (K, Ny, Nx) -> channel-fastest batches (flat, batch ib at ib * npix * Kstride; on stream, default
+        the operator's)."""
+        s = self._s() if stream is None else _stream_handle(stream)
         for ib, b in enumerate(self.batches):
             self._call("dfx_gather_channels", coeffs.data_ptr(), out_k.data_ptr() + 4 * ib * self.batch_elems(),
                        self.npix, b["k_start"], b["K_batch"], self.Kstride, s)
 
-    def from_batches(self, in_k, coeffs):
-        """Channel-fastest batches -> coeffs (K, Ny, Nx)."""
-        s = self._s()
+    def from_batches(self, in_k, coeffs, stream=None):
+        """Channel-fastest batches -> coeffs (K, Ny, Nx) (on stream, default the operator's)."""
+        s = self._s() if stream is None else _stream_handle(stream)
         for ib, b in enumerate(self.batches):
             self._call("dfx_scatter_channels", in_k.data_ptr() + 4 * ib * self.batch_elems(), coeffs.data_ptr(),
                        self.npix, b["k_start"], b["K_batch"], self.Kstride, s)

@@ -275,7 +275,7 @@ class SPDHGPoisson:
         if self.tv_tree is not None:
             raise NotImplementedError("tv_tree needs an operator with the local coefficient layout")
         self._setup(x0, b, weights, gain, background, state)
-        self._iterate(n_epochs, verbose, diagnostics_interval, callback)
+        self._iterate(n_epochs, verbose, diagnostics_interval, callback, defer_final=True)
         return self._finish()
 
     def _setup_data(self, b, weights, gain, background):
@@ -536,13 +536,15 @@ class SPDHGPoisson:
         self._stage = None if len(resident) == len(self._names) else KMajorStaging(op)
         self.dzk = torch.empty(be, dtype=torch.float32, device=dev)
         self.x = None
+        # a host x0 of a resident x is uploaded after the step sizes' passes are queued, on a side stream, so that
+        # the copy overlaps them (they do not read x)
+        upload_x = self.X.resident and not self._x_on_gpu
         if self.X.resident:
             if self._x_on_gpu:
                 self.x = x0
+                op.to_batches(self.x, self.X.dev)
             else:
                 self.x = torch.empty(cshape, dtype=torch.float32, device=dev)
-                host_copier().to_device(self._host_x, self.x)
-            op.to_batches(self.x, self.X.dev)
         else:
             self._stage.load(self._host_x.reshape(-1), self.X, self.pipe)
         if state is not None and state.get("z") is not None:
@@ -615,6 +617,12 @@ class SPDHGPoisson:
             _lib.call("dfx_tfinal", tb, be, s)           # padding channels were never reached: T = 0 there
 
         self.pipe.run([], [T], t_batch)
+        if upload_x:
+            side = torch.cuda.Stream(dev)
+            side.wait_stream(op.stream())               # x's allocation and the work before it
+            host_copier().to_device(self._host_x, self.x, stream=side)
+            op.stream().wait_stream(side)
+            op.to_batches(self.x, self.X.dev)
 
         def project_x(ib, s_):                          # x on the support, >= 0, padding 0
             _lib.call("dfx_batch_support", self.X.ptr(ib, s_), None, sp, npix, op.Kstride,
@@ -625,6 +633,16 @@ class SPDHGPoisson:
             host_copier().to_device(as_host(state["y"], dshape, "state['y']"), self.y)
             if state.get("z") is None:
                 self.pipe.run([], [self.Z], lambda ib, s_: op._adjoint_batch_k(self.y, ib, self.Z.ptr(ib, s_)))
+        # the host arrays the run ends with (z, y, and a NumPy x0 that receives x) have their pages mapped by the
+        # copy threads while the device iterates, so that the final downloads run at the copy rate
+        self._host_out, self._prefault = None, []
+        if self.Z.resident:
+            hc = host_copier()
+            z_host, y_host = np.empty(cshape, np.float32), np.empty(dshape, np.float32)
+            self._prefault = hc.prefault(z_host, False) + hc.prefault(y_host, False)
+            if self.X.resident and not self._x_on_gpu:
+                self._prefault += hc.prefault(self._host_x, True)
+            self._host_out = (z_host, y_host)
         self._graphs = {}
         self.graph_replays = 0
         self._t_setup = time.perf_counter() - self._t_start
@@ -644,12 +662,18 @@ class SPDHGPoisson:
             self._pass(None, self._seq[0])
 
     @on_op_stream
-    def _iterate(self, n_epochs, verbose=0, diagnostics_interval=1, callback=None, final=True):
+    def _iterate(self, n_epochs, verbose=0, diagnostics_interval=1, callback=None, final=True, defer_final=False):
         """n_epochs epochs (spdhg_poisson.py:664-719). final=False: the last of them is not the run's last (no
-        closing full forward unless diagnostics fall there), so that epochs can be run in several calls."""
+        closing full forward unless diagnostics fall there), so that epochs can be run in several calls.
+        defer_final (run()): the closing full forward and the objective of the run's last epoch are left to _finish,
+        which queues them beside the downloads of x, z and y (same values; the last epoch's "f" is filled in there)."""
         op = self.op
         dev = op.device
         seq = self._seq
+        # the closing full forward and objective of the run's last epoch can wait for _finish, which overlaps them
+        # with the state's downloads (nobody reads the objective before: no callback, no printing)
+        defer = (defer_final and final and callback is None and not verbose and self.tv == 0 and self.X.resident
+                 and self.Z.resident)
         for e in range(n_epochs):
             ep = self._ep0 + len(self.iter_stats) + 1
             last = final and e + 1 == n_epochs
@@ -673,7 +697,9 @@ class SPDHGPoisson:
                     self._dual(adj)
                 if full:
                     self._pass(adj, None, tv=tvb)
-                    if (end_of_epoch and want_f) or m_next is not None:
+                    if last and end_of_epoch and defer:
+                        self._final_pending = True           # _finish runs it beside the downloads
+                    elif (end_of_epoch and want_f) or m_next is not None:
                         op._fill(self.D, 0.0)
                         self._pass(None, "full")
                         if end_of_epoch and want_f:
@@ -726,8 +752,14 @@ class SPDHGPoisson:
         g.replay()
         self.graph_replays += 1
 
+    def _wait_prefault(self):
+        for f in self._prefault:
+            f.result()
+        self._prefault = []
+
     def _x_out(self):
         """x in the (K, Ny, Nx) layout of the caller's array (the CUDA x0, or the NumPy x0's device copy and x0)."""
+        self._wait_prefault()
         op = self.op
         if self.X.resident:
             op.from_batches(self.X.dev, self.x)
@@ -759,11 +791,37 @@ class SPDHGPoisson:
     @on_op_stream
     def _finish(self):
         op = self.op
+        if getattr(self, "_final_pending", False):
+            # the closing full forward (writes D only, reads x) and the objective on the operator's stream; x, z and y
+            # (final since the last update) converted and downloaded on a side stream meanwhile
+            self._final_pending = False
+            side = torch.cuda.Stream(op.device)
+            side.wait_stream(op.stream())
+            op._fill(self.D, 0.0)
+            self._pass(None, "full")
+            self._wait_prefault()
+            z_host, y_host = self._host_out
+            with torch.cuda.stream(side):
+                if not self._x_on_gpu:
+                    op.from_batches(self.X.dev, self.x, stream=side)
+                    host_copier().to_host(self.x, self._host_x, stream=side)
+                z = torch.empty(op.coeff_shape, dtype=torch.float32, device=op.device)
+                op.from_batches(self.Z.dev, z, stream=side)
+                host_copier().to_host(z, z_host, stream=side)
+                host_copier().to_host(self.y, y_host, stream=side)
+            side.synchronize()
+            del z
+            self._f = self._deviance(self.D)
+            if self.iter_stats:
+                self.iter_stats[-1]["f"] = self._f
+            if self._x_on_gpu:
+                op.from_batches(self.X.dev, self.x)
+            return self._finish_state(z_host, y_host, {})
         self._x_out()
         if self.Z.resident:
             z = torch.empty(op.coeff_shape, dtype=torch.float32, device=op.device)
             op.from_batches(self.Z.dev, z)
-            z_host = np.empty(op.coeff_shape, np.float32)
+            z_host = self._host_out[0]
             host_copier().to_host(z, z_host)
             del z
         else:
@@ -782,8 +840,11 @@ class SPDHGPoisson:
                 self._stage.store(arr, h.reshape(-1), self.pipe)
             tv_state[nm] = h
         self.pipe.synchronize()
-        y_host = np.empty(op.data_shape, np.float32)
+        y_host = self._host_out[1] if self._host_out is not None else np.empty(op.data_shape, np.float32)
         host_copier().to_host(self.y, y_host)
+        return self._finish_state(z_host, y_host, tv_state)
+
+    def _finish_state(self, z_host, y_host, tv_state):
         self.state = {"epoch": self._ep0 + len(self.iter_stats), "z": z_host, "y": y_host, **tv_state}
         self.final_stats = {"epochs": len(self.iter_stats), "final_f": self._f, "setup_s": self._t_setup,
                             "rho": self.rho_used, "subsets": self.M, "resident": self.resident_used,

@@ -295,6 +295,22 @@ class HostCopier:
     def _bytes(a: np.ndarray):
         return a.reshape(-1).view(np.uint8)
 
+    def prefault(self, host: np.ndarray, keep: bool):
+        """Touches every 4 KB page of host (C-contiguous) on the copy threads, so that a later download into it runs
+        at the copy rate of mapped memory instead of the page-fault rate of fresh memory; keep: write back each
+        touched byte (the contents stay), else write 0. Returns the futures; a later copy into host must wait for
+        them (a run does this work while the device computes)."""
+        v = self._bytes(host)
+        page = 4096
+
+        def touch(o, m):
+            sl = v[o:o + m:page]
+            if keep:
+                sl[...] = sl.copy()
+            else:
+                sl[...] = 0
+        return [self.pool.submit(touch, o, min(_COPY_CHUNK, v.size - o)) for o in range(0, v.size, _COPY_CHUNK)]
+
     def to_device(self, host: np.ndarray, dev: torch.Tensor, stream=None):
         """dev <- host (C-contiguous, same number of bytes); returns after the copies are enqueued on stream (the
         pinned buffers are not reused before their DMA has finished)."""
