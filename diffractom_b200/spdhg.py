@@ -545,6 +545,8 @@ class SPDHGPoisson:
                 op.to_batches(self.x, self.X.dev)
             else:
                 self.x = torch.empty(cshape, dtype=torch.float32, device=dev)
+                x_alloc = torch.cuda.Event()
+                x_alloc.record(op.stream())             # the side stream writes x after this point only
         else:
             self._stage.load(self._host_x.reshape(-1), self.X, self.pipe)
         if state is not None and state.get("z") is not None:
@@ -616,10 +618,29 @@ class SPDHGPoisson:
                 _lib.call("dfx_batch_support", tb, self.dzk.data_ptr(), sp, npix, op.Kstride, kb, c, 2, s)
             _lib.call("dfx_tfinal", tb, be, s)           # padding channels were never reached: T = 0 there
 
-        self.pipe.run([], [T], t_batch)
+        if bf16 and T.resident:
+            # subset by subset: one tensor-core PF adjoint for all batches, then every batch's backprojection and
+            # running minimum (the same columns as batch by batch, in a twentieth of the PF launches)
+            for ib in range(nbt):
+                _lib.call("dfx_tinit", T.ptr(ib, None), be, s)
+            for m in range(self.M):
+                e = op._sub[m]
+                z = op._z(e["n"])
+                op._pf_tc_adjoint(e["omegas"], e["n"], z)
+                for ib, bt in enumerate(op.batches):
+                    kb = bt["K_batch"]
+                    _lib.call("dfx_radon_backward_bf16", z.data_ptr() + 2 * ib * op.Kstride, op.Ktot,
+                              self.dzk.data_ptr(), e["geo"].data_ptr(), e["n"], op.Nx, op.Ny, op.My, op.Kstride, kb,
+                              op._kernel_id, int(op.radon_geo.n_taps), s)
+                    _lib.call("dfx_batch_support", T.ptr(ib, None), self.dzk.data_ptr(), sp, npix, op.Kstride, kb, c,
+                              2, s)
+            for ib in range(nbt):
+                _lib.call("dfx_tfinal", T.ptr(ib, None), be, s)
+        else:
+            self.pipe.run([], [T], t_batch)
         if upload_x:
             side = torch.cuda.Stream(dev)
-            side.wait_stream(op.stream())               # x's allocation and the work before it
+            side.wait_event(x_alloc)                    # not the step sizes' passes queued since
             host_copier().to_device(self._host_x, self.x, stream=side)
             op.stream().wait_stream(side)
             op.to_batches(self.x, self.X.dev)
