@@ -666,6 +666,7 @@ class SPDHGPoisson:
             self._host_out = (z_host, y_host)
         self._graphs = {}
         self.graph_replays = 0
+        self._final_pending = False
         self._t_setup = time.perf_counter() - self._t_start
         self._ep0 = int(state["epoch"]) if state is not None else 0
         self.iter_stats = []
@@ -812,7 +813,7 @@ class SPDHGPoisson:
     @on_op_stream
     def _finish(self):
         op = self.op
-        if getattr(self, "_final_pending", False):
+        if self._final_pending:
             # the closing full forward (writes D only, reads x) and the objective on the operator's stream; x, z and y
             # (final since the last update) converted and downloaded on a side stream meanwhile
             self._final_pending = False
