@@ -554,8 +554,11 @@ def chambolle_pock_poisson_tv(A, D, b, gain, tv, free, eps=1e-3, n_iter=20000):
         v = y + sig * (K @ xb)
         vp = v[:nA] + sa * r
         y[:nA] = 0.5 * ((c + vp) - np.sqrt((vp - c) ** 2 + 4.0 * sa * c * b))
-        q = v[nA:].reshape(-1, 2)
-        y[nA:] = (q / np.maximum(1.0, np.hypot(q[:, 0], q[:, 1]) / tv)[:, None]).ravel()
+        if tv > 0:
+            q = v[nA:].reshape(-1, 2)
+            y[nA:] = (q / np.maximum(1.0, np.hypot(q[:, 0], q[:, 1]) / tv)[:, None]).ravel()
+        else:                                    # |q_p| <= 0
+            y[nA:] = 0.0
         xn = np.maximum(0.0, x - tau * (KT @ y))
         xb = 2.0 * xn - x
         x = xn
