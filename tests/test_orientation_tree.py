@@ -1,7 +1,7 @@
 """OrientationTree (the nested cells of the hierarchical total variation) as the reference's
 tests/test_tree_tv.py:18-35 checks it: a symmetric copy of an orientation falls in its cell at every level, the cells
 nest, edges and leaf edge follow the radii; and the node-pixel arrays the solver's tree kernels use against a
-construction pixel by pixel. CPU only."""
+construction pixel by pixel and against the explicit penalty rows. CPU only."""
 import numpy as np
 import pytest
 
@@ -98,3 +98,31 @@ def test_tree_level_arrays_against_pixelwise_construction():
         assert np.count_nonzero(lev["map"] >= 0) == len(k)
         for a in ("ptr", "idx", "map", "right", "down", "left", "up"):
             assert lev[a].dtype == np.int32
+
+
+def test_level_arrays_give_the_explicit_penalty():
+    """The penalty of the tree levels computed on the node-pixel arrays (sums over the CSR lists, differences to the
+    right / down neighbours, edge-weighted norms) equals the norms of the explicit penalty rows of the GPU test, on
+    random coefficients with every coefficient free."""
+    from test_gpu_tree_tv import _tree_rows
+    from diffractom_b200 import OrientationTree
+    from diffractom_b200.orientation_tree import tree_level_arrays
+    rng = np.random.default_rng(11)
+    K, Ny, Nx = 10, 6, 7
+    tree = OrientationTree(_rotations(K, seed=2), None, (150.0, 80.0, 30.0))
+    mask = rng.random((K, Ny, Nx)) < 0.5
+    k, iy, ix = np.nonzero(mask)
+    n = len(k)
+    pi = rng.permutation(n)
+    x = rng.random(n)
+    levels = tree_level_arrays(k, iy, ix, pi, Ny, Nx, n, np.ones(n, np.float32), tree)
+    got = 0.0
+    for lev in levels:
+        s = np.array([x[lev["idx"][lev["ptr"][j]:lev["ptr"][j + 1]]].sum() for j in range(lev["n"])])
+        gx = np.where(lev["right"] >= 0, s[np.maximum(lev["right"], 0)] - s, 0.0)
+        gy = np.where(lev["down"] >= 0, s[np.maximum(lev["down"], 0)] - s, 0.0)
+        got += lev["edge"] * np.hypot(gx, gy).sum()
+    D = _tree_rows(k, iy, ix, pi, Ny, Nx, n, tree, np.ones(n, bool))
+    leaf_rows = 2 * K * Ny * Nx                              # the leaf level's rows come first
+    g = (D @ x)[leaf_rows:].reshape(-1, 2)
+    assert abs(np.hypot(g[:, 0], g[:, 1]).sum() - got) <= 1e-12 * got
