@@ -30,11 +30,15 @@ def check_device(a, shape, name):
     return a
 
 
-def as_host(a, shape, name):
-    """A C-contiguous float32 NumPy array of the given shape: a itself if it already is one, else a converted copy."""
+def as_host(a, shape, name, writeable=False):
+    """A C-contiguous float32 NumPy array of the given shape: a itself if it already is one, else a converted copy.
+    writeable: the caller writes its result into the array (a solver's x0), so a read-only array (a read-only memory
+    map, a view of bytes) is copied as well; the copy is what the solver returns."""
     out = np.ascontiguousarray(a, dtype=np.float32)
     if out.shape != tuple(shape):
         raise ValueError(f"{name} must have shape {tuple(shape)}, not {out.shape}")
+    if writeable and not out.flags.writeable:
+        out = out.copy()
     return out
 
 

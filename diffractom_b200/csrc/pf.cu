@@ -8,8 +8,6 @@
 
 #include <cuda_bf16.h>
 
-#include <mutex>
-
 #include "dfx_common.cuh"
 
 namespace dfx {
@@ -346,14 +344,9 @@ extern "C" int dfx_scan_exclusive_i32(const int32_t *in, int32_t *out, int64_t n
 // ---- the exclusive scan without caller scratch ----
 // Its tile sums live in this array, which the CUDA runtime places in the memory of every device that loads this
 // library and keeps there until the process exits. Host code only knows a stand-in for its name: the device address
-// comes from cudaGetSymbolAddress, looked up once per device (with that device current) and cached.
+// comes from cudaGetSymbolAddress, looked up on every call with the caller's device current. No address is cached,
+// so a context that was destroyed and made again (cudaDeviceReset, another driver context) never sees a stale one.
 static __device__ __align__(256) int32_t g_scan_tile_sums[DFX_SCAN_STATIC_MAX_N / SCAN_TILE + 1];
-
-namespace dfx {
-constexpr int MAX_DEVICES = 64;
-static std::mutex g_scan_mu;
-static int32_t *g_scan_ptr[MAX_DEVICES] = {nullptr};
-}  // namespace dfx
 
 extern "C" int dfx_scan_exclusive_i32_static(const int32_t *in, int32_t *out, int64_t n, void *stream)
 {
@@ -363,27 +356,15 @@ extern "C" int dfx_scan_exclusive_i32_static(const int32_t *in, int32_t *out, in
                 "scan_static: n = %lld is beyond the %lld elements its built-in scratch covers; use "
                 "dfx_scan_exclusive_i32 with scratch of dfx_scan_scratch_bytes(n) bytes", (long long)n,
                 (long long)DFX_SCAN_STATIC_MAX_N);
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    // the array's address in the current context (the first lookup on a device may load this library's module
+    // there; the later ones only read a table)
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_scan_tile_sums);
     if (e != cudaSuccess) {
-        set_error("scan_static: cudaGetDevice: %s", cudaGetErrorString(e));
+        set_error("scan_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
         return DFX_ECUDA;
     }
-    DFX_REQUIRE(dev >= 0 && dev < MAX_DEVICES, "scan_static: device %d beyond the %d supported", dev, MAX_DEVICES);
-    int32_t *sums = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_scan_mu);
-        if (!g_scan_ptr[dev]) {            // once per device, with that device current (the caller's)
-            void *p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_scan_tile_sums);
-            if (e != cudaSuccess) {
-                set_error("scan_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-                return DFX_ECUDA;
-            }
-            g_scan_ptr[dev] = static_cast<int32_t *>(p);
-        }
-        sums = g_scan_ptr[dev];
-    }
+    int32_t *sums = static_cast<int32_t *>(p);
     // every slot the later passes read is written by the first pass of this call: nothing to clear
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t tiles = cdiv(n > 0 ? n : 1, SCAN_TILE);

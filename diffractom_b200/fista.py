@@ -107,7 +107,7 @@ class FISTAPoisson:
         if is_device(x0):
             x = check_device(x0, cshape, "x0")
         else:
-            host_x0 = as_host(x0, cshape, "x0")
+            host_x0 = as_host(x0, cshape, "x0", writeable=True)
             x = torch.empty(cshape, dtype=torch.float32, device=dev)
             host_copier().to_device(host_x0, x)
         self.b = as_device_data(b, dshape, dev)

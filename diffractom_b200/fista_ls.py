@@ -80,7 +80,7 @@ class FISTAHuber:
         niter = int(niter)
         x_on_gpu = is_device(x0_gpu)
         x_dev = check_device(x0_gpu, cshape, "x0") if x_on_gpu else None
-        host_x = None if x_on_gpu else as_host(x0_gpu, cshape, "x0")
+        host_x = None if x_on_gpu else as_host(x0_gpu, cshape, "x0", writeable=True)
         b = as_device_data(out_gpu, dshape, dev)
         w, pw = periodic(weights, dshape, "weights", dev) if self.weighted else (None, 0)
         use_w = pw != 0
@@ -194,7 +194,7 @@ class FISTAHuber:
         n4 = -(-n // 4) * 4
         x_on_gpu = is_device(x0)
         x_dev = check_device(x0, (n,), "x0") if x_on_gpu else None
-        host_x = None if x_on_gpu else as_host(x0, (n,), "x0")
+        host_x = None if x_on_gpu else as_host(x0, (n,), "x0", writeable=True)
         b = as_device_data(out_gpu, dshape, dev)
         w, pw = periodic(weights, dshape, "weights", dev) if self.weighted else (None, 0)
         red = Reducer(op)

@@ -37,7 +37,7 @@ def _x_in(op, x0):
     cshape = tuple(op.coeff_shape)
     if is_device(x0):
         return check_device(x0, cshape, "x0"), None
-    host = as_host(x0, cshape, "x0")
+    host = as_host(x0, cshape, "x0", writeable=True)
     x = torch.empty(cshape, dtype=torch.float32, device=op.device)
     host_copier().to_device(host, x)
     return x, host

@@ -320,7 +320,7 @@ class SPDHGPoisson:
         n = int(op.n_coef)
         cshape, dshape = (n,), tuple(op.data_shape)
         x_on_gpu = is_device(x0)
-        host_x = None if x_on_gpu else as_host(x0, cshape, "x0")
+        host_x = None if x_on_gpu else as_host(x0, cshape, "x0", writeable=True)
         if x_on_gpu:
             x = check_device(x0, cshape, "x0")
         else:
@@ -518,7 +518,7 @@ class SPDHGPoisson:
         npix = op.npix
         s = op._s()
         self._x_on_gpu = is_device(x0)
-        self._host_x = None if self._x_on_gpu else as_host(x0, cshape, "x0")
+        self._host_x = None if self._x_on_gpu else as_host(x0, cshape, "x0", writeable=True)
         gamma = self._setup_data(b, weights, gain, background)
         supp = self.support_gpu
         sp = None if supp is None else supp.data_ptr()

@@ -300,6 +300,8 @@ class HostCopier:
         at the copy rate of mapped memory instead of the page-fault rate of fresh memory; keep: write back each
         touched byte (the contents stay), else write 0. Returns the futures; a later copy into host must wait for
         them (a run does this work while the device computes)."""
+        if not host.flags.writeable:
+            raise ValueError("prefault: the host array is read-only (its pages cannot be prepared for a download)")
         v = self._bytes(host)
         page = 4096
 

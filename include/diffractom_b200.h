@@ -194,8 +194,9 @@ int dfx_scan_exclusive_i32(const int32_t *in, int32_t *out, int64_t n, void *scr
  * its scratch (one int32 per 2048 elements) is a fixed array inside the library, present on every GPU that loads it
  * until the process exits (256 KiB per device). Limits and rules:
  *   n <= DFX_SCAN_STATIC_MAX_N, else DFX_EINVAL with a message (the other entry point has no such limit);
- *   the first call on a device looks up the array's address on that device (the calling thread's current device),
- *   so make that first call before any stream capture;
+ *   every call looks up the array's address in the calling thread's current context (nothing is cached, so a
+ *   context that was reset and made again is handled); the first lookup on a device may load the library's module
+ *   there, so make the first call on each device before any stream capture;
  *   all calls on a device share the array: calls that overlap on the GPU (other streams, other threads) race and
  *   corrupt each other's result; serialise them. Nothing has to be cleared between calls (each call writes every
  *   slot it later reads). */

@@ -1,7 +1,7 @@
 """Generate the golden fixtures of the parity tests from the reference implementation (diffractom).
 
-Run in a container where the reference's source tree is available (its path is the first argument, default
-/root/reference); the fixtures it writes (tests/golden/*.npz) are committed, so the tests never need the reference.
+Usage: python tests/golden/make_golden.py <path of the reference's source tree> (required). The fixtures it writes
+(tests/golden/*.npz) are committed, so the tests never need the reference.
 
 The reference's device code is OpenCL (pyopencl), which is not installed here. Its host code is plain NumPy, so
 the pyopencl modules are replaced by stubs and an operator object is assembled from the reference's own host
@@ -30,7 +30,9 @@ from unittest import mock
 
 import numpy as np
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) < 2:
+    sys.exit("usage: make_golden.py <path of the reference's source tree (the directory holding src/diffractom)>")
+REF = Path(sys.argv[1])
 OUT = Path(__file__).resolve().parent
 
 for m in ["pyopencl", "pyopencl.array", "pyopencl.tools", "pyopencl.scan", "pyopencl.elementwise",

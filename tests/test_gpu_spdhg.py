@@ -156,3 +156,28 @@ def test_spdhg_cuda_graphs_equal_plain_iterations(golden, precision):
     (x0, f0, z0, y0, n0), (x1, f1, z1, y1, n1) = runs
     assert n0 == 0 and n1 > 0
     assert np.array_equal(x0, x1) and f0 == f1 and np.array_equal(z0, z1) and np.array_equal(y0, y1)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+def test_deferred_closing_forward_equals_the_plain_one(golden, precision):
+    """run() without callback or printing leaves the last epoch's closing full forward and objective to _finish
+    (beside the downloads); with a callback it runs inside the epoch loop. Both give the same final objective, x, z
+    and y bit for bit, and the same per-epoch objectives."""
+    from diffractom_b200 import SinglePhaseForwardOperator, SPDHGPoisson
+    d = golden("al5_small")
+    cfg, mat, grid = case_inputs(d)
+    kw = {} if precision == "fp32" else {"precision": "bf16"}
+    op = SinglePhaseForwardOperator(cfg, mat, grid, 1e-5, normalized=True, quadrature=d["quadrature"], **kw)
+    rng = np.random.default_rng(4)
+    x_true = (rng.random(op.coeff_shape) * (rng.random(op.coeff_shape) < 0.2) * op.support_mask()[None]
+              ).astype(np.float32)
+    b = rng.poisson(op.direct(torch.as_tensor(x_true, device="cuda")).cpu().numpy() * 50).astype(np.float32)
+    runs = []
+    for cb in (None, lambda ep, x, stats: False):
+        sp = SPDHGPoisson(op, subsets=3, seed=2)
+        x = sp.run(np.zeros(op.coeff_shape, np.float32), b, 3, diagnostics_interval=1, callback=cb)
+        runs.append((x, sp.state, sp.final_stats["final_f"], [s["f"] for s in sp.iter_stats]))
+    (x0, s0, f0, fs0), (x1, s1, f1, fs1) = runs
+    assert f0 == f1 and fs0 == fs1
+    assert np.array_equal(x0, x1)
+    assert np.array_equal(s0["z"], s1["z"]) and np.array_equal(s0["y"], s1["y"])

@@ -35,3 +35,24 @@ def test_prefault_keeps_or_zeroes(n):
     assert np.all(v[touched] == 0)
     assert np.array_equal(v[~touched], np.full(n, 7.0, np.float32).view(np.uint8)[~touched])
     hc.pool.shutdown()
+
+
+def test_prefault_rejects_read_only_arrays_at_once():
+    hc = _copier()
+    a = np.zeros(1000, np.float32)
+    a.setflags(write=False)
+    with pytest.raises(ValueError, match="read-only"):
+        hc.prefault(a, True)
+    hc.pool.shutdown()
+
+
+def test_read_only_x0_is_copied_for_the_solvers():
+    """A solver writes its result into a NumPy x0; a read-only one is replaced by a writeable copy at set-up, so
+    nothing fails after the iterations have run."""
+    from diffractom_b200.arrays import as_host
+    a = np.arange(12, dtype=np.float32).reshape(3, 4)
+    assert as_host(a, (3, 4), "x0", writeable=True) is a
+    a.setflags(write=False)
+    assert as_host(a, (3, 4), "x0") is a
+    c = as_host(a, (3, 4), "x0", writeable=True)
+    assert c is not a and c.flags.writeable and np.array_equal(c, a)

@@ -43,6 +43,32 @@ def test_static_scan_matches_scratch_scan_twice():
         assert np.array_equal(out.cpu().numpy().astype(np.int64), expect)
 
 
+def test_static_scan_empty_and_largest_sizes():
+    """n = 0 (only the tile-sum passes run: out[0] = 0) and n = DFX_SCAN_STATIC_MAX_N, which fills every tile slot
+    of the built-in array plus the total's slot."""
+    from diffractom_b200 import _lib
+    torch.cuda.set_device(0)
+    lib = _lib.lib()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    one = torch.zeros(1, dtype=torch.int32, device="cuda")
+    out = torch.full((1,), -7, dtype=torch.int32, device="cuda")
+    assert lib.dfx_scan_exclusive_i32_static(one.data_ptr(), out.data_ptr(), 0, stream) == 0, lib.dfx_last_error()
+    torch.cuda.synchronize()
+    assert int(out.item()) == 0
+    n = 65536 * 2048                                  # DFX_SCAN_STATIC_MAX_N: 512 MiB of int32 input
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    x = torch.randint(0, 8, (n,), dtype=torch.int32, device="cuda", generator=g)
+    ref = _scan_with_scratch(lib, x, n, stream)
+    out = torch.full((n + 1,), -1, dtype=torch.int32, device="cuda")
+    assert lib.dfx_scan_exclusive_i32_static(x.data_ptr(), out.data_ptr(), n, stream) == 0, lib.dfx_last_error()
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref)
+    assert int(out[-1].item()) == int(x.sum(dtype=torch.int64).item())
+    del x, out, ref
+    torch.cuda.empty_cache()
+
+
 def test_static_scan_rejects_sizes_beyond_its_limit():
     from diffractom_b200 import _lib
     lib = _lib.lib()
