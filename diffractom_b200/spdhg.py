@@ -54,12 +54,15 @@ class SPDHGPoisson:
     # products). The pass's per-batch interleaving of the two becomes all updates, then all forwards: every batch's
     # forward still reads its updated x and adds into the rows of nb in batch order, so the values are the same bits.
     use_graphs = False
-    # with an operator of precision "bf16", the step sizes S and T come from the BF16 operator (the one the iterations
-    # apply); False: from the float32 operator, as the reference computes them
-    bf16_steps = True
-    # with an operator of precision "bf16", the full forward passes (the objective of the diagnostics epochs, whose
-    # rows also serve the next subset) run on the BF16 tensor-core path too; False: float32
-    bf16_diagnostics = True
+    # With an operator of precision "bf16" the subset iterations run the BF16 tensor-core path (Radon and PF
+    # contraction in BF16, float32 accumulation). The other passes follow the precision recipe by default:
+    # bf16_steps False: the step sizes S and T come from the float32 operator, as the reference computes them (they
+    # agree with float64 ones to 1e-5); True: from the BF16 operator (the one the iterations apply; about a quarter of
+    # the set-up time, S and T within 1e-2 of float64).
+    bf16_steps = False
+    # bf16_diagnostics False: the full forward of a diagnostics epoch (the residual A x, whose rows feed the float64
+    # deviance and the next subset) is recomputed with the float32 operator; True: through the BF16 path as well.
+    bf16_diagnostics = False
 
     def __init__(self, operator, subsets=8, prox_kind="nonneg", lam=0.0, support="fov", eps_counts=1e-3, rho="auto",
                  seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None, shards=None):

@@ -135,6 +135,25 @@ void orc_scatter(const float *img, float *coeffs, int Npix, int k0, int Kb, int 
             coeffs[(size_t)(k0 + k) * Npix + p] = img[(size_t)p * Kstride + k];
 }
 
+/* dst (cols, rows) = src (rows, cols)^T, blocked and spread over the threads: the layout changes between the
+ * coefficients (K, Npix) and the channel-fastest batch (Npix, K) that the reference's gather / scatter kernels do on
+ * the device (radon_kernels.cl:192-244). src_ld / dst_ld: row strides in elements. */
+#define TRANSPOSE(NAME, T)                                                                                         \
+    void NAME(const T *src, T *dst, int64_t rows, int64_t cols, int64_t src_ld, int64_t dst_ld)                   \
+    {                                                                                                              \
+        const int64_t B = 64;                                                                                      \
+        _Pragma("omp parallel for collapse(2) schedule(static)")                                                  \
+        for (int64_t r0 = 0; r0 < rows; r0 += B)                                                                   \
+            for (int64_t c0 = 0; c0 < cols; c0 += B) {                                                             \
+                const int64_t r1 = r0 + B < rows ? r0 + B : rows, c1 = c0 + B < cols ? c0 + B : cols;            \
+                for (int64_t c = c0; c < c1; ++c)                                                                  \
+                    for (int64_t r = r0; r < r1; ++r) dst[c * dst_ld + r] = src[r * src_ld + c];                   \
+            }                                                                                                      \
+    }
+TRANSPOSE(orc_transpose_f32, float)
+TRANSPOSE(orc_transpose_f64, double)
+#undef TRANSPOSE
+
 static inline float pv(const float *a, uint64_t period, uint64_t i, float dflt) { return period ? a[i % period] : dflt; }
 
 /* SPDHG dual step on the rows of the angles omegas (spdhg_poisson.py:69-91, dual_update_sub): on entry d holds A x

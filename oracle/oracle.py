@@ -8,7 +8,10 @@ and the SPDHG iteration of the reference (functions cite the reference file:line
   OracleOperator    forward / adjoint of SinglePhaseForwardOperator (SPFO:1646-1728, 1966-2033), full or per angle
                     subset, batch by batch, with the PF matrix evaluated densely (create_pfo_matrix.py:108-199) and
                     compacted into the two CSR copies (pf_kernels.cl:482-548)
-  spdhg_reference   SPDHGPoisson.run (optimization/spdhg_poisson.py:513-751) for GPU-resident arrays, without TV
+  spdhg_reference   SPDHGPoisson.run (optimization/spdhg_poisson.py:513-751) for GPU-resident arrays (float32 state,
+                    float64 prox and sums, as the reference), with the TV block
+  spdhg_reference64 the same loop entirely in float64 (state, data, images, step sizes): the FP64 oracle that the
+                    float32 and BF16 paths' errors are stated against
   chambolle_pock_poisson_tv   a float64 primal-dual solve of the Poisson + (hierarchical) TV problem on explicit
                     matrices: the independent optimum the tree-TV tests compare SPDHG's objective with
 
@@ -57,6 +60,8 @@ def lib():
         h.orc_deviance.argtypes = [P, P, P, c_uint64, P, c_uint64, P, c_uint64, F, c_uint64]
         h.orc_deviance.restype = c_double
         h.orc_num_threads.restype = c_int
+        for suf in ("_f32", "_f64"):
+            getattr(h, "orc_transpose" + suf).argtypes = [P, P, c_int64, c_int64, c_int64, c_int64]
         _lib = h
     return _lib
 
@@ -136,9 +141,9 @@ class OracleOperator:
         return self._csr[key]
 
     # ---- operator
-    def forward(self, x, subset=None, data=None):
+    def forward(self, x, subset=None, data=None, accumulate=False):
         """data (R, My, CP) = A x; subset (angle indices): only those rows are written (the others kept from data,
-        default zeros)."""
+        default zeros); accumulate: A x is added to those rows of data instead (the batched products' beta = 1)."""
         x = _c(x, self.io).reshape(self.K, -1)
         npix = self.Nx * self.Ny
         if data is None:
@@ -146,12 +151,13 @@ class OracleOperator:
         else:
             data = _c(data, self.io)
         angles = np.arange(self.R) if subset is None else np.asarray(subset, np.int64)
-        data[angles] = 0.0
+        if not accumulate:
+            data[angles] = 0.0
         om = _c(angles, np.int32)
         geo = _c(self.geo[angles], np.float32)
         L = lib()
         for k0, kb in self.batches:
-            img = _c(x[k0:k0 + kb].T, self.io)                    # (npix, kb) channel-fastest
+            img = self._transposed(x[k0:k0 + kb])                # (npix, kb) channel-fastest
             sino = np.empty((len(angles), self.My, kb), self.io)
             getattr(L, "orc_radon_forward" + self.suffix)(_p(img), _p(sino), _p(geo), len(angles), self.Nx, self.Ny,
                                                           self.My, kb, kb, self.kernel, self.scale)
@@ -179,8 +185,19 @@ class OracleOperator:
             img = np.empty((npix, kb), self.io)
             getattr(L, "orc_radon_backward" + self.suffix)(_p(sino), _p(img), _p(geo), len(angles), self.Nx, self.Ny,
                                                            self.My, kb, kb, self.kernel)
-            out[k0:k0 + kb] = img.T
+            self._transposed(img, out=out[k0:k0 + kb])
         return out.reshape(self.K, self.Ny, self.Nx)
+
+    def _transposed(self, a, out=None):
+        """a (rows, cols) C-contiguous in the io type -> its transpose (cols, rows), by the oracle's threads."""
+        a = _c(a, self.io)
+        rows, cols = a.shape
+        if out is None:
+            out = np.empty((cols, rows), self.io)
+        assert out.flags.c_contiguous and out.shape == (cols, rows) and out.dtype == self.io
+        fn = lib().orc_transpose_f64 if self.io == np.float64 else lib().orc_transpose_f32
+        fn(_p(a), _p(out), rows, cols, cols, rows)
+        return out
 
 
 def periodic(a, n_data, dshape):
@@ -375,6 +392,127 @@ def spdhg_reference(op: OracleOperator, subsets, b, n_epochs, x0=None, weights=N
         if nseq is not None:
             seq = nseq
     return x.reshape(K, op.Ny, op.Nx), y, z.reshape(K, op.Ny, op.Nx), devs, rho
+
+
+def _full64(a, n):
+    """A periodic float32 array (weights / gain / background) expanded to n float64 values, or None."""
+    if a is None:
+        return None
+    h = np.ascontiguousarray(a, np.float32).ravel()
+    return np.resize(h, n).astype(np.float64)
+
+
+def deviance64(mu, b, w=None, g=None, bg=None, eps=1e-3):
+    """Poisson deviance with every operand in float64 (fista_poisson.py:72-113, mode 0): sum w / g [m - b + b log(b /
+    m)], m = max(mu, 0) + bg + eps g, over the points with w != 0."""
+    mu = np.asarray(mu, np.float64).ravel()
+    b = np.asarray(b, np.float32).ravel().astype(np.float64)
+    n = b.size
+    wv, gv, bgv = _full64(w, n), _full64(g, n), _full64(bg, n)
+    gg = np.ones(n) if gv is None else gv
+    m = np.maximum(mu, 0.0) + (0.0 if bgv is None else bgv) + float(np.float32(eps)) * gg
+    with np.errstate(divide="ignore", invalid="ignore"):
+        term = m - b + np.where(b > 0, b * np.log(np.where(b > 0, b, 1.0) / m), 0.0)
+    sc = (1.0 if wv is None else wv) / gg
+    live = np.ones(n, bool) if wv is None else wv != 0
+    return float(np.sum((sc * term)[live]))
+
+
+def spdhg_reference64(op: OracleOperator, subsets, b, n_epochs, x0=None, weights=None, gain=None, background=None,
+                      support=None, eps_counts=1e-3, rho="auto", seed=0, lam=0.0, diagnostics_interval=1):
+    """SPDHGPoisson.run (spdhg_poisson.py:513-719, set-up 558-662) entirely in float64: the operator's forward and
+    adjoint with float64 images, sinograms and data (op built with precision "f64io"; the tap weights and PF values
+    are the operator's float32 ones), float64 step sizes S and T, dual step (the closed-form prox of
+    spdhg_poisson.py:69-91), primal step (spdhg_poisson.py:95-106) and deviance. The same subset schedule
+    (default_rng(seed)) as the float32 loops; no TV block. Returns (x, y, z, [deviance per diagnostics epoch], rho,
+    {"S": S, "T": T}) with x, z (K, Ny, Nx) and y, S data-shaped, all float64."""
+    if op.io is not np.float64:
+        raise ValueError("spdhg_reference64 needs an oracle operator of precision 'f64io'")
+    R, My, CP = op.R, op.My, op.CP
+    dshape = (R, My, CP)
+    b32 = np.ascontiguousarray(b, np.float32).reshape(dshape)
+    n = b32.size
+    b64 = b32.astype(np.float64)
+    wv, gv, bgv = _full64(weights, n), _full64(gain, n), _full64(background, n)
+    M = len(subsets)
+    subsets = [np.asarray(s_, np.int64) for s_ in subsets]
+    p = 1.0 / M
+    K, npix = op.K, op.Nx * op.Ny
+    supp = np.ones(npix, bool) if support is None else np.asarray(support, bool).ravel()
+    counted = np.ones(n, bool) if wv is None else wv != 0
+    if rho == "auto":
+        mean_b = float(np.sum(b64.ravel()[counted])) / max(float(np.count_nonzero(counted)), 1.0)
+        rho = 3e4 / mean_b ** 2 if mean_b > 0 else 1.0
+    gamma = float(np.sqrt(rho))
+    ones = np.broadcast_to(supp.astype(np.float64), (K, npix)).reshape(K, op.Ny, op.Nx)
+    rowsum = op.forward(ones).ravel()
+    S = np.where(counted & (rowsum > 0), gamma / np.where(rowsum > 0, rowsum, 1.0), 0.0)
+    mask = counted.astype(np.float64).reshape(dshape)
+    T = np.full((K, npix), np.inf)
+    for s_ in subsets:
+        cs = op.adjoint(mask, subset=s_).reshape(K, npix)
+        upd = supp[None, :] & (cs > 0)
+        T = np.where(upd, np.minimum(T, (p / gamma) / np.where(cs > 0, cs, 1.0)), T)
+    T[np.isinf(T)] = 0.0
+    x = np.zeros((K, npix)) if x0 is None else np.asarray(x0, np.float64).reshape(K, npix).copy()
+    x[:, ~supp] = 0.0
+    x = np.maximum(x, 0.0)
+    z = np.zeros((K, npix))
+    y = np.zeros(n)
+    D = np.zeros(dshape)
+    row = My * CP
+    g1 = np.ones(n) if gv is None else gv
+    sc_all = (1.0 if wv is None else wv) / g1
+    r_all = (0.0 if bgv is None else bgv) + float(np.float32(eps_counts)) * g1
+    live_all = counted & (S != 0)
+
+    def dual(m):
+        """The Poisson conjugate prox on the rows of subset m; D holds A x there on entry, the dual change on exit."""
+        idx = (subsets[m][:, None] * row + np.arange(row)[None, :]).ravel()
+        Dv = D.reshape(-1)
+        yo, si, sc = y[idx], S[idx], sc_all if np.isscalar(sc_all) else sc_all[idx]
+        v = yo + si * Dv[idx] + si * (r_all[idx] if not np.isscalar(r_all) else r_all)
+        dd = v - sc
+        yn = 0.5 * (v + sc - np.sqrt(dd * dd + 4.0 * si * sc * b64.ravel()[idx]))
+        yn = np.where(live_all[idx], yn, 0.0)
+        Dv[idx] = yn - yo
+        y[idx] = yn
+
+    rng = np.random.default_rng(seed)
+    last = None
+    devs = []
+    seq, last = epoch_sequence(rng, M, last, 0)
+    D = op.forward(x, subset=subsets[seq[0]], data=D)
+    inv_p = float(M)
+    for e in range(n_epochs):
+        final = e + 1 == n_epochs
+        want = (e + 1) % max(1, diagnostics_interval) == 0 or final
+        nseq = None
+        for j, m in enumerate(seq):
+            eoe = j + 1 == len(seq)
+            if not eoe:
+                nb = seq[j + 1]
+            elif not final:
+                nseq, last = epoch_sequence(rng, M, last, 0)
+                nb = nseq[0]
+            else:
+                nb = None
+            dual(m)
+            dz = op.adjoint(D, subset=subsets[m]).reshape(K, npix)
+            z += dz
+            zb = z + inv_p * dz
+            x = np.where(T > 0, np.maximum(0.0, x - T * (zb + lam)), 0.0)
+            if (eoe and want) or nb is None or nb == m:
+                if (eoe and want) or nb is not None:
+                    D = op.forward(x)
+                    if eoe and want:
+                        devs.append(deviance64(D, b32, weights, gain, background, eps_counts))
+            else:
+                D = op.forward(x, subset=subsets[nb], data=D)
+        if nseq is not None:
+            seq = nseq
+    return (x.reshape(K, op.Ny, op.Nx), y.reshape(dshape), z.reshape(K, op.Ny, op.Nx), devs, rho,
+            {"S": S.reshape(dshape), "T": T.reshape(K, op.Ny, op.Nx)})
 
 
 def fista_ls_reference(op: OracleOperator, b, niter, tau, x0=None, prox="nonneg", lam=0.0, support=None, clip=False,

@@ -160,3 +160,28 @@ def test_float64_io_variant_and_finite_differences(golden, name):
     fd = (io.forward(c + h * dr) - io.forward(c - h * dr)) / (2 * h)
     ad = io.forward(dr)
     assert np.abs(fd - ad).max() <= 1e-7 * np.abs(ad).max()
+
+
+def test_float64_spdhg_loop_against_the_float32_storage_loop(golden):
+    """spdhg_reference64 (every operand float64) and spdhg_reference (float32 state, float64 prox and sums) run the
+    same schedule and steps: their iterates and deviances differ by float32 rounding only; the float64 deviance of
+    a float32 prediction equals the C deviance."""
+    from oracle.oracle import deviance64, spdhg_reference, spdhg_reference64
+    d = golden("al5_small")
+    g = case_geometry(d)
+    o32 = OracleOperator.from_operator(g, precision="f64")
+    o64 = OracleOperator.from_operator(g, precision="f64io")
+    rng = np.random.default_rng(3)
+    supp = g.support_mask()
+    x_true = (rng.random((g.K, g.Ny, g.Nx)) * (rng.random((g.K, g.Ny, g.Nx)) < 0.2) * supp[None]).astype(np.float32)
+    b = rng.poisson(o32.forward(x_true) * 50).astype(np.float32)
+    subsets = [np.arange(m, g.N_Omega, 3) for m in range(3)]
+    x32, y32, z32, dev32, rho32 = spdhg_reference(o32, subsets, b, 4, support=supp, seed=1)
+    x64, y64, z64, dev64, rho64, steps = spdhg_reference64(o64, subsets, b, 4, support=supp, seed=1)
+    assert rho32 == rho64 and x64.dtype == np.float64 and len(dev64) == len(dev32) == 4
+    np.testing.assert_allclose(dev32, dev64, rtol=1e-6)
+    assert np.linalg.norm(x32 - x64) <= 1e-5 * np.linalg.norm(x64)
+    assert np.linalg.norm(y32 - y64) <= 1e-5 * np.linalg.norm(y64)
+    assert steps["T"].shape == x64.shape and steps["S"].shape == b.shape
+    mu = o32.forward(x32)
+    assert abs(deviance64(mu, b) - deviance(mu, b)) <= 1e-12 * abs(deviance(mu, b))
