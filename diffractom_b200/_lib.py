@@ -57,6 +57,10 @@ SIGNATURES = {
     "dfx_scan_exclusive_i32_static": ([P, P, L, S], c_int),
     "dfx_spmm_pf_forward": ([P, P, P, P, P, P, I, I, I, I, I, I, S], c_int),
     "dfx_spmm_pf_adjoint": ([P, P, P, P, P, P, I, I, I, I, I, F, I, S], c_int),
+    "dfx_pf_fblock_rows": ([I, I, I], c_int64),
+    "dfx_pf_fblock_count": ([P, P, I, I, I, P, P, S], c_int),
+    "dfx_pf_fblock_fill": ([P, P, P, I, I, I, P, P, P, S], c_int),
+    "dfx_spmm_pf_forward_blocked": ([P, P, P, P, P, P, P, I, I, I, I, I, I, S], c_int),
     "dfx_zero_rows": ([P, P, I, L, S], c_int),
     "dfx_fill_f32": ([P, F, L, S], c_int),
     "dfx_spdhg_dual_update": ([P, P, P, P, P, L, P, L, P, L, F, P, I, L, S], c_int),

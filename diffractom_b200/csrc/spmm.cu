@@ -6,7 +6,9 @@
 // a chunk of columns] in shared memory transposed (the TY values of one column contiguous, read as float4); every
 // thread walks its row's entries in groups of four, loading the next group while it applies the current one, and
 // uses each entry TY times from a register. Rows are sorted by column, so a thread keeps its place from one chunk to
-// the next. No atomics: every output is written by one thread.
+// the next. No atomics: every output is written by one thread. The adjoint launches spmm_adjoint8_kernel (eight lines
+// per thread, the whole data row staged at once); the forward over stored copies runs over eta blocks
+// (spmm_forward_b4_kernel), the CSR kernel serving generated copies.
 #include "dfx_common.cuh"
 
 namespace dfx {
@@ -127,18 +129,30 @@ __global__ void __launch_bounds__(SP_ROWS) spmm_forward_kernel(
     }
 }
 
-// adjoint: sino[s, y, k] = alpha sum_j PF[k, j] data[r, y, j]   (rows k over the adjoint CSR)
-__global__ void __launch_bounds__(SP_ROWS) spmm_adjoint_kernel(
+// ---- adjoint with eight lines per thread ----
+// adjoint: sino[s, y, k] = alpha sum_j PF[k, j] data[r, y, j] (rows k over the adjoint CSR), per row k over its
+// entries j ascending, fmaf from 0, times alpha, with the
+// work laid out for the adjoint's shape: a block owns AJ_ROWS orientations of one angle and AJ_TY detector lines and
+// stages those lines of the data row as wide as shared memory allows (the whole row for CP <= AJ_MAX_CHUNK), so a thread
+// walks its row in one pass with no chunk boundaries. The staged lines are split in two halves of four (half h of
+// column c at float4 index h * cn + c): the two 16-byte loads of an entry fall on bank groups that depend on c alone,
+// spreading a warp's random columns over all eight groups.
+constexpr int AJ_TY = 8;
+constexpr int AJ_ROWS = 512;
+constexpr int AJ_MAX_CHUNK = 3072;        // 3072 columns x 8 lines x 4 B = 96 KB (two blocks per SM)
+
+__global__ void __launch_bounds__(AJ_ROWS) spmm_adjoint8_kernel(
     const float *__restrict__ data, const int32_t *__restrict__ row_ptr, const uint16_t *__restrict__ col_j,
     const float *__restrict__ val, float *__restrict__ sino, const int32_t *__restrict__ omegas, int my, int kb,
-    int cp, int kstride, float alpha, int compact)
+    int cp, int kstride, float alpha, int compact, int chunk)
 {
-    __shared__ __align__(16) float tile[SP_CHUNK * SP_TYP];
-    const int k = blockIdx.x * SP_ROWS + threadIdx.x;
-    const int y0 = blockIdx.y * SP_TY;
+    extern __shared__ __align__(16) float4 tile4[];
+    float *tile = reinterpret_cast<float *>(tile4);
+    const int k = blockIdx.x * AJ_ROWS + threadIdx.x;
+    const int y0 = blockIdx.y * AJ_TY;
     const int s = blockIdx.z;
     const int r = omegas ? __ldg(omegas + s) : s;
-    const int ny = min(SP_TY, my - y0);
+    const int ny = min(AJ_TY, my - y0);
     int i = 0, e = 0;
     if (k < kb) {
         const int64_t rr = (int64_t)(compact ? s : r) * kb + k;
@@ -147,21 +161,200 @@ __global__ void __launch_bounds__(SP_ROWS) spmm_adjoint_kernel(
     }
     Group g;
     load_group(g, col_j, val, i, e);
-    float acc[SP_TY];
+    float acc[AJ_TY];
 #pragma unroll
-    for (int t = 0; t < SP_TY; ++t) acc[t] = 0.0f;
-    for (int c0 = 0; c0 < cp; c0 += SP_CHUNK) {
-        const int cn = min(SP_CHUNK, cp - c0);
+    for (int t = 0; t < AJ_TY; ++t) acc[t] = 0.0f;
+    const int64_t line0 = (int64_t)r * my + y0;
+    for (int c0 = 0; c0 < cp; c0 += chunk) {
+        const int cn = min(chunk, cp - c0);
         if (c0) __syncthreads();
-        stage(tile, data, (int64_t)r * my + y0, cp, ny, c0, cn);
+        for (int idx = threadIdx.x; idx < AJ_TY * cn; idx += blockDim.x) {
+            const int t = idx / cn, c = idx - t * cn;
+            tile[((t >> 2) * cn + c) * 4 + (t & 3)] = t < ny ? __ldg(data + (line0 + t) * cp + c0 + c) : 0.0f;
+        }
         __syncthreads();
-        i = walk_row(acc, tile, col_j, val, i, e, g, c0, c0 + cn);
+        const int c_end = c0 + cn;
+        while (i < e && g.c[0] < c_end) {
+            Group n;
+            const bool whole = g.c[3] < c_end;             // the group lies in this chunk (or ends the row)
+            if (whole) load_group(n, col_j, val, i + 4, e);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (i + u >= e || g.c[u] >= c_end) break;
+                const int c = g.c[u] - c0;
+                const float4 z0 = tile4[c], z1 = tile4[cn + c];
+                const float v = g.v[u];
+                acc[0] = __fmaf_rn(v, z0.x, acc[0]);
+                acc[1] = __fmaf_rn(v, z0.y, acc[1]);
+                acc[2] = __fmaf_rn(v, z0.z, acc[2]);
+                acc[3] = __fmaf_rn(v, z0.w, acc[3]);
+                acc[4] = __fmaf_rn(v, z1.x, acc[4]);
+                acc[5] = __fmaf_rn(v, z1.y, acc[5]);
+                acc[6] = __fmaf_rn(v, z1.z, acc[6]);
+                acc[7] = __fmaf_rn(v, z1.w, acc[7]);
+            }
+            if (whole) {
+                g = n;
+                i += 4;
+            } else {                                        // the chunk ends inside the group: realign at its end
+                int u = 0;
+                while (u < 4 && i + u < e && g.c[u] < c_end) ++u;
+                i += u;
+                load_group(g, col_j, val, i, e);
+            }
+        }
     }
     if (k < kstride) {
         float *zl = sino + ((int64_t)s * my + y0) * kstride + k;
 #pragma unroll
-        for (int t = 0; t < SP_TY; ++t)
+        for (int t = 0; t < AJ_TY; ++t)
             if (t < ny) zl[(int64_t)t * kstride] = k < kb ? alpha * acc[t] : 0.0f;
+    }
+}
+
+// ---- eta-blocked forward rows ----
+// The forward CSR of a batch (rows r * CP + j, j = c * P + p, each listing its orientations k ascending) regrouped
+// into block rows (r, cb, p), q = cb * P + p: the rows of the eta bins c = 4 cb .. 4 cb + 3 of ring p merged into one
+// list of k ascending whose entries carry four values (0 where that bin's row has no entry k). Neighbouring eta bins
+// of a ring share most orientations (a kernel's pole figure crosses a ring over several bins), so an entry's Z column
+// is staged once for four outputs. mask bit u: the row of bin 4 cb + u has entries (its output is written). Rings run
+// fastest, so the 32 threads of a warp (eight rings of four eta blocks) store to four 32-byte sectors per line.
+constexpr int FB_W = 4;
+
+__device__ __forceinline__ int fb_heads(const int32_t *__restrict__ row_ptr, int64_t row0, int P, int C, int cb,
+                                        int (&b)[FB_W], int (&e)[FB_W])
+{
+    int m = 0;
+#pragma unroll
+    for (int u = 0; u < FB_W; ++u) {
+        const int c = FB_W * cb + u;
+        b[u] = e[u] = 0;
+        if (c < C) {
+            const int64_t row = row0 + (int64_t)c * P;
+            b[u] = __ldg(row_ptr + row);
+            e[u] = __ldg(row_ptr + row + 1);
+        }
+        m |= (b[u] < e[u]) << u;
+    }
+    return m;
+}
+
+// FILL 0: counts[q] = entries of block row q, mask[q]; FILL 1: the entries at fb_ptr[q] ...
+template <int FILL>
+__global__ void fb_build_kernel(const int32_t *__restrict__ row_ptr, const uint16_t *__restrict__ col_k,
+                                const float *__restrict__ val, int64_t n_blocks, int P, int C, int ncb,
+                                int32_t *__restrict__ counts, uint8_t *__restrict__ mask,
+                                const int32_t *__restrict__ fb_ptr, uint16_t *__restrict__ fb_k,
+                                float4 *__restrict__ fb_v)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_blocks) return;
+    const int64_t per_angle = (int64_t)P * ncb;
+    const int64_t r = g / per_angle;
+    const int q = (int)(g - r * per_angle), cb = q / P, p = q - (q / P) * P;
+    int b[FB_W], e[FB_W];
+    const int m = fb_heads(row_ptr, r * (int64_t)C * P + p, P, C, cb, b, e);
+    int head[FB_W];
+#pragma unroll
+    for (int u = 0; u < FB_W; ++u) head[u] = b[u] < e[u] ? (int)__ldg(col_k + b[u]) : 0x10000;
+    int n = 0;
+    int64_t o = FILL ? __ldg(fb_ptr + g) : 0;
+    while (true) {
+        int k = 0x10000;
+#pragma unroll
+        for (int u = 0; u < FB_W; ++u) k = min(k, head[u]);
+        if (k == 0x10000) break;
+        float v[FB_W];
+#pragma unroll
+        for (int u = 0; u < FB_W; ++u) {
+            v[u] = 0.0f;
+            if (head[u] == k) {
+                if (FILL) v[u] = __ldg(val + b[u]);
+                ++b[u];
+                head[u] = b[u] < e[u] ? (int)__ldg(col_k + b[u]) : 0x10000;
+            }
+        }
+        if (FILL) {
+            fb_k[o] = (uint16_t)k;
+            fb_v[o] = make_float4(v[0], v[1], v[2], v[3]);
+            ++o;
+        }
+        ++n;
+    }
+    if (!FILL) {
+        counts[g] = n;
+        mask[g] = (uint8_t)m;
+    }
+}
+
+// forward over the blocked rows: data[r, y, (4 cb + u) P + p] += sum_k v_u sino[s, y, k] for the bins with entries.
+// A thread owns one block row and SP_TY lines (4 x SP_TY accumulators); per entry one staged column of SP_TY values
+// feeds 4 SP_TY fused multiply-adds. The sums run over k ascending from 0 with fmaf, as spmm_forward_kernel's: a zero
+// value adds exactly 0, so the results are that kernel's bit for bit.
+__global__ void __launch_bounds__(SP_ROWS) spmm_forward_b4_kernel(
+    const float *__restrict__ sino, const int32_t *__restrict__ fb_ptr, const uint16_t *__restrict__ fb_k,
+    const float4 *__restrict__ fb_v, const uint8_t *__restrict__ fb_mask, float *__restrict__ data,
+    const int32_t *__restrict__ omegas, int my, int P, int C, int ncb, int kstride, int kb)
+{
+    __shared__ __align__(16) float tile[SP_CHUNK * SP_TYP];
+    const int per_angle = P * ncb;
+    const int q = blockIdx.x * SP_ROWS + threadIdx.x;
+    const int y0 = blockIdx.y * SP_TY;
+    const int s = blockIdx.z;
+    const int r = omegas ? __ldg(omegas + s) : s;
+    const int ny = min(SP_TY, my - y0);
+    int i = 0, e = 0, m = 0;
+    if (q < per_angle) {
+        const int64_t g = (int64_t)r * per_angle + q;
+        i = __ldg(fb_ptr + g);
+        e = __ldg(fb_ptr + g + 1);
+        m = __ldg(fb_mask + g);
+    }
+    int kn = i < e ? (int)__ldg(fb_k + i) : 0x7fffffff;
+    float4 vn = i < e ? __ldg(fb_v + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+    float acc[FB_W][SP_TY];
+#pragma unroll
+    for (int u = 0; u < FB_W; ++u)
+#pragma unroll
+        for (int t = 0; t < SP_TY; ++t) acc[u][t] = 0.0f;
+    for (int c0 = 0; c0 < kb; c0 += SP_CHUNK) {
+        const int cn = min(SP_CHUNK, kb - c0);
+        if (c0) __syncthreads();
+        stage(tile, sino, (int64_t)s * my + y0, kstride, ny, c0, cn);
+        __syncthreads();
+        while (kn < c0 + cn) {
+            const int k = kn;
+            const float4 v = vn;
+            ++i;
+            kn = i < e ? (int)__ldg(fb_k + i) : 0x7fffffff;
+            vn = i < e ? __ldg(fb_v + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 *t4 = reinterpret_cast<const float4 *>(tile + (k - c0) * SP_TYP);
+#pragma unroll
+            for (int w = 0; w < SP_TY / 4; ++w) {
+                const float4 z = t4[w];
+                const float zz[4] = {z.x, z.y, z.z, z.w};
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    acc[0][4 * w + h] = __fmaf_rn(v.x, zz[h], acc[0][4 * w + h]);
+                    acc[1][4 * w + h] = __fmaf_rn(v.y, zz[h], acc[1][4 * w + h]);
+                    acc[2][4 * w + h] = __fmaf_rn(v.z, zz[h], acc[2][4 * w + h]);
+                    acc[3][4 * w + h] = __fmaf_rn(v.w, zz[h], acc[3][4 * w + h]);
+                }
+            }
+        }
+    }
+    if (q < per_angle && m) {
+        const int cb = q / P, p = q - cb * P;
+        const int cp = C * P;
+        float *dl = data + ((int64_t)r * my + y0) * cp + p;
+#pragma unroll
+        for (int u = 0; u < FB_W; ++u) {
+            if (!((m >> u) & 1)) continue;
+            float *d = dl + (int64_t)(FB_W * cb + u) * P;
+#pragma unroll
+            for (int t = 0; t < SP_TY; ++t)
+                if (t < ny) d[(int64_t)t * cp] += acc[u][t];
+        }
     }
 }
 
@@ -189,8 +382,65 @@ extern "C" int dfx_spmm_pf_adjoint(const float *data, const int32_t *row_ptr, co
     DFX_REQUIRE(sino && row_ptr && col_j && val && data, "spmm_adjoint: null pointer");
     DFX_REQUIRE(n_sub > 0 && my > 0 && cp > 0 && kb > 0 && kb <= kstride, "spmm_adjoint: bad sizes");
     DFX_REQUIRE(n_sub <= 65535 && cdiv(my, SP_TY) <= 65535, "spmm_adjoint: grid too large");
-    dim3 grid((unsigned)cdiv(kstride, SP_ROWS), (unsigned)cdiv(my, SP_TY), (unsigned)n_sub);
-    spmm_adjoint_kernel<<<grid, SP_ROWS, 0, (cudaStream_t)stream>>>(data, row_ptr, col_j, val, sino, omegas, my, kb,
-                                                                    cp, kstride, alpha, compact);
+    DFX_REQUIRE(cdiv(my, AJ_TY) <= 65535, "spmm_adjoint: grid too large");
+    const int chunk = cp < AJ_MAX_CHUNK ? cp : AJ_MAX_CHUNK;
+    const size_t smem = (size_t)AJ_TY * chunk * sizeof(float);
+    const cudaError_t e = cudaFuncSetAttribute(spmm_adjoint8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)(AJ_TY * AJ_MAX_CHUNK * sizeof(float)));
+    if (e != cudaSuccess) {
+        set_error("spmm_adjoint: shared memory attribute: %s", cudaGetErrorString(e));
+        return DFX_ELAUNCH;
+    }
+    dim3 grid((unsigned)cdiv(kstride, AJ_ROWS), (unsigned)cdiv(my, AJ_TY), (unsigned)n_sub);
+    spmm_adjoint8_kernel<<<grid, AJ_ROWS, smem, (cudaStream_t)stream>>>(data, row_ptr, col_j, val, sino, omegas, my,
+                                                                        kb, cp, kstride, alpha, compact, chunk);
     return launch_status("spmm_pf_adjoint");
+}
+
+extern "C" int64_t dfx_pf_fblock_rows(int n_angles, int P, int C)
+{
+    return (int64_t)n_angles * P * cdiv(C, FB_W);
+}
+
+extern "C" int dfx_pf_fblock_count(const int32_t *row_ptr_f, const uint16_t *col_k, int n_angles, int P, int C,
+                                   int32_t *counts, uint8_t *mask, void *stream)
+{
+    DFX_REQUIRE(row_ptr_f && col_k && counts && mask, "pf_fblock_count: null pointer");
+    DFX_REQUIRE(n_angles > 0 && P > 0 && C > 0, "pf_fblock_count: bad sizes");
+    const int ncb = (int)cdiv(C, FB_W);
+    const int64_t n = dfx_pf_fblock_rows(n_angles, P, C);
+    DFX_REQUIRE(cdiv(n, 256) < 2147483647LL, "pf_fblock_count: too many rows");
+    fb_build_kernel<0><<<(unsigned)cdiv(n, 256), 256, 0, (cudaStream_t)stream>>>(
+        row_ptr_f, col_k, nullptr, n, P, C, ncb, counts, mask, nullptr, nullptr, nullptr);
+    return launch_status("pf_fblock_count");
+}
+
+extern "C" int dfx_pf_fblock_fill(const int32_t *row_ptr_f, const uint16_t *col_k, const float *val_f, int n_angles,
+                                  int P, int C, const int32_t *fb_ptr, uint16_t *fb_k, float *fb_v, void *stream)
+{
+    DFX_REQUIRE(row_ptr_f && col_k && val_f && fb_ptr && fb_k && fb_v, "pf_fblock_fill: null pointer");
+    DFX_REQUIRE(((uintptr_t)fb_v % 16) == 0, "pf_fblock_fill: the values must be 16-byte aligned");
+    DFX_REQUIRE(n_angles > 0 && P > 0 && C > 0, "pf_fblock_fill: bad sizes");
+    const int ncb = (int)cdiv(C, FB_W);
+    const int64_t n = dfx_pf_fblock_rows(n_angles, P, C);
+    fb_build_kernel<1><<<(unsigned)cdiv(n, 256), 256, 0, (cudaStream_t)stream>>>(
+        row_ptr_f, col_k, val_f, n, P, C, ncb, nullptr, nullptr, fb_ptr, fb_k, reinterpret_cast<float4 *>(fb_v));
+    return launch_status("pf_fblock_fill");
+}
+
+extern "C" int dfx_spmm_pf_forward_blocked(const float *sino, const int32_t *fb_ptr, const uint16_t *fb_k,
+                                           const float *fb_v, const uint8_t *fb_mask, float *data,
+                                           const int32_t *omegas, int n_sub, int my, int P, int C, int kstride, int kb,
+                                           void *stream)
+{
+    DFX_REQUIRE(sino && fb_ptr && fb_k && fb_v && fb_mask && data, "spmm_forward_blocked: null pointer");
+    DFX_REQUIRE(((uintptr_t)fb_v % 16) == 0, "spmm_forward_blocked: the values must be 16-byte aligned");
+    DFX_REQUIRE(n_sub > 0 && my > 0 && P > 0 && C > 0 && kb > 0 && kb <= kstride, "spmm_forward_blocked: bad sizes");
+    const int ncb = (int)cdiv(C, FB_W);
+    DFX_REQUIRE(n_sub <= 65535 && cdiv(my, SP_TY) <= 65535, "spmm_forward_blocked: grid too large");
+    dim3 grid((unsigned)cdiv((int64_t)P * ncb, SP_ROWS), (unsigned)cdiv(my, SP_TY), (unsigned)n_sub);
+    spmm_forward_b4_kernel<<<grid, SP_ROWS, 0, (cudaStream_t)stream>>>(
+        sino, fb_ptr, fb_k, reinterpret_cast<const float4 *>(fb_v), fb_mask, data, omegas, my, P, C, ncb, kstride,
+        kb);
+    return launch_status("spmm_pf_forward_blocked");
 }

@@ -431,10 +431,7 @@ class LocalSinglePhaseForwardOperator(SinglePhaseForwardOperator):
             if lb is None:
                 continue
             om, n_ang, Kb, m = self._project_local(coeffs, ib, subset)
-            rp, col, val, compact = self._pf_batch(ib, True, m)
-            self._call("dfx_spmm_pf_forward", self.coeffs_sino_C.data_ptr(), rp.data_ptr(), col.data_ptr(),
-                       val.data_ptr(), data.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My,
-                       self.N_seg, self.Kstride, Kb, compact, self._s())
+            self._pf_forward_product(ib, m, self.coeffs_sino_C.data_ptr(), data, om, n_ang, Kb)
 
     @on_op_stream
     def adjoint_cl(self, data, coeffs, subset=None):

@@ -48,6 +48,9 @@ class SinglePhaseForwardOperator:
 
     coefficient_layout = "dense"
     _pf_forward_csr = True
+    # with both CSR copies stored, the forward products run over an eta-blocked copy of the forward CSR (four
+    # neighbouring eta bins of a ring per entry; the same sums bit for bit); False: over the forward CSR itself
+    forward_blocks = True
 
     def __init__(self, cfg: Mapping[str, Any], material, grid, max_gb: float, verbose: bool = False,
                  normalized: bool = False, ctx=None, queue=None, pf_mode: str = "auto", sparse_max_fill: float = 0.3,
@@ -438,68 +441,173 @@ class SinglePhaseForwardOperator:
         self._csr(k0, kb, fwd, rows, row_ptr=rp, out=(col, val))
         return rp, col, val, nnz
 
+    def _make_fblock(self, rpf, ck, vf):
+        """The eta-blocked copy of a batch's stored forward CSR (dfx_pf_fblock_*): (fb_ptr, fb_k, fb_v, fb_mask);
+        the forward products over it are those over the CSR bit for bit, with a staged Z column feeding four
+        outputs."""
+        R, P, C = self.N_Omega, self.N_peaks, self.N_eta
+        s = self._s()
+        n = int(self._lib.dfx_pf_fblock_rows(R, P, C))
+        cnt = torch.empty(n + 1, dtype=torch.int32, device=self.device)
+        mask = torch.empty(n, dtype=torch.uint8, device=self.device)
+        self._call("dfx_pf_fblock_count", rpf.data_ptr(), ck.data_ptr(), R, P, C, cnt.data_ptr(), mask.data_ptr(), s)
+        nb = self._lib.dfx_scan_scratch_bytes(n)
+        scr = self.scratch(nb)
+        self._call("dfx_scan_exclusive_i32", cnt.data_ptr(), cnt.data_ptr(), n, scr.data_ptr(), nb, s)
+        total = max(int(cnt[n].item()), 1)
+        fk = torch.empty(total, dtype=torch.int16, device=self.device)         # uint16 bit pattern
+        fv = torch.empty((total, 4), dtype=torch.float32, device=self.device)
+        self._call("dfx_pf_fblock_fill", rpf.data_ptr(), ck.data_ptr(), vf.data_ptr(), R, P, C, cnt.data_ptr(),
+                   fk.data_ptr(), fv.data_ptr(), s)
+        return dict(fb_ptr=cnt, fb_k=fk, fb_v=fv, fb_mask=mask)
+
+    def _pf_forward_product(self, ib, m, sino_ptr, data, om, n_ang, kb):
+        """data rows += the forward PF product of batch ib's Radon output at sino_ptr (angles om, subset m): over the
+        eta-blocked copy when the batch stores it, else over the (stored or generated) forward CSR."""
+        sb = self.sparse_batches[ib]
+        s = self._s()
+        om_ptr = None if om is None else om.data_ptr()
+        if sb.get("fb_ptr") is not None:
+            self._call("dfx_spmm_pf_forward_blocked", sino_ptr, sb["fb_ptr"].data_ptr(), sb["fb_k"].data_ptr(),
+                       sb["fb_v"].data_ptr(), sb["fb_mask"].data_ptr(), data.data_ptr(), om_ptr, n_ang, self.My,
+                       self.N_peaks, self.N_eta, self.Kstride, kb, s)
+            return
+        rp, col, val, compact = self._pf_batch(ib, True, m)
+        self._call("dfx_spmm_pf_forward", sino_ptr, rp.data_ptr(), col.data_ptr(), val.data_ptr(), data.data_ptr(),
+                   om_ptr, n_ang, self.My, self.N_seg, self.Kstride, kb, compact, s)
+
     def build_sparse_pf(self, mode="auto", max_fill=0.3, max_gb=None, max_fill_partial=0.1):
-        """The sparse PF matrix per orientation batch (SPFO:1207-1373): the fill fraction of the first (dense-sized)
-        batch sets the sparse batch size; both CSR copies of every batch are stored if they fit in max_gb ("sparse"),
-        otherwise (and with mode "generated") the row pointers are kept and the entries are generated again in every
-        call. The structure is the dense batch's CSR, bit for bit (dfx_pf_csr_*)."""
+        """The sparse PF matrix per orientation batch (SPFO:1207-1373). The fill fraction of the first (dense-sized)
+        batch sets the sparse batch size. Then, within max_gb, in the reference's order of preference:
+          "both"      both CSR copies of every batch;
+          "adjoint"   the adjoint CSR of every batch, the forward copy generated again in every call;
+          partial     (mode "auto") the adjoint CSRs of the first batches that fit, the other batches generated in
+                      every call; mode "sparse" raises MemoryError instead;
+        mode "generated" stores nothing. Row pointers are always kept (4 bytes per row). A generated copy is the
+        stored one bit for bit: the structure and values are pure functions of the float32 entries (dfx_pf_csr_*).
+        An allocation that fails while storing (less free memory than the budget assumed) keeps half of what fitted
+        in mode "auto", as the reference does."""
         t0 = time.perf_counter()
         R, CP = self.N_Omega, self.N_seg
         if self.K_batch_max > 65535 or CP > 65535:
             raise ValueError(f"K_batch_max = {self.K_batch_max} or N_eta * N_rings = {CP} exceeds the 16-bit index "
                              "range of the sparse PF matrix; use a smaller max_gb")
+        auto = mode == "auto"
         b0 = self.batches[0]
         _, nnz0 = self._csr(b0["k_start"], b0["K_batch"], False)
         fill = nnz0 / (R * b0["K_batch"] * CP)
         self.sparse_fill_first = fill
-        if mode == "auto" and fill > max_fill:
+        if auto and fill > max_fill:
             warnings.warn(f"PF fill fraction {100 * fill:.1f} % > {100 * max_fill:.1f} %: the reference would apply the "
                           "dense matrix; the sparse products compute the same operator", stacklevel=2)
         self.get_pf_batches_for_material(K_batch=self.sparse_batch_size(fill))
         nb = len(self.batches)
-        est = [int(math.ceil(1.02 * fill * R * b["K_batch"] * CP)) + 16 for b in self.batches]
-        both = sum(12 * n for n in est) + nb * 4 * (R * CP + 1) + sum(4 * (R * b["K_batch"] + 1) for b in self.batches)
+        both, adj, ptr_f, batch_adj = self.sparse_estimates(fill)
         budget = np.inf if max_gb is None else max_gb * 1024 ** 3
-        store = mode in ("auto", "sparse") and both <= budget
-        if mode == "sparse" and not store:
-            raise MemoryError(f"Sparse PF matrix: estimated size {both / 1024 ** 3:.1f} GB > {max_gb:.1f} GB; use "
-                              "pf_mode='generated' or 'auto', or raise sparse_max_gb.")
+        if mode == "generated":
+            store, n_fit = None, 0
+        elif both <= budget and self._pf_forward_csr:
+            store, n_fit = "both", nb
+        elif adj <= budget:
+            store, n_fit = "adjoint", nb
+        elif not auto:
+            raise MemoryError(f"Sparse PF matrix: estimated size {adj / 1024 ** 3:.1f} GB (adjoint CSR only) > "
+                              f"{max_gb:.1f} GB; use pf_mode='generated' or 'auto', or raise sparse_max_gb.")
+        else:                                           # the adjoint CSRs of the first batches that fit
+            store, used_est, n_fit = "adjoint", nb * ptr_f, 0
+            for ib in range(nb):
+                used_est += batch_adj[ib]
+                if used_est > budget:
+                    break
+                n_fit += 1
         self.sparse_batches = []
-        self._gen_cap = 0
         nnz_total = 0
-        for b in self.batches:
+        stored_bytes = 0
+        for ib, b in enumerate(self.batches):
             k0, kb = b["k_start"], b["K_batch"]
-            if store:
-                rpa, cj, va, nnz = self._make_csr(k0, kb, False)
-                rpf, ck, vf, nnz_f = self._make_csr(k0, kb, True)
-                assert nnz_f == nnz, (nnz, nnz_f)
-                self.sparse_batches.append(dict(row_ptr_a=rpa, col_j=cj, val_a=va, row_ptr_f=rpf, col_k=ck, val_f=vf,
-                                                nnz=nnz))
-            else:
-                rpa, nnz = self._csr(k0, kb, False)
-                rpf, _ = self._csr(k0, kb, True)
-                self.sparse_batches.append(dict(row_ptr_a=rpa, row_ptr_f=rpf, nnz=nnz, generated=True))
-                self._gen_cap = max(self._gen_cap, nnz)
-            nnz_total += nnz
-        if not store:
+            sb = None
+            if store is not None and ib < n_fit:
+                try:
+                    rpa, cj, va, nnz = self._make_csr(k0, kb, False)
+                    sb = dict(row_ptr_a=rpa, col_j=cj, val_a=va, nnz=nnz)
+                    if store == "both":
+                        rpf, ck, vf, nnz_f = self._make_csr(k0, kb, True)
+                        assert nnz_f == nnz, (nnz, nnz_f)
+                        sb.update(row_ptr_f=rpf, col_k=ck, val_f=vf)
+                        if self.forward_blocks:
+                            sb.update(self._make_fblock(rpf, ck, vf))
+                    else:
+                        sb["row_ptr_f"], _ = self._csr(k0, kb, True)
+                    torch.cuda.synchronize(self.device)
+                except torch.cuda.OutOfMemoryError:
+                    if not auto:
+                        raise
+                    # less free memory than the budget assumed: keep half of what fitted, generate the rest
+                    sb = None
+                    keep = ib // 2
+                    for j in range(keep, ib):
+                        self.sparse_batches[j] = self._generated_entry(j)
+                    n_fit = keep
+                    torch.cuda.empty_cache()
+            if sb is None:
+                sb = self._generated_entry(ib)
+            self.sparse_batches.append(sb)
+            nnz_total += sb["nnz"]
+        self._gen_cap = max([sb["nnz"] for sb in self.sparse_batches
+                             if not (self._stored(sb, True) and self._stored(sb, False))] or [0])
+        self._gen_col = self._gen_val = None
+        if self._gen_cap:
             n = max(self._gen_cap, 1)
             self._gen_col = torch.empty(n, dtype=torch.int16, device=self.device)
             self._gen_val = torch.empty(n, dtype=torch.float32, device=self.device)
-        self.pf_mode = "sparse" if store else "generated"
-        self.pf_storage = "both" if store else "none"
+        stored = [ib for ib, sb in enumerate(self.sparse_batches) if sb.get("col_j") is not None]
+        for sb in self.sparse_batches:
+            stored_bytes += sum(t.numel() * t.element_size() for k, t in sb.items() if torch.is_tensor(t))
+        self.pf_mode = "sparse" if len(stored) == nb else "generated"
+        if not stored:
+            self.pf_storage = "none"
+        else:
+            self.pf_storage = store + (f", {len(stored)} of {nb} batches" if len(stored) < nb else "")
+        self.pf_stored_bytes = stored_bytes
         self.sparse_nnz = nnz_total
         self.sparse_fill = nnz_total / (R * self.K * CP)
         self.pf_setup_s = time.perf_counter() - t0
         if self.verbose:
             print(f"Sparse PF matrix: {nnz_total} non-zeros (fill {100 * self.sparse_fill:.3f} %), {nb} batches of up "
-                  f"to {self.K_batch_max}, stored: {self.pf_storage}; set up in {self.pf_setup_s:.2f} s")
+                  f"to {self.K_batch_max}, stored: {self.pf_storage} ({stored_bytes / 1024 ** 2:.1f} MB); set up in "
+                  f"{self.pf_setup_s:.2f} s")
+
+    def sparse_estimates(self, fill):
+        """Estimated bytes of the sparse PF matrix at a fill fraction, for the current batches: (both CSR copies,
+        the adjoint copies only, the forward row pointers of one batch, [adjoint copy of batch ib: row pointers +
+        6 bytes per non-zero]); every copy includes its row pointers (4 bytes per row)."""
+        R, CP = self.N_Omega, self.N_seg
+        est = [int(math.ceil(1.02 * fill * R * b["K_batch"] * CP)) + 16 for b in self.batches]
+        nb = len(self.batches)
+        ptr_f = 4 * (R * CP + 1)
+        ptr_a = [4 * (R * b["K_batch"] + 1) for b in self.batches]
+        batch_adj = [pa + 6 * n for pa, n in zip(ptr_a, est)]
+        both = sum(12 * n for n in est) + nb * ptr_f + sum(ptr_a)
+        return both, sum(batch_adj) + nb * ptr_f, ptr_f, batch_adj
+
+    def _generated_entry(self, ib):
+        """A batch whose CSR copies are generated in every call: its row pointers and non-zero count."""
+        b = self.batches[ib]
+        rpa, nnz = self._csr(b["k_start"], b["K_batch"], False)
+        rpf, _ = self._csr(b["k_start"], b["K_batch"], True)
+        return dict(row_ptr_a=rpa, row_ptr_f=rpf, nnz=nnz)
+
+    @staticmethod
+    def _stored(sb, forward):
+        return sb.get("col_k" if forward else "col_j") is not None
 
     def _pf_batch(self, ib, forward, m=None):
-        """(row_ptr, col, val, compact) of batch ib for the forward or adjoint product; m: subset (its rows)."""
+        """(row_ptr, col, val, compact) of batch ib for the forward or adjoint product; m: subset (its rows). A copy
+        that is not stored is generated into the operator's scratch (the subset's rows only, for a subset)."""
         sb = self.sparse_batches[ib]
         b = self.batches[ib]
         key = "f" if forward else "a"
-        if not sb.get("generated"):
+        if self._stored(sb, forward):
             return sb["row_ptr_" + key], sb["col_k" if forward else "col_j"], sb["val_" + key], 0
         if m is None:
             rp, rows, compact = sb["row_ptr_" + key], None, 0
@@ -677,7 +785,7 @@ class SinglePhaseForwardOperator:
             entry = dict(omegas=om, geo=geo, n=len(s), row_ptr=None)
             if self.projector == "fft":
                 entry["fft"] = self._fft.subset(s)
-            if any(sb.get("generated") for sb in self.sparse_batches):
+            if any(not (self._stored(sb, True) and self._stored(sb, False)) for sb in self.sparse_batches):
                 entry["row_ptr"] = []
                 for b in self.batches:
                     rpa, nnz = self._csr(b["k_start"], b["K_batch"], False, om)
@@ -740,10 +848,7 @@ class SinglePhaseForwardOperator:
             geo, n_ang, om = e["geo"], e["n"], e["omegas"]
         self._call("dfx_gather_channels", src.data_ptr(), self._img_k.data_ptr(), self.npix, k_src, Kb, self.Kstride, s)
         self._radon_fwd(self._img_k.data_ptr(), self.coeffs_sino_C.data_ptr(), om, n_ang, Kb, m=m)
-        rp, col, val, compact = self._pf_batch(ib, True, m)
-        self._call("dfx_spmm_pf_forward", self.coeffs_sino_C.data_ptr(), rp.data_ptr(), col.data_ptr(),
-                   val.data_ptr(), data.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My,
-                   self.N_seg, self.Kstride, Kb, compact, s)
+        self._pf_forward_product(ib, m, self.coeffs_sino_C.data_ptr(), data, om, n_ang, Kb)
 
     @on_op_stream
     def adjoint_cl(self, data, coeffs, subset=None):
@@ -795,10 +900,7 @@ class SinglePhaseForwardOperator:
         s = self._s()
         geo, n_ang, om, m = self._geo_of(subset)
         self._radon_fwd(src_ptr, self.coeffs_sino_C.data_ptr(), om, n_ang, Kb, ray=ray, m=m)
-        rp, col, val, compact = self._pf_batch(ib, True, m)
-        self._call("dfx_spmm_pf_forward", self.coeffs_sino_C.data_ptr(), rp.data_ptr(), col.data_ptr(),
-                   val.data_ptr(), data.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My,
-                   self.N_seg, self.Kstride, Kb, compact, s)
+        self._pf_forward_product(ib, m, self.coeffs_sino_C.data_ptr(), data, om, n_ang, Kb)
 
     def _pf_adjoint_to_sino(self, data, ib, subset):
         Kb = self.batches[ib]["K_batch"]

@@ -217,6 +217,27 @@ int dfx_spmm_pf_adjoint(const float *data, const int32_t *row_ptr, const uint16_
                         float *sino, const int32_t *omegas, int n_sub, int my, int kb, int cp, int kstride,
                         float alpha, int compact, void *stream);
 
+/* The forward CSR of a batch regrouped into eta blocks (used by dfx_spmm_pf_forward_blocked in place of
+ * spmm_pf_forward_c, pf_kernels.cl:597-641): block row g = r * P * ncb + cb * P + p (ncb = ceil(C / 4)) merges the
+ * forward rows of the eta bins c = 4 cb .. 4 cb + 3 of ring p (j = c * P + p) into one list of orientations k
+ * ascending, each entry holding k (uint16) and four values (float4; 0 where that bin's row has no entry k).
+ * dfx_pf_fblock_rows: the number of block rows; dfx_pf_fblock_count: counts[g] (entries) and mask[g] (bit u: the row
+ * of bin 4 cb + u has entries); after an exclusive scan of counts into fb_ptr (rows + 1 entries), dfx_pf_fblock_fill
+ * writes fb_k and fb_v (16-byte aligned). */
+int64_t dfx_pf_fblock_rows(int n_angles, int P, int C);
+int dfx_pf_fblock_count(const int32_t *row_ptr_f, const uint16_t *col_k, int n_angles, int P, int C, int32_t *counts,
+                        uint8_t *mask, void *stream);
+int dfx_pf_fblock_fill(const int32_t *row_ptr_f, const uint16_t *col_k, const float *val_f, int n_angles, int P, int C,
+                       const int32_t *fb_ptr, uint16_t *fb_k, float *fb_v, void *stream);
+
+/* replaces spmm_pf_forward_c / spmm_pf_forward_sub (pf_kernels.cl:597-641, SPFO:38-80) over the eta-blocked rows of a
+ * batch: data[omegas[s], y, j] += sum_k val * sino[s, y, k] for the n_sub angles omegas (NULL: all), C eta bins and P
+ * rings; the bins whose forward row is empty are left untouched. The same sums as dfx_spmm_pf_forward on the batch's
+ * forward CSR, bit for bit (over k ascending from 0, fused multiply-adds; a zero value adds exactly 0). */
+int dfx_spmm_pf_forward_blocked(const float *sino, const int32_t *fb_ptr, const uint16_t *fb_k, const float *fb_v,
+                                const uint8_t *fb_mask, float *data, const int32_t *omegas, int n_sub, int my, int P,
+                                int C, int kstride, int kb, void *stream);
+
 /* replaces zero_rows (SPFO:126-132): data rows omegas[s] (row_len floats each) <- 0. */
 int dfx_zero_rows(float *data, const int32_t *omegas, int n_sub, int64_t row_len, void *stream);
 

@@ -10,6 +10,7 @@ and the SPDHG iteration of the reference (functions cite the reference file:line
                     compacted into the two CSR copies (pf_kernels.cl:482-548)
   spdhg_reference   SPDHGPoisson.run (optimization/spdhg_poisson.py:513-751) for GPU-resident arrays (float32 state,
                     float64 prox and sums, as the reference), with the TV block
+  fista_poisson_reference  FISTAPoisson.run (optimization/fista_poisson.py:414-610) for arrays on the device
   spdhg_reference64 the same loop entirely in float64 (state, data, images, step sizes): the FP64 oracle that the
                     float32 and BF16 paths' errors are stated against
   chambolle_pock_poisson_tv   a float64 primal-dual solve of the Poisson + (hierarchical) TV problem on explicit
@@ -513,6 +514,149 @@ def spdhg_reference64(op: OracleOperator, subsets, b, n_epochs, x0=None, weights
             seq = nseq
     return (x.reshape(K, op.Ny, op.Nx), y.reshape(dshape), z.reshape(K, op.Ny, op.Nx), devs, rho,
             {"S": S.reshape(dshape), "T": T.reshape(K, op.Ny, op.Nx)})
+
+
+def fista_poisson_reference(op: OracleOperator, b, niter, x0=None, weights=None, gain=None, background=None,
+                            support=None, lam=0.0, eps_counts=1e-3, floor_counts=1.0,
+                            refresh=(5, 10, 20, 40, 80, 160, 320, 640, 1280, 2560, 5120), refresh_on_failure=True,
+                            max_backtracks=60, start="wls", n_start=20):
+    """FISTAPoisson.run for arrays on the device (fista_poisson.py:414-610; kernels 60-282): FISTA in the diagonal
+    SQS metric D = 1 / A^T(c A 1_S) with descent-lemma backtracking, a metric taken again at y on the first rejected
+    step, function-value restarts, metric refreshes with momentum restarts at the iterations in `refresh`, the
+    weighted least squares start phase (mode 1) from a zero x0, float32 arrays and float64 sums as the reference.
+    Returns (x (K, Ny, Nx) float32, [per-iteration dict: f, obj, theta, backtracks, restart, metric_refresh,
+    local_metric], final dict: final_f, final_obj, adjoint_scale, backtracks, restarts)."""
+    f32, f64 = np.float32, np.float64
+    dshape = (op.R, op.My, op.CP)
+    K, npix = op.K, op.Nx * op.Ny
+    b = _c(b, f32).ravel()
+    n = b.size
+    wv = np.ones(n, f32) if weights is None else np.resize(_c(weights, f32).ravel(), n)
+    gv = np.ones(n, f32) if gain is None else np.resize(_c(gain, f32).ravel(), n)
+    bgv = np.zeros(n, f32) if background is None else np.resize(_c(background, f32).ravel(), n)
+    supp = np.ones(npix, bool) if support is None else np.asarray(support, bool).ravel()
+    eps = f32(eps_counts)
+    floor = f32(floor_counts)
+    counted = wv != 0
+    fwd = lambda v: op.forward(v.reshape(K, op.Ny, op.Nx)).ravel().astype(f32)
+    adj = lambda d: op.adjoint(d.reshape(dshape)).ravel().astype(f32)
+    inside = np.broadcast_to(supp, (K, npix)).ravel()
+
+    def data_term(mu, mode, want_grad):
+        """f (float64) and, with want_grad, df/dmu (float32): poisson_value_grad (fista_poisson.py:71-101)."""
+        sc = wv.astype(f64) / gv.astype(f64)
+        bi = b.astype(f64)
+        if mode == 0:
+            m = np.maximum(mu, f32(0)).astype(f64) + bgv.astype(f64) + f64(eps) * gv.astype(f64)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                v = m - bi + np.where(bi > 0, bi * np.log(np.where(bi > 0, bi, 1.0) / m), 0.0)
+                gr = sc * (1.0 - bi / m)
+        else:
+            r = mu.astype(f64) + bgv.astype(f64) - bi
+            c = sc / np.maximum(bi, f64(floor) * gv.astype(f64))
+            v = 0.5 * c * r * r
+            gr = c * r
+        f = float(np.sum(np.where(counted, sc * v if mode == 0 else v, 0.0)))
+        return f, (np.where(counted, gr, 0.0).astype(f32) if want_grad else None)
+
+    state = {"adjoint_scale": 1.0}
+
+    def metric(mu, mode):
+        """D (float32): times_curvature, the adjoint, invert_metric (fista_poisson.py:103-134, 170-178, 384-411)."""
+        ones = inside.astype(f32)
+        u = fwd(ones)
+        if mode == 0:
+            m = np.maximum(np.maximum(mu, f32(0)) + bgv, floor * gv)
+            c = np.where(counted, wv / gv * np.maximum(b, m) / (m * m), f32(0)).astype(f32)
+        else:
+            c = np.where(counted, wv / (gv * np.maximum(b, floor * gv)), f32(0)).astype(f32)
+        u_r = float(np.sum(c.astype(f64) * u.astype(f64) * u.astype(f64)))
+        u = (u * c).astype(f32)
+        d = adj(u)
+        at_u = float(np.sum(np.where(inside, d.astype(f64), 0.0)))
+        if u_r > 0 and at_u > 0:
+            state["adjoint_scale"] = at_u / u_r
+        with np.errstate(divide="ignore"):
+            return np.where(inside & (d > 0), f32(1) / d, f32(0)).astype(f32)
+
+    x = np.zeros(K * npix, f32) if x0 is None else _c(x0, f32).ravel().copy()
+    x[~inside] = 0
+    x = np.maximum(x, f32(0))
+    zero_start = float(x.max()) == 0.0
+    wls_until = n_start if (start == "wls" and n_start > 0 and zero_start) else 0
+    mode = 1 if wls_until else 0
+    if zero_start and start == "uniform":
+        ones = inside.astype(f32)
+        a1 = fwd(ones)
+        sb = float(np.sum(wv.astype(f64) * b.astype(f64)))
+        sa = float(np.sum(wv.astype(f64) * a1.astype(f64)))
+        if sa > 0 and sb > 0:
+            x = (ones * f32(sb / sa)).astype(f32)
+    t_mom, theta = 1.0, 1.0
+    y = x.copy()
+    Ax = fwd(x)
+    Ay = Ax.copy()
+    D = metric(Ax, mode)
+    f_x, _ = data_term(Ax, mode, False)
+    F_x = f_x + lam * float(np.sum(x.astype(f64)))
+    stats = []
+    n_bt_total = n_restart = 0
+    for k in range(niter):
+        it = k + 1
+        f_y, gmu = data_term(Ay, mode, True)
+        grad = adj(gmu)
+        theta = min(1.0, 2.0 * theta)
+        n_bt, local = 0, False
+        while True:
+            xn = np.where(D > 0, np.maximum(f32(0), y - f32(theta) * D * (grad + f32(lam))), f32(0)).astype(f32)
+            Axn = fwd(xn)
+            f_n, _ = data_term(Axn, mode, False)
+            dd = xn.astype(f64) - y.astype(f64)
+            lin_adj = float(np.sum(grad.astype(f64) * dd))
+            quad_raw = float(np.sum(np.where(D > 0, dd * dd / np.where(D > 0, D, 1).astype(f64), 0.0)))
+            xsum = float(np.sum(xn.astype(f64)))
+            lin = lin_adj / state["adjoint_scale"]
+            quad = quad_raw / (theta * state["adjoint_scale"])
+            if f_n <= f_y + lin + 0.5 * quad + 1e-6 * abs(f_y) or quad == 0.0:
+                break
+            n_bt += 1
+            if not local and refresh_on_failure:
+                D = metric(fwd(y), mode)
+                local, theta = True, 1.0
+                continue
+            theta *= 0.5
+            if n_bt > max_backtracks:
+                raise RuntimeError("fista_poisson_reference: no sufficient decrease")
+        n_bt_total += n_bt
+        F_n = f_n + lam * xsum
+        restarted = F_n > F_x
+        if restarted:
+            t_mom = 1.0
+            n_restart += 1
+        t_new = 0.5 * (1.0 + np.sqrt(1.0 + 4.0 * t_mom * t_mom))
+        beta = f32((t_mom - 1.0) / t_new)
+        t_mom = t_new
+        y = (xn + beta * (xn - x)).astype(f32)
+        Ay = (Axn + beta * (Axn - Ax)).astype(f32)
+        x, Ax = xn, Axn
+        f_x, F_x = f_n, F_n
+        switch = mode == 1 and it >= wls_until
+        if switch:
+            mode = 0
+            f_x, _ = data_term(Ax, mode, False)
+            F_x = f_x + lam * xsum
+        refreshed = (it in refresh or switch) and k + 1 < niter and mode == 0
+        if refreshed:
+            D = metric(Ax, mode)
+            t_mom, theta = 1.0, 1.0
+            y, Ay = x.copy(), Ax.copy()
+        elif it % 50 == 0:
+            Ay = fwd(y)
+        stats.append({"iter": it, "f": f_n, "obj": F_n, "theta": theta, "backtracks": n_bt, "local_metric": local,
+                      "restart": bool(restarted), "metric_refresh": bool(refreshed)})
+    final = {"final_f": f_x, "final_obj": F_x, "adjoint_scale": state["adjoint_scale"], "backtracks": n_bt_total,
+             "restarts": n_restart}
+    return x.reshape(K, op.Ny, op.Nx), stats, final
 
 
 def fista_ls_reference(op: OracleOperator, b, niter, tau, x0=None, prox="nonneg", lam=0.0, support=None, clip=False,

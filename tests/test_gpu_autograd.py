@@ -1,7 +1,8 @@
 """The forward operator as a torch.autograd.Function: gradients are the hand-written adjoint, checked against float64
 finite differences of the oracle's forward model, the adjoint identity on 100 random pairs at the shape of the
-differentiable configuration (bcc Fe, 128 x 128 pixels, 180 angles, 133 translations, 120 eta bins, 5 rings, 5 %
-support; fewer orientations so the test runs in seconds), a batch of slices, and the subset form."""
+differentiable configuration (bcc Fe, 128 x 128 pixels, 180 angles, 133 translations, 120 eta bins, 5 rings,
+K = 5000, 5 % support), a batch of slices, the subset form, and an operator whose PF matrix is generated again in
+every call (memory-bounded: nothing stored, or only some batches) giving the same values and gradients."""
 import numpy as np
 import pytest
 
@@ -45,7 +46,7 @@ def test_gradient_is_adjoint_and_matches_float64_finite_differences(golden):
         assert abs(an - fd) <= 1e-5 * abs(fd), (an, fd)
 
 
-def _fe_config_operator(K=400):
+def _fe_config_operator(K=5000, **kw):
     from diffractom_b200 import Grid, Material, SinglePhaseForwardOperator
     cfg = dict(Nx=128, Ny=128, My=133, N_Omega=180, angle_range=[0, 180], cor_offset=0.0, N_eta=120,
                eta_angle_range=[0, 360], energy=12.398 / 0.3, k_direction_0=[0, 0, 1], p_direction_0=[1, 0, 0],
@@ -53,7 +54,7 @@ def _fe_config_operator(K=400):
     mat = Material.from_lattice_parameters(a=2.87, symmetry_group="cubic", wavelength_A=0.3,
                                            hkl_list=[[1, 1, 0], [2, 0, 0], [2, 1, 1], [2, 2, 0], [3, 1, 0]])
     grid = Grid.from_random_fundamental_zone(K, mat.crystal_system, np.deg2rad(3.0), seed=4)
-    return SinglePhaseForwardOperator(cfg, mat, grid, 0.5, normalized=True)
+    return SinglePhaseForwardOperator(cfg, mat, grid, 0.5, normalized=True, **kw)
 
 
 def test_adjoint_identity_100_pairs_and_slice_batch():
@@ -105,3 +106,29 @@ def test_subset_rows_and_their_gradient(golden):
         forward_operator(op, x.detach().double())
     with pytest.raises(ValueError):
         forward_operator(op, torch.zeros((2, 3), device="cuda"))
+
+
+def test_memory_bounded_operator_gives_the_same_values_and_gradients():
+    """At the Fe configuration (K = 5000), an operator that keeps no PF matrix (pf_mode "generated": the blocks are
+    made again in every call) and one that stores only the first batches (a storage budget below the matrix) give
+    the stored operator's forward values and gradients bit for bit."""
+    from diffractom_b200.autograd import forward_operator
+    stored = _fe_config_operator(pf_mode="sparse")
+    assert stored.pf_storage == "both"
+    both, adj, ptr_f, batch_adj = stored.sparse_estimates(stored.sparse_fill_first)
+    part_gb = (len(stored.batches) * ptr_f + batch_adj[0] + 1) / 1024.0 ** 3
+    ops = [_fe_config_operator(pf_mode="generated"), _fe_config_operator(pf_mode="auto", sparse_max_gb=part_gb)]
+    assert ops[0].pf_storage == "none" and ops[1].pf_storage.startswith("adjoint, 1 of")
+    g = torch.Generator(device="cuda").manual_seed(21)
+    supp = torch.as_tensor(stored.support_mask(), device="cuda")
+    x0 = (torch.rand(stored.coeff_shape, generator=g, device="cuda") < 0.05) * supp * \
+        torch.rand(stored.coeff_shape, generator=g, device="cuda")
+    gy = torch.rand(stored.data_shape, generator=g, device="cuda")
+    out = []
+    for op in [stored] + ops:
+        x = x0.clone().requires_grad_(True)
+        y = forward_operator(op, x)
+        y.backward(gy)
+        out.append((y.detach(), x.grad))
+    for y, gx in out[1:]:
+        assert torch.equal(y, out[0][0]) and torch.equal(gx, out[0][1])

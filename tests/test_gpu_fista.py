@@ -87,3 +87,28 @@ def test_fista_resume_and_numpy(golden):
         FISTAPoisson(op, prox_kind="l1")
     with pytest.raises(ValueError):
         FISTAPoisson(op).run(np.zeros(op.coeff_shape, np.float32), b, 1, gain=np.zeros(op.N_seg, np.float32))
+
+
+@pytest.mark.parametrize("start,gain", [("wls", 0.05), ("uniform", None), ("x0", 0.05)])
+def test_fista_poisson_iterates_match_the_oracle_loop(golden, start, gain):
+    """FISTAPoisson against oracle.fista_poisson_reference (the reference's loop, fista_poisson.py:414-610, on the
+    oracle operator with float32 arrays and float64 sums) iteration by iteration: the same backtracking, restart
+    and metric-refresh decisions, every iteration's deviance to 1e-5 and the final x to 1e-4 of its maximum; through
+    the weighted least squares start, the switch to the deviance and two metric refreshes."""
+    from diffractom_b200 import FISTAPoisson
+    from oracle.oracle import OracleOperator, fista_poisson_reference
+    op, b, g = _problem(golden, seed=11)
+    gain = None if gain is None else g
+    rng = np.random.default_rng(5)
+    x0 = (np.zeros(op.coeff_shape, np.float32) if start != "x0" else
+          (rng.random(op.coeff_shape) * op.support_mask()[None]).astype(np.float32))
+    fs = FISTAPoisson(op, start=start, n_start=4)
+    x = fs.run(torch.as_tensor(x0, device="cuda"), b, 12, gain=gain).cpu().numpy()
+    orc = OracleOperator.from_operator(op)
+    xr, st, fin = fista_poisson_reference(orc, b, 12, x0=x0, gain=gain, support=op.support_mask(), start=start,
+                                          n_start=4)
+    keys = ("backtracks", "restart", "metric_refresh", "local_metric")
+    assert [[s[k] for k in keys] for s in fs.iter_stats] == [[s[k] for k in keys] for s in st]
+    np.testing.assert_allclose([s["f"] for s in fs.iter_stats], [s["f"] for s in st], rtol=1e-5)
+    assert abs(fs.final_stats["adjoint_scale"] / fin["adjoint_scale"] - 1) < 1e-5
+    assert np.abs(x - xr).max() <= 1e-4 * np.abs(xr).max()

@@ -244,3 +244,41 @@ def test_dense_pf_mode_runs_the_sparse_products(golden):
     sparse = make_operator(d, pf_mode="sparse")
     assert dense.pf_mode == "sparse"
     assert np.array_equal(dense.direct(d["c"]), sparse.direct(d["c"]))
+
+
+def test_pf_storage_modes_compute_the_same_operator(golden):
+    """The PF storage preferences of build_sparse_pf (SPFO:1207-1373): both CSR copies, the adjoint copies only (the
+    forward copy generated in every call), the adjoint copies of the first batches (mode "auto" within a budget that
+    holds only some; the others generated in every call), nothing stored; full and subset products are the same bits
+    in every mode. Mode "sparse" with a budget below the adjoint copies raises MemoryError."""
+    d = golden("al5_small")
+    ref = make_operator(d, pf_mode="sparse")
+    assert ref.pf_storage == "both" and len(ref.batches) >= 3
+    both, adj, ptr_f, batch_adj = ref.sparse_estimates(ref.sparse_fill_first)
+    gb = 1024.0 ** 3
+    part = (len(ref.batches) * ptr_f + batch_adj[0] + batch_adj[1] + 1) / gb   # room for two batches' adjoints
+    ops = {"adjoint": make_operator(d, pf_mode="auto", sparse_max_gb=(adj + 1) / gb),
+           "partial": make_operator(d, pf_mode="auto", sparse_max_gb=part),
+           "generated": make_operator(d, pf_mode="generated")}
+    assert ops["adjoint"].pf_storage == "adjoint"
+    assert ops["partial"].pf_storage == f"adjoint, 2 of {len(ref.batches)} batches"
+    assert ops["generated"].pf_storage == "none"
+    rng = np.random.default_rng(2)
+    x = torch.as_tensor(rng.random(ref.coeff_shape).astype(np.float32), device="cuda")
+    y = torch.as_tensor(rng.random(ref.data_shape).astype(np.float32), device="cuda")
+    outs = {}
+    for name, op in [("both", ref)] + list(ops.items()):
+        assert [b["K_batch"] for b in op.batches] == [b["K_batch"] for b in ref.batches]
+        op.set_omega_subsets(3)
+        fx, ay = torch.empty_like(y), torch.empty_like(x)
+        op.direct_cl(x, fx)
+        op.adjoint_cl(y, ay)
+        fs, as_ = torch.zeros_like(y), torch.empty_like(x)
+        op.direct_cl(x, fs, subset=1)
+        op.adjoint_cl(y, as_, subset=2)
+        outs[name] = [t.cpu().numpy() for t in (fx, ay, fs, as_)]
+    for name in ops:
+        for a, b in zip(outs[name], outs["both"]):
+            assert np.array_equal(a, b), name
+    with pytest.raises(MemoryError):
+        make_operator(d, pf_mode="sparse", sparse_max_gb=part)

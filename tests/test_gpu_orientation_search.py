@@ -95,3 +95,43 @@ def test_score_candidates_equals_direct_scores(golden):
         for s in range(len(masks)):
             assert np.array_equal(out[j]["z"][s], np.take_along_axis(z[s].T, out[j]["idx"], 1))
         assert np.all(np.diff(out[j]["z"][0], axis=1) <= 0)
+
+
+def test_refine_candidates_moves_a_candidate_to_the_missing_crystal():
+    """A crystal missing from the model (data = its forward plus a flat background, prediction = the background) and a
+    candidate on its tiles started 3 deg away: refine_candidates (two rotation lattices, scores through a local-basis
+    operator's adjoint on the fitted angles) brings it within 0.6 deg of the truth."""
+    from scipy.spatial.transform import Rotation
+
+    from diffractom_b200 import Material, SinglePhaseForwardOperator
+    from diffractom_b200.grid import MatrixGrid
+    from diffractom_b200.local import LocalSinglePhaseForwardOperator, LocalSupport
+    from diffractom_b200.orientation_search import Candidates, poisson_score_inputs, refine_candidates
+    cfg = dict(Nx=24, Ny=24, My=27, N_Omega=60, angle_range=[0, 180], cor_offset=0.0, N_eta=72,
+               eta_angle_range=[0, 360], energy=12.398 / 0.3, k_direction_0=[0, 0, 1], p_direction_0=[1, 0, 0],
+               detector_direction_origin=[0, -1, 0], detector_direction_positive_90=[0, 0, -1])
+    mat = Material.from_lattice_parameters(a=4.05, symmetry_group="cubic", wavelength_A=0.3,
+                                           hkl_list=[[1, 1, 1], [2, 0, 0], [2, 2, 0], [3, 1, 1]])
+    U = Rotation.from_euler("zxz", [30, 40, 50], degrees=True).as_matrix()[None]
+    truth = SinglePhaseForwardOperator(cfg, mat, MatrixGrid(U, np.deg2rad([1.0])), 0.1, normalized=True)
+    x = np.zeros(truth.coeff_shape, np.float32)
+    x[0, 8:16, 4:12] = 1.0                                     # the grain: tiles (2..3, 1..2) of 4-voxel tiles
+    bg = np.float32(0.5)
+    mu_true = truth.direct(torch.as_tensor(x, device="cuda")).cpu().numpy() * 200 + bg
+    b = np.random.default_rng(3).poisson(mu_true).astype(np.float32)
+    mu = np.full(b.shape, bg, np.float32)
+    e, d = poisson_score_inputs(b, mu, 1.0, np.ones(truth.N_seg, np.float32))
+    off = Rotation.from_rotvec(np.deg2rad([2.0, -1.5, 1.2])).as_matrix()
+    cand = Candidates((U[0] @ off)[None], np.array([1.0]), [np.array([13, 14, 19, 20])], (6, 6))
+    rows = np.ones(truth.N_Omega, bool)
+    rows[::5] = False
+
+    def make(rots, sigs, k, iy, ix):
+        sup = LocalSupport(k, iy, ix, len(rots), (cfg["Ny"], cfg["Nx"]))
+        return LocalSinglePhaseForwardOperator(cfg, mat, MatrixGrid(rots, sigs), 0.1, sup, normalized=True)
+
+    out = refine_candidates(make, cand, e, d, rows, 4, (cfg["Ny"], cfg["Nx"]))
+    mis = np.degrees(Rotation.from_matrix(U[0].T @ out.rotations[0]).magnitude())
+    start = np.degrees(Rotation.from_matrix(U[0].T @ cand.rotations[0]).magnitude())
+    assert mis < 0.6 < start, (start, mis)
+    assert out.tiles is cand.tiles and np.array_equal(out.score, cand.score)
