@@ -277,7 +277,9 @@ def main():
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="ti256", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="ti256", choices=sorted(WORKLOADS) + ["ni512"],
+                    help="ni512: the large tailored-grid slice (Fourier-slice projector, BF16 contraction, streamed "
+                    "T); its own JSON line")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the short serving run of the default line")
@@ -303,6 +305,10 @@ def main():
     if a.impl == "reference":
         return run_reference(a, rank)
     torch.cuda.set_device(local)
+    if a.workload == "ni512":
+        if rank == 0:
+            print(json.dumps(ni512_run(a.steps, a.warmup, a.K)), flush=True)
+        return 0
     if a.projectors:
         if rank == 0:
             print(json.dumps(projector_run(a.K or 256, a.steps, a.warmup)), flush=True)
@@ -646,6 +652,19 @@ def algorithmic_work(op, name, args_list):
             n_sub, my, cp, cp_pad = args[3], args[4], args[5], args[6]
             nb.append(n_sub * my * (4 * cp + 2 * cp_pad))
             nf.append(0)
+        elif name in ("dfx_fr_forward", "dfx_fr_backward"):
+            # the channel-fastest images in or out and the sinogram rows out or in (the transforms' intermediates
+            # are not algorithmic traffic)
+            n_ang, kb = args[0]._obj.R, args[4]
+            nb.append(4 * kb * (npix + n_ang * My))
+            nf.append(0)
+        elif name == "dfx_pf_dense_bf16_rows":
+            n_rows, kb, cp_pad = args[2], args[4], args[7]
+            nb.append(2 * n_rows * kb * cp_pad)
+            nf.append(0)
+        elif name == "dfx_convert_rows":
+            nb.append(6 * args[5] * args[6])
+            nf.append(0)
         elif name in ("dfx_gather_channels", "dfx_scatter_channels"):
             nb.append(2 * 4 * npix * args[4])
             nf.append(0)
@@ -679,6 +698,130 @@ LARGE_SLICE = dict(cfg=dict(Nx=512, Ny=512, My=520, N_Omega=720, angle_range=[0,
                    material=dict(a=3.52, symmetry_group="cubic", wavelength_A=0.3,
                                  hkl_list=[[1, 1, 1], [2, 0, 0], [2, 2, 0], [3, 1, 1], [2, 2, 2], [4, 0, 0]]),
                    sigma_deg=1.0, subsets=36)
+
+
+def clustered_grid(K, clusters, sigma, symmetry, seed=0):
+    """K orientations in seeded clusters (a tailored grid around candidate orientations): uniformly random centres,
+    each member rotated from its centre about a uniformly random axis by |N(0, sigma)|, reduced to the fundamental
+    zone; the clusters are contiguous in the grid's order (so that orientation batches hold whole clusters)."""
+    from diffractom_b200.grid import Grid, random_rotations, reduce_to_fundamental_zone
+    rng = np.random.default_rng(seed)
+    centres = random_rotations(clusters, rng)
+    owner = np.sort(np.arange(K) % clusters)
+    ax = rng.standard_normal((K, 3))
+    ax /= np.linalg.norm(ax, axis=1, keepdims=True)
+    ang = np.abs(rng.standard_normal(K)) * sigma
+    S = np.zeros((K, 3, 3))
+    S[:, 0, 1], S[:, 0, 2], S[:, 1, 2] = -ax[:, 2], ax[:, 1], -ax[:, 0]
+    S[:, 1, 0], S[:, 2, 0], S[:, 2, 1] = ax[:, 2], -ax[:, 1], ax[:, 0]
+    R = (np.eye(3)[None] + np.sin(ang)[:, None, None] * S
+         + (1 - np.cos(ang))[:, None, None] * np.einsum("nij,njk->nik", S, S))           # Rodrigues
+    return Grid.from_rotation_matrices(reduce_to_fundamental_zone(np.einsum("nij,njk->nik", R, centres[owner]),
+                                                                  symmetry), sigma)
+
+
+def counts_batched(op, grains, mean, seed=1):
+    """Poisson counts of a Voronoi-grain phantom (one orientation per grain, weight 1) computed batch by batch in the
+    channel-fastest layout: no (K, Ny, Nx) array of the phantom is made (it would not fit beside the state at the
+    large-slice size)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    supp = op.support_mask().ravel()
+    pix = np.flatnonzero(supp)
+    seeds = rng.choice(len(pix), grains, replace=False)
+    sy, sx = (pix[seeds] // op.Nx).astype(np.float32), (pix[seeds] % op.Nx).astype(np.float32)
+    grain_k = rng.choice(op.K, grains, replace=False)
+    py, px = (pix // op.Nx).astype(np.float32), (pix % op.Nx).astype(np.float32)
+    owner = np.empty(len(pix), np.int64)
+    for a in range(0, len(pix), 8192):
+        d2 = (py[a:a + 8192, None] - sy[None]) ** 2 + (px[a:a + 8192, None] - sx[None]) ** 2
+        owner[a:a + 8192] = grain_k[np.argmin(d2, axis=1)]
+    with torch.cuda.stream(op.stream()):              # the batch kernels run on the operator's stream
+        D = torch.zeros(op.data_shape, dtype=torch.float32, device=op.device)
+        buf = torch.zeros(op.batch_elems(), dtype=torch.float32, device=op.device)
+        for ib, bt in enumerate(op.batches):
+            sel = (owner >= bt["k_start"]) & (owner < bt["k_start"] + bt["K_batch"])
+            if not sel.any():
+                continue
+            buf.zero_()
+            idx = torch.as_tensor(pix[sel] * op.Kstride + (owner[sel] - bt["k_start"]), device=op.device)
+            buf[idx] = 1.0
+            op._direct_batch_k(buf.data_ptr(), ib, D)
+        lam = D * (mean / float(D.double().mean().item()))
+        g = torch.Generator(device=op.device)
+        g.manual_seed(seed + 1)
+        b = torch.poisson(lam, generator=g)
+    op.stream().synchronize()
+    return b
+
+
+NI512 = dict(LARGE_SLICE, K=50000, clusters=500, grains=500, mean_counts=50.0, epochs=10, max_gb=2.0)
+
+
+def ni512_run(steps, warmup, K=None):
+    """The large tailored-grid slice: 512 x 512 pixels, 720 angles over 180 deg, 520 translations, 360 eta bins, 6
+    rings of cubic Ni, K = 50000 orientations in 500 seeded clusters (sigma 1 deg), 36 subsets; the Fourier-slice
+    projector (float32 transforms), the PF contraction in BF16 on the tensor cores with the PF of each subset
+    generated when it is used (no stored PF), x and z resident in float32, T streamed from pinned host memory, the
+    residual recomputed with the float32 operator (its PF rows generated per batch) once per epoch and the deviance
+    in float64. A step is one epoch; CUDA events around `steps` epochs after `warmup`."""
+    import torch
+    from diffractom_b200 import Material, SinglePhaseForwardOperator, SPDHGPoisson, _lib
+    w = dict(NI512)
+    if K:
+        w["K"] = int(K)
+        w["clusters"] = min(w["clusters"], w["K"])
+        w["grains"] = min(w["grains"], w["K"])
+    mat = Material.from_lattice_parameters(**w["material"])
+    grid = clustered_grid(w["K"], w["clusters"], np.deg2rad(w["sigma_deg"]), mat.crystal_system, seed=0)
+    t0 = time.perf_counter()
+    op = SinglePhaseForwardOperator(dict(w["cfg"]), mat, grid, w["max_gb"], normalized=True, projector="fft",
+                                    precision="bf16", bf16_pf="generated", pf_mode="generated")
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t0
+    b = counts_batched(op, w["grains"], w["mean_counts"])
+    sp = SPDHGPoisson(op, subsets=w["subsets"], seed=0, resident=["x", "z"])
+    x0 = np.zeros(op.coeff_shape, np.float32)
+    t0 = time.perf_counter()
+    sp._setup(x0, b)
+    op.stream().synchronize()
+    t_setup = time.perf_counter() - t0
+    sp._iterate(warmup, diagnostics_interval=1, final=False)
+    stream = op.stream()
+    stream.synchronize()
+    timers = KernelTimers(op)
+    clocks = Clocks(torch.cuda.current_device())
+    n0 = _lib.lib().dfx_launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    timers.on()
+    sp._iterate(steps, diagnostics_interval=1, final=False)
+    timers.off()
+    end.record(stream)
+    end.synchronize()
+    launches = _lib.lib().dfx_launch_count() - n0 - timers.n_extra
+    clk = clocks.stop()
+    ms = start.elapsed_time(end)
+    f = [st["f"] for st in sp.iter_stats]
+    mem = torch.cuda.max_memory_allocated(op.device)
+    roof = timers.roofline(op)
+    return {"metric": "SPDHG epochs/s (large tailored-grid slice, Fourier-slice projector, BF16 contraction)",
+            "value": steps / (ms / 1e3), "unit": "epochs/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
+            "ms_per_step": ms / steps, "higher_is_better": True, "dtype": "bf16", "vs_baseline": None,
+            "data": "synthetic (seeded clustered grid, Voronoi phantom, Poisson counts)",
+            "config": {"workload": "ni512", "pixels": f"{op.Nx}x{op.Ny}", "N_Omega": op.N_Omega, "My": op.My,
+                       "N_eta": op.N_eta, "rings": op.N_peaks, "K": op.K, "clusters": w["clusters"],
+                       "subsets": w["subsets"], "batches": len(op.batches), "K_batch_max": op.K_batch_max,
+                       "projector": op.projector, "fft_channels_per_slice": op._fft_channels,
+                       "pf": "BF16 PF of each subset generated when used (two subset buffers); float32 PF rows "
+                             "generated per batch for the residual and the step sizes",
+                       "resident": sp.resident_used, "streamed": [n for n in ("x", "z", "T")
+                                                                  if n not in sp.resident_used],
+                       "operator_build_s": round(t_build, 1), "setup_s": round(t_setup, 1),
+                       "deviance_f64_per_epoch": f, "max_device_gb": round(mem / 1024 ** 3, 1),
+                       "epoch": "36 subset iterations + the float32 residual and float64 deviance every epoch",
+                       "l2": "inputs larger than L2, no flush"},
+            "roofline": roof, "gpu_launches": int(launches), "clocks": clk}
 
 
 def extras_run(K, steps, warmup):
@@ -871,7 +1014,7 @@ def local_run(K, steps, warmup, blob=12):
                        "subsets": 20}, "steps": steps, "warmup": warmup, "data": "synthetic", "local": out}
 
 
-def serving_run(n, rate, px, omega, eta, rings, K, slots, budget_gb, max_epochs, seed, scenario):
+def serving_run(n, rate, px, omega, eta, rings, K, slots, budget_gb, max_epochs, seed, scenario, precision="bf16"):
     """Requests of random size drawn uniformly from the ranges (cubic Al or hexagonal Ti, the first `rings`
     reflections), seeded phantoms and Poisson counts made beforehand, then submitted to a ReconstructionServer at
     Poisson arrival times; returns its latency statistics."""
@@ -902,7 +1045,7 @@ def serving_run(n, rate, px, omega, eta, rings, K, slots, budget_gb, max_epochs,
         b = counts(op, x, 50.0, seed=seed + i).cpu().numpy()
         op.free_memory()
         del op, x
-        reqs.append(Request(cfg, mat, grid, b, subsets=8, max_epochs=max_epochs, tol=1e-3))
+        reqs.append(Request(cfg, mat, grid, b, subsets=8, max_epochs=max_epochs, tol=1e-3, precision=precision))
     torch.cuda.empty_cache()
     t_prep = time.perf_counter() - t_prep
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
@@ -916,7 +1059,7 @@ def serving_run(n, rate, px, omega, eta, rings, K, slots, budget_gb, max_epochs,
     finished = srv.wait_all(timeout=1800)
     srv.stop()
     st = srv.stats()
-    st.update({"scenario": scenario, "slots": slots, "all_finished": bool(finished),
+    st.update({"scenario": scenario, "slots": slots, "all_finished": bool(finished), "precision": precision,
                "input_preparation_s": round(t_prep, 1),
                "converged": int(sum(1 for r in reqs if r.error is None and r.epochs < max_epochs)),
                "epochs_p50": float(np.median([r.epochs for r in reqs])),

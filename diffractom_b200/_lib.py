@@ -43,6 +43,8 @@ SIGNATURES = {
     "dfx_radon_backward_bf16": ([P, L, P, P, I, I, I, I, I, I, I, I, S], c_int),
     "dfx_radon_backward_spdhg_bf16": ([P, L, P, I, I, I, I, I, I, I, I, P, P, P, F, F, P, S], c_int),
     "dfx_radon_backward_spdhg_tc": ([P, L, P, I, I, I, I, I, I, I, I, P, P, P, F, F, P, S], c_int),
+    "dfx_convert_rows": ([I, P, L, P, L, L, I, S], c_int),
+    "dfx_radon_forward_tc": ([P, P, L, I, P, I, I, I, I, I, I, I, F, P, I, S], c_int),
     "dfx_radon_table_count": ([P, I, I, I, I, I, P, P, S], c_int),
     "dfx_radon_table_fill": ([P, I, I, I, I, I, P, P, P, S], c_int),
     "dfx_radon_forward_table": ([P, P, P, P, P, I, I, I, I, F, S], c_int),
@@ -57,6 +59,7 @@ SIGNATURES = {
     "dfx_scan_exclusive_i32_static": ([P, P, L, S], c_int),
     "dfx_spmm_pf_forward": ([P, P, P, P, P, P, I, I, I, I, I, I, S], c_int),
     "dfx_spmm_pf_adjoint": ([P, P, P, P, P, P, I, I, I, I, I, F, I, S], c_int),
+    "dfx_pf_dense_products": ([I, P, I, I, I, P, P, I, I, F, S], c_int),
     "dfx_pf_fblock_rows": ([I, I, I], c_int64),
     "dfx_pf_fblock_count": ([P, P, I, I, I, P, P, S], c_int),
     "dfx_pf_fblock_fill": ([P, P, P, I, I, I, P, P, P, S], c_int),
@@ -65,6 +68,8 @@ SIGNATURES = {
     "dfx_fill_f32": ([P, F, L, S], c_int),
     "dfx_spdhg_dual_update": ([P, P, P, P, P, L, P, L, P, L, F, P, I, L, S], c_int),
     "dfx_spdhg_primal_update": ([P, P, P, P, F, F, L, S], c_int),
+    "dfx_spdhg_primal_update_t16": ([P, P, P, P, F, F, L, S], c_int),
+    "dfx_f32_to_bf16_rz": ([P, P, L, S], c_int),
     "dfx_dual_steps": ([P, P, P, L, F, L, S], c_int),
     "dfx_set_mask_ones": ([P, P, L, L, S], c_int),
     "dfx_tinit": ([P, L, S], c_int),
@@ -116,8 +121,9 @@ SIGNATURES = {
     "dfx_copy_f32": ([P, P, L, S], c_int),
     "dfx_scale_f32": ([P, F, L, S], c_int),
     "dfx_pf_dense_bf16": ([POINTER(PFGeometry), I, I, L, L, I, P, S], c_int),
-    "dfx_pf_tc_forward": ([P, L, L, L, I, I, I, P, P, I, I, P, I, S], c_int),
-    "dfx_pf_tc_adjoint": ([P, L, L, L, I, I, I, P, P, I, I, F, P, S], c_int),
+    "dfx_pf_dense_bf16_rows": ([POINTER(PFGeometry), P, I, I, I, L, L, I, P, S], c_int),
+    "dfx_pf_tc_forward": ([P, L, L, L, I, I, I, P, P, I, I, P, I, I, S], c_int),
+    "dfx_pf_tc_adjoint": ([P, L, L, L, I, I, I, P, P, I, I, F, P, I, S], c_int),
     "dfx_tc_status": ([POINTER(ctypes.c_uint), I], c_int),
     "dfx_rows_to_bf16": ([P, P, P, I, I, I, I, S], c_int),
     "dfx_f32_to_bf16": ([P, P, L, S], c_int),

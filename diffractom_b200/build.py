@@ -59,7 +59,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             subprocess.run(cmd, check=True)
     if force or _stale(LIB, objs):
         cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(LIB), *map(str, objs),
-               "-lcudart", "-lcufft"]
+               "-lcudart", "-lcufft", "-lcublas"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -82,18 +82,20 @@ __global__ void pf_dense_kernel(dfx_pf_geometry g, int k0, int kb, float *__rest
     }
 }
 
-// Dense BF16 batch: rows koff .. koff+kb-1 of (R, ktot, cp_pad), the float32 entry rounded to nearest-even.
-__global__ void pf_dense_bf16_kernel(dfx_pf_geometry g, int k0, int kb, int64_t koff, int64_t ktot, int cp_pad,
-                                     __nv_bfloat16 *__restrict__ out)
+// Dense BF16 batch: rows koff .. koff+kb-1 of (n_rows, ktot, cp_pad), the float32 entry rounded to nearest-even;
+// angle plane s holds angle rows[s] (rows NULL: all R angles, plane r = angle r).
+__global__ void pf_dense_bf16_kernel(dfx_pf_geometry g, const int32_t *__restrict__ rows, int n_rows, int k0, int kb,
+                                     int64_t koff, int64_t ktot, int cp_pad, __nv_bfloat16 *__restrict__ out)
 {
     const int CP = g.C * g.P;
-    const int64_t total = (int64_t)g.R * kb * CP;
+    const int64_t total = (int64_t)n_rows * kb * CP;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
         const int j = (int)(i % CP);
         const int64_t t = i / CP;
         const int k = (int)(t % kb);
-        const int r = (int)(t / kb);
-        out[((int64_t)r * ktot + koff + k) * cp_pad + j] = __float2bfloat16_rn(pf_entry(g, r, k0 + k, j / g.P, j % g.P));
+        const int s = (int)(t / kb);
+        const int r = rows ? __ldg(rows + s) : s;
+        out[((int64_t)s * ktot + koff + k) * cp_pad + j] = __float2bfloat16_rn(pf_entry(g, r, k0 + k, j / g.P, j % g.P));
     }
 }
 
@@ -271,9 +273,23 @@ extern "C" int dfx_pf_dense_bf16(const dfx_pf_geometry *g, int k0, int kb, int64
     DFX_REQUIRE(koff >= 0 && koff + kb <= ktot && cp_pad >= g->C * g->P, "pf_dense_bf16: batch rows %lld + %d outside "
                 "ktot %lld, or cp_pad %d < CP", (long long)koff, kb, (long long)ktot, cp_pad);
     const int64_t n = (int64_t)g->R * kb * g->C * g->P;
-    pf_dense_bf16_kernel<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(*g, k0, kb, koff, ktot, cp_pad,
-                                                                           reinterpret_cast<__nv_bfloat16 *>(out));
+    pf_dense_bf16_kernel<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
+        *g, nullptr, g->R, k0, kb, koff, ktot, cp_pad, reinterpret_cast<__nv_bfloat16 *>(out));
     return launch_status("pf_dense_bf16");
+}
+
+extern "C" int dfx_pf_dense_bf16_rows(const dfx_pf_geometry *g, const int32_t *rows, int n_rows, int k0, int kb,
+                                      int64_t koff, int64_t ktot, int cp_pad, void *out, void *stream)
+{
+    int st = check_geometry(g);
+    if (st) return st;
+    DFX_REQUIRE(out && rows && n_rows > 0 && k0 >= 0 && kb > 0 && k0 + kb <= g->K, "pf_dense_bf16_rows: bad batch");
+    DFX_REQUIRE(koff >= 0 && koff + kb <= ktot && cp_pad >= g->C * g->P, "pf_dense_bf16_rows: batch rows %lld + %d "
+                "outside ktot %lld, or cp_pad %d < CP", (long long)koff, kb, (long long)ktot, cp_pad);
+    const int64_t n = (int64_t)n_rows * kb * g->C * g->P;
+    pf_dense_bf16_kernel<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
+        *g, rows, n_rows, k0, kb, koff, ktot, cp_pad, reinterpret_cast<__nv_bfloat16 *>(out));
+    return launch_status("pf_dense_bf16_rows");
 }
 
 static int pf_csr(const dfx_pf_geometry *g, const int32_t *rows, int n_rows, int k0, int kb, int fwd, int fill,

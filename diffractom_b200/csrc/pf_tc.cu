@@ -43,6 +43,7 @@ struct TcArgs {
     int64_t out_ld;          // forward: CP; adjoint: Ktot
     float alpha;
     int accumulate;
+    int pf_compact;          // the PF holds the subset's angles only: its angle coordinate is the subset index
 };
 
 constexpr uint32_t TMEM_COLS = 256;    // NT <= 256 float32 columns
@@ -66,6 +67,7 @@ __global__ void __launch_bounds__(TC_THREADS) pf_tc_kernel(const __grid_constant
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int rl = blockIdx.z;
     const int r = p.omegas ? __ldg(p.omegas + rl) : rl;
+    const int rp = p.pf_compact ? rl : r;                        // the PF's angle coordinate
     const int m0 = blockIdx.y * TC_M, n0 = blockIdx.x * p.nt;
     const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + S), done = smem_u32(bars + 2 * S);
 
@@ -104,11 +106,11 @@ __global__ void __launch_bounds__(TC_THREADS) pf_tc_kernel(const __grid_constant
             const uint32_t a_dst = smem_u32(a_tiles + (size_t)s * A_STAGE_BYTES);
             const uint32_t b_dst = smem_u32(b_tiles + (size_t)s * b_stage_bytes);
             if (DIR == 0) {
-                tma_load_3d(a_dst, &map_a, fb, m0, kc * TC_BK, r);
-                if (a_hi) tma_load_3d(a_dst + A_STAGE_BYTES / 2, &map_a, fb, m0 + 64, kc * TC_BK, r);
+                tma_load_3d(a_dst, &map_a, fb, m0, kc * TC_BK, rp);
+                if (a_hi) tma_load_3d(a_dst + A_STAGE_BYTES / 2, &map_a, fb, m0 + 64, kc * TC_BK, rp);
                 tma_load_3d(b_dst, &map_b, fb, kc * TC_BK, n0, rl);
             } else {
-                tma_load_3d(a_dst, &map_a, fb, kc * TC_BK, m0, r);
+                tma_load_3d(a_dst, &map_a, fb, kc * TC_BK, m0, rp);
                 tma_load_3d(b_dst, &map_b, fb, kc * TC_BK, n0, r);
             }
         }
@@ -200,6 +202,23 @@ __global__ void f32_to_bf16_kernel(const float4 *__restrict__ in, uint2 *__restr
     }
 }
 
+// Strided row conversions between a float32 sinogram (rows of ld_f32) and BF16 rows (ld_bf16): TO_BF16 rounds to
+// nearest-even, the other way widens exactly. rows x cols elements; one thread per element.
+template <int TO_BF16>
+__global__ void convert_rows_kernel(float *__restrict__ f32, int64_t ld_f32, __nv_bfloat16 *__restrict__ b16,
+                                    int64_t ld_b16, int64_t rows, int cols)
+{
+    const int64_t total = rows * cols;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / cols;
+        const int c = (int)(i - r * cols);
+        if (TO_BF16)
+            b16[r * ld_b16 + c] = __float2bfloat16_rn(f32[r * ld_f32 + c]);
+        else
+            f32[r * ld_f32 + c] = __bfloat162float(b16[r * ld_b16 + c]);
+    }
+}
+
 // ---------------------------------------------------------------------------------------------- host side
 // N tile: the translations split into the fewest tiles of at most 256, each a multiple of 16.
 int n_tile(int my)
@@ -258,7 +277,7 @@ using namespace dfx;
 
 extern "C" int dfx_pf_tc_forward(const void *pf_bf16, int64_t ktot, int64_t k0, int64_t kn, int cp, int cp_pad,
                                  int n_omega, const void *z_bf16, const int32_t *omegas, int n_sub, int my, float *data,
-                                 int accumulate, void *stream)
+                                 int accumulate, int pf_compact, void *stream)
 {
     int st = check_common(pf_bf16, ktot, k0, kn, cp, cp_pad, n_sub, my, n_omega);
     if (st) return st;
@@ -278,8 +297,9 @@ extern "C" int dfx_pf_tc_forward(const void *pf_bf16, int64_t ktot, int64_t k0, 
     a.out_ld = cp;
     a.alpha = 1.0f;
     a.accumulate = accumulate != 0;
-    if ((st = make_map(&ma, pf, (uint64_t)cp_pad, (uint64_t)kn, (uint64_t)n_omega, (uint64_t)cp_pad,
-                       (uint64_t)ktot * cp_pad, 64, 64, "PF")))
+    a.pf_compact = pf_compact != 0;
+    if ((st = make_map(&ma, pf, (uint64_t)cp_pad, (uint64_t)kn, (uint64_t)(pf_compact ? n_sub : n_omega),
+                       (uint64_t)cp_pad, (uint64_t)ktot * cp_pad, 64, 64, "PF")))
         return st;
     if ((st = make_map(&mb, z, (uint64_t)kn, (uint64_t)my, (uint64_t)n_sub, (uint64_t)ktot, (uint64_t)ktot * my, 64,
                        (uint32_t)a.nt, "Z")))
@@ -289,7 +309,7 @@ extern "C" int dfx_pf_tc_forward(const void *pf_bf16, int64_t ktot, int64_t k0, 
 
 extern "C" int dfx_pf_tc_adjoint(const void *pf_bf16, int64_t ktot, int64_t k0, int64_t kn, int cp, int cp_pad,
                                  int n_omega, const void *d_bf16, const int32_t *omegas, int n_sub, int my,
-                                 float alpha, void *z_bf16, void *stream)
+                                 float alpha, void *z_bf16, int pf_compact, void *stream)
 {
     int st = check_common(pf_bf16, ktot, k0, kn, cp, cp_pad, n_sub, my, n_omega);
     if (st) return st;
@@ -307,8 +327,9 @@ extern "C" int dfx_pf_tc_adjoint(const void *pf_bf16, int64_t ktot, int64_t k0, 
     a.out_bf16 = reinterpret_cast<__nv_bfloat16 *>(z_bf16) + k0;
     a.out_ld = ktot;
     a.alpha = alpha;
-    if ((st = make_map(&ma, pf, (uint64_t)cp_pad, (uint64_t)kn, (uint64_t)n_omega, (uint64_t)cp_pad,
-                       (uint64_t)ktot * cp_pad, 64, TC_M, "PF")))
+    a.pf_compact = pf_compact != 0;
+    if ((st = make_map(&ma, pf, (uint64_t)cp_pad, (uint64_t)kn, (uint64_t)(pf_compact ? n_sub : n_omega),
+                       (uint64_t)cp_pad, (uint64_t)ktot * cp_pad, 64, TC_M, "PF")))
         return st;
     if ((st = make_map(&mb, d_bf16, (uint64_t)cp_pad, (uint64_t)my, (uint64_t)n_omega, (uint64_t)cp_pad,
                        (uint64_t)cp_pad * my, 64, (uint32_t)a.nt, "D")))
@@ -318,6 +339,7 @@ extern "C" int dfx_pf_tc_adjoint(const void *pf_bf16, int64_t ktot, int64_t k0, 
 
 namespace dfx {
 unsigned int tcb_status(unsigned int reset);    // the flags of the tensor-core backprojection (radon_tc.cu)
+unsigned int tcf_status(unsigned int reset);    // the flags of the tensor-core forward projection (radon_tc_fwd.cu)
 }
 
 extern "C" int dfx_tc_status(unsigned int *flags, int reset)
@@ -325,6 +347,7 @@ extern "C" int dfx_tc_status(unsigned int *flags, int reset)
     DFX_REQUIRE(flags != nullptr, "tc_status: null output");
     cudaError_t e = cudaMemcpyFromSymbol(flags, g_tc_flags, sizeof(unsigned int));
     *flags |= dfx::tcb_status(reset ? 1u : 0u);
+    *flags |= dfx::tcf_status(reset ? 1u : 0u);
     if (e == cudaSuccess && reset) {
         const unsigned int zero = 0;
         e = cudaMemcpyToSymbol(g_tc_flags, &zero, sizeof(unsigned int));
@@ -357,4 +380,21 @@ extern "C" int dfx_f32_to_bf16(const float *in, void *out, int64_t n, void *stre
     f32_to_bf16_kernel<<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const float4 *>(in), reinterpret_cast<uint2 *>(out), n / 4);
     return launch_status("f32_to_bf16");
+}
+
+extern "C" int dfx_convert_rows(int to_bf16, float *f32, int64_t ld_f32, void *b16, int64_t ld_b16, int64_t rows,
+                                int cols, void *stream)
+{
+    DFX_REQUIRE(f32 && b16, "convert_rows: null pointer");
+    DFX_REQUIRE(rows >= 0 && cols >= 0 && ld_f32 >= cols && ld_b16 >= cols, "convert_rows: bad sizes");
+    const int64_t n = rows * cols;
+    if (n == 0) return DFX_OK;
+    const int64_t blocks = cdiv(n, 256);
+    const unsigned g = (unsigned)(blocks < 148 * 16 ? blocks : 148 * 16);
+    auto *b = reinterpret_cast<__nv_bfloat16 *>(b16);
+    if (to_bf16)
+        convert_rows_kernel<1><<<g, 256, 0, (cudaStream_t)stream>>>(f32, ld_f32, b, ld_b16, rows, cols);
+    else
+        convert_rows_kernel<0><<<g, 256, 0, (cudaStream_t)stream>>>(f32, ld_f32, b, ld_b16, rows, cols);
+    return launch_status("convert_rows");
 }

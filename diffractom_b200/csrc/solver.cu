@@ -4,6 +4,8 @@
 // allows). Reductions sum in float64: every block reduces its grid-stride share with warp shuffles into one partial
 // in the caller's scratch, and one block sums the partials in a fixed order, so the result does not depend on
 // timing (bitwise reproducible for a given launch shape).
+#include <cuda_bf16.h>
+
 #include "dfx_common.cuh"
 
 namespace dfx {
@@ -487,6 +489,28 @@ __global__ void dual_update4_kernel(float4 *__restrict__ y, float4 *__restrict__
     }
 }
 
+// The same step with T held in BF16 (widened exactly): the step sizes of a run whose x, z and T do not all fit in
+// float32 (T rounded toward zero when stored, so never above its float32 value).
+__global__ void primal_update_t16_kernel(float *__restrict__ x, float *__restrict__ z,
+                                         const __nv_bfloat16 *__restrict__ T, const float *__restrict__ dz, float inv_p,
+                                         float lam, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float di = dz[i];
+        const float zi = __fadd_rn(z[i], di);
+        z[i] = zi;
+        const float zb = __fadd_rn(zi, __fmul_rn(inv_p, di));
+        const float t = __bfloat162float(T[i]);
+        x[i] = t > 0.0f ? fmaxf(0.0f, __fsub_rn(x[i], __fmul_rn(t, __fadd_rn(zb, lam)))) : 0.0f;
+    }
+}
+
+__global__ void f32_to_bf16_rz_kernel(const float *__restrict__ in, __nv_bfloat16 *__restrict__ out, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = __float2bfloat16_rz(in[i]);
+}
+
 __global__ void primal_update_kernel(float *__restrict__ x, float *__restrict__ z, const float *__restrict__ T,
                                      const float *__restrict__ dz, float inv_p, float lam, int64_t n)
 {
@@ -917,6 +941,22 @@ extern "C" int dfx_spdhg_primal_update(float *x, float *z, const float *T, const
     DFX_REQUIRE(x && z && T && dz && n >= 0, "primal_update: bad arguments");
     if (n == 0) return DFX_OK;
     EW_LAUNCH(primal_update_kernel, n, stream, x, z, T, dz, inv_p, lam, n);
+}
+
+extern "C" int dfx_spdhg_primal_update_t16(float *x, float *z, const void *T_bf16, const float *dz, float inv_p,
+                                           float lam, int64_t n, void *stream)
+{
+    DFX_REQUIRE(x && z && T_bf16 && dz && n >= 0, "primal_update_t16: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(primal_update_t16_kernel, n, stream, x, z, reinterpret_cast<const __nv_bfloat16 *>(T_bf16), dz, inv_p,
+              lam, n);
+}
+
+extern "C" int dfx_f32_to_bf16_rz(const float *in, void *out, int64_t n, void *stream)
+{
+    DFX_REQUIRE(in && out && n >= 0, "f32_to_bf16_rz: bad arguments");
+    if (n == 0) return DFX_OK;
+    EW_LAUNCH(f32_to_bf16_rz_kernel, n, stream, in, reinterpret_cast<__nv_bfloat16 *>(out), n);
 }
 
 extern "C" int dfx_dual_steps(float *sig, const float *rowsum, const float *w, int64_t pw, float sigma0, int64_t n,

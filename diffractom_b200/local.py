@@ -284,6 +284,8 @@ class LocalSinglePhaseForwardOperator(SinglePhaseForwardOperator):
             raise ValueError("LocalSinglePhaseForwardOperator uses the native projector")
         if kwargs.get("pf_mode", "auto") == "dense":
             raise ValueError("LocalSinglePhaseForwardOperator needs a sparse PF mode ('auto', 'sparse', 'generated')")
+        kwargs.setdefault("sparse_max_fill", 1.0)          # never the dense path (local_forward_operator.py:134-135)
+        kwargs.setdefault("sparse_max_fill_partial", 1.0)
         if kwargs.get("precision", "fp32") != "fp32":
             raise NotImplementedError("LocalSinglePhaseForwardOperator computes in float32")
         if not isinstance(support, LocalSupport):

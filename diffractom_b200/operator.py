@@ -48,6 +48,8 @@ class SinglePhaseForwardOperator:
 
     coefficient_layout = "dense"
     _pf_forward_csr = True
+    # BF16 images are projected on the tensor cores (dfx_radon_forward_tc) where the geometry admits it
+    use_tc_forward = True
     # with both CSR copies stored, the forward products run over an eta-blocked copy of the forward CSR (four
     # neighbouring eta bins of a ring per entry; the same sums bit for bit); False: over the forward CSR itself
     forward_blocks = True
@@ -59,7 +61,7 @@ class SinglePhaseForwardOperator:
                  pf_cutoff_sigma: float | None = 4.0, quadrature="auto", quadrature_tol: float = DEFAULT_TOL,
                  intensity_model=None, sparse_batch_max: int = SPARSE_BATCH_MAX, rings=None, ring_two_theta=None,
                  reflection_two_theta: bool = False, window_parallax=None, ring_intensities=None,
-                 precision: str = "fp32", **kwargs):
+                 precision: str = "fp32", bf16_pf: str = "auto", **kwargs):
         """Arguments as diffractom's (SPFO:169-197). ctx: None, a torch.device or a CUDA device index (the GPU);
         queue: None (the current torch stream at every call) or a torch.cuda.Stream. ring_intensities: with
         normalized=False, the integrated intensity of every ring (diffractom computes them from structure factors,
@@ -68,13 +70,15 @@ class SinglePhaseForwardOperator:
         Fourier-slice one for grids of more than 400 x 400 pixels at float32 precision, SPFO:448-449).
 
         precision: "fp32" (the reference's arithmetic) or "bf16": direct_cl / adjoint_cl on device tensors then run
-        the Radon output through BF16 and the pole-figure products on the tensor cores (dense BF16 PF of all
-        orientations, float32 accumulation); the float32 sparse PF stays available (NumPy (streamed) calls stay
-        float32). reflection_two_theta: every pole axis probes at its reflections' own Bragg angle (the windows of
-        rings= then hold reflections of different angles; SPFO:236-244).
+        the Radon output through BF16 and the pole-figure products on the tensor cores (dense BF16 PF, float32
+        accumulation); the float32 sparse PF stays available (NumPy (streamed) calls stay float32). bf16_pf: "stored"
+        (the BF16 PF of all angles kept), "generated" (the PF of each product's angles generated when it runs) or
+        "auto" (stored if it takes at most half of the free device memory). reflection_two_theta: every pole axis
+        probes at its reflections' own Bragg angle (the windows of rings= then hold reflections of different angles;
+        SPFO:236-244).
 
-        pf_mode "dense" runs the sparse products (the same PF matrix, its zeros skipped). Not provided
-        (NotImplementedError): projector "gratopy", the BF16 path with the Fourier-slice projector."""
+        pf_mode "dense" applies the float32 PF by batched SGEMMs (no omega subsets, as the reference). Not provided
+        (NotImplementedError): projector "gratopy"."""
         lib = _lib.lib()                                    # fails loudly without the CUDA library
         if not torch.cuda.is_available():
             raise RuntimeError("SinglePhaseForwardOperator needs a CUDA device")
@@ -99,11 +103,6 @@ class SinglePhaseForwardOperator:
             raise NotImplementedError("projector 'gratopy' is not provided (the native and 'fft' projectors are)")
         if pf_mode not in ("dense", "sparse", "generated", "auto"):
             raise ValueError(f"pf_mode must be 'dense', 'sparse', 'generated' or 'auto', not {pf_mode!r}")
-        if pf_mode == "dense":
-            # the reference's dense mode applies the float32 PF matrix by GEMMs; the stored sparse matrix is the same
-            # operator (its zeros skipped), so "dense" runs the sparse products (SPFO:1207-1373)
-            warnings.warn("pf_mode='dense': the sparse products apply the same PF matrix and are used", stacklevel=2)
-            pf_mode = "sparse"
         # the native projector's geometry is made in any case (the Fourier-slice projector shares its conventions)
         geom_kernel = "trapezoid" if projector == "fft" or radon_kernel is None else radon_kernel
 
@@ -116,14 +115,12 @@ class SinglePhaseForwardOperator:
         self.geometry = geom
         self.pf_batch_max_gb = float(max_gb)
         if projector == "auto":
-            projector = ("fft" if self.Nx * self.Ny > AUTO_FFT_PIXELS and precision == "fp32"
-                         and radon_kernel in (None, "hat") else "native")
+            projector = ("fft" if self.Nx * self.Ny > AUTO_FFT_PIXELS and radon_kernel in (None, "hat")
+                         else "native")
         if radon_kernel is None:
             radon_kernel = "trapezoid" if projector == "native" else "hat"
         if radon_kernel != "hat" and projector != "native":
             raise ValueError(f"radon_kernel={radon_kernel!r} needs the native projector (projector is {projector!r})")
-        if projector == "fft" and precision == "bf16":
-            raise NotImplementedError("the BF16 precision path needs the native projector")
         self.projector = projector
         self.radon_kernel = radon_kernel
         self._kernel_id = 1 if geom_kernel == "trapezoid" else 0
@@ -147,9 +144,11 @@ class SinglePhaseForwardOperator:
             if window_parallax is not None:
                 self.set_window_parallax(**dict(window_parallax), _build=False)
             self._pf_version = 0
+            self._sub_version = 0
             self._make_pfg()
             self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
             self._ray_supp = {}
+            self._supp_tiles = {}
             self._fft = None
             if self.projector == "fft":
                 self._ray_rp = self._ray_ent = None
@@ -161,6 +160,9 @@ class SinglePhaseForwardOperator:
             self._sub = []
             self._streamer = None
 
+            if precision not in ("fp32", "bf16"):
+                raise ValueError(f"precision must be 'fp32' or 'bf16', not {precision!r}")
+            self.precision = precision
             # ---- batches and the sparse PF matrix (SPFO:1026-1094, 1207-1373)
             self.get_pf_batches_for_material()
             self.pf_mode = pf_mode
@@ -171,10 +173,8 @@ class SinglePhaseForwardOperator:
             self._pf_build = dict(mode=pf_mode, max_fill=sparse_max_fill, max_gb=sparse_max_gb,
                                   max_fill_partial=sparse_max_fill_partial)
             self.build_sparse_pf(**self._pf_build)
-            if precision not in ("fp32", "bf16"):
-                raise ValueError(f"precision must be 'fp32' or 'bf16', not {precision!r}")
-            self.precision = precision
             self.pf_bf16 = None
+            self.bf16_pf = bf16_pf
             if precision == "bf16":
                 self.build_dense_bf16_pf()
 
@@ -387,7 +387,9 @@ class SinglePhaseForwardOperator:
         for name, n in checks:
             if n >= 2 ** 31:
                 raise ValueError(f"The {name} has {n} elements, more than 2^31 - 1; lower max_gb.")
-        self.Kstride = -(-self.K_batch_max // KSTRIDE_ALIGN) * KSTRIDE_ALIGN
+        # BF16 runs pad the channels to the 64-channel image boxes of the tensor-core forward projection
+        align = 64 if getattr(self, "precision", "fp32") == "bf16" else KSTRIDE_ALIGN
+        self.Kstride = -(-self.K_batch_max // align) * align
         self._alloc_batch_buffers()
         return self.batches
 
@@ -464,6 +466,11 @@ class SinglePhaseForwardOperator:
     def _pf_forward_product(self, ib, m, sino_ptr, data, om, n_ang, kb):
         """data rows += the forward PF product of batch ib's Radon output at sino_ptr (angles om, subset m): over the
         eta-blocked copy when the batch stores it, else over the (stored or generated) forward CSR."""
+        if self.pf_mode == "dense":
+            if m is not None:
+                raise NotImplementedError("omega subsets need pf_mode 'sparse' or 'generated'")
+            self._dense_pf_product(ib, False, sino_ptr, data.data_ptr())
+            return
         sb = self.sparse_batches[ib]
         s = self._s()
         om_ptr = None if om is None else om.data_ptr()
@@ -489,17 +496,34 @@ class SinglePhaseForwardOperator:
         in mode "auto", as the reference does."""
         t0 = time.perf_counter()
         R, CP = self.N_Omega, self.N_seg
-        if self.K_batch_max > 65535 or CP > 65535:
-            raise ValueError(f"K_batch_max = {self.K_batch_max} or N_eta * N_rings = {CP} exceeds the 16-bit index "
-                             "range of the sparse PF matrix; use a smaller max_gb")
         auto = mode == "auto"
+        if mode == "dense":
+            self._use_dense_pf()
+            return
+        if self.K_batch_max > 65535 or CP > 65535:
+            if auto:
+                self._use_dense_pf(f"K_batch_max = {self.K_batch_max} or N_eta * N_rings = {CP} exceeds the 16-bit "
+                                   "index range")
+                return
+            raise ValueError(f"K_batch_max = {self.K_batch_max} or N_eta * N_rings = {CP} exceeds the 16-bit index "
+                             "range of the sparse PF matrix; use pf_mode='dense' or a smaller max_gb")
         b0 = self.batches[0]
         _, nnz0 = self._csr(b0["k_start"], b0["K_batch"], False)
         fill = nnz0 / (R * b0["K_batch"] * CP)
         self.sparse_fill_first = fill
+        # mode "auto" applies the dense matrix above max_fill, or above max_fill_partial when the whole sparse
+        # matrix would not fit in max_gb (SPFO:1249-1263)
         if auto and fill > max_fill:
-            warnings.warn(f"PF fill fraction {100 * fill:.1f} % > {100 * max_fill:.1f} %: the reference would apply the "
-                          "dense matrix; the sparse products compute the same operator", stacklevel=2)
+            self._use_dense_pf(f"fill fraction {100 * fill:.2f} % > {100 * max_fill:.2f} %")
+            return
+        if auto and fill > max_fill_partial and max_gb is not None:
+            nb_est = -(-self.K // self.sparse_batch_size(fill))
+            both_est = 12 * fill * R * self.K * CP + 4 * (nb_est * (R * CP + 1) + R * self.K + nb_est)
+            if both_est > max_gb * 1024 ** 3:
+                self._use_dense_pf(f"fill fraction {100 * fill:.2f} % > {100 * max_fill_partial:.2f} % and the "
+                                   f"whole sparse matrix ({both_est / 1024 ** 3:.1f} GB) does not fit in "
+                                   f"{max_gb:.1f} GB")
+                return
         self.get_pf_batches_for_material(K_batch=self.sparse_batch_size(fill))
         nb = len(self.batches)
         both, adj, ptr_f, batch_adj = self.sparse_estimates(fill)
@@ -577,6 +601,28 @@ class SinglePhaseForwardOperator:
                   f"to {self.K_batch_max}, stored: {self.pf_storage} ({stored_bytes / 1024 ** 2:.1f} MB); set up in "
                   f"{self.pf_setup_s:.2f} s")
 
+    def _use_dense_pf(self, reason=None):
+        """pf_mode "dense" (SPFO:1207-1263, 2063-2127): the float32 PF of a batch is generated in every call into a
+        buffer of the dense batch size and applied by batched SGEMMs over the angles (dfx_pf_dense_products); omega
+        subsets are not available, as in the reference."""
+        R, CP = self.N_Omega, self.N_seg
+        self.pf_mode = "dense"
+        self.pf_storage = "none"
+        self.sparse_batches = None
+        self.sparse_nnz = None
+        self._pf_dense = torch.empty((R, self.K_batch_max, CP), dtype=torch.float32, device=self.device)
+        if reason is not None and self.verbose:
+            print(f"Sparse PF matrix: {reason}, using the dense PF path")
+
+    def _dense_pf_product(self, ib, adjoint, src_ptr, dst_ptr, alpha=1.0):
+        """The dense-mode PF product of batch ib over all angles: the batch's float32 PF generated, then forward
+        data (+)= PF^T Z or adjoint Z = alpha PF D by batched SGEMMs."""
+        b = self.batches[ib]
+        s = self._s()
+        self._call("dfx_pf_dense", ctypes.byref(self._pfg), b["k_start"], b["K_batch"], self._pf_dense.data_ptr(), s)
+        self._call("dfx_pf_dense_products", int(adjoint), self._pf_dense.data_ptr(), self.N_Omega, b["K_batch"],
+                   self.N_seg, src_ptr, dst_ptr, self.My, self.Kstride, float(alpha), s)
+
     def sparse_estimates(self, fill):
         """Estimated bytes of the sparse PF matrix at a fill fraction, for the current batches: (both CSR copies,
         the adjoint copies only, the forward row pointers of one batch, [adjoint copy of batch ib: row pointers +
@@ -620,41 +666,64 @@ class SinglePhaseForwardOperator:
     def build_dense_bf16_pf(self, max_z_gb: float = 2.0):
         """The dense BF16 PF of all orientation batches, (N_Omega, Ktot, CPpad) with batch ib at rows ib * Kstride
         (padding rows and columns 0), and the BF16 work buffers of the tensor-core products: Z (angles, My, Ktot),
-        the Radon output of all batches side by side, for up to max_z_gb of angles at a time, and D's BF16 copy."""
+        the Radon output of all batches side by side, for up to max_z_gb of angles at a time, and D's BF16 copy.
+        bf16_pf "generated" (or "auto" when the PF of all angles would take more than half of the free device memory):
+        no PF of all angles is kept; every tensor-core product generates the PF of its angles (dfx_pf_dense_bf16_rows)
+        into one of two buffers, which keep the last two angle lists (an SPDHG iteration's adjoint subset and next
+        forward subset)."""
         R, CP = self.N_Omega, self.N_seg
         self.Ktot = len(self.batches) * self.Kstride
         self.cp_pad = -(-CP // 8) * 8
         nbytes = 2 * R * self.Ktot * self.cp_pad
         free, _ = torch.cuda.mem_get_info(self.device)
-        if nbytes > 0.9 * free:
+        mode = self.bf16_pf
+        if mode not in ("auto", "stored", "generated"):
+            raise ValueError(f"bf16_pf must be 'auto', 'stored' or 'generated', not {mode!r}")
+        if mode == "auto":
+            mode = "stored" if nbytes <= 0.5 * free else "generated"
+        if mode == "stored" and nbytes > 0.9 * free:
             raise MemoryError(f"dense BF16 PF of {nbytes / 1024 ** 3:.1f} GB does not fit in the free device memory "
-                              f"({free / 1024 ** 3:.1f} GB)")
+                              f"({free / 1024 ** 3:.1f} GB); use bf16_pf='generated'")
+        self.bf16_pf_storage = mode
         t0 = time.perf_counter()
-        self.pf_bf16 = torch.zeros((R, self.Ktot, self.cp_pad), dtype=torch.bfloat16, device=self.device)
-        for ib, b in enumerate(self.batches):
-            self._call("dfx_pf_dense_bf16", ctypes.byref(self._pfg), b["k_start"], b["K_batch"], ib * self.Kstride,
-                       self.Ktot, self.cp_pad, self.pf_bf16.data_ptr(), self._s())
-        self._d_bf16 = torch.zeros((R, self.My, self.cp_pad), dtype=torch.bfloat16, device=self.device)
-        self._z_bf16 = torch.empty(0, dtype=torch.bfloat16, device=self.device)
         per_angle = 2 * self.My * self.Ktot
         self._bf16_chunk = max(1, min(R, int(max_z_gb * 1024 ** 3 // per_angle)))
+        self._pf_gen_slots = []
+        if mode == "stored":
+            self.pf_bf16 = torch.zeros((R, self.Ktot, self.cp_pad), dtype=torch.bfloat16, device=self.device)
+            for ib, b in enumerate(self.batches):
+                self._call("dfx_pf_dense_bf16", ctypes.byref(self._pfg), b["k_start"], b["K_batch"],
+                           ib * self.Kstride, self.Ktot, self.cp_pad, self.pf_bf16.data_ptr(), self._s())
+        else:
+            self.pf_bf16 = None
+            self._pf_gen_max = self._bf16_chunk
+        self._d_bf16 = torch.zeros((R, self.My, self.cp_pad), dtype=torch.bfloat16, device=self.device)
+        self._z_bf16 = torch.empty(0, dtype=torch.bfloat16, device=self.device)
         self._all_omegas = torch.arange(R, dtype=torch.int32, device=self.device)
         # the tensor-core backprojection covers a 16 x 8 pixel tile with a 32-bin window per angle
         g = np.abs(np.asarray(self.radon_geo.geo, np.float64))
         hw = (1.0 + np.maximum(g[:, 0], g[:, 1])) / 2.0 if self._kernel_id == 1 else np.ones(R)
         span = 15.0 * g[:, 0] + 7.0 * g[:, 1] + 2.0 * hw + 2.0
         self.tc_backprojection = bool(np.all(span <= 32.0)) and self.Kstride % 16 == 0
+        # the tensor-core forward projection: 8 x 8 pixel tiles on 32-bin windows that start at a multiple of 16
+        # (taps within 17 bins of the tile's first), every bin of an angle in tensor memory (My + 31 <= 512 columns)
+        span_f = 7.0 * (g[:, 0] + g[:, 1]) + 2.0 * hw + 2.0
+        self.tc_forward = (bool(np.all(span_f <= 17.0)) and self.Kstride % 64 == 0 and self.My + 31 <= 512
+                           and self.projector == "native")
         self.pf_bf16_setup_s = time.perf_counter() - t0
 
     def _z(self, n):
         """The BF16 Radon output buffer for n angles, (n, My, Ktot)."""
         need = n * self.My * self.Ktot
         if self._z_bf16.numel() < need:
-            self._z_bf16 = torch.empty(need, dtype=torch.bfloat16, device=self.device)
+            # zeros: the padding channels of a batch whose columns a projection writes for its K_batch channels only
+            # stay finite (they meet zero PF rows in the products)
+            self._z_bf16 = torch.zeros(need, dtype=torch.bfloat16, device=self.device)
         return self._z_bf16[:need].view(n, self.My, self.Ktot)
 
     def _bf16_chunks(self, subset):
-        """(geo, n, omegas) pieces of the angles of subset m (or of all angles), each at most the Z buffer's size."""
+        """(geo, n, omegas, first) pieces of the angles of subset m (or of all angles), each at most the Z buffer's
+        size; first: the piece's first position in the angle list."""
         if subset is None:
             geo, om = self.geo_gpu, self._all_omegas
         else:
@@ -662,50 +731,94 @@ class SinglePhaseForwardOperator:
             geo, om = e["geo"], e["omegas"]
         n = om.numel()
         c = max(self._bf16_chunk, self._max_subset()) if subset is not None else self._bf16_chunk
-        return [(geo[a:a + c], min(c, n - a), om[a:a + c]) for a in range(0, n, c)]
+        return [(geo[a:a + c], min(c, n - a), om[a:a + c], a) for a in range(0, n, c)]
 
     def _max_subset(self):
         return max((e["n"] for e in self._sub), default=1)
 
-    def _radon_forward_bf16(self, src_ptr, ib, z, om, n):
-        """Radon transform of channel-fastest batch ib (float32 at src_ptr) into its columns of Z (BF16)."""
+    def _radon_forward_bf16(self, src_ptr, ib, z, om, n, m=None, row0=0):
+        """Radon transform of channel-fastest batch ib (float32 at src_ptr) into its columns of Z (BF16): the n angles
+        om, which are subset m's, or (m None) angles row0 .. row0 + n - 1 of all. The Fourier-slice projector
+        transforms every angle of the subset (or of all angles) into the float32 batch sinogram, whose rows are then
+        rounded to BF16 (its padding channels are zeros)."""
+        if self.projector == "fft":
+            self._fft_run(True, m, src_ptr, self.coeffs_sino_C.data_ptr(), self.batches[ib]["K_batch"])
+            self._call("dfx_convert_rows", 1, self.coeffs_sino_C.data_ptr() + 4 * row0 * self.My * self.Kstride,
+                       self.Kstride, z.data_ptr() + 2 * ib * self.Kstride, self.Ktot, n * self.My, self.Kstride,
+                       self._s())
+            return
         self._radon_fwd(src_ptr, z.data_ptr() + 2 * ib * self.Kstride, om, n, self.batches[ib]["K_batch"],
                         sld=self.Ktot)
 
+    def _pf_of(self, om, n):
+        """(PF tensor, compact flag) for the tensor-core products over the n angles om: the stored PF of all angles,
+        or the PF of these angles generated into one of two kept buffers (reused while the same angle list comes
+        again: an iteration's adjoint and the next one's forward of the same subset)."""
+        if self.pf_bf16 is not None:
+            return self.pf_bf16, 0
+        key = (om.data_ptr(), int(n), self._pf_version, self._sub_version)
+        for slot in self._pf_gen_slots:
+            if slot["key"] == key:
+                return slot["pf"][:n], 1
+        if n > self._pf_gen_max:
+            self._pf_gen_max = n
+            self._pf_gen_slots = []
+        if len(self._pf_gen_slots) < 2:
+            buf = torch.zeros((self._pf_gen_max, self.Ktot, self.cp_pad), dtype=torch.bfloat16, device=self.device)
+            slot = {"pf": buf, "key": None}
+            self._pf_gen_slots.append(slot)
+        else:
+            slot = self._pf_gen_slots.pop(0)                  # the older list's buffer
+            self._pf_gen_slots.append(slot)
+        slot["key"] = key
+        for ib, b in enumerate(self.batches):
+            self._call("dfx_pf_dense_bf16_rows", ctypes.byref(self._pfg), om.data_ptr(), int(n), b["k_start"],
+                       b["K_batch"], ib * self.Kstride, self.Ktot, self.cp_pad, slot["pf"].data_ptr(), self._s())
+        return slot["pf"][:n], 1
+
     def _pf_tc_forward(self, z, om, n, data, k0=0, kn=None, accumulate=0):
-        self._call("dfx_pf_tc_forward", self.pf_bf16.data_ptr(), self.Ktot, k0, self.Ktot if kn is None else kn,
+        """data rows om (+)= PF Z on the tensor cores (the stored PF, or the PF of these angles generated)."""
+        src, compact = self._pf_of(om, n)
+        self._call("dfx_pf_tc_forward", src.data_ptr(), self.Ktot, k0, self.Ktot if kn is None else kn,
                    self.N_seg, self.cp_pad, self.N_Omega, z.data_ptr(), om.data_ptr(), n, self.My, data.data_ptr(),
-                   accumulate, self._s())
+                   accumulate, compact, self._s())
 
     def _pf_tc_adjoint(self, om, n, z, k0=0, kn=None):
-        """Z = alpha PF^T D for the angles om (D's BF16 copy must hold their rows)."""
+        """Z = alpha PF^T D for the angles om (D's BF16 copy must hold their rows); the PF as in _pf_tc_forward."""
         alpha = float(np.float32(self.N_Omega / np.pi))
-        self._call("dfx_pf_tc_adjoint", self.pf_bf16.data_ptr(), self.Ktot, k0, self.Ktot if kn is None else kn,
+        src, compact = self._pf_of(om, n)
+        self._call("dfx_pf_tc_adjoint", src.data_ptr(), self.Ktot, k0, self.Ktot if kn is None else kn,
                    self.N_seg, self.cp_pad, self.N_Omega, self._d_bf16.data_ptr(), om.data_ptr(), n, self.My, alpha,
-                   z.data_ptr(), self._s())
+                   z.data_ptr(), compact, self._s())
 
     def _rows_to_bf16(self, data, om, n):
         self._call("dfx_rows_to_bf16", data.data_ptr(), self._d_bf16.data_ptr(), om.data_ptr(), n, self.My,
                    self.N_seg, self.cp_pad, self._s())
 
     def _direct_bf16(self, coeffs, data, subset):
-        for geo, n, om in self._bf16_chunks(subset):
+        m = None if subset is None else self._subset(subset)
+        for geo, n, om, a in self._bf16_chunks(subset):
             z = self._z(n)
             for ib, b in enumerate(self.batches):
                 self._call("dfx_gather_channels", coeffs.data_ptr(), self._img_k.data_ptr(), self.npix, b["k_start"],
                            b["K_batch"], self.Kstride, self._s())
-                self._radon_forward_bf16(self._img_k.data_ptr(), ib, z, om, n)
+                self._radon_forward_bf16(self._img_k.data_ptr(), ib, z, om, n, m=m, row0=a)
             self._pf_tc_forward(z, om, n, data)
 
     def _adjoint_bf16(self, data, coeffs, subset):
         chunks = self._bf16_chunks(subset)
-        for geo, n, om in chunks:
+        for geo, n, om, _ in chunks:
             self._rows_to_bf16(data, om, n)
+        fft = self.projector == "fft"
         for ib, b in enumerate(self.batches):
             k0, kb = ib * self.Kstride, b["K_batch"]
-            for ic, (geo, n, om) in enumerate(chunks):
+            for ic, (geo, n, om, a) in enumerate(chunks):
                 z = self._z(n)
                 self._pf_tc_adjoint(om, n, z, k0, self.Kstride)
+                if fft:     # the pieces' rows widened into the float32 batch sinogram, transformed once complete
+                    self._call("dfx_convert_rows", 0, self.coeffs_sino_C.data_ptr() + 4 * a * self.My * self.Kstride,
+                               self.Kstride, z.data_ptr() + 2 * k0, self.Ktot, n * self.My, kb, self._s())
+                    continue
                 # over several angle chunks the backprojections of the chunks are summed in the batch buffer
                 dst = self._img_k if ic == 0 else self._img_acc()
                 self._call("dfx_radon_backward_bf16", z.data_ptr() + 2 * k0, self.Ktot, dst.data_ptr(),
@@ -714,6 +827,9 @@ class SinglePhaseForwardOperator:
                 if ic > 0:
                     with torch.cuda.stream(self.stream()):
                         self._img_k.add_(dst)
+            if fft:
+                self._fft_run(False, None if subset is None else self._subset(subset), self.coeffs_sino_C.data_ptr(),
+                              self._img_k.data_ptr(), kb)
             self._call("dfx_scatter_channels", self._img_k.data_ptr(), coeffs.data_ptr(), self.npix, b["k_start"],
                        kb, self.Kstride, self._s())
 
@@ -731,26 +847,69 @@ class SinglePhaseForwardOperator:
         self._pf_tc_adjoint(e["omegas"], e["n"], z)
         return e["geo"], e["n"], z
 
-    def _bf16_update_batch(self, ib, geo, n, z, x_ptr, z_ptr, T_ptr, inv_p, lam, xb_ptr=None):
-        """SPDHG's update of batch ib from its columns of Z: the backprojection with the primal step fused (and the
-        BF16 copy of the new x written to xb_ptr)."""
+    def _bf16_update_batch(self, ib, geo, n, z, x_ptr, z_ptr, T_ptr, inv_p, lam, xb_ptr=None, subset=None):
+        """SPDHG's update of batch ib from its columns of Z (the n angles of subset m): the backprojection with the
+        primal step fused (and the BF16 copy of the new x written to xb_ptr). The Fourier-slice projector
+        backprojects the columns widened to float32, and the primal step follows as its own kernel."""
+        if self.projector == "fft":
+            kb, s = self.batches[ib]["K_batch"], self._s()
+            self._call("dfx_convert_rows", 0, self.coeffs_sino_C.data_ptr(), self.Kstride,
+                       z.data_ptr() + 2 * ib * self.Kstride, self.Ktot, n * self.My, kb, s)
+            self._fft_run(False, self._subset(subset), self.coeffs_sino_C.data_ptr(), self._img_k.data_ptr(), kb)
+            self._call("dfx_spdhg_primal_update", x_ptr, z_ptr, T_ptr, self._img_k.data_ptr(), float(inv_p),
+                       float(lam), self.batch_elems(), s)
+            if xb_ptr is not None:
+                self._call("dfx_f32_to_bf16", x_ptr, xb_ptr, self.batch_elems(), s)
+            return
         name = "dfx_radon_backward_spdhg_tc" if self.tc_backprojection else "dfx_radon_backward_spdhg_bf16"
         self._call(name, z.data_ptr() + 2 * ib * self.Kstride, self.Ktot, geo.data_ptr(), n, self.Nx, self.Ny,
                    self.My, self.Kstride, self.batches[ib]["K_batch"], self._kernel_id, int(self.radon_geo.n_taps),
                    x_ptr, z_ptr, T_ptr, float(inv_p), float(lam), xb_ptr, self._s())
 
-    def _bf16_forward_sino(self, subset, ib, src_ptr, src_bf16=False, ray=None):
+    def _bf16_forward_sino(self, subset, ib, src_ptr, src_bf16=False, ray=None, tiles=None):
         """Radon transform of batch ib (channel-fastest at src_ptr, float32 or BF16) for the angles of subset m into
-        Z (ray: a support ray table for images that are zero outside the support)."""
-        e = self._sub[self._subset(subset)]
+        Z (ray, tiles: a support ray table and the support's tile list, for images that are zero outside the
+        support)."""
+        m = self._subset(subset)
+        e = self._sub[m]
         if not src_bf16:
-            self._radon_forward_bf16(src_ptr, ib, self._z(e["n"]), e["omegas"], e["n"])
+            self._radon_forward_bf16(src_ptr, ib, self._z(e["n"]), e["omegas"], e["n"], m=m)
             return
+        if self.projector == "fft":
+            raise ValueError("the Fourier-slice projector transforms float32 images only")
         z = self._z(e["n"])
+        self._radon_bf16_image(src_ptr, z.data_ptr() + 2 * ib * self.Kstride, e["geo"], e["omegas"], e["n"],
+                               self.batches[ib]["K_batch"], ray=ray, tiles=tiles)
+
+    def _radon_bf16_image(self, src_ptr, dst_ptr, geo, om, n, kb, ray=None, tiles=None):
+        """The Radon output (BF16, row stride Ktot) of a BF16 channel-fastest batch at src_ptr for the n angles om
+        (geo: their geometry rows): on the tensor cores (dfx_radon_forward_tc) when the geometry admits them and
+        use_tc_forward is set, else through the ray table (ray: a support table; tiles: the support's tile list; an
+        image that is zero outside the support may skip the other tiles)."""
+        if self.use_tc_forward and getattr(self, "tc_forward", False):
+            tp, nt = (None, 0) if tiles is None else (tiles.data_ptr(), int(tiles.numel()))
+            self._call("dfx_radon_forward_tc", src_ptr, dst_ptr, self.Ktot, 0, geo.data_ptr(), n, self.Nx, self.Ny,
+                       self.My, self.Kstride, self._kernel_id, int(self.radon_geo.n_taps),
+                       float(self.radon_geo.scale), tp, nt, self._s())
+            return
         rp, ent = (self._ray_rp, self._ray_ent) if ray is None else ray[:2]
-        self._call("dfx_radon_forward_table_bf16_bf16", src_ptr, z.data_ptr() + 2 * ib * self.Kstride, self.Ktot,
-                   rp.data_ptr(), ent.data_ptr(), e["omegas"].data_ptr(), e["n"], self.My,
-                   self.Kstride, self.batches[ib]["K_batch"], float(self.radon_geo.scale), self._s())
+        self._call("dfx_radon_forward_table_bf16_bf16", src_ptr, dst_ptr, self.Ktot, rp.data_ptr(), ent.data_ptr(),
+                   om.data_ptr(), n, self.My, self.Kstride, kb, float(self.radon_geo.scale), self._s())
+
+    def support_tiles(self, supp):
+        """int32 device tensor of the 8 x 8 pixel tiles (row-major over the tile grid) holding at least one pixel of
+        a support mask (uint8 (Ny * Nx) device tensor); kept per mask content."""
+        key = bytes(supp.cpu().numpy())
+        hit = self._supp_tiles.get(key)
+        if hit is None:
+            m = supp.cpu().numpy().reshape(self.Ny, self.Nx).astype(bool)
+            ty, tx = -(-self.Ny // 8), -(-self.Nx // 8)
+            pad = np.zeros((ty * 8, tx * 8), bool)
+            pad[:self.Ny, :self.Nx] = m
+            any_ = pad.reshape(ty, 8, tx, 8).any(axis=(1, 3)).ravel()
+            hit = torch.as_tensor(np.flatnonzero(any_).astype(np.int32), device=self.device)
+            self._supp_tiles[key] = hit
+        return hit
 
     def _bf16_forward_rows(self, subset, data):
         """data rows of subset m = PF Z over all orientations (the rows are overwritten)."""
@@ -797,6 +956,7 @@ class SinglePhaseForwardOperator:
     def release_omega_subsets(self):
         self._sub = []
         self.omega_subsets = None
+        self._sub_version += 1          # angle lists held by the generated-PF buffers are stale now
 
     @property
     def _sub_omegas(self):
@@ -863,20 +1023,9 @@ class SinglePhaseForwardOperator:
 
     def _adjoint_batch(self, data, ib, target, k_target, K_target, subset=None):
         """A^T data of batch ib into orientations k_target .. k_target+Kb-1 of target (SPFO:1966-2033)."""
-        b = self.batches[ib]
-        Kb = b["K_batch"]
         s = self._s()
-        if subset is None:
-            geo, n_ang, om, m = self.geo_gpu, self.N_Omega, None, None
-        else:
-            m = self._subset(subset)
-            e = self._sub[m]
-            geo, n_ang, om = e["geo"], e["n"], e["omegas"]
-        alpha = float(np.float32(self.N_Omega / np.pi))
-        rp, col, val, compact = self._pf_batch(ib, False, m)
-        self._call("dfx_spmm_pf_adjoint", data.data_ptr(), rp.data_ptr(), col.data_ptr(), val.data_ptr(),
-                   self.coeffs_sino_C.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My, Kb,
-                   self.N_seg, self.Kstride, alpha, compact, s)
+        geo, n_ang, Kb = self._pf_adjoint_to_sino(data, ib, subset)
+        m = None if subset is None else self._subset(subset)
         self._radon_bwd(self.coeffs_sino_C.data_ptr(), self._img_k.data_ptr(), geo, n_ang, Kb, m)
         self._call("dfx_scatter_channels", self._img_k.data_ptr(), target.data_ptr(), self.npix, k_target, Kb,
                    self.Kstride, s)
@@ -906,6 +1055,11 @@ class SinglePhaseForwardOperator:
         Kb = self.batches[ib]["K_batch"]
         geo, n_ang, om, m = self._geo_of(subset)
         alpha = float(np.float32(self.N_Omega / np.pi))
+        if self.pf_mode == "dense":
+            if m is not None:
+                raise NotImplementedError("omega subsets need pf_mode 'sparse' or 'generated'")
+            self._dense_pf_product(ib, True, data.data_ptr(), self.coeffs_sino_C.data_ptr(), alpha)
+            return geo, n_ang, Kb
         rp, col, val, compact = self._pf_batch(ib, False, m)
         self._call("dfx_spmm_pf_adjoint", data.data_ptr(), rp.data_ptr(), col.data_ptr(), val.data_ptr(),
                    self.coeffs_sino_C.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My, Kb,
@@ -1072,7 +1226,8 @@ class SinglePhaseForwardOperator:
         for sb in self.sparse_batches or []:
             n += sum(v.numel() * v.element_size() for v in sb.values() if isinstance(v, torch.Tensor))
         for t in (getattr(self, "_gen_col", None), getattr(self, "_gen_val", None), self.pf_bf16,
-                  getattr(self, "_d_bf16", None), getattr(self, "_z_bf16", None), getattr(self, "_img_k2", None)):
+                  getattr(self, "_d_bf16", None), getattr(self, "_z_bf16", None), getattr(self, "_img_k2", None),
+                  getattr(self, "_pf_dense", None)):
             if t is not None:
                 n += t.numel() * t.element_size()
         return n
@@ -1088,10 +1243,12 @@ class SinglePhaseForwardOperator:
         self.release_omega_subsets()
         self.release_streamer()
         self._ray_supp = {}
+        self._supp_tiles = {}
         self._fft = None
         self.sparse_batches = None
         self.coeffs_sino_C = self._img_k = None
         self._gen_col = self._gen_val = None
+        self._pf_dense = None
         self.pf_bf16 = self._d_bf16 = self._z_bf16 = self._img_k2 = None
         self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
         self.stream().synchronize()          # this operator's work only (other streams keep running)

@@ -42,7 +42,7 @@ class Request:
     subsets: int = 8
     max_epochs: int = 100
     tol: float = 1e-3
-    precision: str = "fp32"
+    precision: str = "bf16"      # the BF16 tensor-core path (float32 step sizes and residual); "fp32" for float32
     max_gb: float = 2.0
     seed: int = 0
     id: int = 0
@@ -53,6 +53,7 @@ class Request:
     finished: float = 0.0
     epochs: int = 0
     deviance: list = field(default_factory=list)
+    timings: dict = field(default_factory=dict)   # build / setup / epochs / finish seconds of the worker
     result: Optional[np.ndarray] = None
     error: Optional[str] = None
 
@@ -61,16 +62,21 @@ class Request:
         return self.finished - self.arrival
 
 
-def estimate_request_bytes(cfg, K, n_rings, fill=0.15) -> int:
+def estimate_request_bytes(cfg, K, n_rings, fill=0.15, precision="fp32") -> int:
     """Device memory of a request, estimated before its operator exists: SPDHG's coefficient arrays (x, z, T in the
     batch layout and x in the (K, Ny, Nx) layout), its data arrays (b, y, S, D), both sparse PF copies at the given
-    fill (12 bytes per non-zero), the ray table and the batch buffers. n_rings: an upper bound (the reflections)."""
+    fill (12 bytes per non-zero, plus the eta-blocked forward copy, ~6 more), the ray table and the batch buffers;
+    with precision "bf16" also the dense BF16 PF (2 bytes per entry), the BF16 copies of x and of the data rows and
+    the Radon output of the subset angles. n_rings: an upper bound (the reflections)."""
     npix = int(cfg["Nx"]) * int(cfg["Ny"])
     R, My = int(cfg["N_Omega"]), int(cfg["My"])
     CP = int(cfg["N_eta"]) * int(n_rings)
     coeff = 4 * K * npix
     data = 4 * R * My * CP
-    return int(4 * coeff + 4 * data + 12 * fill * R * K * CP + 18 * R * npix + 8 * 1024 * (R * My + npix) + (1 << 28))
+    n = 4 * coeff + 4 * data + 18 * fill * R * K * CP + 18 * R * npix + 8 * 1024 * (R * My + npix) + (1 << 28)
+    if precision == "bf16":
+        n += 2 * R * K * CP + coeff // 2 + data // 2 + 2 * R * My * K
+    return int(n)
 
 
 class Scheduler:
@@ -143,7 +149,8 @@ class ReconstructionServer:
     def submit(self, req: Request) -> int:
         with self._lock:
             hkl = getattr(req.material, "hkl", None)
-            nbytes = estimate_request_bytes(req.cfg, len(req.grid), len(hkl) if hkl is not None else 8)
+            nbytes = estimate_request_bytes(req.cfg, len(req.grid), len(hkl) if hkl is not None else 8,
+                                            precision=req.precision)
             self.sched.enqueue(self._next_id, nbytes)       # MemoryError if it can never fit
             req.id = self._next_id
             self._next_id += 1
@@ -176,11 +183,17 @@ class ReconstructionServer:
         if lat.size == 0:
             return {"requests": 0}
         span = max(r.finished for r in self.done) - min(r.arrival for r in self.done)
+        ok = [r for r in self.done if r.error is None]
+        parts = {k: float(np.sum([r.timings.get(k, 0.0) for r in ok])) for k in ("build", "setup", "epochs", "finish")}
+        queued = [r.admitted - r.arrival for r in ok]
         return {"requests": int(lat.size), "p50_s": float(np.percentile(lat, 50)),
                 "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
                 "throughput_rps": float(lat.size / span) if span > 0 else None,
                 "epochs": int(sum(r.epochs for r in self.done)),
-                "failed": int(sum(r.error is not None for r in self.done))}
+                "failed": int(sum(r.error is not None for r in self.done)),
+                "worker_s": {k: round(v, 1) for k, v in parts.items()},
+                "queued_s_p50": float(np.percentile(queued, 50)) if queued else None,
+                "makespan_s": float(span)}
 
     # ---------------------------------------------------------------- server side
     def _loop(self):
@@ -223,13 +236,20 @@ def run_request(req: Request, device, stream):
     import torch
     from .operator import SinglePhaseForwardOperator
     from .spdhg import SPDHGPoisson
+    t0 = time.perf_counter()
+    # SPDHG runs over omega subsets, which need a sparse PF mode: "auto" with the dense switch off (the sparse
+    # matrix stored as far as memory allows, the rest generated in every call)
     op = SinglePhaseForwardOperator(req.cfg, req.material, req.grid, req.max_gb, normalized=True, ctx=device,
-                                    queue=stream, precision=req.precision)
+                                    queue=stream, precision=req.precision, sparse_max_fill=1.0,
+                                    sparse_max_fill_partial=1.0)
+    t1 = time.perf_counter()
     try:
         sp = SPDHGPoisson(op, subsets=req.subsets, seed=req.seed)
         sp.use_graphs = req.graphs
         x0 = torch.zeros(op.coeff_shape, dtype=torch.float32, device=device)
         sp._setup(x0, req.counts)
+        stream.synchronize()
+        t2 = time.perf_counter()
         devs = []
         for e in range(req.max_epochs):
             last = e + 1 == req.max_epochs
@@ -237,8 +257,10 @@ def run_request(req: Request, device, stream):
             devs.append(float(sp._f))
             if len(devs) > 1 and abs(devs[-2] - devs[-1]) <= req.tol * abs(devs[-1]):
                 break
+        t3 = time.perf_counter()
         x = sp._finish()
         out = x.cpu().numpy()
+        req.timings = {"build": t1 - t0, "setup": t2 - t1, "epochs": t3 - t2, "finish": time.perf_counter() - t3}
         return out, len(devs), devs
     finally:
         op.free_memory()

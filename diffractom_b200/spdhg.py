@@ -164,7 +164,8 @@ class SPDHGPoisson:
         dual step and update instead); then the forward of the new x for subset fwd ("full": all rows) added to D
         (spdhg_poisson.py:430-484)."""
         op = self.op
-        if op.precision == "bf16" and fwd == "full" and adj is None and not tv and self.bf16_diagnostics:
+        if (op.precision == "bf16" and fwd == "full" and adj is None and not tv and self.bf16_diagnostics
+                and op.projector != "fft"):
             self._full_forward_bf16()
             return
         if op.precision == "bf16" and fwd != "full":
@@ -203,17 +204,15 @@ class SPDHGPoisson:
         op = self.op
         be = op.batch_elems()
         X = self.X
-        rp, ent = (op._ray_rp, op._ray_ent) if self._ray is None else self._ray[:2]
-        for geo, n, om in op._bf16_chunks(None):
+        for geo, n, om, _ in op._bf16_chunks(None):
             z = op._z(n)
 
-            def compute(ib, s, z=z, n=n, om=om):
+            def compute(ib, s, z=z, n=n, om=om, geo=geo):
                 xb = self.xkb.data_ptr() + (2 * ib * be if X.resident else 0)
                 if not X.resident:
                     _lib.call("dfx_f32_to_bf16", X.ptr(ib, s), xb, be, op._s())
-                _lib.call("dfx_radon_forward_table_bf16_bf16", xb, z.data_ptr() + 2 * ib * op.Kstride, op.Ktot,
-                          rp.data_ptr(), ent.data_ptr(), om.data_ptr(), n, op.My, op.Kstride,
-                          op.batches[ib]["K_batch"], float(op.radon_geo.scale), op._s())
+                op._radon_bf16_image(xb, z.data_ptr() + 2 * ib * op.Kstride, geo, om, n, op.batches[ib]["K_batch"],
+                                     ray=self._ray, tiles=self._tiles)
 
             self.pipe.run([X], [], compute)
             op._pf_tc_forward(z, om, n, self.D)
@@ -224,25 +223,30 @@ class SPDHGPoisson:
         to the BF16 Radon output of all batches, each batch's backprojection applies the primal step and projects the
         new x for subset fwd into its columns of that output, and one tensor-core launch overwrites subset fwd's data
         rows (full forward passes: _full_forward_bf16). The BF16 copy of x that the forward reads is kept for all
-        batches when x is resident, else made per batch (one buffer)."""
+        batches when x is resident, else made per batch (one buffer). With the Fourier-slice projector the forward
+        transforms the float32 x (no BF16 copy) and the rows of its output are rounded to BF16."""
         op = self.op
         be = op.batch_elems()
         X, Z, T = self.X, self.Z, self.T
+        fft = op.projector == "fft"
         if adj is not None:
             geo, n, zb = op._bf16_adjoint_sino(self.D, adj)
 
         def compute(ib, s):
-            xb = self.xkb.data_ptr() + (2 * ib * be if X.resident else 0)
+            xb = None if fft else self.xkb.data_ptr() + (2 * ib * be if X.resident else 0)
             if tv:                          # the TV block, then the BF16 copy of the new x
                 self._tv_batch(ib, s)
-                _lib.call("dfx_f32_to_bf16", X.ptr(ib, s), xb, be, op._s())
+                if not fft:
+                    _lib.call("dfx_f32_to_bf16", X.ptr(ib, s), xb, be, op._s())
             elif adj is not None:
                 op._bf16_update_batch(ib, geo, n, zb, X.ptr(ib, s), Z.ptr(ib, s), T.ptr(ib, s), self._inv_p_data,
-                                      self.lam, xb)
-            elif not X.resident:
+                                      self.lam, xb, subset=adj)
+            elif not X.resident and not fft:
                 _lib.call("dfx_f32_to_bf16", X.ptr(ib, s), xb, be, op._s())
-            if fwd is not None:
-                op._bf16_forward_sino(fwd, ib, xb, src_bf16=True, ray=self._ray)
+            if fwd is not None and fft:
+                op._bf16_forward_sino(fwd, ib, X.ptr(ib, s))
+            elif fwd is not None:
+                op._bf16_forward_sino(fwd, ib, xb, src_bf16=True, ray=self._ray, tiles=self._tiles)
 
         self.pipe.run(*self._arrays(adj is not None, tv), compute)
         if fwd is not None:
@@ -540,21 +544,22 @@ class SPDHGPoisson:
         self.dzk = torch.empty(be, dtype=torch.float32, device=dev)
         self.x = None
         # a host x0 of a resident x is uploaded after the step sizes' passes are queued, on a side stream, so that
-        # the copy overlaps them (they do not read x)
-        upload_x = self.X.resident and not self._x_on_gpu
-        if self.X.resident:
-            if self._x_on_gpu:
-                self.x = x0
-                op.to_batches(self.x, self.X.dev)
-            else:
-                self.x = torch.empty(cshape, dtype=torch.float32, device=dev)
-                x_alloc = torch.cuda.Event()
-                x_alloc.record(op.stream())             # the side stream writes x after this point only
+        # the copy overlaps them (they do not read x). When some array is streamed, device memory is short of a
+        # whole (K, Ny, Nx) array beside the state: host arrays then move through the batch-sized staging buffers
+        # (resident arrays included), here and when the run ends.
+        upload_x = self.X.resident and not self._x_on_gpu and self._stage is None
+        if self._x_on_gpu:
+            self.x = x0
+            op.to_batches(self.x, self.X.dev)
+        elif upload_x:
+            self.x = torch.empty(cshape, dtype=torch.float32, device=dev)
+            x_alloc = torch.cuda.Event()
+            x_alloc.record(op.stream())                 # the side stream writes x after this point only
         else:
             self._stage.load(self._host_x.reshape(-1), self.X, self.pipe)
         if state is not None and state.get("z") is not None:
             z0 = as_host(state["z"], cshape, "state['z']")
-            if self.Z.resident:
+            if self.Z.resident and self._stage is None:
                 op.to_batches(torch.as_tensor(z0, device=dev), self.Z.dev)
             else:
                 self._stage.load(z0.reshape(-1), self.Z, self.pipe)
@@ -572,7 +577,7 @@ class SPDHGPoisson:
                         op._fill(arr.dev, 0.0)
                     else:
                         arr.host.zero_()
-                elif arr.resident:
+                elif arr.resident and self._stage is None:
                     op.to_batches(torch.as_tensor(q0, device=dev), arr.dev)
                 else:
                     self._stage.load(q0.reshape(-1), arr, self.pipe)
@@ -580,17 +585,19 @@ class SPDHGPoisson:
             self.dqy = torch.empty(be, dtype=torch.float32, device=dev)
 
         self._ray = op.support_ray_table(supp) if supp is not None and self.use_support_table else None
+        self._tiles = (op.support_tiles(supp) if supp is not None and self.use_support_table
+                       and op.precision == "bf16" else None)
         # S from the row sums A 1_S (spdhg_poisson.py:621-629); with a BF16 operator from the BF16 operator that the
         # iterations apply (the step sizes of the operator in use, at a quarter of the float32 passes' time)
-        bf16 = op.precision == "bf16" and self.bf16_steps
+        bf16 = op.precision == "bf16" and self.bf16_steps and op.projector != "fft"
         op._fill(self.D, 0.0)
         if bf16:
-            for geo, n, om in op._bf16_chunks(None):
+            for geo, n, om, a in op._bf16_chunks(None):
                 z = op._z(n)
                 for ib, bt in enumerate(op.batches):
                     _lib.call("dfx_batch_support", self.dzk.data_ptr(), None, sp, npix, op.Kstride, bt["K_batch"],
                               0.0, 0, s)
-                    op._radon_forward_bf16(self.dzk.data_ptr(), ib, z, om, n)
+                    op._radon_forward_bf16(self.dzk.data_ptr(), ib, z, om, n, row0=a)
                 op._pf_tc_forward(z, om, n, self.D)
         else:
             for ib, bt in enumerate(op.batches):
@@ -660,7 +667,7 @@ class SPDHGPoisson:
         # the host arrays the run ends with (z, y, and a NumPy x0 that receives x) have their pages mapped by the
         # copy threads while the device iterates, so that the final downloads run at the copy rate
         self._host_out, self._prefault = None, []
-        if self.Z.resident:
+        if self.Z.resident and self._stage is None:
             hc = host_copier()
             z_host, y_host = np.empty(cshape, np.float32), np.empty(dshape, np.float32)
             self._prefault = hc.prefault(z_host, False) + hc.prefault(y_host, False)
@@ -676,7 +683,7 @@ class SPDHGPoisson:
         self._f = float("nan")
         self._seq = self._epoch_sequence()
         self.xkb = None
-        if op.precision == "bf16":       # the BF16 copy of x that the forward projections read
+        if op.precision == "bf16" and op.projector != "fft":   # the BF16 copy of x that the forward projections read
             if self.X.resident:
                 self.xkb = torch.empty(nbt * be, dtype=torch.bfloat16, device=dev)
                 _lib.call("dfx_f32_to_bf16", self.X.dev.data_ptr(), self.xkb.data_ptr(), nbt * be, s)
@@ -698,7 +705,7 @@ class SPDHGPoisson:
         # the closing full forward and objective of the run's last epoch can wait for _finish, which overlaps them
         # with the state's downloads (nobody reads the objective before: no callback, no printing)
         defer = (defer_final and final and callback is None and not verbose and self.tv == 0 and self.X.resident
-                 and self.Z.resident)
+                 and self.Z.resident and self._stage is None)
         for e in range(n_epochs):
             ep = self._ep0 + len(self.iter_stats) + 1
             last = final and e + 1 == n_epochs
@@ -759,8 +766,9 @@ class SPDHGPoisson:
 
     def _graphs_on(self):
         op = self.op
-        return (self.use_graphs and len(self.iter_stats) >= 1 and self.shards is None and self.X.resident
-                and self.tv == 0
+        # a generated BF16 PF is made (or found in its buffers) when a product runs: the host picks, so no graphs
+        return (self.use_graphs and len(self.iter_stats) >= 1 and self.shards is None and self._stage is None
+                and self.tv == 0 and (op.precision != "bf16" or op.pf_bf16 is not None)
                 and torch.cuda.current_stream(op.device) != torch.cuda.default_stream(op.device))
 
     def _replay(self, key, fn):
@@ -786,7 +794,7 @@ class SPDHGPoisson:
         """x in the (K, Ny, Nx) layout of the caller's array (the CUDA x0, or the NumPy x0's device copy and x0)."""
         self._wait_prefault()
         op = self.op
-        if self.X.resident:
+        if self.x is not None:
             op.from_batches(self.X.dev, self.x)
             if not self._x_on_gpu:
                 host_copier().to_host(self.x, self._host_x)
@@ -843,7 +851,7 @@ class SPDHGPoisson:
                 op.from_batches(self.X.dev, self.x)
             return self._finish_state(z_host, y_host, {})
         self._x_out()
-        if self.Z.resident:
+        if self.Z.resident and self._stage is None:
             z = torch.empty(op.coeff_shape, dtype=torch.float32, device=op.device)
             op.from_batches(self.Z.dev, z)
             z_host = self._host_out[0]
@@ -857,7 +865,7 @@ class SPDHGPoisson:
             if arr is None:
                 continue
             h = np.empty(op.coeff_shape, np.float32)
-            if arr.resident:
+            if arr.resident and self._stage is None:
                 q = torch.empty(op.coeff_shape, dtype=torch.float32, device=op.device)
                 op.from_batches(arr.dev, q)
                 host_copier().to_host(q, h)
@@ -877,7 +885,7 @@ class SPDHGPoisson:
                             "graph_replays": self.graph_replays, **self.scales}
         out = self.x if self._x_on_gpu else self._host_x
         self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = None
-        self.X = self.Z = self.T = self.dzk = self.xkb = self._stage = self._ray = None
+        self.X = self.Z = self.T = self.dzk = self.xkb = self._stage = self._ray = self._tiles = None
         self.QX = self.QY = self.dqx = self.dqy = None
         self._graphs = {}
         self.x = None

@@ -238,6 +238,14 @@ int dfx_spmm_pf_forward_blocked(const float *sino, const int32_t *fb_ptr, const 
                                 const uint8_t *fb_mask, float *data, const int32_t *omegas, int n_sub, int my, int P,
                                 int C, int kstride, int kb, void *stream);
 
+/* replaces batched_gemm_clblast / batched_gemm_clblast_adj (SPFO:2063-2127), the products of pf_mode "dense": pf is
+ * the batch's float32 PF (n_omega, kb, cp) (dfx_pf_dense); adjoint 0: out = data (n_omega, my, cp) += in (n_omega, my,
+ * kstride: the Radon output) . PF per angle; adjoint 1: out (n_omega, my, kstride) = alpha in (data) . PF^T per angle,
+ * channels kb .. kstride-1 set to 0. One strided batched cuBLAS SGEMM over the angles in float32 (pedantic math: no
+ * TF32); the cuBLAS handle is made on the first call of each host thread on each device. */
+int dfx_pf_dense_products(int adjoint, const float *pf, int n_omega, int kb, int cp, const float *in, float *out,
+                          int my, int kstride, float alpha, void *stream);
+
 /* replaces zero_rows (SPFO:126-132): data rows omegas[s] (row_len floats each) <- 0. */
 int dfx_zero_rows(float *data, const int32_t *omegas, int n_sub, int64_t row_len, void *stream);
 
@@ -257,6 +265,11 @@ int dfx_spdhg_dual_update(float *y, float *d, const float *sig, const float *b, 
 /* replaces spdhg_update (spdhg_poisson.py:95-106): z += dz; x = T > 0 ? max(0, x - T (z + inv_p dz + lam)) : 0. */
 int dfx_spdhg_primal_update(float *x, float *z, const float *T, const float *dz, float inv_p, float lam, int64_t n,
                             void *stream);
+/* The same step with T stored in BF16 (widened exactly when read). */
+int dfx_spdhg_primal_update_t16(float *x, float *z, const void *T_bf16, const float *dz, float inv_p, float lam,
+                                int64_t n, void *stream);
+/* out[i] = bf16(in[i]) rounded toward zero (stored step sizes never above their float32 values). */
+int dfx_f32_to_bf16_rz(const float *in, void *out, int64_t n, void *stream);
 
 /* replaces dual_steps (optimization/pdhg_poisson.py:79-84): sig = w != 0 && rowsum > 0 ? sigma0 / rowsum : 0. */
 int dfx_dual_steps(float *sig, const float *rowsum, const float *w, int64_t pw, float sigma0, int64_t n, void *stream);
@@ -300,21 +313,43 @@ int dfx_dot_f64(const float *x, const float *y, int64_t n, double *out, void *sc
  * float32 pf_entry values (dfx_pf_dense) rounded to nearest-even BF16. */
 int dfx_pf_dense_bf16(const dfx_pf_geometry *g, int k0, int kb, int64_t koff, int64_t ktot, int cp_pad, void *out,
                       void *stream);
+/* The same entries for the n_rows angles rows[s] only: out (n_rows, ktot, cp_pad), plane s = angle rows[s] (the PF of
+ * one omega subset, generated for every pass in place of a stored dense PF of all angles). */
+int dfx_pf_dense_bf16_rows(const dfx_pf_geometry *g, const int32_t *rows, int n_rows, int k0, int kb, int64_t koff,
+                           int64_t ktot, int cp_pad, void *out, void *stream);
 
 /* replaces batched_gemm_clblast (SPFO:2063-2098) and, in the BF16 path, spmm_pf_forward_c (pf_kernels.cl:597-641):
  * for the n_sub angles r = omegas[s] (omegas NULL: r = s), data[r, y, j] (+)= sum_k PF[r, k, j] Z[s, y, k] over the
  * orientations k = k0 .. k0+kn-1 of the ktot, with tcgen05 BF16 MMAs and float32 accumulation. pf_bf16 (n_omega,
  * ktot, cp_pad), z_bf16 (n_sub, my, ktot) BF16, data (n_omega, my, cp) float32; accumulate = 0 overwrites the rows.
- * ktot, k0 and cp_pad multiples of 8, both BF16 arrays 16-byte aligned. */
+ * ktot, k0 and cp_pad multiples of 8, both BF16 arrays 16-byte aligned. pf_compact: pf_bf16 holds the n_sub listed
+ * angles only, (n_sub, ktot, cp_pad), angle s at row s (a PF generated for one subset). */
 int dfx_pf_tc_forward(const void *pf_bf16, int64_t ktot, int64_t k0, int64_t kn, int cp, int cp_pad, int n_omega,
                       const void *z_bf16, const int32_t *omegas, int n_sub, int my, float *data, int accumulate,
-                      void *stream);
+                      int pf_compact, void *stream);
 /* replaces batched_gemm_clblast_adj (SPFO:2100-2127) and, in the BF16 path, spmm_pf_adjoint_c (pf_kernels.cl:644-687):
  * Z[s, y, k] = alpha sum_j PF[r, k, j] D[r, y, j] for k = k0 .. k0+kn-1 (BF16 out, float32 accumulation), d_bf16
- * (n_omega, my, cp_pad); the other orientations of Z are left as they are. */
+ * (n_omega, my, cp_pad); the other orientations of Z are left as they are; pf_compact as above. */
 int dfx_pf_tc_adjoint(const void *pf_bf16, int64_t ktot, int64_t k0, int64_t kn, int cp, int cp_pad, int n_omega,
                       const void *d_bf16, const int32_t *omegas, int n_sub, int my, float alpha, void *z_bf16,
-                      void *stream);
+                      int pf_compact, void *stream);
+/* Strided row conversion between float32 and BF16 (the Fourier-slice projector's float32 sinogram and the BF16
+ * Radon output of the tensor-core products): to_bf16 1: b16[r * ld_b16 + c] = bf16(f32[r * ld_f32 + c]) (nearest-
+ * even); 0: f32[...] = b16[...] (exact), for r < rows, c < cols. */
+int dfx_convert_rows(int to_bf16, float *f32, int64_t ld_f32, void *b16, int64_t ld_b16, int64_t rows, int cols,
+                     void *stream);
+
+/* Forward projection of a BF16 channel-fastest batch on the tensor cores (tcgen05; the BF16 path's replacement of
+ * radon_forward_k, radon_kernels.cl:44-101): sino[a, s, k] = scale * sum_p K(t_a(p) - s) img[p, k] for the n_angles
+ * rows of geo (the launch's angles), float32 accumulation, written as BF16 (out_f32 0) or float32 with row stride
+ * sino_ld. 8 x 8 pixel tiles against 32-bin windows starting at a multiple of 16 bins, weights as BF16 hi + lo parts;
+ * admissible when every tile's taps span at most 17 bins (7 (|X| + |Y|) + 2 hw + 2 <= 17 per angle), n_det + 31 <=
+ * 512 and kstride is a multiple of 64; taps outside a window are skipped and flagged (DFX_TC_WINDOW). tiles (NULL: all
+ * tiles): the n_tiles tile indices (row-major over ceil(ny / 8) x ceil(nx / 8)) to project; the others must be zero. */
+int dfx_radon_forward_tc(const void *img_bf16, void *sino, int64_t sino_ld, int out_f32, const float *geo,
+                         int n_angles, int nx, int ny, int n_det, int kstride, int kernel, int n_taps, float scale,
+                         const int32_t *tiles, int n_tiles, void *stream);
+
 /* Bits of device-side waits of the tensor-core kernels that ran out since the last reset (DFX_TC_TIMEOUT); the
  * kernels return early on expiry and leave their outputs undefined. Synchronous; no reference counterpart. */
 #define DFX_TC_TIMEOUT 1u

@@ -158,3 +158,38 @@ def test_tc_backprojection_many_tiles_per_cta(kernel):
     g = radon_geometry(ang, nx, ny, ns, float(max(nx, ny)), float(ns), 0.37, np.pi / R, kernel=kernel)
     geo = torch.as_tensor(g.geo, device="cuda")
     _tc_vs_simt(geo, R, nx, ny, ns, 1200, 1 if kernel == "trapezoid" else 0, int(g.n_taps), seed=3)
+
+
+def test_generated_bf16_pf_equals_the_stored_one(golden):
+    """bf16_pf="generated" (no PF of all angles kept; each tensor-core product generates the PF of its angles into
+    one of two buffers) computes the stored PF's operator bit for bit: full and subset products, and a BF16 SPDHG
+    run (the same iterates, deviances and state)."""
+    from diffractom_b200 import SinglePhaseForwardOperator, SPDHGPoisson
+    d = golden("al5_small")
+    cfg, mat, grid = case_inputs(d)
+    ops = [SinglePhaseForwardOperator(cfg, mat, grid, 1e-5, normalized=True, quadrature=d["quadrature"],
+                                      precision="bf16", bf16_pf=mode) for mode in ("stored", "generated")]
+    assert ops[0].bf16_pf_storage == "stored" and ops[1].bf16_pf_storage == "generated" and ops[1].pf_bf16 is None
+    rng = np.random.default_rng(8)
+    x = torch.as_tensor(rng.random(ops[0].coeff_shape).astype(np.float32), device="cuda")
+    y = torch.as_tensor(rng.random(ops[0].data_shape).astype(np.float32), device="cuda")
+    outs = []
+    for op in ops:
+        op.set_omega_subsets(3)
+        r = []
+        for sub in (None, 0, 2, 0):
+            fx, ay = torch.zeros_like(y), torch.empty_like(x)
+            op.direct_cl(x, fx, subset=sub)
+            op.adjoint_cl(y, ay, subset=sub)
+            r += [fx.cpu(), ay.cpu()]
+        outs.append(r)
+    for a, b in zip(*outs):
+        assert torch.equal(a, b)
+    b = np.random.default_rng(3).poisson(np.abs(outs[0][0].numpy()) * 50).astype(np.float32)
+    runs = []
+    for op in ops:
+        sp = SPDHGPoisson(op, subsets=3, seed=4)
+        xr = sp.run(torch.zeros(op.coeff_shape, device="cuda"), b, 3, diagnostics_interval=1).cpu().numpy()
+        runs.append((xr, [s["f"] for s in sp.iter_stats], sp.state["y"]))
+    assert np.array_equal(runs[0][0], runs[1][0]) and runs[0][1] == runs[1][1]
+    assert np.array_equal(runs[0][2], runs[1][2])

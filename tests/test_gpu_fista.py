@@ -15,7 +15,7 @@ def _problem(golden, name="diff_midpoint_hat", seed=7, gain=0.05):
     d = golden(name)
     cfg, mat, grid = case_inputs(d)
     op = SinglePhaseForwardOperator(cfg, mat, grid, 1e-5, normalized=True, quadrature=d["quadrature"],
-                                    radon_kernel=d["kernel"])
+                                    radon_kernel=d["kernel"], pf_mode="sparse")
     rng = np.random.default_rng(seed)
     x_true = (rng.random(op.coeff_shape) * (rng.random(op.coeff_shape) < 0.3) * op.support_mask()[None]
               ).astype(np.float32)

@@ -1,7 +1,8 @@
 """The Fourier-slice projector on the GPU (dfx_fr_forward / dfx_fr_backward: pad, cuFFT, slices, lines; lines,
 cuFFT, spread, cuFFT, crop) against the exact Fourier-slice projection of the oracle, on channel-fastest batches with
 padding channels and several channel slices; a subset's projector gives its angles' rows; forward and backward are
-transposes; the operator with projector="fft" against the oracle's operator."""
+transposes; the operator with projector="fft" against the oracle's operator; precision "bf16" with it (the BF16
+contraction of the float32 transforms' output) against the float32 operator, with T streamed."""
 import numpy as np
 import pytest
 
@@ -138,3 +139,55 @@ def test_spdhg_with_fourier_projector_runs(golden):
     f = [s["f"] for s in sp.iter_stats if s["f"] is not None]
     assert len(f) == 2 and np.isfinite(f).all() and f[1] < f[0]
     assert np.all(x[:, ~op.support_mask()] == 0) and x.min() >= 0
+
+
+def test_bf16_contraction_with_fourier_projector(golden):
+    """precision "bf16" with projector "fft": the Fourier-slice transforms run in float32 and their output is
+    rounded to BF16 once for the tensor-core PF products (PF stored or generated per subset). Forward, adjoint and a
+    subset's rows within 1e-2 of the float32 operator's; SPDHG with T streamed (x and z resident, host arrays
+    through the staging buffers) gives the resident run's iterates, deviances and state bit for bit, and its
+    deviances stay within 1e-3 of the float32 run's."""
+    from conftest import case_inputs
+    from diffractom_b200 import SinglePhaseForwardOperator, SPDHGPoisson
+    d = golden("al5_small")
+    cfg, mat, grid = case_inputs(d)
+    mk = lambda **kw: SinglePhaseForwardOperator(cfg, mat, grid, 1e-5, normalized=True, quadrature=d["quadrature"],
+                                                 projector="fft", **kw)
+    op32 = mk()
+    rng = np.random.default_rng(4)
+    x = rng.random(op32.coeff_shape).astype(np.float32)
+    y = rng.random(op32.data_shape).astype(np.float32)
+    xt, yt = torch.as_tensor(x, device="cuda"), torch.as_tensor(y, device="cuda")
+    f32, a32 = op32.direct(xt).cpu().numpy(), op32.adjoint(yt).cpu().numpy()
+    op32.set_omega_subsets(3)
+    s32 = torch.zeros(op32.data_shape, device="cuda")
+    op32.direct_cl(xt, s32, subset=2)
+    for bf16_pf in ("stored", "generated"):
+        op = mk(precision="bf16", bf16_pf=bf16_pf)
+        assert op.projector == "fft" and op.precision == "bf16" and not op.tc_forward
+        assert np.abs(op.direct(xt).cpu().numpy() - f32).max() <= 1e-2 * np.abs(f32).max()
+        assert np.abs(op.adjoint(yt).cpu().numpy() - a32).max() <= 1e-2 * np.abs(a32).max()
+        op.set_omega_subsets(3)
+        s = torch.zeros(op.data_shape, device="cuda")
+        op.direct_cl(xt, s, subset=2)
+        rows = op.omega_subsets[2]
+        assert np.abs((s - s32).cpu().numpy()[rows]).max() <= 1e-2 * np.abs(f32).max()
+        assert not s.cpu().numpy()[np.setdiff1d(np.arange(op.N_Omega), rows)].any()
+
+    op = mk(precision="bf16")
+    x_true = (rng.random(op.coeff_shape) * (rng.random(op.coeff_shape) < 0.2) * op.support_mask()[None]
+              ).astype(np.float32)
+    b = rng.poisson(np.maximum(op32.direct(torch.as_tensor(x_true, device="cuda")).cpu().numpy(), 0) * 50
+                    ).astype(np.float32)
+    runs = {}
+    for key, o, resident in (("f32", op32, "all"), ("all", op, "all"), ("xz", op, ["x", "z"])):
+        sp = SPDHGPoisson(o, subsets=3, seed=1, resident=resident)
+        xr = sp.run(np.zeros(op.coeff_shape, np.float32), b, 4, diagnostics_interval=1)
+        runs[key] = (xr, [st["f"] for st in sp.iter_stats], sp.state, sp.final_stats["resident"])
+    assert runs["xz"][3] == ("x", "z")
+    assert np.array_equal(runs["xz"][0], runs["all"][0]) and runs["xz"][1] == runs["all"][1]
+    assert np.array_equal(runs["xz"][2]["z"], runs["all"][2]["z"])
+    assert np.array_equal(runs["xz"][2]["y"], runs["all"][2]["y"])
+    np.testing.assert_allclose(runs["all"][1], runs["f32"][1], rtol=1e-3)
+    f = runs["all"][1]
+    assert np.isfinite(f).all() and f[-1] < f[0]

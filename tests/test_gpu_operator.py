@@ -48,7 +48,7 @@ def test_forward_adjoint_match_oracle_and_reference(golden, name):
 @pytest.mark.parametrize("name", ["diff_auto_trapezoid", "al5_small", "ti8_small"])
 def test_sparse_pf_structure_is_bit_exact(golden, name):
     d = golden(name)
-    op = make_operator(d)
+    op = make_operator(d, pf_mode="sparse")
     orc = oracle_of(op)
     for sb, b in zip(op.sparse_batches, op.batches):
         ref = orc.csr(b["k_start"], b["K_batch"])
@@ -160,7 +160,7 @@ def test_fused_backprojection_update_equals_unfused(golden):
 
 def test_argument_errors(golden):
     d = golden("diff_midpoint_hat")
-    op = make_operator(d)
+    op = make_operator(d, pf_mode="sparse")
     with pytest.raises(TypeError):
         op.direct_cl(np.zeros(op.coeff_shape, np.float32), torch.empty(op.data_shape, device="cuda"))
     with pytest.raises(ValueError):
@@ -236,14 +236,26 @@ def test_estimate_L_power_streamed(golden):
     assert abs(Lp / L - 1) < 1e-2
 
 
-def test_dense_pf_mode_runs_the_sparse_products(golden):
-    """pf_mode="dense" (the reference's GEMM path) applies the same PF matrix: it runs the sparse products."""
+def test_dense_pf_mode_gemm_products(golden):
+    """pf_mode "dense" (the reference's float32 GEMM path, SPFO:2063-2127): the batch's PF generated in every call and
+    applied by batched SGEMMs, forward and adjoint within 1e-5 of the sparse products and of the oracle; "auto" takes
+    it above max_fill (SPFO:1249-1263); omega subsets need a sparse mode (NotImplementedError, as the reference)."""
     d = golden("diff_auto_trapezoid")
-    with pytest.warns(UserWarning, match="dense"):
-        dense = make_operator(d, pf_mode="dense")
+    dense = make_operator(d, pf_mode="dense")
     sparse = make_operator(d, pf_mode="sparse")
-    assert dense.pf_mode == "sparse"
-    assert np.array_equal(dense.direct(d["c"]), sparse.direct(d["c"]))
+    auto = make_operator(d)                                # 59 % fill > 30 %
+    assert dense.pf_mode == "dense" and auto.pf_mode == "dense" and sparse.pf_mode == "sparse"
+    assert len(dense.batches) > 1
+    orc = oracle_of(dense)
+    c = torch.as_tensor(d["c"], device="cuda")
+    r = torch.as_tensor(d["r"], device="cuda")
+    fd, fs = dense.direct(c).cpu().numpy(), sparse.direct(c).cpu().numpy()
+    ad, as_ = dense.adjoint(r).cpu().numpy(), sparse.adjoint(r).cpu().numpy()
+    assert rel(fd, fs) < 1e-5 and rel(ad, as_) < 1e-5
+    assert rel(fd, orc.forward(d["c"])) < 1e-5 and rel(ad, orc.adjoint(d["r"])) < 1e-5
+    assert np.array_equal(dense.direct(d["c"]), fd)        # NumPy (streamed batches) path, same bits
+    with pytest.raises(NotImplementedError):
+        dense.set_omega_subsets(3)
 
 
 def test_pf_storage_modes_compute_the_same_operator(golden):

@@ -17,7 +17,7 @@ def _requests(golden):
     for i, name in enumerate(["al5_small", "ti8_small", "adj_0_360"]):
         d = golden(name)
         cfg, mat, grid = case_inputs(d)
-        op = SinglePhaseForwardOperator(cfg, mat, grid, 0.5, normalized=True)
+        op = SinglePhaseForwardOperator(cfg, mat, grid, 0.5, normalized=True, pf_mode="sparse")
         rng = np.random.default_rng(20 + i)
         x_true = (rng.random(op.coeff_shape) * (rng.random(op.coeff_shape) < 0.2) * op.support_mask()[None]
                   ).astype(np.float32)

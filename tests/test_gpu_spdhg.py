@@ -82,7 +82,7 @@ def test_spdhg_streamed_state_equals_resident(golden, precision):
                     callback=cb("ref")).cpu().numpy()
     f_ref = [s["f"] for s in ref.iter_stats]
     assert ref.resident_used == ("x", "z", "T")
-    for resident in ("none", ["x"], ["z", "T"], ["T"], "all"):
+    for resident in ("none", ["x"], ["x", "z"], ["z", "T"], ["T"], "all"):
         sp = SPDHGPoisson(op, subsets=3, seed=1, resident=resident)
         x = sp.run(np.zeros(op.coeff_shape, np.float32), b, 5, diagnostics_interval=2, callback=cb(str(resident)))
         want = {"none": (), "all": ("x", "z", "T")}.get(resident) if isinstance(resident, str) else \

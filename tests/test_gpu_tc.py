@@ -29,6 +29,35 @@ def rand_bf16(shape, gen, density=1.0):
     return x.to(torch.bfloat16)
 
 
+def test_pf_tc_products_with_a_compact_pf():
+    """A PF of the subset's angles only (n_sub, Ktot, CPpad; pf_compact = 1, as generated for one subset) gives the
+    products of the full PF of all angles bit for bit, forward (into the subset's data rows) and adjoint."""
+    lib = _lib()
+    gen = torch.Generator(device="cuda").manual_seed(17)
+    R, ktot, CP, cp_pad, my = 6, 264, 700, 704, 131
+    pf = rand_bf16((R, ktot, cp_pad), gen, density=0.2)
+    pf[:, :, CP:] = 0
+    omegas = torch.tensor([5, 1, 3], dtype=torch.int32, device="cuda")
+    n_sub = omegas.numel()
+    pfc = pf[omegas.long()].contiguous()
+    z = rand_bf16((n_sub, my, ktot), gen)
+    d = rand_bf16((R, my, cp_pad), gen)
+    s = torch.cuda.current_stream().cuda_stream
+    tc_flags()
+    out = []
+    for src, compact in ((pf, 0), (pfc, 1)):
+        data = torch.full((R, my, CP), 3.0, device="cuda")
+        lib.call("dfx_pf_tc_forward", src.data_ptr(), ktot, 0, ktot, CP, cp_pad, R, z.data_ptr(), omegas.data_ptr(),
+                 n_sub, my, data.data_ptr(), 1, compact, s)
+        zo = torch.zeros((n_sub, my, ktot), dtype=torch.bfloat16, device="cuda")
+        lib.call("dfx_pf_tc_adjoint", src.data_ptr(), ktot, 0, ktot, CP, cp_pad, R, d.data_ptr(), omegas.data_ptr(),
+                 n_sub, my, 0.75, zo.data_ptr(), compact, s)
+        torch.cuda.synchronize()
+        out.append((data, zo))
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+    assert tc_flags() == 0
+
+
 @pytest.mark.parametrize("my", [103, 263])
 def test_pf_tc_products_match_fp32_gemm(my):
     lib = _lib()
@@ -44,18 +73,18 @@ def test_pf_tc_products_match_fp32_gemm(my):
     s = torch.cuda.current_stream().cuda_stream
     data = torch.full((R, my, CP), 7.0, device="cuda")
     lib.call("dfx_pf_tc_forward", pf.data_ptr(), ktot, 0, ktot, CP, cp_pad, R, z.data_ptr(), omegas.data_ptr(),
-             n_sub, my, data.data_ptr(), 0, s)
+             n_sub, my, data.data_ptr(), 0, 0, s)
     ref = torch.stack([z[i].float() @ pf[int(r), :, :CP].float() for i, r in enumerate(omegas.tolist())])
     got = data[omegas.long()]
     assert float((got - ref).abs().max() / ref.abs().max()) < 1e-5
     assert torch.all(data[[1, 2]] == 7.0)
     lib.call("dfx_pf_tc_forward", pf.data_ptr(), ktot, 0, ktot, CP, cp_pad, R, z.data_ptr(), omegas.data_ptr(),
-             n_sub, my, data.data_ptr(), 1, s)
+             n_sub, my, data.data_ptr(), 1, 0, s)
     assert float((data[omegas.long()] - 2 * ref).abs().max() / ref.abs().max()) < 1e-5
     # a range of orientations (one batch of a wider Z): rows k0 .. k0+kn-1 only, nothing read past them
     k0, kn = 104, 200
     lib.call("dfx_pf_tc_forward", pf.data_ptr(), ktot, k0, kn, CP, cp_pad, R, z.data_ptr(), omegas.data_ptr(),
-             n_sub, my, data.data_ptr(), 0, s)
+             n_sub, my, data.data_ptr(), 0, 0, s)
     ref = torch.stack([z[i, :, k0:k0 + kn].float() @ pf[int(r), k0:k0 + kn, :CP].float()
                        for i, r in enumerate(omegas.tolist())])
     assert float((data[omegas.long()] - ref).abs().max() / ref.abs().max()) < 1e-5
@@ -65,14 +94,14 @@ def test_pf_tc_products_match_fp32_gemm(my):
     zo = torch.zeros((n_sub, my, ktot), dtype=torch.bfloat16, device="cuda")
     alpha = 57.29
     lib.call("dfx_pf_tc_adjoint", pf.data_ptr(), ktot, 0, ktot, CP, cp_pad, R, d.data_ptr(), omegas.data_ptr(),
-             n_sub, my, alpha, zo.data_ptr(), s)
+             n_sub, my, alpha, zo.data_ptr(), 0, s)
     ref = torch.stack([alpha * (d[int(r)].float() @ pf[int(r)].float().T) for r in omegas.tolist()])
     # the output is rounded to BF16 once: within half a BF16 ulp of the float32 value (2^-9 relative)
     err = (zo.float() - ref).abs()
     assert bool(torch.all(err <= ref.abs() * 2.0 ** -8 + 1e-6 * float(ref.abs().max())))
     zo.fill_(3.0)
     lib.call("dfx_pf_tc_adjoint", pf.data_ptr(), ktot, k0, kn, CP, cp_pad, R, d.data_ptr(), omegas.data_ptr(),
-             n_sub, my, alpha, zo.data_ptr(), s)
+             n_sub, my, alpha, zo.data_ptr(), 0, s)
     err = (zo[:, :, k0:k0 + kn].float() - ref[:, :, k0:k0 + kn]).abs()
     assert bool(torch.all(err <= ref[:, :, k0:k0 + kn].abs() * 2.0 ** -8 + 1e-6 * float(ref.abs().max())))
     assert torch.all(zo[:, :, :k0] == 3.0) and torch.all(zo[:, :, k0 + kn:] == 3.0)
@@ -103,16 +132,16 @@ def test_tc_argument_errors():
     s = torch.cuda.current_stream().cuda_stream
     with pytest.raises(ValueError):      # Ktot not a multiple of 8
         lib.call("dfx_pf_tc_forward", pf.data_ptr(), 12, 0, 12, 16, 16, 2, z.data_ptr(), None, 2, 3, data.data_ptr(),
-                 0, s)
+                 0, 0, s)
     with pytest.raises(ValueError):      # cp_pad < cp
         lib.call("dfx_pf_tc_forward", pf.data_ptr(), 16, 0, 16, 16, 8, 2, z.data_ptr(), None, 2, 3, data.data_ptr(),
-                 0, s)
+                 0, 0, s)
     with pytest.raises(ValueError):      # orientation range start not a multiple of 8 / past Ktot
         lib.call("dfx_pf_tc_forward", pf.data_ptr(), 16, 4, 8, 16, 16, 2, z.data_ptr(), None, 2, 3, data.data_ptr(),
-                 0, s)
+                 0, 0, s)
     with pytest.raises(ValueError):
         lib.call("dfx_pf_tc_forward", pf.data_ptr(), 16, 8, 16, 16, 16, 2, z.data_ptr(), None, 2, 3, data.data_ptr(),
-                 0, s)
+                 0, 0, s)
     with pytest.raises(ValueError):      # misaligned operand
         lib.call("dfx_pf_tc_forward", pf.data_ptr() + 2, 16, 0, 16, 16, 16, 2, z.data_ptr(), None, 2, 3,
-                 data.data_ptr(), 0, s)
+                 data.data_ptr(), 0, 0, s)

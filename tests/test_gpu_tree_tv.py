@@ -181,7 +181,8 @@ def test_tree_state_resumes_and_misuse_raises(golden):
             np.zeros(lop.coeff_shape, np.float32), b, 1, gain=gain)
     d = golden("diff_auto_trapezoid")
     cfg, mat, grid = case_inputs(d)
-    op = SinglePhaseForwardOperator(cfg, mat, grid, 1e-5, normalized=True, quadrature=d["quadrature"])
+    op = SinglePhaseForwardOperator(cfg, mat, grid, 1e-5, normalized=True, quadrature=d["quadrature"],
+                                    pf_mode="sparse")
     with pytest.raises(NotImplementedError):
         SPDHGPoisson(op, subsets=3, tv=0.06, tv_tree=tree).run(np.zeros(op.coeff_shape, np.float32),
                                                               np.zeros(op.data_shape, np.float32), 1)

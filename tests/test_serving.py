@@ -46,3 +46,4 @@ def test_estimate_grows_with_the_request():
     assert estimate_request_bytes(cfg, 1000, 3) > small
     assert estimate_request_bytes({**cfg, "Nx": 128, "Ny": 128}, 500, 3) > small
     assert estimate_request_bytes(cfg, 500, 8) > small
+    assert estimate_request_bytes(cfg, 500, 3, precision="bf16") > small      # + the dense BF16 PF
