@@ -296,6 +296,8 @@ def main():
                     help="both: the BF16 tensor-core path (the value) and the float32 path (for the ratio)")
     ap.add_argument("--no-errors", action="store_true", help="skip the al99 precision check against the float64 "
                     "oracle loop")
+    ap.add_argument("--no-generated", action="store_true", help="skip the arms with the PF generated on the fly "
+                    "(no PF stored: the float32 CSR generated per batch, the BF16 PF per subset)")
     a = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -427,6 +429,32 @@ def main():
             for k in ("deviance_rel_err_bf16_vs_f64", "coef_rel_err_bf16_vs_f64", "deviance_rel_err_fp32_vs_f64",
                       "coef_rel_err_fp32_vs_f64"):
                 cfg_line[k] = errors[k]
+    gen = {}
+    if not a.no_generated:
+        # the same problem with no PF stored: an operator whose float32 products generate the CSR of each batch in
+        # every call and whose BF16 products generate the PF of each subset's angles when they use it
+        op.free_memory()
+        del op
+        torch.cuda.empty_cache()
+        op = SinglePhaseForwardOperator(cfg, mat, grid, w["max_gb"], normalized=True, precision="bf16",
+                                        bf16_pf="generated", pf_mode="generated")
+        for name, prec in (("fp32_generated_pf", "fp32"), ("bf16_generated_pf", "bf16")):
+            if prec == "bf16" and a.precision == "fp32" or prec == "fp32" and a.precision == "bf16":
+                continue
+            gen[name] = timed_epochs(op, w, b, a, prec, dist, local, world, shards, diagnostics=True)
+    if rank == 0 and gen:
+        cfg_line["arms"]["fp32_generated_pf"] = ("as fp32 with no PF stored: the CSR of every batch generated in "
+                                                 "every product (pf_mode 'generated')")
+        cfg_line["arms"]["bf16_generated_pf"] = ("as bf16 with no PF stored: the BF16 PF of a subset's angles "
+                                                 "generated when a product uses it (bf16_pf 'generated'), the float32 "
+                                                 "residual through generated CSRs")
+        for name, r in gen.items():
+            cfg_line[f"{name}_epochs_per_s"] = r["value"]
+            cfg_line[f"{name}_final_deviance_f64"] = r["f"]
+            ref = arms.get(name.split("_")[0])
+            if ref is not None:
+                cfg_line[f"deviance_rel_err_{name}_vs_stored"] = abs(r["f"] - ref["f"]) / ref["f"]
+        gen.clear()
     serve = None
     if not a.no_serve and rank == 0:
         op.free_memory()
@@ -762,9 +790,10 @@ def ni512_run(steps, warmup, K=None):
     """The large tailored-grid slice: 512 x 512 pixels, 720 angles over 180 deg, 520 translations, 360 eta bins, 6
     rings of cubic Ni, K = 50000 orientations in 500 seeded clusters (sigma 1 deg), 36 subsets; the Fourier-slice
     projector (float32 transforms), the PF contraction in BF16 on the tensor cores with the PF of each subset
-    generated when it is used (no stored PF), x and z resident in float32, T streamed from pinned host memory, the
-    residual recomputed with the float32 operator (its PF rows generated per batch) once per epoch and the deviance
-    in float64. A step is one epoch; CUDA events around `steps` epochs after `warmup`."""
+    generated when it is used (no stored PF), x and z resident in float32, T resident in BF16 (rounded toward zero)
+    when it does not fit in float32 beside them, the host x0 moved through the staging buffers, the residual
+    recomputed with the float32 operator (its PF rows generated per batch) once per epoch and the deviance in float64.
+    A step is one epoch; CUDA events around `steps` epochs after `warmup`."""
     import torch
     from diffractom_b200 import Material, SinglePhaseForwardOperator, SPDHGPoisson, _lib
     w = dict(NI512)
@@ -780,7 +809,7 @@ def ni512_run(steps, warmup, K=None):
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t0
     b = counts_batched(op, w["grains"], w["mean_counts"])
-    sp = SPDHGPoisson(op, subsets=w["subsets"], seed=0, resident=["x", "z"])
+    sp = SPDHGPoisson(op, subsets=w["subsets"], seed=0, resident="auto")
     x0 = np.zeros(op.coeff_shape, np.float32)
     t0 = time.perf_counter()
     sp._setup(x0, b)
@@ -815,8 +844,8 @@ def ni512_run(steps, warmup, K=None):
                        "projector": op.projector, "fft_channels_per_slice": op._fft_channels,
                        "pf": "BF16 PF of each subset generated when used (two subset buffers); float32 PF rows "
                              "generated per batch for the residual and the step sizes",
-                       "resident": sp.resident_used, "streamed": [n for n in ("x", "z", "T")
-                                                                  if n not in sp.resident_used],
+                       "resident": sp.resident_used, "T_bf16": sp._t16,
+                       "streamed": [n for n in ("x", "z", "T") if n not in sp.resident_used],
                        "operator_build_s": round(t_build, 1), "setup_s": round(t_setup, 1),
                        "deviance_f64_per_epoch": f, "max_device_gb": round(mem / 1024 ** 3, 1),
                        "epoch": "36 subset iterations + the float32 residual and float64 deviance every epoch",

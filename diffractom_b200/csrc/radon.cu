@@ -262,6 +262,150 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_table(
     st8(out, o);
 }
 
+// ------------------------------------------------------------------------------------------------ grouped table
+// The float32 forward reads each pixel of a row about twice per angle through the per-bin table: a pixel's footprint
+// covers two bins (more for steep trapezoids), and every bin's warp loads it again. The grouped table lists, per
+// (angle, group of GB consecutive bins), every pixel that reaches one of the group's bins, with its weight on each
+// of them (0 where the per-bin row has no entry), in the per-bin rows' order (image row v, then u): one warp loads a
+// pixel's channels once for the whole group, and every bin still adds exactly its per-bin row's taps in its order,
+// so the sums are the per-bin forward's bits.
+constexpr int GB = 4;           // bins per group
+
+template <int KERNEL>
+__global__ void ray_gtable_kernel(const float4 *__restrict__ geo, int n_angles, int nx, int ny, int ns,
+                                  const uint8_t *__restrict__ supp, int32_t *__restrict__ counts,
+                                  const int32_t *__restrict__ row_ptr, int32_t *__restrict__ pix_out,
+                                  float4 *__restrict__ w_out)
+{
+    const int ng = (ns + GB - 1) / GB;
+    const int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;      // a * ng + g
+    if (row >= (int64_t)n_angles * ng) return;
+    const int a = (int)(row / ng), s0 = (int)(row % ng) * GB;
+    const AngleGeo g = load_geo(geo, a);
+    const int nu = g.rows_are_y ? nx : ny, nv = g.rows_are_y ? ny : nx;
+    const float half = KERNEL == 1 ? g.hw : 1.0f;
+    const float inv = __frcp_rn(g.A);
+    int n = 0;
+    int64_t pos = row_ptr ? row_ptr[row] : 0;
+    for (int v = 0; v < nv; ++v) {
+        const float c = __fmaf_rn(g.B, (float)v, g.T0);
+        int u0[GB], u1[GB];
+        int lo = nu, hi = -1;
+#pragma unroll
+        for (int j = 0; j < GB; ++j) {                    // each bin's candidate range, as the per-bin table's
+            const float fs = (float)(s0 + j);
+            const float e1 = (fs - half - c) * inv, e2 = (fs + half - c) * inv;
+            u0[j] = max((int)floorf(fminf(e1, e2) - 1e-3f), 0);
+            u1[j] = min((int)ceilf(fmaxf(e1, e2) + 1e-3f), nu - 1);
+            if (s0 + j >= ns) u1[j] = -1;
+            if (u0[j] <= u1[j]) {
+                lo = min(lo, u0[j]);
+                hi = max(hi, u1[j]);
+            }
+        }
+        for (int u = lo; u <= hi; ++u) {
+            float w[GB];
+            bool any = false;
+#pragma unroll
+            for (int j = 0; j < GB; ++j) {
+                w[j] = 0.0f;
+                if (u < u0[j] || u > u1[j]) continue;
+                const float d = __fsub_rn(__fmaf_rn(g.A, (float)u, c), (float)(s0 + j));
+                w[j] = tap_weight<KERNEL>(g, d);
+                any |= w[j] != 0.0f;
+            }
+            if (!any) continue;
+            const int pix = g.rows_are_y ? u + nx * v : v + nx * u;
+            if (supp && !supp[pix]) continue;
+            if (row_ptr) {
+                pix_out[pos] = pix;
+                w_out[pos++] = make_float4(w[0], w[1], w[2], w[3]);
+            }
+            ++n;
+        }
+    }
+    if (!row_ptr) counts[row] = n;
+}
+
+// Grouped-table forward (float32 image and sinogram rows): warp per (angle, GB bins, 256 channels); U pixels in
+// flight, each pixel's FMAs into the bins whose weight is not 0 (a branch the whole warp takes).
+__global__ void __launch_bounds__(32 * WARPS) radon_forward_gtable(
+    const float *__restrict__ img, float *__restrict__ sino, const int32_t *__restrict__ row_ptr,
+    const int32_t *__restrict__ pix, const float4 *__restrict__ wts, const int32_t *__restrict__ angles, int ns,
+    int kstride, int kb, float scale)
+{
+    constexpr int U = 4;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ng = (ns + GB - 1) / GB;
+    const int grp = blockIdx.x * WARPS + warp;
+    const int al = blockIdx.y;
+    const int k = blockIdx.z * CPW + lane * CPL;
+    if (grp >= ng) return;
+    const bool live = k < kstride;
+    const int s0 = grp * GB;
+    float *out = sino + ((int64_t)al * ns + s0) * kstride + k;
+    const int nb = min(GB, ns - s0);
+    if (blockIdx.z * CPW >= kb) {
+        const float zero[CPL] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (live)
+            for (int j = 0; j < nb; ++j) st8(out + (int64_t)j * kstride, zero);
+        return;
+    }
+    const bool load = k < kb;
+    const int a = angles ? __ldg(angles + al) : al;
+    const int64_t r = (int64_t)a * ng + grp;
+    int e = __ldg(row_ptr + r);
+    const int e1 = __ldg(row_ptr + r + 1);
+    const float *base = img + (load ? k : 0);
+    float acc[GB][CPL];
+#pragma unroll
+    for (int j = 0; j < GB; ++j)
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) acc[j][c] = 0.0f;
+    for (; e + U <= e1; e += U) {
+        int p[U];
+        float4 w[U];
+        Raw8<float> q[U];
+#pragma unroll
+        for (int i = 0; i < U; ++i) {
+            p[i] = __ldg(pix + e + i);
+            w[i] = __ldg(wts + e + i);
+        }
+#pragma unroll
+        for (int i = 0; i < U; ++i) {
+            zraw(q[i]);
+            if (load) ldraw(base + (int64_t)p[i] * kstride, q[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < U; ++i) {
+            if (w[i].x != 0.0f) accraw(acc[0], w[i].x, q[i]);
+            if (w[i].y != 0.0f) accraw(acc[1], w[i].y, q[i]);
+            if (w[i].z != 0.0f) accraw(acc[2], w[i].z, q[i]);
+            if (w[i].w != 0.0f) accraw(acc[3], w[i].w, q[i]);
+        }
+    }
+    for (; e < e1; ++e) {
+        const int p = __ldg(pix + e);
+        const float4 w = __ldg(wts + e);
+        Raw8<float> q;
+        zraw(q);
+        if (load) ldraw(base + (int64_t)p * kstride, q);
+        if (w.x != 0.0f) accraw(acc[0], w.x, q);
+        if (w.y != 0.0f) accraw(acc[1], w.y, q);
+        if (w.z != 0.0f) accraw(acc[2], w.z, q);
+        if (w.w != 0.0f) accraw(acc[3], w.w, q);
+    }
+    if (!live) return;
+#pragma unroll
+    for (int j = 0; j < GB; ++j) {
+        if (j >= nb) break;
+        float o[CPL];
+#pragma unroll
+        for (int q = 0; q < CPL; ++q) o[q] = (k + q < kb) ? __fmul_rn(scale, acc[j][q]) : 0.0f;
+        st8(out + (int64_t)j * kstride, o);
+    }
+}
+
 // ------------------------------------------------------------------------------------------------ backward
 // SPDHG primal step of one coefficient: the operations of primal_update_kernel (solver.cu), bitwise
 __device__ __forceinline__ void primal_step(float &x, float &z, float t, float dz, float inv_p, float lam)
@@ -275,7 +419,10 @@ __device__ __forceinline__ void primal_step(float &x, float &z, float t, float d
 // MODE 0: img (npix, kstride) = backprojection; MODE 1: the backprojection dz is applied to x, z (T the steps):
 // z += dz; x = T > 0 ? max(0, x - T (z + inv_p dz + lam)) : 0. plist (MODE 0, optional): only the pixels plist[0 ..
 // n_out-1], output row r for pixel plist[r] (the same arithmetic per pixel as the whole image).
-template <int KERNEL, int MODE, typename ST>
+// P channel groups of 256 per warp (lane: channels k, k + 256, ...): the pixel's taps and weights are computed once for
+// P x 8 channels per lane, which halves the geometry work per FMA at P = 2; every channel sums the same terms in the
+// same order whatever P is.
+template <int KERNEL, int MODE, typename ST, int P>
 __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
     const ST *__restrict__ sino, int64_t sld, float *__restrict__ img, const float4 *__restrict__ geo, int n_angles, int nx,
     int ny, int ns, int kstride, int kb, int n_taps, float *__restrict__ z, const float *__restrict__ T, float inv_p,
@@ -286,22 +433,33 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t p = (int64_t)blockIdx.x * WARPS + warp;     // output row
-    const int k = blockIdx.y * CPW + lane * CPL;
-    if (p >= n_out || k >= kstride) return;
-    if (blockIdx.y * CPW >= kb) {          // a block of padding channels only: the backprojection is 0 there
+    const int kblk = blockIdx.y * CPW * P;
+    if (p >= n_out || kblk + lane * CPL >= kstride) return;
+    // group h: channels kblk + h CPW + lane CPL (+0..7); live: inside kstride; data: not a block of padding only
+    bool live[P], data[P];
+#pragma unroll
+    for (int h = 0; h < P; ++h) {
+        live[h] = kblk + h * CPW + lane * CPL < kstride;
+        data[h] = live[h] && kblk + h * CPW < kb;
+    }
+    const int64_t pix = plist ? (int64_t)__ldg(plist + p) : p;
+    if (!data[0]) {                        // padding channels only: the backprojection is 0 there
         if (MODE == 0) {
             const float zero[CPL] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            st8(img + p * kstride + k, zero);
+#pragma unroll
+            for (int h = 0; h < P; ++h)
+                if (live[h]) st8(img + p * kstride + kblk + h * CPW + lane * CPL, zero);
         }
         return;                            // MODE 1: dz = 0 leaves z, and x (0 on padding channels), unchanged
     }
-    const int64_t pix = plist ? (int64_t)__ldg(plist + p) : p;
     const int px = (int)(pix % nx), py = (int)(pix / nx);
     const float fx = (float)px, fy = (float)py;
-    float acc[CPL];
+    float acc[P][CPL];
 #pragma unroll
-    for (int c = 0; c < CPL; ++c) acc[c] = 0.0f;
-    const ST *col = sino + k;
+    for (int h = 0; h < P; ++h)
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) acc[h][c] = 0.0f;
+    const ST *col = sino + kblk + lane * CPL;
     const int64_t angle_stride = (int64_t)ns * sld;
     for (int a = 0; a < n_angles; ++a, col += angle_stride) {
         const AngleGeo g = unpack_geo(prm[a]);
@@ -311,11 +469,15 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
         if (ntap == 2 && sf >= 0 && sf + 1 < ns) {        // the common case: two taps inside the detector
             const float w0 = __fmul_rn(g.w, tap_weight<KERNEL>(g, __fsub_rn(t, (float)sf)));
             const float w1 = __fmul_rn(g.w, tap_weight<KERNEL>(g, __fsub_rn(t, (float)(sf + 1))));
-            float4 a0, a1, b0, b1;
-            ld8(col + (int64_t)sf * sld, a0, a1);
-            ld8(col + (int64_t)(sf + 1) * sld, b0, b1);
-            acc8(acc, w0, a0, a1);
-            acc8(acc, w1, b0, b1);
+#pragma unroll
+            for (int h = 0; h < P; ++h) {
+                if (!data[h]) continue;
+                float4 a0, a1, b0, b1;
+                ld8(col + h * CPW + (int64_t)sf * sld, a0, a1);
+                ld8(col + h * CPW + (int64_t)(sf + 1) * sld, b0, b1);
+                acc8(acc[h], w0, a0, a1);
+                acc8(acc[h], w1, b0, b1);
+            }
             continue;
         }
         for (int i = 0; i < ntap; ++i) {
@@ -323,36 +485,47 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
             if (s < 0 || s >= ns) continue;
             const float w = tap_weight<KERNEL>(g, __fsub_rn(t, (float)s));
             if (w == 0.0f) continue;
-            float4 q0, q1;
-            ld8(col + (int64_t)s * sld, q0, q1);
-            acc8(acc, __fmul_rn(g.w, w), q0, q1);
+            const float ww = __fmul_rn(g.w, w);
+#pragma unroll
+            for (int h = 0; h < P; ++h) {
+                if (!data[h]) continue;
+                float4 q0, q1;
+                ld8(col + h * CPW + (int64_t)s * sld, q0, q1);
+                acc8(acc[h], ww, q0, q1);
+            }
         }
     }
-    const int64_t o = p * kstride + k;
-    if (MODE == 0) {
-        float r[CPL];
 #pragma unroll
-        for (int c = 0; c < CPL; ++c) r[c] = (k + c < kb) ? acc[c] : 0.0f;      // padding channels: 0
-        float4 *d = reinterpret_cast<float4 *>(img + o);
-        d[0] = make_float4(r[0], r[1], r[2], r[3]);
-        d[1] = make_float4(r[4], r[5], r[6], r[7]);
-    } else {
-        float xn[CPL];
+    for (int h = 0; h < P; ++h) {
+        const int k = kblk + h * CPW + lane * CPL;
+        const int64_t o = p * kstride + k;
+        if (MODE == 0) {
+            if (!live[h]) continue;
+            float r[CPL];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            float4 *xp = reinterpret_cast<float4 *>(img + o) + h;
-            float4 *zp = reinterpret_cast<float4 *>(z + o) + h;
-            float4 xv = *xp, zv = *zp;
-            const float4 tv = __ldg(reinterpret_cast<const float4 *>(T + o) + h);
-            primal_step(xv.x, zv.x, tv.x, (k + 4 * h + 0 < kb) ? acc[4 * h + 0] : 0.0f, inv_p, lam);
-            primal_step(xv.y, zv.y, tv.y, (k + 4 * h + 1 < kb) ? acc[4 * h + 1] : 0.0f, inv_p, lam);
-            primal_step(xv.z, zv.z, tv.z, (k + 4 * h + 2 < kb) ? acc[4 * h + 2] : 0.0f, inv_p, lam);
-            primal_step(xv.w, zv.w, tv.w, (k + 4 * h + 3 < kb) ? acc[4 * h + 3] : 0.0f, inv_p, lam);
-            *xp = xv;
-            *zp = zv;
-            xn[4 * h] = xv.x; xn[4 * h + 1] = xv.y; xn[4 * h + 2] = xv.z; xn[4 * h + 3] = xv.w;
+            for (int c = 0; c < CPL; ++c) r[c] = (data[h] && k + c < kb) ? acc[h][c] : 0.0f;   // padding: 0
+            float4 *d = reinterpret_cast<float4 *>(img + o);
+            d[0] = make_float4(r[0], r[1], r[2], r[3]);
+            d[1] = make_float4(r[4], r[5], r[6], r[7]);
+        } else {
+            if (!data[h]) continue;
+            float xn[CPL];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                float4 *xp = reinterpret_cast<float4 *>(img + o) + q;
+                float4 *zp = reinterpret_cast<float4 *>(z + o) + q;
+                float4 xv = *xp, zv = *zp;
+                const float4 tv = __ldg(reinterpret_cast<const float4 *>(T + o) + q);
+                primal_step(xv.x, zv.x, tv.x, (k + 4 * q + 0 < kb) ? acc[h][4 * q + 0] : 0.0f, inv_p, lam);
+                primal_step(xv.y, zv.y, tv.y, (k + 4 * q + 1 < kb) ? acc[h][4 * q + 1] : 0.0f, inv_p, lam);
+                primal_step(xv.z, zv.z, tv.z, (k + 4 * q + 2 < kb) ? acc[h][4 * q + 2] : 0.0f, inv_p, lam);
+                primal_step(xv.w, zv.w, tv.w, (k + 4 * q + 3 < kb) ? acc[h][4 * q + 3] : 0.0f, inv_p, lam);
+                *xp = xv;
+                *zp = zv;
+                xn[4 * q] = xv.x; xn[4 * q + 1] = xv.y; xn[4 * q + 2] = xv.z; xn[4 * q + 3] = xv.w;
+            }
+            if (xb) st8(xb + o, xn);       // the BF16 copy of x the next forward projection reads
         }
-        if (xb) st8(xb + o, xn);           // the BF16 copy of x the next forward projection reads
     }
 }
 
@@ -457,15 +630,24 @@ static int launch_backward(const ST *sino, int64_t sld, float *img, const float 
                            __nv_bfloat16 *xb, void *stream, const int32_t *plist = nullptr, int64_t n_list = 0)
 {
     const int64_t npix = plist ? n_list : (int64_t)nx * ny;
-    dim3 grid((unsigned)cdiv(npix, WARPS), (unsigned)cdiv(kstride, CPW));
+    // two channel groups per warp once the batch has more than one (fewer, longer warps: the taps of a pixel are
+    // evaluated once for 16 channels per lane)
+    const bool pair = kstride > CPW;
+    dim3 grid((unsigned)cdiv(npix, WARPS), (unsigned)cdiv(kstride, pair ? 2 * CPW : CPW));
     DFX_REQUIRE(grid.x < 2147483647u && grid.y <= 65535u, "radon: batch too large for one launch");
     const size_t smem = sizeof(AngleParams) * (size_t)(n_angles > 0 ? n_angles : 1);
     DFX_REQUIRE(smem <= 200 * 1024, "radon: %d angles exceed the shared memory of one launch", n_angles);
-    int st = allow_smem(radon_backward_v3<KERNEL, MODE, ST>, smem);
+    int st = pair ? allow_smem(radon_backward_v3<KERNEL, MODE, ST, 2>, smem)
+                  : allow_smem(radon_backward_v3<KERNEL, MODE, ST, 1>, smem);
     if (st) return st;
-    radon_backward_v3<KERNEL, MODE, ST><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
-        sino, sld, img, reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, kstride, kb, n_taps, z, T, inv_p,
-        lam, xb, plist, npix);
+    if (pair)
+        radon_backward_v3<KERNEL, MODE, ST, 2><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
+            sino, sld, img, reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, kstride, kb, n_taps, z, T,
+            inv_p, lam, xb, plist, npix);
+    else
+        radon_backward_v3<KERNEL, MODE, ST, 1><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
+            sino, sld, img, reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, kstride, kb, n_taps, z, T,
+            inv_p, lam, xb, plist, npix);
     return launch_status(MODE ? "radon_backward_spdhg" : "radon_backward");
 }
 
@@ -632,6 +814,60 @@ extern "C" int dfx_radon_table_fill(const float *geo, int n_angles, int nx, int 
         ray_table_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
             reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, nullptr, row_ptr, e);
     return launch_status("radon_table_fill");
+}
+
+extern "C" int dfx_radon_gtable_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
+                                      const uint8_t *supp, int32_t *counts, void *stream)
+{
+    DFX_REQUIRE(geo && counts && ((uintptr_t)geo % 16) == 0, "radon_gtable: null or misaligned pointer");
+    DFX_REQUIRE(n_angles > 0 && nx > 0 && ny > 0 && n_det > 0 && (kernel == 0 || kernel == 1),
+                "radon_gtable: bad sizes or kernel");
+    const int64_t rows = (int64_t)n_angles * cdiv(n_det, GB);
+    DFX_REQUIRE(cdiv(rows, 128) < 2147483647LL, "radon_gtable: too many rows");
+    if (kernel == 1)
+        ray_gtable_kernel<1><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, counts, nullptr, nullptr, nullptr);
+    else
+        ray_gtable_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, counts, nullptr, nullptr, nullptr);
+    return launch_status("radon_gtable_count");
+}
+
+extern "C" int dfx_radon_gtable_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
+                                     const uint8_t *supp, const int32_t *row_ptr, int32_t *pixels, float *weights,
+                                     void *stream)
+{
+    DFX_REQUIRE(geo && row_ptr && pixels && weights && ((uintptr_t)geo % 16) == 0 && ((uintptr_t)weights % 16) == 0,
+                "radon_gtable: null or misaligned pointer");
+    DFX_REQUIRE(n_angles > 0 && nx > 0 && ny > 0 && n_det > 0 && (kernel == 0 || kernel == 1),
+                "radon_gtable: bad sizes or kernel");
+    const int64_t rows = (int64_t)n_angles * cdiv(n_det, GB);
+    float4 *w = reinterpret_cast<float4 *>(weights);
+    if (kernel == 1)
+        ray_gtable_kernel<1><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, nullptr, row_ptr, pixels, w);
+    else
+        ray_gtable_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, nullptr, row_ptr, pixels, w);
+    return launch_status("radon_gtable_fill");
+}
+
+extern "C" int dfx_radon_forward_gtable(const float *img_k, float *sino_k, const int32_t *row_ptr,
+                                        const int32_t *pixels, const float *weights, const int32_t *angles,
+                                        int n_angles, int n_det, int kstride, int kb, float scale, void *stream)
+{
+    DFX_REQUIRE(img_k && sino_k && row_ptr && pixels && weights, "radon_forward_gtable: null pointer");
+    DFX_REQUIRE(((uintptr_t)img_k % 16) == 0 && ((uintptr_t)sino_k % 16) == 0 && ((uintptr_t)weights % 16) == 0,
+                "radon_forward_gtable: misaligned arrays");
+    DFX_REQUIRE(n_angles >= 0 && n_angles <= 65535 && n_det > 0, "radon_forward_gtable: bad sizes");
+    DFX_REQUIRE(kstride > 0 && kstride % CPL == 0 && kb >= 0 && kb <= kstride && cdiv(kstride, CPW) <= 65535,
+                "radon_forward_gtable: kstride (%d) must be a positive multiple of %d and kb (%d) <= kstride",
+                kstride, CPL, kb);
+    if (n_angles == 0) return DFX_OK;
+    dim3 grid((unsigned)cdiv(cdiv(n_det, GB), WARPS), (unsigned)n_angles, (unsigned)cdiv(kstride, CPW));
+    radon_forward_gtable<<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
+        img_k, sino_k, row_ptr, pixels, reinterpret_cast<const float4 *>(weights), angles, n_det, kstride, kb, scale);
+    return launch_status("radon_forward_gtable");
 }
 
 extern "C" int dfx_radon_dtable_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,

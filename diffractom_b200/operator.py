@@ -151,11 +151,12 @@ class SinglePhaseForwardOperator:
             self._supp_tiles = {}
             self._fft = None
             if self.projector == "fft":
-                self._ray_rp = self._ray_ent = None
+                self._ray_rp = self._ray_ent = self._ray_grp = None
                 self.ray_taps = 0
                 self._build_fourier()
             else:
                 self._ray_rp, self._ray_ent, self.ray_taps = self._build_ray_table()
+                self._ray_grp = self._build_group_table()
             self.omega_subsets = None
             self._sub = []
             self._streamer = None
@@ -286,6 +287,30 @@ class SinglePhaseForwardOperator:
                    rp.data_ptr(), ent.data_ptr(), s)
         return rp, ent, total
 
+    def _build_group_table(self, supp=None):
+        """The grouped ray table of the float32 forward (dfx_radon_gtable_*): per (angle, four bins) the pixels that
+        reach them with their four weights, so that each pixel's channels are loaded once per group; the sums are
+        the per-bin table's bits. Returns (row_ptr, pixels, weights)."""
+        R, ns = self.N_Omega, self.My
+        n = R * (-(-ns // 4))
+        s = self._s()
+        sp = None if supp is None else supp.data_ptr()
+        rp = torch.empty(n + 1, dtype=torch.int32, device=self.device)
+        self._call("dfx_radon_gtable_count", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id, sp,
+                   rp.data_ptr(), s)
+        self.stream().synchronize()
+        total = int(rp[:n].to(torch.int64).sum().item())
+        if total >= 2 ** 31:
+            raise ValueError(f"the grouped projector table has {total} entries, more than 2^31 - 1")
+        nb = self._lib.dfx_scan_scratch_bytes(n)
+        scr = self.scratch(nb)
+        self._call("dfx_scan_exclusive_i32", rp.data_ptr(), rp.data_ptr(), n, scr.data_ptr(), nb, s)
+        pix = torch.empty(max(total, 1), dtype=torch.int32, device=self.device)
+        w = torch.empty((max(total, 1), 4), dtype=torch.float32, device=self.device)
+        self._call("dfx_radon_gtable_fill", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id, sp,
+                   rp.data_ptr(), pix.data_ptr(), w.data_ptr(), s)
+        return rp, pix, w
+
     @on_op_stream
     def support_ray_table(self, supp):
         """The ray table restricted to a support mask (uint8 (Ny * Nx) device tensor), built once per mask content
@@ -296,7 +321,7 @@ class SinglePhaseForwardOperator:
         key = bytes(supp.cpu().numpy())
         hit = self._ray_supp.get(key)
         if hit is None:
-            hit = self._build_ray_table(supp)
+            hit = self._build_ray_table(supp) + (self._build_group_table(supp),)
             self._ray_supp[key] = hit
         return hit
 
@@ -340,7 +365,12 @@ class SinglePhaseForwardOperator:
             return
         om_ptr = None if om is None else om.data_ptr()
         rp, ent = (self._ray_rp, self._ray_ent) if ray is None else ray[:2]
-        if sld is None:
+        grp = self._ray_grp if ray is None else (ray[3] if len(ray) > 3 else None)
+        if sld is None and grp is not None:
+            self._call("dfx_radon_forward_gtable", src_ptr, dst_ptr, grp[0].data_ptr(), grp[1].data_ptr(),
+                       grp[2].data_ptr(), om_ptr, n_ang, self.My, self.Kstride, kb, float(self.radon_geo.scale),
+                       self._s())
+        elif sld is None:
             self._call("dfx_radon_forward_table", src_ptr, dst_ptr, rp.data_ptr(), ent.data_ptr(),
                        om_ptr, n_ang, self.My, self.Kstride, kb, float(self.radon_geo.scale), self._s())
         else:
@@ -377,6 +407,8 @@ class SinglePhaseForwardOperator:
             kbm = min(max(int(max_bytes // bytes_per_K), 1), K)
         else:
             kbm = 1
+        if getattr(self, "precision", "fp32") == "bf16" and 64 < kbm < K:
+            kbm = kbm // 64 * 64        # whole 64-channel image boxes: no padding channels in the BF16 batches
         self.batches = [{"k_start": k0, "k_end": min(k0 + kbm, K), "K_batch": min(k0 + kbm, K) - k0}
                         for k0 in range(0, K, kbm)]
         self.K_batch_max = -(-max(b["K_batch"] for b in self.batches) // 4) * 4
@@ -847,20 +879,24 @@ class SinglePhaseForwardOperator:
         self._pf_tc_adjoint(e["omegas"], e["n"], z)
         return e["geo"], e["n"], z
 
-    def _bf16_update_batch(self, ib, geo, n, z, x_ptr, z_ptr, T_ptr, inv_p, lam, xb_ptr=None, subset=None):
+    def _bf16_update_batch(self, ib, geo, n, z, x_ptr, z_ptr, T_ptr, inv_p, lam, xb_ptr=None, subset=None,
+                           t_bf16=False):
         """SPDHG's update of batch ib from its columns of Z (the n angles of subset m): the backprojection with the
         primal step fused (and the BF16 copy of the new x written to xb_ptr). The Fourier-slice projector
-        backprojects the columns widened to float32, and the primal step follows as its own kernel."""
+        backprojects the columns widened to float32, and the primal step follows as its own kernel (t_bf16: T stored
+        in BF16)."""
         if self.projector == "fft":
             kb, s = self.batches[ib]["K_batch"], self._s()
             self._call("dfx_convert_rows", 0, self.coeffs_sino_C.data_ptr(), self.Kstride,
                        z.data_ptr() + 2 * ib * self.Kstride, self.Ktot, n * self.My, kb, s)
             self._fft_run(False, self._subset(subset), self.coeffs_sino_C.data_ptr(), self._img_k.data_ptr(), kb)
-            self._call("dfx_spdhg_primal_update", x_ptr, z_ptr, T_ptr, self._img_k.data_ptr(), float(inv_p),
-                       float(lam), self.batch_elems(), s)
+            self._call("dfx_spdhg_primal_update_t16" if t_bf16 else "dfx_spdhg_primal_update", x_ptr, z_ptr, T_ptr,
+                       self._img_k.data_ptr(), float(inv_p), float(lam), self.batch_elems(), s)
             if xb_ptr is not None:
                 self._call("dfx_f32_to_bf16", x_ptr, xb_ptr, self.batch_elems(), s)
             return
+        if t_bf16:
+            raise ValueError("T in BF16 needs the Fourier-slice projector")
         name = "dfx_radon_backward_spdhg_tc" if self.tc_backprojection else "dfx_radon_backward_spdhg_bf16"
         self._call(name, z.data_ptr() + 2 * ib * self.Kstride, self.Ktot, geo.data_ptr(), n, self.Nx, self.Ny,
                    self.My, self.Kstride, self.batches[ib]["K_batch"], self._kernel_id, int(self.radon_geo.n_taps),
@@ -1243,6 +1279,7 @@ class SinglePhaseForwardOperator:
         self.release_omega_subsets()
         self.release_streamer()
         self._ray_supp = {}
+        self._ray_grp = None
         self._supp_tiles = {}
         self._fft = None
         self.sparse_batches = None

@@ -65,7 +65,8 @@ class Request:
 def estimate_request_bytes(cfg, K, n_rings, fill=0.15, precision="fp32") -> int:
     """Device memory of a request, estimated before its operator exists: SPDHG's coefficient arrays (x, z, T in the
     batch layout and x in the (K, Ny, Nx) layout), its data arrays (b, y, S, D), both sparse PF copies at the given
-    fill (12 bytes per non-zero, plus the eta-blocked forward copy, ~6 more), the ray table and the batch buffers;
+    fill (12 bytes per non-zero, plus the eta-blocked forward copy, ~6 more), the ray tables (per-bin and grouped, for
+    the whole image and the support) and the batch buffers;
     with precision "bf16" also the dense BF16 PF (2 bytes per entry), the BF16 copies of x and of the data rows and
     the Radon output of the subset angles. n_rings: an upper bound (the reflections)."""
     npix = int(cfg["Nx"]) * int(cfg["Ny"])
@@ -73,7 +74,7 @@ def estimate_request_bytes(cfg, K, n_rings, fill=0.15, precision="fp32") -> int:
     CP = int(cfg["N_eta"]) * int(n_rings)
     coeff = 4 * K * npix
     data = 4 * R * My * CP
-    n = 4 * coeff + 4 * data + 18 * fill * R * K * CP + 18 * R * npix + 8 * 1024 * (R * My + npix) + (1 << 28)
+    n = 4 * coeff + 4 * data + 18 * fill * R * K * CP + 90 * R * npix + 8 * 1024 * (R * My + npix) + (1 << 28)
     if precision == "bf16":
         n += 2 * R * K * CP + coeff // 2 + data // 2 + 2 * R * My * K
     return int(n)

@@ -63,6 +63,11 @@ class SPDHGPoisson:
     # bf16_diagnostics False: the full forward of a diagnostics epoch (the residual A x, whose rows feed the float64
     # deviance and the next subset) is recomputed with the float32 operator; True: through the BF16 path as well.
     bf16_diagnostics = False
+    # T in BF16, rounded toward zero (never above its float32 value, so the steps still meet SPDHG's step condition),
+    # kept on the device: with an operator of precision "bf16" and the Fourier-slice projector (whose primal step is
+    # its own kernel). "auto" (resident="auto" only): when x and z fit in float32 and T then fits in BF16 but not in
+    # float32, instead of streaming T from host memory in every iteration; True: always with such an operator.
+    bf16_T = "auto"
 
     def __init__(self, operator, subsets=8, prox_kind="nonneg", lam=0.0, support="fov", eps_counts=1e-3, rho="auto",
                  seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None, shards=None):
@@ -112,6 +117,7 @@ class SPDHGPoisson:
         self.support_gpu = support_mask_to_device(operator, support, operator.device)
         self.shards = shards
         self.state = None
+        self._t16 = False
 
     # ---------------------------------------------------------------- schedule
     def _epoch_order(self):
@@ -240,7 +246,7 @@ class SPDHGPoisson:
                     _lib.call("dfx_f32_to_bf16", X.ptr(ib, s), xb, be, op._s())
             elif adj is not None:
                 op._bf16_update_batch(ib, geo, n, zb, X.ptr(ib, s), Z.ptr(ib, s), T.ptr(ib, s), self._inv_p_data,
-                                      self.lam, xb, subset=adj)
+                                      self.lam, xb, subset=adj, t_bf16=self._t16)
             elif not X.resident and not fft:
                 _lib.call("dfx_f32_to_bf16", X.ptr(ib, s), xb, be, op._s())
             if fwd is not None and fft:
@@ -538,9 +544,11 @@ class SPDHGPoisson:
             raise ValueError("continuing a TV run needs the state's z")
         resident = self._choose_resident()
         self.resident_used = tuple(nm for nm in self._names if nm in resident)
-        self.X, self.Z, self.T = (CoeffArray(op, nm, nm in resident) for nm in NAMES)
+        self.X, self.Z = (CoeffArray(op, nm, nm in resident) for nm in NAMES[:2])
+        self.T = CoeffArray(op, "T", "T" in resident, torch.bfloat16 if self._t16 else torch.float32)
         self.pipe = BatchPipeline(op)
-        self._stage = None if len(resident) == len(self._names) else KMajorStaging(op)
+        # staged host IO (no (K, Ny, Nx) device temporary) when memory is short: some array streamed, or T in BF16
+        self._stage = None if len(resident) == len(self._names) and not self._t16 else KMajorStaging(op)
         self.dzk = torch.empty(be, dtype=torch.float32, device=dev)
         self.x = None
         # a host x0 of a resident x is uploaded after the step sizes' passes are queued, on a side stream, so that
@@ -612,8 +620,10 @@ class SPDHGPoisson:
         if bf16:
             op._rows_to_bf16(self.D, op._all_omegas, op.N_Omega)
 
+        tk = torch.empty(be, dtype=torch.float32, device=dev) if self._t16 else None
+
         def t_batch(ib, s_):
-            tb, kb = T.ptr(ib, s_), op.batches[ib]["K_batch"]
+            tb, kb = (tk.data_ptr() if self._t16 else T.ptr(ib, s_)), op.batches[ib]["K_batch"]
             _lib.call("dfx_tinit", tb, be, s)
             for m in range(self.M):
                 if bf16:                                   # this batch's columns of A_m^T 1_counted, BF16 operator
@@ -627,8 +637,10 @@ class SPDHGPoisson:
                     op._adjoint_batch_k(self.D, ib, self.dzk.data_ptr(), subset=m)
                 _lib.call("dfx_batch_support", tb, self.dzk.data_ptr(), sp, npix, op.Kstride, kb, c, 2, s)
             _lib.call("dfx_tfinal", tb, be, s)           # padding channels were never reached: T = 0 there
+            if self._t16:
+                _lib.call("dfx_f32_to_bf16_rz", tb, T.ptr(ib, s_), be, s)
 
-        if bf16 and T.resident:
+        if bf16 and T.resident and not self._t16:
             # subset by subset: one tensor-core PF adjoint for all batches, then every batch's backprojection and
             # running minimum (the same columns as batch by batch, in a twentieth of the PF launches)
             for ib in range(nbt):
@@ -806,19 +818,27 @@ class SPDHGPoisson:
         resident="all"; for "auto" as many of x, z, T (in this order) as fit into the free device memory less the
         streaming buffers and a margin."""
         names = self._names
+        op = self.op
+        t16_ok = op.precision == "bf16" and op.projector == "fft" and self.tv == 0
+        if self.bf16_T is True and not t16_ok:
+            raise ValueError("bf16_T needs an operator of precision 'bf16' with the Fourier-slice projector, no tv")
+        self._t16 = self.bf16_T is True
         if self._x_on_gpu or self.resident == "all":
             return set(names)
         if self.resident == "none":
             return set()
         if self.resident != "auto":
             return set(self.resident) & set(names)
-        op = self.op
         be = op.batch_elems()
         nbytes = 4 * be * len(op.batches)
         free, _ = torch.cuda.mem_get_info(op.device)
         # two slots per streamed array, the k-major staging buffer, the batch scratch and a BF16 batch of x
         staging = (4 * 2 * len(names) + 4 + 4 + 2 + (8 if self.tv > 0 else 0)) * be
-        n = int(max(0, free - staging - MARGIN_GB * 1024 ** 3) // nbytes)
+        room = max(0, free - staging - MARGIN_GB * 1024 ** 3)
+        n = int(room // nbytes)
+        if n == 2 and len(names) == 3 and t16_ok and self.bf16_T == "auto" and room >= 2.5 * nbytes:
+            self._t16 = True
+            return set(names)
         return set(names[:min(n, len(names))])
 
     @on_op_stream
@@ -882,7 +902,7 @@ class SPDHGPoisson:
         self.final_stats = {"epochs": len(self.iter_stats), "final_f": self._f, "setup_s": self._t_setup,
                             "rho": self.rho_used, "subsets": self.M, "resident": self.resident_used,
                             "time": time.perf_counter() - self._t_start, "tv": self.tv, "tv_prob": self.tv_prob,
-                            "graph_replays": self.graph_replays, **self.scales}
+                            "graph_replays": self.graph_replays, "T_bf16": self._t16, **self.scales}
         out = self.x if self._x_on_gpu else self._host_x
         self.b = self.w = self.g = self.bg = self.y = self.sig = self.D = None
         self.X = self.Z = self.T = self.dzk = self.xkb = self._stage = self._ray = self._tiles = None

@@ -124,6 +124,20 @@ int dfx_radon_forward_table_bf16_bf16(const void *img_bf16, void *sino_bf16, int
                                       const int32_t *entries, const int32_t *angles, int n_angles, int n_det,
                                       int kstride, int kb, float scale, void *stream);
 
+/* Grouped ray table (no reference counterpart): row a * ceil(n_det / 4) + g lists, in the per-bin rows' order, every
+ * pixel that reaches one of the bins 4 g .. 4 g + 3 of angle a, as an int32 pixel index and a float4 of its weights
+ * on those four bins (0 where the per-bin row has no entry; 16-byte aligned); count / fill / supp as for the per-bin
+ * table. dfx_radon_forward_gtable: dfx_radon_forward_table over it (float32 sinogram rows of stride kstride): each
+ * pixel's channels are loaded once per group of four bins, and each bin sums its per-bin row's taps in the same
+ * order, so the result is dfx_radon_forward_table's, bit for bit. */
+int dfx_radon_gtable_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel, const uint8_t *supp,
+                           int32_t *counts, void *stream);
+int dfx_radon_gtable_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel, const uint8_t *supp,
+                          const int32_t *row_ptr, int32_t *pixels, float *weights, void *stream);
+int dfx_radon_forward_gtable(const float *img_k, float *sino_k, const int32_t *row_ptr, const int32_t *pixels,
+                             const float *weights, const int32_t *angles, int n_angles, int n_det, int kstride,
+                             int kb, float scale, void *stream);
+
 /* replaces support_ones / project_support / tmin (fista_poisson.py:256-263, 277-281; spdhg_poisson.py:259-265) on a
  * channel-fastest batch (npix, kstride) with padding channels kb .. kstride-1 (supp (npix) uint8 or NULL):
  * mode 0: x = 1 on live channels of support pixels, else 0; mode 1: x = 0 outside them or where negative;

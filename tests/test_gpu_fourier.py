@@ -146,7 +146,7 @@ def test_bf16_contraction_with_fourier_projector(golden):
     rounded to BF16 once for the tensor-core PF products (PF stored or generated per subset). Forward, adjoint and a
     subset's rows within 1e-2 of the float32 operator's; SPDHG with T streamed (x and z resident, host arrays
     through the staging buffers) gives the resident run's iterates, deviances and state bit for bit, and its
-    deviances stay within 1e-3 of the float32 run's."""
+    deviances stay within 1e-3 of the float32 run's, as do those of a run with T stored in BF16."""
     from conftest import case_inputs
     from diffractom_b200 import SinglePhaseForwardOperator, SPDHGPoisson
     d = golden("al5_small")
@@ -180,14 +180,17 @@ def test_bf16_contraction_with_fourier_projector(golden):
     b = rng.poisson(np.maximum(op32.direct(torch.as_tensor(x_true, device="cuda")).cpu().numpy(), 0) * 50
                     ).astype(np.float32)
     runs = {}
-    for key, o, resident in (("f32", op32, "all"), ("all", op, "all"), ("xz", op, ["x", "z"])):
+    for key, o, resident in (("f32", op32, "all"), ("all", op, "all"), ("xz", op, ["x", "z"]), ("t16", op, "all")):
         sp = SPDHGPoisson(o, subsets=3, seed=1, resident=resident)
+        sp.bf16_T = key == "t16"
         xr = sp.run(np.zeros(op.coeff_shape, np.float32), b, 4, diagnostics_interval=1)
         runs[key] = (xr, [st["f"] for st in sp.iter_stats], sp.state, sp.final_stats["resident"])
+        assert sp.final_stats["T_bf16"] == (key == "t16")
     assert runs["xz"][3] == ("x", "z")
     assert np.array_equal(runs["xz"][0], runs["all"][0]) and runs["xz"][1] == runs["all"][1]
     assert np.array_equal(runs["xz"][2]["z"], runs["all"][2]["z"])
     assert np.array_equal(runs["xz"][2]["y"], runs["all"][2]["y"])
     np.testing.assert_allclose(runs["all"][1], runs["f32"][1], rtol=1e-3)
+    np.testing.assert_allclose(runs["t16"][1], runs["f32"][1], rtol=1e-3)       # T rounded toward zero in BF16
     f = runs["all"][1]
     assert np.isfinite(f).all() and f[-1] < f[0]
