@@ -296,6 +296,9 @@ def main():
                     help="both: the BF16 tensor-core path (the value) and the float32 path (for the ratio)")
     ap.add_argument("--no-errors", action="store_true", help="skip the al99 precision check against the float64 "
                     "oracle loop")
+    ap.add_argument("--tc-forward", default="auto", choices=["auto", "on", "off"],
+                    help="the BF16 passes' forward projection on the tensor cores (dfx_radon_forward_tc) or through "
+                    "the ray table; auto: the operator's default")
     ap.add_argument("--no-generated", action="store_true", help="skip the arms with the PF generated on the fly "
                     "(no PF stored: the float32 CSR generated per batch, the BF16 PF per subset)")
     a = ap.parse_args()
@@ -350,6 +353,8 @@ def main():
                                     precision="bf16" if a.precision in ("bf16", "both") else "fp32")
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
+    if a.tc_forward != "auto":
+        op.use_tc_forward = a.tc_forward == "on"
     op.precision = "fp32"
     x_true = phantom(op, dict(w, grains=min(w["grains"], op.K)), seed=1 + rank)
     b = counts(op, x_true, w["mean_counts"], dist=dist)
@@ -630,6 +635,15 @@ def algorithmic_work(op, name, args_list):
             n_ang, kb = args[4], args[9]
             nb.append(4 * kb * npix + 2 * kb * n_ang * My)
             nf.append(2 * 2 * npix * n_ang * kb)
+        elif name == "dfx_radon_forward_gtable":
+            n_ang, kb = args[6], args[9]
+            nb.append(4 * kb * (npix + n_ang * My))
+            nf.append(2 * 2 * npix * n_ang * kb)
+        elif name == "dfx_radon_forward_tc":
+            # BF16 image in, sinogram rows out (BF16, or float32 when out_f32); the MMAs count the taps' FMAs
+            n_ang, kst, osz = args[5], args[9], 4 if args[3] else 2
+            nb.append(2 * kst * npix + osz * kst * n_ang * My)
+            nf.append(2 * 2 * npix * n_ang * kst)
         elif name == "dfx_radon_forward_table":
             n_ang, kb = args[5], args[8]
             nb.append(4 * kb * (npix + n_ang * My))

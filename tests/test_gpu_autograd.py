@@ -117,7 +117,8 @@ def test_memory_bounded_operator_gives_the_same_values_and_gradients():
     assert stored.pf_storage == "both"
     both, adj, ptr_f, batch_adj = stored.sparse_estimates(stored.sparse_fill_first)
     part_gb = (len(stored.batches) * ptr_f + batch_adj[0] + 1) / 1024.0 ** 3
-    ops = [_fe_config_operator(pf_mode="generated"), _fe_config_operator(pf_mode="auto", sparse_max_gb=part_gb)]
+    ops = [_fe_config_operator(pf_mode="generated"),
+           _fe_config_operator(pf_mode="auto", sparse_max_gb=part_gb, sparse_max_fill=1.0, sparse_max_fill_partial=1.0)]
     assert ops[0].pf_storage == "none" and ops[1].pf_storage.startswith("adjoint, 1 of")
     g = torch.Generator(device="cuda").manual_seed(21)
     supp = torch.as_tensor(stored.support_mask(), device="cuda")
