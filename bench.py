@@ -296,9 +296,10 @@ def main():
                     help="both: the BF16 tensor-core path (the value) and the float32 path (for the ratio)")
     ap.add_argument("--no-errors", action="store_true", help="skip the al99 precision check against the float64 "
                     "oracle loop")
-    ap.add_argument("--tc-forward", default="auto", choices=["auto", "on", "off"],
-                    help="the BF16 passes' forward projection on the tensor cores (dfx_radon_forward_tc) or through "
-                    "the ray table; auto: the operator's default")
+    ap.add_argument("--tc-forward", default="auto", choices=["auto", "on", "builder", "off"],
+                    help="the BF16 passes' forward projection on the tensor cores (on: weights from the per-geometry "
+                    "table, dfx_radon_forward_tc_table; builder: weights built per CTA, dfx_radon_forward_tc) or "
+                    "through the ray table (off); auto: the operator's default")
     ap.add_argument("--no-generated", action="store_true", help="skip the arms with the PF generated on the fly "
                     "(no PF stored: the float32 CSR generated per batch, the BF16 PF per subset)")
     a = ap.parse_args()
@@ -354,7 +355,9 @@ def main():
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
     if a.tc_forward != "auto":
-        op.use_tc_forward = a.tc_forward == "on"
+        op.use_tc_forward = a.tc_forward in ("on", "builder")
+        if a.tc_forward == "builder":
+            op.tc_weight_table_max_frac = 0.0
     op.precision = "fp32"
     x_true = phantom(op, dict(w, grains=min(w["grains"], op.K)), seed=1 + rank)
     b = counts(op, x_true, w["mean_counts"], dist=dist)

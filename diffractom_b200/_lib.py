@@ -45,6 +45,9 @@ SIGNATURES = {
     "dfx_radon_backward_spdhg_tc": ([P, L, P, I, I, I, I, I, I, I, I, P, P, P, F, F, P, S], c_int),
     "dfx_convert_rows": ([I, P, L, P, L, L, I, S], c_int),
     "dfx_radon_forward_tc": ([P, P, L, I, P, I, I, I, I, I, I, I, F, P, I, S], c_int),
+    "dfx_radon_tc_weights_bytes": ([I, I, I], c_int64),
+    "dfx_radon_tc_weights": ([P, I, I, I, I, I, I, P, P, S], c_int),
+    "dfx_radon_forward_tc_table": ([P, P, L, I, P, P, P, I, I, I, I, I, F, P, I, S], c_int),
     "dfx_radon_table_count": ([P, I, I, I, I, I, P, P, S], c_int),
     "dfx_radon_table_fill": ([P, I, I, I, I, I, P, P, P, S], c_int),
     "dfx_radon_forward_table": ([P, P, P, P, P, I, I, I, I, F, S], c_int),

@@ -302,6 +302,203 @@ __global__ void __launch_bounds__(TF_THREADS, 1) tc_forward(const __grid_constan
     }
 }
 
+// ---------------------------------------------------------------------------------------------- weight-table variant
+// The weight tiles depend on (angle, tile) only, not on the channels: built once per geometry into a table (hi and lo
+// tiles in the B operand's shared-memory layout, 8 KB per (angle, tile), and the window start), they are loaded by
+// the producer with the image tile (a bulk copy beside the TMA), so the MMA warp waits for copies only.
+constexpr int TW_W_BYTES = 2 * TF_W_BYTES;                  // hi | lo
+constexpr int TW_STAGE_BYTES = TF_X_BYTES + TW_W_BYTES;     // 24 KB: image tile, then its weights
+constexpr int TW_STAGES = 6;
+constexpr int TW_THREADS = 192;                             // warp 0 loads, warp 1 MMAs, warps 2-5 epilogue
+
+template <int KERNEL>
+__global__ void __launch_bounds__(TF_PX) tcf_weights_kernel(const float4 *__restrict__ geo, int nx, int ny, int ns,
+                                                           int n_taps, int tiles_x, int n_tiles_img,
+                                                           uint8_t *__restrict__ weights, int32_t *__restrict__ windows)
+{
+    const int t = blockIdx.x, a = blockIdx.y, m = threadIdx.x;
+    const AngleGeo ga = load_geo(geo, a);
+    const int px0 = (t % tiles_x) * TF_T, py0 = (t / tiles_x) * TF_T;
+    const int sw = window16<KERNEL>(ga, px0, py0, ns);
+    const int64_t row = (int64_t)a * n_tiles_img + t;
+    uint8_t *wh = weights + row * TW_W_BYTES, *wl = wh + TF_W_BYTES;
+    uint4 *w4 = reinterpret_cast<uint4 *>(wh);
+    for (int i = m; i < TW_W_BYTES / 16; i += TF_PX) w4[i] = make_uint4(0, 0, 0, 0);
+    if (m == 0) windows[row] = sw;
+    __syncthreads();
+    const int px = px0 + (m & (TF_T - 1)), py = py0 + (m >> 3);
+    if (px >= nx || py >= ny) return;
+    const float fx = (float)px, fy = (float)py;
+    const float tt = __fmaf_rn(ga.A, ga.rows_are_y ? fx : fy, __fmaf_rn(ga.B, ga.rows_are_y ? fy : fx, ga.T0));
+    const int sf = KERNEL == 1 ? (int)floorf(__fsub_rn(tt, ga.hw)) + 1 : (int)floorf(tt);
+    const int nt = KERNEL == 1 ? min(max(2, (int)ceilf(1.0f + fabsf(ga.A) - 1e-6f)), n_taps) : 2;
+    for (int q = 0; q < nt; ++q) {
+        const int s = sf + q;
+        if (s < 0 || s >= ns) continue;
+        const float w = tap_weight<KERNEL>(ga, __fsub_rn(tt, (float)s));
+        if (w == 0.0f) continue;
+        const int n = s - sw;
+        if (n < 0 || n >= TF_NW) {
+            atomicOr(&g_tcf_flags, DFX_TC_WINDOW);
+            continue;
+        }
+        const __nv_bfloat16 hi = __float2bfloat16_rn(w);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(__fsub_rn(w, __bfloat162float(hi)));
+        *reinterpret_cast<__nv_bfloat16 *>(wh + w_offset(n, m)) = hi;
+        *reinterpret_cast<__nv_bfloat16 *>(wl + w_offset(n, m)) = lo;
+    }
+}
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+struct TwArgs {
+    const uint8_t *weights;
+    const int32_t *windows;
+    const int32_t *angle_rows;                  // table row of each launch angle (NULL: the launch angle)
+    int n_tiles_img;
+};
+
+__global__ void __launch_bounds__(TW_THREADS, 1) tc_forward_tab(const __grid_constant__ CUtensorMap xmap, TfArgs p,
+                                                               TwArgs q)
+{
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TW_STAGES * TW_STAGE_BYTES);   // full[S], empty[S], done
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * TW_STAGES + 1);
+    int *n_issued = reinterpret_cast<int *>(tmem_slot + 1), *n_used = n_issued + 1;
+    volatile int *abort = n_issued + 2;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int a = blockIdx.x, k0 = blockIdx.y * TF_CH;
+    const int arow = q.angle_rows ? __ldg(q.angle_rows + a) : a;
+    const uint32_t full0 = smem_u32(bars), empty0 = full0 + 8 * TW_STAGES, done = empty0 + 8 * TW_STAGES;
+
+    if (tid == 0) {
+        for (int st = 0; st < TW_STAGES; ++st) {
+            mbar_init(full0 + 8 * st, 1);
+            mbar_init(empty0 + 8 * st, 1);
+        }
+        mbar_init(done, 1);
+        *n_issued = *n_used = 0;
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&xmap)) : "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"((uint32_t)p.tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    if (warp >= 2) {
+        const uint32_t lanes = (uint32_t)(32 * (warp & 3)) << 16;
+        for (int c = 0; c < p.tmem_cols; c += 16) tmem_st16_zero(tmem + lanes + (uint32_t)c);
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+
+    const int n_tiles = p.n_tiles;
+    const uint8_t *wrow = q.weights + (int64_t)arow * q.n_tiles_img * TW_W_BYTES;
+    const int32_t *winrow = q.windows + (int64_t)arow * q.n_tiles_img;
+    if (warp == 0) {
+        // ---- producer: image tile (TMA) and its weight tiles (bulk copy), up to TW_STAGES ahead of the MMAs
+        if (lane == 0) {
+            int issued = 0;
+            for (int i = 0; i < n_tiles; ++i) {
+                const int st = i % TW_STAGES;
+                if (i >= TW_STAGES && !wait_or_abort(empty0 + 8 * st, ((i - TW_STAGES) / TW_STAGES) & 1, abort))
+                    break;
+                const int t = p.tiles ? __ldg(p.tiles + i) : i;
+                const int px0 = (t % p.tiles_x) * TF_T, py0 = (t / p.tiles_x) * TF_T;
+                const uint32_t fb = full0 + 8 * st, xs = smem_u32(smem + st * TW_STAGE_BYTES);
+                mbar_expect_tx(fb, (uint32_t)TW_STAGE_BYTES);
+                tma_load_3d(xs, &xmap, fb, k0, px0, py0);
+                tma_load_3d(xs + TF_X_BYTES / 2, &xmap, fb, k0 + 64, px0, py0);
+                bulk_load(xs + TF_X_BYTES, wrow + (int64_t)t * TW_W_BYTES, (uint32_t)TW_W_BYTES, fb);
+                issued = i + 1;
+            }
+            *n_issued = issued;
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = instr_desc(TF_NW, 1, 0);
+            for (int i = 0; i < n_tiles; ++i) {
+                const int st = i % TW_STAGES;
+                if (!wait_or_abort(full0 + 8 * st, (i / TW_STAGES) & 1, abort)) break;
+                *n_used = i + 1;
+                tc_fence_after();
+                const int t = p.tiles ? __ldg(p.tiles + i) : i;
+                const uint32_t dcol = tmem + (uint32_t)__ldg(winrow + t);
+                const uint32_t xb = smem_u32(smem + st * TW_STAGE_BYTES);
+                const uint32_t hb = xb + TF_X_BYTES, lb = hb + TF_W_BYTES;
+#pragma unroll
+                for (int kk = 0; kk < TF_PX / 16; ++kk) {
+                    const uint64_t ad = smem_desc(xb + kk * 2048, TF_X_BYTES / 2, 1024, SW_128B);
+                    mma_bf16(dcol, ad, smem_desc(hb + kk * 256, 128, 1024, SW_NONE), idesc, 1);
+                    mma_bf16(dcol, ad, smem_desc(lb + kk * 256, 128, 1024, SW_NONE), idesc, 1);
+                }
+                mma_commit(empty0 + 8 * st);
+            }
+            mma_commit(done);
+        }
+    } else {
+        // ---- epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. + 31 = channels k0 + 32 (w % 4) + lane
+        bool ok = wait_or_abort(done, 0, abort);
+        ok = __all_sync(0xffffffffu, ok && !*abort);
+        tc_fence_after();
+        const int q4 = warp & 3;
+        const int k = k0 + 32 * q4 + lane;
+        if (ok) {
+            const uint32_t lanes = (uint32_t)(32 * q4) << 16;
+            for (int c0 = 0; c0 < p.ns; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + lanes + (uint32_t)c0, v);
+                if (k < p.kstride) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int s = c0 + j;
+                        if (s >= p.ns) break;
+                        const int64_t o = ((int64_t)a * p.ns + s) * p.sld + k;
+                        const float val = __fmul_rn(p.scale, v[j]);
+                        if (p.out_f32)
+                            reinterpret_cast<float *>(p.out)[o] = val;
+                        else
+                            reinterpret_cast<__nv_bfloat16 *>(p.out)[o] = __float2bfloat16_rn(val);
+                    }
+                }
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 32) mbar_wait(done, 0, DFX_TC_TIMEOUT, &g_tcf_flags);      // every MMA has completed
+    if (tid == 64) {
+        // loads issued but never consumed (only after an expired wait): let them land before the CTA exits
+        for (int i = *n_used; i < *n_issued; ++i)
+            if (!mbar_wait(full0 + 8 * (i % TW_STAGES), (i / TW_STAGES) & 1, DFX_TC_TIMEOUT, &g_tcf_flags)) break;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)p.tmem_cols));
+    }
+}
+
+size_t tw_smem_bytes() { return 1024 + (size_t)TW_STAGES * TW_STAGE_BYTES + 256; }
+
 size_t tf_smem_bytes() { return 1024 + (size_t)TF_STAGES * TF_X_BYTES + (size_t)TF_WBUF * 2 * TF_W_BYTES + 256; }
 
 // 3-D BF16 image batch (channels, x, y) with a box of 64 channels x 8 x 8 pixels, 128-byte swizzle
@@ -338,6 +535,81 @@ unsigned int tcf_status(unsigned int reset)
 }  // namespace dfx
 
 using namespace dfx;
+
+extern "C" int64_t dfx_radon_tc_weights_bytes(int n_angles, int nx, int ny)
+{
+    if (n_angles <= 0 || nx <= 0 || ny <= 0) return 0;
+    return (int64_t)n_angles * cdiv(nx, TF_T) * cdiv(ny, TF_T) * TW_W_BYTES;
+}
+
+extern "C" int dfx_radon_tc_weights(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel, int n_taps,
+                                    void *weights, int32_t *windows, void *stream)
+{
+    DFX_REQUIRE(geo && weights && windows, "radon_tc_weights: null pointer");
+    DFX_REQUIRE(((uintptr_t)geo % 16) == 0 && ((uintptr_t)weights % 16) == 0, "radon_tc_weights: misaligned arrays");
+    DFX_REQUIRE(n_angles > 0 && n_angles <= 65535 && nx > 0 && ny > 0 && n_det > 0, "radon_tc_weights: bad sizes");
+    DFX_REQUIRE(kernel == 0 || kernel == 1, "radon_tc_weights: kernel must be 0 or 1");
+    DFX_REQUIRE(n_taps >= 2 && n_taps <= 64, "radon_tc_weights: n_taps (%d) out of range", n_taps);
+    const int tiles_x = (int)cdiv(nx, TF_T), n_tiles = tiles_x * (int)cdiv(ny, TF_T);
+    const dim3 grid((unsigned)n_tiles, (unsigned)n_angles);
+    if (kernel == 1)
+        tcf_weights_kernel<1><<<grid, TF_PX, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), nx, ny, n_det, n_taps, tiles_x, n_tiles,
+            reinterpret_cast<uint8_t *>(weights), windows);
+    else
+        tcf_weights_kernel<0><<<grid, TF_PX, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), nx, ny, n_det, n_taps, tiles_x, n_tiles,
+            reinterpret_cast<uint8_t *>(weights), windows);
+    return launch_status("radon_tc_weights");
+}
+
+extern "C" int dfx_radon_forward_tc_table(const void *img_bf16, void *sino, int64_t sino_ld, int out_f32,
+                                          const void *weights, const int32_t *windows, const int32_t *angle_rows,
+                                          int n_angles, int nx, int ny, int n_det, int kstride, float scale,
+                                          const int32_t *tiles, int n_tiles, void *stream)
+{
+    DFX_REQUIRE(img_bf16 && sino && weights && windows, "radon_forward_tc_table: null pointer");
+    DFX_REQUIRE(((uintptr_t)weights % 16) == 0, "radon_forward_tc_table: weights must be 16-byte aligned");
+    DFX_REQUIRE(n_angles >= 0 && n_angles <= 65535 && nx > 0 && ny > 0 && n_det > 0,
+                "radon_forward_tc_table: bad sizes (angles %d, %d x %d, %d bins)", n_angles, nx, ny, n_det);
+    DFX_REQUIRE(kstride > 0 && kstride % 64 == 0, "radon_forward_tc_table: kstride (%d) must be a multiple of 64",
+                kstride);
+    DFX_REQUIRE(sino_ld >= kstride && sino_ld % 8 == 0, "radon_forward_tc_table: bad sinogram row stride");
+    const int tiles_x = (int)cdiv(nx, TF_T), tiles_img = tiles_x * (int)cdiv(ny, TF_T);
+    DFX_REQUIRE(tiles == nullptr ? true : (n_tiles >= 0 && n_tiles <= tiles_img),
+                "radon_forward_tc_table: bad tile list");
+    int cols = 32;
+    while (cols < n_det + TF_NW - 1) cols *= 2;
+    DFX_REQUIRE(cols <= 512, "radon_forward_tc_table: %d bins exceed the tensor memory of one CTA", n_det);
+    if (n_angles == 0) return DFX_OK;
+    CUtensorMap xmap;
+    int st = make_image_map(&xmap, img_bf16, kstride, nx, ny);
+    if (st) return st;
+    TfArgs a{};
+    a.n_angles = n_angles;
+    a.nx = nx;
+    a.ny = ny;
+    a.ns = n_det;
+    a.kstride = kstride;
+    a.tiles = tiles;
+    a.n_tiles = tiles ? n_tiles : tiles_img;
+    a.tiles_x = tiles_x;
+    a.tmem_cols = cols;
+    a.out = sino;
+    a.sld = sino_ld;
+    a.scale = scale;
+    a.out_f32 = out_f32 ? 1 : 0;
+    TwArgs q{reinterpret_cast<const uint8_t *>(weights), windows, angle_rows, tiles_img};
+    const size_t smem = tw_smem_bytes();
+    const cudaError_t e = cudaFuncSetAttribute(tc_forward_tab, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+        set_error("radon_forward_tc_table: shared memory attribute: %s", cudaGetErrorString(e));
+        return DFX_ELAUNCH;
+    }
+    const dim3 grid((unsigned)n_angles, (unsigned)cdiv(kstride, TF_CH));
+    tc_forward_tab<<<grid, TW_THREADS, smem, (cudaStream_t)stream>>>(xmap, a, q);
+    return launch_status("radon_forward_tc_table");
+}
 
 extern "C" int dfx_radon_forward_tc(const void *img_bf16, void *sino, int64_t sino_ld, int out_f32, const float *geo,
                                     int n_angles, int nx, int ny, int n_det, int kstride, int kernel, int n_taps,

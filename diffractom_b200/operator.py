@@ -36,6 +36,7 @@ AUTO_FFT_PIXELS = 400 * 400   # projector="auto": the Fourier-slice projector fo
 SPARSE_MIN_BATCHES = 4    # sparse modes: at least this many batches (SPFO:135)
 CAND_BYTES = 2 + 4 + 4 + 4 + 4          # per candidate / non-zero scratch of the reference's generator
 NNZ_BYTES = 2 + 4 + 4 + 2 + 4 + 2 + 4   # (pf_generate.py:29-30), used by the batch-size rule
+GTABLE_MIN_ANGLES = 64                   # float32 forward projections of this many angles read the grouped table
 KSTRIDE_ALIGN = 16                       # channel stride of the batch buffers (16 channels per tensor-memory load)
 
 
@@ -368,6 +369,10 @@ class SinglePhaseForwardOperator:
         om_ptr = None if om is None else om.data_ptr()
         rp, ent = (self._ray_rp, self._ray_ent) if ray is None else ray[:2]
         grp = self._ray_grp if ray is None else (ray[3] if len(ray) > 3 else None)
+        # the grouped table has a quarter of the warps: for a few angles (a subset) the per-bin one fills the GPU
+        # better (at 256 x 256, 1024 channels: 18 angles 0.57 vs 0.67 ms; 360 angles 8.6 ms grouped)
+        if grp is not None and n_ang < GTABLE_MIN_ANGLES:
+            grp = None
         if sld is None and grp is not None:
             self._call("dfx_radon_forward_gtable", src_ptr, dst_ptr, grp[0].data_ptr(), grp[1].data_ptr(),
                        grp[2].data_ptr(), om_ptr, n_ang, self.My, self.Kstride, kb, float(self.radon_geo.scale),
@@ -926,6 +931,12 @@ class SinglePhaseForwardOperator:
         image that is zero outside the support may skip the other tiles)."""
         if self.use_tc_forward and getattr(self, "tc_forward", False):
             tp, nt = (None, 0) if tiles is None else (tiles.data_ptr(), int(tiles.numel()))
+            tab = self._tc_weight_table()
+            if tab is not None:
+                self._call("dfx_radon_forward_tc_table", src_ptr, dst_ptr, self.Ktot, 0, tab[0].data_ptr(),
+                           tab[1].data_ptr(), om.data_ptr(), n, self.Nx, self.Ny, self.My, self.Kstride,
+                           float(self.radon_geo.scale), tp, nt, self._s())
+                return
             self._call("dfx_radon_forward_tc", src_ptr, dst_ptr, self.Ktot, 0, geo.data_ptr(), n, self.Nx, self.Ny,
                        self.My, self.Kstride, self._kernel_id, int(self.radon_geo.n_taps),
                        float(self.radon_geo.scale), tp, nt, self._s())
@@ -933,6 +944,29 @@ class SinglePhaseForwardOperator:
         rp, ent = (self._ray_rp, self._ray_ent) if ray is None else ray[:2]
         self._call("dfx_radon_forward_table_bf16_bf16", src_ptr, dst_ptr, self.Ktot, rp.data_ptr(), ent.data_ptr(),
                    om.data_ptr(), n, self.My, self.Kstride, kb, float(self.radon_geo.scale), self._s())
+
+    # the tensor-core forward reads its weight tiles from a table built once per geometry (8 KB per angle and 8 x 8
+    # pixel tile) when that takes at most this fraction of the free device memory; else each CTA builds them
+    tc_weight_table_max_frac = 0.1
+
+    def _tc_weight_table(self):
+        """(weights, windows) of dfx_radon_tc_weights for every angle, built on first use, or None."""
+        tab = getattr(self, "_tcf_tab", None)
+        if tab is not None:
+            return tab or None
+        R = self.N_Omega
+        nb = int(self._lib.dfx_radon_tc_weights_bytes(R, self.Nx, self.Ny))
+        free, _ = torch.cuda.mem_get_info(self.device)
+        if nb <= 0 or nb > self.tc_weight_table_max_frac * free:
+            self._tcf_tab = ()
+            return None
+        n_tiles = (-(-self.Nx // 8)) * (-(-self.Ny // 8))
+        w = torch.empty(nb, dtype=torch.uint8, device=self.device)
+        win = torch.empty(R * n_tiles, dtype=torch.int32, device=self.device)
+        self._call("dfx_radon_tc_weights", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, self.My, self._kernel_id,
+                   int(self.radon_geo.n_taps), w.data_ptr(), win.data_ptr(), self._s())
+        self._tcf_tab = (w, win)
+        return self._tcf_tab
 
     def support_tiles(self, supp):
         """int32 device tensor of the 8 x 8 pixel tiles (row-major over the tile grid) holding at least one pixel of
@@ -1282,6 +1316,7 @@ class SinglePhaseForwardOperator:
         self.release_streamer()
         self._ray_supp = {}
         self._ray_grp = None
+        self._tcf_tab = None
         self._supp_tiles = {}
         self._fft = None
         self.sparse_batches = None

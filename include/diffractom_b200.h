@@ -363,6 +363,18 @@ int dfx_convert_rows(int to_bf16, float *f32, int64_t ld_f32, void *b16, int64_t
 int dfx_radon_forward_tc(const void *img_bf16, void *sino, int64_t sino_ld, int out_f32, const float *geo,
                          int n_angles, int nx, int ny, int n_det, int kstride, int kernel, int n_taps, float scale,
                          const int32_t *tiles, int n_tiles, void *stream);
+/* The weight tiles of dfx_radon_forward_tc precomputed per geometry (no reference counterpart): for every angle a of
+ * geo and 8 x 8 pixel tile t (row-major over the tile grid), 8192 bytes at weights + (a * n_tiles + t) * 8192 (the
+ * tap weights of the tile's pixels on its 32-bin window as BF16 hi and lo parts, in the MMA operand's layout) and
+ * the window's first bin at windows[a * n_tiles + t]; weights 16-byte aligned, dfx_radon_tc_weights_bytes long.
+ * dfx_radon_forward_tc_table: dfx_radon_forward_tc reading them (launch angle i = row angle_rows[i] of the table,
+ * angle_rows NULL: i), the same products in the same order, hence the same bits. */
+int64_t dfx_radon_tc_weights_bytes(int n_angles, int nx, int ny);
+int dfx_radon_tc_weights(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel, int n_taps,
+                         void *weights, int32_t *windows, void *stream);
+int dfx_radon_forward_tc_table(const void *img_bf16, void *sino, int64_t sino_ld, int out_f32, const void *weights,
+                               const int32_t *windows, const int32_t *angle_rows, int n_angles, int nx, int ny,
+                               int n_det, int kstride, float scale, const int32_t *tiles, int n_tiles, void *stream);
 
 /* Bits of device-side waits of the tensor-core kernels that ran out since the last reset (DFX_TC_TIMEOUT); the
  * kernels return early on expiry and leave their outputs undefined. Synchronous; no reference counterpart. */

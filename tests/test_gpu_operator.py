@@ -202,22 +202,28 @@ def test_ray_table_forward_equals_footprint_forward(golden, name):
     op._radon_fwd(img.data_ptr(), zb.data_ptr(), None, R, kb, sld=ks + 8)
     assert torch.equal(zb[:, :, :ks], a.to(torch.bfloat16))
     assert op.ray_taps == int(op._ray_rp[-1].item()) > 0
-    # the float32 forward reads the grouped table (four bins per pixel load): the per-bin table's bits, also for a
-    # support's tables and a subset's angles
+    # the float32 forward of many angles reads the grouped table (four bins per pixel load): the per-bin table's
+    # bits, for all angles, a subset's angles, and a support's tables
     assert op._ray_grp is not None
-    t = torch.empty((R, ns, ks), device="cuda")
-    _lib.call("dfx_radon_forward_table", img.data_ptr(), t.data_ptr(), op._ray_rp.data_ptr(), op._ray_ent.data_ptr(),
-              None, R, ns, ks, kb, float(op.radon_geo.scale), s)
-    assert torch.equal(t, a)
+
+    def grouped(src, rows, tabs):
+        n = R if rows is None else rows.numel()
+        out = torch.empty((n, ns, ks), device="cuda")
+        _lib.call("dfx_radon_forward_gtable", src.data_ptr(), out.data_ptr(), tabs[0].data_ptr(), tabs[1].data_ptr(),
+                  tabs[2].data_ptr(), None if rows is None else rows.data_ptr(), n, ns, ks, kb,
+                  float(op.radon_geo.scale), s)
+        return out
+
+    assert torch.equal(grouped(img, None, op._ray_grp), a)
+    assert torch.equal(grouped(img, om, op._ray_grp), a[om.long()])
     supp = torch.as_tensor(op.support_mask().ravel().astype(np.uint8), device="cuda")
     ray = op.support_ray_table(supp)
     assert len(ray) == 4 and int(ray[3][0][-1].item()) <= int(op._ray_grp[0][-1].item())
     imgs = img * supp.float()[:, None]
-    g, t = torch.empty((om.numel(), ns, ks), device="cuda"), torch.empty((om.numel(), ns, ks), device="cuda")
-    op._radon_fwd(imgs.data_ptr(), g.data_ptr(), om, om.numel(), kb, ray=ray)
+    t = torch.empty((om.numel(), ns, ks), device="cuda")
     _lib.call("dfx_radon_forward_table", imgs.data_ptr(), t.data_ptr(), ray[0].data_ptr(), ray[1].data_ptr(),
               om.data_ptr(), om.numel(), ns, ks, kb, float(op.radon_geo.scale), s)
-    assert torch.equal(g, t)
+    assert torch.equal(grouped(imgs, om, ray[3]), t)
 
 
 def test_operator_on_its_own_queue_equals_current_stream(golden):

@@ -3,7 +3,8 @@ hi + lo parts, float32 accumulation) against the table-driven forward of the sam
 the image widened to float32, exactly): float32 outputs within 2e-5 of the largest value, for the trapezoid and the
 hat kernel, every angle of the golden geometries and of a 256 x 256, 360-angle scan; a tile list that skips the
 tiles outside a support equals the full projection of an image that is zero there; BF16 output rows in a wider
-sinogram; no tensor-core wait ran out and no tap left its window; BF16 SPDHG with and without it."""
+sinogram; the weight-table variant gives the same bits; no tensor-core wait ran out and no tap left its window;
+BF16 SPDHG with and without it."""
 import ctypes
 
 import numpy as np
@@ -97,6 +98,46 @@ def test_tc_forward_full_scan_support_tiles_and_bf16_rows():
     torch.cuda.synchronize()
     assert torch.equal(z[:, :, op.Kstride:2 * op.Kstride], tc.to(torch.bfloat16))
     assert not z[:, :, :op.Kstride].any() and not z[:, :, 2 * op.Kstride:].any()
+    assert _flags(lib) == 0
+
+
+@pytest.mark.parametrize("case", ["al5_small", "ti256"])
+def test_tc_forward_from_the_weight_table_equals_the_built_weights(golden, case):
+    """dfx_radon_forward_tc_table (weight tiles precomputed per geometry by dfx_radon_tc_weights, loaded beside the
+    image tiles) gives dfx_radon_forward_tc's bits: all angles, a subset's angle rows with a support tile list, BF16
+    rows in a wider sinogram."""
+    from diffractom_b200 import SinglePhaseForwardOperator, _lib
+    if case == "ti256":
+        op = _ti256_operator()
+    else:
+        d = golden(case)
+        cfg, mat, grid = case_inputs(d)
+        op = SinglePhaseForwardOperator(cfg, mat, grid, 1e-5, normalized=True, quadrature=d["quadrature"],
+                                        precision="bf16")
+    assert op.tc_forward
+    lib = _lib.lib()
+    _flags(lib)
+    R, My, ks, s = op.N_Omega, op.My, op.Kstride, op._s()
+    w, win = op._tc_weight_table()
+    assert w.numel() == lib.dfx_radon_tc_weights_bytes(R, op.Nx, op.Ny)
+    supp = op.support_mask()
+    img = _image(op, 8, supp)
+    tiles = op.support_tiles(torch.as_tensor(supp.ravel().astype(np.uint8), device="cuda"))
+    om = torch.arange(2, R, 5, dtype=torch.int32, device="cuda")
+    geo_sub = op.geo_gpu[om.long()].contiguous()
+    for rows, geo, tl in ((None, op.geo_gpu, None), (om, geo_sub, tiles)):
+        n = R if rows is None else rows.numel()
+        tp, nt = (None, 0) if tl is None else (tl.data_ptr(), int(tl.numel()))
+        ref = torch.full((n, My, 2 * ks), 7.0, dtype=torch.bfloat16, device="cuda")
+        got = torch.full((n, My, 2 * ks), 7.0, dtype=torch.bfloat16, device="cuda")
+        _lib.call("dfx_radon_forward_tc", img.data_ptr(), ref.data_ptr() + 2 * ks, 2 * ks, 0, geo.data_ptr(), n,
+                  op.Nx, op.Ny, My, ks, op._kernel_id, int(op.radon_geo.n_taps), float(op.radon_geo.scale), tp, nt, s)
+        _lib.call("dfx_radon_forward_tc_table", img.data_ptr(), got.data_ptr() + 2 * ks, 2 * ks, 0, w.data_ptr(),
+                  win.data_ptr(), None if rows is None else rows.data_ptr(), n, op.Nx, op.Ny, My, ks,
+                  float(op.radon_geo.scale), tp, nt, s)
+        torch.cuda.synchronize()
+        assert torch.equal(got, ref)
+        assert torch.all(got[:, :, :ks] == 7.0)
     assert _flags(lib) == 0
 
 
