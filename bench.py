@@ -108,7 +108,7 @@ def counts(op, x_true, mean, seed=2, dist=None):
     ax = op.direct(x_true)
     if dist is not None:
         dist.all_reduce(ax)
-    lam = ax * (mean / float(ax.double().mean().item()))
+    lam = (ax * (mean / float(ax.double().mean().item()))).clamp_min_(0.0)
     g = torch.Generator(device=op.device)
     g.manual_seed(seed)
     b = torch.poisson(lam, generator=g)
@@ -792,7 +792,9 @@ def counts_batched(op, grains, mean, seed=1):
             idx = torch.as_tensor(pix[sel] * op.Kstride + (owner[sel] - bt["k_start"]), device=op.device)
             buf[idx] = 1.0
             op._direct_batch_k(buf.data_ptr(), ib, D)
-        lam = D * (mean / float(D.double().mean().item()))
+        # the Fourier-slice projection of a non-negative image can dip slightly below zero (the interpolation's
+        # ringing): Poisson rates are clamped at 0
+        lam = (D * (mean / float(D.double().mean().item()))).clamp_min_(0.0)
         g = torch.Generator(device=op.device)
         g.manual_seed(seed + 1)
         b = torch.poisson(lam, generator=g)

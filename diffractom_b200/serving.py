@@ -46,7 +46,9 @@ class Request:
     max_gb: float = 2.0
     seed: int = 0
     id: int = 0
-    graphs: bool = True          # replay the SPDHG iterations as CUDA graphs from the second epoch on
+    # replay the SPDHG iterations as CUDA graphs from the second epoch on; off by default: a capture on one request's
+    # stream is invalidated when another request's thread synchronises the device meanwhile (an operator build does)
+    graphs: bool = False
     # filled in by the server
     arrival: float = 0.0
     admitted: float = 0.0
@@ -203,8 +205,11 @@ class ReconstructionServer:
             with self._lock:
                 if self._stop:
                     return
-                free, _ = torch.cuda.mem_get_info(self.device)
-                for rid in self.sched.admit(free_bytes=int(free) - (1 << 30)):
+                try:
+                    free = int(torch.cuda.mem_get_info(self.device)[0]) - (1 << 30)
+                except RuntimeError:            # a query failing now and then must not end the admissions
+                    free = None
+                for rid in self.sched.admit(free_bytes=free):
                     req = self.requests[rid]
                     req.admitted = self.now()
                     w = threading.Thread(target=self._work, args=(req,), name=f"dfx-request-{rid}", daemon=True)

