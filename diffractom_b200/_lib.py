@@ -39,6 +39,7 @@ SIGNATURES = {
     "dfx_radon_backward": ([P, P, P, I, I, I, I, I, I, I, I, S], c_int),
     "dfx_radon_backward_pixels": ([P, P, P, I, I, I, I, I, I, I, I, P, L, S], c_int),
     "dfx_radon_backward_spdhg": ([P, P, I, I, I, I, I, I, I, I, P, P, P, F, F, S], c_int),
+    "dfx_radon_backward_quads": ([I], c_int),
     "dfx_radon_forward_bf16": ([P, P, L, P, I, I, I, I, I, I, I, F, S], c_int),
     "dfx_radon_backward_bf16": ([P, L, P, P, I, I, I, I, I, I, I, I, S], c_int),
     "dfx_radon_backward_spdhg_bf16": ([P, L, P, I, I, I, I, I, I, I, I, P, P, P, F, F, P, S], c_int),

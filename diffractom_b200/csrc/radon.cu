@@ -529,6 +529,124 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
     }
 }
 
+// Four neighbouring pixels per warp (flat indices 4 w .. 4 w + 3, a row's neighbours when nx is a multiple of 4):
+// per angle their taps cover a few adjacent bins, so each bin row in the union of their taps is loaded once and added
+// to every pixel whose taps include it. Per pixel the taps, weights and their order are those of radon_backward_v3
+// (the two-tap case adds both taps, the general case skips zero weights and bins off the detector), so the sums are
+// its bits, with about half of its loads through L1.
+template <int KERNEL, int MODE, typename ST>
+__global__ void __launch_bounds__(32 * WARPS) radon_backward_q4(
+    const ST *__restrict__ sino, int64_t sld, float *__restrict__ img, const float4 *__restrict__ geo, int n_angles,
+    int nx, int npix, int ns, int kstride, int kb, int n_taps, float *__restrict__ z, const float *__restrict__ T,
+    float inv_p, float lam, __nv_bfloat16 *__restrict__ xb)
+{
+    constexpr int NP = 4;
+    extern __shared__ AngleParams prm[];
+    for (int i = threadIdx.x; i < n_angles; i += blockDim.x) prm[i] = pack_geo(load_geo(geo, i));
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t p0 = ((int64_t)blockIdx.x * WARPS + warp) * NP;
+    const int k = blockIdx.y * CPW + lane * CPL;
+    if (p0 >= npix || k >= kstride) return;
+    const int np = (int)min((int64_t)NP, (int64_t)npix - p0);
+    if (blockIdx.y * CPW >= kb) {          // a block of padding channels only
+        if (MODE == 0) {
+            const float zero[CPL] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            for (int j = 0; j < np; ++j) st8(img + (p0 + j) * kstride + k, zero);
+        }
+        return;
+    }
+    float fx[NP], fy[NP];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+        const int64_t pix = p0 + min(j, np - 1);
+        fx[j] = (float)(int)(pix % nx);
+        fy[j] = (float)(int)(pix / nx);
+    }
+    float acc[NP][CPL];
+#pragma unroll
+    for (int j = 0; j < NP; ++j)
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) acc[j][c] = 0.0f;
+    const ST *col = sino + k;
+    const int64_t angle_stride = (int64_t)ns * sld;
+    for (int a = 0; a < n_angles; ++a, col += angle_stride) {
+        const AngleGeo g = unpack_geo(prm[a]);
+        const int ntap = taps_of(g, KERNEL, n_taps);
+        float t[NP];
+        int sf[NP];
+        bool fast[NP];
+        int lo = 0x7fffffff, hi = -0x7fffffff;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+            t[j] = __fmaf_rn(g.A, g.rows_are_y ? fx[j] : fy[j], __fmaf_rn(g.B, g.rows_are_y ? fy[j] : fx[j], g.T0));
+            sf[j] = first_tap<KERNEL>(g, t[j]);
+            fast[j] = ntap == 2 && sf[j] >= 0 && sf[j] + 1 < ns;
+            if (j < np) {
+                lo = min(lo, sf[j]);
+                hi = max(hi, sf[j] + ntap - 1);
+            }
+        }
+        lo = max(lo, 0);
+        hi = min(hi, ns - 1);
+        for (int sb = lo; sb <= hi; ++sb) {
+            float w[NP];
+            bool use[NP];
+            bool any = false;
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+                use[j] = false;
+                w[j] = 0.0f;
+                const int d = sb - sf[j];
+                if (j < np && d >= 0 && d < ntap) {
+                    const float wt = tap_weight<KERNEL>(g, __fsub_rn(t[j], (float)sb));
+                    if (fast[j] || wt != 0.0f) {
+                        use[j] = true;
+                        w[j] = __fmul_rn(g.w, wt);
+                        any = true;
+                    }
+                }
+            }
+            if (!any) continue;
+            float4 q0, q1;
+            ld8(col + (int64_t)sb * sld, q0, q1);
+#pragma unroll
+            for (int j = 0; j < NP; ++j)
+                if (use[j]) acc8(acc[j], w[j], q0, q1);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+        if (j >= np) break;
+        const int64_t o = (p0 + j) * kstride + k;
+        if (MODE == 0) {
+            float r[CPL];
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) r[c] = (k + c < kb) ? acc[j][c] : 0.0f;
+            float4 *d = reinterpret_cast<float4 *>(img + o);
+            d[0] = make_float4(r[0], r[1], r[2], r[3]);
+            d[1] = make_float4(r[4], r[5], r[6], r[7]);
+        } else {
+            float xn[CPL];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                float4 *xp = reinterpret_cast<float4 *>(img + o) + q;
+                float4 *zp = reinterpret_cast<float4 *>(z + o) + q;
+                float4 xv = *xp, zv = *zp;
+                const float4 tv = __ldg(reinterpret_cast<const float4 *>(T + o) + q);
+                primal_step(xv.x, zv.x, tv.x, (k + 4 * q + 0 < kb) ? acc[j][4 * q + 0] : 0.0f, inv_p, lam);
+                primal_step(xv.y, zv.y, tv.y, (k + 4 * q + 1 < kb) ? acc[j][4 * q + 1] : 0.0f, inv_p, lam);
+                primal_step(xv.z, zv.z, tv.z, (k + 4 * q + 2 < kb) ? acc[j][4 * q + 2] : 0.0f, inv_p, lam);
+                primal_step(xv.w, zv.w, tv.w, (k + 4 * q + 3 < kb) ? acc[j][4 * q + 3] : 0.0f, inv_p, lam);
+                *xp = xv;
+                *zp = zv;
+                xn[4 * q] = xv.x; xn[4 * q + 1] = xv.y; xn[4 * q + 2] = xv.z; xn[4 * q + 3] = xv.w;
+            }
+            if (xb) st8(xb + o, xn);
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------------------------ batch helpers
 // Element-wise on channel-fastest batches (npix, kstride) whose channels kb .. kstride-1 are padding:
 // mode 0: x = 1 inside the support on live channels, else 0 (support_ones); mode 1: x = 0 outside the support, on
@@ -624,12 +742,28 @@ static int allow_smem(Kernel kernel, size_t bytes)
     return DFX_OK;
 }
 
+// the whole-image SIMT backprojection runs four pixels per warp (radon_backward_q4; dfx_radon_backward_quads)
+static bool backward_quads = true;
+
 template <int KERNEL, int MODE, typename ST>
 static int launch_backward(const ST *sino, int64_t sld, float *img, const float *geo, int n_angles, int nx, int ny,
                            int n_det, int kstride, int kb, int n_taps, float *z, const float *T, float inv_p, float lam,
                            __nv_bfloat16 *xb, void *stream, const int32_t *plist = nullptr, int64_t n_list = 0)
 {
     const int64_t npix = plist ? n_list : (int64_t)nx * ny;
+    if (!plist && backward_quads) {
+        // four neighbouring pixels per warp share their bin loads (radon_backward_q4)
+        dim3 grid((unsigned)cdiv(npix, 4 * WARPS), (unsigned)cdiv(kstride, CPW));
+        DFX_REQUIRE(grid.x < 2147483647u && grid.y <= 65535u, "radon: batch too large for one launch");
+        const size_t smem = sizeof(AngleParams) * (size_t)(n_angles > 0 ? n_angles : 1);
+        DFX_REQUIRE(smem <= 200 * 1024, "radon: %d angles exceed the shared memory of one launch", n_angles);
+        int st = allow_smem(radon_backward_q4<KERNEL, MODE, ST>, smem);
+        if (st) return st;
+        radon_backward_q4<KERNEL, MODE, ST><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
+            sino, sld, img, reinterpret_cast<const float4 *>(geo), n_angles, nx, (int)npix, n_det, kstride, kb, n_taps,
+            z, T, inv_p, lam, xb);
+        return launch_status(MODE ? "radon_backward_spdhg" : "radon_backward");
+    }
     // two channel groups per warp once the batch has more than one (fewer, longer warps: the taps of a pixel are
     // evaluated once for 16 channels per lane)
     const bool pair = kstride > CPW;
@@ -814,6 +948,13 @@ extern "C" int dfx_radon_table_fill(const float *geo, int n_angles, int nx, int 
         ray_table_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
             reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, nullptr, row_ptr, e);
     return launch_status("radon_table_fill");
+}
+
+extern "C" int dfx_radon_backward_quads(int on)
+{
+    const int was = backward_quads ? 1 : 0;
+    if (on >= 0) backward_quads = on != 0;
+    return was;
 }
 
 extern "C" int dfx_radon_gtable_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,

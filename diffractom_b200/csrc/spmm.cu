@@ -165,7 +165,51 @@ __global__ void __launch_bounds__(AJ_ROWS) spmm_adjoint8_kernel(
 #pragma unroll
     for (int t = 0; t < AJ_TY; ++t) acc[t] = 0.0f;
     const int64_t line0 = (int64_t)r * my + y0;
-    for (int c0 = 0; c0 < cp; c0 += chunk) {
+    if (chunk == cp) {
+        // the whole row in one pass: entries loaded four at a time (8-byte columns, 16-byte values) once the row
+        // position is a multiple of four, the same entries in the same order as the general loop below
+        for (int idx = threadIdx.x; idx < AJ_TY * cp; idx += blockDim.x) {
+            const int t = idx / cp, c = idx - t * cp;
+            tile[((t >> 2) * cp + c) * 4 + (t & 3)] = t < ny ? __ldg(data + (line0 + t) * cp + c) : 0.0f;
+        }
+        __syncthreads();
+        const bool vec = ((reinterpret_cast<uintptr_t>(col_j) & 7) == 0) &&
+                         ((reinterpret_cast<uintptr_t>(val) & 15) == 0);
+        auto apply = [&](int c, float v) {
+            const float4 z0 = tile4[c], z1 = tile4[cp + c];
+            acc[0] = __fmaf_rn(v, z0.x, acc[0]);
+            acc[1] = __fmaf_rn(v, z0.y, acc[1]);
+            acc[2] = __fmaf_rn(v, z0.z, acc[2]);
+            acc[3] = __fmaf_rn(v, z0.w, acc[3]);
+            acc[4] = __fmaf_rn(v, z1.x, acc[4]);
+            acc[5] = __fmaf_rn(v, z1.y, acc[5]);
+            acc[6] = __fmaf_rn(v, z1.z, acc[6]);
+            acc[7] = __fmaf_rn(v, z1.w, acc[7]);
+        };
+        if (vec) {
+            for (; i < e && (i & 3); ++i) apply(__ldg(col_j + i), __ldg(val + i));
+            if (i + 4 <= e) {
+                uint2 cc = __ldg(reinterpret_cast<const uint2 *>(col_j + i));
+                float4 vv = __ldg(reinterpret_cast<const float4 *>(val + i));
+                for (; i + 4 <= e; i += 4) {
+                    uint2 cn_ = cc;
+                    float4 vn_ = vv;
+                    if (i + 8 <= e) {              // the next four in flight while these are applied
+                        cn_ = __ldg(reinterpret_cast<const uint2 *>(col_j + i + 4));
+                        vn_ = __ldg(reinterpret_cast<const float4 *>(val + i + 4));
+                    }
+                    apply((int)(cc.x & 0xffffu), vv.x);
+                    apply((int)(cc.x >> 16), vv.y);
+                    apply((int)(cc.y & 0xffffu), vv.z);
+                    apply((int)(cc.y >> 16), vv.w);
+                    cc = cn_;
+                    vv = vn_;
+                }
+            }
+        }
+        for (; i < e; ++i) apply(__ldg(col_j + i), __ldg(val + i));
+    }
+    for (int c0 = 0; c0 < cp && chunk < cp; c0 += chunk) {
         const int cn = min(chunk, cp - c0);
         if (c0) __syncthreads();
         for (int idx = threadIdx.x; idx < AJ_TY * cn; idx += blockDim.x) {

@@ -77,6 +77,11 @@ int dfx_radon_backward_pixels(const float *sino_k, float *img_k, const float *ge
 int dfx_radon_backward_spdhg(const float *sino_k, const float *geo, int n_angles, int nx, int ny, int n_det,
                              int kstride, int kb, int kernel, int n_taps, float *x_k, float *z_k, const float *T_k,
                              float inv_p, float lam, void *stream);
+/* The whole-image SIMT backprojections above (float32 and BF16 sinograms, plain and with the primal step) run four
+ * neighbouring pixels per warp, loading each bin row of the union of their taps once (on: 1, the default), or one
+ * pixel per warp (0); the sums are the same bits either way. Returns the previous setting; on < 0 only queries it.
+ * No reference counterpart (a performance switch of this library, process-wide). */
+int dfx_radon_backward_quads(int on);
 
 /* The three Radon entry points above for the BF16 precision path: the sinogram is BF16 with sino_ld elements between
  * consecutive bins (sino_ld >= kstride, a multiple of 8: the batches of all orientations side by side, the layout of

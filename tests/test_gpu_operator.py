@@ -226,6 +226,50 @@ def test_ray_table_forward_equals_footprint_forward(golden, name):
     assert torch.equal(grouped(imgs, om, ray[3]), t)
 
 
+@pytest.mark.parametrize("name", ["ti8_small", "diff_midpoint_hat", "al5_small"])
+def test_four_pixel_backprojection_equals_one_pixel_per_warp(golden, name):
+    """The SIMT backprojections with four neighbouring pixels per warp (shared bin loads) give the one-pixel-per-warp
+    kernel's bits: plain and with the SPDHG primal step (x, z, the BF16 copy of x), float32 and BF16 sinograms, a
+    subset's angles, padding channels."""
+    from diffractom_b200 import _lib
+    d = golden(name)
+    op = make_operator(d)
+    rng = np.random.default_rng(6)
+    R, ns, ks, kb = op.N_Omega, op.My, op.Kstride, op.batches[0]["K_batch"] - 1
+    s = op._s()
+    sino = torch.as_tensor(rng.standard_normal((R, ns, ks)).astype(np.float32), device="cuda")
+    sb = sino.to(torch.bfloat16)
+    x0 = torch.as_tensor(rng.random((op.npix, ks)).astype(np.float32), device="cuda")
+    z0 = torch.as_tensor(rng.standard_normal((op.npix, ks)).astype(np.float32), device="cuda")
+    T = torch.as_tensor(rng.random((op.npix, ks)).astype(np.float32), device="cuda")
+    T[:, kb:] = 0
+    geo, n = op.geo_gpu[1::3].contiguous(), len(range(1, R, 3))
+    args = (op.Nx, op.Ny, ns, ks, kb, op._kernel_id, int(op.radon_geo.n_taps))
+    outs = []
+    prev = _lib.lib().dfx_radon_backward_quads(-1)
+    try:
+        for quads in (0, 1):
+            _lib.lib().dfx_radon_backward_quads(quads)
+            img = torch.empty((op.npix, ks), device="cuda")
+            _lib.call("dfx_radon_backward", sino.data_ptr(), img.data_ptr(), geo.data_ptr(), n, *args, s)
+            imgb = torch.empty((op.npix, ks), device="cuda")
+            _lib.call("dfx_radon_backward_bf16", sb.data_ptr(), ks, imgb.data_ptr(), geo.data_ptr(), n, *args, s)
+            x, z = x0.clone(), z0.clone()
+            _lib.call("dfx_radon_backward_spdhg", sino.data_ptr(), geo.data_ptr(), n, *args, x.data_ptr(),
+                      z.data_ptr(), T.data_ptr(), 3.0, 0.1, s)
+            xb_, zb_ = x0.clone(), z0.clone()
+            xc = torch.zeros((op.npix, ks), dtype=torch.bfloat16, device="cuda")
+            _lib.call("dfx_radon_backward_spdhg_bf16", sb.data_ptr(), ks, geo.data_ptr(), n, *args, xb_.data_ptr(),
+                      zb_.data_ptr(), T.data_ptr(), 3.0, 0.1, xc.data_ptr(), s)
+            torch.cuda.synchronize()
+            outs.append((img, imgb, x, z, xb_, zb_, xc))
+    finally:
+        _lib.lib().dfx_radon_backward_quads(prev)
+    for a, b in zip(*outs):
+        assert torch.equal(a, b)
+    assert not outs[0][0][:, kb:].any()
+
+
 def test_operator_on_its_own_queue_equals_current_stream(golden):
     """An operator built with queue=<a stream that is not current> gives the bits of one on the current stream: its
     build, forward, adjoint (device and NumPy) and an SPDHG run order themselves against the caller's stream."""
