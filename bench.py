@@ -497,7 +497,7 @@ def timed_epochs(op, w, b, a, precision, dist, local, world, shards=None, diagno
     x0 = torch.zeros(op.coeff_shape, dtype=torch.float32, device=op.device)
     sp._setup(x0, b)
     interval = 1 if diagnostics else 1 << 30
-    sp._iterate(a.warmup, diagnostics_interval=interval, final=False)
+    sp._iterate(a.warmup, diagnostics_interval=interval, final=False, async_diagnostics=True)
     stream = op.stream()
     timers = KernelTimers(op)
     stream.synchronize()
@@ -508,7 +508,7 @@ def timed_epochs(op, w, b, a, precision, dist, local, world, shards=None, diagno
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
     timers.on()
-    sp._iterate(a.steps, diagnostics_interval=interval, final=False)
+    sp._iterate(a.steps, diagnostics_interval=interval, final=False, async_diagnostics=True)
     timers.off()
     end.record(stream)
     end.synchronize()

@@ -73,6 +73,13 @@ class Reducer:
                   scr.data_ptr(), nb, self.op._s())
         return float(self.out[0].item())
 
+    def deviance_into(self, out, mu, b, w, pw, g, pg, bg, pbg, eps):
+        """deviance() written to the float64 device tensor out[0] on the operator's stream (no host read); out has
+        room for the kernel's 4 values."""
+        scr, nb = self._scr(mu.numel())
+        _lib.call("dfx_poisson_value_grad", mu.data_ptr(), b.data_ptr(), _p(w), pw, _p(g), pg, _p(bg), pbg,
+                  float(eps), 0, 0, 1.0, mu.numel(), out.data_ptr(), scr.data_ptr(), nb, self.op._s())
+
     def mean_counted(self, a, w, pw):
         scr, nb = self._scr(a.numel())
         _lib.call("dfx_mean_counted", a.data_ptr(), _p(w), pw, a.numel(), self.out.data_ptr(), scr.data_ptr(), nb,

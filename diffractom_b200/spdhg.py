@@ -68,6 +68,12 @@ class SPDHGPoisson:
     # its own kernel). "auto" (resident="auto" only): when x and z fit in float32 and T then fits in BF16 but not in
     # float32, instead of streaming T from host memory in every iteration; True: always with such an operator.
     bf16_T = "auto"
+    # With an operator of precision "bf16" (native projector) and float32 diagnostics, the residual of a diagnostics
+    # epoch (the float32 forward A x of the epoch's last x and its float64 deviance) runs on a side stream from a copy
+    # of x while the next epoch's iterations go on; the next subset's rows then come from the BF16 forward like every
+    # other iteration's. The objective is read when the run ends (or the next time it is needed). Off: the residual
+    # runs in line and its rows serve the next subset. Not with callbacks, printing, TV, shards or streamed state.
+    overlap_residual = True
 
     def __init__(self, operator, subsets=8, prox_kind="nonneg", lam=0.0, support="fov", eps_counts=1e-3, rho="auto",
                  seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None, shards=None):
@@ -118,6 +124,8 @@ class SPDHGPoisson:
         self.shards = shards
         self.state = None
         self._t16 = False
+        self._side = None
+        self._pending = []
 
     # ---------------------------------------------------------------- schedule
     def _epoch_order(self):
@@ -288,7 +296,7 @@ class SPDHGPoisson:
         if self.tv_tree is not None:
             raise NotImplementedError("tv_tree needs an operator with the local coefficient layout")
         self._setup(x0, b, weights, gain, background, state)
-        self._iterate(n_epochs, verbose, diagnostics_interval, callback, defer_final=True)
+        self._iterate(n_epochs, verbose, diagnostics_interval, callback, defer_final=True, async_diagnostics=True)
         return self._finish()
 
     def _setup_data(self, b, weights, gain, background):
@@ -706,7 +714,8 @@ class SPDHGPoisson:
             self._pass(None, self._seq[0])
 
     @on_op_stream
-    def _iterate(self, n_epochs, verbose=0, diagnostics_interval=1, callback=None, final=True, defer_final=False):
+    def _iterate(self, n_epochs, verbose=0, diagnostics_interval=1, callback=None, final=True, defer_final=False,
+                 async_diagnostics=False):
         """n_epochs epochs (spdhg_poisson.py:664-719). final=False: the last of them is not the run's last (no
         closing full forward unless diagnostics fall there), so that epochs can be run in several calls.
         defer_final (run()): the closing full forward and the objective of the run's last epoch are left to _finish,
@@ -718,6 +727,10 @@ class SPDHGPoisson:
         # with the state's downloads (nobody reads the objective before: no callback, no printing)
         defer = (defer_final and final and callback is None and not verbose and self.tv == 0 and self.X.resident
                  and self.Z.resident and self._stage is None)
+        overlap = (async_diagnostics and self.overlap_residual and callback is None and not verbose
+                   and op.precision == "bf16"
+                   and op.projector != "fft" and not self.bf16_diagnostics and self.tv == 0 and self.shards is None
+                   and self._stage is None and not self._graphs_on())
         for e in range(n_epochs):
             ep = self._ep0 + len(self.iter_stats) + 1
             last = final and e + 1 == n_epochs
@@ -736,6 +749,14 @@ class SPDHGPoisson:
                 tvb = adj is None
                 m_next = nb if nb is not None and nb >= 0 else None
                 full = (end_of_epoch and want_f) or nb is None or (m_next is not None and m_next == adj)
+                if overlap and full and end_of_epoch and want_f and m_next is not None and m_next != adj:
+                    # this epoch's residual on the side stream; the next subset's rows by the usual pass
+                    if adj is not None:
+                        self._dual(adj)
+                    op.zero_subset_rows(self.D, m_next)
+                    self._pass(adj, m_next, tv=tvb)
+                    self._residual_async(len(self.iter_stats))
+                    continue
                 graphed = not full and not tvb and m_next is not None and self._graphs_on()
                 if adj is not None and not graphed:
                     self._dual(adj)
@@ -763,7 +784,8 @@ class SPDHGPoisson:
             self._seq = seq
             if callback is not None or verbose:
                 op.stream().synchronize()
-            stats = {"epoch": ep, "f": self._f if want_f else None, "rho": self.rho_used,
+            async_f = overlap and want_f and self._pending and self._pending[-1][0] == len(self.iter_stats)
+            stats = {"epoch": ep, "f": None if async_f or not want_f else self._f, "rho": self.rho_used,
                      "time": time.perf_counter() - self._t_start}
             self.iter_stats.append(stats)
             stop = False
@@ -775,6 +797,56 @@ class SPDHGPoisson:
                       flush=True)
             if stop:
                 break
+        if self._pending:                   # the caller's next work (and its timing) comes after the residuals
+            op.stream().wait_event(self._pending[-1][2])
+
+    def _residual_async(self, index):
+        """The residual of the current x on the side stream: x copied on the operator's stream (the next update writes
+        x), then the float32 full forward of the copy into a separate data buffer and its float64 deviance, with the
+        side stream's own batch sinogram and scratch; iter_stats[index]["f"] is filled in by _resolve_pending."""
+        op = self.op
+        main = op.stream()
+        if self._side is None:
+            self._side = torch.cuda.Stream(op.device)
+            self._x_snap = torch.empty_like(self.X.dev)
+            self._D_diag = torch.empty_like(self.D)
+            self._side_sino = torch.empty_like(op.coeffs_sino_C)
+            self._side_scratch = torch.empty(0, dtype=torch.uint8, device=op.device)
+        if self._pending:                   # the previous residual has read its copy of x
+            main.wait_event(self._pending[-1][2])
+        with torch.cuda.stream(main):
+            self._x_snap.copy_(self.X.dev)
+        ev = torch.cuda.Event()
+        ev.record(main)
+        self._side.wait_event(ev)
+        out = torch.empty(4, dtype=torch.float64, device=op.device)
+        saved = (op.queue, op.coeffs_sino_C, op._scratch)
+        op.queue, op.coeffs_sino_C, op._scratch = self._side, self._side_sino, self._side_scratch
+        try:
+            be = op.batch_elems()
+            op._fill(self._D_diag, 0.0)
+            for ib in range(len(op.batches)):
+                op._direct_batch_k(self._x_snap.data_ptr() + 4 * ib * be, ib, self._D_diag, ray=self._ray)
+            self.red.deviance_into(out, self._D_diag, self.b, self.w, self.pw, self.g, self.pg, self.bg, self.pbg,
+                                   self.eps_counts)
+        finally:
+            self._side_scratch = op._scratch
+            op.queue, op.coeffs_sino_C, op._scratch = saved
+        done = torch.cuda.Event()
+        done.record(self._side)
+        self._pending.append((index, out, done))
+
+    def _resolve_pending(self):
+        """Reads the objectives of the residuals run on the side stream into iter_stats (and into the current
+        objective when it is the latest epoch's)."""
+        for index, out, done in self._pending:
+            done.synchronize()
+            f = float(out[0].item())
+            if index < len(self.iter_stats):
+                self.iter_stats[index]["f"] = f
+            if index == len(self.iter_stats) - 1:
+                self._f = f
+        self._pending = []
 
     def _graphs_on(self):
         op = self.op
@@ -844,6 +916,7 @@ class SPDHGPoisson:
     @on_op_stream
     def _finish(self):
         op = self.op
+        self._resolve_pending()
         if self._final_pending:
             # the closing full forward (writes D only, reads x) and the objective on the operator's stream; x, z and y
             # (final since the last update) converted and downloaded on a side stream meanwhile
@@ -908,6 +981,7 @@ class SPDHGPoisson:
         self.X = self.Z = self.T = self.dzk = self.xkb = self._stage = self._ray = self._tiles = None
         self.QX = self.QY = self.dqx = self.dqy = None
         self._graphs = {}
+        self._side = self._x_snap = self._D_diag = self._side_sino = self._side_scratch = None
         self.x = None
         return out
 

@@ -1,6 +1,7 @@
 """The BF16 tensor-core precision path of the operator and of SPDHGPoisson against the float64 oracle: operator
 values within the BF16 bound, subset rows, angle-chunked products, and the SPDHG deviance within 1e-3 relative of
-the float64 run of the same loop (same subsets, schedule and step sizes)."""
+the float64 run of the same loop (same subsets, schedule and step sizes); the side-stream residual against the
+in-line one."""
 import numpy as np
 import pytest
 
@@ -95,6 +96,33 @@ def test_bf16_spdhg_deviance_within_1e3_of_float64(golden):
     coef_err = float(np.linalg.norm(x - xr) / np.linalg.norm(xr))
     assert dev_err <= DEV_TOL, (dev_err, coef_err)
     assert coef_err < 5e-2, coef_err
+
+
+def test_side_stream_residual_matches_the_inline_one(golden):
+    """The residual of every diagnostics epoch run on a side stream from a copy of x (SPDHGPoisson.overlap_residual,
+    run()'s default with a BF16 operator): every epoch's objective is filled in, and the objectives and the final x
+    agree with those of the in-line residual, whose rows also serve the next subset (where the BF16 forward's rows do
+    otherwise), to 1e-4 and 1e-3."""
+    from diffractom_b200 import SPDHGPoisson
+    d = golden("al5_small")
+    op = make_operator(d, precision="bf16")
+    assert len(op.batches) > 2
+    rng = np.random.default_rng(12)
+    x_true = (rng.random(op.coeff_shape) * (rng.random(op.coeff_shape) < 0.2) * op.support_mask()[None]
+              ).astype(np.float32)
+    op.precision = "fp32"
+    b = rng.poisson(op.direct(x_true) * 50).astype(np.float32)
+    op.precision = "bf16"
+    out = {}
+    for overlap in (False, True):
+        sp = SPDHGPoisson(op, subsets=3, seed=1)
+        sp.overlap_residual = overlap
+        x = sp.run(np.zeros(op.coeff_shape, np.float32), b, 5, diagnostics_interval=1)
+        out[overlap] = (x, [st["f"] for st in sp.iter_stats], sp.final_stats["final_f"])
+    (x0, f0, l0), (x1, f1, l1) = out[False], out[True]
+    assert all(f is not None for f in f1) and l1 == f1[-1]
+    np.testing.assert_allclose(f1, f0, rtol=1e-4)
+    assert np.linalg.norm(x1 - x0) <= 1e-3 * np.linalg.norm(x0)
 
 
 def _tc_vs_simt(geo, R, nx, ny, ns, kb, kernel_id, n_taps, seed=8):
