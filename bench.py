@@ -827,13 +827,18 @@ def ni512_run(steps, warmup, K=None):
                                     precision="bf16", bf16_pf="generated", pf_mode="generated")
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t0
+    gib = lambda: round(torch.cuda.memory_allocated(op.device) / 1024 ** 3, 1)
+    mem = {"operator": gib()}
     b = counts_batched(op, w["grains"], w["mean_counts"])
+    torch.cuda.empty_cache()
+    mem["counts"] = gib()
     sp = SPDHGPoisson(op, subsets=w["subsets"], seed=0, resident="auto")
     x0 = np.zeros(op.coeff_shape, np.float32)
     t0 = time.perf_counter()
     sp._setup(x0, b)
     op.stream().synchronize()
     t_setup = time.perf_counter() - t0
+    mem["setup"] = gib()
     sp._iterate(warmup, diagnostics_interval=1, final=False)
     stream = op.stream()
     stream.synchronize()
@@ -851,7 +856,7 @@ def ni512_run(steps, warmup, K=None):
     clk = clocks.stop()
     ms = start.elapsed_time(end)
     f = [st["f"] for st in sp.iter_stats]
-    mem = torch.cuda.max_memory_allocated(op.device)
+    peak = torch.cuda.max_memory_allocated(op.device)
     roof = timers.roofline(op)
     return {"metric": "SPDHG epochs/s (large tailored-grid slice, Fourier-slice projector, BF16 contraction)",
             "value": steps / (ms / 1e3), "unit": "epochs/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
@@ -866,7 +871,7 @@ def ni512_run(steps, warmup, K=None):
                        "resident": sp.resident_used, "T_bf16": sp._t16,
                        "streamed": [n for n in ("x", "z", "T") if n not in sp.resident_used],
                        "operator_build_s": round(t_build, 1), "setup_s": round(t_setup, 1),
-                       "deviance_f64_per_epoch": f, "max_device_gb": round(mem / 1024 ** 3, 1),
+                       "deviance_f64_per_epoch": f, "device_gib": {**mem, "max": round(peak / 1024 ** 3, 1)},
                        "epoch": "36 subset iterations + the float32 residual and float64 deviance every epoch",
                        "l2": "inputs larger than L2, no flush"},
             "roofline": roof, "gpu_launches": int(launches), "clocks": clk}

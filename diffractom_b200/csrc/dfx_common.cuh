@@ -18,6 +18,22 @@ int launch_status(const char *what);
 
 inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Allows a kernel the device's whole opt-in shared memory (less its static shared memory) as dynamic shared memory.
+// The same value on every call, so that host threads launching the kernel with different sizes concurrently (the
+// serving loop) never lower the limit under another thread's launch; occupancy follows each launch's actual size.
+template <typename Kernel>
+inline cudaError_t allow_max_dynamic_smem(Kernel kernel)
+{
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    int dev = 0, optin = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
 #define DFX_REQUIRE(cond, ...)                  \
     do {                                        \
         if (!(cond)) {                          \

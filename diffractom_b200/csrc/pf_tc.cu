@@ -244,8 +244,7 @@ template <int DIR>
 int launch(const CUtensorMap &ma, const CUtensorMap &mb, TcArgs a, int m_tiles, cudaStream_t stream)
 {
     const size_t smem = smem_bytes(a.nt, a.stages);
-    const cudaError_t e = cudaFuncSetAttribute(pf_tc_kernel<DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)smem);
+    const cudaError_t e = allow_max_dynamic_smem(pf_tc_kernel<DIR>);
     if (e != cudaSuccess) {
         set_error("pf_tc: shared memory attribute: %s", cudaGetErrorString(e));
         return DFX_ELAUNCH;

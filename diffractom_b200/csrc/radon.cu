@@ -734,7 +734,7 @@ template <typename Kernel>
 static int allow_smem(Kernel kernel, size_t bytes)
 {
     if (bytes <= 48 * 1024) return DFX_OK;
-    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    const cudaError_t e = allow_max_dynamic_smem(kernel);
     if (e != cudaSuccess) {
         set_error("radon: %zu bytes of shared memory: %s", bytes, cudaGetErrorString(e));
         return DFX_ECUDA;

@@ -467,11 +467,11 @@ extern "C" int dfx_radon_backward_spdhg_tc(const void *sino_bf16, int64_t sino_l
     const dim3 grid((unsigned)(n_tiles < sms ? n_tiles : sms));
     cudaError_t e;
     if (kernel == 1) {
-        e = cudaFuncSetAttribute(tc_backproject_spdhg<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = allow_max_dynamic_smem(tc_backproject_spdhg<1>);
         if (e == cudaSuccess)
             tc_backproject_spdhg<1><<<grid, TP_THREADS, smem, (cudaStream_t)stream>>>(zmap, (const float4 *)geo, a);
     } else {
-        e = cudaFuncSetAttribute(tc_backproject_spdhg<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = allow_max_dynamic_smem(tc_backproject_spdhg<0>);
         if (e == cudaSuccess)
             tc_backproject_spdhg<0><<<grid, TP_THREADS, smem, (cudaStream_t)stream>>>(zmap, (const float4 *)geo, a);
     }

@@ -373,6 +373,9 @@ __global__ void __launch_bounds__(TW_THREADS, 1) tc_forward_tab(const __grid_con
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * TW_STAGES + 1);
     int *n_issued = reinterpret_cast<int *>(tmem_slot + 1), *n_used = n_issued + 1;
     volatile int *abort = n_issued + 2;
+    // the launch's tile sequence and each tile's window start, read from global memory once per CTA (the MMA
+    // issuer would otherwise wait for a global load before every tile's MMAs)
+    int32_t *s_tile = reinterpret_cast<int32_t *>(n_issued + 4), *s_win = s_tile + p.n_tiles;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int a = blockIdx.x, k0 = blockIdx.y * TF_CH;
@@ -411,6 +414,12 @@ __global__ void __launch_bounds__(TW_THREADS, 1) tc_forward_tab(const __grid_con
     const int n_tiles = p.n_tiles;
     const uint8_t *wrow = q.weights + (int64_t)arow * q.n_tiles_img * TW_W_BYTES;
     const int32_t *winrow = q.windows + (int64_t)arow * q.n_tiles_img;
+    for (int i = tid; i < n_tiles; i += TW_THREADS) {
+        const int t = p.tiles ? __ldg(p.tiles + i) : i;
+        s_tile[i] = t;
+        s_win[i] = __ldg(winrow + t);
+    }
+    __syncthreads();
     if (warp == 0) {
         // ---- producer: image tile (TMA) and its weight tiles (bulk copy), up to TW_STAGES ahead of the MMAs
         if (lane == 0) {
@@ -419,7 +428,7 @@ __global__ void __launch_bounds__(TW_THREADS, 1) tc_forward_tab(const __grid_con
                 const int st = i % TW_STAGES;
                 if (i >= TW_STAGES && !wait_or_abort(empty0 + 8 * st, ((i - TW_STAGES) / TW_STAGES) & 1, abort))
                     break;
-                const int t = p.tiles ? __ldg(p.tiles + i) : i;
+                const int t = s_tile[i];
                 const int px0 = (t % p.tiles_x) * TF_T, py0 = (t / p.tiles_x) * TF_T;
                 const uint32_t fb = full0 + 8 * st, xs = smem_u32(smem + st * TW_STAGE_BYTES);
                 mbar_expect_tx(fb, (uint32_t)TW_STAGE_BYTES);
@@ -439,8 +448,7 @@ __global__ void __launch_bounds__(TW_THREADS, 1) tc_forward_tab(const __grid_con
                 if (!wait_or_abort(full0 + 8 * st, (i / TW_STAGES) & 1, abort)) break;
                 *n_used = i + 1;
                 tc_fence_after();
-                const int t = p.tiles ? __ldg(p.tiles + i) : i;
-                const uint32_t dcol = tmem + (uint32_t)__ldg(winrow + t);
+                const uint32_t dcol = tmem + (uint32_t)s_win[i];
                 const uint32_t xb = smem_u32(smem + st * TW_STAGE_BYTES);
                 const uint32_t hb = xb + TF_X_BYTES, lb = hb + TF_W_BYTES;
 #pragma unroll
@@ -497,7 +505,7 @@ __global__ void __launch_bounds__(TW_THREADS, 1) tc_forward_tab(const __grid_con
     }
 }
 
-size_t tw_smem_bytes() { return 1024 + (size_t)TW_STAGES * TW_STAGE_BYTES + 256; }
+size_t tw_smem_bytes(int n_tiles) { return 1024 + (size_t)TW_STAGES * TW_STAGE_BYTES + 256 + 8 * (size_t)n_tiles; }
 
 size_t tf_smem_bytes() { return 1024 + (size_t)TF_STAGES * TF_X_BYTES + (size_t)TF_WBUF * 2 * TF_W_BYTES + 256; }
 
@@ -600,8 +608,9 @@ extern "C" int dfx_radon_forward_tc_table(const void *img_bf16, void *sino, int6
     a.scale = scale;
     a.out_f32 = out_f32 ? 1 : 0;
     TwArgs q{reinterpret_cast<const uint8_t *>(weights), windows, angle_rows, tiles_img};
-    const size_t smem = tw_smem_bytes();
-    const cudaError_t e = cudaFuncSetAttribute(tc_forward_tab, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = tw_smem_bytes(a.n_tiles);
+    DFX_REQUIRE(smem <= 227 * 1024, "radon_forward_tc_table: %d tiles exceed the shared memory of one CTA", a.n_tiles);
+    const cudaError_t e = allow_max_dynamic_smem(tc_forward_tab);
     if (e != cudaSuccess) {
         set_error("radon_forward_tc_table: shared memory attribute: %s", cudaGetErrorString(e));
         return DFX_ELAUNCH;
@@ -654,11 +663,11 @@ extern "C" int dfx_radon_forward_tc(const void *img_bf16, void *sino, int64_t si
     const dim3 grid((unsigned)n_angles, (unsigned)cdiv(kstride, TF_CH));
     cudaError_t e;
     if (kernel == 1) {
-        e = cudaFuncSetAttribute(tc_forward<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = allow_max_dynamic_smem(tc_forward<1>);
         if (e == cudaSuccess)
             tc_forward<1><<<grid, TF_THREADS, smem, (cudaStream_t)stream>>>(xmap, (const float4 *)geo, n_taps, a);
     } else {
-        e = cudaFuncSetAttribute(tc_forward<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = allow_max_dynamic_smem(tc_forward<0>);
         if (e == cudaSuccess)
             tc_forward<0><<<grid, TF_THREADS, smem, (cudaStream_t)stream>>>(xmap, (const float4 *)geo, n_taps, a);
     }

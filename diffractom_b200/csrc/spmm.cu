@@ -429,8 +429,7 @@ extern "C" int dfx_spmm_pf_adjoint(const float *data, const int32_t *row_ptr, co
     DFX_REQUIRE(cdiv(my, AJ_TY) <= 65535, "spmm_adjoint: grid too large");
     const int chunk = cp < AJ_MAX_CHUNK ? cp : AJ_MAX_CHUNK;
     const size_t smem = (size_t)AJ_TY * chunk * sizeof(float);
-    const cudaError_t e = cudaFuncSetAttribute(spmm_adjoint8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)(AJ_TY * AJ_MAX_CHUNK * sizeof(float)));
+    const cudaError_t e = allow_max_dynamic_smem(spmm_adjoint8_kernel);
     if (e != cudaSuccess) {
         set_error("spmm_adjoint: shared memory attribute: %s", cudaGetErrorString(e));
         return DFX_ELAUNCH;

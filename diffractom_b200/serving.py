@@ -56,6 +56,7 @@ class Request:
     epochs: int = 0
     deviance: list = field(default_factory=list)
     timings: dict = field(default_factory=dict)   # build / setup / epochs / finish seconds of the worker
+    stage: str = "queued"        # queued, build, setup, epochs, finish, done (progress of a running request)
     result: Optional[np.ndarray] = None
     error: Optional[str] = None
 
@@ -189,6 +190,8 @@ class ReconstructionServer:
         ok = [r for r in self.done if r.error is None]
         parts = {k: float(np.sum([r.timings.get(k, 0.0) for r in ok])) for k in ("build", "setup", "epochs", "finish")}
         queued = [r.admitted - r.arrival for r in ok]
+        done_ids = {r.id for r in self.done}
+        pending = [r for r in self.requests.values() if r.id not in done_ids]
         return {"requests": int(lat.size), "p50_s": float(np.percentile(lat, 50)),
                 "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
                 "throughput_rps": float(lat.size / span) if span > 0 else None,
@@ -196,7 +199,8 @@ class ReconstructionServer:
                 "failed": int(sum(r.error is not None for r in self.done)),
                 "worker_s": {k: round(v, 1) for k, v in parts.items()},
                 "queued_s_p50": float(np.percentile(queued, 50)) if queued else None,
-                "makespan_s": float(span)}
+                "makespan_s": float(span),
+                "unfinished": [(r.id, r.stage, r.epochs) for r in pending][:16]}
 
     # ---------------------------------------------------------------- server side
     def _loop(self):
@@ -243,6 +247,7 @@ def run_request(req: Request, device, stream):
     from .operator import SinglePhaseForwardOperator
     from .spdhg import SPDHGPoisson
     t0 = time.perf_counter()
+    req.stage = "build"
     # SPDHG runs over omega subsets, which need a sparse PF mode: "auto" with the dense switch off (the sparse
     # matrix stored as far as memory allows, the rest generated in every call)
     op = SinglePhaseForwardOperator(req.cfg, req.material, req.grid, req.max_gb, normalized=True, ctx=device,
@@ -253,20 +258,25 @@ def run_request(req: Request, device, stream):
         sp = SPDHGPoisson(op, subsets=req.subsets, seed=req.seed)
         sp.use_graphs = req.graphs
         x0 = torch.zeros(op.coeff_shape, dtype=torch.float32, device=device)
+        req.stage = "setup"
         sp._setup(x0, req.counts)
         stream.synchronize()
         t2 = time.perf_counter()
         devs = []
+        req.stage = "epochs"
         for e in range(req.max_epochs):
             last = e + 1 == req.max_epochs
             sp._iterate(1, diagnostics_interval=1, final=last)
             devs.append(float(sp._f))
+            req.epochs = len(devs)
             if len(devs) > 1 and abs(devs[-2] - devs[-1]) <= req.tol * abs(devs[-1]):
                 break
         t3 = time.perf_counter()
+        req.stage = "finish"
         x = sp._finish()
         out = x.cpu().numpy()
         req.timings = {"build": t1 - t0, "setup": t2 - t1, "epochs": t3 - t2, "finish": time.perf_counter() - t3}
+        req.stage = "done"
         return out, len(devs), devs
     finally:
         op.free_memory()
