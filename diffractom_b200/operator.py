@@ -56,6 +56,9 @@ class SinglePhaseForwardOperator:
     # with both CSR copies stored, the forward products run over an eta-blocked copy of the forward CSR (four
     # neighbouring eta bins of a ring per entry; the same sums bit for bit); False: over the forward CSR itself
     forward_blocks = True
+    # the blocked forward with the lanes on detector lines (dfx_spmm_pf_forward_lines; the same bits); False: one
+    # block row per thread (dfx_spmm_pf_forward_blocked)
+    forward_lines = True
 
     def __init__(self, cfg: Mapping[str, Any], material, grid, max_gb: float, verbose: bool = False,
                  normalized: bool = False, ctx=None, queue=None, pf_mode: str = "auto", sparse_max_fill: float = 0.3,
@@ -514,7 +517,9 @@ class SinglePhaseForwardOperator:
         s = self._s()
         om_ptr = None if om is None else om.data_ptr()
         if sb.get("fb_ptr") is not None:
-            self._call("dfx_spmm_pf_forward_blocked", sino_ptr, sb["fb_ptr"].data_ptr(), sb["fb_k"].data_ptr(),
+            name = ("dfx_spmm_pf_forward_lines" if self.forward_lines and self.N_peaks <= 16
+                    else "dfx_spmm_pf_forward_blocked")
+            self._call(name, sino_ptr, sb["fb_ptr"].data_ptr(), sb["fb_k"].data_ptr(),
                        sb["fb_v"].data_ptr(), sb["fb_mask"].data_ptr(), data.data_ptr(), om_ptr, n_ang, self.My,
                        self.N_peaks, self.N_eta, self.Kstride, kb, s)
             return

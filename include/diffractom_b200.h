@@ -256,6 +256,12 @@ int dfx_pf_fblock_fill(const int32_t *row_ptr_f, const uint16_t *col_k, const fl
 int dfx_spmm_pf_forward_blocked(const float *sino, const int32_t *fb_ptr, const uint16_t *fb_k, const float *fb_v,
                                 const uint8_t *fb_mask, float *data, const int32_t *omegas, int n_sub, int my, int P,
                                 int C, int kstride, int kb, void *stream);
+/* dfx_spmm_pf_forward_blocked with the work laid out on detector lines (same arguments, same result bit for bit):
+ * a block owns one angle, 32 lines and 8 eta blocks of every ring, one warp per ring (P <= 16) walks its 8 block rows
+ * with the lanes on the lines, and the outputs are added to the data rows line by line through shared memory. */
+int dfx_spmm_pf_forward_lines(const float *sino, const int32_t *fb_ptr, const uint16_t *fb_k, const float *fb_v,
+                              const uint8_t *fb_mask, float *data, const int32_t *omegas, int n_sub, int my, int P,
+                              int C, int kstride, int kb, void *stream);
 
 /* replaces batched_gemm_clblast / batched_gemm_clblast_adj (SPFO:2063-2127), the products of pf_mode "dense": pf is
  * the batch's float32 PF (n_omega, kb, cp) (dfx_pf_dense); adjoint 0: out = data (n_omega, my, cp) += in (n_omega, my,

@@ -270,6 +270,33 @@ def test_four_pixel_backprojection_equals_one_pixel_per_warp(golden, name):
     assert not outs[0][0][:, kb:].any()
 
 
+@pytest.mark.parametrize("name", ["al5_small", "ti8_small"])
+def test_forward_pf_product_on_lines_equals_the_blocked_one(golden, name):
+    """dfx_spmm_pf_forward_lines (lanes on detector lines, outputs added line by line) adds the same bits to the data
+    rows as dfx_spmm_pf_forward_blocked (one block row per thread), for all angles and a subset's angle list."""
+    from diffractom_b200 import _lib
+    d = golden(name)
+    op = make_operator(d, pf_mode="sparse")
+    sb = op.sparse_batches[0]
+    assert sb.get("fb_ptr") is not None
+    rng = np.random.default_rng(8)
+    R, ns, ks, kb = op.N_Omega, op.My, op.Kstride, op.batches[0]["K_batch"]
+    sino = torch.as_tensor(rng.standard_normal((R, ns, ks)).astype(np.float32), device="cuda")
+    start = torch.as_tensor(rng.standard_normal(op.data_shape).astype(np.float32), device="cuda")
+    om = torch.arange(0, R, 4, dtype=torch.int32, device="cuda")
+    for rows, n in ((None, R), (om, om.numel())):
+        outs = []
+        for name_k in ("dfx_spmm_pf_forward_blocked", "dfx_spmm_pf_forward_lines"):
+            data = start.clone()
+            _lib.call(name_k, sino.data_ptr(), sb["fb_ptr"].data_ptr(), sb["fb_k"].data_ptr(), sb["fb_v"].data_ptr(),
+                      sb["fb_mask"].data_ptr(), data.data_ptr(), None if rows is None else rows.data_ptr(), n, ns,
+                      op.N_peaks, op.N_eta, ks, kb, op._s())
+            torch.cuda.synchronize()
+            outs.append(data)
+        assert torch.equal(outs[0], outs[1])
+        assert not torch.equal(outs[0], start)
+
+
 def test_operator_on_its_own_queue_equals_current_stream(golden):
     """An operator built with queue=<a stream that is not current> gives the bits of one on the current stream: its
     build, forward, adjoint (device and NumPy) and an SPDHG run order themselves against the caller's stream."""
