@@ -406,6 +406,91 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_gtable(
     }
 }
 
+// The grouped-table forward with four channels per lane (128 per warp): twice the warps of radon_forward_gtable, for
+// launches of few angles (an omega subset), which would leave the 8-channel kernel's last wave mostly empty. Same
+// entries, weights and order per channel, the same paired FMAs: the same bits.
+__device__ __forceinline__ void acc4(float (&a)[4], float w, const float4 &p)
+{
+    const float2 ww = make_float2(w, w);
+    float2 r0 = __ffma2_rn(ww, make_float2(p.x, p.y), make_float2(a[0], a[1]));
+    float2 r1 = __ffma2_rn(ww, make_float2(p.z, p.w), make_float2(a[2], a[3]));
+    a[0] = r0.x; a[1] = r0.y; a[2] = r1.x; a[3] = r1.y;
+}
+
+__global__ void __launch_bounds__(32 * WARPS) radon_forward_gtable4(
+    const float *__restrict__ img, float *__restrict__ sino, const int32_t *__restrict__ row_ptr,
+    const int32_t *__restrict__ pix, const float4 *__restrict__ wts, const int32_t *__restrict__ angles, int ns,
+    int kstride, int kb, float scale)
+{
+    constexpr int U = 4, C4 = 4, CW = 32 * C4;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ng = (ns + GB - 1) / GB;
+    const int grp = blockIdx.x * WARPS + warp;
+    const int al = blockIdx.y;
+    const int k = blockIdx.z * CW + lane * C4;
+    if (grp >= ng) return;
+    const bool live = k < kstride;
+    const int s0 = grp * GB;
+    float *out = sino + ((int64_t)al * ns + s0) * kstride + k;
+    const int nb = min(GB, ns - s0);
+    if (blockIdx.z * CW >= kb) {
+        if (live)
+            for (int j = 0; j < nb; ++j)
+                *reinterpret_cast<float4 *>(out + (int64_t)j * kstride) = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const bool load = k < kb;
+    const int a = angles ? __ldg(angles + al) : al;
+    const int64_t r = (int64_t)a * ng + grp;
+    int e = __ldg(row_ptr + r);
+    const int e1 = __ldg(row_ptr + r + 1);
+    const float *base = img + (load ? k : 0);
+    float acc[GB][C4];
+#pragma unroll
+    for (int j = 0; j < GB; ++j)
+#pragma unroll
+        for (int c = 0; c < C4; ++c) acc[j][c] = 0.0f;
+    for (; e + U <= e1; e += U) {
+        int p[U];
+        float4 w[U], q[U];
+#pragma unroll
+        for (int i = 0; i < U; ++i) {
+            p[i] = __ldg(pix + e + i);
+            w[i] = __ldg(wts + e + i);
+        }
+#pragma unroll
+        for (int i = 0; i < U; ++i)
+            q[i] = load ? __ldg(reinterpret_cast<const float4 *>(base + (int64_t)p[i] * kstride))
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < U; ++i) {
+            if (w[i].x != 0.0f) acc4(acc[0], w[i].x, q[i]);
+            if (w[i].y != 0.0f) acc4(acc[1], w[i].y, q[i]);
+            if (w[i].z != 0.0f) acc4(acc[2], w[i].z, q[i]);
+            if (w[i].w != 0.0f) acc4(acc[3], w[i].w, q[i]);
+        }
+    }
+    for (; e < e1; ++e) {
+        const int p = __ldg(pix + e);
+        const float4 w = __ldg(wts + e);
+        const float4 q = load ? __ldg(reinterpret_cast<const float4 *>(base + (int64_t)p * kstride))
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (w.x != 0.0f) acc4(acc[0], w.x, q);
+        if (w.y != 0.0f) acc4(acc[1], w.y, q);
+        if (w.z != 0.0f) acc4(acc[2], w.z, q);
+        if (w.w != 0.0f) acc4(acc[3], w.w, q);
+    }
+    if (!live) return;
+#pragma unroll
+    for (int j = 0; j < GB; ++j) {
+        if (j >= nb) break;
+        float o[C4];
+#pragma unroll
+        for (int c = 0; c < C4; ++c) o[c] = (k + c < kb) ? __fmul_rn(scale, acc[j][c]) : 0.0f;
+        *reinterpret_cast<float4 *>(out + (int64_t)j * kstride) = make_float4(o[0], o[1], o[2], o[3]);
+    }
+}
+
 // ------------------------------------------------------------------------------------------------ backward
 // SPDHG primal step of one coefficient: the operations of primal_update_kernel (solver.cu), bitwise
 __device__ __forceinline__ void primal_step(float &x, float &z, float t, float dz, float inv_p, float lam)
@@ -1005,6 +1090,16 @@ extern "C" int dfx_radon_forward_gtable(const float *img_k, float *sino_k, const
                 "radon_forward_gtable: kstride (%d) must be a positive multiple of %d and kb (%d) <= kstride",
                 kstride, CPL, kb);
     if (n_angles == 0) return DFX_OK;
+    // four channels per lane when eight would give fewer than about five waves of warps (few angles)
+    const int64_t warps8 = (int64_t)cdiv(n_det, GB) * n_angles * cdiv(kstride, CPW);
+    if (warps8 < 16384 && kstride % 4 == 0) {
+        DFX_REQUIRE(cdiv(kstride, 128) <= 65535, "radon_forward_gtable: kstride too large for one launch");
+        dim3 grid((unsigned)cdiv(cdiv(n_det, GB), WARPS), (unsigned)n_angles, (unsigned)cdiv(kstride, 128));
+        radon_forward_gtable4<<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
+            img_k, sino_k, row_ptr, pixels, reinterpret_cast<const float4 *>(weights), angles, n_det, kstride, kb,
+            scale);
+        return launch_status("radon_forward_gtable");
+    }
     dim3 grid((unsigned)cdiv(cdiv(n_det, GB), WARPS), (unsigned)n_angles, (unsigned)cdiv(kstride, CPW));
     radon_forward_gtable<<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
         img_k, sino_k, row_ptr, pixels, reinterpret_cast<const float4 *>(weights), angles, n_det, kstride, kb, scale);

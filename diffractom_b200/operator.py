@@ -36,7 +36,6 @@ AUTO_FFT_PIXELS = 400 * 400   # projector="auto": the Fourier-slice projector fo
 SPARSE_MIN_BATCHES = 4    # sparse modes: at least this many batches (SPFO:135)
 CAND_BYTES = 2 + 4 + 4 + 4 + 4          # per candidate / non-zero scratch of the reference's generator
 NNZ_BYTES = 2 + 4 + 4 + 2 + 4 + 2 + 4   # (pf_generate.py:29-30), used by the batch-size rule
-GTABLE_MIN_ANGLES = 64                   # float32 forward projections of this many angles read the grouped table
 KSTRIDE_ALIGN = 16                       # channel stride of the batch buffers (16 channels per tensor-memory load)
 
 
@@ -372,10 +371,6 @@ class SinglePhaseForwardOperator:
         om_ptr = None if om is None else om.data_ptr()
         rp, ent = (self._ray_rp, self._ray_ent) if ray is None else ray[:2]
         grp = self._ray_grp if ray is None else (ray[3] if len(ray) > 3 else None)
-        # the grouped table has a quarter of the warps: for a few angles (a subset) the per-bin one fills the GPU
-        # better (at 256 x 256, 1024 channels: 18 angles 0.57 vs 0.67 ms; 360 angles 8.6 ms grouped)
-        if grp is not None and n_ang < GTABLE_MIN_ANGLES:
-            grp = None
         if sld is None and grp is not None:
             self._call("dfx_radon_forward_gtable", src_ptr, dst_ptr, grp[0].data_ptr(), grp[1].data_ptr(),
                        grp[2].data_ptr(), om_ptr, n_ang, self.My, self.Kstride, kb, float(self.radon_geo.scale),

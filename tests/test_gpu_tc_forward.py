@@ -4,7 +4,7 @@ the image widened to float32, exactly): float32 outputs within 2e-5 of the large
 hat kernel, every angle of the golden geometries and of a 256 x 256, 360-angle scan; a tile list that skips the
 tiles outside a support equals the full projection of an image that is zero there; BF16 output rows in a wider
 sinogram; the weight-table variant gives the same bits; no tensor-core wait ran out and no tap left its window;
-BF16 SPDHG with and without it."""
+BF16 SPDHG with and without it; the float32 grouped-table forward of the same 360-angle scan."""
 import ctypes
 
 import numpy as np
@@ -99,6 +99,32 @@ def test_tc_forward_full_scan_support_tiles_and_bf16_rows():
     assert torch.equal(z[:, :, op.Kstride:2 * op.Kstride], tc.to(torch.bfloat16))
     assert not z[:, :, :op.Kstride].any() and not z[:, :, 2 * op.Kstride:].any()
     assert _flags(lib) == 0
+
+
+def test_grouped_table_forward_of_a_full_scan():
+    """The float32 forward through the grouped table (dfx_radon_forward_gtable) at 360 angles and 256 x 256 pixels,
+    where it runs eight channels per lane, and for a subset's 18 angles (four per lane): the per-bin table's bits."""
+    from diffractom_b200 import _lib
+    op = _ti256_operator()
+    assert op._ray_grp is not None
+    R, My, ks, s = op.N_Omega, op.My, op.Kstride, op._s()
+    kb = op.batches[0]["K_batch"]
+    g = torch.Generator(device="cuda").manual_seed(7)
+    img = torch.rand((op.npix, ks), generator=g, device="cuda")
+    img[:, kb:] = 0
+    om = torch.arange(3, R, 20, dtype=torch.int32, device="cuda")
+    for rows in (None, om):
+        n = R if rows is None else rows.numel()
+        rp = None if rows is None else rows.data_ptr()
+        a = torch.empty((n, My, ks), device="cuda")
+        b = torch.empty((n, My, ks), device="cuda")
+        _lib.call("dfx_radon_forward_table", img.data_ptr(), a.data_ptr(), op._ray_rp.data_ptr(),
+                  op._ray_ent.data_ptr(), rp, n, My, ks, kb, float(op.radon_geo.scale), s)
+        grp = op._ray_grp
+        _lib.call("dfx_radon_forward_gtable", img.data_ptr(), b.data_ptr(), grp[0].data_ptr(), grp[1].data_ptr(),
+                  grp[2].data_ptr(), rp, n, My, ks, kb, float(op.radon_geo.scale), s)
+        torch.cuda.synchronize()
+        assert torch.equal(a, b)
 
 
 @pytest.mark.parametrize("case", ["al5_small", "ti256"])
