@@ -55,6 +55,9 @@ SIGNATURES = {
     "dfx_radon_gtable_count": ([P, I, I, I, I, I, P, P, S], c_int),
     "dfx_radon_gtable_fill": ([P, I, I, I, I, I, P, P, P, P, S], c_int),
     "dfx_radon_forward_gtable": ([P, P, P, P, P, P, I, I, I, I, F, S], c_int),
+    "dfx_radon_ptable_count": ([P, I, I, I, I, I, P, P, S], c_int),
+    "dfx_radon_ptable_fill": ([P, I, I, I, I, I, P, P, P, P, S], c_int),
+    "dfx_radon_forward_ptable": ([P, P, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_radon_forward_table_bf16": ([P, P, L, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_radon_forward_table_bf16_bf16": ([P, P, L, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_batch_support": ([P, P, P, L, I, I, F, I, S], c_int),

@@ -406,6 +406,193 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_gtable(
     }
 }
 
+// ------------------------------------------------------------------------------------------------ paired table
+// For the forward of all angles, consecutive angles 2i and 2i + 1 share most pixels of a bin group (their rays differ
+// by half a degree): the paired table lists, per (angle pair, four bins), the pixels that reach one of the eight
+// (angle, bin) outputs with their eight weights, so a pixel's channels are loaded once for both angles. When the
+// two angles parametrise the image alike (rows along the same axis) the two angles' per-bin lists are merged in
+// their common (row, column) order; otherwise the first angle's entries come first, then the second's. Either way
+// each (angle, bin) sums its per-bin row's taps in that row's order: the per-bin forward's bits.
+template <int KERNEL>
+__device__ void pair_rows(const AngleGeo (&g)[2], const bool (&ok)[2], int which, int nx, int ny, int ns, int s0,
+                          const uint8_t *__restrict__ supp, int &n, int64_t &pos, int32_t *__restrict__ pix_out,
+                          float4 *__restrict__ w_out)
+{
+    // which: 0 = angle 0 only, 1 = angle 1 only, 2 = both (merged)
+    const AngleGeo &gr = g[which == 1 ? 1 : 0];
+    const int nu = gr.rows_are_y ? nx : ny, nv = gr.rows_are_y ? ny : nx;
+    float inv[2], half[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        inv[h] = __frcp_rn(g[h].A);
+        half[h] = KERNEL == 1 ? g[h].hw : 1.0f;
+    }
+    for (int v = 0; v < nv; ++v) {
+        float c[2];
+        int u0[2][GB], u1[2][GB];
+        int lo = nu, hi = -1;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const bool use = ok[h] && (which == 2 || which == h);
+            c[h] = __fmaf_rn(g[h].B, (float)v, g[h].T0);
+#pragma unroll
+            for (int j = 0; j < GB; ++j) {
+                u0[h][j] = 0;
+                u1[h][j] = -1;
+                if (!use || s0 + j >= ns) continue;
+                const float fs = (float)(s0 + j);
+                const float e1 = (fs - half[h] - c[h]) * inv[h], e2 = (fs + half[h] - c[h]) * inv[h];
+                u0[h][j] = max((int)floorf(fminf(e1, e2) - 1e-3f), 0);
+                u1[h][j] = min((int)ceilf(fmaxf(e1, e2) + 1e-3f), nu - 1);
+                if (u0[h][j] <= u1[h][j]) {
+                    lo = min(lo, u0[h][j]);
+                    hi = max(hi, u1[h][j]);
+                }
+            }
+        }
+        for (int u = lo; u <= hi; ++u) {
+            float w[2][GB];
+            bool any = false;
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int j = 0; j < GB; ++j) {
+                    w[h][j] = 0.0f;
+                    if (u < u0[h][j] || u > u1[h][j]) continue;
+                    const float d = __fsub_rn(__fmaf_rn(g[h].A, (float)u, c[h]), (float)(s0 + j));
+                    w[h][j] = tap_weight<KERNEL>(g[h], d);
+                    any |= w[h][j] != 0.0f;
+                }
+            if (!any) continue;
+            const int pix = gr.rows_are_y ? u + nx * v : v + nx * u;
+            if (supp && !supp[pix]) continue;
+            if (pix_out) {
+                pix_out[pos] = pix;
+                w_out[2 * pos] = make_float4(w[0][0], w[0][1], w[0][2], w[0][3]);
+                w_out[2 * pos + 1] = make_float4(w[1][0], w[1][1], w[1][2], w[1][3]);
+                ++pos;
+            }
+            ++n;
+        }
+    }
+}
+
+template <int KERNEL>
+__global__ void ray_ptable_kernel(const float4 *__restrict__ geo, int n_angles, int nx, int ny, int ns,
+                                  const uint8_t *__restrict__ supp, int32_t *__restrict__ counts,
+                                  const int32_t *__restrict__ row_ptr, int32_t *__restrict__ pix_out,
+                                  float4 *__restrict__ w_out)
+{
+    const int ng = (ns + GB - 1) / GB, npairs = (n_angles + 1) / 2;
+    const int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;      // pair * ng + g
+    if (row >= (int64_t)npairs * ng) return;
+    const int pr = (int)(row / ng), s0 = (int)(row % ng) * GB;
+    AngleGeo g[2];
+    bool ok[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int a = 2 * pr + h;
+        ok[h] = a < n_angles;
+        g[h] = load_geo(geo, ok[h] ? a : 2 * pr);
+    }
+    int n = 0;
+    int64_t pos = row_ptr ? row_ptr[row] : 0;
+    if (!ok[1] || g[0].rows_are_y == g[1].rows_are_y) {
+        pair_rows<KERNEL>(g, ok, 2, nx, ny, ns, s0, supp, n, pos, row_ptr ? pix_out : nullptr, w_out);
+    } else {
+        pair_rows<KERNEL>(g, ok, 0, nx, ny, ns, s0, supp, n, pos, row_ptr ? pix_out : nullptr, w_out);
+        pair_rows<KERNEL>(g, ok, 1, nx, ny, ns, s0, supp, n, pos, row_ptr ? pix_out : nullptr, w_out);
+    }
+    if (!row_ptr) counts[row] = n;
+}
+
+// Paired-table forward of all angles: warp per (angle pair, four bins, 256 channels), eight accumulators of 8
+// channels per lane, U pixels in flight, FMAs only for the non-zero weights (a branch the whole warp takes).
+__global__ void __launch_bounds__(32 * WARPS) radon_forward_ptable(
+    const float *__restrict__ img, float *__restrict__ sino, const int32_t *__restrict__ row_ptr,
+    const int32_t *__restrict__ pix, const float4 *__restrict__ wts, int n_angles, int ns, int kstride, int kb,
+    float scale)
+{
+    constexpr int U = 2;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ng = (ns + GB - 1) / GB;
+    const int grp = blockIdx.x * WARPS + warp;
+    const int pr = blockIdx.y;
+    const int k = blockIdx.z * CPW + lane * CPL;
+    if (grp >= ng) return;
+    const bool live = k < kstride;
+    const int s0 = grp * GB, nb = min(GB, ns - s0);
+    const int na = min(2, n_angles - 2 * pr);
+    if (blockIdx.z * CPW >= kb) {
+        const float zero[CPL] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (live)
+            for (int h = 0; h < na; ++h)
+                for (int j = 0; j < nb; ++j) st8(sino + ((int64_t)(2 * pr + h) * ns + s0 + j) * kstride + k, zero);
+        return;
+    }
+    const bool load = k < kb;
+    const int64_t r = (int64_t)pr * ng + grp;
+    int e = __ldg(row_ptr + r);
+    const int e1 = __ldg(row_ptr + r + 1);
+    const float *base = img + (load ? k : 0);
+    float acc[2][GB][CPL];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int j = 0; j < GB; ++j)
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) acc[h][j][c] = 0.0f;
+    auto apply = [&](const float4 &wa, const float4 &wb, const Raw8<float> &q) {
+        if (wa.x != 0.0f) accraw(acc[0][0], wa.x, q);
+        if (wa.y != 0.0f) accraw(acc[0][1], wa.y, q);
+        if (wa.z != 0.0f) accraw(acc[0][2], wa.z, q);
+        if (wa.w != 0.0f) accraw(acc[0][3], wa.w, q);
+        if (wb.x != 0.0f) accraw(acc[1][0], wb.x, q);
+        if (wb.y != 0.0f) accraw(acc[1][1], wb.y, q);
+        if (wb.z != 0.0f) accraw(acc[1][2], wb.z, q);
+        if (wb.w != 0.0f) accraw(acc[1][3], wb.w, q);
+    };
+    for (; e + U <= e1; e += U) {
+        int p[U];
+        float4 wa[U], wb[U];
+        Raw8<float> q[U];
+#pragma unroll
+        for (int i = 0; i < U; ++i) {
+            p[i] = __ldg(pix + e + i);
+            wa[i] = __ldg(wts + 2 * (e + i));
+            wb[i] = __ldg(wts + 2 * (e + i) + 1);
+        }
+#pragma unroll
+        for (int i = 0; i < U; ++i) {
+            zraw(q[i]);
+            if (load) ldraw(base + (int64_t)p[i] * kstride, q[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < U; ++i) apply(wa[i], wb[i], q[i]);
+    }
+    for (; e < e1; ++e) {
+        const int p = __ldg(pix + e);
+        const float4 wa = __ldg(wts + 2 * e), wb = __ldg(wts + 2 * e + 1);
+        Raw8<float> q;
+        zraw(q);
+        if (load) ldraw(base + (int64_t)p * kstride, q);
+        apply(wa, wb, q);
+    }
+    if (!live) return;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        if (h >= na) break;
+#pragma unroll
+        for (int j = 0; j < GB; ++j) {
+            if (j >= nb) break;
+            float o[CPL];
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) o[c] = (k + c < kb) ? __fmul_rn(scale, acc[h][j][c]) : 0.0f;
+            st8(sino + ((int64_t)(2 * pr + h) * ns + s0 + j) * kstride + k, o);
+        }
+    }
+}
+
 // The grouped-table forward with four channels per lane (128 per warp): twice the warps of radon_forward_gtable, for
 // launches of few angles (an omega subset), which would leave the 8-channel kernel's last wave mostly empty. Same
 // entries, weights and order per channel, the same paired FMAs: the same bits.
@@ -1076,6 +1263,61 @@ extern "C" int dfx_radon_gtable_fill(const float *geo, int n_angles, int nx, int
         ray_gtable_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
             reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, nullptr, row_ptr, pixels, w);
     return launch_status("radon_gtable_fill");
+}
+
+extern "C" int dfx_radon_ptable_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
+                                      const uint8_t *supp, int32_t *counts, void *stream)
+{
+    DFX_REQUIRE(geo && counts && ((uintptr_t)geo % 16) == 0, "radon_ptable: null or misaligned pointer");
+    DFX_REQUIRE(n_angles > 0 && nx > 0 && ny > 0 && n_det > 0 && (kernel == 0 || kernel == 1),
+                "radon_ptable: bad sizes or kernel");
+    const int64_t rows = (int64_t)cdiv(n_angles, 2) * cdiv(n_det, GB);
+    DFX_REQUIRE(cdiv(rows, 128) < 2147483647LL, "radon_ptable: too many rows");
+    if (kernel == 1)
+        ray_ptable_kernel<1><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, counts, nullptr, nullptr, nullptr);
+    else
+        ray_ptable_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, counts, nullptr, nullptr, nullptr);
+    return launch_status("radon_ptable_count");
+}
+
+extern "C" int dfx_radon_ptable_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
+                                     const uint8_t *supp, const int32_t *row_ptr, int32_t *pixels, float *weights,
+                                     void *stream)
+{
+    DFX_REQUIRE(geo && row_ptr && pixels && weights && ((uintptr_t)geo % 16) == 0 && ((uintptr_t)weights % 16) == 0,
+                "radon_ptable: null or misaligned pointer");
+    DFX_REQUIRE(n_angles > 0 && nx > 0 && ny > 0 && n_det > 0 && (kernel == 0 || kernel == 1),
+                "radon_ptable: bad sizes or kernel");
+    const int64_t rows = (int64_t)cdiv(n_angles, 2) * cdiv(n_det, GB);
+    float4 *w = reinterpret_cast<float4 *>(weights);
+    if (kernel == 1)
+        ray_ptable_kernel<1><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, nullptr, row_ptr, pixels, w);
+    else
+        ray_ptable_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
+            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, nullptr, row_ptr, pixels, w);
+    return launch_status("radon_ptable_fill");
+}
+
+extern "C" int dfx_radon_forward_ptable(const float *img_k, float *sino_k, const int32_t *row_ptr,
+                                        const int32_t *pixels, const float *weights, int n_angles, int n_det,
+                                        int kstride, int kb, float scale, void *stream)
+{
+    DFX_REQUIRE(img_k && sino_k && row_ptr && pixels && weights, "radon_forward_ptable: null pointer");
+    DFX_REQUIRE(((uintptr_t)img_k % 16) == 0 && ((uintptr_t)sino_k % 16) == 0 && ((uintptr_t)weights % 16) == 0,
+                "radon_forward_ptable: misaligned arrays");
+    DFX_REQUIRE(n_angles >= 0 && cdiv(n_angles, 2) <= 65535 && n_det > 0, "radon_forward_ptable: bad sizes");
+    DFX_REQUIRE(kstride > 0 && kstride % CPL == 0 && kb >= 0 && kb <= kstride && cdiv(kstride, CPW) <= 65535,
+                "radon_forward_ptable: kstride (%d) must be a positive multiple of %d and kb (%d) <= kstride",
+                kstride, CPL, kb);
+    if (n_angles == 0) return DFX_OK;
+    dim3 grid((unsigned)cdiv(cdiv(n_det, GB), WARPS), (unsigned)cdiv(n_angles, 2), (unsigned)cdiv(kstride, CPW));
+    radon_forward_ptable<<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
+        img_k, sino_k, row_ptr, pixels, reinterpret_cast<const float4 *>(weights), n_angles, n_det, kstride, kb,
+        scale);
+    return launch_status("radon_forward_ptable");
 }
 
 extern "C" int dfx_radon_forward_gtable(const float *img_k, float *sino_k, const int32_t *row_ptr,

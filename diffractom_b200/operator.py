@@ -156,12 +156,13 @@ class SinglePhaseForwardOperator:
             self._supp_tiles = {}
             self._fft = None
             if self.projector == "fft":
-                self._ray_rp = self._ray_ent = self._ray_grp = None
+                self._ray_rp = self._ray_ent = self._ray_grp = self._ray_pair = None
                 self.ray_taps = 0
                 self._build_fourier()
             else:
                 self._ray_rp, self._ray_ent, self.ray_taps = self._build_ray_table()
                 self._ray_grp = self._build_group_table()
+                self._ray_pair = self._build_group_table(pairs=True)
             self.omega_subsets = None
             self._sub = []
             self._streamer = None
@@ -292,16 +293,18 @@ class SinglePhaseForwardOperator:
                    rp.data_ptr(), ent.data_ptr(), s)
         return rp, ent, total
 
-    def _build_group_table(self, supp=None):
+    def _build_group_table(self, supp=None, pairs=False):
         """The grouped ray table of the float32 forward (dfx_radon_gtable_*): per (angle, four bins) the pixels that
         reach them with their four weights, so that each pixel's channels are loaded once per group; the sums are
-        the per-bin table's bits. Returns (row_ptr, pixels, weights)."""
+        the per-bin table's bits. pairs: the paired table of the forward of all angles (dfx_radon_ptable_*, per
+        pair of consecutive angles and four bins, eight weights). Returns (row_ptr, pixels, weights)."""
         R, ns = self.N_Omega, self.My
-        n = R * (-(-ns // 4))
+        kind = "ptable" if pairs else "gtable"
+        n = (-(-R // 2) if pairs else R) * (-(-ns // 4))
         s = self._s()
         sp = None if supp is None else supp.data_ptr()
         rp = torch.empty(n + 1, dtype=torch.int32, device=self.device)
-        self._call("dfx_radon_gtable_count", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id, sp,
+        self._call(f"dfx_radon_{kind}_count", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id, sp,
                    rp.data_ptr(), s)
         self.stream().synchronize()
         total = int(rp[:n].to(torch.int64).sum().item())
@@ -311,8 +314,8 @@ class SinglePhaseForwardOperator:
         scr = self.scratch(nb)
         self._call("dfx_scan_exclusive_i32", rp.data_ptr(), rp.data_ptr(), n, scr.data_ptr(), nb, s)
         pix = torch.empty(max(total, 1), dtype=torch.int32, device=self.device)
-        w = torch.empty((max(total, 1), 4), dtype=torch.float32, device=self.device)
-        self._call("dfx_radon_gtable_fill", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id, sp,
+        w = torch.empty((max(total, 1), 8 if pairs else 4), dtype=torch.float32, device=self.device)
+        self._call(f"dfx_radon_{kind}_fill", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id, sp,
                    rp.data_ptr(), pix.data_ptr(), w.data_ptr(), s)
         return rp, pix, w
 
@@ -326,7 +329,8 @@ class SinglePhaseForwardOperator:
         key = bytes(supp.cpu().numpy())
         hit = self._ray_supp.get(key)
         if hit is None:
-            hit = self._build_ray_table(supp) + (self._build_group_table(supp),)
+            hit = self._build_ray_table(supp) + (self._build_group_table(supp),
+                                                 self._build_group_table(supp, pairs=True))
             self._ray_supp[key] = hit
         return hit
 
@@ -371,7 +375,11 @@ class SinglePhaseForwardOperator:
         om_ptr = None if om is None else om.data_ptr()
         rp, ent = (self._ray_rp, self._ray_ent) if ray is None else ray[:2]
         grp = self._ray_grp if ray is None else (ray[3] if len(ray) > 3 else None)
-        if sld is None and grp is not None:
+        pair = self._ray_pair if ray is None else (ray[4] if len(ray) > 4 else None)
+        if sld is None and pair is not None and om is None and n_ang == self.N_Omega:
+            self._call("dfx_radon_forward_ptable", src_ptr, dst_ptr, pair[0].data_ptr(), pair[1].data_ptr(),
+                       pair[2].data_ptr(), n_ang, self.My, self.Kstride, kb, float(self.radon_geo.scale), self._s())
+        elif sld is None and grp is not None:
             self._call("dfx_radon_forward_gtable", src_ptr, dst_ptr, grp[0].data_ptr(), grp[1].data_ptr(),
                        grp[2].data_ptr(), om_ptr, n_ang, self.My, self.Kstride, kb, float(self.radon_geo.scale),
                        self._s())
@@ -1315,7 +1323,7 @@ class SinglePhaseForwardOperator:
         self.release_omega_subsets()
         self.release_streamer()
         self._ray_supp = {}
-        self._ray_grp = None
+        self._ray_grp = self._ray_pair = None
         self._tcf_tab = None
         self._supp_tiles = {}
         self._fft = None

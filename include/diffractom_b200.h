@@ -142,6 +142,19 @@ int dfx_radon_gtable_fill(const float *geo, int n_angles, int nx, int ny, int n_
 int dfx_radon_forward_gtable(const float *img_k, float *sino_k, const int32_t *row_ptr, const int32_t *pixels,
                              const float *weights, const int32_t *angles, int n_angles, int n_det, int kstride,
                              int kb, float scale, void *stream);
+/* Paired ray table (no reference counterpart), for the forward of all angles: row (i, g) = i * ceil(n_det / 4) + g
+ * lists the pixels reaching one of the bins 4 g .. 4 g + 3 of angle 2 i or 2 i + 1, with their eight weights (two
+ * float4: angle 2 i, then 2 i + 1; 0 where the per-bin row has no entry), each angle's entries in its per-bin rows'
+ * order; count / fill / supp as for the per-bin table (weights: 32 bytes per entry, 16-byte aligned).
+ * dfx_radon_forward_ptable: dfx_radon_forward_table of all n_angles angles over it, the same bits, each pixel's
+ * channels loaded once for both angles of a pair. */
+int dfx_radon_ptable_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel, const uint8_t *supp,
+                           int32_t *counts, void *stream);
+int dfx_radon_ptable_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel, const uint8_t *supp,
+                          const int32_t *row_ptr, int32_t *pixels, float *weights, void *stream);
+int dfx_radon_forward_ptable(const float *img_k, float *sino_k, const int32_t *row_ptr, const int32_t *pixels,
+                             const float *weights, int n_angles, int n_det, int kstride, int kb, float scale,
+                             void *stream);
 
 /* replaces support_ones / project_support / tmin (fista_poisson.py:256-263, 277-281; spdhg_poisson.py:259-265) on a
  * channel-fastest batch (npix, kstride) with padding channels kb .. kstride-1 (supp (npix) uint8 or NULL):

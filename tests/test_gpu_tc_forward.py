@@ -103,7 +103,8 @@ def test_tc_forward_full_scan_support_tiles_and_bf16_rows():
 
 def test_grouped_table_forward_of_a_full_scan():
     """The float32 forward through the grouped table (dfx_radon_forward_gtable) at 360 angles and 256 x 256 pixels,
-    where it runs eight channels per lane, and for a subset's 18 angles (four per lane): the per-bin table's bits."""
+    where it runs eight channels per lane, and for a subset's 18 angles (four per lane), and through the paired table
+    of the full scan (dfx_radon_forward_ptable): the per-bin table's bits."""
     from diffractom_b200 import _lib
     op = _ti256_operator()
     assert op._ray_grp is not None
@@ -125,6 +126,13 @@ def test_grouped_table_forward_of_a_full_scan():
                   grp[2].data_ptr(), rp, n, My, ks, kb, float(op.radon_geo.scale), s)
         torch.cuda.synchronize()
         assert torch.equal(a, b)
+        if rows is None:                  # the paired table (two consecutive angles per entry) of the full scan
+            c = torch.empty((n, My, ks), device="cuda")
+            pair = op._ray_pair
+            _lib.call("dfx_radon_forward_ptable", img.data_ptr(), c.data_ptr(), pair[0].data_ptr(),
+                      pair[1].data_ptr(), pair[2].data_ptr(), n, My, ks, kb, float(op.radon_geo.scale), s)
+            torch.cuda.synchronize()
+            assert torch.equal(a, c)
 
 
 @pytest.mark.parametrize("case", ["al5_small", "ti256"])
