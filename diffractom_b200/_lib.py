@@ -60,6 +60,7 @@ SIGNATURES = {
     "dfx_radon_forward_ptable": ([P, P, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_radon_forward_table_bf16": ([P, P, L, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_radon_forward_table_bf16_bf16": ([P, P, L, P, P, P, I, I, I, I, F, S], c_int),
+    "dfx_radon_forward_gtable_bf16_bf16": ([P, P, L, P, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_batch_support": ([P, P, P, L, I, I, F, I, S], c_int),
     "dfx_pf_dense": ([POINTER(PFGeometry), I, I, P, S], c_int),
     "dfx_pf_csr_count": ([POINTER(PFGeometry), P, I, I, I, I, P, S], c_int),

@@ -678,6 +678,86 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_gtable4(
     }
 }
 
+// The grouped-table forward of a BF16 image into BF16 sinogram rows of stride sld (the BF16 passes' Z columns): four
+// channels per lane (8-byte loads, widened exactly), float32 sums of the per-bin rows' taps in their order, rounded
+// once on store: dfx_radon_forward_table_bf16_bf16's bits.
+__global__ void __launch_bounds__(32 * WARPS) radon_forward_gtable4_bb(
+    const __nv_bfloat16 *__restrict__ img, __nv_bfloat16 *__restrict__ sino, int64_t sld,
+    const int32_t *__restrict__ row_ptr, const int32_t *__restrict__ pix, const float4 *__restrict__ wts,
+    const int32_t *__restrict__ angles, int ns, int kstride, int kb, float scale)
+{
+    constexpr int U = 8, C4 = 4, CW = 32 * C4;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ng = (ns + GB - 1) / GB;
+    const int grp = blockIdx.x * WARPS + warp;
+    const int al = blockIdx.y;
+    const int k = blockIdx.z * CW + lane * C4;
+    if (grp >= ng) return;
+    const bool live = k < kstride;
+    const int s0 = grp * GB;
+    __nv_bfloat16 *out = sino + ((int64_t)al * ns + s0) * sld + k;
+    const int nb = min(GB, ns - s0);
+    if (blockIdx.z * CW >= kb) {
+        if (live)
+            for (int j = 0; j < nb; ++j) *reinterpret_cast<uint2 *>(out + (int64_t)j * sld) = make_uint2(0, 0);
+        return;
+    }
+    const bool load = k < kb;
+    const int a = angles ? __ldg(angles + al) : al;
+    const int64_t r = (int64_t)a * ng + grp;
+    int e = __ldg(row_ptr + r);
+    const int e1 = __ldg(row_ptr + r + 1);
+    const __nv_bfloat16 *base = img + (load ? k : 0);
+    float acc[GB][C4];
+#pragma unroll
+    for (int j = 0; j < GB; ++j)
+#pragma unroll
+        for (int c = 0; c < C4; ++c) acc[j][c] = 0.0f;
+    auto widen = [](uint2 u) {
+        return make_float4(bf_lo(u.x), bf_hi(u.x), bf_lo(u.y), bf_hi(u.y));
+    };
+    for (; e + U <= e1; e += U) {
+        int p[U];
+        float4 w[U];
+        uint2 q[U];
+#pragma unroll
+        for (int i = 0; i < U; ++i) {
+            p[i] = __ldg(pix + e + i);
+            w[i] = __ldg(wts + e + i);
+        }
+#pragma unroll
+        for (int i = 0; i < U; ++i)
+            q[i] = load ? __ldg(reinterpret_cast<const uint2 *>(base + (int64_t)p[i] * kstride)) : make_uint2(0, 0);
+#pragma unroll
+        for (int i = 0; i < U; ++i) {
+            const float4 x = widen(q[i]);
+            if (w[i].x != 0.0f) acc4(acc[0], w[i].x, x);
+            if (w[i].y != 0.0f) acc4(acc[1], w[i].y, x);
+            if (w[i].z != 0.0f) acc4(acc[2], w[i].z, x);
+            if (w[i].w != 0.0f) acc4(acc[3], w[i].w, x);
+        }
+    }
+    for (; e < e1; ++e) {
+        const int p = __ldg(pix + e);
+        const float4 w = __ldg(wts + e);
+        const float4 x = widen(load ? __ldg(reinterpret_cast<const uint2 *>(base + (int64_t)p * kstride))
+                                    : make_uint2(0, 0));
+        if (w.x != 0.0f) acc4(acc[0], w.x, x);
+        if (w.y != 0.0f) acc4(acc[1], w.y, x);
+        if (w.z != 0.0f) acc4(acc[2], w.z, x);
+        if (w.w != 0.0f) acc4(acc[3], w.w, x);
+    }
+    if (!live) return;
+#pragma unroll
+    for (int j = 0; j < GB; ++j) {
+        if (j >= nb) break;
+        float o[C4];
+#pragma unroll
+        for (int c = 0; c < C4; ++c) o[c] = (k + c < kb) ? __fmul_rn(scale, acc[j][c]) : 0.0f;
+        *reinterpret_cast<uint2 *>(out + (int64_t)j * sld) = make_uint2(pack_bf16(o[0], o[1]), pack_bf16(o[2], o[3]));
+    }
+}
+
 // ------------------------------------------------------------------------------------------------ backward
 // SPDHG primal step of one coefficient: the operations of primal_update_kernel (solver.cu), bitwise
 __device__ __forceinline__ void primal_step(float &x, float &z, float t, float dz, float inv_p, float lam)
@@ -1014,8 +1094,9 @@ static int allow_smem(Kernel kernel, size_t bytes)
     return DFX_OK;
 }
 
-// the whole-image SIMT backprojection runs four pixels per warp (radon_backward_q4; dfx_radon_backward_quads)
-static bool backward_quads = true;
+// the whole-image SIMT backprojection with four pixels per warp (radon_backward_q4; dfx_radon_backward_quads): off by
+// default, at ti256 it took 0.75 ms per launch with the primal step against 0.65 ms for two channel groups per warp
+static bool backward_quads = false;
 
 template <int KERNEL, int MODE, typename ST>
 static int launch_backward(const ST *sino, int64_t sld, float *img, const float *geo, int n_angles, int nx, int ny,
@@ -1389,6 +1470,28 @@ extern "C" int dfx_radon_forward_table_bf16_bf16(const void *img_bf16, void *sin
     return radon_forward_table_any(reinterpret_cast<const __nv_bfloat16 *>(img_bf16),
                                    reinterpret_cast<__nv_bfloat16 *>(sino_bf16), sino_ld, row_ptr, entries, angles,
                                    n_angles, n_det, kstride, kb, scale, stream);
+}
+
+extern "C" int dfx_radon_forward_gtable_bf16_bf16(const void *img_bf16, void *sino_bf16, int64_t sino_ld,
+                                                  const int32_t *row_ptr, const int32_t *pixels, const float *weights,
+                                                  const int32_t *angles, int n_angles, int n_det, int kstride, int kb,
+                                                  float scale, void *stream)
+{
+    DFX_REQUIRE(img_bf16 && sino_bf16 && row_ptr && pixels && weights, "radon_forward_gtable_bf16: null pointer");
+    DFX_REQUIRE(((uintptr_t)img_bf16 % 16) == 0 && ((uintptr_t)sino_bf16 % 8) == 0 && ((uintptr_t)weights % 16) == 0,
+                "radon_forward_gtable_bf16: misaligned arrays");
+    DFX_REQUIRE(n_angles >= 0 && n_angles <= 65535 && n_det > 0, "radon_forward_gtable_bf16: bad sizes");
+    DFX_REQUIRE(kstride > 0 && kstride % CPL == 0 && kb >= 0 && kb <= kstride && cdiv(kstride, 128) <= 65535,
+                "radon_forward_gtable_bf16: kstride (%d) must be a positive multiple of %d and kb (%d) <= kstride",
+                kstride, CPL, kb);
+    DFX_REQUIRE(sino_ld >= kstride && sino_ld % CPL == 0, "radon_forward_gtable_bf16: sinogram row stride (%lld) "
+                "must be a multiple of %d >= kstride", (long long)sino_ld, CPL);
+    if (n_angles == 0) return DFX_OK;
+    dim3 grid((unsigned)cdiv(cdiv(n_det, GB), WARPS), (unsigned)n_angles, (unsigned)cdiv(kstride, 128));
+    radon_forward_gtable4_bb<<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<const __nv_bfloat16 *>(img_bf16), reinterpret_cast<__nv_bfloat16 *>(sino_bf16), sino_ld,
+        row_ptr, pixels, reinterpret_cast<const float4 *>(weights), angles, n_det, kstride, kb, scale);
+    return launch_status("radon_forward_gtable_bf16");
 }
 
 extern "C" int dfx_batch_support(float *x_k, const float *colsum_k, const uint8_t *supp, int64_t npix, int kstride,

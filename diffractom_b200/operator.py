@@ -780,6 +780,20 @@ class SinglePhaseForwardOperator:
         c = max(self._bf16_chunk, self._max_subset()) if subset is not None else self._bf16_chunk
         return [(geo[a:a + c], min(c, n - a), om[a:a + c], a) for a in range(0, n, c)]
 
+    def lazy_bytes(self) -> int:
+        """Device memory the operator allocates on first use during a solver's iterations (the BF16 Radon output of
+        the largest subset, the generated BF16 PF buffers, the Fourier-slice scratch), for callers that size their
+        own arrays beforehand."""
+        n = 0
+        if self.precision == "bf16":
+            ns = self._max_subset() if self._sub else self._bf16_chunk
+            n += 2 * ns * self.My * self.Ktot
+            if self.pf_bf16 is None:
+                n += 2 * 2 * ns * self.Ktot * self.cp_pad
+        if self.projector == "fft":
+            n += int(self.fft_max_gb * 1024 ** 3)
+        return int(n)
+
     def _max_subset(self):
         return max((e["n"] for e in self._sub), default=1)
 
@@ -948,6 +962,12 @@ class SinglePhaseForwardOperator:
             self._call("dfx_radon_forward_tc", src_ptr, dst_ptr, self.Ktot, 0, geo.data_ptr(), n, self.Nx, self.Ny,
                        self.My, self.Kstride, self._kernel_id, int(self.radon_geo.n_taps),
                        float(self.radon_geo.scale), tp, nt, self._s())
+            return
+        grp = self._ray_grp if ray is None else (ray[3] if len(ray) > 3 else None)
+        if grp is not None:
+            self._call("dfx_radon_forward_gtable_bf16_bf16", src_ptr, dst_ptr, self.Ktot, grp[0].data_ptr(),
+                       grp[1].data_ptr(), grp[2].data_ptr(), om.data_ptr(), n, self.My, self.Kstride, kb,
+                       float(self.radon_geo.scale), self._s())
             return
         rp, ent = (self._ray_rp, self._ray_ent) if ray is None else ray[:2]
         self._call("dfx_radon_forward_table_bf16_bf16", src_ptr, dst_ptr, self.Ktot, rp.data_ptr(), ent.data_ptr(),

@@ -210,9 +210,21 @@ class ReconstructionServer:
                 if self._stop:
                     return
                 try:
-                    free = int(torch.cuda.mem_get_info(self.device)[0]) - (1 << 30)
+                    # free device memory plus what this process's allocator holds cached (finished requests' buffers,
+                    # which the next request's tensors reuse)
+                    free = (int(torch.cuda.mem_get_info(self.device)[0]) + int(torch.cuda.memory_reserved(self.device))
+                            - int(torch.cuda.memory_allocated(self.device)) - (1 << 30))
                 except RuntimeError:            # a query failing now and then must not end the admissions
                     free = None
+                if not self.sched.running and self.sched.queue and free is not None and self.sched.queue[0][1] > free:
+                    # nothing runs and the oldest request still does not fit: it never will
+                    rid, nb = self.sched.queue.pop(0)
+                    req = self.requests[rid]
+                    req.error = (f"MemoryError: request needs {nb / 1e9:.1f} GB, more than the device's "
+                                 f"{max(free, 0) / 1e9:.1f} GB free")
+                    req.admitted = req.finished = self.now()
+                    self.done.append(req)
+                    self._lock.notify_all()
                 for rid in self.sched.admit(free_bytes=free):
                     req = self.requests[rid]
                     req.admitted = self.now()

@@ -68,12 +68,13 @@ class SPDHGPoisson:
     # its own kernel). "auto" (resident="auto" only): when x and z fit in float32 and T then fits in BF16 but not in
     # float32, instead of streaming T from host memory in every iteration; True: always with such an operator.
     bf16_T = "auto"
-    # With an operator of precision "bf16" (native projector) and float32 diagnostics, the residual of a diagnostics
-    # epoch (the float32 forward A x of the epoch's last x and its float64 deviance) runs on a side stream from a copy
-    # of x while the next epoch's iterations go on; the next subset's rows then come from the BF16 forward like every
-    # other iteration's. The objective is read when the run ends (or the next time it is needed). Off: the residual
-    # runs in line and its rows serve the next subset. Not with callbacks, printing, TV, shards or streamed state.
-    overlap_residual = True
+    # True: with an operator of precision "bf16" (native projector) and float32 diagnostics, the residual of a
+    # diagnostics epoch (the float32 forward A x of the epoch's last x and its float64 deviance) runs on a side stream
+    # from a copy of x while the next epoch's iterations go on; the next subset's rows then come from the BF16 forward
+    # like every other iteration's, and the objective is read when the run ends. Not with callbacks, printing, TV,
+    # shards or streamed state. Off by default: at ti256 the two streams share a GPU that either keeps busy, and the
+    # epoch rate stayed the same (1.89 against 1.91 epochs/s) while the iterations' kernels ran half as fast.
+    overlap_residual = False
 
     def __init__(self, operator, subsets=8, prox_kind="nonneg", lam=0.0, support="fov", eps_counts=1e-3, rho="auto",
                  seed=0, resident="auto", tv=0.0, tv_prob=None, tv_tree=None, shards=None):
@@ -124,6 +125,7 @@ class SPDHGPoisson:
         self.shards = shards
         self.state = None
         self._t16 = False
+        self._stage_io = False
         self._side = None
         self._pending = []
 
@@ -556,7 +558,8 @@ class SPDHGPoisson:
         self.T = CoeffArray(op, "T", "T" in resident, torch.bfloat16 if self._t16 else torch.float32)
         self.pipe = BatchPipeline(op)
         # staged host IO (no (K, Ny, Nx) device temporary) when memory is short: some array streamed, or T in BF16
-        self._stage = None if len(resident) == len(self._names) and not self._t16 else KMajorStaging(op)
+        self._stage = (None if len(resident) == len(self._names) and not self._t16 and not self._stage_io
+                       else KMajorStaging(op))
         self.dzk = torch.empty(be, dtype=torch.float32, device=dev)
         self.x = None
         # a host x0 of a resident x is uploaded after the step sizes' passes are queued, on a side stream, so that
@@ -891,6 +894,7 @@ class SPDHGPoisson:
         streaming buffers and a margin."""
         names = self._names
         op = self.op
+        self._stage_io = False
         t16_ok = op.precision == "bf16" and op.projector == "fft" and self.tv == 0
         if self.bf16_T is True and not t16_ok:
             raise ValueError("bf16_T needs an operator of precision 'bf16' with the Fourier-slice projector, no tv")
@@ -906,8 +910,12 @@ class SPDHGPoisson:
         free, _ = torch.cuda.mem_get_info(op.device)
         # two slots per streamed array, the k-major staging buffer, the batch scratch and a BF16 batch of x
         staging = (4 * 2 * len(names) + 4 + 4 + 2 + (8 if self.tv > 0 else 0)) * be
-        room = max(0, free - staging - MARGIN_GB * 1024 ** 3)
+        room = max(0, free - staging - MARGIN_GB * 1024 ** 3 - op.lazy_bytes())
         n = int(room // nbytes)
+        if n >= len(names):
+            # a host x0 of a resident x goes through a (K, Ny, Nx) device copy unless that does not fit as well
+            self._stage_io = room < (len(names) + 1) * nbytes
+            return set(names)
         if n == 2 and len(names) == 3 and t16_ok and self.bf16_T == "auto" and room >= 2.5 * nbytes:
             self._t16 = True
             return set(names)

@@ -78,8 +78,8 @@ int dfx_radon_backward_spdhg(const float *sino_k, const float *geo, int n_angles
                              int kstride, int kb, int kernel, int n_taps, float *x_k, float *z_k, const float *T_k,
                              float inv_p, float lam, void *stream);
 /* The whole-image SIMT backprojections above (float32 and BF16 sinograms, plain and with the primal step) run four
- * neighbouring pixels per warp, loading each bin row of the union of their taps once (on: 1, the default), or one
- * pixel per warp (0); the sums are the same bits either way. Returns the previous setting; on < 0 only queries it.
+ * neighbouring pixels per warp, loading each bin row of the union of their taps once (on: 1), or one pixel per warp
+ * (0, the default); the sums are the same bits either way. Returns the previous setting; on < 0 only queries it.
  * No reference counterpart (a performance switch of this library, process-wide). */
 int dfx_radon_backward_quads(int on);
 
@@ -128,6 +128,11 @@ int dfx_radon_forward_table_bf16(const float *img_k, void *sino_bf16, int64_t si
 int dfx_radon_forward_table_bf16_bf16(const void *img_bf16, void *sino_bf16, int64_t sino_ld, const int32_t *row_ptr,
                                       const int32_t *entries, const int32_t *angles, int n_angles, int n_det,
                                       int kstride, int kb, float scale, void *stream);
+/* The same through the grouped table (dfx_radon_gtable_*; four channels per lane): each pixel's channels loaded once
+ * per four bins, the same sums and roundings: dfx_radon_forward_table_bf16_bf16's bits. */
+int dfx_radon_forward_gtable_bf16_bf16(const void *img_bf16, void *sino_bf16, int64_t sino_ld, const int32_t *row_ptr,
+                                       const int32_t *pixels, const float *weights, const int32_t *angles,
+                                       int n_angles, int n_det, int kstride, int kb, float scale, void *stream);
 
 /* Grouped ray table (no reference counterpart): row a * ceil(n_det / 4) + g lists, in the per-bin rows' order, every
  * pixel that reaches one of the bins 4 g .. 4 g + 3 of angle a, as an int32 pixel index and a float4 of its weights

@@ -126,6 +126,19 @@ def test_grouped_table_forward_of_a_full_scan():
                   grp[2].data_ptr(), rp, n, My, ks, kb, float(op.radon_geo.scale), s)
         torch.cuda.synchronize()
         assert torch.equal(a, b)
+        # the BF16 image into BF16 rows of a wider sinogram: grouped table = per-bin table
+        imgb = img.to(torch.bfloat16)
+        zt = torch.zeros((n, My, 2 * ks), dtype=torch.bfloat16, device="cuda")
+        zg = torch.zeros((n, My, 2 * ks), dtype=torch.bfloat16, device="cuda")
+        ent = (op._ray_rp, op._ray_ent)
+        rr = rows if rows is not None else torch.arange(R, dtype=torch.int32, device="cuda")
+        _lib.call("dfx_radon_forward_table_bf16_bf16", imgb.data_ptr(), zt.data_ptr() + 2 * ks, 2 * ks,
+                  ent[0].data_ptr(), ent[1].data_ptr(), rr.data_ptr(), n, My, ks, kb, float(op.radon_geo.scale), s)
+        _lib.call("dfx_radon_forward_gtable_bf16_bf16", imgb.data_ptr(), zg.data_ptr() + 2 * ks, 2 * ks,
+                  grp[0].data_ptr(), grp[1].data_ptr(), grp[2].data_ptr(), rr.data_ptr(), n, My, ks, kb,
+                  float(op.radon_geo.scale), s)
+        torch.cuda.synchronize()
+        assert torch.equal(zt, zg) and not zg[:, :, :ks].any()
         if rows is None:                  # the paired table (two consecutive angles per entry) of the full scan
             c = torch.empty((n, My, ks), device="cuda")
             pair = op._ray_pair
