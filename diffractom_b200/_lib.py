@@ -39,7 +39,6 @@ SIGNATURES = {
     "dfx_radon_backward": ([P, P, P, I, I, I, I, I, I, I, I, S], c_int),
     "dfx_radon_backward_pixels": ([P, P, P, I, I, I, I, I, I, I, I, P, L, S], c_int),
     "dfx_radon_backward_spdhg": ([P, P, I, I, I, I, I, I, I, I, P, P, P, F, F, S], c_int),
-    "dfx_radon_backward_quads": ([I], c_int),
     "dfx_radon_forward_bf16": ([P, P, L, P, I, I, I, I, I, I, I, F, S], c_int),
     "dfx_radon_backward_bf16": ([P, L, P, P, I, I, I, I, I, I, I, I, S], c_int),
     "dfx_radon_backward_spdhg_bf16": ([P, L, P, I, I, I, I, I, I, I, I, P, P, P, F, F, P, S], c_int),
@@ -55,12 +54,8 @@ SIGNATURES = {
     "dfx_radon_gtable_count": ([P, I, I, I, I, I, P, P, S], c_int),
     "dfx_radon_gtable_fill": ([P, I, I, I, I, I, P, P, P, P, S], c_int),
     "dfx_radon_forward_gtable": ([P, P, P, P, P, P, I, I, I, I, F, S], c_int),
-    "dfx_radon_ptable_count": ([P, I, I, I, I, I, P, P, S], c_int),
-    "dfx_radon_ptable_fill": ([P, I, I, I, I, I, P, P, P, P, S], c_int),
-    "dfx_radon_forward_ptable": ([P, P, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_radon_forward_table_bf16": ([P, P, L, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_radon_forward_table_bf16_bf16": ([P, P, L, P, P, P, I, I, I, I, F, S], c_int),
-    "dfx_radon_forward_gtable_bf16_bf16": ([P, P, L, P, P, P, P, I, I, I, I, F, S], c_int),
     "dfx_batch_support": ([P, P, P, L, I, I, F, I, S], c_int),
     "dfx_pf_dense": ([POINTER(PFGeometry), I, I, P, S], c_int),
     "dfx_pf_csr_count": ([POINTER(PFGeometry), P, I, I, I, I, P, S], c_int),
@@ -75,7 +70,6 @@ SIGNATURES = {
     "dfx_pf_fblock_count": ([P, P, I, I, I, P, P, S], c_int),
     "dfx_pf_fblock_fill": ([P, P, P, I, I, I, P, P, P, S], c_int),
     "dfx_spmm_pf_forward_blocked": ([P, P, P, P, P, P, P, I, I, I, I, I, I, S], c_int),
-    "dfx_spmm_pf_forward_lines": ([P, P, P, P, P, P, P, I, I, I, I, I, I, S], c_int),
     "dfx_zero_rows": ([P, P, I, L, S], c_int),
     "dfx_fill_f32": ([P, F, L, S], c_int),
     "dfx_spdhg_dual_update": ([P, P, P, P, P, L, P, L, P, L, F, P, I, L, S], c_int),

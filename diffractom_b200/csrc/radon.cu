@@ -406,358 +406,6 @@ __global__ void __launch_bounds__(32 * WARPS) radon_forward_gtable(
     }
 }
 
-// ------------------------------------------------------------------------------------------------ paired table
-// For the forward of all angles, consecutive angles 2i and 2i + 1 share most pixels of a bin group (their rays differ
-// by half a degree): the paired table lists, per (angle pair, four bins), the pixels that reach one of the eight
-// (angle, bin) outputs with their eight weights, so a pixel's channels are loaded once for both angles. When the
-// two angles parametrise the image alike (rows along the same axis) the two angles' per-bin lists are merged in
-// their common (row, column) order; otherwise the first angle's entries come first, then the second's. Either way
-// each (angle, bin) sums its per-bin row's taps in that row's order: the per-bin forward's bits.
-template <int KERNEL>
-__device__ void pair_rows(const AngleGeo (&g)[2], const bool (&ok)[2], int which, int nx, int ny, int ns, int s0,
-                          const uint8_t *__restrict__ supp, int &n, int64_t &pos, int32_t *__restrict__ pix_out,
-                          float4 *__restrict__ w_out)
-{
-    // which: 0 = angle 0 only, 1 = angle 1 only, 2 = both (merged)
-    const AngleGeo &gr = g[which == 1 ? 1 : 0];
-    const int nu = gr.rows_are_y ? nx : ny, nv = gr.rows_are_y ? ny : nx;
-    float inv[2], half[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        inv[h] = __frcp_rn(g[h].A);
-        half[h] = KERNEL == 1 ? g[h].hw : 1.0f;
-    }
-    for (int v = 0; v < nv; ++v) {
-        float c[2];
-        int u0[2][GB], u1[2][GB];
-        int lo = nu, hi = -1;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const bool use = ok[h] && (which == 2 || which == h);
-            c[h] = __fmaf_rn(g[h].B, (float)v, g[h].T0);
-#pragma unroll
-            for (int j = 0; j < GB; ++j) {
-                u0[h][j] = 0;
-                u1[h][j] = -1;
-                if (!use || s0 + j >= ns) continue;
-                const float fs = (float)(s0 + j);
-                const float e1 = (fs - half[h] - c[h]) * inv[h], e2 = (fs + half[h] - c[h]) * inv[h];
-                u0[h][j] = max((int)floorf(fminf(e1, e2) - 1e-3f), 0);
-                u1[h][j] = min((int)ceilf(fmaxf(e1, e2) + 1e-3f), nu - 1);
-                if (u0[h][j] <= u1[h][j]) {
-                    lo = min(lo, u0[h][j]);
-                    hi = max(hi, u1[h][j]);
-                }
-            }
-        }
-        for (int u = lo; u <= hi; ++u) {
-            float w[2][GB];
-            bool any = false;
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-#pragma unroll
-                for (int j = 0; j < GB; ++j) {
-                    w[h][j] = 0.0f;
-                    if (u < u0[h][j] || u > u1[h][j]) continue;
-                    const float d = __fsub_rn(__fmaf_rn(g[h].A, (float)u, c[h]), (float)(s0 + j));
-                    w[h][j] = tap_weight<KERNEL>(g[h], d);
-                    any |= w[h][j] != 0.0f;
-                }
-            if (!any) continue;
-            const int pix = gr.rows_are_y ? u + nx * v : v + nx * u;
-            if (supp && !supp[pix]) continue;
-            if (pix_out) {
-                pix_out[pos] = pix;
-                w_out[2 * pos] = make_float4(w[0][0], w[0][1], w[0][2], w[0][3]);
-                w_out[2 * pos + 1] = make_float4(w[1][0], w[1][1], w[1][2], w[1][3]);
-                ++pos;
-            }
-            ++n;
-        }
-    }
-}
-
-template <int KERNEL>
-__global__ void ray_ptable_kernel(const float4 *__restrict__ geo, int n_angles, int nx, int ny, int ns,
-                                  const uint8_t *__restrict__ supp, int32_t *__restrict__ counts,
-                                  const int32_t *__restrict__ row_ptr, int32_t *__restrict__ pix_out,
-                                  float4 *__restrict__ w_out)
-{
-    const int ng = (ns + GB - 1) / GB, npairs = (n_angles + 1) / 2;
-    const int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;      // pair * ng + g
-    if (row >= (int64_t)npairs * ng) return;
-    const int pr = (int)(row / ng), s0 = (int)(row % ng) * GB;
-    AngleGeo g[2];
-    bool ok[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int a = 2 * pr + h;
-        ok[h] = a < n_angles;
-        g[h] = load_geo(geo, ok[h] ? a : 2 * pr);
-    }
-    int n = 0;
-    int64_t pos = row_ptr ? row_ptr[row] : 0;
-    if (!ok[1] || g[0].rows_are_y == g[1].rows_are_y) {
-        pair_rows<KERNEL>(g, ok, 2, nx, ny, ns, s0, supp, n, pos, row_ptr ? pix_out : nullptr, w_out);
-    } else {
-        pair_rows<KERNEL>(g, ok, 0, nx, ny, ns, s0, supp, n, pos, row_ptr ? pix_out : nullptr, w_out);
-        pair_rows<KERNEL>(g, ok, 1, nx, ny, ns, s0, supp, n, pos, row_ptr ? pix_out : nullptr, w_out);
-    }
-    if (!row_ptr) counts[row] = n;
-}
-
-// Paired-table forward of all angles: warp per (angle pair, four bins, 256 channels), eight accumulators of 8
-// channels per lane, U pixels in flight, FMAs only for the non-zero weights (a branch the whole warp takes).
-__global__ void __launch_bounds__(32 * WARPS) radon_forward_ptable(
-    const float *__restrict__ img, float *__restrict__ sino, const int32_t *__restrict__ row_ptr,
-    const int32_t *__restrict__ pix, const float4 *__restrict__ wts, int n_angles, int ns, int kstride, int kb,
-    float scale)
-{
-    constexpr int U = 2;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ng = (ns + GB - 1) / GB;
-    const int grp = blockIdx.x * WARPS + warp;
-    const int pr = blockIdx.y;
-    const int k = blockIdx.z * CPW + lane * CPL;
-    if (grp >= ng) return;
-    const bool live = k < kstride;
-    const int s0 = grp * GB, nb = min(GB, ns - s0);
-    const int na = min(2, n_angles - 2 * pr);
-    if (blockIdx.z * CPW >= kb) {
-        const float zero[CPL] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (live)
-            for (int h = 0; h < na; ++h)
-                for (int j = 0; j < nb; ++j) st8(sino + ((int64_t)(2 * pr + h) * ns + s0 + j) * kstride + k, zero);
-        return;
-    }
-    const bool load = k < kb;
-    const int64_t r = (int64_t)pr * ng + grp;
-    int e = __ldg(row_ptr + r);
-    const int e1 = __ldg(row_ptr + r + 1);
-    const float *base = img + (load ? k : 0);
-    float acc[2][GB][CPL];
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-#pragma unroll
-        for (int j = 0; j < GB; ++j)
-#pragma unroll
-            for (int c = 0; c < CPL; ++c) acc[h][j][c] = 0.0f;
-    auto apply = [&](const float4 &wa, const float4 &wb, const Raw8<float> &q) {
-        if (wa.x != 0.0f) accraw(acc[0][0], wa.x, q);
-        if (wa.y != 0.0f) accraw(acc[0][1], wa.y, q);
-        if (wa.z != 0.0f) accraw(acc[0][2], wa.z, q);
-        if (wa.w != 0.0f) accraw(acc[0][3], wa.w, q);
-        if (wb.x != 0.0f) accraw(acc[1][0], wb.x, q);
-        if (wb.y != 0.0f) accraw(acc[1][1], wb.y, q);
-        if (wb.z != 0.0f) accraw(acc[1][2], wb.z, q);
-        if (wb.w != 0.0f) accraw(acc[1][3], wb.w, q);
-    };
-    for (; e + U <= e1; e += U) {
-        int p[U];
-        float4 wa[U], wb[U];
-        Raw8<float> q[U];
-#pragma unroll
-        for (int i = 0; i < U; ++i) {
-            p[i] = __ldg(pix + e + i);
-            wa[i] = __ldg(wts + 2 * (e + i));
-            wb[i] = __ldg(wts + 2 * (e + i) + 1);
-        }
-#pragma unroll
-        for (int i = 0; i < U; ++i) {
-            zraw(q[i]);
-            if (load) ldraw(base + (int64_t)p[i] * kstride, q[i]);
-        }
-#pragma unroll
-        for (int i = 0; i < U; ++i) apply(wa[i], wb[i], q[i]);
-    }
-    for (; e < e1; ++e) {
-        const int p = __ldg(pix + e);
-        const float4 wa = __ldg(wts + 2 * e), wb = __ldg(wts + 2 * e + 1);
-        Raw8<float> q;
-        zraw(q);
-        if (load) ldraw(base + (int64_t)p * kstride, q);
-        apply(wa, wb, q);
-    }
-    if (!live) return;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        if (h >= na) break;
-#pragma unroll
-        for (int j = 0; j < GB; ++j) {
-            if (j >= nb) break;
-            float o[CPL];
-#pragma unroll
-            for (int c = 0; c < CPL; ++c) o[c] = (k + c < kb) ? __fmul_rn(scale, acc[h][j][c]) : 0.0f;
-            st8(sino + ((int64_t)(2 * pr + h) * ns + s0 + j) * kstride + k, o);
-        }
-    }
-}
-
-// The grouped-table forward with four channels per lane (128 per warp): twice the warps of radon_forward_gtable, for
-// launches of few angles (an omega subset), which would leave the 8-channel kernel's last wave mostly empty. Same
-// entries, weights and order per channel, the same paired FMAs: the same bits.
-__device__ __forceinline__ void acc4(float (&a)[4], float w, const float4 &p)
-{
-    const float2 ww = make_float2(w, w);
-    float2 r0 = __ffma2_rn(ww, make_float2(p.x, p.y), make_float2(a[0], a[1]));
-    float2 r1 = __ffma2_rn(ww, make_float2(p.z, p.w), make_float2(a[2], a[3]));
-    a[0] = r0.x; a[1] = r0.y; a[2] = r1.x; a[3] = r1.y;
-}
-
-__global__ void __launch_bounds__(32 * WARPS) radon_forward_gtable4(
-    const float *__restrict__ img, float *__restrict__ sino, const int32_t *__restrict__ row_ptr,
-    const int32_t *__restrict__ pix, const float4 *__restrict__ wts, const int32_t *__restrict__ angles, int ns,
-    int kstride, int kb, float scale)
-{
-    constexpr int U = 4, C4 = 4, CW = 32 * C4;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ng = (ns + GB - 1) / GB;
-    const int grp = blockIdx.x * WARPS + warp;
-    const int al = blockIdx.y;
-    const int k = blockIdx.z * CW + lane * C4;
-    if (grp >= ng) return;
-    const bool live = k < kstride;
-    const int s0 = grp * GB;
-    float *out = sino + ((int64_t)al * ns + s0) * kstride + k;
-    const int nb = min(GB, ns - s0);
-    if (blockIdx.z * CW >= kb) {
-        if (live)
-            for (int j = 0; j < nb; ++j)
-                *reinterpret_cast<float4 *>(out + (int64_t)j * kstride) = make_float4(0.f, 0.f, 0.f, 0.f);
-        return;
-    }
-    const bool load = k < kb;
-    const int a = angles ? __ldg(angles + al) : al;
-    const int64_t r = (int64_t)a * ng + grp;
-    int e = __ldg(row_ptr + r);
-    const int e1 = __ldg(row_ptr + r + 1);
-    const float *base = img + (load ? k : 0);
-    float acc[GB][C4];
-#pragma unroll
-    for (int j = 0; j < GB; ++j)
-#pragma unroll
-        for (int c = 0; c < C4; ++c) acc[j][c] = 0.0f;
-    for (; e + U <= e1; e += U) {
-        int p[U];
-        float4 w[U], q[U];
-#pragma unroll
-        for (int i = 0; i < U; ++i) {
-            p[i] = __ldg(pix + e + i);
-            w[i] = __ldg(wts + e + i);
-        }
-#pragma unroll
-        for (int i = 0; i < U; ++i)
-            q[i] = load ? __ldg(reinterpret_cast<const float4 *>(base + (int64_t)p[i] * kstride))
-                        : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-        for (int i = 0; i < U; ++i) {
-            if (w[i].x != 0.0f) acc4(acc[0], w[i].x, q[i]);
-            if (w[i].y != 0.0f) acc4(acc[1], w[i].y, q[i]);
-            if (w[i].z != 0.0f) acc4(acc[2], w[i].z, q[i]);
-            if (w[i].w != 0.0f) acc4(acc[3], w[i].w, q[i]);
-        }
-    }
-    for (; e < e1; ++e) {
-        const int p = __ldg(pix + e);
-        const float4 w = __ldg(wts + e);
-        const float4 q = load ? __ldg(reinterpret_cast<const float4 *>(base + (int64_t)p * kstride))
-                              : make_float4(0.f, 0.f, 0.f, 0.f);
-        if (w.x != 0.0f) acc4(acc[0], w.x, q);
-        if (w.y != 0.0f) acc4(acc[1], w.y, q);
-        if (w.z != 0.0f) acc4(acc[2], w.z, q);
-        if (w.w != 0.0f) acc4(acc[3], w.w, q);
-    }
-    if (!live) return;
-#pragma unroll
-    for (int j = 0; j < GB; ++j) {
-        if (j >= nb) break;
-        float o[C4];
-#pragma unroll
-        for (int c = 0; c < C4; ++c) o[c] = (k + c < kb) ? __fmul_rn(scale, acc[j][c]) : 0.0f;
-        *reinterpret_cast<float4 *>(out + (int64_t)j * kstride) = make_float4(o[0], o[1], o[2], o[3]);
-    }
-}
-
-// The grouped-table forward of a BF16 image into BF16 sinogram rows of stride sld (the BF16 passes' Z columns): four
-// channels per lane (8-byte loads, widened exactly), float32 sums of the per-bin rows' taps in their order, rounded
-// once on store: dfx_radon_forward_table_bf16_bf16's bits.
-__global__ void __launch_bounds__(32 * WARPS) radon_forward_gtable4_bb(
-    const __nv_bfloat16 *__restrict__ img, __nv_bfloat16 *__restrict__ sino, int64_t sld,
-    const int32_t *__restrict__ row_ptr, const int32_t *__restrict__ pix, const float4 *__restrict__ wts,
-    const int32_t *__restrict__ angles, int ns, int kstride, int kb, float scale)
-{
-    constexpr int U = 8, C4 = 4, CW = 32 * C4;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ng = (ns + GB - 1) / GB;
-    const int grp = blockIdx.x * WARPS + warp;
-    const int al = blockIdx.y;
-    const int k = blockIdx.z * CW + lane * C4;
-    if (grp >= ng) return;
-    const bool live = k < kstride;
-    const int s0 = grp * GB;
-    __nv_bfloat16 *out = sino + ((int64_t)al * ns + s0) * sld + k;
-    const int nb = min(GB, ns - s0);
-    if (blockIdx.z * CW >= kb) {
-        if (live)
-            for (int j = 0; j < nb; ++j) *reinterpret_cast<uint2 *>(out + (int64_t)j * sld) = make_uint2(0, 0);
-        return;
-    }
-    const bool load = k < kb;
-    const int a = angles ? __ldg(angles + al) : al;
-    const int64_t r = (int64_t)a * ng + grp;
-    int e = __ldg(row_ptr + r);
-    const int e1 = __ldg(row_ptr + r + 1);
-    const __nv_bfloat16 *base = img + (load ? k : 0);
-    float acc[GB][C4];
-#pragma unroll
-    for (int j = 0; j < GB; ++j)
-#pragma unroll
-        for (int c = 0; c < C4; ++c) acc[j][c] = 0.0f;
-    auto widen = [](uint2 u) {
-        return make_float4(bf_lo(u.x), bf_hi(u.x), bf_lo(u.y), bf_hi(u.y));
-    };
-    for (; e + U <= e1; e += U) {
-        int p[U];
-        float4 w[U];
-        uint2 q[U];
-#pragma unroll
-        for (int i = 0; i < U; ++i) {
-            p[i] = __ldg(pix + e + i);
-            w[i] = __ldg(wts + e + i);
-        }
-#pragma unroll
-        for (int i = 0; i < U; ++i)
-            q[i] = load ? __ldg(reinterpret_cast<const uint2 *>(base + (int64_t)p[i] * kstride)) : make_uint2(0, 0);
-#pragma unroll
-        for (int i = 0; i < U; ++i) {
-            const float4 x = widen(q[i]);
-            if (w[i].x != 0.0f) acc4(acc[0], w[i].x, x);
-            if (w[i].y != 0.0f) acc4(acc[1], w[i].y, x);
-            if (w[i].z != 0.0f) acc4(acc[2], w[i].z, x);
-            if (w[i].w != 0.0f) acc4(acc[3], w[i].w, x);
-        }
-    }
-    for (; e < e1; ++e) {
-        const int p = __ldg(pix + e);
-        const float4 w = __ldg(wts + e);
-        const float4 x = widen(load ? __ldg(reinterpret_cast<const uint2 *>(base + (int64_t)p * kstride))
-                                    : make_uint2(0, 0));
-        if (w.x != 0.0f) acc4(acc[0], w.x, x);
-        if (w.y != 0.0f) acc4(acc[1], w.y, x);
-        if (w.z != 0.0f) acc4(acc[2], w.z, x);
-        if (w.w != 0.0f) acc4(acc[3], w.w, x);
-    }
-    if (!live) return;
-#pragma unroll
-    for (int j = 0; j < GB; ++j) {
-        if (j >= nb) break;
-        float o[C4];
-#pragma unroll
-        for (int c = 0; c < C4; ++c) o[c] = (k + c < kb) ? __fmul_rn(scale, acc[j][c]) : 0.0f;
-        *reinterpret_cast<uint2 *>(out + (int64_t)j * sld) = make_uint2(pack_bf16(o[0], o[1]), pack_bf16(o[2], o[3]));
-    }
-}
-
 // ------------------------------------------------------------------------------------------------ backward
 // SPDHG primal step of one coefficient: the operations of primal_update_kernel (solver.cu), bitwise
 __device__ __forceinline__ void primal_step(float &x, float &z, float t, float dz, float inv_p, float lam)
@@ -881,124 +529,6 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
     }
 }
 
-// Four neighbouring pixels per warp (flat indices 4 w .. 4 w + 3, a row's neighbours when nx is a multiple of 4):
-// per angle their taps cover a few adjacent bins, so each bin row in the union of their taps is loaded once and added
-// to every pixel whose taps include it. Per pixel the taps, weights and their order are those of radon_backward_v3
-// (the two-tap case adds both taps, the general case skips zero weights and bins off the detector), so the sums are
-// its bits, with about half of its loads through L1.
-template <int KERNEL, int MODE, typename ST>
-__global__ void __launch_bounds__(32 * WARPS) radon_backward_q4(
-    const ST *__restrict__ sino, int64_t sld, float *__restrict__ img, const float4 *__restrict__ geo, int n_angles,
-    int nx, int npix, int ns, int kstride, int kb, int n_taps, float *__restrict__ z, const float *__restrict__ T,
-    float inv_p, float lam, __nv_bfloat16 *__restrict__ xb)
-{
-    constexpr int NP = 4;
-    extern __shared__ AngleParams prm[];
-    for (int i = threadIdx.x; i < n_angles; i += blockDim.x) prm[i] = pack_geo(load_geo(geo, i));
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t p0 = ((int64_t)blockIdx.x * WARPS + warp) * NP;
-    const int k = blockIdx.y * CPW + lane * CPL;
-    if (p0 >= npix || k >= kstride) return;
-    const int np = (int)min((int64_t)NP, (int64_t)npix - p0);
-    if (blockIdx.y * CPW >= kb) {          // a block of padding channels only
-        if (MODE == 0) {
-            const float zero[CPL] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            for (int j = 0; j < np; ++j) st8(img + (p0 + j) * kstride + k, zero);
-        }
-        return;
-    }
-    float fx[NP], fy[NP];
-#pragma unroll
-    for (int j = 0; j < NP; ++j) {
-        const int64_t pix = p0 + min(j, np - 1);
-        fx[j] = (float)(int)(pix % nx);
-        fy[j] = (float)(int)(pix / nx);
-    }
-    float acc[NP][CPL];
-#pragma unroll
-    for (int j = 0; j < NP; ++j)
-#pragma unroll
-        for (int c = 0; c < CPL; ++c) acc[j][c] = 0.0f;
-    const ST *col = sino + k;
-    const int64_t angle_stride = (int64_t)ns * sld;
-    for (int a = 0; a < n_angles; ++a, col += angle_stride) {
-        const AngleGeo g = unpack_geo(prm[a]);
-        const int ntap = taps_of(g, KERNEL, n_taps);
-        float t[NP];
-        int sf[NP];
-        bool fast[NP];
-        int lo = 0x7fffffff, hi = -0x7fffffff;
-#pragma unroll
-        for (int j = 0; j < NP; ++j) {
-            t[j] = __fmaf_rn(g.A, g.rows_are_y ? fx[j] : fy[j], __fmaf_rn(g.B, g.rows_are_y ? fy[j] : fx[j], g.T0));
-            sf[j] = first_tap<KERNEL>(g, t[j]);
-            fast[j] = ntap == 2 && sf[j] >= 0 && sf[j] + 1 < ns;
-            if (j < np) {
-                lo = min(lo, sf[j]);
-                hi = max(hi, sf[j] + ntap - 1);
-            }
-        }
-        lo = max(lo, 0);
-        hi = min(hi, ns - 1);
-        for (int sb = lo; sb <= hi; ++sb) {
-            float w[NP];
-            bool use[NP];
-            bool any = false;
-#pragma unroll
-            for (int j = 0; j < NP; ++j) {
-                use[j] = false;
-                w[j] = 0.0f;
-                const int d = sb - sf[j];
-                if (j < np && d >= 0 && d < ntap) {
-                    const float wt = tap_weight<KERNEL>(g, __fsub_rn(t[j], (float)sb));
-                    if (fast[j] || wt != 0.0f) {
-                        use[j] = true;
-                        w[j] = __fmul_rn(g.w, wt);
-                        any = true;
-                    }
-                }
-            }
-            if (!any) continue;
-            float4 q0, q1;
-            ld8(col + (int64_t)sb * sld, q0, q1);
-#pragma unroll
-            for (int j = 0; j < NP; ++j)
-                if (use[j]) acc8(acc[j], w[j], q0, q1);
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < NP; ++j) {
-        if (j >= np) break;
-        const int64_t o = (p0 + j) * kstride + k;
-        if (MODE == 0) {
-            float r[CPL];
-#pragma unroll
-            for (int c = 0; c < CPL; ++c) r[c] = (k + c < kb) ? acc[j][c] : 0.0f;
-            float4 *d = reinterpret_cast<float4 *>(img + o);
-            d[0] = make_float4(r[0], r[1], r[2], r[3]);
-            d[1] = make_float4(r[4], r[5], r[6], r[7]);
-        } else {
-            float xn[CPL];
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                float4 *xp = reinterpret_cast<float4 *>(img + o) + q;
-                float4 *zp = reinterpret_cast<float4 *>(z + o) + q;
-                float4 xv = *xp, zv = *zp;
-                const float4 tv = __ldg(reinterpret_cast<const float4 *>(T + o) + q);
-                primal_step(xv.x, zv.x, tv.x, (k + 4 * q + 0 < kb) ? acc[j][4 * q + 0] : 0.0f, inv_p, lam);
-                primal_step(xv.y, zv.y, tv.y, (k + 4 * q + 1 < kb) ? acc[j][4 * q + 1] : 0.0f, inv_p, lam);
-                primal_step(xv.z, zv.z, tv.z, (k + 4 * q + 2 < kb) ? acc[j][4 * q + 2] : 0.0f, inv_p, lam);
-                primal_step(xv.w, zv.w, tv.w, (k + 4 * q + 3 < kb) ? acc[j][4 * q + 3] : 0.0f, inv_p, lam);
-                *xp = xv;
-                *zp = zv;
-                xn[4 * q] = xv.x; xn[4 * q + 1] = xv.y; xn[4 * q + 2] = xv.z; xn[4 * q + 3] = xv.w;
-            }
-            if (xb) st8(xb + o, xn);
-        }
-    }
-}
-
 // ------------------------------------------------------------------------------------------------ batch helpers
 // Element-wise on channel-fastest batches (npix, kstride) whose channels kb .. kstride-1 are padding:
 // mode 0: x = 1 inside the support on live channels, else 0 (support_ones); mode 1: x = 0 outside the support, on
@@ -1094,29 +624,12 @@ static int allow_smem(Kernel kernel, size_t bytes)
     return DFX_OK;
 }
 
-// the whole-image SIMT backprojection with four pixels per warp (radon_backward_q4; dfx_radon_backward_quads): off by
-// default, at ti256 it took 0.75 ms per launch with the primal step against 0.65 ms for two channel groups per warp
-static bool backward_quads = false;
-
 template <int KERNEL, int MODE, typename ST>
 static int launch_backward(const ST *sino, int64_t sld, float *img, const float *geo, int n_angles, int nx, int ny,
                            int n_det, int kstride, int kb, int n_taps, float *z, const float *T, float inv_p, float lam,
                            __nv_bfloat16 *xb, void *stream, const int32_t *plist = nullptr, int64_t n_list = 0)
 {
     const int64_t npix = plist ? n_list : (int64_t)nx * ny;
-    if (!plist && backward_quads) {
-        // four neighbouring pixels per warp share their bin loads (radon_backward_q4)
-        dim3 grid((unsigned)cdiv(npix, 4 * WARPS), (unsigned)cdiv(kstride, CPW));
-        DFX_REQUIRE(grid.x < 2147483647u && grid.y <= 65535u, "radon: batch too large for one launch");
-        const size_t smem = sizeof(AngleParams) * (size_t)(n_angles > 0 ? n_angles : 1);
-        DFX_REQUIRE(smem <= 200 * 1024, "radon: %d angles exceed the shared memory of one launch", n_angles);
-        int st = allow_smem(radon_backward_q4<KERNEL, MODE, ST>, smem);
-        if (st) return st;
-        radon_backward_q4<KERNEL, MODE, ST><<<grid, 32 * WARPS, smem, (cudaStream_t)stream>>>(
-            sino, sld, img, reinterpret_cast<const float4 *>(geo), n_angles, nx, (int)npix, n_det, kstride, kb, n_taps,
-            z, T, inv_p, lam, xb);
-        return launch_status(MODE ? "radon_backward_spdhg" : "radon_backward");
-    }
     // two channel groups per warp once the batch has more than one (fewer, longer warps: the taps of a pixel are
     // evaluated once for 16 channels per lane)
     const bool pair = kstride > CPW;
@@ -1303,13 +816,6 @@ extern "C" int dfx_radon_table_fill(const float *geo, int n_angles, int nx, int 
     return launch_status("radon_table_fill");
 }
 
-extern "C" int dfx_radon_backward_quads(int on)
-{
-    const int was = backward_quads ? 1 : 0;
-    if (on >= 0) backward_quads = on != 0;
-    return was;
-}
-
 extern "C" int dfx_radon_gtable_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
                                       const uint8_t *supp, int32_t *counts, void *stream)
 {
@@ -1346,61 +852,6 @@ extern "C" int dfx_radon_gtable_fill(const float *geo, int n_angles, int nx, int
     return launch_status("radon_gtable_fill");
 }
 
-extern "C" int dfx_radon_ptable_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
-                                      const uint8_t *supp, int32_t *counts, void *stream)
-{
-    DFX_REQUIRE(geo && counts && ((uintptr_t)geo % 16) == 0, "radon_ptable: null or misaligned pointer");
-    DFX_REQUIRE(n_angles > 0 && nx > 0 && ny > 0 && n_det > 0 && (kernel == 0 || kernel == 1),
-                "radon_ptable: bad sizes or kernel");
-    const int64_t rows = (int64_t)cdiv(n_angles, 2) * cdiv(n_det, GB);
-    DFX_REQUIRE(cdiv(rows, 128) < 2147483647LL, "radon_ptable: too many rows");
-    if (kernel == 1)
-        ray_ptable_kernel<1><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
-            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, counts, nullptr, nullptr, nullptr);
-    else
-        ray_ptable_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
-            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, counts, nullptr, nullptr, nullptr);
-    return launch_status("radon_ptable_count");
-}
-
-extern "C" int dfx_radon_ptable_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel,
-                                     const uint8_t *supp, const int32_t *row_ptr, int32_t *pixels, float *weights,
-                                     void *stream)
-{
-    DFX_REQUIRE(geo && row_ptr && pixels && weights && ((uintptr_t)geo % 16) == 0 && ((uintptr_t)weights % 16) == 0,
-                "radon_ptable: null or misaligned pointer");
-    DFX_REQUIRE(n_angles > 0 && nx > 0 && ny > 0 && n_det > 0 && (kernel == 0 || kernel == 1),
-                "radon_ptable: bad sizes or kernel");
-    const int64_t rows = (int64_t)cdiv(n_angles, 2) * cdiv(n_det, GB);
-    float4 *w = reinterpret_cast<float4 *>(weights);
-    if (kernel == 1)
-        ray_ptable_kernel<1><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
-            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, nullptr, row_ptr, pixels, w);
-    else
-        ray_ptable_kernel<0><<<(unsigned)cdiv(rows, 128), 128, 0, (cudaStream_t)stream>>>(
-            reinterpret_cast<const float4 *>(geo), n_angles, nx, ny, n_det, supp, nullptr, row_ptr, pixels, w);
-    return launch_status("radon_ptable_fill");
-}
-
-extern "C" int dfx_radon_forward_ptable(const float *img_k, float *sino_k, const int32_t *row_ptr,
-                                        const int32_t *pixels, const float *weights, int n_angles, int n_det,
-                                        int kstride, int kb, float scale, void *stream)
-{
-    DFX_REQUIRE(img_k && sino_k && row_ptr && pixels && weights, "radon_forward_ptable: null pointer");
-    DFX_REQUIRE(((uintptr_t)img_k % 16) == 0 && ((uintptr_t)sino_k % 16) == 0 && ((uintptr_t)weights % 16) == 0,
-                "radon_forward_ptable: misaligned arrays");
-    DFX_REQUIRE(n_angles >= 0 && cdiv(n_angles, 2) <= 65535 && n_det > 0, "radon_forward_ptable: bad sizes");
-    DFX_REQUIRE(kstride > 0 && kstride % CPL == 0 && kb >= 0 && kb <= kstride && cdiv(kstride, CPW) <= 65535,
-                "radon_forward_ptable: kstride (%d) must be a positive multiple of %d and kb (%d) <= kstride",
-                kstride, CPL, kb);
-    if (n_angles == 0) return DFX_OK;
-    dim3 grid((unsigned)cdiv(cdiv(n_det, GB), WARPS), (unsigned)cdiv(n_angles, 2), (unsigned)cdiv(kstride, CPW));
-    radon_forward_ptable<<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
-        img_k, sino_k, row_ptr, pixels, reinterpret_cast<const float4 *>(weights), n_angles, n_det, kstride, kb,
-        scale);
-    return launch_status("radon_forward_ptable");
-}
-
 extern "C" int dfx_radon_forward_gtable(const float *img_k, float *sino_k, const int32_t *row_ptr,
                                         const int32_t *pixels, const float *weights, const int32_t *angles,
                                         int n_angles, int n_det, int kstride, int kb, float scale, void *stream)
@@ -1413,16 +864,6 @@ extern "C" int dfx_radon_forward_gtable(const float *img_k, float *sino_k, const
                 "radon_forward_gtable: kstride (%d) must be a positive multiple of %d and kb (%d) <= kstride",
                 kstride, CPL, kb);
     if (n_angles == 0) return DFX_OK;
-    // four channels per lane when eight would give fewer than about five waves of warps (few angles)
-    const int64_t warps8 = (int64_t)cdiv(n_det, GB) * n_angles * cdiv(kstride, CPW);
-    if (warps8 < 16384 && kstride % 4 == 0) {
-        DFX_REQUIRE(cdiv(kstride, 128) <= 65535, "radon_forward_gtable: kstride too large for one launch");
-        dim3 grid((unsigned)cdiv(cdiv(n_det, GB), WARPS), (unsigned)n_angles, (unsigned)cdiv(kstride, 128));
-        radon_forward_gtable4<<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
-            img_k, sino_k, row_ptr, pixels, reinterpret_cast<const float4 *>(weights), angles, n_det, kstride, kb,
-            scale);
-        return launch_status("radon_forward_gtable");
-    }
     dim3 grid((unsigned)cdiv(cdiv(n_det, GB), WARPS), (unsigned)n_angles, (unsigned)cdiv(kstride, CPW));
     radon_forward_gtable<<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
         img_k, sino_k, row_ptr, pixels, reinterpret_cast<const float4 *>(weights), angles, n_det, kstride, kb, scale);
@@ -1470,28 +911,6 @@ extern "C" int dfx_radon_forward_table_bf16_bf16(const void *img_bf16, void *sin
     return radon_forward_table_any(reinterpret_cast<const __nv_bfloat16 *>(img_bf16),
                                    reinterpret_cast<__nv_bfloat16 *>(sino_bf16), sino_ld, row_ptr, entries, angles,
                                    n_angles, n_det, kstride, kb, scale, stream);
-}
-
-extern "C" int dfx_radon_forward_gtable_bf16_bf16(const void *img_bf16, void *sino_bf16, int64_t sino_ld,
-                                                  const int32_t *row_ptr, const int32_t *pixels, const float *weights,
-                                                  const int32_t *angles, int n_angles, int n_det, int kstride, int kb,
-                                                  float scale, void *stream)
-{
-    DFX_REQUIRE(img_bf16 && sino_bf16 && row_ptr && pixels && weights, "radon_forward_gtable_bf16: null pointer");
-    DFX_REQUIRE(((uintptr_t)img_bf16 % 16) == 0 && ((uintptr_t)sino_bf16 % 8) == 0 && ((uintptr_t)weights % 16) == 0,
-                "radon_forward_gtable_bf16: misaligned arrays");
-    DFX_REQUIRE(n_angles >= 0 && n_angles <= 65535 && n_det > 0, "radon_forward_gtable_bf16: bad sizes");
-    DFX_REQUIRE(kstride > 0 && kstride % CPL == 0 && kb >= 0 && kb <= kstride && cdiv(kstride, 128) <= 65535,
-                "radon_forward_gtable_bf16: kstride (%d) must be a positive multiple of %d and kb (%d) <= kstride",
-                kstride, CPL, kb);
-    DFX_REQUIRE(sino_ld >= kstride && sino_ld % CPL == 0, "radon_forward_gtable_bf16: sinogram row stride (%lld) "
-                "must be a multiple of %d >= kstride", (long long)sino_ld, CPL);
-    if (n_angles == 0) return DFX_OK;
-    dim3 grid((unsigned)cdiv(cdiv(n_det, GB), WARPS), (unsigned)n_angles, (unsigned)cdiv(kstride, 128));
-    radon_forward_gtable4_bb<<<grid, 32 * WARPS, 0, (cudaStream_t)stream>>>(
-        reinterpret_cast<const __nv_bfloat16 *>(img_bf16), reinterpret_cast<__nv_bfloat16 *>(sino_bf16), sino_ld,
-        row_ptr, pixels, reinterpret_cast<const float4 *>(weights), angles, n_det, kstride, kb, scale);
-    return launch_status("radon_forward_gtable_bf16");
 }
 
 extern "C" int dfx_batch_support(float *x_k, const float *colsum_k, const uint8_t *supp, int64_t npix, int kstride,

@@ -402,103 +402,6 @@ __global__ void __launch_bounds__(SP_ROWS) spmm_forward_b4_kernel(
     }
 }
 
-// Forward over the blocked rows with the lanes on detector lines: a block owns one angle, 32 lines and WL_CB eta
-// blocks of every ring; warp p walks ring p's WL_CB block rows together (one entry of each in turn, the next entry's
-// loads in flight meanwhile), every lane applying an entry's four values to its own line's staged Z column (the
-// entry is the same for the whole warp: one broadcast load, conflict-free shared-memory reads). The block's outputs
-// (32 lines x WL_CB x 4 eta bins x P rings, a contiguous stretch of each data line) go through shared memory and are
-// added to the data rows line by line. Per output the same fmaf chain over k ascending as the CSR product: its bits.
-constexpr int WL_LINES = 32;
-constexpr int WL_CB = 8;                  // eta blocks (of four bins) per block and ring
-constexpr int WL_CHUNK = 256;             // orientations staged per pass
-constexpr int WL_LD = WL_LINES + 1;       // staged column stride (bank = column + lane)
-
-__global__ void __launch_bounds__(512) spmm_forward_wl_kernel(
-    const float *__restrict__ sino, const int32_t *__restrict__ fb_ptr, const uint16_t *__restrict__ fb_k,
-    const float4 *__restrict__ fb_v, const uint8_t *__restrict__ fb_mask, float *__restrict__ data,
-    const int32_t *__restrict__ omegas, int my, int P, int C, int ncb, int kstride, int kb)
-{
-    extern __shared__ float wl_sm[];
-    const int seg = WL_CB * FB_W * P;                      // output segments of the block per line
-    const int seg_ld = seg | 1;                            // odd stride: lanes (lines) on distinct banks
-    float *tile = wl_sm;                                   // [WL_CHUNK][WL_LD]
-    float *outb = tile + WL_CHUNK * WL_LD;                 // [WL_LINES][seg_ld]
-    uint8_t *flag = reinterpret_cast<uint8_t *>(outb + WL_LINES * seg_ld);   // [seg]: output written
-    const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;                  // warp = ring
-    const int cb0 = blockIdx.x * WL_CB, y0 = blockIdx.y * WL_LINES, s = blockIdx.z;
-    const int r = omegas ? __ldg(omegas + s) : s;
-    const int ny = min(WL_LINES, my - y0), per_angle = P * ncb;
-    const int nthr = blockDim.x;
-    for (int i = threadIdx.x; i < seg; i += nthr) flag[i] = 0;
-    int pos[WL_CB], end[WL_CB], kc[WL_CB];
-    float4 vc[WL_CB];
-    float acc[WL_CB][FB_W];
-#pragma unroll
-    for (int b = 0; b < WL_CB; ++b) {
-        const int cb = cb0 + b;
-        pos[b] = end[b] = 0;
-        if (cb < ncb) {
-            const int64_t g = (int64_t)r * per_angle + (int64_t)cb * P + p;
-            pos[b] = __ldg(fb_ptr + g);
-            end[b] = __ldg(fb_ptr + g + 1);
-        }
-        kc[b] = pos[b] < end[b] ? (int)__ldg(fb_k + pos[b]) : 0x7fffffff;
-        vc[b] = pos[b] < end[b] ? __ldg(fb_v + pos[b]) : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-        for (int u = 0; u < FB_W; ++u) acc[b][u] = 0.0f;
-    }
-    const float *zl = sino + ((int64_t)s * my + y0) * kstride;
-    for (int c0 = 0; c0 < kb; c0 += WL_CHUNK) {
-        const int cn = min(WL_CHUNK, kb - c0), c_end = c0 + cn;
-        if (c0) __syncthreads();
-        for (int idx = threadIdx.x; idx < WL_LINES * cn; idx += nthr) {
-            const int t = idx / cn, c = idx - t * cn;
-            tile[c * WL_LD + t] = t < ny ? __ldg(zl + (int64_t)t * kstride + c0 + c) : 0.0f;
-        }
-        __syncthreads();
-        bool more = true;
-        while (more) {
-            more = false;
-#pragma unroll
-            for (int b = 0; b < WL_CB; ++b) {
-                if (kc[b] >= c_end) continue;                      // the whole warp agrees (same row)
-                const float x = tile[(kc[b] - c0) * WL_LD + lane];
-                const float4 v = vc[b];
-                ++pos[b];
-                kc[b] = pos[b] < end[b] ? (int)__ldg(fb_k + pos[b]) : 0x7fffffff;
-                vc[b] = pos[b] < end[b] ? __ldg(fb_v + pos[b]) : make_float4(0.f, 0.f, 0.f, 0.f);
-                acc[b][0] = __fmaf_rn(v.x, x, acc[b][0]);
-                acc[b][1] = __fmaf_rn(v.y, x, acc[b][1]);
-                acc[b][2] = __fmaf_rn(v.z, x, acc[b][2]);
-                acc[b][3] = __fmaf_rn(v.w, x, acc[b][3]);
-                more = true;
-            }
-        }
-    }
-    // outputs: segment (4 cb + u) P + p of the line, relative to the block's first (4 cb0 P)
-#pragma unroll
-    for (int b = 0; b < WL_CB; ++b) {
-        const int cb = cb0 + b;
-        if (cb >= ncb) break;
-        const int m = __ldg(fb_mask + (int64_t)r * per_angle + (int64_t)cb * P + p);
-#pragma unroll
-        for (int u = 0; u < FB_W; ++u) {
-            if (!((m >> u) & 1)) continue;
-            const int j = (FB_W * b + u) * P + p;
-            outb[lane * seg_ld + j] = acc[b][u];
-            if (lane == 0) flag[j] = 1;
-        }
-    }
-    __syncthreads();
-    const int cp = C * P;
-    const int j_end = min(seg, cp - FB_W * cb0 * P);
-    for (int t = 0; t < ny; ++t) {
-        float *dl = data + ((int64_t)r * my + y0 + t) * cp + (int64_t)FB_W * cb0 * P;
-        for (int j = threadIdx.x; j < j_end; j += nthr)
-            if (flag[j]) dl[j] += outb[t * seg_ld + j];
-    }
-}
-
 }  // namespace dfx
 
 using namespace dfx;
@@ -535,30 +438,6 @@ extern "C" int dfx_spmm_pf_adjoint(const float *data, const int32_t *row_ptr, co
     spmm_adjoint8_kernel<<<grid, AJ_ROWS, smem, (cudaStream_t)stream>>>(data, row_ptr, col_j, val, sino, omegas, my,
                                                                         kb, cp, kstride, alpha, compact, chunk);
     return launch_status("spmm_pf_adjoint");
-}
-
-extern "C" int dfx_spmm_pf_forward_lines(const float *sino, const int32_t *fb_ptr, const uint16_t *fb_k,
-                                         const float *fb_v, const uint8_t *fb_mask, float *data, const int32_t *omegas,
-                                         int n_sub, int my, int P, int C, int kstride, int kb, void *stream)
-{
-    DFX_REQUIRE(sino && fb_ptr && fb_k && fb_v && fb_mask && data, "spmm_forward_lines: null pointer");
-    DFX_REQUIRE(((uintptr_t)fb_v % 16) == 0, "spmm_forward_lines: the values must be 16-byte aligned");
-    DFX_REQUIRE(n_sub > 0 && my > 0 && C > 0 && kb > 0 && kb <= kstride, "spmm_forward_lines: bad sizes");
-    DFX_REQUIRE(P >= 1 && P <= 16, "spmm_forward_lines: %d rings (one warp per ring, at most 16)", P);
-    const int ncb = (int)cdiv(C, FB_W);
-    DFX_REQUIRE(n_sub <= 65535 && cdiv(my, WL_LINES) <= 65535, "spmm_forward_lines: grid too large");
-    const int seg = WL_CB * FB_W * P;
-    const size_t smem = sizeof(float) * ((size_t)WL_CHUNK * WL_LD + (size_t)WL_LINES * (seg | 1)) + seg;
-    const cudaError_t e = allow_max_dynamic_smem(spmm_forward_wl_kernel);
-    if (e != cudaSuccess) {
-        set_error("spmm_forward_lines: shared memory attribute: %s", cudaGetErrorString(e));
-        return DFX_ELAUNCH;
-    }
-    dim3 grid((unsigned)cdiv(ncb, WL_CB), (unsigned)cdiv(my, WL_LINES), (unsigned)n_sub);
-    spmm_forward_wl_kernel<<<grid, 32 * P, smem, (cudaStream_t)stream>>>(
-        sino, fb_ptr, fb_k, reinterpret_cast<const float4 *>(fb_v), fb_mask, data, omegas, my, P, C, ncb, kstride,
-        kb);
-    return launch_status("spmm_pf_forward_lines");
 }
 
 extern "C" int64_t dfx_pf_fblock_rows(int n_angles, int P, int C)

@@ -454,7 +454,6 @@ def set_proj_parameters(op, cor=None, shift=None):
         op.geo_gpu = torch.as_tensor(rg.geo, device=op.device)
         op._ray_rp, op._ray_ent, op.ray_taps = op._build_ray_table()
         op._ray_grp = op._build_group_table()
-        op._ray_pair = op._build_group_table(pairs=True)
         op._tcf_tab = None
         op._ray_supp = {}
         op.release_streamer()

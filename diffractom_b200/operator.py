@@ -36,6 +36,7 @@ AUTO_FFT_PIXELS = 400 * 400   # projector="auto": the Fourier-slice projector fo
 SPARSE_MIN_BATCHES = 4    # sparse modes: at least this many batches (SPFO:135)
 CAND_BYTES = 2 + 4 + 4 + 4 + 4          # per candidate / non-zero scratch of the reference's generator
 NNZ_BYTES = 2 + 4 + 4 + 2 + 4 + 2 + 4   # (pf_generate.py:29-30), used by the batch-size rule
+GTABLE_MIN_ANGLES = 64                   # float32 forwards of this many angles read the grouped table
 KSTRIDE_ALIGN = 16                       # channel stride of the batch buffers (16 channels per tensor-memory load)
 
 
@@ -55,9 +56,6 @@ class SinglePhaseForwardOperator:
     # with both CSR copies stored, the forward products run over an eta-blocked copy of the forward CSR (four
     # neighbouring eta bins of a ring per entry; the same sums bit for bit); False: over the forward CSR itself
     forward_blocks = True
-    # the blocked forward with the lanes on detector lines (dfx_spmm_pf_forward_lines; the same bits); False: one
-    # block row per thread (dfx_spmm_pf_forward_blocked)
-    forward_lines = True
 
     def __init__(self, cfg: Mapping[str, Any], material, grid, max_gb: float, verbose: bool = False,
                  normalized: bool = False, ctx=None, queue=None, pf_mode: str = "auto", sparse_max_fill: float = 0.3,
@@ -156,13 +154,12 @@ class SinglePhaseForwardOperator:
             self._supp_tiles = {}
             self._fft = None
             if self.projector == "fft":
-                self._ray_rp = self._ray_ent = self._ray_grp = self._ray_pair = None
+                self._ray_rp = self._ray_ent = self._ray_grp = None
                 self.ray_taps = 0
                 self._build_fourier()
             else:
                 self._ray_rp, self._ray_ent, self.ray_taps = self._build_ray_table()
                 self._ray_grp = self._build_group_table()
-                self._ray_pair = self._build_group_table(pairs=True)
             self.omega_subsets = None
             self._sub = []
             self._streamer = None
@@ -293,18 +290,16 @@ class SinglePhaseForwardOperator:
                    rp.data_ptr(), ent.data_ptr(), s)
         return rp, ent, total
 
-    def _build_group_table(self, supp=None, pairs=False):
-        """The grouped ray table of the float32 forward (dfx_radon_gtable_*): per (angle, four bins) the pixels that
-        reach them with their four weights, so that each pixel's channels are loaded once per group; the sums are
-        the per-bin table's bits. pairs: the paired table of the forward of all angles (dfx_radon_ptable_*, per
-        pair of consecutive angles and four bins, eight weights). Returns (row_ptr, pixels, weights)."""
+    def _build_group_table(self, supp=None):
+        """The grouped ray table of the float32 forward of many angles (dfx_radon_gtable_*): per (angle, four bins)
+        the pixels that reach them with their four weights, so that each pixel's channels are loaded once per group;
+        the sums are the per-bin table's bits. Returns (row_ptr, pixels, weights)."""
         R, ns = self.N_Omega, self.My
-        kind = "ptable" if pairs else "gtable"
-        n = (-(-R // 2) if pairs else R) * (-(-ns // 4))
+        n = R * (-(-ns // 4))
         s = self._s()
         sp = None if supp is None else supp.data_ptr()
         rp = torch.empty(n + 1, dtype=torch.int32, device=self.device)
-        self._call(f"dfx_radon_{kind}_count", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id, sp,
+        self._call("dfx_radon_gtable_count", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id, sp,
                    rp.data_ptr(), s)
         self.stream().synchronize()
         total = int(rp[:n].to(torch.int64).sum().item())
@@ -314,8 +309,8 @@ class SinglePhaseForwardOperator:
         scr = self.scratch(nb)
         self._call("dfx_scan_exclusive_i32", rp.data_ptr(), rp.data_ptr(), n, scr.data_ptr(), nb, s)
         pix = torch.empty(max(total, 1), dtype=torch.int32, device=self.device)
-        w = torch.empty((max(total, 1), 8 if pairs else 4), dtype=torch.float32, device=self.device)
-        self._call(f"dfx_radon_{kind}_fill", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id, sp,
+        w = torch.empty((max(total, 1), 4), dtype=torch.float32, device=self.device)
+        self._call("dfx_radon_gtable_fill", self.geo_gpu.data_ptr(), R, self.Nx, self.Ny, ns, self._kernel_id, sp,
                    rp.data_ptr(), pix.data_ptr(), w.data_ptr(), s)
         return rp, pix, w
 
@@ -329,8 +324,7 @@ class SinglePhaseForwardOperator:
         key = bytes(supp.cpu().numpy())
         hit = self._ray_supp.get(key)
         if hit is None:
-            hit = self._build_ray_table(supp) + (self._build_group_table(supp),
-                                                 self._build_group_table(supp, pairs=True))
+            hit = self._build_ray_table(supp) + (self._build_group_table(supp),)
             self._ray_supp[key] = hit
         return hit
 
@@ -375,11 +369,9 @@ class SinglePhaseForwardOperator:
         om_ptr = None if om is None else om.data_ptr()
         rp, ent = (self._ray_rp, self._ray_ent) if ray is None else ray[:2]
         grp = self._ray_grp if ray is None else (ray[3] if len(ray) > 3 else None)
-        pair = self._ray_pair if ray is None else (ray[4] if len(ray) > 4 else None)
-        if sld is None and pair is not None and om is None and n_ang == self.N_Omega:
-            self._call("dfx_radon_forward_ptable", src_ptr, dst_ptr, pair[0].data_ptr(), pair[1].data_ptr(),
-                       pair[2].data_ptr(), n_ang, self.My, self.Kstride, kb, float(self.radon_geo.scale), self._s())
-        elif sld is None and grp is not None:
+        # the grouped table has a quarter of the warps: for a few angles (a subset) the per-bin one fills the GPU
+        # better (at 256 x 256, 1024 channels and 18 angles: 0.56 ms per-bin, 0.63 to 0.67 ms grouped)
+        if sld is None and grp is not None and n_ang >= GTABLE_MIN_ANGLES:
             self._call("dfx_radon_forward_gtable", src_ptr, dst_ptr, grp[0].data_ptr(), grp[1].data_ptr(),
                        grp[2].data_ptr(), om_ptr, n_ang, self.My, self.Kstride, kb, float(self.radon_geo.scale),
                        self._s())
@@ -520,9 +512,7 @@ class SinglePhaseForwardOperator:
         s = self._s()
         om_ptr = None if om is None else om.data_ptr()
         if sb.get("fb_ptr") is not None:
-            name = ("dfx_spmm_pf_forward_lines" if self.forward_lines and self.N_peaks <= 16
-                    else "dfx_spmm_pf_forward_blocked")
-            self._call(name, sino_ptr, sb["fb_ptr"].data_ptr(), sb["fb_k"].data_ptr(),
+            self._call("dfx_spmm_pf_forward_blocked", sino_ptr, sb["fb_ptr"].data_ptr(), sb["fb_k"].data_ptr(),
                        sb["fb_v"].data_ptr(), sb["fb_mask"].data_ptr(), data.data_ptr(), om_ptr, n_ang, self.My,
                        self.N_peaks, self.N_eta, self.Kstride, kb, s)
             return
@@ -963,12 +953,6 @@ class SinglePhaseForwardOperator:
                        self.My, self.Kstride, self._kernel_id, int(self.radon_geo.n_taps),
                        float(self.radon_geo.scale), tp, nt, self._s())
             return
-        grp = self._ray_grp if ray is None else (ray[3] if len(ray) > 3 else None)
-        if grp is not None:
-            self._call("dfx_radon_forward_gtable_bf16_bf16", src_ptr, dst_ptr, self.Ktot, grp[0].data_ptr(),
-                       grp[1].data_ptr(), grp[2].data_ptr(), om.data_ptr(), n, self.My, self.Kstride, kb,
-                       float(self.radon_geo.scale), self._s())
-            return
         rp, ent = (self._ray_rp, self._ray_ent) if ray is None else ray[:2]
         self._call("dfx_radon_forward_table_bf16_bf16", src_ptr, dst_ptr, self.Ktot, rp.data_ptr(), ent.data_ptr(),
                    om.data_ptr(), n, self.My, self.Kstride, kb, float(self.radon_geo.scale), self._s())
@@ -1343,7 +1327,7 @@ class SinglePhaseForwardOperator:
         self.release_omega_subsets()
         self.release_streamer()
         self._ray_supp = {}
-        self._ray_grp = self._ray_pair = None
+        self._ray_grp = None
         self._tcf_tab = None
         self._supp_tiles = {}
         self._fft = None

@@ -77,11 +77,6 @@ int dfx_radon_backward_pixels(const float *sino_k, float *img_k, const float *ge
 int dfx_radon_backward_spdhg(const float *sino_k, const float *geo, int n_angles, int nx, int ny, int n_det,
                              int kstride, int kb, int kernel, int n_taps, float *x_k, float *z_k, const float *T_k,
                              float inv_p, float lam, void *stream);
-/* The whole-image SIMT backprojections above (float32 and BF16 sinograms, plain and with the primal step) run four
- * neighbouring pixels per warp, loading each bin row of the union of their taps once (on: 1), or one pixel per warp
- * (0, the default); the sums are the same bits either way. Returns the previous setting; on < 0 only queries it.
- * No reference counterpart (a performance switch of this library, process-wide). */
-int dfx_radon_backward_quads(int on);
 
 /* The three Radon entry points above for the BF16 precision path: the sinogram is BF16 with sino_ld elements between
  * consecutive bins (sino_ld >= kstride, a multiple of 8: the batches of all orientations side by side, the layout of
@@ -128,11 +123,6 @@ int dfx_radon_forward_table_bf16(const float *img_k, void *sino_bf16, int64_t si
 int dfx_radon_forward_table_bf16_bf16(const void *img_bf16, void *sino_bf16, int64_t sino_ld, const int32_t *row_ptr,
                                       const int32_t *entries, const int32_t *angles, int n_angles, int n_det,
                                       int kstride, int kb, float scale, void *stream);
-/* The same through the grouped table (dfx_radon_gtable_*; four channels per lane): each pixel's channels loaded once
- * per four bins, the same sums and roundings: dfx_radon_forward_table_bf16_bf16's bits. */
-int dfx_radon_forward_gtable_bf16_bf16(const void *img_bf16, void *sino_bf16, int64_t sino_ld, const int32_t *row_ptr,
-                                       const int32_t *pixels, const float *weights, const int32_t *angles,
-                                       int n_angles, int n_det, int kstride, int kb, float scale, void *stream);
 
 /* Grouped ray table (no reference counterpart): row a * ceil(n_det / 4) + g lists, in the per-bin rows' order, every
  * pixel that reaches one of the bins 4 g .. 4 g + 3 of angle a, as an int32 pixel index and a float4 of its weights
@@ -147,19 +137,6 @@ int dfx_radon_gtable_fill(const float *geo, int n_angles, int nx, int ny, int n_
 int dfx_radon_forward_gtable(const float *img_k, float *sino_k, const int32_t *row_ptr, const int32_t *pixels,
                              const float *weights, const int32_t *angles, int n_angles, int n_det, int kstride,
                              int kb, float scale, void *stream);
-/* Paired ray table (no reference counterpart), for the forward of all angles: row (i, g) = i * ceil(n_det / 4) + g
- * lists the pixels reaching one of the bins 4 g .. 4 g + 3 of angle 2 i or 2 i + 1, with their eight weights (two
- * float4: angle 2 i, then 2 i + 1; 0 where the per-bin row has no entry), each angle's entries in its per-bin rows'
- * order; count / fill / supp as for the per-bin table (weights: 32 bytes per entry, 16-byte aligned).
- * dfx_radon_forward_ptable: dfx_radon_forward_table of all n_angles angles over it, the same bits, each pixel's
- * channels loaded once for both angles of a pair. */
-int dfx_radon_ptable_count(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel, const uint8_t *supp,
-                           int32_t *counts, void *stream);
-int dfx_radon_ptable_fill(const float *geo, int n_angles, int nx, int ny, int n_det, int kernel, const uint8_t *supp,
-                          const int32_t *row_ptr, int32_t *pixels, float *weights, void *stream);
-int dfx_radon_forward_ptable(const float *img_k, float *sino_k, const int32_t *row_ptr, const int32_t *pixels,
-                             const float *weights, int n_angles, int n_det, int kstride, int kb, float scale,
-                             void *stream);
 
 /* replaces support_ones / project_support / tmin (fista_poisson.py:256-263, 277-281; spdhg_poisson.py:259-265) on a
  * channel-fastest batch (npix, kstride) with padding channels kb .. kstride-1 (supp (npix) uint8 or NULL):
@@ -274,12 +251,6 @@ int dfx_pf_fblock_fill(const int32_t *row_ptr_f, const uint16_t *col_k, const fl
 int dfx_spmm_pf_forward_blocked(const float *sino, const int32_t *fb_ptr, const uint16_t *fb_k, const float *fb_v,
                                 const uint8_t *fb_mask, float *data, const int32_t *omegas, int n_sub, int my, int P,
                                 int C, int kstride, int kb, void *stream);
-/* dfx_spmm_pf_forward_blocked with the work laid out on detector lines (same arguments, same result bit for bit):
- * a block owns one angle, 32 lines and 8 eta blocks of every ring, one warp per ring (P <= 16) walks its 8 block rows
- * with the lanes on the lines, and the outputs are added to the data rows line by line through shared memory. */
-int dfx_spmm_pf_forward_lines(const float *sino, const int32_t *fb_ptr, const uint16_t *fb_k, const float *fb_v,
-                              const uint8_t *fb_mask, float *data, const int32_t *omegas, int n_sub, int my, int P,
-                              int C, int kstride, int kb, void *stream);
 
 /* replaces batched_gemm_clblast / batched_gemm_clblast_adj (SPFO:2063-2127), the products of pf_mode "dense": pf is
  * the batch's float32 PF (n_omega, kb, cp) (dfx_pf_dense); adjoint 0: out = data (n_omega, my, cp) += in (n_omega, my,

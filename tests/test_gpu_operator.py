@@ -203,7 +203,7 @@ def test_ray_table_forward_equals_footprint_forward(golden, name):
     assert torch.equal(zb[:, :, :ks], a.to(torch.bfloat16))
     assert op.ray_taps == int(op._ray_rp[-1].item()) > 0
     # the float32 forward of many angles reads the grouped table (four bins per pixel load): the per-bin table's
-    # bits, for all angles, a subset's angles, and a support's tables
+    # bits, for all angles, a subset's angles, and a support's tables (the kernel called directly)
     assert op._ray_grp is not None
 
     def grouped(src, rows, tabs):
@@ -224,77 +224,6 @@ def test_ray_table_forward_equals_footprint_forward(golden, name):
     _lib.call("dfx_radon_forward_table", imgs.data_ptr(), t.data_ptr(), ray[0].data_ptr(), ray[1].data_ptr(),
               om.data_ptr(), om.numel(), ns, ks, kb, float(op.radon_geo.scale), s)
     assert torch.equal(grouped(imgs, om, ray[3]), t)
-
-
-@pytest.mark.parametrize("name", ["ti8_small", "diff_midpoint_hat", "al5_small"])
-def test_four_pixel_backprojection_equals_one_pixel_per_warp(golden, name):
-    """The SIMT backprojections with four neighbouring pixels per warp (shared bin loads) give the one-pixel-per-warp
-    kernel's bits: plain and with the SPDHG primal step (x, z, the BF16 copy of x), float32 and BF16 sinograms, a
-    subset's angles, padding channels."""
-    from diffractom_b200 import _lib
-    d = golden(name)
-    op = make_operator(d)
-    rng = np.random.default_rng(6)
-    R, ns, ks, kb = op.N_Omega, op.My, op.Kstride, op.batches[0]["K_batch"] - 1
-    s = op._s()
-    sino = torch.as_tensor(rng.standard_normal((R, ns, ks)).astype(np.float32), device="cuda")
-    sb = sino.to(torch.bfloat16)
-    x0 = torch.as_tensor(rng.random((op.npix, ks)).astype(np.float32), device="cuda")
-    z0 = torch.as_tensor(rng.standard_normal((op.npix, ks)).astype(np.float32), device="cuda")
-    T = torch.as_tensor(rng.random((op.npix, ks)).astype(np.float32), device="cuda")
-    T[:, kb:] = 0
-    geo, n = op.geo_gpu[1::3].contiguous(), len(range(1, R, 3))
-    args = (op.Nx, op.Ny, ns, ks, kb, op._kernel_id, int(op.radon_geo.n_taps))
-    outs = []
-    prev = _lib.lib().dfx_radon_backward_quads(-1)
-    try:
-        for quads in (0, 1):
-            _lib.lib().dfx_radon_backward_quads(quads)
-            img = torch.empty((op.npix, ks), device="cuda")
-            _lib.call("dfx_radon_backward", sino.data_ptr(), img.data_ptr(), geo.data_ptr(), n, *args, s)
-            imgb = torch.empty((op.npix, ks), device="cuda")
-            _lib.call("dfx_radon_backward_bf16", sb.data_ptr(), ks, imgb.data_ptr(), geo.data_ptr(), n, *args, s)
-            x, z = x0.clone(), z0.clone()
-            _lib.call("dfx_radon_backward_spdhg", sino.data_ptr(), geo.data_ptr(), n, *args, x.data_ptr(),
-                      z.data_ptr(), T.data_ptr(), 3.0, 0.1, s)
-            xb_, zb_ = x0.clone(), z0.clone()
-            xc = torch.zeros((op.npix, ks), dtype=torch.bfloat16, device="cuda")
-            _lib.call("dfx_radon_backward_spdhg_bf16", sb.data_ptr(), ks, geo.data_ptr(), n, *args, xb_.data_ptr(),
-                      zb_.data_ptr(), T.data_ptr(), 3.0, 0.1, xc.data_ptr(), s)
-            torch.cuda.synchronize()
-            outs.append((img, imgb, x, z, xb_, zb_, xc))
-    finally:
-        _lib.lib().dfx_radon_backward_quads(prev)
-    for a, b in zip(*outs):
-        assert torch.equal(a, b)
-    assert not outs[0][0][:, kb:].any()
-
-
-@pytest.mark.parametrize("name", ["al5_small", "ti8_small"])
-def test_forward_pf_product_on_lines_equals_the_blocked_one(golden, name):
-    """dfx_spmm_pf_forward_lines (lanes on detector lines, outputs added line by line) adds the same bits to the data
-    rows as dfx_spmm_pf_forward_blocked (one block row per thread), for all angles and a subset's angle list."""
-    from diffractom_b200 import _lib
-    d = golden(name)
-    op = make_operator(d, pf_mode="sparse")
-    sb = op.sparse_batches[0]
-    assert sb.get("fb_ptr") is not None
-    rng = np.random.default_rng(8)
-    R, ns, ks, kb = op.N_Omega, op.My, op.Kstride, op.batches[0]["K_batch"]
-    sino = torch.as_tensor(rng.standard_normal((R, ns, ks)).astype(np.float32), device="cuda")
-    start = torch.as_tensor(rng.standard_normal(op.data_shape).astype(np.float32), device="cuda")
-    om = torch.arange(0, R, 4, dtype=torch.int32, device="cuda")
-    for rows, n in ((None, R), (om, om.numel())):
-        outs = []
-        for name_k in ("dfx_spmm_pf_forward_blocked", "dfx_spmm_pf_forward_lines"):
-            data = start.clone()
-            _lib.call(name_k, sino.data_ptr(), sb["fb_ptr"].data_ptr(), sb["fb_k"].data_ptr(), sb["fb_v"].data_ptr(),
-                      sb["fb_mask"].data_ptr(), data.data_ptr(), None if rows is None else rows.data_ptr(), n, ns,
-                      op.N_peaks, op.N_eta, ks, kb, op._s())
-            torch.cuda.synchronize()
-            outs.append(data)
-        assert torch.equal(outs[0], outs[1])
-        assert not torch.equal(outs[0], start)
 
 
 def test_operator_on_its_own_queue_equals_current_stream(golden):
