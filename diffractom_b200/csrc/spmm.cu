@@ -354,11 +354,8 @@ __global__ void __launch_bounds__(SP_ROWS) spmm_forward_b4_kernel(
         e = __ldg(fb_ptr + g + 1);
         m = __ldg(fb_mask + g);
     }
-    // entries i (kn, vn) and i + 1 (kn2, vn2) in registers: the loads of entry i + 2 go out while entry i is applied
     int kn = i < e ? (int)__ldg(fb_k + i) : 0x7fffffff;
     float4 vn = i < e ? __ldg(fb_v + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-    int kn2 = i + 1 < e ? (int)__ldg(fb_k + i + 1) : 0x7fffffff;
-    float4 vn2 = i + 1 < e ? __ldg(fb_v + i + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
     float acc[FB_W][SP_TY];
 #pragma unroll
     for (int u = 0; u < FB_W; ++u)
@@ -373,10 +370,8 @@ __global__ void __launch_bounds__(SP_ROWS) spmm_forward_b4_kernel(
             const int k = kn;
             const float4 v = vn;
             ++i;
-            kn = kn2;
-            vn = vn2;
-            kn2 = i + 1 < e ? (int)__ldg(fb_k + i + 1) : 0x7fffffff;
-            vn2 = i + 1 < e ? __ldg(fb_v + i + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
+            kn = i < e ? (int)__ldg(fb_k + i) : 0x7fffffff;
+            vn = i < e ? __ldg(fb_v + i) : make_float4(0.f, 0.f, 0.f, 0.f);
             const float4 *t4 = reinterpret_cast<const float4 *>(tile + (k - c0) * SP_TYP);
 #pragma unroll
             for (int w = 0; w < SP_TY / 4; ++w) {
