@@ -672,8 +672,9 @@ def algorithmic_work(op, name, args_list):
             n_ang, kb = args[3], args[8]
             nb.append(2 * kb * n_ang * My + (4 * 5 + (2 if args[16] else 0)) * npix * kb)
             nf.append(2 * 2 * npix * n_ang * kb)
-        elif name == "dfx_spmm_pf_forward_blocked":
-            n_sub, kb = args[7], args[12]
+        elif name in ("dfx_spmm_pf_forward_blocked", "dfx_spmm_pf_forward_blocked_zt"):
+            # the transposed copy of the Radon output is not algorithmic traffic
+            n_sub, kb = (args[7], args[12]) if name == "dfx_spmm_pf_forward_blocked" else (args[9], args[14])
             frac = n_sub / op.N_Omega
             nnz = sum(sb["nnz"] for sb in op.sparse_batches) / len(op.sparse_batches) * frac
             nb.append(4 * n_sub * My * (kb + 2 * op.N_seg) + 6 * nnz)

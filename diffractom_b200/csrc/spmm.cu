@@ -11,6 +11,8 @@
 // (spmm_forward_b4_kernel), the CSR kernel serving generated copies.
 #include "dfx_common.cuh"
 
+#include <algorithm>
+
 namespace dfx {
 
 constexpr int SP_ROWS = 256;              // CSR rows per block
@@ -402,6 +404,149 @@ __global__ void __launch_bounds__(SP_ROWS) spmm_forward_b4_kernel(
     }
 }
 
+// ---- blocked forward over the lines-fastest sinogram ----
+// zt[s][k][y] (line stride ly = 32 * groups, lines my .. ly - 1 zero) is the Radon output of one launch's angles with
+// the detector lines fastest. A warp owns one block row (four eta bins of one ring) of one angle and 32 ZT_G lines:
+// lane l holds the lines y0 + l + 32 t. Per entry the warp reads the entry once (the same address in every lane) and
+// one coalesced 128-byte segment of Z column k per 32 lines, and applies the entry's four values to it. A block holds
+// the G * P block rows of G consecutive eta blocks (all rings), whose outputs j = 4 cb P .. 4 (cb + G) P - 1 are
+// contiguous in a data row: they go through shared memory and are added to the data rows a whole row segment at a
+// time. The sums per output run over the block row's entries in order with fmaf, each added once to the data row, as
+// in spmm_forward_b4_kernel: the results are that kernel's (and the CSR kernel's) bit for bit.
+constexpr int ZT_G = 9;                  // 32-line groups per warp at most (288 lines)
+constexpr int ZT_TR = 32;                // transpose tile
+
+// zt[s][k][y] = sino[s][y][k] (k < kb, y < my; zero for my <= y < ly)
+__global__ void __launch_bounds__(256) zt_transpose_kernel(const float *__restrict__ sino, float *__restrict__ zt,
+                                                           int my, int ly, int kstride, int kb)
+{
+    __shared__ float tile[ZT_TR][ZT_TR + 1];
+    const int s = blockIdx.z, k0 = blockIdx.x * ZT_TR, y0 = blockIdx.y * ZT_TR;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int yy = ty; yy < ZT_TR; yy += 8) {
+        const int y = y0 + yy, k = k0 + tx;
+        tile[yy][tx] = (y < my && k < kb) ? __ldg(sino + ((int64_t)s * my + y) * kstride + k) : 0.0f;
+    }
+    __syncthreads();
+    for (int kk = ty; kk < ZT_TR; kk += 8) {
+        const int k = k0 + kk;
+        if (k < kb) zt[((int64_t)s * kb + k) * ly + y0 + tx] = tile[tx][kk];
+    }
+}
+
+template <int MT>
+__device__ __forceinline__ void zt_apply(float (&acc)[FB_W][MT], const float *__restrict__ zc, const float4 v,
+                                         int g0, int ngroups)
+{
+    float z[MT];
+#pragma unroll
+    for (int t = 0; t < MT; ++t) z[t] = g0 + t < ngroups ? __ldg(zc + 32 * t) : 0.0f;
+#pragma unroll
+    for (int t = 0; t < MT; ++t) {
+        acc[0][t] = __fmaf_rn(v.x, z[t], acc[0][t]);
+        acc[1][t] = __fmaf_rn(v.y, z[t], acc[1][t]);
+        acc[2][t] = __fmaf_rn(v.z, z[t], acc[2][t]);
+        acc[3][t] = __fmaf_rn(v.w, z[t], acc[3][t]);
+    }
+}
+
+template <int MT>
+__global__ void __launch_bounds__(256) spmm_forward_zt_kernel(
+    const float *__restrict__ zt, const int32_t *__restrict__ fb_ptr, const uint16_t *__restrict__ fb_k,
+    const float4 *__restrict__ fb_v, const uint8_t *__restrict__ fb_mask, float *__restrict__ data,
+    const int32_t *__restrict__ omegas, int r0, int my, int ly, int P, int PW, int nrg, int C, int ncb, int G,
+    int kb)
+{
+    extern __shared__ float s_out[];                  // [32 MT lines][width + 1]
+    __shared__ uint8_t s_own[FB_W * 32];              // output j of the block written (its bin's row has entries)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s = blockIdx.z;
+    const int r = omegas ? __ldg(omegas + s) : r0 + s;
+    const int ngroups = ly >> 5;
+    const int g0 = blockIdx.y * MT;                   // first 32-line group of the block
+    const int y0 = g0 * 32;
+    const int cbg = blockIdx.x / nrg, rg = blockIdx.x - cbg * nrg;
+    const int cbw = warp / PW, p = rg * PW + (warp - cbw * PW);
+    const int cb = cbg * G + cbw;
+    const int width = FB_W * G * P, wp = width + 1;
+    for (int t = threadIdx.x; t < width; t += blockDim.x) s_own[t] = 0;
+    int i = 0, e = 0, m = 0;
+    if (cb < ncb && p < P) {
+        const int64_t g = (int64_t)r * P * ncb + (int64_t)cb * P + p;
+        i = __ldg(fb_ptr + g);
+        e = __ldg(fb_ptr + g + 1);
+        m = __ldg(fb_mask + g);
+    }
+    float acc[FB_W][MT];
+#pragma unroll
+    for (int u = 0; u < FB_W; ++u)
+#pragma unroll
+        for (int t = 0; t < MT; ++t) acc[u][t] = 0.0f;
+    const float *zs = zt + (int64_t)s * kb * ly + y0 + lane;
+    // entries in pairs, the next pair's loads issued before the current pair is applied
+    int ka = 0, kc = 0;
+    float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vc = va;
+    if (i < e) {
+        ka = __ldg(fb_k + i);
+        va = __ldg(fb_v + i);
+    }
+    if (i + 1 < e) {
+        kc = __ldg(fb_k + i + 1);
+        vc = __ldg(fb_v + i + 1);
+    }
+    for (; i + 1 < e; i += 2) {
+        const int k0 = ka, k1 = kc;
+        const float4 v0 = va, v1 = vc;
+        if (i + 2 < e) {
+            ka = __ldg(fb_k + i + 2);
+            va = __ldg(fb_v + i + 2);
+        }
+        if (i + 3 < e) {
+            kc = __ldg(fb_k + i + 3);
+            vc = __ldg(fb_v + i + 3);
+        }
+        float z0[MT], z1[MT];
+        const float *zc0 = zs + (int64_t)k0 * ly, *zc1 = zs + (int64_t)k1 * ly;
+#pragma unroll
+        for (int t = 0; t < MT; ++t) {
+            z0[t] = g0 + t < ngroups ? __ldg(zc0 + 32 * t) : 0.0f;
+            z1[t] = g0 + t < ngroups ? __ldg(zc1 + 32 * t) : 0.0f;
+        }
+#pragma unroll
+        for (int t = 0; t < MT; ++t) {
+            acc[0][t] = __fmaf_rn(v0.x, z0[t], acc[0][t]);
+            acc[1][t] = __fmaf_rn(v0.y, z0[t], acc[1][t]);
+            acc[2][t] = __fmaf_rn(v0.z, z0[t], acc[2][t]);
+            acc[3][t] = __fmaf_rn(v0.w, z0[t], acc[3][t]);
+            acc[0][t] = __fmaf_rn(v1.x, z1[t], acc[0][t]);
+            acc[1][t] = __fmaf_rn(v1.y, z1[t], acc[1][t]);
+            acc[2][t] = __fmaf_rn(v1.z, z1[t], acc[2][t]);
+            acc[3][t] = __fmaf_rn(v1.w, z1[t], acc[3][t]);
+        }
+    }
+    if (i < e) zt_apply<MT>(acc, zs + (int64_t)ka * ly, va, g0, ngroups);
+    // outputs of the block through shared memory: local j of bin u = (4 cbw + u) P + p
+    __syncthreads();                                  // s_own cleared
+    if (p < P) {
+        const int jl = FB_W * cbw * P + p;
+#pragma unroll
+        for (int u = 0; u < FB_W; ++u) {
+#pragma unroll
+            for (int t = 0; t < MT; ++t) s_out[(lane + 32 * t) * wp + jl + u * P] = acc[u][t];
+            if (lane == 0) s_own[jl + u * P] = (uint8_t)((m >> u) & 1);
+        }
+    }
+    __syncthreads();
+    const int cp = C * P;
+    const int ny = min(32 * MT, my - y0);
+    const int rows_per_pass = blockDim.x / width;     // at least 1: width = 4 G P <= 32 G PW = blockDim
+    const int tj = threadIdx.x % width, ty = threadIdx.x / width;
+    if (ty < rows_per_pass && s_own[tj]) {
+        float *d = data + ((int64_t)r * my + y0) * cp + (int64_t)FB_W * cbg * G * P + tj;
+        for (int yl = ty; yl < ny; yl += rows_per_pass) d[(int64_t)yl * cp] += s_out[yl * wp + tj];
+    }
+}
+
 }  // namespace dfx
 
 using namespace dfx;
@@ -486,4 +631,84 @@ extern "C" int dfx_spmm_pf_forward_blocked(const float *sino, const int32_t *fb_
         sino, fb_ptr, fb_k, reinterpret_cast<const float4 *>(fb_v), fb_mask, data, omegas, my, P, C, ncb, kstride,
         kb);
     return launch_status("spmm_pf_forward_blocked");
+}
+
+extern "C" int64_t dfx_spmm_pf_forward_zt_floats(int n_angles, int my, int kb)
+{
+    if (n_angles <= 0 || my <= 0 || kb <= 0) return -1;
+    return (int64_t)n_angles * kb * (cdiv(my, 32) * 32);
+}
+
+template <int MT>
+static int launch_zt(const float *zt, const int32_t *fb_ptr, const uint16_t *fb_k, const float *fb_v,
+                     const uint8_t *fb_mask, float *data, const int32_t *omegas, int r0, int na, int my, int ly,
+                     int nyb, int P, int PW, int nrg, int C, int ncb, int G, int kb, cudaStream_t st)
+{
+    const cudaError_t err = allow_max_dynamic_smem(spmm_forward_zt_kernel<MT>);
+    if (err != cudaSuccess) {
+        set_error("spmm_forward_blocked_zt: shared memory attribute: %s", cudaGetErrorString(err));
+        return DFX_ELAUNCH;
+    }
+    const int width = FB_W * G * P;
+    const size_t smem = (size_t)32 * MT * (width + 1) * sizeof(float);
+    dim3 grid((unsigned)(cdiv(ncb, G) * nrg), (unsigned)nyb, (unsigned)na);
+    spmm_forward_zt_kernel<MT><<<grid, 32 * G * PW, smem, st>>>(
+        zt, fb_ptr, fb_k, reinterpret_cast<const float4 *>(fb_v), fb_mask, data, omegas, r0, my, ly, P, PW, nrg, C,
+        ncb, G, kb);
+    return launch_status("spmm_pf_forward_blocked_zt");
+}
+
+extern "C" int dfx_spmm_pf_forward_blocked_zt(const float *sino, float *zt, int64_t zt_floats, const int32_t *fb_ptr,
+                                              const uint16_t *fb_k, const float *fb_v, const uint8_t *fb_mask,
+                                              float *data, const int32_t *omegas, int n_sub, int my, int P, int C,
+                                              int kstride, int kb, int max_groups, void *stream)
+{
+    DFX_REQUIRE(sino && zt && fb_ptr && fb_k && fb_v && fb_mask && data, "spmm_forward_blocked_zt: null pointer");
+    DFX_REQUIRE(((uintptr_t)fb_v % 16) == 0, "spmm_forward_blocked_zt: the values must be 16-byte aligned");
+    DFX_REQUIRE(n_sub > 0 && my > 0 && P > 0 && C > 0 && kb > 0 && kb <= kstride,
+                "spmm_forward_blocked_zt: bad sizes");
+    DFX_REQUIRE(P <= 32, "spmm_forward_blocked_zt: more than 32 rings");
+    const int64_t per_angle = dfx_spmm_pf_forward_zt_floats(1, my, kb);
+    DFX_REQUIRE(zt_floats >= per_angle, "spmm_forward_blocked_zt: the transpose buffer holds less than one angle");
+    const int ly = (int)(cdiv(my, 32) * 32), ngroups = ly / 32;
+    DFX_REQUIRE(max_groups >= 0 && max_groups <= ZT_G, "spmm_forward_blocked_zt: max_groups outside 0 .. 9");
+    const int gmax = max_groups ? max_groups : ZT_G;
+    const int nyb = (int)cdiv(ngroups, gmax), mt = (int)cdiv(ngroups, nyb);
+    // blocks of G eta blocks x PW rings, at most 8 warps: G = 8 / P below 8 rings, else ring groups of <= 8
+    const int G = P >= 8 ? 1 : 8 / P;
+    const int nrg = (int)cdiv(P, 8), PW = (int)cdiv(P, nrg);
+    const int ncb = (int)cdiv(C, FB_W);
+    DFX_REQUIRE(nyb <= 65535 && cdiv(kb, ZT_TR) <= 2147483647LL, "spmm_forward_blocked_zt: grid too large");
+    const int chunk = (int)std::min<int64_t>(std::min<int64_t>(n_sub, zt_floats / per_angle), 65535);
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int s0 = 0; s0 < n_sub; s0 += chunk) {
+        const int na = std::min(chunk, n_sub - s0);
+        dim3 tg((unsigned)cdiv(kb, ZT_TR), (unsigned)(ly / ZT_TR), (unsigned)na);
+        zt_transpose_kernel<<<tg, 256, 0, st>>>(sino + (int64_t)s0 * my * kstride, zt, my, ly, kstride, kb);
+        int rc = launch_status("spmm_pf_forward_blocked_zt: transpose");
+        if (rc) return rc;
+        const int32_t *om = omegas ? omegas + s0 : nullptr;
+        switch (mt) {
+#define DFX_ZT_CASE(M)                                                                                                 \
+    case M:                                                                                                            \
+        rc = launch_zt<M>(zt, fb_ptr, fb_k, fb_v, fb_mask, data, om, s0, na, my, ly, nyb, P, PW, nrg, C, ncb, G, kb, \
+                          st);                                                                                 \
+        break;
+            DFX_ZT_CASE(1)
+            DFX_ZT_CASE(2)
+            DFX_ZT_CASE(3)
+            DFX_ZT_CASE(4)
+            DFX_ZT_CASE(5)
+            DFX_ZT_CASE(6)
+            DFX_ZT_CASE(7)
+            DFX_ZT_CASE(8)
+            DFX_ZT_CASE(9)
+#undef DFX_ZT_CASE
+        default:
+            set_error("spmm_forward_blocked_zt: %d line groups per warp", mt);
+            return DFX_EINVAL;
+        }
+        if (rc) return rc;
+    }
+    return DFX_OK;
 }

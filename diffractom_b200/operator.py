@@ -56,6 +56,12 @@ class SinglePhaseForwardOperator:
     # with both CSR copies stored, the forward products run over an eta-blocked copy of the forward CSR (four
     # neighbouring eta bins of a ring per entry; the same sums bit for bit); False: over the forward CSR itself
     forward_blocks = True
+    # the blocked forward products read the Radon output transposed to detector lines fastest (one warp per block
+    # row, whole 128-byte segments of a Z column per entry; dfx_spmm_pf_forward_blocked_zt, the same bits) through a
+    # buffer of up to zt_max_angles angles of a batch; False: dfx_spmm_pf_forward_blocked on the channel-fastest output
+    forward_lines_fastest = True
+    zt_max_angles = 128
+    zt_max_groups = 0
 
     def __init__(self, cfg: Mapping[str, Any], material, grid, max_gb: float, verbose: bool = False,
                  normalized: bool = False, ctx=None, queue=None, pf_mode: str = "auto", sparse_max_fill: float = 0.3,
@@ -150,6 +156,7 @@ class SinglePhaseForwardOperator:
             self._sub_version = 0
             self._make_pfg()
             self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
+            self._zt = None
             self._ray_supp = {}
             self._supp_tiles = {}
             self._fft = None
@@ -511,6 +518,12 @@ class SinglePhaseForwardOperator:
         sb = self.sparse_batches[ib]
         s = self._s()
         om_ptr = None if om is None else om.data_ptr()
+        if sb.get("fb_ptr") is not None and self.forward_lines_fastest and self.N_peaks <= 32:
+            zt = self._zt_buffer()
+            self._call("dfx_spmm_pf_forward_blocked_zt", sino_ptr, zt.data_ptr(), zt.numel(), sb["fb_ptr"].data_ptr(),
+                       sb["fb_k"].data_ptr(), sb["fb_v"].data_ptr(), sb["fb_mask"].data_ptr(), data.data_ptr(),
+                       om_ptr, n_ang, self.My, self.N_peaks, self.N_eta, self.Kstride, kb, int(self.zt_max_groups), s)
+            return
         if sb.get("fb_ptr") is not None:
             self._call("dfx_spmm_pf_forward_blocked", sino_ptr, sb["fb_ptr"].data_ptr(), sb["fb_k"].data_ptr(),
                        sb["fb_v"].data_ptr(), sb["fb_mask"].data_ptr(), data.data_ptr(), om_ptr, n_ang, self.My,
@@ -519,6 +532,20 @@ class SinglePhaseForwardOperator:
         rp, col, val, compact = self._pf_batch(ib, True, m)
         self._call("dfx_spmm_pf_forward", sino_ptr, rp.data_ptr(), col.data_ptr(), val.data_ptr(), data.data_ptr(),
                    om_ptr, n_ang, self.My, self.N_seg, self.Kstride, kb, compact, s)
+
+    def _zt_floats(self):
+        kmax = max(b["K_batch"] for b in self.batches)
+        na = max(1, min(int(self.zt_max_angles), self.N_Omega))
+        return int(self._lib.dfx_spmm_pf_forward_zt_floats(na, self.My, kmax))
+
+    def _zt_buffer(self):
+        """The lines-fastest copy of the Radon output the blocked forward reads (zt_max_angles angles of the largest
+        batch; allocated on first use)."""
+        need = self._zt_floats()
+        if self._zt is None or self._zt.numel() < need:
+            self._zt = None
+            self._zt = torch.empty(need, dtype=torch.float32, device=self.device)
+        return self._zt
 
     def build_sparse_pf(self, mode="auto", max_fill=0.3, max_gb=None, max_fill_partial=0.1):
         """The sparse PF matrix per orientation batch (SPFO:1207-1373). The fill fraction of the first (dense-sized)
@@ -782,6 +809,9 @@ class SinglePhaseForwardOperator:
                 n += 2 * 2 * ns * self.Ktot * self.cp_pad
         if self.projector == "fft":
             n += int(self.fft_max_gb * 1024 ** 3)
+        if (self._zt is None and self.forward_lines_fastest and self.sparse_batches
+                and any(sb.get("fb_ptr") is not None for sb in self.sparse_batches)):
+            n += 4 * self._zt_floats()
         return int(n)
 
     def _max_subset(self):
@@ -1337,6 +1367,7 @@ class SinglePhaseForwardOperator:
         self._pf_dense = None
         self.pf_bf16 = self._d_bf16 = self._z_bf16 = self._img_k2 = None
         self._scratch = torch.empty(0, dtype=torch.uint8, device=self.device)
+        self._zt = None
         self.stream().synchronize()          # this operator's work only (other streams keep running)
 
 

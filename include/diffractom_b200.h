@@ -252,6 +252,17 @@ int dfx_spmm_pf_forward_blocked(const float *sino, const int32_t *fb_ptr, const 
                                 const uint8_t *fb_mask, float *data, const int32_t *omegas, int n_sub, int my, int P,
                                 int C, int kstride, int kb, void *stream);
 
+/* The same product as dfx_spmm_pf_forward_blocked, bit for bit (the same sums in the same order), through the
+ * Radon output transposed to detector lines fastest: per chunk of angles, zt[s][k][y] (line stride 32 ceil(my / 32))
+ * is written from sino, then one warp per block row and 32 lines reads each entry once and Z column k as whole
+ * 128-byte segments. zt holds zt_floats floats, at least dfx_spmm_pf_forward_zt_floats(1, my, kb) (one angle); the
+ * angles run in chunks of what fits. max_groups: 32-line groups per warp at most (1 .. 9; 0: 9). P <= 32 rings. */
+int64_t dfx_spmm_pf_forward_zt_floats(int n_angles, int my, int kb);
+int dfx_spmm_pf_forward_blocked_zt(const float *sino, float *zt, int64_t zt_floats, const int32_t *fb_ptr,
+                                   const uint16_t *fb_k, const float *fb_v, const uint8_t *fb_mask, float *data,
+                                   const int32_t *omegas, int n_sub, int my, int P, int C, int kstride, int kb,
+                                   int max_groups, void *stream);
+
 /* replaces batched_gemm_clblast / batched_gemm_clblast_adj (SPFO:2063-2127), the products of pf_mode "dense": pf is
  * the batch's float32 PF (n_omega, kb, cp) (dfx_pf_dense); adjoint 0: out = data (n_omega, my, cp) += in (n_omega, my,
  * kstride: the Radon output) . PF per angle; adjoint 1: out (n_omega, my, kstride) = alpha in (data) . PF^T per angle,
