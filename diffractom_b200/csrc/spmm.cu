@@ -124,10 +124,14 @@ __global__ void __launch_bounds__(SP_ROWS) spmm_forward_kernel(
         i = walk_row(acc, tile, col_k, val, i, e, g, c0, c0 + cn);
     }
     if (j < cp && nonempty) {
+        // all old values loaded before the first store (one round trip, not one per line)
         float *dl = data + ((int64_t)r * my + y0) * cp + j;
+        float old[SP_TY];
+#pragma unroll
+        for (int t = 0; t < SP_TY; ++t) old[t] = t < ny ? dl[(int64_t)t * cp] : 0.0f;
 #pragma unroll
         for (int t = 0; t < SP_TY; ++t)
-            if (t < ny) dl[(int64_t)t * cp] += acc[t];
+            if (t < ny) dl[(int64_t)t * cp] = old[t] + acc[t];
     }
 }
 
@@ -406,14 +410,17 @@ __global__ void __launch_bounds__(SP_ROWS) spmm_forward_b4_kernel(
 
 // ---- blocked forward over the lines-fastest sinogram ----
 // zt[s][k][y] (line stride ly = 32 * groups, lines my .. ly - 1 zero) is the Radon output of one launch's angles with
-// the detector lines fastest. A warp owns one block row (four eta bins of one ring) of one angle and 32 ZT_G lines:
-// lane l holds the lines y0 + l + 32 t. Per entry the warp reads the entry once (the same address in every lane) and
-// one coalesced 128-byte segment of Z column k per 32 lines, and applies the entry's four values to it. A block holds
-// the G * P block rows of G consecutive eta blocks (all rings), whose outputs j = 4 cb P .. 4 (cb + G) P - 1 are
-// contiguous in a data row: they go through shared memory and are added to the data rows a whole row segment at a
-// time. The sums per output run over the block row's entries in order with fmaf, each added once to the data row, as
-// in spmm_forward_b4_kernel: the results are that kernel's (and the CSR kernel's) bit for bit.
+// the detector lines fastest. A warp owns one block row (four eta bins of one ring) of one angle and up to 32 ZT_G
+// lines: lane l holds the lines y0 + l + 32 t. Per entry the warp reads the entry once (the same address in every
+// lane) and one coalesced 128-byte segment of Z column k per 32 lines, four entries in flight, and applies the
+// entry's four values with paired fused multiply-adds (fma.rn.f32x2: two IEEE fmaf in one instruction, lines t and
+// t + 1). A block holds the G * P block rows of G consecutive eta blocks (all rings; ring groups of at most 8 above
+// 8 rings), whose outputs j = 4 cb P .. 4 (cb + G) P - 1 are contiguous in a data row. The block copies those data
+// row segments into shared memory (cp.async) when it starts, so the epilogue adds each output to its old value there
+// and only stores. The sums per output run over the block row's entries in order with fmaf, each added once to the
+// data row, as in spmm_forward_b4_kernel: the results are that kernel's (and the CSR kernel's) bit for bit.
 constexpr int ZT_G = 9;                  // 32-line groups per warp at most (288 lines)
+constexpr int ZT_U = 4;                  // entries in flight per warp
 constexpr int ZT_TR = 32;                // transpose tile
 
 // zt[s][k][y] = sino[s][y][k] (k < kb, y < my; zero for my <= y < ly)
@@ -434,30 +441,35 @@ __global__ void __launch_bounds__(256) zt_transpose_kernel(const float *__restri
     }
 }
 
-template <int MT>
-__device__ __forceinline__ void zt_apply(float (&acc)[FB_W][MT], const float *__restrict__ zc, const float4 v,
-                                         int g0, int ngroups)
+// a0 = fmaf(v, z0, a0), a1 = fmaf(v, z1, a1) in one instruction (same rounding as two fmaf)
+__device__ __forceinline__ void fma_pair(float &a0, float &a1, float v, float z0, float z1)
 {
-    float z[MT];
-#pragma unroll
-    for (int t = 0; t < MT; ++t) z[t] = g0 + t < ngroups ? __ldg(zc + 32 * t) : 0.0f;
-#pragma unroll
-    for (int t = 0; t < MT; ++t) {
-        acc[0][t] = __fmaf_rn(v.x, z[t], acc[0][t]);
-        acc[1][t] = __fmaf_rn(v.y, z[t], acc[1][t]);
-        acc[2][t] = __fmaf_rn(v.z, z[t], acc[2][t]);
-        acc[3][t] = __fmaf_rn(v.w, z[t], acc[3][t]);
-    }
+    asm("{\n.reg .b64 A, Z, V;\nmov.b64 A, {%0, %1};\nmov.b64 Z, {%3, %4};\nmov.b64 V, {%2, %2};\n"
+        "fma.rn.f32x2 A, V, Z, A;\nmov.b64 {%0, %1}, A;\n}"
+        : "+f"(a0), "+f"(a1)
+        : "f"(v), "f"(z0), "f"(z1));
+}
+
+__device__ __forceinline__ void cp_async16(float *dst, const float *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(float *dst, const float *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
 }
 
 template <int MT>
-__global__ void __launch_bounds__(256) spmm_forward_zt_kernel(
+__global__ void __launch_bounds__(256, 2) spmm_forward_zt_kernel(
     const float *__restrict__ zt, const int32_t *__restrict__ fb_ptr, const uint16_t *__restrict__ fb_k,
     const float4 *__restrict__ fb_v, const uint8_t *__restrict__ fb_mask, float *__restrict__ data,
     const int32_t *__restrict__ omegas, int r0, int my, int ly, int P, int PW, int nrg, int C, int ncb, int G,
     int kb)
 {
-    extern __shared__ float s_out[];                  // [32 MT lines][width + 1]
+    extern __shared__ __align__(16) float s_dyn[];
     __shared__ uint8_t s_own[FB_W * 32];              // output j of the block written (its bin's row has entries)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s = blockIdx.z;
@@ -469,7 +481,27 @@ __global__ void __launch_bounds__(256) spmm_forward_zt_kernel(
     const int cbw = warp / PW, p = rg * PW + (warp - cbw * PW);
     const int cb = cbg * G + cbw;
     const int width = FB_W * G * P, wp = width + 1;
+    const int cp = C * P;
+    const int j0 = FB_W * cbg * G * P;                // first output of the block in a data row
+    const int wj = min(width, cp - j0);
+    const int ny = min(32 * MT, my - y0);
+    float *s_out = s_dyn;                             // [32 MT][wp]: the block's sums
+    float *s_old = s_dyn + 32 * MT * wp;              // [32 MT][width]: the data row segments before the launch
+    float *drow = data + ((int64_t)r * my + y0) * cp + j0;
     for (int t = threadIdx.x; t < width; t += blockDim.x) s_own[t] = 0;
+    if ((cp & 3) == 0) {                              // rows and segments 16-byte aligned (j0, width multiples of 4)
+        const int q4 = wj >> 2;
+        for (int idx = threadIdx.x; idx < ny * q4; idx += blockDim.x) {
+            const int yl = idx / q4, c = idx - yl * q4;
+            cp_async16(s_old + yl * width + 4 * c, drow + (int64_t)yl * cp + 4 * c);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < ny * wj; idx += blockDim.x) {
+            const int yl = idx / wj, c = idx - yl * wj;
+            cp_async4(s_old + yl * width + c, drow + (int64_t)yl * cp + c);
+        }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
     int i = 0, e = 0, m = 0;
     if (cb < ncb && p < P) {
         const int64_t g = (int64_t)r * P * ncb + (int64_t)cb * P + p;
@@ -483,51 +515,50 @@ __global__ void __launch_bounds__(256) spmm_forward_zt_kernel(
 #pragma unroll
         for (int t = 0; t < MT; ++t) acc[u][t] = 0.0f;
     const float *zs = zt + (int64_t)s * kb * ly + y0 + lane;
-    // entries in pairs, the next pair's loads issued before the current pair is applied
-    int ka = 0, kc = 0;
-    float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vc = va;
-    if (i < e) {
-        ka = __ldg(fb_k + i);
-        va = __ldg(fb_v + i);
-    }
-    if (i + 1 < e) {
-        kc = __ldg(fb_k + i + 1);
-        vc = __ldg(fb_v + i + 1);
-    }
-    for (; i + 1 < e; i += 2) {
-        const int k0 = ka, k1 = kc;
-        const float4 v0 = va, v1 = vc;
-        if (i + 2 < e) {
-            ka = __ldg(fb_k + i + 2);
-            va = __ldg(fb_v + i + 2);
-        }
-        if (i + 3 < e) {
-            kc = __ldg(fb_k + i + 3);
-            vc = __ldg(fb_v + i + 3);
-        }
-        float z0[MT], z1[MT];
-        const float *zc0 = zs + (int64_t)k0 * ly, *zc1 = zs + (int64_t)k1 * ly;
+    int kq[ZT_U];
+    float4 vq[ZT_U];
 #pragma unroll
-        for (int t = 0; t < MT; ++t) {
-            z0[t] = g0 + t < ngroups ? __ldg(zc0 + 32 * t) : 0.0f;
-            z1[t] = g0 + t < ngroups ? __ldg(zc1 + 32 * t) : 0.0f;
+    for (int q = 0; q < ZT_U; ++q) {
+        kq[q] = i + q < e ? __ldg(fb_k + i + q) : 0;
+        vq[q] = i + q < e ? __ldg(fb_v + i + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for (; i < e; i += ZT_U) {
+        float4 vc[ZT_U];
+        float z[ZT_U][MT];
+#pragma unroll
+        for (int q = 0; q < ZT_U; ++q) {
+            vc[q] = vq[q];
+            const float *zc = zs + (int64_t)kq[q] * ly;
+#pragma unroll
+            for (int t = 0; t < MT; ++t) z[q][t] = g0 + t < ngroups ? __ldg(zc + 32 * t) : 0.0f;
         }
 #pragma unroll
-        for (int t = 0; t < MT; ++t) {
-            acc[0][t] = __fmaf_rn(v0.x, z0[t], acc[0][t]);
-            acc[1][t] = __fmaf_rn(v0.y, z0[t], acc[1][t]);
-            acc[2][t] = __fmaf_rn(v0.z, z0[t], acc[2][t]);
-            acc[3][t] = __fmaf_rn(v0.w, z0[t], acc[3][t]);
-            acc[0][t] = __fmaf_rn(v1.x, z1[t], acc[0][t]);
-            acc[1][t] = __fmaf_rn(v1.y, z1[t], acc[1][t]);
-            acc[2][t] = __fmaf_rn(v1.z, z1[t], acc[2][t]);
-            acc[3][t] = __fmaf_rn(v1.w, z1[t], acc[3][t]);
+        for (int q = 0; q < ZT_U; ++q) {              // the next entries' loads go out while these are applied
+            kq[q] = i + ZT_U + q < e ? __ldg(fb_k + i + ZT_U + q) : 0;
+            vq[q] = i + ZT_U + q < e ? __ldg(fb_v + i + ZT_U + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int q = 0; q < ZT_U; ++q) {
+            if (i + q < e) {
+#pragma unroll
+                for (int t = 0; t + 1 < MT; t += 2) {
+                    fma_pair(acc[0][t], acc[0][t + 1], vc[q].x, z[q][t], z[q][t + 1]);
+                    fma_pair(acc[1][t], acc[1][t + 1], vc[q].y, z[q][t], z[q][t + 1]);
+                    fma_pair(acc[2][t], acc[2][t + 1], vc[q].z, z[q][t], z[q][t + 1]);
+                    fma_pair(acc[3][t], acc[3][t + 1], vc[q].w, z[q][t], z[q][t + 1]);
+                }
+                if (MT & 1) {
+                    acc[0][MT - 1] = __fmaf_rn(vc[q].x, z[q][MT - 1], acc[0][MT - 1]);
+                    acc[1][MT - 1] = __fmaf_rn(vc[q].y, z[q][MT - 1], acc[1][MT - 1]);
+                    acc[2][MT - 1] = __fmaf_rn(vc[q].z, z[q][MT - 1], acc[2][MT - 1]);
+                    acc[3][MT - 1] = __fmaf_rn(vc[q].w, z[q][MT - 1], acc[3][MT - 1]);
+                }
+            }
         }
     }
-    if (i < e) zt_apply<MT>(acc, zs + (int64_t)ka * ly, va, g0, ngroups);
-    // outputs of the block through shared memory: local j of bin u = (4 cbw + u) P + p
-    __syncthreads();                                  // s_own cleared
-    if (p < P) {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();                                  // s_own cleared, s_old in place
+    if (p < P) {                                      // local j of bin u = (4 cbw + u) P + p
         const int jl = FB_W * cbw * P + p;
 #pragma unroll
         for (int u = 0; u < FB_W; ++u) {
@@ -537,14 +568,11 @@ __global__ void __launch_bounds__(256) spmm_forward_zt_kernel(
         }
     }
     __syncthreads();
-    const int cp = C * P;
-    const int ny = min(32 * MT, my - y0);
     const int rows_per_pass = blockDim.x / width;     // at least 1: width = 4 G P <= 32 G PW = blockDim
     const int tj = threadIdx.x % width, ty = threadIdx.x / width;
-    if (ty < rows_per_pass && s_own[tj]) {
-        float *d = data + ((int64_t)r * my + y0) * cp + (int64_t)FB_W * cbg * G * P + tj;
-        for (int yl = ty; yl < ny; yl += rows_per_pass) d[(int64_t)yl * cp] += s_out[yl * wp + tj];
-    }
+    if (ty < rows_per_pass && s_own[tj])
+        for (int yl = ty; yl < ny; yl += rows_per_pass)
+            drow[(int64_t)yl * cp + tj] = s_old[yl * width + tj] + s_out[yl * wp + tj];
 }
 
 }  // namespace dfx
@@ -650,7 +678,7 @@ static int launch_zt(const float *zt, const int32_t *fb_ptr, const uint16_t *fb_
         return DFX_ELAUNCH;
     }
     const int width = FB_W * G * P;
-    const size_t smem = (size_t)32 * MT * (width + 1) * sizeof(float);
+    const size_t smem = ((size_t)32 * MT * (width + 1) + (size_t)32 * MT * width) * sizeof(float);
     dim3 grid((unsigned)(cdiv(ncb, G) * nrg), (unsigned)nyb, (unsigned)na);
     spmm_forward_zt_kernel<MT><<<grid, 32 * G * PW, smem, st>>>(
         zt, fb_ptr, fb_k, reinterpret_cast<const float4 *>(fb_v), fb_mask, data, omegas, r0, my, ly, P, PW, nrg, C,
