@@ -679,9 +679,13 @@ def algorithmic_work(op, name, args_list):
             nnz = sum(sb["nnz"] for sb in op.sparse_batches) / len(op.sparse_batches) * frac
             nb.append(4 * n_sub * My * (kb + 2 * op.N_seg) + 6 * nnz)
             nf.append(2 * nnz * My)
-        elif name in ("dfx_spmm_pf_forward", "dfx_spmm_pf_adjoint"):
-            n_sub = args[6]
-            kb = args[10] if name == "dfx_spmm_pf_forward" else args[8]
+        elif name in ("dfx_spmm_pf_forward", "dfx_spmm_pf_adjoint", "dfx_spmm_pf_adjoint_zt"):
+            # (the transposed copy of the data rows of dfx_spmm_pf_adjoint_zt is not algorithmic traffic)
+            if name == "dfx_spmm_pf_adjoint_zt":
+                n_sub, kb = args[8], args[10]
+            else:
+                n_sub = args[6]
+                kb = args[10] if name == "dfx_spmm_pf_forward" else args[8]
             frac = n_sub / op.N_Omega
             nnz = sum(sb["nnz"] for sb in op.sparse_batches) / len(op.sparse_batches) * frac
             nb.append(4 * n_sub * My * (kb + 2 * op.N_seg) + 6 * nnz)

@@ -72,6 +72,8 @@ SIGNATURES = {
     "dfx_spmm_pf_forward_blocked": ([P, P, P, P, P, P, P, I, I, I, I, I, I, S], c_int),
     "dfx_spmm_pf_forward_zt_floats": ([I, I, I], c_int64),
     "dfx_spmm_pf_forward_blocked_zt": ([P, P, L, P, P, P, P, P, P, I, I, I, I, I, I, I, S], c_int),
+    "dfx_spmm_pf_adjoint_zt_floats": ([I, I, I], c_int64),
+    "dfx_spmm_pf_adjoint_zt": ([P, P, L, P, P, P, P, P, I, I, I, I, I, F, I, I, S], c_int),
     "dfx_zero_rows": ([P, P, I, L, S], c_int),
     "dfx_fill_f32": ([P, F, L, S], c_int),
     "dfx_spdhg_dual_update": ([P, P, P, P, P, L, P, L, P, L, F, P, I, L, S], c_int),

@@ -575,6 +575,107 @@ __global__ void __launch_bounds__(256, 2) spmm_forward_zt_kernel(
             drow[(int64_t)yl * cp + tj] = s_old[yl * width + tj] + s_out[yl * wp + tj];
 }
 
+// ---- adjoint over the lines-fastest data rows ----
+// dt[s][j][y] (line stride ly, lines my .. ly - 1 zero): the data rows of one launch's angles with the detector lines
+// fastest. A warp owns AZ_KW consecutive orientation rows k of one angle, one after the other, and up to 32 ZT_G lines
+// (lane l: lines y0 + l + 32 t); per entry (j, v) of a row it reads the entry once and one coalesced 128-byte segment
+// of column j per 32 lines, four entries in flight, paired fused multiply-adds. A block's 8 warps hold 32 consecutive
+// orientations, written as whole 128-byte row segments of the Radon input through shared memory. Per output the sum
+// runs over the row's entries in order with fmaf from 0 and is scaled by alpha: spmm_adjoint8_kernel's bits.
+constexpr int AZ_KW = 4;                 // orientation rows per warp
+constexpr int AZ_WARPS = 8;
+constexpr int AZ_K = AZ_KW * AZ_WARPS;   // orientations per block
+
+// dt[s][j][y] = data[r(s)][y][j] (j < cp, y < my; zero for my <= y < ly), r(s) = omegas[s] or r0 + s
+__global__ void __launch_bounds__(256) dt_transpose_kernel(const float *__restrict__ data, float *__restrict__ dt,
+                                                           const int32_t *__restrict__ omegas, int r0, int my, int ly,
+                                                           int cp)
+{
+    __shared__ float tile[ZT_TR][ZT_TR + 1];
+    const int s = blockIdx.z, j0 = blockIdx.x * ZT_TR, y0 = blockIdx.y * ZT_TR;
+    const int r = omegas ? __ldg(omegas + s) : r0 + s;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int yy = ty; yy < ZT_TR; yy += 8) {
+        const int y = y0 + yy, j = j0 + tx;
+        tile[yy][tx] = (y < my && j < cp) ? __ldg(data + ((int64_t)r * my + y) * cp + j) : 0.0f;
+    }
+    __syncthreads();
+    for (int jj = ty; jj < ZT_TR; jj += 8) {
+        const int j = j0 + jj;
+        if (j < cp) dt[((int64_t)s * cp + j) * ly + y0 + tx] = tile[tx][jj];
+    }
+}
+
+template <int MT>
+__global__ void __launch_bounds__(32 * AZ_WARPS, 3) spmm_adjoint_zt_kernel(
+    const float *__restrict__ dt, const int32_t *__restrict__ row_ptr, const uint16_t *__restrict__ col_j,
+    const float *__restrict__ val, float *__restrict__ sino, const int32_t *__restrict__ omegas, int r0, int my,
+    int ly, int kb, int cp, int kstride, float alpha, int compact)
+{
+    extern __shared__ float s_outk[];                 // [32 MT][AZ_K + 1]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s = blockIdx.z;
+    const int r = omegas ? __ldg(omegas + s) : r0 + s;
+    const int ngroups = ly >> 5;
+    const int g0 = blockIdx.y * MT;
+    const int y0 = g0 * 32;
+    const int k0 = blockIdx.x * AZ_K;
+    const float *ds = dt + (int64_t)s * cp * ly + y0 + lane;
+    for (int kk = 0; kk < AZ_KW; ++kk) {
+        const int kl = warp * AZ_KW + kk, k = k0 + kl;
+        int i = 0, e = 0;
+        if (k < kb) {
+            const int64_t rr = (int64_t)(compact ? s : r) * kb + k;
+            i = __ldg(row_ptr + rr);
+            e = __ldg(row_ptr + rr + 1);
+        }
+        float acc[MT];
+#pragma unroll
+        for (int t = 0; t < MT; ++t) acc[t] = 0.0f;
+        int jq[ZT_U];
+        float vq[ZT_U];
+#pragma unroll
+        for (int q = 0; q < ZT_U; ++q) {
+            jq[q] = i + q < e ? __ldg(col_j + i + q) : 0;
+            vq[q] = i + q < e ? __ldg(val + i + q) : 0.0f;
+        }
+        for (; i < e; i += ZT_U) {
+            float vc[ZT_U];
+            float z[ZT_U][MT];
+#pragma unroll
+            for (int q = 0; q < ZT_U; ++q) {
+                vc[q] = vq[q];
+                const float *zc = ds + (int64_t)jq[q] * ly;
+#pragma unroll
+                for (int t = 0; t < MT; ++t) z[q][t] = g0 + t < ngroups ? __ldg(zc + 32 * t) : 0.0f;
+            }
+#pragma unroll
+            for (int q = 0; q < ZT_U; ++q) {
+                jq[q] = i + ZT_U + q < e ? __ldg(col_j + i + ZT_U + q) : 0;
+                vq[q] = i + ZT_U + q < e ? __ldg(val + i + ZT_U + q) : 0.0f;
+            }
+#pragma unroll
+            for (int q = 0; q < ZT_U; ++q) {
+                if (i + q < e) {
+#pragma unroll
+                    for (int t = 0; t + 1 < MT; t += 2) fma_pair(acc[t], acc[t + 1], vc[q], z[q][t], z[q][t + 1]);
+                    if (MT & 1) acc[MT - 1] = __fmaf_rn(vc[q], z[q][MT - 1], acc[MT - 1]);
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < MT; ++t) s_outk[(lane + 32 * t) * (AZ_K + 1) + kl] = k < kb ? alpha * acc[t] : 0.0f;
+    }
+    __syncthreads();
+    const int ny = min(32 * MT, my - y0);
+    const int kl = threadIdx.x & (AZ_K - 1), ty = threadIdx.x / AZ_K;
+    const int k = k0 + kl;
+    if (k < kstride) {
+        float *zl = sino + ((int64_t)s * my + y0) * kstride + k;
+        for (int yl = ty; yl < ny; yl += (32 * AZ_WARPS) / AZ_K) zl[(int64_t)yl * kstride] = s_outk[yl * (AZ_K + 1) + kl];
+    }
+}
+
 }  // namespace dfx
 
 using namespace dfx;
@@ -734,6 +835,80 @@ extern "C" int dfx_spmm_pf_forward_blocked_zt(const float *sino, float *zt, int6
 #undef DFX_ZT_CASE
         default:
             set_error("spmm_forward_blocked_zt: %d line groups per warp", mt);
+            return DFX_EINVAL;
+        }
+        if (rc) return rc;
+    }
+    return DFX_OK;
+}
+
+extern "C" int64_t dfx_spmm_pf_adjoint_zt_floats(int n_angles, int my, int cp)
+{
+    if (n_angles <= 0 || my <= 0 || cp <= 0) return -1;
+    return (int64_t)n_angles * cp * (cdiv(my, 32) * 32);
+}
+
+template <int MT>
+static int launch_az(const float *dt, const int32_t *row_ptr, const uint16_t *col_j, const float *val, float *sino,
+                     const int32_t *omegas, int r0, int na, int my, int ly, int nyb, int kb, int cp, int kstride,
+                     float alpha, int compact, cudaStream_t st)
+{
+    const cudaError_t err = allow_max_dynamic_smem(spmm_adjoint_zt_kernel<MT>);
+    if (err != cudaSuccess) {
+        set_error("spmm_adjoint_zt: shared memory attribute: %s", cudaGetErrorString(err));
+        return DFX_ELAUNCH;
+    }
+    const size_t smem = (size_t)32 * MT * (AZ_K + 1) * sizeof(float);
+    dim3 grid((unsigned)cdiv(kstride, AZ_K), (unsigned)nyb, (unsigned)na);
+    spmm_adjoint_zt_kernel<MT><<<grid, 32 * AZ_WARPS, smem, st>>>(dt, row_ptr, col_j, val, sino, omegas, r0, my, ly,
+                                                                  kb, cp, kstride, alpha, compact);
+    return launch_status("spmm_pf_adjoint_zt");
+}
+
+extern "C" int dfx_spmm_pf_adjoint_zt(const float *data, float *dt, int64_t dt_floats, const int32_t *row_ptr,
+                                      const uint16_t *col_j, const float *val, float *sino, const int32_t *omegas,
+                                      int n_sub, int my, int kb, int cp, int kstride, float alpha, int compact,
+                                      int max_groups, void *stream)
+{
+    DFX_REQUIRE(data && dt && row_ptr && col_j && val && sino, "spmm_adjoint_zt: null pointer");
+    DFX_REQUIRE(n_sub > 0 && my > 0 && cp > 0 && kb > 0 && kb <= kstride, "spmm_adjoint_zt: bad sizes");
+    DFX_REQUIRE(cp <= 65536, "spmm_adjoint_zt: more than 65536 segments per data row");
+    DFX_REQUIRE(max_groups >= 0 && max_groups <= ZT_G, "spmm_adjoint_zt: max_groups outside 0 .. 9");
+    const int64_t per_angle = dfx_spmm_pf_adjoint_zt_floats(1, my, cp);
+    DFX_REQUIRE(dt_floats >= per_angle, "spmm_adjoint_zt: the transpose buffer holds less than one angle");
+    const int ly = (int)(cdiv(my, 32) * 32), ngroups = ly / 32;
+    const int gmax = max_groups ? max_groups : ZT_G;
+    const int nyb = (int)cdiv(ngroups, gmax), mt = (int)cdiv(ngroups, nyb);
+    DFX_REQUIRE(nyb <= 65535 && cdiv(kstride, AZ_K) <= 2147483647LL, "spmm_adjoint_zt: grid too large");
+    const int chunk = (int)std::min<int64_t>(std::min<int64_t>(n_sub, dt_floats / per_angle), 65535);
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int s0 = 0; s0 < n_sub; s0 += chunk) {
+        const int na = std::min(chunk, n_sub - s0);
+        const int32_t *om = omegas ? omegas + s0 : nullptr;
+        dim3 tg((unsigned)cdiv(cp, ZT_TR), (unsigned)(ly / ZT_TR), (unsigned)na);
+        dt_transpose_kernel<<<tg, 256, 0, st>>>(data, dt, om, s0, my, ly, cp);
+        int rc = launch_status("spmm_pf_adjoint_zt: transpose");
+        if (rc) return rc;
+        // compact rows are numbered by the position in the subset: the chunk's rows start at s0 * kb
+        const int32_t *rp = compact ? row_ptr + (int64_t)s0 * kb : row_ptr;
+        float *out = sino + (int64_t)s0 * my * kstride;
+        switch (mt) {
+#define DFX_AZ_CASE(M)                                                                                                 \
+    case M:                                                                                                            \
+        rc = launch_az<M>(dt, rp, col_j, val, out, om, s0, na, my, ly, nyb, kb, cp, kstride, alpha, compact, st);      \
+        break;
+            DFX_AZ_CASE(1)
+            DFX_AZ_CASE(2)
+            DFX_AZ_CASE(3)
+            DFX_AZ_CASE(4)
+            DFX_AZ_CASE(5)
+            DFX_AZ_CASE(6)
+            DFX_AZ_CASE(7)
+            DFX_AZ_CASE(8)
+            DFX_AZ_CASE(9)
+#undef DFX_AZ_CASE
+        default:
+            set_error("spmm_adjoint_zt: %d line groups per warp", mt);
             return DFX_EINVAL;
         }
         if (rc) return rc;

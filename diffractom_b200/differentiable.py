@@ -299,8 +299,8 @@ class ProjGradient:
             for ib, b in enumerate(op.batches):
                 kb = b["K_batch"]
                 rp, col, val, compact = op._pf_batch(ib, False)
-                op._call("dfx_spmm_pf_adjoint", r.data_ptr(), rp.data_ptr(), col.data_ptr(), val.data_ptr(),
-                         op.coeffs_sino_C.data_ptr(), None, R, My, kb, op.N_seg, op.Kstride, 1.0, compact, s)
+                op._pf_adjoint_product(r.data_ptr(), rp, col, val, op.coeffs_sino_C.data_ptr(), None, R, kb, 1.0,
+                                       compact, s)
                 _project_batch(op, c, ib)
                 op._call("dfx_radon_forward_table", op._img_k.data_ptr(), self.dS.data_ptr(), op._ray_rp.data_ptr(),
                          self.dent.data_ptr(), None, R, My, op.Kstride, kb, float(op.radon_geo.scale), s)

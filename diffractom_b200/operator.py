@@ -60,7 +60,11 @@ class SinglePhaseForwardOperator:
     # row, whole 128-byte segments of a Z column per entry; dfx_spmm_pf_forward_blocked_zt, the same bits) through a
     # buffer of up to zt_max_angles angles of a batch; False: dfx_spmm_pf_forward_blocked on the channel-fastest output
     forward_lines_fastest = True
-    zt_max_angles = 128
+    # the adjoint products read the data rows transposed to detector lines fastest (one warp per orientation row,
+    # whole 128-byte segments of a data column per entry; dfx_spmm_pf_adjoint_zt, the same bits) through the same
+    # buffer; False: dfx_spmm_pf_adjoint on the segment-fastest rows
+    adjoint_lines_fastest = True
+    zt_max_angles = 64
     zt_max_groups = 0
 
     def __init__(self, cfg: Mapping[str, Any], material, grid, max_gb: float, verbose: bool = False,
@@ -536,11 +540,16 @@ class SinglePhaseForwardOperator:
     def _zt_floats(self):
         kmax = max(b["K_batch"] for b in self.batches)
         na = max(1, min(int(self.zt_max_angles), self.N_Omega))
-        return int(self._lib.dfx_spmm_pf_forward_zt_floats(na, self.My, kmax))
+        n = 0
+        if self.forward_lines_fastest:
+            n = int(self._lib.dfx_spmm_pf_forward_zt_floats(na, self.My, kmax))
+        if self.adjoint_lines_fastest:
+            n = max(n, int(self._lib.dfx_spmm_pf_adjoint_zt_floats(na, self.My, self.N_seg)))
+        return n
 
     def _zt_buffer(self):
-        """The lines-fastest copy of the Radon output the blocked forward reads (zt_max_angles angles of the largest
-        batch; allocated on first use)."""
+        """The lines-fastest copy of the Radon output the blocked forward reads, or of the data rows the adjoint
+        reads (zt_max_angles angles; allocated on first use)."""
         need = self._zt_floats()
         if self._zt is None or self._zt.numel() < need:
             self._zt = None
@@ -809,8 +818,9 @@ class SinglePhaseForwardOperator:
                 n += 2 * 2 * ns * self.Ktot * self.cp_pad
         if self.projector == "fft":
             n += int(self.fft_max_gb * 1024 ** 3)
-        if (self._zt is None and self.forward_lines_fastest and self.sparse_batches
-                and any(sb.get("fb_ptr") is not None for sb in self.sparse_batches)):
+        if self._zt is None and self.pf_mode != "dense" and (self.adjoint_lines_fastest or (
+                self.forward_lines_fastest and self.sparse_batches
+                and any(sb.get("fb_ptr") is not None for sb in self.sparse_batches))):
             n += 4 * self._zt_floats()
         return int(n)
 
@@ -1175,10 +1185,23 @@ class SinglePhaseForwardOperator:
             self._dense_pf_product(ib, True, data.data_ptr(), self.coeffs_sino_C.data_ptr(), alpha)
             return geo, n_ang, Kb
         rp, col, val, compact = self._pf_batch(ib, False, m)
-        self._call("dfx_spmm_pf_adjoint", data.data_ptr(), rp.data_ptr(), col.data_ptr(), val.data_ptr(),
-                   self.coeffs_sino_C.data_ptr(), None if om is None else om.data_ptr(), n_ang, self.My, Kb,
-                   self.N_seg, self.Kstride, alpha, compact, self._s())
+        self._pf_adjoint_product(data.data_ptr(), rp, col, val, self.coeffs_sino_C.data_ptr(), om, n_ang, Kb, alpha,
+                                 compact, self._s())
         return geo, n_ang, Kb
+
+    def _pf_adjoint_product(self, data_ptr, rp, col, val, out_ptr, om, n_ang, kb, alpha, compact, s):
+        """out (Radon input, n_ang x My x Kstride) = alpha PF^T data rows over the adjoint CSR (rp, col, val): through
+        the lines-fastest copy of the data rows (dfx_spmm_pf_adjoint_zt) when adjoint_lines_fastest is set, else
+        dfx_spmm_pf_adjoint; the same bits."""
+        om_ptr = None if om is None else om.data_ptr()
+        if self.adjoint_lines_fastest:
+            zt = self._zt_buffer()
+            self._call("dfx_spmm_pf_adjoint_zt", data_ptr, zt.data_ptr(), zt.numel(), rp.data_ptr(), col.data_ptr(),
+                       val.data_ptr(), out_ptr, om_ptr, n_ang, self.My, kb, self.N_seg, self.Kstride, alpha, compact,
+                       int(self.zt_max_groups), s)
+            return
+        self._call("dfx_spmm_pf_adjoint", data_ptr, rp.data_ptr(), col.data_ptr(), val.data_ptr(), out_ptr, om_ptr,
+                   n_ang, self.My, kb, self.N_seg, self.Kstride, alpha, compact, s)
 
     def _adjoint_batch_k(self, data, ib, out_ptr, subset=None):
         """A^T data of batch ib into a channel-fastest batch at device address out_ptr."""
@@ -1285,9 +1308,8 @@ class SinglePhaseForwardOperator:
                             self._fill(blk, 0.0)
                             consume(i, si, k0, Kb, blk)
                             continue
-                        self._call("dfx_spmm_pf_adjoint", datas[i].data_ptr(), rp.data_ptr(), col.data_ptr(),
-                                   val.data_ptr(), self.coeffs_sino_C.data_ptr(), None if om is None else om.data_ptr(),
-                                   n_ang, self.My, Kb, self.N_seg, self.Kstride, alpha, compact, s)
+                        self._pf_adjoint_product(datas[i].data_ptr(), rp, col, val, self.coeffs_sino_C.data_ptr(), om,
+                                                 n_ang, Kb, alpha, compact, s)
                         if pixels is None:
                             self._call("dfx_radon_backward", self.coeffs_sino_C.data_ptr(), self._img_k.data_ptr(),
                                        geo.data_ptr(), n_ang, self.Nx, self.Ny, self.My, self.Kstride, Kb,

@@ -263,6 +263,18 @@ int dfx_spmm_pf_forward_blocked_zt(const float *sino, float *zt, int64_t zt_floa
                                    const int32_t *omegas, int n_sub, int my, int P, int C, int kstride, int kb,
                                    int max_groups, void *stream);
 
+/* The same product as dfx_spmm_pf_adjoint, bit for bit, through the data rows transposed to detector lines fastest:
+ * per chunk of angles, dt[s][j][y] (line stride 32 ceil(my / 32)) is written from the rows omegas[s] (NULL: s) of
+ * data, then one warp per orientation row and 32 lines reads each entry once and data column j as whole 128-byte
+ * segments; the outputs (alpha times the sums; 0 for kb <= k < kstride) are written as whole row segments. dt holds
+ * dt_floats floats, at least dfx_spmm_pf_adjoint_zt_floats(1, my, cp); max_groups as in
+ * dfx_spmm_pf_forward_blocked_zt. cp <= 65536. */
+int64_t dfx_spmm_pf_adjoint_zt_floats(int n_angles, int my, int cp);
+int dfx_spmm_pf_adjoint_zt(const float *data, float *dt, int64_t dt_floats, const int32_t *row_ptr,
+                           const uint16_t *col_j, const float *val, float *sino, const int32_t *omegas, int n_sub,
+                           int my, int kb, int cp, int kstride, float alpha, int compact, int max_groups,
+                           void *stream);
+
 /* replaces batched_gemm_clblast / batched_gemm_clblast_adj (SPFO:2063-2127), the products of pf_mode "dense": pf is
  * the batch's float32 PF (n_omega, kb, cp) (dfx_pf_dense); adjoint 0: out = data (n_omega, my, cp) += in (n_omega, my,
  * kstride: the Radon output) . PF per angle; adjoint 1: out (n_omega, my, kstride) = alpha in (data) . PF^T per angle,

@@ -101,3 +101,55 @@ def test_lines_fastest_blocked_forward_rejects_bad_arguments():
                                                 mg, s)
         assert rc != 0
     assert lib.dfx_spmm_pf_forward_zt_floats(0, 40, 8) < 0
+
+
+def _csr_rows(rng, n_rows, n_cols, max_len):
+    """Random CSR rows (columns ascending, distinct): (row_ptr int32, cols uint16, vals float32)."""
+    ptr, cols, vals = [0], [], []
+    for _ in range(n_rows):
+        cnt = int(rng.integers(0, max_len + 1)) if rng.random() > 0.1 else 0
+        c = np.sort(rng.choice(n_cols, size=min(cnt, n_cols), replace=False)).astype(np.uint16)
+        cols.append(c)
+        vals.append(rng.standard_normal(len(c)).astype(np.float32))
+        ptr.append(ptr[-1] + len(c))
+    c = np.concatenate(cols) if ptr[-1] else np.zeros(1, np.uint16)
+    v = np.concatenate(vals) if ptr[-1] else np.zeros(1, np.float32)
+    return np.array(ptr, np.int32), c, v
+
+
+@pytest.mark.parametrize("cp,my,kb,R,subset,compact", [
+    (2880, 263, 300, 4, None, 0),
+    (2880, 263, 1012, 3, [2, 0], 0),
+    (30, 40, 77, 4, [3, 0, 2], 1),
+    (7, 31, 33, 3, None, 0),
+    (108, 300, 64, 2, [1], 1),
+])
+@pytest.mark.parametrize("max_groups,one_angle", [(0, False), (1, True), (4, False)])
+def test_lines_fastest_adjoint_equals_adjoint(cp, my, kb, R, subset, compact, max_groups, one_angle):
+    from diffractom_b200 import _lib
+    rng = np.random.default_rng(cp + my + kb + max_groups + compact)
+    n_sub = R if subset is None else len(subset)
+    rows = (n_sub if compact else R) * kb
+    ptr, col, val = _csr_rows(rng, rows, cp, 48)
+    kstride = kb + 7
+    dev = "cuda"
+    data = torch.as_tensor(rng.standard_normal((R, my, cp)).astype(np.float32), device=dev)
+    t_ptr = torch.as_tensor(ptr, device=dev)
+    t_c = torch.as_tensor(col.view(np.int16), device=dev)
+    t_v = torch.as_tensor(val, device=dev)
+    om = None if subset is None else torch.as_tensor(np.array(subset, np.int32), device=dev)
+    om_ptr = None if om is None else om.data_ptr()
+    s = torch.cuda.current_stream().cuda_stream
+    alpha = float(np.float32(0.37))
+    a = torch.full((n_sub, my, kstride), -5.0, device=dev)
+    b = torch.full((n_sub, my, kstride), -6.0, device=dev)
+    _lib.call("dfx_spmm_pf_adjoint", data.data_ptr(), t_ptr.data_ptr(), t_c.data_ptr(), t_v.data_ptr(), a.data_ptr(),
+              om_ptr, n_sub, my, kb, cp, kstride, alpha, compact, s)
+    per = int(_lib.lib().dfx_spmm_pf_adjoint_zt_floats(1, my, cp))
+    assert per == cp * 32 * (-(-my // 32))
+    dt = torch.full((per if one_angle else per * n_sub,), float("nan"), device=dev)
+    _lib.call("dfx_spmm_pf_adjoint_zt", data.data_ptr(), dt.data_ptr(), dt.numel(), t_ptr.data_ptr(), t_c.data_ptr(),
+              t_v.data_ptr(), b.data_ptr(), om_ptr, n_sub, my, kb, cp, kstride, alpha, compact, max_groups, s)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    assert torch.all(b[:, :, kb:] == 0)
