@@ -8,7 +8,11 @@
 // uses each entry TY times from a register. Rows are sorted by column, so a thread keeps its place from one chunk to
 // the next. No atomics: every output is written by one thread. The adjoint launches spmm_adjoint8_kernel (eight lines
 // per thread, the whole data row staged at once); the forward over stored copies runs over eta blocks
-// (spmm_forward_b4_kernel), the CSR kernel serving generated copies.
+// (spmm_forward_b4_kernel), the CSR kernel serving generated copies. The lines-fastest forms turn the work around:
+// the dense operand (the Radon output for the forward, the data rows for the adjoint) is first transposed to detector
+// lines fastest, then a warp walks one row's entries with its lanes on the lines, reading every entry once and a
+// whole 128-byte segment of the column per 32 lines (spmm_forward_zt_kernel, spmm_adjoint_zt_kernel); their sums
+// are the kernels' above bit for bit.
 #include "dfx_common.cuh"
 
 #include <algorithm>
