@@ -448,10 +448,9 @@ __global__ void __launch_bounds__(256) zt_transpose_kernel(const float *__restri
 // a0 = fmaf(v, z0, a0), a1 = fmaf(v, z1, a1) in one instruction (same rounding as two fmaf)
 __device__ __forceinline__ void fma_pair(float &a0, float &a1, float v, float z0, float z1)
 {
-    asm("{\n.reg .b64 A, Z, V;\nmov.b64 A, {%0, %1};\nmov.b64 Z, {%3, %4};\nmov.b64 V, {%2, %2};\n"
-        "fma.rn.f32x2 A, V, Z, A;\nmov.b64 {%0, %1}, A;\n}"
-        : "+f"(a0), "+f"(a1)
-        : "f"(v), "f"(z0), "f"(z1));
+    const float2 r = __ffma2_rn(make_float2(v, v), make_float2(z0, z1), make_float2(a0, a1));
+    a0 = r.x;
+    a1 = r.y;
 }
 
 __device__ __forceinline__ void cp_async16(float *dst, const float *src)
@@ -581,14 +580,14 @@ __global__ void __launch_bounds__(256, 2) spmm_forward_zt_kernel(
 
 // ---- adjoint over the lines-fastest data rows ----
 // dt[s][j][y] (line stride ly, lines my .. ly - 1 zero): the data rows of one launch's angles with the detector lines
-// fastest. A warp owns AZ_KW consecutive orientation rows k of one angle, one after the other, and up to 32 ZT_G lines
-// (lane l: lines y0 + l + 32 t); per entry (j, v) of a row it reads the entry once and one coalesced 128-byte segment
-// of column j per 32 lines, four entries in flight, paired fused multiply-adds. A block's 8 warps hold 32 consecutive
-// orientations, written as whole 128-byte row segments of the Radon input through shared memory. Per output the sum
-// runs over the row's entries in order with fmaf from 0 and is scaled by alpha: spmm_adjoint8_kernel's bits.
-constexpr int AZ_KW = 4;                 // orientation rows per warp
+// fastest. A warp owns kw (1, 2 or 4) consecutive orientation rows k of one angle, one after the other, and up to
+// 32 ZT_G lines (lane l: lines y0 + l + 32 t); per entry (j, v) of a row it reads the entry once and one coalesced
+// 128-byte segment of column j per 32 lines, four entries in flight, paired fused multiply-adds. A block's 8 warps
+// hold 8 kw consecutive orientations, written as whole row segments of the Radon input through shared memory (kw is
+// the largest that still gives the launch a few waves of blocks). Per output the sum runs over the row's entries in
+// order with fmaf from 0 and is scaled by alpha: spmm_adjoint8_kernel's bits.
+constexpr int AZ_KW = 4;                 // orientation rows per warp at most
 constexpr int AZ_WARPS = 8;
-constexpr int AZ_K = AZ_KW * AZ_WARPS;   // orientations per block
 
 // dt[s][j][y] = data[r(s)][y][j] (j < cp, y < my; zero for my <= y < ly), r(s) = omegas[s] or r0 + s
 __global__ void __launch_bounds__(256) dt_transpose_kernel(const float *__restrict__ data, float *__restrict__ dt,
@@ -614,19 +613,20 @@ template <int MT>
 __global__ void __launch_bounds__(32 * AZ_WARPS, 3) spmm_adjoint_zt_kernel(
     const float *__restrict__ dt, const int32_t *__restrict__ row_ptr, const uint16_t *__restrict__ col_j,
     const float *__restrict__ val, float *__restrict__ sino, const int32_t *__restrict__ omegas, int r0, int my,
-    int ly, int kb, int cp, int kstride, float alpha, int compact)
+    int ly, int kb, int cp, int kstride, float alpha, int compact, int kw)
 {
-    extern __shared__ float s_outk[];                 // [32 MT][AZ_K + 1]
+    extern __shared__ float s_outk[];                 // [32 MT][8 kw + 1]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s = blockIdx.z;
     const int r = omegas ? __ldg(omegas + s) : r0 + s;
     const int ngroups = ly >> 5;
     const int g0 = blockIdx.y * MT;
     const int y0 = g0 * 32;
-    const int k0 = blockIdx.x * AZ_K;
+    const int nk = AZ_WARPS * kw, ldk = nk + 1;
+    const int k0 = blockIdx.x * nk;
     const float *ds = dt + (int64_t)s * cp * ly + y0 + lane;
-    for (int kk = 0; kk < AZ_KW; ++kk) {
-        const int kl = warp * AZ_KW + kk, k = k0 + kl;
+    for (int kk = 0; kk < kw; ++kk) {
+        const int kl = warp * kw + kk, k = k0 + kl;
         int i = 0, e = 0;
         if (k < kb) {
             const int64_t rr = (int64_t)(compact ? s : r) * kb + k;
@@ -668,15 +668,15 @@ __global__ void __launch_bounds__(32 * AZ_WARPS, 3) spmm_adjoint_zt_kernel(
             }
         }
 #pragma unroll
-        for (int t = 0; t < MT; ++t) s_outk[(lane + 32 * t) * (AZ_K + 1) + kl] = k < kb ? alpha * acc[t] : 0.0f;
+        for (int t = 0; t < MT; ++t) s_outk[(lane + 32 * t) * ldk + kl] = k < kb ? alpha * acc[t] : 0.0f;
     }
     __syncthreads();
     const int ny = min(32 * MT, my - y0);
-    const int kl = threadIdx.x & (AZ_K - 1), ty = threadIdx.x / AZ_K;
+    const int kl = threadIdx.x % nk, ty = threadIdx.x / nk;
     const int k = k0 + kl;
     if (k < kstride) {
         float *zl = sino + ((int64_t)s * my + y0) * kstride + k;
-        for (int yl = ty; yl < ny; yl += (32 * AZ_WARPS) / AZ_K) zl[(int64_t)yl * kstride] = s_outk[yl * (AZ_K + 1) + kl];
+        for (int yl = ty; yl < ny; yl += (32 * AZ_WARPS) / nk) zl[(int64_t)yl * kstride] = s_outk[yl * ldk + kl];
     }
 }
 
@@ -862,10 +862,16 @@ static int launch_az(const float *dt, const int32_t *row_ptr, const uint16_t *co
         set_error("spmm_adjoint_zt: shared memory attribute: %s", cudaGetErrorString(err));
         return DFX_ELAUNCH;
     }
-    const size_t smem = (size_t)32 * MT * (AZ_K + 1) * sizeof(float);
-    dim3 grid((unsigned)cdiv(kstride, AZ_K), (unsigned)nyb, (unsigned)na);
+    // orientation rows per warp: the most (of 4, 2, 1) that still gives the launch about four waves of blocks (three
+    // blocks of 8 warps per SM)
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    int kw = AZ_KW;
+    while (kw > 1 && cdiv(kstride, AZ_WARPS * kw) * nyb * na < 4LL * 3 * nsm) kw >>= 1;
+    const size_t smem = (size_t)32 * MT * (AZ_WARPS * kw + 1) * sizeof(float);
+    dim3 grid((unsigned)cdiv(kstride, AZ_WARPS * kw), (unsigned)nyb, (unsigned)na);
     spmm_adjoint_zt_kernel<MT><<<grid, 32 * AZ_WARPS, smem, st>>>(dt, row_ptr, col_j, val, sino, omegas, r0, my, ly,
-                                                                  kb, cp, kstride, alpha, compact);
+                                                                  kb, cp, kstride, alpha, compact, kw);
     return launch_status("spmm_pf_adjoint_zt");
 }
 
@@ -883,7 +889,7 @@ extern "C" int dfx_spmm_pf_adjoint_zt(const float *data, float *dt, int64_t dt_f
     const int ly = (int)(cdiv(my, 32) * 32), ngroups = ly / 32;
     const int gmax = max_groups ? max_groups : ZT_G;
     const int nyb = (int)cdiv(ngroups, gmax), mt = (int)cdiv(ngroups, nyb);
-    DFX_REQUIRE(nyb <= 65535 && cdiv(kstride, AZ_K) <= 2147483647LL, "spmm_adjoint_zt: grid too large");
+    DFX_REQUIRE(nyb <= 65535 && cdiv(kstride, AZ_WARPS) <= 2147483647LL, "spmm_adjoint_zt: grid too large");
     const int chunk = (int)std::min<int64_t>(std::min<int64_t>(n_sub, dt_floats / per_angle), 65535);
     cudaStream_t st = (cudaStream_t)stream;
     for (int s0 = 0; s0 < n_sub; s0 += chunk) {

@@ -117,7 +117,22 @@ def _csr_rows(rng, n_rows, n_cols, max_len):
     return np.array(ptr, np.int32), c, v
 
 
+def _csr_rows_fast(rng, n_rows, n_cols, max_len):
+    """As _csr_rows, vectorised (many rows)."""
+    L = np.minimum(rng.integers(0, max_len + 1, n_rows), n_cols)
+    L[rng.random(n_rows) < 0.1] = 0
+    order = np.argsort(rng.random((n_rows, n_cols)), axis=1)
+    chosen = np.where(np.arange(n_cols)[None, :] < L[:, None], order, n_cols)
+    chosen.sort(axis=1)
+    cols = chosen[chosen < n_cols].astype(np.uint16)
+    ptr = np.concatenate([[0], np.cumsum(L)]).astype(np.int32)
+    vals = rng.standard_normal(len(cols)).astype(np.float32)
+    return ptr, (cols if len(cols) else np.zeros(1, np.uint16)), (vals if len(vals) else np.zeros(1, np.float32))
+
+
 @pytest.mark.parametrize("cp,my,kb,R,subset,compact", [
+    (30, 40, 2000, 30, None, 0),          # many blocks: four orientation rows per warp
+    (30, 40, 2000, 20, None, 1),          # two per warp
     (2880, 263, 300, 4, None, 0),
     (2880, 263, 1012, 3, [2, 0], 0),
     (30, 40, 77, 4, [3, 0, 2], 1),
@@ -130,7 +145,7 @@ def test_lines_fastest_adjoint_equals_adjoint(cp, my, kb, R, subset, compact, ma
     rng = np.random.default_rng(cp + my + kb + max_groups + compact)
     n_sub = R if subset is None else len(subset)
     rows = (n_sub if compact else R) * kb
-    ptr, col, val = _csr_rows(rng, rows, cp, 48)
+    ptr, col, val = (_csr_rows if rows < 5000 else _csr_rows_fast)(rng, rows, cp, 48)
     kstride = kb + 7
     dev = "cuda"
     data = torch.as_tensor(rng.standard_normal((R, my, cp)).astype(np.float32), device=dev)
