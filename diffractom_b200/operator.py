@@ -1175,6 +1175,20 @@ class SinglePhaseForwardOperator:
         self._radon_fwd(src_ptr, self.coeffs_sino_C.data_ptr(), om, n_ang, Kb, ray=ray, m=m)
         self._pf_forward_product(ib, m, self.coeffs_sino_C.data_ptr(), data, om, n_ang, Kb)
 
+    def _direct_channel_constant(self, src_ptr, kb_src, data, ray=None):
+        """Add to data the forward projection, through every batch, of an image that is the same in every channel:
+        src_ptr holds it channel-fastest for kb_src >= every batch's K_batch channels. Its Radon transform is computed
+        once and every batch's PF product reads its own channels of it; per channel the Radon output does not depend
+        on the batch (the native projector: the same taps in the same order), so data gets the bits of
+        _direct_batch_k batch by batch."""
+        if self.projector != "native" or kb_src < max(b["K_batch"] for b in self.batches):
+            raise ValueError("_direct_channel_constant needs the native projector and the widest batch's channels")
+        geo, n_ang, om, m = self._geo_of(None)
+        sino = self.coeffs_sino_C.data_ptr()
+        self._radon_fwd(src_ptr, sino, om, n_ang, kb_src, ray=ray, m=m)
+        for ib, b in enumerate(self.batches):
+            self._pf_forward_product(ib, m, sino, data, om, n_ang, b["K_batch"])
+
     def _pf_adjoint_to_sino(self, data, ib, subset):
         Kb = self.batches[ib]["K_batch"]
         geo, n_ang, om, m = self._geo_of(subset)

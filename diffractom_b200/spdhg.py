@@ -618,6 +618,12 @@ class SPDHGPoisson:
                               0.0, 0, s)
                     op._radon_forward_bf16(self.dzk.data_ptr(), ib, z, om, n, row0=a)
                 op._pf_tc_forward(z, om, n, self.D)
+        elif op.projector == "native":
+            # 1_S is the same image in every channel: one Radon transform (the widest batch's channels) serves every
+            # batch's PF product, the bits of the batch-by-batch passes
+            kbm = max(bt["K_batch"] for bt in op.batches)
+            _lib.call("dfx_batch_support", self.dzk.data_ptr(), None, sp, npix, op.Kstride, kbm, 0.0, 0, s)
+            op._direct_channel_constant(self.dzk.data_ptr(), kbm, self.D, ray=self._ray)
         else:
             for ib, bt in enumerate(op.batches):
                 _lib.call("dfx_batch_support", self.dzk.data_ptr(), None, sp, npix, op.Kstride, bt["K_batch"], 0.0,

@@ -322,3 +322,35 @@ def test_pf_storage_modes_compute_the_same_operator(golden):
             assert np.array_equal(a, b), name
     with pytest.raises(MemoryError):
         make_operator(d, pf_mode="sparse", sparse_max_gb=part)
+
+
+@pytest.mark.parametrize("pf_mode", ["sparse", "generated"])
+def test_channel_constant_forward_equals_batch_by_batch(golden, pf_mode):
+    """_direct_channel_constant (one Radon transform of an image that is the same in every channel, read by every
+    batch's PF product; the step sizes' row sums A 1_S) gives the bits of the forward batch by batch, with the full
+    ray table and with a support's table, for batches of different widths."""
+    d = golden("al5_small")
+    op = make_operator(d, pf_mode=pf_mode)
+    widths = [b["K_batch"] for b in op.batches]
+    assert len(widths) > 1
+    kbm = max(widths)
+    npix, ks = op.Nx * op.Ny, op.Kstride
+    rng = np.random.default_rng(11)
+    supp = torch.as_tensor(op.support_mask().ravel().astype(np.uint8), device="cuda")
+    pattern = torch.as_tensor(rng.random(npix).astype(np.float32), device="cuda") * supp.float()
+    for ray in (None, op.support_ray_table(supp)):
+        img = torch.zeros((npix, ks), device="cuda")
+        img[:, :kbm] = pattern[:, None]
+        one = torch.zeros(op.data_shape, device="cuda")
+        torch.cuda.synchronize()
+        op._direct_channel_constant(img.data_ptr(), kbm, one, ray=ray)
+        torch.cuda.synchronize()
+        each = torch.zeros(op.data_shape, device="cuda")
+        for ib, kb in enumerate(widths):
+            imb = torch.zeros((npix, ks), device="cuda")
+            imb[:, :kb] = pattern[:, None]
+            torch.cuda.synchronize()
+            op._direct_batch_k(imb.data_ptr(), ib, each, ray=ray)
+            torch.cuda.synchronize()
+        assert torch.equal(one, each)
+        assert float(one.abs().max()) > 0
