@@ -64,7 +64,8 @@ class SinglePhaseForwardOperator:
     # whole 128-byte segments of a data column per entry; dfx_spmm_pf_adjoint_zt, the same bits) through the same
     # buffer; False: dfx_spmm_pf_adjoint on the segment-fastest rows
     adjoint_lines_fastest = True
-    zt_max_angles = 64
+    zt_max_angles = 64                   # angles per transpose chunk at most
+    zt_max_bytes = 256 * 1024 ** 2       # the transpose buffer at most (at least one angle)
     zt_max_groups = 0
 
     def __init__(self, cfg: Mapping[str, Any], material, grid, max_gb: float, verbose: bool = False,
@@ -539,13 +540,13 @@ class SinglePhaseForwardOperator:
 
     def _zt_floats(self):
         kmax = max(b["K_batch"] for b in self.batches)
-        na = max(1, min(int(self.zt_max_angles), self.N_Omega))
-        n = 0
+        per = 0                                          # floats per angle of the widest use
         if self.forward_lines_fastest:
-            n = int(self._lib.dfx_spmm_pf_forward_zt_floats(na, self.My, kmax))
+            per = int(self._lib.dfx_spmm_pf_forward_zt_floats(1, self.My, kmax))
         if self.adjoint_lines_fastest:
-            n = max(n, int(self._lib.dfx_spmm_pf_adjoint_zt_floats(na, self.My, self.N_seg)))
-        return n
+            per = max(per, int(self._lib.dfx_spmm_pf_adjoint_zt_floats(1, self.My, self.N_seg)))
+        na = min(int(self.zt_max_angles), self.N_Omega, int(self.zt_max_bytes) // max(4 * per, 1))
+        return max(1, na) * per
 
     def _zt_buffer(self):
         """The lines-fastest copy of the Radon output the blocked forward reads, or of the data rows the adjoint
