@@ -99,6 +99,7 @@ __device__ __forceinline__ int window_start(const AngleGeo &g, int px0, int py0,
     return min(max(sf, 0), ns - 1);
 }
 
+constexpr int PREFETCH_ROUNDS = 1;             // epilogue: L2 prefetch of x, z, T this many rounds ahead (2: slower)
 constexpr int TP_EPI0 = 5;                     // first epilogue warp
 constexpr int TP_EPI_WARPS = 8;
 constexpr int TP_THREADS = (TP_EPI0 + TP_EPI_WARPS) * 32;   // 416
@@ -147,6 +148,22 @@ __device__ __forceinline__ void tile_origin(const TbArgs &p, int t, int &px0, in
     px0 = (pt % p.tiles_x) * TB_TX;
     py0 = (pt / p.tiles_x) * TB_TY;
     k0 = cb * TB_N;
+}
+
+// L2 prefetch of one epilogue round: the rows of x, z and T of the 4 pixels px .. px + 3 of image row qy, 128
+// channels from kc (48 lines of 128 B; lane l takes lines l and l + 32); pixels and channels outside are skipped
+__device__ __forceinline__ void prefetch_round(const TbArgs &p, int qy, int px, int kc, int lane)
+{
+    if (qy >= p.ny) return;
+    const int nv = min(4, p.nx - px);
+    const int64_t nb = ((int64_t)qy * p.nx + px) * p.kstride + kc;
+    for (int L = lane; L < 48; L += 32) {
+        const int u = L / 12, arr = (L >> 2) % 3, c = L & 3;
+        if (u < nv && kc + 32 * c < p.kb) {
+            const float *src = arr == 0 ? p.x : (arr == 1 ? p.z : p.T);
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(src + nb + (int64_t)u * p.kstride + 32 * c));
+        }
+    }
 }
 
 template <int KERNEL>
@@ -342,6 +359,25 @@ __global__ void __launch_bounds__(TP_THREADS, 1) tc_backproject_spdhg(const __gr
                     for (int r0 = 0; r0 < 16; r0 += 4) {
                         const int nv = min(4, p.nx - (px0 + r0));     // pixels of these 4 rows inside the image
                         const int64_t base = ((int64_t)qy * p.nx + px0 + r0) * ks + k;
+                        if (PREFETCH_ROUNDS > 0) {
+                            // the rows of x, z and T of the round PREFETCH_ROUNDS ahead into L2 while these are
+                            // loaded and stepped: 4 pixels further, else in the next channel half, else in the CTA's
+                            // next tile
+                            int rr = r0 / 4 + PREFETCH_ROUNDS, hh = h, tt = t, tx0 = px0, ty0 = py0, tk0 = k0,
+                                tnh = nh;
+                            while (rr >= 4 && tt < n_tiles) {
+                                rr -= 4;
+                                if (++hh >= tnh) {
+                                    hh = 0;
+                                    tt += gridDim.x;
+                                    if (tt < n_tiles) {
+                                        tile_origin(p, tt, tx0, ty0, tk0);
+                                        tnh = (tk0 + 128 < p.kb) ? 2 : 1;
+                                    }
+                                }
+                            }
+                            if (tt < n_tiles) prefetch_round(p, ty0 + ew, tx0 + 4 * rr, tk0 + hh * 128, lane);
+                        }
                         float4 xv[4], zv[4], tv[4];
 #pragma unroll
                         for (int u = 0; u < 4; ++u) {
