@@ -454,19 +454,6 @@ __global__ void __launch_bounds__(32 * WARPS) radon_backward_v3(
     }
     const int px = (int)(pix % nx), py = (int)(pix / nx);
     const float fx = (float)px, fy = (float)py;
-    if (MODE == 1) {
-        // this pixel's rows of x, z and T (P x 256 channels, 8 lines of 128 B each) into L2 while the angles are
-        // summed, so that the primal step below does not wait on DRAM
-        const int64_t o0 = p * kstride + kblk;
-        const int arr = lane >> 3, c = lane & 7;          // lanes 0-23: array (x, z, T) and line
-#pragma unroll
-        for (int h = 0; h < P; ++h) {
-            if (lane < 24 && data[h] && kblk + h * CPW + 32 * c < kstride) {
-                const float *src = arr == 0 ? img : (arr == 1 ? z : T);
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(src + o0 + h * CPW + 32 * c));
-            }
-        }
-    }
     float acc[P][CPL];
 #pragma unroll
     for (int h = 0; h < P; ++h)
