@@ -414,15 +414,17 @@ __global__ void __launch_bounds__(SP_ROWS) spmm_forward_b4_kernel(
 
 // ---- blocked forward over the lines-fastest sinogram ----
 // zt[s][k][y] (line stride ly = 32 * groups, lines my .. ly - 1 zero) is the Radon output of one launch's angles with
-// the detector lines fastest. A warp owns one block row (four eta bins of one ring) of one angle and up to 32 ZT_G
-// lines: lane l holds the lines y0 + l + 32 t. Per entry the warp reads the entry once (the same address in every
-// lane) and one coalesced 128-byte segment of Z column k per 32 lines, four entries in flight, and applies the
+// the detector lines fastest. A warp applies one block row (four eta bins of one ring) of one angle at a time to up
+// to 32 ZT_G lines: lane l holds the lines y0 + l + 32 t. Per entry the warp reads the entry once (the same address in
+// every lane) and one coalesced 128-byte segment of Z column k per 32 lines, four entries in flight, and applies the
 // entry's four values with paired fused multiply-adds (fma.rn.f32x2: two IEEE fmaf in one instruction, lines t and
-// t + 1). A block holds the G * P block rows of G consecutive eta blocks (all rings; ring groups of at most 8 above
-// 8 rings), whose outputs j = 4 cb P .. 4 (cb + G) P - 1 are contiguous in a data row. The block copies those data
-// row segments into shared memory (cp.async) when it starts, so the epilogue adds each output to its old value there
-// and only stores. The sums per output run over the block row's entries in order with fmaf, each added once to the
-// data row, as in spmm_forward_b4_kernel: the results are that kernel's (and the CSR kernel's) bit for bit.
+// t + 1). A block of 8 warps owns the block rows of nb consecutive eta blocks, all rings (nb * P <= 16 rows; one eta
+// block above 16 rings), whose outputs j = 4 cb P .. 4 (cb + nb) P - 1 are contiguous in a data row. The rows differ
+// in length, so the warps take them longest first from a shared counter instead of one row each: the block no longer
+// waits for its longest row with most warps idle. The sums go to shared memory; the block's data row segments, put in
+// L2 by a prefetch when the block starts, are then read a batch of lines at a time and written back whole. The sums
+// per output run over the block row's entries in order with fmaf, each added once to the data row, as in
+// spmm_forward_b4_kernel: the results are that kernel's (and the CSR kernel's) bit for bit.
 constexpr int ZT_G = 9;                  // 32-line groups per warp at most (288 lines)
 constexpr int ZT_U = 4;                  // entries in flight per warp
 constexpr int ZT_TR = 32;                // transpose tile
@@ -453,116 +455,117 @@ __device__ __forceinline__ void fma_pair(float &a0, float &a1, float v, float z0
     a1 = r.y;
 }
 
-__device__ __forceinline__ void cp_async16(float *dst, const float *src)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
-}
-
-__device__ __forceinline__ void cp_async4(float *dst, const float *src)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
-}
+constexpr int ZT_ROWS_MAX = 32;         // block rows per block at most (one eta block of 32 rings)
+constexpr int ZT_NB_LINES = 9;           // data row lines read per batch in the write-back
 
 template <int MT>
 __global__ void __launch_bounds__(256, 2) spmm_forward_zt_kernel(
     const float *__restrict__ zt, const int32_t *__restrict__ fb_ptr, const uint16_t *__restrict__ fb_k,
     const float4 *__restrict__ fb_v, const uint8_t *__restrict__ fb_mask, float *__restrict__ data,
-    const int32_t *__restrict__ omegas, int r0, int my, int ly, int P, int PW, int nrg, int C, int ncb, int G,
-    int kb)
+    const int32_t *__restrict__ omegas, int r0, int my, int ly, int P, int C, int ncb, int nb, int kb)
 {
-    extern __shared__ __align__(16) float s_dyn[];
-    __shared__ uint8_t s_own[FB_W * 32];              // output j of the block written (its bin's row has entries)
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    extern __shared__ __align__(16) float s_out[];    // [32 MT][width + 1]: the block's sums
+    __shared__ uint8_t s_own[FB_W * ZT_ROWS_MAX];      // output j of the block written (its bin's row has entries)
+    __shared__ int s_order[ZT_ROWS_MAX];               // the block's rows, longest first
+    __shared__ int s_next;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int s = blockIdx.z;
     const int r = omegas ? __ldg(omegas + s) : r0 + s;
     const int ngroups = ly >> 5;
     const int g0 = blockIdx.y * MT;                   // first 32-line group of the block
     const int y0 = g0 * 32;
-    const int cbg = blockIdx.x / nrg, rg = blockIdx.x - cbg * nrg;
-    const int cbw = warp / PW, p = rg * PW + (warp - cbw * PW);
-    const int cb = cbg * G + cbw;
-    const int width = FB_W * G * P, wp = width + 1;
+    const int cb0 = blockIdx.x * nb;
+    const int nrows = nb * P;                         // row q: eta block cb0 + q / P, ring q % P
+    const int width = FB_W * nb * P, wp = width + 1;
     const int cp = C * P;
-    const int j0 = FB_W * cbg * G * P;                // first output of the block in a data row
+    const int j0 = FB_W * cb0 * P;                    // first output of the block in a data row
     const int wj = min(width, cp - j0);
     const int ny = min(32 * MT, my - y0);
-    float *s_out = s_dyn;                             // [32 MT][wp]: the block's sums
-    float *s_old = s_dyn + 32 * MT * wp;              // [32 MT][width]: the data row segments before the launch
     float *drow = data + ((int64_t)r * my + y0) * cp + j0;
-    for (int t = threadIdx.x; t < width; t += blockDim.x) s_own[t] = 0;
-    if ((cp & 3) == 0) {                              // rows and segments 16-byte aligned (j0, width multiples of 4)
-        const int q4 = wj >> 2;
-        for (int idx = threadIdx.x; idx < ny * q4; idx += blockDim.x) {
-            const int yl = idx / q4, c = idx - yl * q4;
-            cp_async16(s_old + yl * width + 4 * c, drow + (int64_t)yl * cp + 4 * c);
-        }
-    } else {
-        for (int idx = threadIdx.x; idx < ny * wj; idx += blockDim.x) {
-            const int yl = idx / wj, c = idx - yl * wj;
-            cp_async4(s_old + yl * width + c, drow + (int64_t)yl * cp + c);
-        }
+    // the data row segments into L2 while the rows are summed (read and written back at the end)
+    const int lines = (wj + 31) >> 5;
+    for (int idx = tid; idx < ny * lines; idx += blockDim.x) {
+        const int yl = idx / lines, c = idx - yl * lines;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(drow + (int64_t)yl * cp + 32 * c));
     }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    int i = 0, e = 0, m = 0;
-    if (cb < ncb && p < P) {
-        const int64_t g = (int64_t)r * P * ncb + (int64_t)cb * P + p;
-        i = __ldg(fb_ptr + g);
-        e = __ldg(fb_ptr + g + 1);
-        m = __ldg(fb_mask + g);
+    for (int t = tid; t < width; t += blockDim.x) s_own[t] = 0;
+    if (warp == 0) {                                  // rank of every row by length (ties: lower row first)
+        int len = -1;
+        if (lane < nrows) {
+            const int cb = cb0 + lane / P, p = lane - (lane / P) * P;
+            if (cb < ncb) {
+                const int64_t g = (int64_t)r * P * ncb + (int64_t)cb * P + p;
+                len = __ldg(fb_ptr + g + 1) - __ldg(fb_ptr + g);
+            }
+        }
+        int rank = 0;
+        for (int j = 0; j < nrows; ++j) {
+            const int lj = __shfl_sync(0xffffffffu, len, j);
+            rank += (lj > len || (lj == len && j < lane)) ? 1 : 0;
+        }
+        if (lane < nrows) s_order[rank] = lane;
+        if (lane == 0) s_next = 0;
     }
-    float acc[FB_W][MT];
-#pragma unroll
-    for (int u = 0; u < FB_W; ++u)
-#pragma unroll
-        for (int t = 0; t < MT; ++t) acc[u][t] = 0.0f;
+    __syncthreads();
     const float *zs = zt + (int64_t)s * kb * ly + y0 + lane;
-    int kq[ZT_U];
-    float4 vq[ZT_U];
+    while (true) {
+        int idx = 0;
+        if (lane == 0) idx = atomicAdd(&s_next, 1);
+        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (idx >= nrows) break;
+        const int q = s_order[idx], cbw = q / P, p = q - cbw * P, cb = cb0 + cbw;
+        if (cb >= ncb) continue;
+        const int64_t g = (int64_t)r * P * ncb + (int64_t)cb * P + p;
+        int i = __ldg(fb_ptr + g);
+        const int e = __ldg(fb_ptr + g + 1);
+        const int m = __ldg(fb_mask + g);
+        float acc[FB_W][MT];
 #pragma unroll
-    for (int q = 0; q < ZT_U; ++q) {
-        kq[q] = i + q < e ? __ldg(fb_k + i + q) : 0;
-        vq[q] = i + q < e ? __ldg(fb_v + i + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    for (; i < e; i += ZT_U) {
-        float4 vc[ZT_U];
-        float z[ZT_U][MT];
+        for (int u = 0; u < FB_W; ++u)
 #pragma unroll
-        for (int q = 0; q < ZT_U; ++q) {
-            vc[q] = vq[q];
-            const float *zc = zs + (int64_t)kq[q] * ly;
+            for (int t = 0; t < MT; ++t) acc[u][t] = 0.0f;
+        int kq[ZT_U];
+        float4 vq[ZT_U];
 #pragma unroll
-            for (int t = 0; t < MT; ++t) z[q][t] = g0 + t < ngroups ? __ldg(zc + 32 * t) : 0.0f;
+        for (int qq = 0; qq < ZT_U; ++qq) {
+            kq[qq] = i + qq < e ? __ldg(fb_k + i + qq) : 0;
+            vq[qq] = i + qq < e ? __ldg(fb_v + i + qq) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
+        for (; i < e; i += ZT_U) {
+            float4 vc[ZT_U];
+            float z[ZT_U][MT];
 #pragma unroll
-        for (int q = 0; q < ZT_U; ++q) {              // the next entries' loads go out while these are applied
-            kq[q] = i + ZT_U + q < e ? __ldg(fb_k + i + ZT_U + q) : 0;
-            vq[q] = i + ZT_U + q < e ? __ldg(fb_v + i + ZT_U + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
+            for (int qq = 0; qq < ZT_U; ++qq) {
+                vc[qq] = vq[qq];
+                const float *zc = zs + (int64_t)kq[qq] * ly;
 #pragma unroll
-        for (int q = 0; q < ZT_U; ++q) {
-            if (i + q < e) {
+                for (int t = 0; t < MT; ++t) z[qq][t] = g0 + t < ngroups ? __ldg(zc + 32 * t) : 0.0f;
+            }
 #pragma unroll
-                for (int t = 0; t + 1 < MT; t += 2) {
-                    fma_pair(acc[0][t], acc[0][t + 1], vc[q].x, z[q][t], z[q][t + 1]);
-                    fma_pair(acc[1][t], acc[1][t + 1], vc[q].y, z[q][t], z[q][t + 1]);
-                    fma_pair(acc[2][t], acc[2][t + 1], vc[q].z, z[q][t], z[q][t + 1]);
-                    fma_pair(acc[3][t], acc[3][t + 1], vc[q].w, z[q][t], z[q][t + 1]);
-                }
-                if (MT & 1) {
-                    acc[0][MT - 1] = __fmaf_rn(vc[q].x, z[q][MT - 1], acc[0][MT - 1]);
-                    acc[1][MT - 1] = __fmaf_rn(vc[q].y, z[q][MT - 1], acc[1][MT - 1]);
-                    acc[2][MT - 1] = __fmaf_rn(vc[q].z, z[q][MT - 1], acc[2][MT - 1]);
-                    acc[3][MT - 1] = __fmaf_rn(vc[q].w, z[q][MT - 1], acc[3][MT - 1]);
+            for (int qq = 0; qq < ZT_U; ++qq) {        // the next entries' loads go out while these are applied
+                kq[qq] = i + ZT_U + qq < e ? __ldg(fb_k + i + ZT_U + qq) : 0;
+                vq[qq] = i + ZT_U + qq < e ? __ldg(fb_v + i + ZT_U + qq) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int qq = 0; qq < ZT_U; ++qq) {
+                if (i + qq < e) {
+#pragma unroll
+                    for (int t = 0; t + 1 < MT; t += 2) {
+                        fma_pair(acc[0][t], acc[0][t + 1], vc[qq].x, z[qq][t], z[qq][t + 1]);
+                        fma_pair(acc[1][t], acc[1][t + 1], vc[qq].y, z[qq][t], z[qq][t + 1]);
+                        fma_pair(acc[2][t], acc[2][t + 1], vc[qq].z, z[qq][t], z[qq][t + 1]);
+                        fma_pair(acc[3][t], acc[3][t + 1], vc[qq].w, z[qq][t], z[qq][t + 1]);
+                    }
+                    if (MT & 1) {
+                        acc[0][MT - 1] = __fmaf_rn(vc[qq].x, z[qq][MT - 1], acc[0][MT - 1]);
+                        acc[1][MT - 1] = __fmaf_rn(vc[qq].y, z[qq][MT - 1], acc[1][MT - 1]);
+                        acc[2][MT - 1] = __fmaf_rn(vc[qq].z, z[qq][MT - 1], acc[2][MT - 1]);
+                        acc[3][MT - 1] = __fmaf_rn(vc[qq].w, z[qq][MT - 1], acc[3][MT - 1]);
+                    }
                 }
             }
         }
-    }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    __syncthreads();                                  // s_own cleared, s_old in place
-    if (p < P) {                                      // local j of bin u = (4 cbw + u) P + p
-        const int jl = FB_W * cbw * P + p;
+        const int jl = FB_W * cbw * P + p;            // local j of bin u: (4 cbw + u) P + p
 #pragma unroll
         for (int u = 0; u < FB_W; ++u) {
 #pragma unroll
@@ -571,11 +574,24 @@ __global__ void __launch_bounds__(256, 2) spmm_forward_zt_kernel(
         }
     }
     __syncthreads();
-    const int rows_per_pass = blockDim.x / width;     // at least 1: width = 4 G P <= 32 G PW = blockDim
-    const int tj = threadIdx.x % width, ty = threadIdx.x / width;
-    if (ty < rows_per_pass && s_own[tj])
-        for (int yl = ty; yl < ny; yl += rows_per_pass)
-            drow[(int64_t)yl * cp + tj] = s_old[yl * width + tj] + s_out[yl * wp + tj];
+    // write-back: per pass rows_per_pass lines of the segment, the old values of ZT_NB_LINES passes loaded first
+    const int rows_per_pass = blockDim.x / width;     // at least 2: width <= 128
+    const int tj = tid % width, ty = tid / width;
+    if (ty < rows_per_pass && s_own[tj]) {
+        for (int yb = ty; yb < ny; yb += ZT_NB_LINES * rows_per_pass) {
+            float old[ZT_NB_LINES];
+#pragma unroll
+            for (int n = 0; n < ZT_NB_LINES; ++n) {
+                const int yl = yb + n * rows_per_pass;
+                old[n] = yl < ny ? drow[(int64_t)yl * cp + tj] : 0.0f;
+            }
+#pragma unroll
+            for (int n = 0; n < ZT_NB_LINES; ++n) {
+                const int yl = yb + n * rows_per_pass;
+                if (yl < ny) drow[(int64_t)yl * cp + tj] = old[n] + s_out[yl * wp + tj];
+            }
+        }
+    }
 }
 
 // ---- adjoint over the lines-fastest data rows ----
@@ -775,19 +791,18 @@ extern "C" int64_t dfx_spmm_pf_forward_zt_floats(int n_angles, int my, int kb)
 template <int MT>
 static int launch_zt(const float *zt, const int32_t *fb_ptr, const uint16_t *fb_k, const float *fb_v,
                      const uint8_t *fb_mask, float *data, const int32_t *omegas, int r0, int na, int my, int ly,
-                     int nyb, int P, int PW, int nrg, int C, int ncb, int G, int kb, cudaStream_t st)
+                     int nyb, int P, int C, int ncb, int nb, int kb, cudaStream_t st)
 {
     const cudaError_t err = allow_max_dynamic_smem(spmm_forward_zt_kernel<MT>);
     if (err != cudaSuccess) {
         set_error("spmm_forward_blocked_zt: shared memory attribute: %s", cudaGetErrorString(err));
         return DFX_ELAUNCH;
     }
-    const int width = FB_W * G * P;
-    const size_t smem = ((size_t)32 * MT * (width + 1) + (size_t)32 * MT * width) * sizeof(float);
-    dim3 grid((unsigned)(cdiv(ncb, G) * nrg), (unsigned)nyb, (unsigned)na);
-    spmm_forward_zt_kernel<MT><<<grid, 32 * G * PW, smem, st>>>(
-        zt, fb_ptr, fb_k, reinterpret_cast<const float4 *>(fb_v), fb_mask, data, omegas, r0, my, ly, P, PW, nrg, C,
-        ncb, G, kb);
+    const int width = FB_W * nb * P;
+    const size_t smem = (size_t)32 * MT * (width + 1) * sizeof(float);
+    dim3 grid((unsigned)cdiv(ncb, nb), (unsigned)nyb, (unsigned)na);
+    spmm_forward_zt_kernel<MT><<<grid, 256, smem, st>>>(zt, fb_ptr, fb_k, reinterpret_cast<const float4 *>(fb_v),
+                                                        fb_mask, data, omegas, r0, my, ly, P, C, ncb, nb, kb);
     return launch_status("spmm_pf_forward_blocked_zt");
 }
 
@@ -807,9 +822,8 @@ extern "C" int dfx_spmm_pf_forward_blocked_zt(const float *sino, float *zt, int6
     DFX_REQUIRE(max_groups >= 0 && max_groups <= ZT_G, "spmm_forward_blocked_zt: max_groups outside 0 .. 9");
     const int gmax = max_groups ? max_groups : ZT_G;
     const int nyb = (int)cdiv(ngroups, gmax), mt = (int)cdiv(ngroups, nyb);
-    // blocks of G eta blocks x PW rings, at most 8 warps: G = 8 / P below 8 rings, else ring groups of <= 8
-    const int G = P >= 8 ? 1 : 8 / P;
-    const int nrg = (int)cdiv(P, 8), PW = (int)cdiv(P, nrg);
+    // blocks of nb eta blocks x all rings: at most 16 rows (one eta block above 16 rings)
+    const int nb = P >= 16 ? 1 : 16 / P;
     const int ncb = (int)cdiv(C, FB_W);
     DFX_REQUIRE(nyb <= 65535 && cdiv(kb, ZT_TR) <= 2147483647LL, "spmm_forward_blocked_zt: grid too large");
     const int chunk = (int)std::min<int64_t>(std::min<int64_t>(n_sub, zt_floats / per_angle), 65535);
@@ -824,8 +838,7 @@ extern "C" int dfx_spmm_pf_forward_blocked_zt(const float *sino, float *zt, int6
         switch (mt) {
 #define DFX_ZT_CASE(M)                                                                                                 \
     case M:                                                                                                            \
-        rc = launch_zt<M>(zt, fb_ptr, fb_k, fb_v, fb_mask, data, om, s0, na, my, ly, nyb, P, PW, nrg, C, ncb, G, kb, \
-                          st);                                                                                 \
+        rc = launch_zt<M>(zt, fb_ptr, fb_k, fb_v, fb_mask, data, om, s0, na, my, ly, nyb, P, C, ncb, nb, kb, st);       \
         break;
             DFX_ZT_CASE(1)
             DFX_ZT_CASE(2)
