@@ -254,8 +254,8 @@ int dfx_spmm_pf_forward_blocked(const float *sino, const int32_t *fb_ptr, const 
 
 /* The same product as dfx_spmm_pf_forward_blocked, bit for bit (the same sums in the same order), through the
  * Radon output transposed to detector lines fastest: per chunk of angles, zt[s][k][y] (line stride 32 ceil(my / 32))
- * is written from sino, then one warp per block row and 32 lines reads each entry once and Z column k as whole
- * 128-byte segments. zt holds zt_floats floats, at least dfx_spmm_pf_forward_zt_floats(1, my, kb) (one angle); the
+ * is written from sino, then each warp takes block rows (a block's rows longest first) and, per row, reads each entry
+ * once and Z column k as whole 128-byte segments, 32 lines per lane group. zt holds zt_floats floats, at least dfx_spmm_pf_forward_zt_floats(1, my, kb) (one angle); the
  * angles run in chunks of what fits. max_groups: 32-line groups per warp at most (1 .. 9; 0: 9). P <= 32 rings. */
 int64_t dfx_spmm_pf_forward_zt_floats(int n_angles, int my, int kb);
 int dfx_spmm_pf_forward_blocked_zt(const float *sino, float *zt, int64_t zt_floats, const int32_t *fb_ptr,
