@@ -46,3 +46,21 @@ def test_status_codes_map_to_exceptions():
     with pytest.raises(ValueError, match="null pointer"):
         _lib.check(st)
     assert lib.dfx_scan_scratch_bytes(10) >= 8
+
+
+def test_lines_fastest_buffer_sizes():
+    """The transpose buffers of the lines-fastest PF products, host-side queries: angles x columns x lines rounded up
+    to 32; a bad size gives -1. The entry points reject null pointers on the host, before any launch."""
+    from diffractom_b200 import _lib
+    lib = _lib.lib()
+    assert lib.dfx_spmm_pf_forward_zt_floats(18, 263, 1012) == 18 * 1012 * 288
+    assert lib.dfx_spmm_pf_forward_zt_floats(1, 32, 5) == 5 * 32
+    assert lib.dfx_spmm_pf_adjoint_zt_floats(360, 263, 2880) == 360 * 2880 * 288
+    assert lib.dfx_spmm_pf_adjoint_zt_floats(2, 33, 7) == 2 * 7 * 64
+    for f in (lib.dfx_spmm_pf_forward_zt_floats, lib.dfx_spmm_pf_adjoint_zt_floats):
+        assert f(0, 10, 10) == -1 and f(1, 0, 10) == -1 and f(1, 10, 0) == -1
+    st = lib.dfx_spmm_pf_forward_blocked_zt(None, None, 0, None, None, None, None, None, None, 1, 8, 8, 4, 8, 8, 0,
+                                            None)
+    assert st == _lib.DFX_EINVAL
+    st = lib.dfx_spmm_pf_adjoint_zt(None, None, 0, None, None, None, None, None, 1, 8, 8, 8, 8, 1.0, 0, 0, None)
+    assert st == _lib.DFX_EINVAL
